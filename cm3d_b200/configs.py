@@ -1,0 +1,325 @@
+"""Synthetic workloads written in CM3D's own input formats.
+
+Every workload the engine is measured on is generated here, seeded, and can be
+written out as a complete CM3D input deck (keyword file, ``~mol_def`` set file,
+``~mol_name_def`` topology, ``~inter_parm``/``~bond_parm``/``~bend_parm``
+parameter base and an ``istart{2}`` restart file holding positions *and*
+velocities), so that CM3D itself and this engine start from bit-identical
+initial conditions.
+
+Formats follow CM3D's readers:
+  keyword file      input/md_readsim.c, input/md_setsimkey.c
+  set file          input/md_readset.c:46-48        (~mol_def)
+  topology          input/md_getmols.c:48-51,162-165 (~mol_name_def, ~atom_def,
+                                                     ~bond_def, ~bend_def)
+  parameter base    input/md_getparm.c:73-143        (~inter_parm) and
+                    input/md_searchbase.c            (~bond_parm, ~bend_parm)
+  restart (istart 2) input/md_readpos.c:137-227
+
+Units are CM3D's (include/md_numbers.h): energy in K, length in Angstrom,
+time in ps, mass in amu*MCONV, charge in e*sqrt(CCONV).  Bond force constants
+follow the 1/2 k (x - x0)^2 convention (energy/intra/md_fbond.c) and bend
+equilibrium angles are given in degrees (input/md_searchbase.c:571).
+"""
+from __future__ import annotations
+
+import math
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+# include/md_numbers.h
+KCAL = 503.22289                      # K per kcal/mol
+BOLTS = 1.38065812e-23
+DCONV = BOLTS * 1.0e23
+MCONV = 10.0 / (6.022045 * DCONV)     # g/mol -> K ps^2 / A^2
+CCONV = 167102.4                      # e^2 -> K A
+TCONV = 1.0e-3                        # fs -> ps (input/md_readsim.c:474)
+
+# water model shared by the water configurations (flexible 3-site)
+WATER = dict(q_o=-0.8476, q_h=0.4238, sig_oo=3.166, eps_oo=0.1553 * KCAL,
+             m_o=15.9994, m_h=1.008, r0=1.0, k_bond=1059.0 * KCAL,
+             theta0=109.47, k_bend=75.9 * KCAL)
+WATER_SPACING = 49.66 / 16.0          # 1.0 g/cm^3 on a cubic molecular grid
+
+ARGON = dict(sig=3.405, eps=0.2381 * KCAL, mass=39.948)
+
+
+@dataclass
+class Workload:
+    """A complete, seeded simulation set-up in CM3D's vocabulary."""
+    name: str
+    keywords: dict                       # \keyword{value} pairs of the input file
+    species: list                        # [(mol_name, nmol, topology text)]
+    inter_parms: list                    # ~inter_parm texts
+    bond_parms: list = field(default_factory=list)
+    bend_parms: list = field(default_factory=list)
+    pos: np.ndarray = None               # (N, 3) Angstrom
+    vel: np.ndarray = None               # (N, 3) Angstrom / ps
+    mass_amu: np.ndarray = None          # (N,)
+    box: float = 0.0                     # cubic edge, Angstrom
+    temp: float = 0.0
+    dt_fs: float = 1.0
+
+    @property
+    def natoms(self) -> int:
+        return int(self.pos.shape[0])
+
+    # ------------------------------------------------------------- writers
+    def input_text(self) -> str:
+        lines = [f"\\{k}{{{v}}}" for k, v in self.keywords.items()]
+        return "\n".join(lines) + "\n"
+
+    def set_text(self) -> str:
+        out = []
+        for idx, (mol, nmol, _top) in enumerate(self.species, start=1):
+            out.append(f"~mol_def[\\mol_parm_file{{{mol}.top}} "
+                       f"\\mol_therm_opt{{none}} \\nmol{{{nmol}}} "
+                       f"\\mol_index{{{idx}}}]")
+        return "\n".join(out) + "\n"
+
+    def database_text(self) -> str:
+        return "\n".join(self.inter_parms + self.bond_parms + self.bend_parms) + "\n"
+
+    def restart_text(self) -> str:
+        """istart{2} restart: header, averages, x v per atom, hmat, vvol9."""
+        n = self.natoms
+        dt_ps = self.dt_fs * TCONV
+        rows = [f"0 {n} 0 0 0 {self.temp!r} 0 {dt_ps!r}",
+                " ".join(["0"] * 8), " ".join(["0"] * 10), " ".join(["0"] * 5),
+                " ".join(["0"] * 9)]
+        fmt = "%.17g %.17g %.17g %.17g %.17g %.17g"
+        for i in range(n):
+            rows.append(fmt % (*self.pos[i], *self.vel[i]))
+        L = self.box
+        rows += [f"{L!r} 0 0", f"0 {L!r} 0", f"0 0 {L!r}"]
+        rows += ["0 0 0"] * 3
+        return "\n".join(rows) + "\n"
+
+    def write(self, directory: str) -> str:
+        """Write the full input deck; returns the keyword-file path."""
+        os.makedirs(directory, exist_ok=True)
+        for mol, _n, top in self.species:
+            with open(os.path.join(directory, f"{mol}.top"), "w") as fh:
+                fh.write(top)
+        files = {f"{self.name}.input": self.input_text(),
+                 f"{self.name}.set": self.set_text(),
+                 "data_base": self.database_text(),
+                 f"{self.name}.rest": self.restart_text()}
+        for fn, txt in files.items():
+            with open(os.path.join(directory, fn), "w") as fh:
+                fh.write(txt)
+        return os.path.join(directory, f"{self.name}.input")
+
+
+def _base_keywords(name: str, dt_fs: float, temp: float, ntime: int) -> dict:
+    return {
+        "calculation": "md", "ensemble": "nve", "istart": 2, "ntime": ntime,
+        "iperd": 3, "dt": dt_fs, "t_ext": temp,
+        "iwr_screen": max(ntime, 1), "iwr_dump": 0, "iwr_inst": 0,
+        "iwr_confp": 0, "iwr_confv": 0,
+        "dpi_file": f"{name}.rest", "dpo_file": f"{name}.save",
+        "ham_file": f"{name}.ham", "eng_file": f"{name}.eng",
+        "eval_file": f"{name}.eval", "pos_file": f"{name}.conf",
+        "vel_file": f"{name}.vel", "mol_set_file": f"{name}.set",
+        "inter_file": "data_base", "bond_file": "data_base",
+        "bend_file": "data_base", "torsion_file": "data_base",
+        "onefour_file": "data_base",
+    }
+
+
+def maxwell_boltzmann(mass_amu: np.ndarray, temp: float, rng) -> np.ndarray:
+    """Gaussian velocities, net momentum removed, rescaled to exactly `temp`
+    with ndof = 3N - 3 (CM3D's samvel/zerotm/scale, integrate/md_zeroam.c:33-47)."""
+    n = mass_amu.shape[0]
+    m = mass_amu * MCONV
+    v = rng.standard_normal((n, 3)) * np.sqrt(temp / m)[:, None]
+    v -= (m[:, None] * v).sum(0) / m.sum()
+    ndof = max(3 * n - 3, 1)
+    t_now = float((m[:, None] * v * v).sum()) / ndof
+    if t_now > 0:
+        v *= math.sqrt(temp / t_now)
+    return v
+
+
+def _lj_parm(a: str, b: str, eps: float, sig: float, rmin: float,
+             rmax: float, rres: float) -> str:
+    return (f"~inter_parm[\\atom1{{{a}}}\\atom2{{{b}}}\\pot_type{{lennard-jones}}"
+            f"\\eps{{{eps!r}}}\\sig{{{sig!r}}}\\min_dist{{{rmin!r}}}"
+            f"\\max_dist{{{rmax!r}}}\\res_dist{{{rres!r}}}]")
+
+
+def _null_parm(a: str, b: str) -> str:
+    return f"~inter_parm[\\atom1{{{a}}}\\atom2{{{b}}}\\pot_type{{null}}]"
+
+
+# ----------------------------------------------------------------- argon
+def argon_fcc(ncell: int = 6, density: float = 0.8442, temp: float = 120.0,
+              seed: int = 1, rc_sigma: float = 2.5, skin_sigma: float = 0.3,
+              dt_fs: float = 5.0, ntime: int = 1000, name: str = "argon") -> Workload:
+    """LJ argon on an FCC lattice, reduced density `density`; cut and shifted
+    LJ at `rc_sigma` sigma; Verlet list with a `skin_sigma` sigma skin."""
+    sig, eps, mass = ARGON["sig"], ARGON["eps"], ARGON["mass"]
+    n = 4 * ncell ** 3
+    L = (n / density) ** (1.0 / 3.0) * sig
+    a = L / ncell
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.array([(i, j, k) for i in range(ncell) for j in range(ncell)
+                      for k in range(ncell)], dtype=float)
+    pos = ((cells[:, None, :] + basis[None, :, :] + 0.25) * a).reshape(-1, 3)
+    rng = np.random.default_rng(seed)
+    m = np.full(n, mass)
+    vel = maxwell_boltzmann(m, temp, rng)
+    rc = rc_sigma * sig
+    kw = _base_keywords(name, dt_fs, temp, ntime)
+    kw.update({"skin": skin_sigma * sig, "shift": 1, "nres_lrf": 1,
+               "nres_intra": 1, "nres_tors": 1, "neighbor_list": "verlist"})
+    top = (f"~mol_name_def[\\mol_name{{argon}}\\natom{{1}}\\nbond{{0}}]\n"
+           f"~atom_def[\\atom_typ{{ar}}\\atom_ind{{1}}\\mass{{{mass!r}}}\\charge{{0}}]\n")
+    return Workload(name=name, keywords=kw, species=[("argon", n, top)],
+                    inter_parms=[_lj_parm("ar", "ar", eps, sig, 0.55 * sig, rc, rc)],
+                    pos=pos, vel=vel, mass_amu=m, box=L, temp=temp, dt_fs=dt_fs)
+
+
+# ----------------------------------------------------------------- water
+def _random_rotations(n: int, rng) -> np.ndarray:
+    q = rng.standard_normal((n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], 1)
+
+
+def water_box(ngrid: int = 16, temp: float = 300.0, seed: int = 1,
+              rc: float | None = None, alpha: float = 0.31, kmax: int = 7,
+              skin: float = 0.5, dt_fs: float = 2.0, nres_intra: int = 4,
+              ntime: int = 1000, ntable: int = 500, name: str = "water") -> Workload:
+    """Flexible 3-site water: ngrid^3 molecules on a cubic grid at 1.0 g/cm^3
+    with seeded random orientations.  Ewald with `alpha` and a spherical
+    k-space cutoff `kmax` (CM3D's kmax keyword, md_ewald.c:93-114)."""
+    w = WATER
+    nmol = ngrid ** 3
+    L = ngrid * WATER_SPACING
+    if rc is None:
+        rc = min(10.0, 0.45 * L)
+    rng = np.random.default_rng(seed)
+    grid = np.array([(i, j, k) for i in range(ngrid) for j in range(ngrid)
+                     for k in range(ngrid)], dtype=float)
+    o = (grid + 0.5) * WATER_SPACING
+    half = math.radians(w["theta0"]) / 2.0
+    h1 = np.array([math.sin(half), 0.0, math.cos(half)]) * w["r0"]
+    h2 = np.array([-math.sin(half), 0.0, math.cos(half)]) * w["r0"]
+    R = _random_rotations(nmol, rng)
+    pos = np.empty((nmol, 3, 3))
+    pos[:, 0] = o
+    pos[:, 1] = o + R @ h1
+    pos[:, 2] = o + R @ h2
+    # re-draw the orientation of any molecule with an intermolecular contact
+    # closer than `min_contact` to a grid neighbour, so the start is not a
+    # high-energy overlap (random orientations on a 3.1 A grid otherwise put
+    # some H atoms within 1 A of each other)
+    min_contact = 1.9
+    g = pos.reshape(ngrid, ngrid, ngrid, 3, 3)
+    for _sweep in range(200):
+        bad = np.zeros((ngrid, ngrid, ngrid), dtype=bool)
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    if (dx, dy, dz) == (0, 0, 0):
+                        continue
+                    nb = np.roll(g, shift=(dx, dy, dz), axis=(0, 1, 2))
+                    d = g[:, :, :, :, None, :] - nb[:, :, :, None, :, :]
+                    d -= L * np.round(d / L)
+                    r = np.sqrt((d * d).sum(-1)).min(axis=(-1, -2))
+                    bad |= r < min_contact
+        nbad = int(bad.sum())
+        if nbad == 0:
+            break
+        idx = np.argwhere(bad)
+        # re-draw only a checkerboard subset per sweep so neighbours that
+        # clash with each other do not both move at once
+        sel = idx[(idx.sum(1) + _sweep) % 2 == 0]
+        if sel.shape[0] == 0:
+            sel = idx[:1]
+        Rn = _random_rotations(sel.shape[0], rng)
+        oo = g[sel[:, 0], sel[:, 1], sel[:, 2], 0]
+        g[sel[:, 0], sel[:, 1], sel[:, 2], 1] = oo + Rn @ h1
+        g[sel[:, 0], sel[:, 1], sel[:, 2], 2] = oo + Rn @ h2
+    pos = g.reshape(-1, 3)
+    m = np.tile([w["m_o"], w["m_h"], w["m_h"]], nmol)
+    vel = maxwell_boltzmann(m, temp, rng)
+    kw = _base_keywords(name, dt_fs, temp, ntime)
+    kw.update({"skin": skin, "nres_lrf": 1, "nres_intra": nres_intra,
+               "nres_tors": 1, "alp_ewald": alpha, "kmax": kmax,
+               "rcute_max": rc, "rcute_resp": rc, "rcute_min": 1.0,
+               "ntable": ntable, "neighbor_list": "verlist"})
+    top = ("~mol_name_def[\\mol_name{water}\\natom{3}\\nbond{2}\\nbend{1}]\n"
+           f"~atom_def[\\atom_typ{{ow}}\\atom_ind{{1}}\\mass{{{w['m_o']!r}}}"
+           f"\\charge{{{w['q_o']!r}}}]\n"
+           f"~atom_def[\\atom_typ{{hw}}\\atom_ind{{2}}\\mass{{{w['m_h']!r}}}"
+           f"\\charge{{{w['q_h']!r}}}]\n"
+           f"~atom_def[\\atom_typ{{hw}}\\atom_ind{{3}}\\mass{{{w['m_h']!r}}}"
+           f"\\charge{{{w['q_h']!r}}}]\n"
+           "~bond_def[\\atom1{1}\\atom2{2}]\n~bond_def[\\atom1{1}\\atom2{3}]\n"
+           "~bend_def[\\atom1{2}\\atom2{1}\\atom3{3}]\n")
+    inter = [_lj_parm("ow", "ow", w["eps_oo"], w["sig_oo"], 1.8, rc, rc),
+             _null_parm("ow", "hw"), _null_parm("hw", "hw")]
+    bonds = [f"~bond_parm[\\atom1{{ow}}\\atom2{{hw}}\\pot_type{{harm}}"
+             f"\\fk{{{w['k_bond']!r}}}\\eq{{{w['r0']!r}}}]"]
+    bends = [f"~bend_parm[\\atom1{{hw}}\\atom2{{ow}}\\atom3{{hw}}\\pot_type{{harm}}"
+             f"\\fk{{{w['k_bend']!r}}}\\eq{{{w['theta0']!r}}}]"]
+    return Workload(name=name, keywords=kw, species=[("water", nmol, top)],
+                    inter_parms=inter, bond_parms=bonds, bend_parms=bends,
+                    pos=pos, vel=vel, mass_amu=m, box=L, temp=temp, dt_fs=dt_fs)
+
+
+# ------------------------------------------------------ charged LJ binary
+def charged_binary(natoms: int = 256, density: float = 0.75, tstar: float = 1.0,
+                   seed: int = 1, charge: float = 0.5, kmax: int = 5,
+                   dt_fs: float = 5.0, ntime: int = 2000,
+                   name: str = "binary") -> Workload:
+    """Equimolar charged LJ binary mixture (argon LJ parameters, charges
+    +/- `charge` e) on an FCC start; rc = min(2.5 sigma, 0.45 L),
+    Ewald alpha = 3.2 / rc, spherical kmax."""
+    sig, eps, mass = ARGON["sig"], ARGON["eps"], ARGON["mass"]
+    ncell = max(1, int(round((natoms / 4) ** (1.0 / 3.0))))
+    n = 4 * ncell ** 3
+    L = (n / density) ** (1.0 / 3.0) * sig
+    a = L / ncell
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.array([(i, j, k) for i in range(ncell) for j in range(ncell)
+                      for k in range(ncell)], dtype=float)
+    pos = ((cells[:, None, :] + basis[None, :, :] + 0.25) * a).reshape(-1, 3)
+    temp = tstar * eps
+    rng = np.random.default_rng(seed)
+    m = np.full(n, mass)
+    vel = maxwell_boltzmann(m, temp, rng)
+    rc = min(2.5 * sig, 0.45 * L)
+    alpha = 3.2 / rc
+    skin = 0.3 * sig
+    kw = _base_keywords(name, dt_fs, temp, ntime)
+    kw.update({"skin": skin, "nres_lrf": 1, "nres_intra": 1, "nres_tors": 1,
+               "alp_ewald": alpha, "kmax": kmax, "rcute_max": rc,
+               "rcute_resp": rc, "rcute_min": 1.0, "shift": 1,
+               "neighbor_list": "verlist"})
+    # one "molecule" per atom; the two species alternate so that the
+    # mixture is equimolar and both species sit on every sublattice
+    topa = (f"~mol_name_def[\\mol_name{{cat}}\\natom{{1}}\\nbond{{0}}]\n"
+            f"~atom_def[\\atom_typ{{ca}}\\atom_ind{{1}}\\mass{{{mass!r}}}"
+            f"\\charge{{{charge!r}}}]\n")
+    topb = (f"~mol_name_def[\\mol_name{{ani}}\\natom{{1}}\\nbond{{0}}]\n"
+            f"~atom_def[\\atom_typ{{an}}\\atom_ind{{1}}\\mass{{{mass!r}}}"
+            f"\\charge{{{-charge!r}}}]\n")
+    perm = rng.permutation(n)
+    pos = pos[perm]
+    inter = [_lj_parm("ca", "ca", eps, sig, 0.55 * sig, rc, rc),
+             _lj_parm("an", "an", eps, sig, 0.55 * sig, rc, rc),
+             _lj_parm("an", "ca", eps, sig, 0.55 * sig, rc, rc)]
+    return Workload(name=name, keywords=kw,
+                    species=[("cat", n // 2, topa), ("ani", n - n // 2, topb)],
+                    inter_parms=inter, pos=pos, vel=vel, mass_amu=m, box=L,
+                    temp=temp, dt_fs=dt_fs)

@@ -1,0 +1,270 @@
+/*
+ * cm3d_nb.h -- C ABI of the B200 nonbonded force engine for CM3D.
+ *
+ * The engine replaces CM3D's nonbonded force path: the Verlet/link-cell
+ * neighbour lists with minimum image, the tabulated Lennard-Jones and
+ * real-space Ewald pair kernels, the reciprocal-space structure-factor sums
+ * with the excluded-pair correction, and (so the whole RESPA step can stay on
+ * the GPU) the harmonic bond/bend inner level and the velocity/position
+ * updates.  Every entry point below names the CM3D routine it replaces
+ * (file:line within the CM3D source tree).
+ *
+ * Conventions
+ *   - Only plain C types cross this boundary: pointers, sizes, doubles.
+ *   - Arrays follow CM3D's layout: per-atom SoA blocks (px, py, pz ...),
+ *     the cell matrix hmat[9] row-major as COORDS.hmat, per-interaction
+ *     tables of length ntable stored back to back as INTER.vtab[0].
+ *   - Units are CM3D's (K, Angstrom, ps, amu*MCONV, e*sqrt(CCONV)).
+ *   - The stored forces are accelerations, as in CM3D after rmass()
+ *     (energy/control/md_fcntr.c:74-75).
+ *   - Every function returns CM3D_NB_OK (0) or a negative error code; the
+ *     message of the last error on the calling thread is available from
+ *     cm3d_nb_last_error().  Nothing here exits the process: the CM3D-side
+ *     shim turns errors into md_error()/md_warning() as CM3D would.
+ *   - A context is single-threaded, like CM3D's own state (module statics
+ *     in md_fnopol.c:33, finter_e.c:31, md_finter.c:48); separate contexts
+ *     may be driven from separate threads.
+ */
+#ifndef CM3D_NB_H
+#define CM3D_NB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CM3D_NB_OK 0
+#define CM3D_NB_ERR_ARG -1        /* invalid argument / unsupported input */
+#define CM3D_NB_ERR_CUDA -2       /* CUDA runtime failure */
+#define CM3D_NB_ERR_NOMEM -3      /* device allocation failed */
+#define CM3D_NB_ERR_STATE -4      /* call out of order (e.g. force before get_ngbr) */
+#define CM3D_NB_ERR_OVERFLOW -5   /* a device list outgrew its capacity (engine retries) */
+#define CM3D_NB_ERR_NODEV -6      /* no CUDA device */
+
+/* precision modes */
+#define CM3D_NB_PLAIN_FP64 0      /* FP64 throughout, pair-per-thread over CM3D's
+                                     half lists, atomic force scatter: the plain
+                                     one-system-per-launch comparator */
+#define CM3D_NB_MIXED 1           /* FP32 distances/tables/phases on
+                                     cell-relative coordinates, FP64
+                                     accumulation, full lists, no atomics */
+
+/* which force block (COORDS fields) */
+#define CM3D_NB_FXL 0             /* fxl,fyl,fzl: long-range nonbonded */
+#define CM3D_NB_FXS 1             /* fxs,fys,fzs: short (switched) nonbonded */
+#define CM3D_NB_FXA 2             /* fxa,fya,fza: bonds + bends */
+
+/* which pair list (NGBR fields) */
+#define CM3D_NB_LIST_T 0          /* inpt/jnpt:   LJ, r^2 < rmaxl_skin2[intr] */
+#define CM3D_NB_LIST_S 1          /* inps/jnps:   LJ, r^2 < rmaxs_skin2[intr] */
+#define CM3D_NB_LIST_TE 2         /* inpte/jnpte: charged, r^2 < rmaxl_skin2_e */
+#define CM3D_NB_LIST_SE 3         /* inpse/jnpse: charged, r^2 < rmaxs_skin2_e */
+
+/*
+ * System description.  Field names follow CM3D's structs so the shim can fill
+ * it straight from SIMPARMS / COORDS / INTER / COUL / BONDS / BENDS
+ * (include/md_typedef.h:59-268).  All pointers are host memory and are only
+ * read during cm3d_nb_create(); the engine keeps device copies.
+ */
+typedef struct cm3d_nb_system {
+  /* SIMPARMS (md_typedef.h:120) */
+  int natoms;
+  int iperd;                 /* periodicity; the engine requires 3 */
+  int nres_lrf;              /* SIMPARMS.ninter */
+  int nres_intra;            /* SIMPARMS.ninnra */
+  int nres_tors;             /* SIMPARMS.ninrra */
+  int ndof;
+  double dt;                 /* ps (after TCONV) */
+  double vlrc, wlrc;         /* long-range corrections (md_searchbase.c:212-235) */
+  /* COORDS (md_typedef.h:201) */
+  double hmat[9];
+  const double *px, *py, *pz;
+  const double *vx, *vy, *vz;
+  const double *amass;
+  const double *qch;
+  /* INTER (md_typedef.h:255) */
+  int ntypes;                /* atom types */
+  const int *itype;          /* [natoms] */
+  const int *map;            /* [ntypes*ntypes], interaction index or -1 (null) */
+  int ninter;                /* INTER.ntype: non-null interactions */
+  int ntable;
+  const double *vtab;        /* [ninter*ntable] V */
+  const double *dvtab;       /* [ninter*ntable] (dV/dr)/r */
+  const double *switchs;     /* [ninter*ntable] RESPA switch */
+  const double *rmaxs_cut2, *rmins_cut2, *rmaxl_cut2, *rminl_cut2;
+  const double *rmaxs_skin2, *rmaxl_skin2, *dx2tab;     /* [ninter] */
+  double skin_ter, rheal;
+  const double *coultab, *dcoultab, *switchse;          /* [ntable]; NULL if no charges */
+  double dx2coul, rmins_coul2, rmaxs_coul2, rminl_coul2, rmaxl_coul2;
+  double rmaxs_skin2_e, rmaxl_skin2_e;
+  const int *excl_off, *excl_idx;   /* INTER.nexclude/exclude as CSR: atom i's
+                                       sorted list is excl_idx[excl_off[i]..excl_off[i+1]) */
+  /* COUL (md_typedef.h:59) */
+  const int *cexcl_off, *cexcl_idx; /* COUL.nexclude/exclude as CSR */
+  int ktot;
+  const int *ka, *kb, *kc;          /* k-vectors in CM3D's order (md_ewald.c:93-114) */
+  double kappa, falp2, ewald_self, ewald_bkg;
+  int necorr;
+  const int *iecorr, *jecorr;
+  /* BONDS / BENDS (md_typedef.h:71-79); harmonic forms only */
+  int nbonds, nbond_types;
+  const int *ibond, *jbond, *idxbond, *itypbond;
+  const double *eqbond, *fkbond;
+  int nbends, nbend_types;
+  const int *ibend, *jbend, *kbend, *idxbend, *itypbend;
+  const double *eqbend, *fkbend;
+  int ntors, n14, nbondx;    /* must be 0 for cm3d_nb_step() */
+} cm3d_nb_system;
+
+typedef struct cm3d_nb_options {
+  int device;                /* CUDA device ordinal */
+  int mode;                  /* CM3D_NB_PLAIN_FP64 or CM3D_NB_MIXED */
+  int need_short;            /* 1: always produce fxs at level 1 (CM3D does);
+                                0: only when nres_lrf > 1 (fxs is multiplied by
+                                dter1 = 0 otherwise, md_step.c:78,99) */
+  int tpa;                   /* mixed pair kernel: lanes per atom (0 = auto) */
+  int use_graph;             /* capture cm3d_nb_step() in a CUDA graph */
+} cm3d_nb_options;
+
+/* energies/virials collected as getvireal()+geteng() do (md_fcntr.c:136-308) */
+typedef struct cm3d_nb_energies {
+  double vinter, vhinter, winter, wintertensor[9];   /* getsvirter  md_fnopol.c:386 */
+  double velec, welec, welectensor[9];               /* getsvirter_e finter_e.c:410 */
+  double vewald, wewald, wewaldtensor[9];            /* getvewald   md_ewald.c:364 */
+  double vbond, vbend, wbond, wbend;
+  double US, U, W, Wtensor[9];
+  double zke, p2m_tensor[9];                         /* get_p2mt md_fcntr.c:332 */
+  double prsi, prs_tensor[9], tiout, poter, poth, potra;
+} cm3d_nb_energies;
+
+typedef struct cm3d_nb_status_t {
+  long long table_underflow;  /* pairs below the table start (md_fnopol.c:133-140) */
+  long long rebuilds;         /* neighbour-list rebuilds so far */
+  long long resets;           /* RESETPOS events (md_finter.c:79-95) */
+  long long overflows;        /* list-capacity overflows handled by regrowth */
+  int nonfinite;              /* a NaN/Inf reached the forces or energies */
+  int last_istep;
+} cm3d_nb_status_t;
+
+typedef struct cm3d_nb_ctx cm3d_nb_ctx;
+
+/* ------------------------------------------------------------ library */
+int cm3d_nb_version(void);
+const char *cm3d_nb_last_error(void);
+int cm3d_nb_device_count(int *count);
+void cm3d_nb_default_options(cm3d_nb_options *opt);
+
+/* ------------------------------------------------------------ context */
+/* Upload a system; replaces the allocations CM3D makes in read_parmfile /
+   allocate_lists / set_charges (md_readparm.c:35, ngbr_list.c:584,
+   elec_ngbr.c:36).  Lists are not built until cm3d_nb_get_ngbr(). */
+int cm3d_nb_create(const cm3d_nb_system *sys, const cm3d_nb_options *opt,
+                   cm3d_nb_ctx **out);
+void cm3d_nb_destroy(cm3d_nb_ctx *ctx);
+
+/* host <-> device state (COORDS.px..pz, vx..vz, hmat) */
+int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py,
+                          const double *pz);
+int cm3d_nb_get_positions(cm3d_nb_ctx *ctx, double *px, double *py, double *pz);
+int cm3d_nb_set_velocities(cm3d_nb_ctx *ctx, const double *vx, const double *vy,
+                           const double *vz);
+int cm3d_nb_get_velocities(cm3d_nb_ctx *ctx, double *vx, double *vy, double *vz);
+int cm3d_nb_get_forces(cm3d_nb_ctx *ctx, int which, double *fx, double *fy,
+                       double *fz);
+int cm3d_nb_set_forces(cm3d_nb_ctx *ctx, int which, const double *fx,
+                       const double *fy, const double *fz);
+
+/* ------------------------------------------------- CM3D entry points */
+/* get_ngbr()        energy/control/ngbr_list.c:297 (with get_ngbr_e,
+                     elec_ngbr.c:220): rebuild all four lists from the
+                     current positions and snapshot them into dxn. */
+int cm3d_nb_get_ngbr(cm3d_nb_ctx *ctx);
+/* nrefsh()          energy/control/md_finter.c:43: rebuild when any atom
+                     moved more than skin/2, with the RESETPOS pull-back
+                     when the previous rebuild is fewer than 3 steps old. */
+int cm3d_nb_nrefsh(cm3d_nb_ctx *ctx, int istep, int *rebuilt);
+/* force()           energy/control/md_fcntr.c:44 for iflg 0 (short
+                     nonbonded), 1 (full nonbonded + Ewald) and 2 (bonds and
+                     bends); results stored as accelerations. */
+int cm3d_nb_force(cm3d_nb_ctx *ctx, int iflg);
+/* force_ter()       energy/control/md_finter.c:110 -> force_npol()
+                     energy/inter/md_fnopol.c:46: LJ over the t (iflg 1) or
+                     s (iflg 0) list; adds raw forces to fxl/fxs (iflg 1) or
+                     fxs (iflg 0) and resets the LJ accumulators (zero_potl). */
+int cm3d_nb_force_ter(cm3d_nb_ctx *ctx, int iflg);
+/* force_ter_e()     energy/control/md_finter_e.c:78 -> force_e()
+                     energy/inter/finter_e.c:42: real-space Ewald over the te
+                     (iflg 1) or se (iflg 0) list. */
+int cm3d_nb_force_ter_e(cm3d_nb_ctx *ctx, int iflg);
+/* fk_ewald()        energy/inter/md_ewald.c:185: structure factors,
+                     reciprocal energy/virial, adds forces to fxl. */
+int cm3d_nb_fk_ewald(cm3d_nb_ctx *ctx);
+/* ecorr()           energy/inter/md_ewald.c:385: excluded-pair correction,
+                     adds forces to fxl. */
+int cm3d_nb_ecorr(cm3d_nb_ctx *ctx);
+/* zero a force block / rmass() utils/md_util.new.c:219 on it */
+int cm3d_nb_zero_forces(cm3d_nb_ctx *ctx, int which);
+int cm3d_nb_rmass(cm3d_nb_ctx *ctx, int which);
+/* getsvirter()      energy/inter/md_fnopol.c:386 (adds, as CM3D does) */
+int cm3d_nb_getsvirter(cm3d_nb_ctx *ctx, double *vhinter, double *vinter,
+                       double *winter, double wintert[9]);
+/* getsvirter_e()    energy/inter/finter_e.c:410 */
+int cm3d_nb_getsvirter_e(cm3d_nb_ctx *ctx, double *velec, double *welec,
+                         double welectensor[9]);
+/* getvewald()       energy/inter/md_ewald.c:364 */
+int cm3d_nb_getvewald(cm3d_nb_ctx *ctx, double *pot_ewald, double *prs_ewald,
+                      double prs_ewald_tensor[9]);
+/* step_init()       integrate/md_step.c:32: lists, forces at levels 1 and 2,
+                     energies. */
+int cm3d_nb_step_init(cm3d_nb_ctx *ctx);
+/* step()            integrate/md_step.c:62, nsteps times starting at
+                     SIMPARMS.istep = istep0 (NVE; torsions, thermostats and
+                     barostats are not part of the engine). */
+int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps);
+/* getvireal(...,1)+geteng() md_fcntr.c:136,259 from the device accumulators */
+int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e);
+
+/* pair lists in CM3D's NGBR form: pairs (i, j) of atom indices */
+int cm3d_nb_list_count(cm3d_nb_ctx *ctx, int which, long long *npairs);
+int cm3d_nb_get_list(cm3d_nb_ctx *ctx, int which, int *ip, int *jp,
+                     long long capacity, long long *npairs);
+
+int cm3d_nb_get_status(cm3d_nb_ctx *ctx, cm3d_nb_status_t *st);
+int cm3d_nb_synchronize(cm3d_nb_ctx *ctx);
+/* the CUDA stream every kernel of this context runs on (cudaStream_t) */
+void *cm3d_nb_stream(cm3d_nb_ctx *ctx);
+
+/* --------------------------------------------------------- timing */
+/* Bracket every launch of kernel class `cls` with CUDA events on the
+   context's stream; cm3d_nb_kernel_time returns the summed device time in
+   ms and the number of launches since timing was enabled.
+   cls: 0 = pair kernel(s), 1 = k-space, 2 = list build, 3 = integrate. */
+int cm3d_nb_enable_timing(cm3d_nb_ctx *ctx, int enable);
+int cm3d_nb_kernel_time(cm3d_nb_ctx *ctx, int cls, double *ms, long long *launches);
+/* number of kernel launches this context issued so far */
+long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx);
+
+/* ------------------------------------------ host set-up restatements */
+/* One interaction's LJ table, as get_ter_parm() builds it
+   (input/md_getparm.c:236-237, 321-366 with func_lj md_funcvdw.c:40):
+   ntable points uniform in r^2 from rmin^2; V, (dV/dr)/r and the cubic
+   RESPA switch over [rres-rheal, rres].  `shift` subtracts V[ntable-3]
+   (md_searchbase.c:181-188).  Outputs are ntable long; *dx2tab is set. */
+int cm3d_nb_lj_table(double eps, double sig, double rmin, double rmax,
+                     double rres, double rheal, double skin, int ntable,
+                     int shift, double *vtab, double *dvtab, double *switchs,
+                     double *dx2tab);
+/* The real-space Ewald table of set_charges() (elec_ngbr.c:51-103 with
+   func_kerf md_funcvdw.c:219; func_coul when iperd != 3). */
+int cm3d_nb_coul_table(double alpha, double rcute_min, double rcute_resp,
+                       double rcute_max, double rheal, double skin, int ntable,
+                       int iperd, int shift, double *coultab, double *dcoultab,
+                       double *switchse, double *dx2coul);
+/* The half-space spherical k-vector set of ewald_setup() (md_ewald.c:93-114);
+   with ka == NULL only *ktot is returned. */
+int cm3d_nb_ewald_kvectors(int kmax, int *ka, int *kb, int *kc, int *kup,
+                           int *ktot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CM3D_NB_H */

@@ -1,0 +1,1178 @@
+/*
+ * cm3d_oracle.c -- CPU restatement of CM3D's nonbonded force path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see cm3d_oracle.h).  Every function restates the
+ * CM3D routine named in its comment, keeping CM3D's operation order so that
+ * the results match the reference bit for bit when compiled without FMA
+ * contraction (-ffp-contract=off): pair lists in link-cell traversal order,
+ * pair kernels over nlen-sized chunks with per-chunk energy partials, the
+ * Ewald kc-recursion, and the same accumulation order of every sum.
+ */
+#include "cm3d_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* include/md_macros.h:52 (LINUX build): round half away from zero through a
+   truncating int conversion */
+#define ANINT(A) ((int)((A) + ((A) >= 0 ? .5 : -.5)))
+#define TPI (2. * M_PI)
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+struct orc {
+  int n, ntypes, ninter, ntable, ncells, nocell_all, nlen, iperd;
+  int nres_lrf, nres_intra, nres_tors, ndof;
+  double dt, vlrc, wlrc, skin, rheal;
+  double hmat[9], hmati[9];
+  double *px, *py, *pz, *vx, *vy, *vz, *amass, *qch;
+  int *itype, *map;
+  double *vtab, *dvtab, *switchs;
+  double *rmaxs_cut2, *rmins_cut2, *rmaxl_cut2, *rminl_cut2, *rmaxs_skin2,
+      *rmaxl_skin2, *dx2tab;
+  double *coultab, *dcoultab, *switchse;
+  double dx2coul, rmins_coul2, rmaxs_coul2, rminl_coul2, rmaxl_coul2,
+      rmaxs_skin2_e, rmaxl_skin2_e;
+  int *excl_off, *excl_idx, *cexcl_off, *cexcl_idx;
+  int ncharge, *icharge;
+  int ktot, *ka, *kb, *kc, *kup;
+  double kappa, kappa2, falp2, ewald_self, ewald_bkg;
+  int necorr, *iecorr, *jecorr;
+  int nbonds, *ibond, *jbond, *idxbond, *itypbond;
+  double *eqbond, *fkbond;
+  int nbends, *ibend, *jbend, *kbend, *idxbend, *itypbend;
+  double *eqbend, *fkbend;
+  /* forces (3n blocks: x | y | z), scratch, neighbour state */
+  double *fxl, *fxs, *fxa, *scr, *rec, *dxn;
+  long long nprt, nprs, nprte, nprse, cap_t, cap_s, cap_te, cap_se;
+  int *inpt, *jnpt, *inps, *jnps, *inpte, *jnpte, *inpse, *jnpse;
+  int npaircell, *icell, *jcell, npaircelle, *icelle, *jcelle;
+  int *hlist, *lnk, cells_ready;
+  int isteplast;
+  long long rebuilds, resets, underflows;
+  /* module statics of md_fnopol.c:33, finter_e.c:31, COUL accumulators */
+  double spotl, spothl, sprsl, sprslt[9];
+  double spote, spothe, sprse, sprset[9];
+  double vk_ewald, vp_ewald, vp_ewald_tensor[9];
+  double pot_ecorr, prs_ecorr, prs_ecorr_tensor[9];
+  double vbond, wbond, wbondt[9], vbend;
+};
+
+static void *dup(const void *p, size_t bytes)
+{
+  void *q = malloc(bytes > 0 ? bytes : 1);
+  if (p && bytes) memcpy(q, p, bytes);
+  else memset(q, 0, bytes > 0 ? bytes : 1);
+  return q;
+}
+
+/* gethinv9  utils/md_mathlib.c:30-50 */
+static double gethinv9(const double h[9], double hi[9])
+{
+  double rvol = 1. / (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                      h[2] * (h[3] * h[7] - h[4] * h[6]));
+  hi[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
+  hi[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
+  hi[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
+  hi[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
+  hi[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
+  hi[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
+  hi[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
+  hi[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
+  hi[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
+  return 1. / rvol;
+}
+
+/* get_deth  utils/md_mathlib.c:53-60 */
+static double get_deth(const double h[9])
+{
+  return (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+          h[2] * (h[3] * h[7] - h[4] * h[6]));
+}
+
+/* period_new  integrate/md_period.new.c:39-52 (iperd 3) */
+static void period(int n, double *dx, double *dy, double *dz, const double *h,
+                   const double *hi)
+{
+  int j;
+  for (j = 0; j < n; j++) {
+    double sx = dx[j] * hi[0] + dy[j] * hi[1] + dz[j] * hi[2];
+    double sy = dx[j] * hi[3] + dy[j] * hi[4] + dz[j] * hi[5];
+    double sz = dx[j] * hi[6] + dy[j] * hi[7] + dz[j] * hi[8];
+    sx -= ANINT(sx);
+    sy -= ANINT(sy);
+    sz -= ANINT(sz);
+    dx[j] = sx * h[0] + sy * h[1] + sz * h[2];
+    dy[j] = sx * h[3] + sy * h[4] + sz * h[5];
+    dz[j] = sx * h[6] + sy * h[7] + sz * h[8];
+  }
+}
+
+/* locate/exclij  utils/utils.c:125-172: is (i, j) in the sorted exclusion
+   list stored at the lower index */
+static int exclij(int i, int j, const int *off, const int *idx)
+{
+  int a = i < j ? i : j, b = i < j ? j : i;
+  int lo = off[a], hi = off[a + 1];
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (idx[mid] == b) return 1;
+    if (idx[mid] < b) lo = mid + 1;
+    else hi = mid;
+  }
+  return 0;
+}
+
+orc *orc_create(const cm3d_nb_system *s, int ncells, int nocell_all, int nlen)
+{
+  orc *o = (orc *)calloc(1, sizeof(orc));
+  int n = s->natoms, i, nt = s->ntable, ni = s->ninter;
+  o->n = n;
+  o->ntypes = s->ntypes;
+  o->ninter = ni;
+  o->ntable = nt;
+  o->ncells = ncells;
+  o->nocell_all = nocell_all;
+  o->nlen = nlen;
+  o->iperd = s->iperd;
+  o->nres_lrf = s->nres_lrf;
+  o->nres_intra = s->nres_intra;
+  o->nres_tors = s->nres_tors;
+  o->ndof = s->ndof;
+  o->dt = s->dt;
+  o->vlrc = s->vlrc;
+  o->wlrc = s->wlrc;
+  o->skin = s->skin_ter;
+  o->rheal = s->rheal;
+  memcpy(o->hmat, s->hmat, sizeof o->hmat);
+  gethinv9(o->hmat, o->hmati);
+  o->px = (double *)dup(s->px, n * 8.);
+  o->py = (double *)dup(s->py, n * 8.);
+  o->pz = (double *)dup(s->pz, n * 8.);
+  o->vx = (double *)dup(s->vx, n * 8.);
+  o->vy = (double *)dup(s->vy, n * 8.);
+  o->vz = (double *)dup(s->vz, n * 8.);
+  o->amass = (double *)dup(s->amass, n * 8.);
+  o->qch = (double *)dup(s->qch, n * 8.);
+  o->itype = (int *)dup(s->itype, n * 4.);
+  o->map = (int *)dup(s->map, (size_t)s->ntypes * s->ntypes * 4);
+  o->vtab = (double *)dup(s->vtab, (size_t)ni * nt * 8);
+  o->dvtab = (double *)dup(s->dvtab, (size_t)ni * nt * 8);
+  o->switchs = (double *)dup(s->switchs, (size_t)ni * nt * 8);
+  o->rmaxs_cut2 = (double *)dup(s->rmaxs_cut2, ni * 8.);
+  o->rmins_cut2 = (double *)dup(s->rmins_cut2, ni * 8.);
+  o->rmaxl_cut2 = (double *)dup(s->rmaxl_cut2, ni * 8.);
+  o->rminl_cut2 = (double *)dup(s->rminl_cut2, ni * 8.);
+  o->rmaxs_skin2 = (double *)dup(s->rmaxs_skin2, ni * 8.);
+  o->rmaxl_skin2 = (double *)dup(s->rmaxl_skin2, ni * 8.);
+  o->dx2tab = (double *)dup(s->dx2tab, ni * 8.);
+  o->coultab = (double *)dup(s->coultab, s->coultab ? nt * 8. : 0);
+  o->dcoultab = (double *)dup(s->dcoultab, s->dcoultab ? nt * 8. : 0);
+  o->switchse = (double *)dup(s->switchse, s->switchse ? nt * 8. : 0);
+  o->dx2coul = s->dx2coul;
+  o->rmins_coul2 = s->rmins_coul2;
+  o->rmaxs_coul2 = s->rmaxs_coul2;
+  o->rminl_coul2 = s->rminl_coul2;
+  o->rmaxl_coul2 = s->rmaxl_coul2;
+  o->rmaxs_skin2_e = s->rmaxs_skin2_e;
+  o->rmaxl_skin2_e = s->rmaxl_skin2_e;
+  o->excl_off = (int *)dup(s->excl_off, (n + 1) * 4.);
+  o->excl_idx = (int *)dup(s->excl_idx, s->excl_off[n] * 4.);
+  o->cexcl_off = (int *)dup(s->cexcl_off, (n + 1) * 4.);
+  o->cexcl_idx = (int *)dup(s->cexcl_idx, s->cexcl_off[n] * 4.);
+  /* icharge: set_charges elec_ngbr.c:115-121 */
+  o->icharge = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  for (i = 0; i < n; i++)
+    if (o->qch[i] != 0.) o->icharge[o->ncharge++] = i;
+  o->ktot = s->ktot;
+  o->ka = (int *)dup(s->ka, s->ktot * 4.);
+  o->kb = (int *)dup(s->kb, s->ktot * 4.);
+  o->kc = (int *)dup(s->kc, s->ktot * 4.);
+  /* kup: first vector of every (ka, kb) row (ewald_setup md_ewald.c:95,102) */
+  o->kup = (int *)calloc((size_t)s->ktot + 1, sizeof(int));
+  for (i = 0; i < s->ktot; i++)
+    o->kup[i] = (i == 0 || o->ka[i] != o->ka[i - 1] || o->kb[i] != o->kb[i - 1]);
+  o->kappa = s->kappa;
+  o->kappa2 = s->kappa * s->kappa;
+  o->falp2 = s->falp2;
+  o->ewald_self = s->ewald_self;
+  o->ewald_bkg = s->ewald_bkg;
+  o->necorr = s->necorr;
+  o->iecorr = (int *)dup(s->iecorr, s->necorr * 4.);
+  o->jecorr = (int *)dup(s->jecorr, s->necorr * 4.);
+  o->nbonds = s->nbonds;
+  o->ibond = (int *)dup(s->ibond, s->nbonds * 4.);
+  o->jbond = (int *)dup(s->jbond, s->nbonds * 4.);
+  o->idxbond = (int *)dup(s->idxbond, s->nbonds * 4.);
+  o->itypbond = (int *)dup(s->itypbond, s->nbond_types * 4.);
+  o->eqbond = (double *)dup(s->eqbond, s->nbond_types * 8.);
+  o->fkbond = (double *)dup(s->fkbond, s->nbond_types * 8.);
+  o->nbends = s->nbends;
+  o->ibend = (int *)dup(s->ibend, s->nbends * 4.);
+  o->jbend = (int *)dup(s->jbend, s->nbends * 4.);
+  o->kbend = (int *)dup(s->kbend, s->nbends * 4.);
+  o->idxbend = (int *)dup(s->idxbend, s->nbends * 4.);
+  o->itypbend = (int *)dup(s->itypbend, s->nbend_types * 4.);
+  o->eqbend = (double *)dup(s->eqbend, s->nbend_types * 8.);
+  o->fkbend = (double *)dup(s->fkbend, s->nbend_types * 8.);
+  o->fxl = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->fxs = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->fxa = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->scr = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->rec = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->dxn = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->lnk = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+  o->hlist = (int *)malloc(sizeof(int) * (size_t)ncells * ncells * ncells);
+  return o;
+}
+
+void orc_destroy(orc *o)
+{
+  void *ptrs[] = {o->px, o->py, o->pz, o->vx, o->vy, o->vz, o->amass, o->qch,
+                  o->itype, o->map, o->vtab, o->dvtab, o->switchs, o->rmaxs_cut2,
+                  o->rmins_cut2, o->rmaxl_cut2, o->rminl_cut2, o->rmaxs_skin2,
+                  o->rmaxl_skin2, o->dx2tab, o->coultab, o->dcoultab, o->switchse,
+                  o->excl_off, o->excl_idx, o->cexcl_off, o->cexcl_idx, o->icharge,
+                  o->ka, o->kb, o->kc, o->kup, o->iecorr, o->jecorr, o->ibond,
+                  o->jbond, o->idxbond, o->itypbond, o->eqbond, o->fkbond, o->ibend,
+                  o->jbend, o->kbend, o->idxbend, o->itypbend, o->eqbend, o->fkbend,
+                  o->fxl, o->fxs, o->fxa, o->scr, o->rec, o->dxn, o->inpt, o->jnpt,
+                  o->inps, o->jnps, o->inpte, o->jnpte, o->inpse, o->jnpse, o->icell,
+                  o->jcell, o->icelle, o->jcelle, o->hlist, o->lnk};
+  size_t i;
+  for (i = 0; i < sizeof ptrs / sizeof ptrs[0]; i++) free(ptrs[i]);
+  free(o);
+}
+
+void orc_set_positions(orc *o, const double *px, const double *py, const double *pz)
+{
+  memcpy(o->px, px, o->n * 8.);
+  memcpy(o->py, py, o->n * 8.);
+  memcpy(o->pz, pz, o->n * 8.);
+}
+void orc_get_positions(orc *o, double *px, double *py, double *pz)
+{
+  memcpy(px, o->px, o->n * 8.);
+  memcpy(py, o->py, o->n * 8.);
+  memcpy(pz, o->pz, o->n * 8.);
+}
+void orc_set_velocities(orc *o, const double *vx, const double *vy, const double *vz)
+{
+  memcpy(o->vx, vx, o->n * 8.);
+  memcpy(o->vy, vy, o->n * 8.);
+  memcpy(o->vz, vz, o->n * 8.);
+}
+void orc_get_velocities(orc *o, double *vx, double *vy, double *vz)
+{
+  memcpy(vx, o->vx, o->n * 8.);
+  memcpy(vy, o->vy, o->n * 8.);
+  memcpy(vz, o->vz, o->n * 8.);
+}
+static double *block(orc *o, int which)
+{
+  return which == 0 ? o->fxl : which == 1 ? o->fxs : o->fxa;
+}
+void orc_get_forces(orc *o, int which, double *fx, double *fy, double *fz)
+{
+  double *b = block(o, which);
+  memcpy(fx, b, o->n * 8.);
+  memcpy(fy, b + o->n, o->n * 8.);
+  memcpy(fz, b + 2 * o->n, o->n * 8.);
+}
+void orc_zero_forces(orc *o, int which)
+{
+  memset(block(o, which), 0, 3 * (size_t)o->n * 8);
+}
+
+/* ------------------------------------------------------------ link cells */
+/* set_link  energy/control/set_link.c:31-201: half-shell cell pairs whose
+   (conservative) separation is below rmax (LJ) / rmaxe (charges) */
+static void set_link(orc *o, double rmax, double rmaxe)
+{
+  const double *h = o->hmat;
+  int ncell = o->ncells, nmax = ncell / 2, ncell2 = ncell * ncell;
+  int ncells = ncell * ncell2, icell, ic, jc, kc, i, j, k, in, jn, kn, cap;
+  double rcell = 1. / (double)ncell, ddot, sinangle, dx, dy, dz, r;
+  free(o->icell); free(o->jcell); free(o->icelle); free(o->jcelle);
+  cap = ncells * (nmax + 1) * (2 * nmax + 1) * (2 * nmax + 1) + 1;
+  o->icell = (int *)malloc(sizeof(int) * cap);
+  o->jcell = (int *)malloc(sizeof(int) * cap);
+  o->icelle = (int *)malloc(sizeof(int) * cap);
+  o->jcelle = (int *)malloc(sizeof(int) * cap);
+  o->npaircell = o->npaircelle = 0;
+  ddot = h[0] * h[3] + h[1] * h[4] + h[2] * h[5];
+  ddot /= (sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]) * sqrt(h[3] * h[3] + h[4] * h[4] + h[5] * h[5]));
+  sinangle = sin(acos(ddot));
+  ddot = h[0] * h[6] + h[1] * h[7] + h[2] * h[8];
+  ddot /= (sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]) * sqrt(h[6] * h[6] + h[7] * h[7] + h[8] * h[8]));
+  ddot = sin(acos(ddot));
+  if (ddot < sinangle) sinangle = ddot;
+  ddot = h[3] * h[6] + h[4] * h[7] + h[5] * h[8];
+  ddot /= (sqrt(h[3] * h[3] + h[4] * h[4] + h[5] * h[5]) * sqrt(h[6] * h[6] + h[7] * h[7] + h[8] * h[8]));
+  ddot = sin(acos(ddot));
+  if (ddot < sinangle) sinangle = ddot;
+  for (icell = 0; icell < ncells; icell++) {
+    ic = icell / ncell2;
+    jc = (icell - ic * ncell2) / ncell;
+    kc = (icell - ic * ncell2 - jc * ncell);
+    for (i = 0; i <= nmax; i++) {
+      for (j = (i == 0) ? 0 : -nmax; j <= nmax; j++) {
+        for (k = (i == 0 && j == 0) ? 0 : -nmax; k <= nmax; k++) {
+          in = (ic + i) % ncell;
+          jn = (jc + j) % ncell;
+          kn = (kc + k) % ncell;
+          in = abs(ic - in);
+          jn = abs(jc - jn);
+          kn = abs(kc - kn);
+          if (o->iperd > 0 && in > ncell / 2) in = ncell - in;
+          if (o->iperd > 1 && jn > ncell / 2) jn = ncell - jn;
+          if (o->iperd > 2 && kn > ncell / 2) kn = ncell - kn;
+          if (in > 0) in--;
+          if (jn > 0) jn--;
+          if (kn > 0) kn--;
+          dx = h[0] * in * rcell + h[1] * jn * rcell + h[2] * kn * rcell;
+          dy = h[3] * in * rcell + h[4] * jn * rcell + h[5] * kn * rcell;
+          dz = h[6] * in * rcell + h[7] * jn * rcell + h[8] * kn * rcell;
+          r = sqrt(dx * dx + dy * dy + dz * dz) * sinangle;
+          if (r < rmax || r < rmaxe) {
+            in = ic + i; jn = jc + j; kn = kc + k;
+            if (in < 0) in += ncell;
+            if (jn < 0) jn += ncell;
+            if (kn < 0) kn += ncell;
+            if (in >= ncell) in -= ncell;
+            if (jn >= ncell) jn -= ncell;
+            if (kn >= ncell) kn -= ncell;
+            if (r < rmax) {
+              o->icell[o->npaircell] = icell;
+              o->jcell[o->npaircell++] = in * ncell2 + jn * ncell + kn;
+            }
+            if (r < rmaxe) {
+              o->icelle[o->npaircelle] = icell;
+              o->jcelle[o->npaircelle++] = in * ncell2 + jn * ncell + kn;
+            }
+          }
+        }
+      }
+    }
+  }
+  o->cells_ready = 1;
+}
+
+/* get_lnklist / get_lnklist_e  set_link.c:203-300: chains built from the last
+   atom down so that every chain is in ascending atom order; only charged
+   atoms when `charged_only` */
+static void get_lnklist(orc *o, int charged_only)
+{
+  int ncell = o->ncells, ncell2 = ncell * ncell, ncell3 = ncell * ncell2;
+  int ncellm1 = ncell - 1, i, ic, jc, kc, icell;
+  double hi[9];
+  gethinv9(o->hmat, hi);
+  for (i = 0; i < ncell3; i++) o->hlist[i] = -1;
+  for (i = o->n - 1; i >= 0; i--) {
+    double sx, sy, sz;
+    if (charged_only && o->qch[i] == 0.0) continue;
+    sx = o->px[i] * hi[0] + o->py[i] * hi[1] + o->pz[i] * hi[2];
+    sy = o->px[i] * hi[3] + o->py[i] * hi[4] + o->pz[i] * hi[5];
+    sz = o->px[i] * hi[6] + o->py[i] * hi[7] + o->pz[i] * hi[8];
+    if (o->iperd > 0) sx -= ANINT(sx);
+    if (o->iperd > 1) sy -= ANINT(sy);
+    if (o->iperd > 2) sz -= ANINT(sz);
+    ic = (int)((sx + .5) * ncell);
+    jc = (int)((sy + .5) * ncell);
+    kc = (int)((sz + .5) * ncell);
+    ic = ic > 0 ? ic : 0; jc = jc > 0 ? jc : 0; kc = kc > 0 ? kc : 0;
+    ic = ic < ncellm1 ? ic : ncellm1;
+    jc = jc < ncellm1 ? jc : ncellm1;
+    kc = kc < ncellm1 ? kc : ncellm1;
+    icell = ic * ncell2 + jc * ncell + kc;
+    o->lnk[i] = o->hlist[icell];
+    o->hlist[icell] = i;
+  }
+}
+
+/* ------------------------------------------------------ Verlet lists */
+static void push(int **ip, int **jp, long long *np, long long *cap, int i, int j)
+{
+  if (*np >= *cap) {
+    *cap = *cap ? 2 * *cap : 1024;
+    *ip = (int *)realloc(*ip, sizeof(int) * (size_t)*cap);
+    *jp = (int *)realloc(*jp, sizeof(int) * (size_t)*cap);
+  }
+  (*ip)[*np] = i;
+  (*jp)[*np] = j;
+  (*np)++;
+}
+
+/* candidate test of ngbr_list  ngbr_list.c:60-97: min-image r^2 against the
+   per-interaction skin radii (t list; s list nested inside) */
+static void test_lj(orc *o, int in, int jn)
+{
+  double xd = o->px[in] - o->px[jn], yd = o->py[in] - o->py[jn], zd = o->pz[in] - o->pz[jn];
+  double r2;
+  int intr;
+  period(1, &xd, &yd, &zd, o->hmat, o->hmati);
+  r2 = xd * xd + yd * yd + zd * zd;
+  intr = o->map[o->itype[in] * o->ntypes + o->itype[jn]];
+  if (r2 < o->rmaxl_skin2[intr]) {
+    push(&o->inpt, &o->jnpt, &o->nprt, &o->cap_t, in, jn);
+    if (r2 < o->rmaxs_skin2[intr]) push(&o->inps, &o->jnps, &o->nprs, &o->cap_s, in, jn);
+  }
+}
+
+/* ngbr_liste  ngbr_list.c:114-140 */
+static void test_el(orc *o, int in, int jn)
+{
+  double xd = o->px[in] - o->px[jn], yd = o->py[in] - o->py[jn], zd = o->pz[in] - o->pz[jn];
+  double r2;
+  period(1, &xd, &yd, &zd, o->hmat, o->hmati);
+  r2 = xd * xd + yd * yd + zd * zd;
+  if (r2 < o->rmaxl_skin2_e) {
+    push(&o->inpte, &o->jnpte, &o->nprte, &o->cap_te, in, jn);
+    if (r2 < o->rmaxs_skin2_e) push(&o->inpse, &o->jnpse, &o->nprse, &o->cap_se, in, jn);
+  }
+}
+
+/* get_ngbr  ngbr_list.c:297-581 and get_ngbr_e  elec_ngbr.c:220-358 */
+void orc_get_ngbr(orc *o)
+{
+  int n = o->n, i, j, p;
+  gethinv9(o->hmat, o->hmati);
+  o->nprt = o->nprs = o->nprte = o->nprse = 0;
+  if (!o->cells_ready && o->nocell_all) {
+    double r2 = 0;
+    for (i = 0; i < o->ninter; i++)
+      if (o->rmaxl_skin2[i] > r2) r2 = o->rmaxl_skin2[i];
+    set_link(o, sqrt(r2) + o->skin, sqrt(o->rmaxl_skin2_e) + o->skin);
+  }
+  /* LJ lists */
+  if (o->nocell_all == 0) {
+    for (i = 0; i < n; i++)
+      for (j = i + 1; j < n; j++) {
+        if (exclij(i, j, o->excl_off, o->excl_idx)) continue;
+        if (o->map[o->itype[i] * o->ntypes + o->itype[j]] == -1) continue;
+        test_lj(o, i, j);
+      }
+  } else {
+    get_lnklist(o, 0);
+    for (p = 0; p < o->npaircell; p++) {
+      int icell = o->icell[p], jcell = o->jcell[p];
+      int ii = o->hlist[icell];
+      while (ii != -1) {
+        int jj = (icell == jcell) ? o->lnk[ii] : o->hlist[jcell];
+        while (jj != -1) {
+          if (o->map[o->itype[ii] * o->ntypes + o->itype[jj]] != -1 &&
+              !exclij(ii, jj, o->excl_off, o->excl_idx))
+            test_lj(o, ii, jj);
+          jj = o->lnk[jj];
+        }
+        ii = o->lnk[ii];
+      }
+    }
+  }
+  /* charged lists */
+  if (o->ncharge > 0) {
+    if (o->nocell_all == 0) {
+      for (i = 0; i < o->ncharge; i++)
+        for (j = i + 1; j < o->ncharge; j++) {
+          int ii = o->icharge[i], jj = o->icharge[j];
+          if (exclij(ii, jj, o->cexcl_off, o->cexcl_idx)) continue;
+          test_el(o, ii, jj);
+        }
+    } else {
+      get_lnklist(o, 1);
+      for (p = 0; p < o->npaircelle; p++) {
+        int icell = o->icelle[p], jcell = o->jcelle[p];
+        int ii = o->hlist[icell];
+        while (ii != -1) {
+          int jj = (icell == jcell) ? o->lnk[ii] : o->hlist[jcell];
+          while (jj != -1) {
+            if (!exclij(ii, jj, o->cexcl_off, o->cexcl_idx)) test_el(o, ii, jj);
+            jj = o->lnk[jj];
+          }
+          ii = o->lnk[ii];
+        }
+      }
+    }
+  }
+  /* positions snapshot  ngbr_list.c:577-580 */
+  memcpy(o->dxn, o->px, n * 8.);
+  memcpy(o->dxn + n, o->py, n * 8.);
+  memcpy(o->dxn + 2 * n, o->pz, n * 8.);
+  o->rebuilds++;
+}
+
+long long orc_list_count(orc *o, int which)
+{
+  return which == 0 ? o->nprt : which == 1 ? o->nprs : which == 2 ? o->nprte : o->nprse;
+}
+void orc_get_list(orc *o, int which, int *ip, int *jp)
+{
+  long long n = orc_list_count(o, which);
+  int *a = which == 0 ? o->inpt : which == 1 ? o->inps : which == 2 ? o->inpte : o->inpse;
+  int *b = which == 0 ? o->jnpt : which == 1 ? o->jnps : which == 2 ? o->jnpte : o->jnpse;
+  if (n > 0) {
+    memcpy(ip, a, sizeof(int) * (size_t)n);
+    memcpy(jp, b, sizeof(int) * (size_t)n);
+  }
+}
+
+/* ------------------------------------------------------- pair kernels */
+/* 3-point table interpolation  md_fnopol.c:148 */
+#define INTERP(t, k, p) ((t)[k] + .5 * (p) * ((t)[(k) + 1] - (t)[(k) - 1] + (p) * ((t)[(k) - 1] - 2. * (t)[k] + (t)[(k) + 1])))
+
+/* force_npol  energy/inter/md_fnopol.c:46-255 over one chunk */
+static void force_npol(orc *o, int nlen, const int *indx, const int *jndx, int iflg)
+{
+  int n = o->n, n2 = 2 * n, j;
+  const double *rmax2 = iflg == 0 ? o->rmaxs_cut2 : o->rmaxl_cut2;
+  double spotlt = 0., spothlt = 0.;
+  double *xd = (double *)malloc(6 * sizeof(double) * (size_t)(nlen > 0 ? nlen : 1));
+  double *yd = xd + nlen, *zd = xd + 2 * nlen, *fxd = xd + 3 * nlen, *fyd = xd + 4 * nlen,
+         *fzd = xd + 5 * nlen;
+  int ntm4 = o->ntable - 4;
+  double hi[9];
+  gethinv9(o->hmat, hi);
+  for (j = 0; j < nlen; j++) {
+    xd[j] = o->px[indx[j]] - o->px[jndx[j]];
+    yd[j] = o->py[indx[j]] - o->py[jndx[j]];
+    zd[j] = o->pz[indx[j]] - o->pz[jndx[j]];
+  }
+  period(nlen, xd, yd, zd, o->hmat, hi);
+  for (j = 0; j < nlen; j++) {
+    int in = o->map[o->itype[indx[j]] * o->ntypes + o->itype[jndx[j]]];
+    double dis2 = xd[j] * xd[j] + yd[j] * yd[j] + zd[j] * zd[j];
+    if (dis2 < rmax2[in]) {
+      double p = (dis2 - o->rmins_cut2[in]) * o->dx2tab[in], f, swv;
+      int k = (int)p;
+      const double *t = o->dvtab + (size_t)in * o->ntable;
+      if (k < 1) {
+        o->underflows++;
+        k = 1;
+        p = 1.;
+      }
+      p = p - (double)k;
+      f = INTERP(t, k, p);
+      if (dis2 > o->rminl_cut2[in]) {
+        const double *sw = o->switchs + (size_t)in * o->ntable;
+        swv = INTERP(sw, k, p);
+      } else {
+        swv = 1.;
+      }
+      if (iflg == 1) {
+        const double *vt = o->vtab + (size_t)in * o->ntable;
+        double fcc;
+        o->sprsl -= dis2 * f;
+        o->sprslt[0] -= xd[j] * xd[j] * f;
+        o->sprslt[1] -= yd[j] * xd[j] * f;
+        o->sprslt[2] -= zd[j] * xd[j] * f;
+        o->sprslt[4] -= yd[j] * yd[j] * f;
+        o->sprslt[5] -= zd[j] * yd[j] * f;
+        o->sprslt[8] -= zd[j] * zd[j] * f;
+        xd[j] *= f;
+        yd[j] *= f;
+        zd[j] *= f;
+        fxd[j] = xd[j] * swv;
+        fyd[j] = yd[j] * swv;
+        fzd[j] = zd[j] * swv;
+        fcc = INTERP(vt, k, p);
+        spotlt += fcc;
+        spothlt += fcc - vt[ntm4];
+      } else {
+        f *= swv;
+        xd[j] *= f;
+        yd[j] *= f;
+        zd[j] *= f;
+      }
+    } else {
+      xd[j] = yd[j] = zd[j] = 0.;
+      fxd[j] = fyd[j] = fzd[j] = 0.;
+    }
+  }
+  if (iflg == 1) {
+    o->sprslt[3] = o->sprslt[1];
+    o->sprslt[6] = o->sprslt[2];
+    o->sprslt[7] = o->sprslt[5];
+  }
+  o->spotl += spotlt;
+  o->spothl += spothlt;
+  for (j = 0; j < nlen; j++) {
+    int ni = indx[j], nj = jndx[j];
+    o->scr[ni] -= xd[j];
+    o->scr[ni + n] -= yd[j];
+    o->scr[ni + n2] -= zd[j];
+    o->scr[nj] += xd[j];
+    o->scr[nj + n] += yd[j];
+    o->scr[nj + n2] += zd[j];
+    if (iflg == 1) {
+      o->rec[ni] -= fxd[j];
+      o->rec[ni + n] -= fyd[j];
+      o->rec[ni + n2] -= fzd[j];
+      o->rec[nj] += fxd[j];
+      o->rec[nj + n] += fyd[j];
+      o->rec[nj + n2] += fzd[j];
+    }
+  }
+  free(xd);
+}
+
+/* force_ter  energy/control/md_finter.c:110-310 (verlist branch) */
+void orc_force_ter(orc *o, int iflg)
+{
+  int n3 = 3 * o->n, i;
+  long long np = iflg == 0 ? o->nprs : o->nprt, s;
+  const int *ip = iflg == 0 ? o->inps : o->inpt, *jp = iflg == 0 ? o->jnps : o->jnpt;
+  double *fx = iflg == 0 ? o->fxs : o->fxl;
+  if (iflg == 1) {
+    o->spotl = o->spothl = o->sprsl = 0.;
+    for (i = 0; i < 9; i++) o->sprslt[i] = 0.;
+    for (i = 0; i < n3; i++) o->scr[i] = o->rec[i] = 0.;
+  } else {
+    for (i = 0; i < n3; i++) o->scr[i] = 0.;
+  }
+  for (s = 0; s < np; s += o->nlen) {
+    int k = (int)(np - s < o->nlen ? np - s : o->nlen);
+    force_npol(o, k, ip + s, jp + s, iflg);
+  }
+  for (i = 0; i < n3; i++) fx[i] += o->scr[i];
+  if (iflg == 1)
+    for (i = 0; i < n3; i++) o->fxs[i] += o->rec[i];
+}
+
+/* force_e  energy/inter/finter_e.c:42-233 over one chunk; note the
+   fall-through of its switch (finter_e.c:72-83): both levels use the full
+   rmaxl_coul2 cutoff and the switch never engages */
+static void force_e(orc *o, int nlen, const int *indx, const int *jndx, int iflg)
+{
+  int n = o->n, n2 = 2 * n, j, ntable = o->ntable;
+  double rmax2 = o->rmaxl_coul2, rmin2 = o->rmaxl_coul2, tablast = o->coultab[ntable - 4];
+  double sphet = 0., spet = 0.;
+  double *xd = (double *)malloc(10 * sizeof(double) * (size_t)(nlen > 0 ? nlen : 1));
+  double *yd = xd + nlen, *zd = xd + 2 * nlen, *fxd = xd + 3 * nlen, *fyd = xd + 4 * nlen,
+         *fzd = xd + 5 * nlen, *qij = xd + 6 * nlen, *fx = xd + 7 * nlen, *fy = xd + 8 * nlen,
+         *fz = xd + 9 * nlen;
+  double hi[9];
+  gethinv9(o->hmat, hi);
+  for (j = 0; j < nlen; j++) {
+    xd[j] = o->px[indx[j]] - o->px[jndx[j]];
+    yd[j] = o->py[indx[j]] - o->py[jndx[j]];
+    zd[j] = o->pz[indx[j]] - o->pz[jndx[j]];
+    qij[j] = o->qch[indx[j]] * o->qch[jndx[j]];
+  }
+  period(nlen, xd, yd, zd, o->hmat, hi);
+  for (j = 0; j < nlen; j++) {
+    double dis2 = xd[j] * xd[j] + yd[j] * yd[j] + zd[j] * zd[j];
+    if (dis2 < rmax2) {
+      double p = (dis2 - o->rmins_coul2) * o->dx2coul, f, swv, fcc, q;
+      int k = (int)p;
+      if (k < 1) {
+        o->underflows++;
+        k = 1;
+        p = 1;
+      }
+      p = p - (double)k;
+      f = INTERP(o->dcoultab, k, p);
+      if (dis2 > rmin2) swv = INTERP(o->switchse, k, p);
+      else swv = 1.;
+      q = qij[j];
+      fcc = q * f;
+      if (iflg == 1) {
+        o->sprse -= dis2 * fcc;
+        o->sprset[0] -= xd[j] * xd[j] * fcc;
+        o->sprset[1] -= yd[j] * xd[j] * fcc;
+        o->sprset[2] -= zd[j] * xd[j] * fcc;
+        o->sprset[4] -= yd[j] * yd[j] * fcc;
+        o->sprset[5] -= zd[j] * yd[j] * fcc;
+        o->sprset[8] -= zd[j] * zd[j] * fcc;
+        fx[j] = xd[j] * fcc;
+        fy[j] = yd[j] * fcc;
+        fz[j] = zd[j] * fcc;
+        fxd[j] = fx[j] * swv;
+        fyd[j] = fy[j] * swv;
+        fzd[j] = fz[j] * swv;
+        f = INTERP(o->coultab, k, p);
+        sphet += q * (f - tablast);
+        spet += q * f;
+      } else {
+        fcc *= swv;
+        fx[j] = xd[j] * fcc;
+        fy[j] = yd[j] * fcc;
+        fz[j] = zd[j] * fcc;
+      }
+    } else {
+      fx[j] = fy[j] = fz[j] = 0.;
+      fxd[j] = fyd[j] = fzd[j] = 0.;
+    }
+  }
+  o->spothe += sphet;
+  o->spote += spet;
+  if (iflg == 1) {
+    o->sprset[3] = o->sprset[1];
+    o->sprset[6] = o->sprset[2];
+    o->sprset[7] = o->sprset[5];
+  }
+  for (j = 0; j < nlen; j++) {
+    int ni = indx[j], nj = jndx[j];
+    o->scr[ni] -= fx[j];
+    o->scr[ni + n] -= fy[j];
+    o->scr[ni + n2] -= fz[j];
+    o->scr[nj] += fx[j];
+    o->scr[nj + n] += fy[j];
+    o->scr[nj + n2] += fz[j];
+    if (iflg == 1) {
+      o->rec[ni] -= fxd[j];
+      o->rec[ni + n] -= fyd[j];
+      o->rec[ni + n2] -= fzd[j];
+      o->rec[nj] += fxd[j];
+      o->rec[nj + n] += fyd[j];
+      o->rec[nj + n2] += fzd[j];
+    }
+  }
+  free(xd);
+}
+
+/* force_ter_e  energy/control/md_finter_e.c:78-233 (verlist branch) */
+void orc_force_ter_e(orc *o, int iflg)
+{
+  int n3 = 3 * o->n, i;
+  long long np = iflg == 0 ? o->nprse : o->nprte, s;
+  const int *ip = iflg == 0 ? o->inpse : o->inpte, *jp = iflg == 0 ? o->jnpse : o->jnpte;
+  double *fx = iflg == 0 ? o->fxs : o->fxl;
+  for (i = 0; i < n3; i++) o->scr[i] = o->rec[i] = 0.;
+  if (iflg == 1) {
+    o->spothe = o->spote = o->sprse = 0.;
+    for (i = 0; i < 9; i++) o->sprset[i] = 0.;
+  }
+  if (o->ncharge == 0) return;
+  for (s = 0; s < np; s += o->nlen) {
+    int k = (int)(np - s < o->nlen ? np - s : o->nlen);
+    force_e(o, k, ip + s, jp + s, iflg);
+  }
+  for (i = 0; i < n3; i++) fx[i] += o->scr[i];
+  if (iflg == 1)
+    for (i = 0; i < n3; i++) o->fxs[i] += o->rec[i];
+}
+
+/* fk_ewald  energy/inter/md_ewald.c:185-361 (serial: one rank holds every k) */
+void orc_fk_ewald(orc *o)
+{
+  int nq = o->ncharge, i, j, n = o->n;
+  double fact = sqrt(4.0 * M_PI), hi[9], rvol, vk = 0., vp = 0., vpt[9] = {0};
+  double *tx, *ty, *tz, *tq, *cossc, *sinsc, *helr, *heli, six;
+  double *fx = o->fxl, *fy = o->fxl + n, *fz = o->fxl + 2 * n;
+  rvol = 1. / gethinv9(o->hmat, hi);
+  if (nq == 0 || o->ktot == 0) {
+    o->vk_ewald = o->vp_ewald = 0.;
+    memset(o->vp_ewald_tensor, 0, sizeof o->vp_ewald_tensor);
+    return;
+  }
+  tx = (double *)malloc(8 * sizeof(double) * (size_t)nq);
+  ty = tx + nq; tz = tx + 2 * nq; tq = tx + 3 * nq;
+  cossc = tx + 4 * nq; sinsc = tx + 5 * nq; helr = tx + 6 * nq; heli = tx + 7 * nq;
+  for (j = 0; j < nq; j++) {
+    int jj = o->icharge[j];
+    tx[j] = o->px[jj]; ty[j] = o->py[jj]; tz[j] = o->pz[jj];
+    tq[j] = o->qch[jj] * fact;
+  }
+  for (j = 0; j < nq; j++) {
+    double akc = (tx[j] * hi[6] + ty[j] * hi[7] + tz[j] * hi[8]) * TPI;
+    cossc[j] = cos(akc);
+    sinsc[j] = sin(akc);
+  }
+  for (i = 0; i < o->ktot; i++) {
+    double sx = TPI * o->ka[i], sy = TPI * o->kb[i], sz = TPI * o->kc[i];
+    double aka = (sx * hi[0] + sy * hi[3] + sz * hi[6]);
+    double akb = (sx * hi[1] + sy * hi[4] + sz * hi[7]);
+    double akc = (sx * hi[2] + sy * hi[5] + sz * hi[8]);
+    double g2 = aka * aka + akb * akb + akc * akc;
+    double preg = exp(-g2 * o->falp2) * rvol / g2;
+    double prep = -2. * preg * (g2 * o->falp2 + 1.) / g2;
+    double sumr, sumi, smag;
+    if (o->kup[i] || i == 0) {
+      for (j = 0; j < nq; j++) {
+        double rk = (tx[j] * aka + ty[j] * akb + tz[j] * akc);
+        helr[j] = cos(rk);
+        heli[j] = sin(rk);
+      }
+    } else {
+      for (j = 0; j < nq; j++) {
+        double rhr = helr[j], rhi = heli[j];
+        sumr = cossc[j];
+        sumi = sinsc[j];
+        helr[j] = rhr * sumr - rhi * sumi;
+        heli[j] = rhi * sumr + rhr * sumi;
+      }
+    }
+    sumr = sumi = 0.;
+    for (j = 0; j < nq; j++) {
+      sumr += tq[j] * helr[j];
+      sumi += tq[j] * heli[j];
+    }
+    smag = sumr * sumr + sumi * sumi;
+    vk += preg * smag;
+    vp += prep * smag * g2;
+    vpt[0] += prep * smag * aka * aka;
+    vpt[1] += prep * smag * akb * aka;
+    vpt[2] += prep * smag * akc * aka;
+    vpt[3] += prep * smag * aka * akb;
+    vpt[4] += prep * smag * akb * akb;
+    vpt[5] += prep * smag * akc * akb;
+    vpt[6] += prep * smag * aka * akc;
+    vpt[7] += prep * smag * akb * akc;
+    vpt[8] += prep * smag * akc * akc;
+    sumr *= 2. * preg;
+    sumi *= 2. * preg;
+    for (j = 0; j < nq; j++) {
+      int jj = o->icharge[j];
+      double q = tq[j], rhr = helr[j], rhi = heli[j];
+      double srx = aka * sumr * q, sry = akb * sumr * q, srz = akc * sumr * q;
+      double sxi = aka * sumi * q, syi = akb * sumi * q, szi = akc * sumi * q;
+      fx[jj] += srx * rhi - sxi * rhr;
+      fy[jj] += sry * rhi - syi * rhr;
+      fz[jj] += srz * rhi - szi * rhr;
+    }
+  }
+  six = o->ewald_bkg / get_deth(o->hmat);
+  o->vk_ewald = vk + six + o->ewald_self;
+  o->vp_ewald = vp + 3. * (vk + six);
+  for (i = 0; i < 9; i++) o->vp_ewald_tensor[i] = vpt[i];
+  o->vp_ewald_tensor[0] += vk + six;
+  o->vp_ewald_tensor[4] += vk + six;
+  o->vp_ewald_tensor[8] += vk + six;
+  free(tx);
+}
+
+/* ecorr  energy/inter/md_ewald.c:385-453 (no minimum image, as in CM3D) */
+void orc_ecorr(orc *o)
+{
+  int i, n = o->n;
+  double spot = 0., sprs = 0., st[9] = {0}, sqrt_pi = 1. / sqrt(M_PI);
+  double *fx = o->fxl, *fy = o->fxl + n, *fz = o->fxl + 2 * n;
+  for (i = 0; i < o->necorr; i++) {
+    int ii = o->iecorr[i], jj = o->jecorr[i];
+    double xd = o->px[ii] - o->px[jj], yd = o->py[ii] - o->py[jj], zd = o->pz[ii] - o->pz[jj];
+    double dis2 = xd * xd + yd * yd + zd * zd, dis = sqrt(dis2);
+    double qijr = o->qch[ii] * o->qch[jj] / dis, ralp = dis * o->kappa, erfr = erf(ralp), dv;
+    spot += -qijr * erfr;
+    dv = -qijr * (-2. * o->kappa * exp(-o->kappa2 * dis2) * sqrt_pi + erfr / dis);
+    sprs += dis * dv;
+    dv /= dis;
+    st[0] += dv * xd * xd; st[1] += dv * xd * yd; st[2] += dv * xd * zd;
+    st[3] += dv * yd * xd; st[4] += dv * yd * yd; st[5] += dv * yd * zd;
+    st[6] += dv * zd * xd; st[7] += dv * zd * yd; st[8] += dv * zd * zd;
+    xd *= dv; yd *= dv; zd *= dv;
+    fx[ii] += xd; fy[ii] += yd; fz[ii] += zd;
+    fx[jj] -= xd; fy[jj] -= yd; fz[jj] -= zd;
+  }
+  o->pot_ecorr = spot;
+  o->prs_ecorr = sprs;
+  memcpy(o->prs_ecorr_tensor, st, sizeof st);
+}
+
+/* fbond  energy/intra/md_fbond.c:76-125 (harmonic) */
+void orc_fbond(orc *o)
+{
+  int nb, n = o->n;
+  double *fx = o->fxa, *fy = o->fxa + n, *fz = o->fxa + 2 * n;
+  for (nb = 0; nb < o->nbonds; nb++) {
+    int i = o->ibond[nb], j = o->jbond[nb], idx = o->idxbond[nb];
+    double dx = o->px[i] - o->px[j], dy = o->py[i] - o->py[j], dz = o->pz[i] - o->pz[j];
+    double r = sqrt(dx * dx + dy * dy + dz * dz), dr = r - o->eqbond[idx];
+    double fr = o->fkbond[idx] * dr / r;
+    dx *= fr; dy *= fr; dz *= fr;
+    fx[i] -= dx; fy[i] -= dy; fz[i] -= dz;
+    fx[j] += dx; fy[j] += dy; fz[j] += dz;
+  }
+}
+
+/* fbend  energy/intra/md_fbend.c:126-260 (harmonic) */
+void orc_fbend(orc *o)
+{
+  int nb, n = o->n;
+  double *fx = o->fxa, *fy = o->fxa + n, *fz = o->fxa + 2 * n;
+  double *f9 = (double *)malloc(9 * sizeof(double) * (size_t)(o->nbends > 0 ? o->nbends : 1));
+  for (nb = 0; nb < o->nbends; nb++) {
+    int i = o->ibend[nb], j = o->jbend[nb], k = o->kbend[nb], idx = o->idxbend[nb];
+    double ax = o->px[i] - o->px[j], ay = o->py[i] - o->py[j], az = o->pz[i] - o->pz[j];
+    double al = ax * ax + ay * ay + az * az;
+    double bx = o->px[k] - o->px[j], by = o->py[k] - o->py[j], bz = o->pz[k] - o->pz[j];
+    double bl = bx * bx + by * by + bz * bz;
+    double adotb = ax * bx + ay * by + az * bz;
+    double r11 = 1. / sqrt(al * bl), costh = adotb * r11, th, dth, dudth, dthdcos, dudcos;
+    double d1x, d1y, d1z, d3x, d3y, d3z;
+    if (fabs(costh) >= 1.) {
+      dthdcos = -1.;
+      dudth = 0.;
+    } else {
+      th = acos(costh);
+      dth = th - o->eqbend[idx];
+      dudth = o->fkbend[idx] * dth;
+      dthdcos = -1. / sqrt(1. - costh * costh);
+    }
+    dudcos = dudth * dthdcos;
+    d1x = costh * ax / al - bx * r11;
+    d1y = costh * ay / al - by * r11;
+    d1z = costh * az / al - bz * r11;
+    d3x = costh * bx / bl - ax * r11;
+    d3y = costh * by / bl - ay * r11;
+    d3z = costh * bz / bl - az * r11;
+    f9[9 * nb + 0] = dudcos * d1x;
+    f9[9 * nb + 1] = dudcos * d1y;
+    f9[9 * nb + 2] = dudcos * d1z;
+    f9[9 * nb + 3] = dudcos * (-d1x - d3x);
+    f9[9 * nb + 4] = dudcos * (-d1y - d3y);
+    f9[9 * nb + 5] = dudcos * (-d1z - d3z);
+    f9[9 * nb + 6] = dudcos * d3x;
+    f9[9 * nb + 7] = dudcos * d3y;
+    f9[9 * nb + 8] = dudcos * d3z;
+  }
+  for (nb = 0; nb < o->nbends; nb++) {
+    int i = o->ibend[nb], j = o->jbend[nb], k = o->kbend[nb];
+    fx[i] += f9[9 * nb + 0]; fy[i] += f9[9 * nb + 1]; fz[i] += f9[9 * nb + 2];
+    fx[j] += f9[9 * nb + 3]; fy[j] += f9[9 * nb + 4]; fz[j] += f9[9 * nb + 5];
+    fx[k] += f9[9 * nb + 6]; fy[k] += f9[9 * nb + 7]; fz[k] += f9[9 * nb + 8];
+  }
+  free(f9);
+}
+
+/* rmass  utils/md_util.new.c:219 */
+void orc_rmass(orc *o, int which)
+{
+  double *b = block(o, which);
+  int i, n = o->n;
+  for (i = 0; i < n; i++) {
+    double r = 1. / o->amass[i];
+    b[i] *= r;
+    b[i + n] *= r;
+    b[i + 2 * n] *= r;
+  }
+}
+
+/* force  energy/control/md_fcntr.c:44-134 (levels 0, 1, 2) */
+void orc_force(orc *o, int iflg)
+{
+  switch (iflg) {
+    case 0:
+      orc_zero_forces(o, 1);
+      orc_force_ter(o, 0);
+      orc_force_ter_e(o, 0);
+      orc_rmass(o, 1);
+      break;
+    case 1:
+      orc_zero_forces(o, 1);
+      orc_zero_forces(o, 0);
+      orc_force_ter(o, 1);
+      orc_force_ter_e(o, 1);
+      if (o->iperd == 3) {
+        orc_fk_ewald(o);
+        orc_ecorr(o);
+      }
+      orc_rmass(o, 0);
+      orc_rmass(o, 1);
+      break;
+    case 2:
+      orc_zero_forces(o, 2);
+      orc_fbond(o);
+      orc_fbend(o);
+      orc_rmass(o, 2);
+      break;
+    default:
+      break;
+  }
+}
+
+/* getvbond / getvbend energies  md_fbond.c:131-220, md_fbend.c:262-410
+   (the bend virial is compiled only with -DPRESSURE, off by default) */
+static void bonded_energies(orc *o)
+{
+  int nb, i;
+  o->vbond = o->wbond = o->vbend = 0.;
+  for (i = 0; i < 9; i++) o->wbondt[i] = 0.;
+  for (nb = 0; nb < o->nbonds; nb++) {
+    int a = o->ibond[nb], b = o->jbond[nb], idx = o->idxbond[nb];
+    double dx = o->px[a] - o->px[b], dy = o->py[a] - o->py[b], dz = o->pz[a] - o->pz[b];
+    double r = sqrt(dx * dx + dy * dy + dz * dz), dr = r - o->eqbond[idx];
+    double fk = o->fkbond[idx];
+    o->vbond += .5 * fk * dr * dr;
+    fk = fk * dr / r;
+    o->wbond -= fk * r * r;
+    o->wbondt[0] -= fk * dx * dx; o->wbondt[1] -= fk * dy * dx; o->wbondt[2] -= fk * dz * dx;
+    o->wbondt[3] -= fk * dx * dy; o->wbondt[4] -= fk * dy * dy; o->wbondt[5] -= fk * dz * dy;
+    o->wbondt[6] -= fk * dx * dz; o->wbondt[7] -= fk * dy * dz; o->wbondt[8] -= fk * dz * dz;
+  }
+  for (nb = 0; nb < o->nbends; nb++) {
+    int a = o->ibend[nb], b = o->jbend[nb], c = o->kbend[nb], idx = o->idxbend[nb];
+    double ax = o->px[a] - o->px[b], ay = o->py[a] - o->py[b], az = o->pz[a] - o->pz[b];
+    double al = ax * ax + ay * ay + az * az;
+    double bx = o->px[c] - o->px[b], by = o->py[c] - o->py[b], bz = o->pz[c] - o->pz[b];
+    double bl = bx * bx + by * by + bz * bz;
+    double r11 = 1. / sqrt(al * bl), costh = (ax * bx + ay * by + az * bz) * r11, th, dth;
+    costh = costh < 1. ? costh : 1.;
+    costh = costh > -1. ? costh : -1.;
+    th = fabs(costh) >= 1. ? 1. : acos(costh);
+    dth = th - o->eqbend[idx];
+    o->vbend += .5 * o->fkbend[idx] * dth * dth;
+  }
+}
+
+/* getvireal(...,1) + geteng  md_fcntr.c:136-308 for the terms of this path */
+void orc_get_energies(orc *o, cm3d_nb_energies *e)
+{
+  int i, n = o->n;
+  double vol = get_deth(o->hmat), rvol = 1. / vol, p2m;
+  memset(e, 0, sizeof *e);
+  e->vhinter = o->spothl;
+  e->vinter = o->spotl;
+  e->winter = o->sprsl;
+  for (i = 0; i < 9; i++) e->wintertensor[i] = o->sprslt[i];
+  e->velec = o->spote;
+  e->welec = o->sprse;
+  for (i = 0; i < 9; i++) e->welectensor[i] = o->sprset[i];
+  if (o->iperd == 3) {
+    e->vewald = o->vk_ewald + o->pot_ecorr;
+    e->wewald = o->vp_ewald + o->prs_ecorr;
+    for (i = 0; i < 9; i++) e->wewaldtensor[i] = o->vp_ewald_tensor[i] + o->prs_ecorr_tensor[i];
+  }
+  bonded_energies(o);
+  e->vbond = o->vbond;
+  e->wbond = o->wbond;
+  e->vbend = o->vbend;
+  e->wbend = 0.;
+  e->US = e->vhinter + e->velec + e->vewald;
+  e->U = e->vinter + e->velec + e->vewald;
+  e->W = e->winter + e->welec + e->wewald;
+  for (i = 0; i < 9; i++) e->Wtensor[i] = e->wintertensor[i] + e->welectensor[i] + e->wewaldtensor[i];
+  if (o->iperd == 3) {
+    e->W -= 3 * o->wlrc * rvol;
+    e->Wtensor[0] -= o->wlrc * rvol;
+    e->Wtensor[4] -= o->wlrc * rvol;
+    e->Wtensor[8] -= o->wlrc * rvol;
+  }
+  /* get_p2mt  md_fcntr.c:332-354 */
+  for (i = 0; i < n; i++) {
+    double am = o->amass[i];
+    e->p2m_tensor[0] += am * (o->vx[i] * o->vx[i]);
+    e->p2m_tensor[4] += am * (o->vy[i] * o->vy[i]);
+    e->p2m_tensor[8] += am * (o->vz[i] * o->vz[i]);
+    e->p2m_tensor[1] += am * (o->vy[i] * o->vx[i]);
+    e->p2m_tensor[2] += am * (o->vz[i] * o->vx[i]);
+    e->p2m_tensor[5] += am * (o->vz[i] * o->vy[i]);
+  }
+  e->p2m_tensor[3] = e->p2m_tensor[1];
+  e->p2m_tensor[6] = e->p2m_tensor[2];
+  e->p2m_tensor[7] = e->p2m_tensor[5];
+  p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
+  {
+    double UI = e->vbond + e->vbend, WI = e->wbond, wit[9];
+    for (i = 0; i < 9; i++) wit[i] = o->wbondt[i];
+    e->poth = e->US;
+    e->poter = e->U;
+    e->potra = UI;
+    if (o->iperd == 3) {
+      e->poter += o->vlrc / vol;
+      e->poth += o->vlrc / vol;
+    }
+    e->prsi = (p2m + e->W + WI) / (3 * vol);
+    for (i = 0; i < 9; i++) e->prs_tensor[i] = (e->p2m_tensor[i] + e->Wtensor[i] + wit[i]) / vol;
+  }
+  e->zke = .5 * p2m;
+  e->tiout = p2m / (double)o->ndof;
+}
+
+/* nrefsh  energy/control/md_finter.c:43-108 (verlist branch) */
+static void nrefsh(orc *o, int istep)
+{
+  int i, n = o->n, iflag = 0;
+  double skin2 = .25 * o->skin * o->skin;
+  for (i = 0; i < n; i++) {
+    double xc = o->dxn[i] - o->px[i], yc = o->dxn[i + n] - o->py[i], zc = o->dxn[i + 2 * n] - o->pz[i];
+    if (xc * xc + yc * yc + zc * zc > skin2) {
+      iflag = 1;
+      break;
+    }
+  }
+  if (iflag) {
+    if (istep - o->isteplast < 3) {
+      o->resets++;
+      for (i = 0; i < n; i++) {
+        double xc = o->px[i] - o->dxn[i], yc = o->py[i] - o->dxn[i + n], zc = o->pz[i] - o->dxn[i + 2 * n];
+        if (xc * xc + yc * yc + zc * zc > skin2) {
+          double scale = skin2 / (xc * xc + yc * yc + zc * zc);
+          o->px[i] = o->dxn[i] + scale * xc;
+          o->py[i] = o->dxn[i + n] + scale * yc;
+          o->pz[i] = o->dxn[i + 2 * n] + scale * zc;
+        }
+      }
+    }
+    orc_get_ngbr(o);
+    o->isteplast = istep;
+  }
+}
+
+/* step_init  integrate/md_step.c:32-59 (nonbonded + bonded levels) */
+void orc_step_init(orc *o)
+{
+  o->isteplast = 0;
+  orc_get_ngbr(o);
+  orc_force(o, 1);
+  orc_force(o, 2);
+}
+
+/* step  integrate/md_step.c:62-159 (NVE, no torsion level) */
+void orc_step(orc *o, int istep0, int nsteps)
+{
+  int s, n3 = 3 * o->n, i;
+  int ninter = o->nres_lrf, ninrra = o->nres_tors, ninnra = o->nres_intra;
+  double dtl2 = .5 * o->dt, dts2 = dtl2 / (double)ninter, dtr2 = dts2 / (double)ninrra;
+  double dta2 = dtr2 / (double)ninnra, dter = (double)ninter * dts2,
+         dter1 = (double)(1 - ninter) * dts2;
+  double *pos = o->px, *vel = o->vx;
+  /* CM3D keeps px,py,pz (and vx,vy,vz) contiguous (md_util.new.c:113-119) and
+     loops over 3N; the oracle keeps separate arrays, so loop per block */
+  double *P[3] = {o->px, o->py, o->pz}, *V[3] = {o->vx, o->vy, o->vz};
+  int n = o->n;
+  (void)pos; (void)vel; (void)n3;
+  for (s = 0; s < nsteps; s++) {
+    int istep = istep0 + s, intr, inrra, intra, c;
+    for (intr = 0; intr < ninter; intr++) {
+      for (c = 0; c < 3; c++) {
+        if (intr == 0) {
+          for (i = 0; i < n; i++) V[c][i] += dter * o->fxl[c * n + i] + dter1 * o->fxs[c * n + i];
+        } else {
+          for (i = 0; i < n; i++) V[c][i] += dts2 * o->fxs[c * n + i];
+        }
+      }
+      for (inrra = 0; inrra < ninrra; inrra++) {
+        /* the torsion level contributes fxr = 0 (no torsions in the engine) */
+        for (intra = 0; intra < ninnra; intra++) {
+          for (c = 0; c < 3; c++)
+            for (i = 0; i < n; i++) V[c][i] += dta2 * o->fxa[c * n + i];
+          for (c = 0; c < 3; c++)
+            for (i = 0; i < n; i++) P[c][i] += dta2 * V[c][i];
+          for (c = 0; c < 3; c++)
+            for (i = 0; i < n; i++) P[c][i] += dta2 * V[c][i];
+          orc_force(o, 2);
+          for (c = 0; c < 3; c++)
+            for (i = 0; i < n; i++) V[c][i] += dta2 * o->fxa[c * n + i];
+        }
+        for (c = 0; c < 3; c++)
+          for (i = 0; i < n; i++) V[c][i] += dtr2 * 0.0;
+      }
+      nrefsh(o, istep);
+      if (intr == ninter - 1) {
+        orc_force(o, 1);
+        for (c = 0; c < 3; c++)
+          for (i = 0; i < n; i++) V[c][i] += dter * o->fxl[c * n + i] + dter1 * o->fxs[c * n + i];
+      } else {
+        orc_force(o, 0);
+        for (c = 0; c < 3; c++)
+          for (i = 0; i < n; i++) V[c][i] += dts2 * o->fxs[c * n + i];
+      }
+    }
+  }
+}
+
+long long orc_rebuilds(orc *o) { return o->rebuilds; }
+long long orc_resets(orc *o) { return o->resets; }
+long long orc_underflows(orc *o) { return o->underflows; }
