@@ -1,0 +1,869 @@
+// nb_capi.cu -- the extern "C" entry points of include/cm3d_nb.h.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "nb_common.cuh"
+
+namespace cm3d {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  set_error("CUDA error in %s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+  if (e == cudaErrorMemoryAllocation) return CM3D_NB_ERR_NOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return CM3D_NB_ERR_NODEV;
+  return CM3D_NB_ERR_CUDA;
+}
+
+void tbegin(Ctx *c, int cls, cudaEvent_t *e0) {
+  *e0 = nullptr;
+  if (!c->timing.on) return;
+  cudaEvent_t a, b;
+  if (c->timing.pool.size() >= 1) {
+    a = c->timing.pool.back().first;
+    b = c->timing.pool.back().second;
+    c->timing.pool.pop_back();
+  } else {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+  }
+  cudaEventRecord(a, c->st);
+  c->timing.pending[cls].push_back({a, b});
+  *e0 = a;
+}
+
+void tend(Ctx *c, int cls, cudaEvent_t e0) {
+  if (!c->timing.on || !e0) return;
+  cudaEventRecord(c->timing.pending[cls].back().second, c->st);
+  c->timing.launches[cls]++;
+}
+
+static void collect_timing(Ctx *c) {
+  cudaStreamSynchronize(c->st);
+  for (int k = 0; k < 4; k++) {
+    for (auto &pr : c->timing.pending[k]) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, pr.first, pr.second);
+      c->timing.ms[k] += ms;
+      c->timing.pool.push_back(pr);
+    }
+    c->timing.pending[k].clear();
+  }
+}
+
+template <typename T>
+static int upload(T **dst, const T *src, size_t count) {
+  size_t bytes = sizeof(T) * (count > 0 ? count : 1);
+  CK(cudaMalloc(dst, bytes));
+  if (src && count) CK(cudaMemcpy(*dst, src, sizeof(T) * count, cudaMemcpyHostToDevice));
+  else CK(cudaMemset(*dst, 0, bytes));
+  return CM3D_NB_OK;
+}
+
+static void destroy(Ctx *c) {
+  if (!c) return;
+  cudaSetDevice(c->dev);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  void *ptrs[] = {c->pos, c->vel, c->fxl, c->fxs, c->fxa, c->mass, c->q, c->dxn, c->snap, c->itype, c->map,
+                  c->vtab, c->dvtab, c->switchs, c->icut, c->coultab, c->dcoultab, c->switchse, c->excl_off,
+                  c->excl_idx, c->cexcl_off, c->cexcl_idx, c->ftab_lj, c->ftab_el, c->fcut, c->rows, c->row_k0,
+                  c->sk, c->spart, c->akf, c->akd, c->kfrac, c->kposd, c->icharge, c->ka_d, c->kb_d, c->kc_d,
+                  c->ecorr_pairs, c->grp_atom_off, c->grp_atoms, c->grp_bond_off, c->grp_bend_off,
+                  c->grp_ecorr_off, c->bond_ij, c->bond_p, c->bend_ijk, c->bend_p, c->ecorr_ij, c->cell_of,
+                  c->cell_start, c->cell_cursor, c->cell_atoms, c->rank, c->cnt, c->off, c->ltot, c->lst[0],
+                  c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->styp, c->shift, c->corner, c->cimg, c->acc,
+                  c->stat, c->istate};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot};
+  for (void *p : hp)
+    if (p) cudaFreeHost(p);
+  for (int k = 0; k < 4; k++)
+    for (auto &pr : c->timing.pending[k]) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  for (auto &pr : c->timing.pool) {
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out) {
+  if (!s || !out) {
+    set_error("cm3d_nb_create: null argument");
+    return CM3D_NB_ERR_ARG;
+  }
+  if (s->natoms <= 0) {
+    set_error("cm3d_nb_create: natoms = %d", s->natoms);
+    return CM3D_NB_ERR_ARG;
+  }
+  if (s->iperd != 3) {
+    set_error("cm3d_nb_create: only iperd 3 (three-dimensional periodicity) is supported, got %d", s->iperd);
+    return CM3D_NB_ERR_ARG;
+  }
+  if (s->ntable < 5) {
+    set_error("cm3d_nb_create: ntable = %d is too small", s->ntable);
+    return CM3D_NB_ERR_ARG;
+  }
+  cm3d_nb_options o;
+  cm3d_nb_default_options(&o);
+  if (opt) o = *opt;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_error("cm3d_nb_create: no CUDA device (%s)", e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
+    return CM3D_NB_ERR_NODEV;
+  }
+  if (o.mode == CM3D_NB_MIXED && s->natoms > MAX_ATOMS_MIXED) {
+    set_error("cm3d_nb_create: the mixed engine holds at most %d atoms per system", MAX_ATOMS_MIXED);
+    return CM3D_NB_ERR_ARG;
+  }
+  Ctx *c = new Ctx();
+  *out = c;
+  c->dev = o.device;
+  CK(cudaSetDevice(c->dev));
+  CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  c->mode = o.mode;
+  c->need_short = o.need_short;
+  c->tpa = o.tpa;
+  c->use_graph = o.use_graph;
+  const int n = s->natoms;
+  c->n = n;
+  c->ntypes = s->ntypes;
+  c->ninter = s->ninter;
+  c->ntable = s->ntable;
+  c->iperd = s->iperd;
+  c->nres_lrf = s->nres_lrf > 0 ? s->nres_lrf : 1;
+  c->nres_intra = s->nres_intra > 0 ? s->nres_intra : 1;
+  c->nres_tors = s->nres_tors > 0 ? s->nres_tors : 1;
+  c->ndof = s->ndof > 0 ? s->ndof : 1;
+  c->dt = s->dt;
+  c->vlrc = s->vlrc;
+  c->wlrc = s->wlrc;
+  c->skin = s->skin_ter;
+  c->rheal = s->rheal;
+  memcpy(c->hmat, s->hmat, sizeof c->hmat);
+  {
+    const double *h = c->hmat;
+    double *hi = c->hmati;
+    double rvol = 1. / (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                        h[2] * (h[3] * h[7] - h[4] * h[6]));
+    hi[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
+    hi[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
+    hi[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
+    hi[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
+    hi[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
+    hi[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
+    hi[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
+    hi[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
+    hi[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
+  }
+  c->kappa = s->kappa;
+  c->kappa2 = s->kappa * s->kappa;
+  c->falp2 = s->falp2;
+  c->ewald_self = s->ewald_self;
+  c->ewald_bkg = s->ewald_bkg;
+  c->dx2coul = s->dx2coul;
+  c->rmins_coul2 = s->rmins_coul2;
+  c->rmaxs_coul2 = s->rmaxs_coul2;
+  c->rminl_coul2 = s->rminl_coul2;
+  c->rmaxl_coul2 = s->rmaxl_coul2;
+  c->rmaxs_skin2_e = s->rmaxs_skin2_e;
+  c->rmaxl_skin2_e = s->rmaxl_skin2_e;
+  c->ktot = s->ktot;
+  c->necorr = s->necorr;
+  c->nbonds = s->nbonds;
+  c->nbends = s->nbends;
+  // charged atoms (set_charges, elec_ngbr.c:115-121)
+  std::vector<int> ich;
+  for (int i = 0; i < n; i++)
+    if (s->qch[i] != 0.) ich.push_back(i);
+  c->ncharge = (int)ich.size();
+  if (c->ncharge > 0 && (!s->coultab || !s->dcoultab)) {
+    set_error("cm3d_nb_create: charged atoms but no coultab/dcoultab");
+    return CM3D_NB_ERR_ARG;
+  }
+  c->tablast_e = c->ncharge > 0 ? s->coultab[s->ntable - 4] : 0.0;
+  // largest list radius
+  double r2 = 0;
+  std::vector<double> icut(8 * (size_t)(s->ninter > 0 ? s->ninter : 1), 0.0);
+  for (int in = 0; in < s->ninter; in++) {
+    icut[8 * in + 0] = s->rmaxs_cut2[in];
+    icut[8 * in + 1] = s->rmins_cut2[in];
+    icut[8 * in + 2] = s->rmaxl_cut2[in];
+    icut[8 * in + 3] = s->rminl_cut2[in];
+    icut[8 * in + 4] = s->rmaxs_skin2[in];
+    icut[8 * in + 5] = s->rmaxl_skin2[in];
+    icut[8 * in + 6] = s->dx2tab[in];
+    icut[8 * in + 7] = s->vtab[(size_t)in * s->ntable + s->ntable - 4];
+    r2 = std::max(r2, s->rmaxl_skin2[in]);
+    c->rc_lj_max = std::max(c->rc_lj_max, sqrt(s->rmaxl_cut2[in]));
+  }
+  if (c->ncharge > 0) r2 = std::max(r2, s->rmaxl_skin2_e);
+  c->rlist_max = sqrt(r2);
+  // device arrays
+  const size_t n3 = 3 * (size_t)n;
+  std::vector<double> pos(n3), vel(n3);
+  for (int i = 0; i < n; i++) {
+    pos[i] = s->px[i];
+    pos[n + i] = s->py[i];
+    pos[2 * n + i] = s->pz[i];
+    vel[i] = s->vx ? s->vx[i] : 0.;
+    vel[n + i] = s->vy ? s->vy[i] : 0.;
+    vel[2 * n + i] = s->vz ? s->vz[i] : 0.;
+  }
+  int rc;
+  if ((rc = upload(&c->pos, pos.data(), n3))) return rc;
+  if ((rc = upload(&c->vel, vel.data(), n3))) return rc;
+  if ((rc = upload<double>(&c->fxl, nullptr, n3))) return rc;
+  if ((rc = upload<double>(&c->fxs, nullptr, n3))) return rc;
+  if ((rc = upload<double>(&c->fxa, nullptr, n3))) return rc;
+  if ((rc = upload<double>(&c->dxn, pos.data(), n3))) return rc;
+  if ((rc = upload<double>(&c->snap, nullptr, 6 * n3 + 8))) return rc;
+  if ((rc = upload(&c->mass, s->amass, n))) return rc;
+  if ((rc = upload(&c->q, s->qch, n))) return rc;
+  if ((rc = upload(&c->itype, s->itype, n))) return rc;
+  if ((rc = upload(&c->map, s->map, (size_t)s->ntypes * s->ntypes))) return rc;
+  const size_t nt = (size_t)s->ninter * s->ntable;
+  if ((rc = upload(&c->vtab, s->vtab, nt))) return rc;
+  if ((rc = upload(&c->dvtab, s->dvtab, nt))) return rc;
+  if ((rc = upload(&c->switchs, s->switchs, nt))) return rc;
+  if ((rc = upload(&c->icut, icut.data(), icut.size()))) return rc;
+  if ((rc = upload(&c->coultab, c->ncharge ? s->coultab : nullptr, s->ntable))) return rc;
+  if ((rc = upload(&c->dcoultab, c->ncharge ? s->dcoultab : nullptr, s->ntable))) return rc;
+  if ((rc = upload(&c->switchse, c->ncharge && s->switchse ? s->switchse : nullptr, s->ntable))) return rc;
+  std::vector<int> zoff(n + 1, 0);
+  const int *eo = s->excl_off ? s->excl_off : zoff.data();
+  const int *co = s->cexcl_off ? s->cexcl_off : zoff.data();
+  if ((rc = upload(&c->excl_off, eo, n + 1))) return rc;
+  if ((rc = upload(&c->excl_idx, s->excl_idx, (size_t)eo[n]))) return rc;
+  if ((rc = upload(&c->cexcl_off, co, n + 1))) return rc;
+  if ((rc = upload(&c->cexcl_idx, s->cexcl_idx, (size_t)co[n]))) return rc;
+  if ((rc = upload(&c->icharge, ich.data(), ich.size()))) return rc;
+  // accumulators + device copies of hmati (ACC_COUNT..+9) and hmat (+9..+18)
+  std::vector<double> acc0(ACC_COUNT + 18, 0.0);
+  for (int k = 0; k < 9; k++) {
+    acc0[ACC_COUNT + k] = c->hmati[k];
+    acc0[ACC_COUNT + 9 + k] = c->hmat[k];
+  }
+  if ((rc = upload(&c->acc, acc0.data(), acc0.size()))) return rc;
+  if ((rc = upload<long long>(&c->stat, nullptr, ST_COUNT))) return rc;
+  if ((rc = upload<int>(&c->istate, nullptr, IS_COUNT))) return rc;
+  CK(cudaMallocHost(&c->h_acc, sizeof(double) * (ACC_COUNT + 18)));
+  CK(cudaMallocHost(&c->h_stat, sizeof(long long) * ST_COUNT));
+  CK(cudaMallocHost(&c->h_istate, sizeof(int) * IS_COUNT));
+  memset(c->h_istate, 0, sizeof(int) * IS_COUNT);
+  if ((rc = list_setup(c))) return rc;
+  if ((rc = pair_setup(c))) return rc;
+  if ((rc = kspace_setup(c, s))) return rc;
+  if ((rc = step_setup(c, s))) return rc;
+  if (s->ntors > 0 || s->n14 > 0 || s->nbondx > 0) c->name = "has-torsions";
+  CK(cudaDeviceSynchronize());
+  return CM3D_NB_OK;
+}
+
+__global__ void k_scale_rmass(int n, double *__restrict__ f, const double *__restrict__ mass) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double r = 1. / mass[i];
+  f[i] *= r;
+  f[n + i] *= r;
+  f[2 * n + i] *= r;
+}
+
+static double *block_of(Ctx *c, int which) {
+  return which == CM3D_NB_FXL ? c->fxl : which == CM3D_NB_FXS ? c->fxs : which == CM3D_NB_FXA ? c->fxa : nullptr;
+}
+
+static int pull_acc(Ctx *c) {
+  CK(cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * ACC_COUNT, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CM3D_NB_OK;
+}
+
+static void sym9(const double *a, int base, double t[9]) {
+  t[0] = a[base + 0];
+  t[1] = a[base + 1];
+  t[2] = a[base + 2];
+  t[4] = a[base + 4];
+  t[5] = a[base + 5];
+  t[8] = a[base + 8];
+  t[3] = t[1];
+  t[6] = t[2];
+  t[7] = t[5];
+}
+
+static double deth(const double *h) {
+  return (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+          h[2] * (h[3] * h[7] - h[4] * h[6]));
+}
+
+}  // namespace cm3d
+
+using namespace cm3d;
+
+extern "C" {
+
+struct cm3d_nb_ctx {
+  Ctx c;
+};
+
+int cm3d_nb_version(void) { return 10000; }
+
+const char *cm3d_nb_last_error(void) { return g_err; }
+
+int cm3d_nb_device_count(int *count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (count) *count = e == cudaSuccess ? n : 0;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+  return CM3D_NB_OK;
+}
+
+void cm3d_nb_default_options(cm3d_nb_options *opt) {
+  opt->device = 0;
+  opt->mode = CM3D_NB_MIXED;
+  opt->need_short = 0;
+  opt->tpa = 0;
+  opt->use_graph = 1;
+}
+
+int cm3d_nb_create(const cm3d_nb_system *sys, const cm3d_nb_options *opt, cm3d_nb_ctx **out) {
+  Ctx *c = nullptr;
+  int rc = create(sys, opt, &c);
+  if (rc) {
+    destroy(c);
+    if (out) *out = nullptr;
+    return rc;
+  }
+  *out = reinterpret_cast<cm3d_nb_ctx *>(c);
+  return CM3D_NB_OK;
+}
+
+void cm3d_nb_destroy(cm3d_nb_ctx *ctx) { destroy(reinterpret_cast<Ctx *>(ctx)); }
+
+#define CTX                                         \
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);            \
+  if (!c) {                                         \
+    set_error("null context");                      \
+    return CM3D_NB_ERR_ARG;                         \
+  }                                                 \
+  do {                                              \
+    cudaError_t _e = cudaSetDevice(c->dev);         \
+    if (_e != cudaSuccess) return cuda_fail(_e, "cudaSetDevice"); \
+  } while (0)
+
+static int put3(Ctx *c, double *dst, const double *x, const double *y, const double *z) {
+  const size_t n = c->n;
+  CK(cudaMemcpyAsync(dst, x, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dst + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dst + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CM3D_NB_OK;
+}
+
+static int get3(Ctx *c, const double *src, double *x, double *y, double *z) {
+  const size_t n = c->n;
+  CK(cudaMemcpyAsync(x, src, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(y, src + n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(z, src + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py, const double *pz) {
+  CTX;
+  return put3(c, c->pos, px, py, pz);
+}
+int cm3d_nb_get_positions(cm3d_nb_ctx *ctx, double *px, double *py, double *pz) {
+  CTX;
+  return get3(c, c->pos, px, py, pz);
+}
+int cm3d_nb_set_velocities(cm3d_nb_ctx *ctx, const double *vx, const double *vy, const double *vz) {
+  CTX;
+  return put3(c, c->vel, vx, vy, vz);
+}
+int cm3d_nb_get_velocities(cm3d_nb_ctx *ctx, double *vx, double *vy, double *vz) {
+  CTX;
+  return get3(c, c->vel, vx, vy, vz);
+}
+int cm3d_nb_get_forces(cm3d_nb_ctx *ctx, int which, double *fx, double *fy, double *fz) {
+  CTX;
+  double *b = block_of(c, which);
+  if (!b) {
+    set_error("get_forces: unknown block %d", which);
+    return CM3D_NB_ERR_ARG;
+  }
+  return get3(c, b, fx, fy, fz);
+}
+int cm3d_nb_set_forces(cm3d_nb_ctx *ctx, int which, const double *fx, const double *fy, const double *fz) {
+  CTX;
+  double *b = block_of(c, which);
+  if (!b) {
+    set_error("set_forces: unknown block %d", which);
+    return CM3D_NB_ERR_ARG;
+  }
+  return put3(c, b, fx, fy, fz);
+}
+
+int cm3d_nb_get_ngbr(cm3d_nb_ctx *ctx) {
+  CTX;
+  return build_lists(c, false);
+}
+
+int cm3d_nb_nrefsh(cm3d_nb_ctx *ctx, int istep, int *rebuilt) {
+  CTX;
+  int rc;
+  if (rebuilt) *rebuilt = 0;
+  if (!c->lists_built) {
+    set_error("nrefsh() before get_ngbr()");
+    return CM3D_NB_ERR_STATE;
+  }
+  c->h_istate[IS_ISTEP] = istep;
+  CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  if ((rc = check_displacement(c))) return rc;
+  if ((rc = reset_positions(c))) return rc;
+  CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (c->h_istate[IS_REBUILD]) {
+    if ((rc = build_lists(c, false))) return rc;
+    if (rebuilt) *rebuilt = 1;
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_force(cm3d_nb_ctx *ctx, int iflg) {
+  CTX;
+  return run_force(c, iflg);
+}
+
+static int zero_slots(Ctx *c, int first, int count) {
+  CK(cudaMemsetAsync(c->acc + first, 0, sizeof(double) * count, c->st));
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_force_ter(cm3d_nb_ctx *ctx, int iflg) {
+  CTX;
+  if (!c->lists_built) {
+    set_error("force_ter() before get_ngbr()");
+    return CM3D_NB_ERR_STATE;
+  }
+  if (iflg != 0 && iflg != 1) {
+    set_error("force_ter(): level must be 0 or 1");
+    return CM3D_NB_ERR_ARG;
+  }
+  int rc;
+  if (iflg == 1 && (rc = zero_slots(c, ACC_SPOTL, 12))) return rc;   // zero_potl md_fnopol.c:38
+  return pair_forces(c, iflg, 1);
+}
+
+int cm3d_nb_force_ter_e(cm3d_nb_ctx *ctx, int iflg) {
+  CTX;
+  if (!c->lists_built) {
+    set_error("force_ter_e() before get_ngbr()");
+    return CM3D_NB_ERR_STATE;
+  }
+  if (iflg != 0 && iflg != 1) {
+    set_error("force_ter_e(): level must be 0 or 1");
+    return CM3D_NB_ERR_ARG;
+  }
+  int rc;
+  if (iflg == 1 && (rc = zero_slots(c, ACC_SPOTE, 12))) return rc;   // zero_pote finter_e.c:34
+  return pair_forces(c, iflg, 2);
+}
+
+int cm3d_nb_fk_ewald(cm3d_nb_ctx *ctx) {
+  CTX;
+  int rc;
+  if ((rc = zero_slots(c, ACC_VK, 11))) return rc;
+  return kspace_forces(c);
+}
+
+int cm3d_nb_ecorr(cm3d_nb_ctx *ctx) {
+  CTX;
+  int rc;
+  if ((rc = zero_slots(c, ACC_POT_ECORR, 11))) return rc;
+  return plain_ecorr(c, c->ecorr_pairs);
+}
+
+int cm3d_nb_zero_forces(cm3d_nb_ctx *ctx, int which) {
+  CTX;
+  double *b = block_of(c, which);
+  if (!b) {
+    set_error("zero_forces: unknown block %d", which);
+    return CM3D_NB_ERR_ARG;
+  }
+  CK(cudaMemsetAsync(b, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_rmass(cm3d_nb_ctx *ctx, int which) {
+  CTX;
+  double *b = block_of(c, which);
+  if (!b) {
+    set_error("rmass: unknown block %d", which);
+    return CM3D_NB_ERR_ARG;
+  }
+  k_scale_rmass<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, b, c->mass);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_getsvirter(cm3d_nb_ctx *ctx, double *vhinter, double *vinter, double *winter, double wintert[9]) {
+  CTX;
+  int rc;
+  if ((rc = pull_acc(c))) return rc;
+  double t[9];
+  sym9(c->h_acc, ACC_SPRSLT, t);
+  *vhinter += c->h_acc[ACC_SPOTHL];
+  *vinter += c->h_acc[ACC_SPOTL];
+  *winter += c->h_acc[ACC_SPRSL];
+  for (int k = 0; k < 9; k++) wintert[k] += t[k];
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_getsvirter_e(cm3d_nb_ctx *ctx, double *velec, double *welec, double welectensor[9]) {
+  CTX;
+  int rc;
+  if ((rc = pull_acc(c))) return rc;
+  double t[9];
+  sym9(c->h_acc, ACC_SPRSET, t);
+  *velec += c->h_acc[ACC_SPOTE];
+  *welec += c->h_acc[ACC_SPRSE];
+  for (int k = 0; k < 9; k++) welectensor[k] += t[k];
+  return CM3D_NB_OK;
+}
+
+// fk_ewald's totals (md_ewald.c:336-348) plus ecorr, as getvewald adds them
+static void ewald_totals(Ctx *c, double *pot, double *prs, double tens[9]) {
+  const double *a = c->h_acc;
+  double six = c->ncharge > 0 ? c->ewald_bkg / deth(c->hmat) : 0.0;
+  double vk = a[ACC_VK], vp = a[ACC_VP];
+  double vk_ewald = 0, vp_ewald = 0, vpt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (c->iperd == 3) {
+    vk_ewald = vk + six + (c->ncharge > 0 ? c->ewald_self : 0.0);
+    vp_ewald = vp + 3. * (vk + six);
+    for (int k = 0; k < 9; k++) vpt[k] = a[ACC_VPT + k];
+    vpt[0] += vk + six;
+    vpt[4] += vk + six;
+    vpt[8] += vk + six;
+  }
+  double ct[9];
+  sym9(a, ACC_PRS_ECORRT, ct);
+  *pot = vk_ewald + a[ACC_POT_ECORR];
+  *prs = vp_ewald + a[ACC_PRS_ECORR];
+  for (int k = 0; k < 9; k++) tens[k] = vpt[k] + ct[k];
+}
+
+int cm3d_nb_getvewald(cm3d_nb_ctx *ctx, double *pot_ewald, double *prs_ewald, double prs_ewald_tensor[9]) {
+  CTX;
+  int rc;
+  if ((rc = pull_acc(c))) return rc;
+  double p, w, t[9];
+  ewald_totals(c, &p, &w, t);
+  *pot_ewald += p;
+  *prs_ewald += w;
+  for (int k = 0; k < 9; k++) prs_ewald_tensor[k] += t[k];
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_step_init(cm3d_nb_ctx *ctx) {
+  CTX;
+  int rc;
+  if (c->name == "has-torsions") {
+    set_error("step_init(): torsions, 1-4 terms and cross bonds are not part of the engine");
+    return CM3D_NB_ERR_ARG;
+  }
+  c->h_istate[IS_ISTEP] = 0;
+  c->h_istate[IS_ISTEPLAST] = 0;
+  CK(cudaMemcpyAsync(c->istate, c->h_istate, sizeof(int) * 2, cudaMemcpyHostToDevice, c->st));
+  if ((rc = build_lists(c, false))) return rc;
+  if ((rc = run_force(c, 1))) return rc;
+  if ((rc = run_force(c, 2))) return rc;
+  c->forces_valid = true;
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
+  CTX;
+  if (c->name == "has-torsions") {
+    set_error("step(): torsions, 1-4 terms and cross bonds are not part of the engine");
+    return CM3D_NB_ERR_ARG;
+  }
+  return run_step(c, istep0, nsteps);
+}
+
+int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e) {
+  CTX;
+  int rc;
+  if ((rc = pull_acc(c))) return rc;
+  const double *a = c->h_acc;
+  memset(e, 0, sizeof *e);
+  e->vinter = a[ACC_SPOTL];
+  e->vhinter = a[ACC_SPOTHL];
+  e->winter = a[ACC_SPRSL];
+  sym9(a, ACC_SPRSLT, e->wintertensor);
+  e->velec = a[ACC_SPOTE];
+  e->welec = a[ACC_SPRSE];
+  sym9(a, ACC_SPRSET, e->welectensor);
+  ewald_totals(c, &e->vewald, &e->wewald, e->wewaldtensor);
+  e->vbond = a[ACC_VBOND];
+  e->wbond = a[ACC_WBOND];
+  e->vbend = a[ACC_VBEND];
+  e->wbend = 0.;
+  double vol = deth(c->hmat), rvol = 1. / vol;
+  e->US = e->vhinter + e->velec + e->vewald;
+  e->U = e->vinter + e->velec + e->vewald;
+  e->W = e->winter + e->welec + e->wewald;
+  for (int k = 0; k < 9; k++) e->Wtensor[k] = e->wintertensor[k] + e->welectensor[k] + e->wewaldtensor[k];
+  e->W -= 3 * c->wlrc * rvol;
+  e->Wtensor[0] -= c->wlrc * rvol;
+  e->Wtensor[4] -= c->wlrc * rvol;
+  e->Wtensor[8] -= c->wlrc * rvol;
+  sym9(a, ACC_P2MT, e->p2m_tensor);
+  double p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
+  double UI = e->vbond + e->vbend, WI = e->wbond;
+  e->poth = e->US + c->vlrc / vol;
+  e->poter = e->U + c->vlrc / vol;
+  e->potra = UI;
+  e->prsi = (p2m + e->W + WI) / (3 * vol);
+  for (int k = 0; k < 9; k++) e->prs_tensor[k] = (e->p2m_tensor[k] + e->Wtensor[k] + a[ACC_WBONDT + k]) / vol;
+  e->zke = .5 * p2m;
+  e->tiout = p2m / (double)c->ndof;
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_list_count(cm3d_nb_ctx *ctx, int which, long long *npairs) {
+  CTX;
+  if (which < 0 || which > 3) {
+    set_error("list_count: unknown list %d", which);
+    return CM3D_NB_ERR_ARG;
+  }
+  *npairs = c->lists_built ? c->hcount[which] : 0;
+  if (c->lists_built && c->use_graph) {
+    // device-gated rebuilds may have changed the counts since the host looked
+    CK(cudaMemcpyAsync(c->h_ltot, c->ltot, sizeof(long long) * LT_COUNT, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < LT_COUNT; k++) c->hcount[k] = c->h_ltot[k];
+    *npairs = c->hcount[which];
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_get_list(cm3d_nb_ctx *ctx, int which, int *ip, int *jp, long long capacity, long long *npairs) {
+  CTX;
+  long long np = 0;
+  int rc = cm3d_nb_list_count(ctx, which, &np);
+  if (rc) return rc;
+  if (npairs) *npairs = np;
+  if (np > capacity) {
+    set_error("get_list: %lld pairs do not fit in %lld", np, capacity);
+    return CM3D_NB_ERR_ARG;
+  }
+  if (np == 0) return CM3D_NB_OK;
+  std::vector<int2> h((size_t)np);
+  CK(cudaMemcpyAsync(h.data(), c->lst[which], sizeof(int2) * (size_t)np, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (long long k = 0; k < np; k++) {
+    ip[k] = h[k].x;
+    jp[k] = h[k].y;
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_get_status(cm3d_nb_ctx *ctx, cm3d_nb_status_t *st) {
+  CTX;
+  CK(cudaMemcpyAsync(c->h_stat, c->stat, sizeof(long long) * ST_COUNT, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  st->table_underflow = c->h_stat[ST_UNDERFLOW];
+  st->rebuilds = c->h_stat[ST_REBUILDS];
+  st->resets = c->h_stat[ST_RESETS];
+  st->overflows = c->overflows_host;
+  st->nonfinite = (int)c->h_stat[ST_NONFINITE];
+  st->last_istep = c->h_istate[IS_ISTEP];
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_synchronize(cm3d_nb_ctx *ctx) {
+  CTX;
+  CK(cudaStreamSynchronize(c->st));
+  return CM3D_NB_OK;
+}
+
+void *cm3d_nb_stream(cm3d_nb_ctx *ctx) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  return c ? (void *)c->st : nullptr;
+}
+
+int cm3d_nb_enable_timing(cm3d_nb_ctx *ctx, int enable) {
+  CTX;
+  collect_timing(c);
+  c->timing.on = enable != 0;
+  for (int k = 0; k < 4; k++) {
+    c->timing.ms[k] = 0;
+    c->timing.launches[k] = 0;
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_kernel_time(cm3d_nb_ctx *ctx, int cls, double *ms, long long *launches) {
+  CTX;
+  if (cls < 0 || cls > 3) {
+    set_error("kernel_time: unknown class %d", cls);
+    return CM3D_NB_ERR_ARG;
+  }
+  collect_timing(c);
+  if (ms) *ms = c->timing.ms[cls];
+  if (launches) *launches = c->timing.launches[cls];
+  return CM3D_NB_OK;
+}
+
+long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  return c ? c->launches : 0;
+}
+
+// ------------------------------------------------- host set-up restatements
+// func_lj  energy/inter/md_funcvdw.c:40-46
+static void func_lj(double x, double *f, double *df, double eps, double sig) {
+  *f = 4. * eps * (pow(sig / x, 12.) - pow(sig / x, 6.));
+  *df = 4. * eps * (6. * pow(sig, 6.) * pow(x, -7.) - 12. * pow(sig, 12.) * pow(x, -13.));
+  *df /= x;
+}
+
+// func_kerf  md_funcvdw.c:219-227 ; func_coul md_funcvdw.c:243-249
+static void func_kerf(double x, double *f, double *df, double alpha) {
+  *f = erfc(alpha * x) / x;
+  *df = -erfc(alpha * x) / (x * x) - 2. * alpha * exp(-alpha * alpha * x * x) / (sqrt(M_PI) * x);
+  *df /= x;
+}
+static void func_coul(double x, double *f, double *df) {
+  *f = 1. / x;
+  *df = -1. / (x * x);
+  *df /= x;
+}
+
+int cm3d_nb_lj_table(double eps, double sig, double rmin, double rmax, double rres, double rheal, double skin,
+                     int ntable, int shift, double *vtab, double *dvtab, double *switchs, double *dx2tab) {
+  if (ntable < 5 || rmax <= rmin || !vtab || !dvtab || !switchs || !dx2tab) {
+    set_error("lj_table: bad arguments (ntable %d, rmin %g, rmax %g)", ntable, rmin, rmax);
+    return CM3D_NB_ERR_ARG;
+  }
+  // get_ter_parm md_getparm.c:222-254
+  double rmins, rminl, rres_dist = rres;
+  if (rres < rmax) {
+    rmins = rmin;
+    rminl = rres - rheal;
+  } else {
+    rmins = rmin;
+    rminl = rmax + 2. * skin;
+    rres_dist = rmax + 2. * rheal;
+  }
+  *dx2tab = ((double)ntable - 3.) / (rmax * rmax - rmin * rmin);
+  if (rminl - skin < rmin) {
+    set_error("lj_table: RESPA distance, healing length, skin and minimum distance are inconsistent");
+    return CM3D_NB_ERR_ARG;
+  }
+  double rch = (rres_dist - rheal);
+  double rhl = rheal == 0. ? 1. : 1. / rheal;
+  for (int i = 0; i < ntable; i++) {
+    double xt = i / (*dx2tab) + rmins * rmins, f, df;
+    if (xt < 0) {
+      set_error("lj_table: negative table abscissa");
+      return CM3D_NB_ERR_ARG;
+    }
+    func_lj(sqrt(xt), &f, &df, eps, sig);
+    vtab[i] = f * 1.0;     // scaleeps = 1 (md_setsimdef.c:63)
+    dvtab[i] = df * 1.0;
+    if (xt <= rch * rch) switchs[i] = 1.0;
+    if (xt > rch * rch && xt < rres_dist * rres_dist) {
+      double br = (sqrt(xt) - rch) * rhl, sm = (1. + br * br * (2. * br - 3.));
+      switchs[i] = sm;
+    }
+    if (xt >= rres_dist * rres_dist) switchs[i] = 0.0;
+  }
+  if (shift) {
+    double vs = vtab[ntable - 3];   // md_searchbase.c:181-188
+    for (int i = 0; i < ntable; i++) vtab[i] -= vs;
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_coul_table(double alpha, double rcute_min, double rcute_resp, double rcute_max, double rheal,
+                       double skin, int ntable, int iperd, int shift, double *coultab, double *dcoultab,
+                       double *switchse, double *dx2coul) {
+  (void)skin;
+  if (ntable < 5 || rcute_max <= rcute_min || !coultab || !dcoultab || !switchse || !dx2coul) {
+    set_error("coul_table: bad arguments");
+    return CM3D_NB_ERR_ARG;
+  }
+  // set_charges elec_ngbr.c:51-103
+  double rmins2 = rcute_min * rcute_min, rmaxs2 = rcute_resp * rcute_resp;
+  double rminl2 = ((rcute_resp - rheal) * (rcute_resp - rheal)), rmaxl2 = rcute_max * rcute_max;
+  *dx2coul = (((double)ntable - 3.) / (rmaxl2 - rmins2));
+  for (int i = 0; i < ntable; i++) {
+    double xt = i / *dx2coul + rmins2, f, df;
+    if (xt < 0) {
+      set_error("coul_table: negative table abscissa");
+      return CM3D_NB_ERR_ARG;
+    }
+    if (iperd == 3) func_kerf(sqrt(xt), &f, &df, alpha);
+    else func_coul(sqrt(xt), &f, &df);
+    coultab[i] = f;
+    dcoultab[i] = df;
+    if (xt <= rminl2) switchse[i] = 1.;
+    if (xt > rminl2 && xt < rmaxs2) {
+      double br = (sqrt(xt) - sqrt(rminl2)) / rheal, sm = (1. + br * br * (2. * br - 3.));
+      switchse[i] = sm;
+    }
+    if (xt >= rmaxs2) switchse[i] = 0.;
+  }
+  if (shift) {
+    double vs = coultab[ntable - 3];
+    for (int i = 0; i < ntable; i++) coultab[i] -= vs;
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_ewald_kvectors(int kmax, int *ka, int *kb, int *kc, int *kup, int *ktot) {
+  // ewald_setup md_ewald.c:93-114: half space ka >= 0, spherical cutoff
+  int n = 0, ksqmax = kmax * kmax;
+  for (int i = 0; i <= kmax; i++)
+    for (int j = (i == 0) ? 0 : -kmax; j <= kmax; j++) {
+      int first = 1;
+      for (int k = (i == 0 && j == 0) ? 1 : -kmax; k <= kmax; k++) {
+        if (i * i + j * j + k * k <= ksqmax) {
+          if (ka) {
+            ka[n] = i;
+            kb[n] = j;
+            kc[n] = k;
+            if (kup) kup[n] = first;
+          }
+          first = 0;
+          n++;
+        }
+      }
+    }
+  if (ka && kup) kup[n] = 0;
+  *ktot = n;
+  return CM3D_NB_OK;
+}
+
+}  // extern "C"

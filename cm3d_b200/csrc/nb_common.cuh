@@ -1,0 +1,293 @@
+// nb_common.cuh -- engine context and helpers shared by the CUDA sources.
+//
+// Device layout (one system per context):
+//   pos, vel, fxl, fxs, fxa     3N doubles each, x | y | z blocks, original
+//                               atom order -- the layout of CM3D's contiguous
+//                               COORDS blocks (utils/md_util.new.c:113-141)
+//   acc[]                       FP64 energy/virial accumulators (ACC_* below)
+//   cell grid + sorted arrays   rebuilt with the lists (nb_list.cu)
+//   half lists t/s/te/se        CM3D's NGBR lists as (i, j) pairs
+//   full list (mixed mode)      per sorted atom, packed 32-bit entries
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cm3d_nb.h"
+
+namespace cm3d {
+
+// ------------------------------------------------------------ accumulators
+enum {
+  ACC_SPOTL = 0,          // sum V_LJ                     (md_fnopol.c spotl)
+  ACC_SPOTHL = 1,         // sum V_LJ - V(ntable-4)       (spothl)
+  ACC_SPRSL = 2,          // sum -r^2 f                   (sprsl)
+  ACC_SPRSLT = 3,         // 9: LJ virial tensor          (sprslt)
+  ACC_SPOTE = 12,         // elec energy                  (finter_e.c spote)
+  ACC_SPOTHE = 13,        // shifted elec energy          (spothe)
+  ACC_SPRSE = 14,         // elec virial                  (sprse)
+  ACC_SPRSET = 15,        // 9: elec virial tensor        (sprset)
+  ACC_VK = 24,            // sum preg |S|^2               (fk_ewald vk)
+  ACC_VP = 25,            // sum prep |S|^2 g2            (vp)
+  ACC_VPT = 26,           // 9: reciprocal virial tensor  (vp_tensor)
+  ACC_POT_ECORR = 35,     // md_ewald.c ecorr spot
+  ACC_PRS_ECORR = 36,     // ecorr sprs
+  ACC_PRS_ECORRT = 37,    // 9
+  ACC_VBOND = 46,         // getvbond energy
+  ACC_WBOND = 47,         // getvbond virial
+  ACC_WBONDT = 48,        // 9
+  ACC_VBEND = 57,         // getvbend energy
+  ACC_P2MT = 58,          // 9: get_p2mt kinetic tensor
+  ACC_COUNT = 72
+};
+// device status words (long long)
+enum {
+  ST_UNDERFLOW = 0,       // table underflows (k < 1)
+  ST_NONFINITE = 1,
+  ST_OVERFLOW = 2,        // a list fill ran past its capacity
+  ST_RESETS = 3,          // RESETPOS events
+  ST_REBUILDS = 4,
+  ST_COUNT = 8
+};
+// device integer state
+enum {
+  IS_ISTEP = 0,           // SIMPARMS.istep of the step being taken
+  IS_ISTEPLAST = 1,       // md_finter.c:48 static isteplast
+  IS_REBUILD = 2,         // rebuild requested by the displacement check
+  IS_COUNT = 8
+};
+// list totals (long long) written by the list builder
+enum { LT_T = 0, LT_S = 1, LT_TE = 2, LT_SE = 3, LT_FULL = 4, LT_COUNT = 5 };
+
+// packed full-list entry (mixed mode): j (sorted index) | shift code | flags
+constexpr int ENT_JBITS = 22;
+constexpr uint32_t ENT_JMASK = (1u << ENT_JBITS) - 1;
+constexpr int ENT_CODE_SHIFT = 22;          // 5 bits: 27 cell-shift codes
+constexpr uint32_t ENT_LJ = 1u << 27;       // pair is in CM3D's t list
+constexpr uint32_t ENT_EL = 1u << 28;       // pair is in CM3D's te list
+constexpr uint32_t ENT_LJS = 1u << 29;      // pair is in CM3D's s list
+constexpr uint32_t ENT_ELS = 1u << 30;      // pair is in CM3D's se list
+constexpr int MAX_ATOMS_MIXED = 1 << ENT_JBITS;
+
+struct Timing {
+  bool on = false;
+  double ms[4] = {0, 0, 0, 0};
+  long long launches[4] = {0, 0, 0, 0};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[4];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+};
+
+struct Ctx {
+  // ---- configuration
+  int dev = 0;
+  cudaStream_t st = nullptr;
+  int mode = CM3D_NB_MIXED;
+  int need_short = 0;
+  int tpa = 0;
+  int use_graph = 1;
+  // ---- sizes and scalars
+  int n = 0, ntypes = 0, ninter = 0, ntable = 0, ncharge = 0, ktot = 0, necorr = 0;
+  int nbonds = 0, nbends = 0, nres_lrf = 1, nres_intra = 1, nres_tors = 1, ndof = 1;
+  int iperd = 3;
+  double dt = 0, vlrc = 0, wlrc = 0, skin = 0, rheal = 0;
+  double hmat[9], hmati[9];
+  double rlist_max = 0;        // largest list radius (LJ or charge, with skin)
+  double rc_lj_max = 0;
+  double kappa = 0, kappa2 = 0, falp2 = 0, ewald_self = 0, ewald_bkg = 0;
+  double dx2coul = 0, rmins_coul2 = 0, rmaxs_coul2 = 0, rminl_coul2 = 0, rmaxl_coul2 = 0;
+  double rmaxs_skin2_e = 0, rmaxl_skin2_e = 0;
+  double tablast_e = 0;        // coultab[ntable-4] (finter_e.c:67)
+  // ---- per-atom device arrays (original order)
+  double *pos = nullptr, *vel = nullptr, *fxl = nullptr, *fxs = nullptr, *fxa = nullptr;
+  double *mass = nullptr, *q = nullptr, *dxn = nullptr, *snap = nullptr;
+  int *itype = nullptr;
+  // ---- parameters on device
+  int *map = nullptr;                   // ntypes^2
+  double *vtab = nullptr, *dvtab = nullptr, *switchs = nullptr;   // ninter*ntable
+  double *icut = nullptr;               // 8*ninter: rmaxs_cut2 rmins_cut2 rmaxl_cut2
+                                        // rminl_cut2 rmaxs_skin2 rmaxl_skin2 dx2tab vt[ntm4]
+  double *coultab = nullptr, *dcoultab = nullptr, *switchse = nullptr;
+  int *excl_off = nullptr, *excl_idx = nullptr, *cexcl_off = nullptr, *cexcl_idx = nullptr;
+  // FP32 coefficient tables (mixed): per index k two float4
+  //   LJ:   {dv0, dvA, dvB, v0} {vA, vB, sw0, swA}  + swB in a third
+  //   elec: {dc0, dcA, dcB, c0} {cA, cB, 0, 0}
+  float4 *ftab_lj = nullptr;            // 3 * ninter * ntable
+  float4 *ftab_el = nullptr;            // 2 * ntable
+  float *fcut = nullptr;                // 6*ninter FP32: rmaxl_cut2 rmins*dx2 dx2 rminl_cut2 rmaxs_cut2 vt[ntm4]
+  // ---- Ewald
+  int nrows = 0;                        // k rows of constant (ka, kb)
+  int4 *rows = nullptr;                 // {ka, kb, kc_lo, len}
+  int *row_k0 = nullptr;                // index of the row's first k
+  double2 *sk = nullptr;                // S(k) FP64
+  double2 *spart = nullptr;             // per-tile partial S(k)
+  float2 *akf = nullptr;                // 2 preg S(k), FP32 (mixed)
+  double2 *akd = nullptr;               // 2 preg S(k), FP64 (plain)
+  uint4 *kfrac = nullptr;               // per charged atom: fixed-point fractional coords + tq
+  double4 *kposd = nullptr;             // per charged atom (plain): x y z tq
+  int *icharge = nullptr;
+  int *ka_d = nullptr, *kb_d = nullptr, *kc_d = nullptr;
+  int ks_tiles = 0, ks_tile_atoms = 0, kf_split = 1;
+  size_t kf_smem = 0;
+  int2 *ecorr_pairs = nullptr;          // CM3D's iecorr/jecorr order
+  // ---- bonded groups (connected components of bonds/bends/ecorr)
+  int ngroups = 0;
+  int *grp_atom_off = nullptr, *grp_atoms = nullptr;
+  int *grp_bond_off = nullptr, *grp_bend_off = nullptr, *grp_ecorr_off = nullptr;
+  int4 *bond_ij = nullptr;              // {i, j, -, -} grouped order
+  double2 *bond_p = nullptr;            // {eq, fk}
+  int4 *bend_ijk = nullptr;
+  double2 *bend_p = nullptr;
+  int2 *ecorr_ij = nullptr;             // grouped order
+  // ---- cell grid and lists
+  int nc[3] = {1, 1, 1}, ncells = 1;
+  int *cell_of = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *cell_atoms = nullptr;
+  int *rank = nullptr;                  // original -> sorted
+  int *cnt = nullptr;                   // 5 per atom counts (t s te se full)
+  long long *off = nullptr;             // 5*(n+1) exclusive offsets
+  long long *ltot = nullptr;            // LT_COUNT device totals
+  long long lcap[LT_COUNT] = {0, 0, 0, 0, 0};
+  long long hcount[LT_COUNT] = {0, 0, 0, 0, 0};
+  int2 *lst[4] = {nullptr, nullptr, nullptr, nullptr};   // t s te se half lists
+  uint32_t *nbr = nullptr;              // full list (mixed)
+  float4 *xq = nullptr;                 // sorted: cell-relative FP32 pos + q
+  int *styp = nullptr;                  // sorted type
+  int *sorig = nullptr;                 // sorted -> original (== cell_atoms)
+  float4 *shift = nullptr;              // 27 FP32 cell-shift vectors
+  double *corner = nullptr;             // per sorted atom cell-origin offset (3n FP64)
+  int4 *cimg = nullptr;                 // per atom: packed cell coords | periodic image
+  // ---- accumulators, status, state
+  double *acc = nullptr;
+  long long *stat = nullptr;
+  int *istate = nullptr;
+  double *h_acc = nullptr;              // pinned mirrors
+  long long *h_stat = nullptr;
+  int *h_istate = nullptr;
+  long long *h_ltot = nullptr;
+  // ---- host bookkeeping
+  bool lists_built = false;
+  bool forces_valid = false;
+  long long launches = 0;
+  long long rebuilds_host = 0, overflows_host = 0;
+  Timing timing;
+  cudaGraphExec_t graph = nullptr;
+  long long graph_launches = 0;
+  std::string name;
+};
+
+// ------------------------------------------------------------ error handling
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cuda_fail(_e, #call); \
+  } while (0)
+#define CKL(ctx) CK(cudaPeekAtLastError())
+
+// timing helpers (class: 0 pair, 1 kspace, 2 list, 3 integrate)
+void tbegin(Ctx *c, int cls, cudaEvent_t *e0);
+void tend(Ctx *c, int cls, cudaEvent_t e0);
+
+// ------------------------------------------------------------ device helpers
+// anint of CM3D's Linux build (include/md_macros.h:52): truncation toward
+// zero of A +/- 0.5, i.e. round half away from zero
+__device__ __forceinline__ double anint_ref(double a) {
+  return (double)(int)(a >= 0.0 ? __dadd_rn(a, 0.5) : __dadd_rn(a, -0.5));
+}
+
+// period_new (integrate/md_period.new.c:39-52) for one displacement, in
+// CM3D's operation order with every product and sum rounded separately (no
+// FMA contraction) so that r^2 is bit-identical to CM3D's
+__device__ __forceinline__ void period_ref(double &dx, double &dy, double &dz,
+                                           const double *h, const double *hi) {
+  double sx = __dadd_rn(__dadd_rn(__dmul_rn(dx, hi[0]), __dmul_rn(dy, hi[1])), __dmul_rn(dz, hi[2]));
+  double sy = __dadd_rn(__dadd_rn(__dmul_rn(dx, hi[3]), __dmul_rn(dy, hi[4])), __dmul_rn(dz, hi[5]));
+  double sz = __dadd_rn(__dadd_rn(__dmul_rn(dx, hi[6]), __dmul_rn(dy, hi[7])), __dmul_rn(dz, hi[8]));
+  sx = __dsub_rn(sx, anint_ref(sx));
+  sy = __dsub_rn(sy, anint_ref(sy));
+  sz = __dsub_rn(sz, anint_ref(sz));
+  dx = __dadd_rn(__dadd_rn(__dmul_rn(sx, h[0]), __dmul_rn(sy, h[1])), __dmul_rn(sz, h[2]));
+  dy = __dadd_rn(__dadd_rn(__dmul_rn(sx, h[3]), __dmul_rn(sy, h[4])), __dmul_rn(sz, h[5]));
+  dz = __dadd_rn(__dadd_rn(__dmul_rn(sx, h[6]), __dmul_rn(sy, h[7])), __dmul_rn(sz, h[8]));
+}
+
+__device__ __forceinline__ double r2_ref(double dx, double dy, double dz) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// membership of (i, j) in a CSR exclusion list stored at the lower index
+__device__ __forceinline__ bool excluded(int i, int j, const int *__restrict__ off,
+                                         const int *__restrict__ idx) {
+  int a = i < j ? i : j, b = i < j ? j : i;
+  int lo = off[a], hi = off[a + 1];
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    int v = idx[mid];
+    if (v == b) return true;
+    if (v < b) lo = mid + 1;
+    else hi = mid;
+  }
+  return false;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// block-wide sum of NV doubles into acc[slot..slot+NV) with one atomic per
+// value per block; all threads of the block must call it
+template <int NV>
+__device__ __forceinline__ void block_acc(double (&v)[NV], double *acc, const int *slots) {
+  __shared__ double red[32][NV];
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) red[w][k] = v[k];
+  }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double s = lane < nw ? red[lane][k] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0 && s != 0.0) atomicAdd(acc + slots[k], s);
+    }
+  }
+}
+
+// ------------------------------------------------------------ host helpers
+int plain_pairs(Ctx *c, int iflg, int which);   // nb_plain.cu
+int plain_ecorr(Ctx *c, const int2 *ij);        // nb_plain.cu
+int mixed_pairs(Ctx *c, int iflg, int mask);    // nb_pair.cu
+int build_lists(Ctx *c, bool device_flag);      // nb_list.cu
+int list_setup(Ctx *c);                         // nb_list.cu
+int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused
+int pair_setup(Ctx *c);                         // nb_pair.cu
+int kspace_forces(Ctx *c);                      // nb_kspace.cu
+int kspace_setup(Ctx *c, const cm3d_nb_system *s);
+int ecorr_forces(Ctx *c);                       // nb_kspace.cu (plain, atomic)
+int step_setup(Ctx *c, const cm3d_nb_system *s);// nb_step.cu
+int run_step(Ctx *c, int istep0, int nsteps);   // nb_step.cu
+int run_force(Ctx *c, int iflg);                // nb_step.cu
+int run_bonded(Ctx *c);                         // nb_step.cu
+int group_init(Ctx *c, bool zero_fxs);          // nb_step.cu
+int finish_level1(Ctx *c, double dter, double dter1, bool kick);   // nb_step.cu
+int check_displacement(Ctx *c);                 // nb_step.cu
+int reset_positions(Ctx *c);                    // nb_step.cu
+
+inline int grid_for(long long n, int block) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 2147483647LL) g = 2147483647LL;
+  return (int)g;
+}
+
+}  // namespace cm3d

@@ -1,0 +1,461 @@
+// nb_kspace.cu -- Ewald reciprocal space: fk_ewald (energy/inter/md_ewald.c:185-361)
+// and its getvewald totals (md_ewald.c:336-348, 364-380).
+//
+// CM3D's k set (ewald_setup, md_ewald.c:93-114) comes in rows of constant
+// (ka, kb) with consecutive kc; fk_ewald seeds cos/sin(k.r) at the start of
+// every row and advances along kc by a complex multiply with
+// exp(i 2 pi s_c) (md_ewald.c:239-280).  Both engines keep that structure:
+//
+//   k_sfac_*   structure factors: a block owns a tile of charged atoms and a
+//              chunk of rows; every thread carries A atoms' phases through the
+//              row, the per-k sums are reduced across the warp and then across
+//              the block in FP64 and written as per-tile partials
+//   k_sred     sums the tiles in FP64 (fixed order: deterministic), forms
+//              preg, prep, the energy and the virial tensor of every k and the
+//              force coefficients A(k) = 2 preg S(k)
+//   k_kforce_* per atom, the sum over all k of k (Re A sin - Im A cos),
+//              accumulated per row in FP32 (mixed) and across rows in FP64
+//
+// Mixed mode forms every phase from fixed-point fractional coordinates:
+// s = H^-1 r is taken in FP64, its fractional part stored as a 32-bit
+// integer, and ka*u0 + kb*u1 + kc*u2 evaluated in wrapping 32-bit integer
+// arithmetic -- an exact phase modulo 2 pi whatever the size of k.r -- so
+// the only FP32 error is that of the sin/cos of a number in [-pi, pi) and of
+// the recurrence along one row.  The plain mode does everything in FP64 with
+// CM3D's expressions (rk = x aka + y akb + z akc, md_ewald.c:264).
+#include "nb_common.cuh"
+
+namespace cm3d {
+
+constexpr int KS_THREADS = 256;
+constexpr int KS_A = 8;            // atoms per thread, structure factors
+constexpr int KF_A = 2;            // atoms per thread, forces
+constexpr int MAX_ROWLEN = 128;    // 2 kmax + 1 <= 128
+
+// ------------------------------------------------------------ mixed mode
+__global__ void k_kprep(int nq, const int *__restrict__ icharge, int n, const double *__restrict__ pos,
+                        const double *__restrict__ q, const double *__restrict__ hmati, uint4 *__restrict__ kfrac,
+                        double4 *__restrict__ kposd) {
+  int jq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jq >= nq) return;
+  int i = icharge[jq];
+  double x = pos[i], y = pos[n + i], z = pos[2 * n + i];
+  const double fact = sqrt(4.0 * M_PI);   // md_ewald.c:202
+  double tq = q[i] * fact;
+  unsigned u[3];
+  for (int d = 0; d < 3; d++) {
+    double s = x * hmati[3 * d] + y * hmati[3 * d + 1] + z * hmati[3 * d + 2];
+    double f = s - floor(s);
+    unsigned long long w = (unsigned long long)(f * 4294967296.0);
+    u[d] = (unsigned)(w & 0xffffffffull);
+  }
+  if (kfrac) kfrac[jq] = make_uint4(u[0], u[1], u[2], __float_as_uint((float)tq));
+  if (kposd) kposd[jq] = make_double4(x, y, z, tq);
+}
+
+__device__ __forceinline__ float phase_rad(unsigned phi) {
+  // (int)phi / 2^32 of a turn, in [-pi, pi)
+  return (float)(int)phi * 1.4629180792671596e-09f;   // 2 pi / 2^32
+}
+
+__global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *__restrict__ kfrac, int nrows,
+                                                           const int4 *__restrict__ rows,
+                                                           const int *__restrict__ row_k0, int rows_per_block,
+                                                           int ktot, double2 *__restrict__ spart) {
+  __shared__ float2 red[KS_THREADS / 32][MAX_ROWLEN];
+  const int tile = blockIdx.x;
+  const int r0 = blockIdx.y * rows_per_block;
+  const int r1 = min(nrows, r0 + rows_per_block);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned u0[KS_A], u1[KS_A], u2[KS_A];
+  float tq[KS_A], cs[KS_A], sn[KS_A];
+#pragma unroll
+  for (int m = 0; m < KS_A; m++) {
+    int a = tile * (KS_THREADS * KS_A) + m * KS_THREADS + threadIdx.x;
+    if (a < nq) {
+      uint4 v = kfrac[a];
+      u0[m] = v.x; u1[m] = v.y; u2[m] = v.z;
+      tq[m] = __uint_as_float(v.w);
+      // step exp(i 2 pi s_c), accurately (it is applied up to 2 kmax times)
+      sincospif((float)(int)v.z * 4.656612873077393e-10f, &sn[m], &cs[m]);
+    } else {
+      u0[m] = u1[m] = u2[m] = 0;
+      tq[m] = 0.f; cs[m] = 1.f; sn[m] = 0.f;
+    }
+  }
+  for (int r = r0; r < r1; r++) {
+    const int4 row = rows[r];
+    const int len = row.w;
+    float c[KS_A], s[KS_A];
+#pragma unroll
+    for (int m = 0; m < KS_A; m++) {
+      unsigned phi = (unsigned)row.x * u0[m] + (unsigned)row.y * u1[m] + (unsigned)row.z * u2[m];
+      __sincosf(phase_rad(phi), &s[m], &c[m]);
+    }
+    for (int kk = 0; kk < len; kk++) {
+      float sr = 0.f, si = 0.f;
+#pragma unroll
+      for (int m = 0; m < KS_A; m++) {
+        sr = fmaf(tq[m], c[m], sr);
+        si = fmaf(tq[m], s[m], si);
+        float cn = c[m] * cs[m] - s[m] * sn[m];
+        float snn = s[m] * cs[m] + c[m] * sn[m];
+        c[m] = cn;
+        s[m] = snn;
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if (lane == 0) red[w][kk] = make_float2(sr, si);
+    }
+    __syncthreads();
+    const int k0 = row_k0[r];
+    for (int kk = threadIdx.x; kk < len; kk += blockDim.x) {
+      double ar = 0, ai = 0;
+#pragma unroll
+      for (int q2 = 0; q2 < KS_THREADS / 32; q2++) {
+        ar += red[q2][kk].x;
+        ai += red[q2][kk].y;
+      }
+      spart[(size_t)tile * ktot + k0 + kk] = make_double2(ar, ai);
+    }
+    __syncthreads();
+  }
+}
+
+// per-k totals; every k of CM3D's list is one thread (md_ewald.c:247-305)
+__global__ void k_sred(int ktot, int ntiles, const double2 *__restrict__ spart, const int *__restrict__ ka,
+                       const int *__restrict__ kb, const int *__restrict__ kc, const double *__restrict__ hmati,
+                       double rvol, double falp2, double2 *__restrict__ sk, float2 *__restrict__ akf,
+                       double2 *__restrict__ akd, double *__restrict__ acc) {
+  double v[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const double TPI = 2.0 * M_PI;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ktot; k += gridDim.x * blockDim.x) {
+    double sr = 0, si = 0;
+    for (int t = 0; t < ntiles; t++) {
+      double2 p = spart[(size_t)t * ktot + k];
+      sr += p.x;
+      si += p.y;
+    }
+    double six = TPI * ka[k], siy = TPI * kb[k], siz = TPI * kc[k];
+    double aka = (six * hmati[0] + siy * hmati[3] + siz * hmati[6]);
+    double akb = (six * hmati[1] + siy * hmati[4] + siz * hmati[7]);
+    double akc = (six * hmati[2] + siy * hmati[5] + siz * hmati[8]);
+    double g2 = aka * aka + akb * akb + akc * akc;
+    double preg = exp(-g2 * falp2) * rvol / g2;
+    double prep = -2. * preg * (g2 * falp2 + 1.) / g2;
+    double smag = sr * sr + si * si;
+    v[0] += preg * smag;
+    v[1] += prep * smag * g2;
+    double ps = prep * smag;
+    v[2] += ps * aka * aka; v[3] += ps * akb * aka; v[4] += ps * akc * aka;
+    v[5] += ps * aka * akb; v[6] += ps * akb * akb; v[7] += ps * akc * akb;
+    v[8] += ps * aka * akc; v[9] += ps * akb * akc; v[10] += ps * akc * akc;
+    sk[k] = make_double2(sr, si);
+    if (akf) akf[k] = make_float2((float)(2. * preg * sr), (float)(2. * preg * si));
+    if (akd) akd[k] = make_double2(2. * preg * sr, 2. * preg * si);
+  }
+  const int slots[11] = {ACC_VK, ACC_VP, ACC_VPT + 0, ACC_VPT + 1, ACC_VPT + 2, ACC_VPT + 3,
+                         ACC_VPT + 4, ACC_VPT + 5, ACC_VPT + 6, ACC_VPT + 7, ACC_VPT + 8};
+  block_acc<11>(v, acc, slots);
+}
+
+__global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4 *__restrict__ kfrac,
+                                                             const int *__restrict__ icharge, int n, int nrows,
+                                                             const int4 *__restrict__ rows,
+                                                             const int *__restrict__ row_k0, int rows_per_split,
+                                                             const float2 *__restrict__ akf, int ktot,
+                                                             const double *__restrict__ hmati, int atomic,
+                                                             double *__restrict__ fxl) {
+  extern __shared__ float2 ak_s[];
+  const int r0 = blockIdx.y * rows_per_split;
+  const int r1 = min(nrows, r0 + rows_per_split);
+  if (r0 >= r1) return;
+  const int kbase = row_k0[r0];
+  const int kend = (r1 < nrows) ? row_k0[r1] : ktot;
+  for (int k = threadIdx.x; k < kend - kbase; k += blockDim.x) ak_s[k] = akf[kbase + k];
+  __syncthreads();
+  unsigned u0[KF_A], u1[KF_A], u2[KF_A];
+  float cs[KF_A], sn[KF_A], tq[KF_A];
+  double U0[KF_A], U1[KF_A], U2[KF_A];
+  int jq[KF_A];
+#pragma unroll
+  for (int m = 0; m < KF_A; m++) {
+    jq[m] = blockIdx.x * (blockDim.x * KF_A) + m * blockDim.x + threadIdx.x;
+    U0[m] = U1[m] = U2[m] = 0.0;
+    if (jq[m] < nq) {
+      uint4 v = kfrac[jq[m]];
+      u0[m] = v.x; u1[m] = v.y; u2[m] = v.z;
+      tq[m] = __uint_as_float(v.w);
+      sincospif((float)(int)v.z * 4.656612873077393e-10f, &sn[m], &cs[m]);
+    } else {
+      u0[m] = u1[m] = u2[m] = 0;
+      tq[m] = 0.f; cs[m] = 1.f; sn[m] = 0.f;
+    }
+  }
+  for (int r = r0; r < r1; r++) {
+    const int4 row = rows[r];
+    const int len = row.w;
+    const int kb0 = row_k0[r] - kbase;
+    float c[KF_A], s[KF_A], W0[KF_A], W1[KF_A];
+#pragma unroll
+    for (int m = 0; m < KF_A; m++) {
+      unsigned phi = (unsigned)row.x * u0[m] + (unsigned)row.y * u1[m] + (unsigned)row.z * u2[m];
+      __sincosf(phase_rad(phi), &s[m], &c[m]);
+      W0[m] = W1[m] = 0.f;
+    }
+    float kcf = (float)row.z;
+    for (int kk = 0; kk < len; kk++) {
+      const float2 a = ak_s[kb0 + kk];
+#pragma unroll
+      for (int m = 0; m < KF_A; m++) {
+        float wv = a.x * s[m] - a.y * c[m];
+        W0[m] += wv;
+        W1[m] = fmaf(kcf, wv, W1[m]);
+        float cn = c[m] * cs[m] - s[m] * sn[m];
+        float snn = s[m] * cs[m] + c[m] * sn[m];
+        c[m] = cn;
+        s[m] = snn;
+      }
+      kcf += 1.f;
+    }
+#pragma unroll
+    for (int m = 0; m < KF_A; m++) {
+      U0[m] += (double)row.x * (double)W0[m];
+      U1[m] += (double)row.y * (double)W0[m];
+      U2[m] += (double)W1[m];
+    }
+  }
+  const double TPI = 2.0 * M_PI;
+#pragma unroll
+  for (int m = 0; m < KF_A; m++) {
+    if (jq[m] >= nq) continue;
+    int i = icharge[jq[m]];
+    double t = TPI * (double)tq[m];
+    // F = tq 2 pi H^-T U  (k = 2 pi H^-T n, md_ewald.c:248-251)
+    double fx = t * (hmati[0] * U0[m] + hmati[3] * U1[m] + hmati[6] * U2[m]);
+    double fy = t * (hmati[1] * U0[m] + hmati[4] * U1[m] + hmati[7] * U2[m]);
+    double fz = t * (hmati[2] * U0[m] + hmati[5] * U1[m] + hmati[8] * U2[m]);
+    if (atomic) {
+      atomicAdd(fxl + i, fx);
+      atomicAdd(fxl + n + i, fy);
+      atomicAdd(fxl + 2 * n + i, fz);
+    } else {
+      fxl[i] += fx;
+      fxl[n + i] += fy;
+      fxl[2 * n + i] += fz;
+    }
+  }
+}
+
+// ------------------------------------------------------------ plain FP64
+__global__ void __launch_bounds__(KS_THREADS) k_sfac_plain(int nq, const double4 *__restrict__ kp, int nrows,
+                                                           const int4 *__restrict__ rows,
+                                                           const int *__restrict__ row_k0, int rows_per_block,
+                                                           int ktot, const double *__restrict__ hmati,
+                                                           double2 *__restrict__ spart) {
+  __shared__ double2 red[KS_THREADS / 32][MAX_ROWLEN];
+  const int tile = blockIdx.x;
+  const int r0 = blockIdx.y * rows_per_block;
+  const int r1 = min(nrows, r0 + rows_per_block);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const double TPI = 2.0 * M_PI;
+  const int a = tile * KS_THREADS + threadIdx.x;
+  double4 p = a < nq ? kp[a] : make_double4(0, 0, 0, 0);
+  double akc0 = (p.x * hmati[6] + p.y * hmati[7] + p.z * hmati[8]) * TPI;   // md_ewald.c:240
+  double cs = cos(akc0), sn = sin(akc0);
+  for (int r = r0; r < r1; r++) {
+    const int4 row = rows[r];
+    double six = TPI * row.x, siy = TPI * row.y, siz = TPI * row.z;
+    double aka = (six * hmati[0] + siy * hmati[3] + siz * hmati[6]);
+    double akb = (six * hmati[1] + siy * hmati[4] + siz * hmati[7]);
+    double akc = (six * hmati[2] + siy * hmati[5] + siz * hmati[8]);
+    double rk = (p.x * aka + p.y * akb + p.z * akc);
+    double c = cos(rk), s = sin(rk);
+    for (int kk = 0; kk < row.w; kk++) {
+      double sr = warp_sum(p.w * c), si = warp_sum(p.w * s);
+      if (lane == 0) red[w][kk] = make_double2(sr, si);
+      double cn = c * cs - s * sn;
+      double snn = s * cs + c * sn;
+      c = cn;
+      s = snn;
+    }
+    __syncthreads();
+    const int k0 = row_k0[r];
+    for (int kk = threadIdx.x; kk < row.w; kk += blockDim.x) {
+      double ar = 0, ai = 0;
+      for (int q2 = 0; q2 < KS_THREADS / 32; q2++) {
+        ar += red[q2][kk].x;
+        ai += red[q2][kk].y;
+      }
+      spart[(size_t)tile * ktot + k0 + kk] = make_double2(ar, ai);
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_kforce_plain(int nq, const double4 *__restrict__ kp, const int *__restrict__ icharge, int n,
+                               int nrows, const int4 *__restrict__ rows, const int *__restrict__ row_k0,
+                               int rows_per_split, const double2 *__restrict__ akd, int ktot,
+                               const double *__restrict__ hmati, int atomic, double *__restrict__ fxl) {
+  const int jq = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r0 = blockIdx.y * rows_per_split;
+  const int r1 = min(nrows, r0 + rows_per_split);
+  if (jq >= nq || r0 >= r1) return;
+  const double TPI = 2.0 * M_PI;
+  const double4 p = kp[jq];
+  const double akc0 = (p.x * hmati[6] + p.y * hmati[7] + p.z * hmati[8]) * TPI;   // md_ewald.c:240
+  const double cs = cos(akc0), sn = sin(akc0);
+  double fx = 0, fy = 0, fz = 0;
+  for (int r = r0; r < r1; r++) {
+    const int4 row = rows[r];
+    const double six = TPI * row.x, siy = TPI * row.y;
+    double c = 1.0, s = 0.0;
+    for (int kk = 0; kk < row.w; kk++) {
+      const double siz = TPI * (row.z + kk);
+      const double aka = (six * hmati[0] + siy * hmati[3] + siz * hmati[6]);
+      const double akb = (six * hmati[1] + siy * hmati[4] + siz * hmati[7]);
+      const double akc = (six * hmati[2] + siy * hmati[5] + siz * hmati[8]);
+      if (kk == 0) {
+        // seed at the start of every row (md_ewald.c:261-267)
+        const double rk = (p.x * aka + p.y * akb + p.z * akc);
+        c = cos(rk);
+        s = sin(rk);
+      } else {
+        // cos(a+b), sin(a+b) recursion along kc (md_ewald.c:273-278)
+        const double cn = c * cs - s * sn, snn = s * cs + c * sn;
+        c = cn;
+        s = snn;
+      }
+      const double2 a = akd[row_k0[r] + kk];
+      const double wv = a.x * s - a.y * c;
+      fx += aka * wv;
+      fy += akb * wv;
+      fz += akc * wv;
+    }
+  }
+  const int i = icharge[jq];
+  fx *= p.w;
+  fy *= p.w;
+  fz *= p.w;
+  if (atomic) {
+    atomicAdd(fxl + i, fx);
+    atomicAdd(fxl + n + i, fy);
+    atomicAdd(fxl + 2 * n + i, fz);
+  } else {
+    fxl[i] += fx;
+    fxl[n + i] += fy;
+    fxl[2 * n + i] += fz;
+  }
+}
+
+// ------------------------------------------------------------------ host
+int kspace_setup(Ctx *c, const cm3d_nb_system *s) {
+  if (c->ncharge == 0 || c->ktot == 0) return CM3D_NB_OK;
+  std::vector<int4> rows;
+  std::vector<int> k0;
+  for (int k = 0; k < s->ktot;) {
+    int e = k + 1;
+    while (e < s->ktot && s->ka[e] == s->ka[k] && s->kb[e] == s->kb[k] && s->kc[e] == s->kc[e - 1] + 1 &&
+           e - k < MAX_ROWLEN)
+      e++;
+    rows.push_back(make_int4(s->ka[k], s->kb[k], s->kc[k], e - k));
+    k0.push_back(k);
+    k = e;
+  }
+  c->nrows = (int)rows.size();
+  CK(cudaMalloc(&c->rows, sizeof(int4) * rows.size()));
+  CK(cudaMalloc(&c->row_k0, sizeof(int) * k0.size()));
+  CK(cudaMemcpy(c->rows, rows.data(), sizeof(int4) * rows.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->row_k0, k0.data(), sizeof(int) * k0.size(), cudaMemcpyHostToDevice));
+  int per_tile = c->mode == CM3D_NB_MIXED ? KS_THREADS * KS_A : KS_THREADS;
+  c->ks_tiles = (c->ncharge + per_tile - 1) / per_tile;
+  c->ks_tile_atoms = per_tile;
+  CK(cudaMalloc(&c->spart, sizeof(double2) * (size_t)c->ks_tiles * c->ktot));
+  CK(cudaMalloc(&c->sk, sizeof(double2) * (size_t)c->ktot));
+  if (c->mode == CM3D_NB_MIXED) {
+    CK(cudaMalloc(&c->akf, sizeof(float2) * (size_t)c->ktot));
+    CK(cudaMalloc(&c->kfrac, sizeof(uint4) * (size_t)c->ncharge));
+  } else {
+    CK(cudaMalloc(&c->akd, sizeof(double2) * (size_t)c->ktot));
+  }
+  CK(cudaMalloc(&c->kposd, sizeof(double4) * (size_t)c->ncharge));
+  CK(cudaMalloc(&c->ka_d, sizeof(int) * (size_t)c->ktot));
+  CK(cudaMalloc(&c->kb_d, sizeof(int) * (size_t)c->ktot));
+  CK(cudaMalloc(&c->kc_d, sizeof(int) * (size_t)c->ktot));
+  CK(cudaMemcpy(c->ka_d, s->ka, sizeof(int) * (size_t)c->ktot, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->kb_d, s->kb, sizeof(int) * (size_t)c->ktot, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->kc_d, s->kc, sizeof(int) * (size_t)c->ktot, cudaMemcpyHostToDevice));
+  // split the rows over enough blocks to fill the machine in the force pass
+  int per_block = c->mode == CM3D_NB_MIXED ? KS_THREADS * KF_A : KS_THREADS;
+  int tiles = (c->ncharge + per_block - 1) / per_block;
+  int split = 1;
+  while (tiles * split < 148 * 4 && split < c->nrows) split *= 2;
+  // every split's A(k) must fit in shared memory
+  for (;;) {
+    int rps = (c->nrows + split - 1) / split;
+    size_t mx = 0;
+    for (int r0 = 0; r0 < c->nrows; r0 += rps) {
+      int r1 = r0 + rps < c->nrows ? r0 + rps : c->nrows;
+      size_t nk = (size_t)((r1 < c->nrows ? k0[r1] : c->ktot) - k0[r0]);
+      if (nk > mx) mx = nk;
+    }
+    c->kf_smem = mx * sizeof(float2);
+    if (c->kf_smem <= 180 * 1024 || split >= c->nrows) break;
+    split *= 2;
+  }
+  if (split > c->nrows) split = c->nrows;
+  c->kf_split = split;
+  return CM3D_NB_OK;
+}
+
+int kspace_forces(Ctx *c) {
+  if (c->ncharge == 0 || c->ktot == 0) return CM3D_NB_OK;
+  const double *dhmati = c->acc + ACC_COUNT;
+  double vol = c->hmat[0] * (c->hmat[4] * c->hmat[8] - c->hmat[5] * c->hmat[7]) +
+               c->hmat[1] * (c->hmat[5] * c->hmat[6] - c->hmat[3] * c->hmat[8]) +
+               c->hmat[2] * (c->hmat[3] * c->hmat[7] - c->hmat[4] * c->hmat[6]);
+  cudaEvent_t e0;
+  tbegin(c, 1, &e0);
+  const bool mixed = c->mode == CM3D_NB_MIXED;
+  k_kprep<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, dhmati,
+                                                         mixed ? c->kfrac : nullptr, c->kposd);
+  // structure factors: enough row chunks per tile to fill the machine
+  int rpb = c->nrows;
+  while (rpb > 1 && (long long)c->ks_tiles * ((c->nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
+  dim3 gs(c->ks_tiles, (c->nrows + rpb - 1) / rpb);
+  if (mixed)
+    k_sfac_mixed<<<gs, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
+                                               c->spart);
+  else
+    k_sfac_plain<<<gs, KS_THREADS, 0, c->st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
+                                               dhmati, c->spart);
+  int ib = 256, gb = grid_for(c->ktot, ib);
+  if (gb > 148 * 4) gb = 148 * 4;
+  k_sred<<<gb, ib, 0, c->st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
+                               c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc);
+  int split = c->kf_split;
+  int rps = (c->nrows + split - 1) / split;
+  if (mixed) {
+    int per = KS_THREADS * KF_A;
+    dim3 gf((c->ncharge + per - 1) / per, split);
+    // shared memory: the A(k) of one split's rows
+    size_t smem = c->kf_smem;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_kforce_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+      attr = true;
+    }
+    k_kforce_mixed<<<gf, KS_THREADS, smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows, c->rows,
+                                                     c->row_k0, rps, c->akf, c->ktot, dhmati, split > 1, c->fxl);
+  } else {
+    dim3 gf((c->ncharge + 255) / 256, split);
+    k_kforce_plain<<<gf, 256, 0, c->st>>>(c->ncharge, c->kposd, c->icharge, c->n, c->nrows, c->rows, c->row_k0,
+                                          rps, c->akd, c->ktot, dhmati, split > 1, c->fxl);
+  }
+  c->launches += 4;
+  tend(c, 1, e0);
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+}  // namespace cm3d

@@ -1,0 +1,429 @@
+// nb_pair.cu -- mixed-precision fused LJ + real-space Ewald pair kernel.
+//
+// The same physics as force_npol (energy/inter/md_fnopol.c:46-255) and
+// force_e (energy/inter/finter_e.c:42-233) -- table lookups with CM3D's
+// 3-point interpolation f = f0 + p (A + p B), A = (f1 - f-1)/2,
+// B = (f-1 - 2 f0 + f1)/2 (md_fnopol.c:148), the RESPA switch, CM3D's energy
+// shifts -- computed in one pass over one list:
+//
+//   * atoms are cell-sorted; each carries FP32 coordinates relative to its
+//     cell's corner (fixed between list rebuilds), so distances are formed
+//     from numbers of at most a cell width instead of absolute coordinates;
+//     the minimum-image shift of a pair is a per-entry 5-bit code into a
+//     27-entry table of cell shifts;
+//   * the list is full (both directions), so a group of TPA lanes owns atom i
+//     and reduces its force with warp shuffles: no atomics, every force is
+//     written exactly once;
+//   * interpolation coefficients are FP32 float4 tables held in shared memory;
+//   * forces are summed per lane in FP32 over chunks of 16 pairs and then in
+//     FP64; energies and virials are reduced in FP64 across lanes.
+#include "nb_common.cuh"
+
+namespace cm3d {
+
+struct MixedP {
+  int n, ntypes, ninter, ntable, iflg, mask;  // mask: bit0 LJ, bit1 charges
+  float rc2_el, dx2c, offc, tablast_e;
+  float hF[9], hiF[9];
+  int tab_smem;
+};
+
+__global__ void k_xq_update(int n, const int *__restrict__ sorig, const double *__restrict__ pos,
+                            const double *__restrict__ corner, const double *__restrict__ q,
+                            float4 *__restrict__ xq) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  int i = sorig[t];
+  xq[t] = make_float4((float)(pos[i] - corner[t]), (float)(pos[n + i] - corner[n + t]),
+                      (float)(pos[2 * n + i] - corner[2 * n + t]), (float)q[i]);
+}
+
+__device__ __forceinline__ float poly(float p, float c0, float a, float b) {
+  return fmaf(p, fmaf(p, b, a), c0);
+}
+
+template <int TPA, bool SMALLBOX, bool NEED_S>
+__global__ void __launch_bounds__(256) k_pair_mixed(
+    MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
+    const long long *__restrict__ off, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
+    const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
+    const float4 *__restrict__ gte, double *__restrict__ fout, double *__restrict__ fshort,
+    double *__restrict__ acc, long long *__restrict__ stat) {
+  extern __shared__ float4 sm[];
+  float4 *shift = sm;                                   // 27
+  float *fcut = reinterpret_cast<float *>(sm + 28);     // 8 * ninter
+  int nf4 = (8 * P.ninter + 3) / 4;
+  int *map = reinterpret_cast<int *>(sm + 28 + nf4);    // ntypes^2
+  int nm4 = (P.ntypes * P.ntypes + 3) / 4;
+  float4 *tl_s = sm + 28 + nf4 + nm4;
+  const float4 *tl = gtl, *te = gte;
+  for (int k = threadIdx.x; k < 27; k += blockDim.x) shift[k] = gshift[k];
+  for (int k = threadIdx.x; k < 8 * P.ninter; k += blockDim.x) fcut[k] = gfcut[k];
+  for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) map[k] = gmap[k];
+  if (P.tab_smem) {
+    int nl = (P.mask & 1) ? 3 * P.ninter * P.ntable : 0;
+    int ne = (P.mask & 2) ? 2 * P.ntable : 0;
+    for (int k = threadIdx.x; k < nl; k += blockDim.x) tl_s[k] = gtl[k];
+    float4 *te_s = tl_s + 3 * P.ninter * P.ntable;
+    for (int k = threadIdx.x; k < ne; k += blockDim.x) te_s[k] = gte[k];
+    tl = tl_s;
+    te = te_s;
+  }
+  __syncthreads();
+
+  const int g = threadIdx.x % TPA;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) / TPA;
+  const bool active = t < P.n;
+  double Fx = 0, Fy = 0, Fz = 0, Sx = 0, Sy = 0, Sz = 0;
+  float elj = 0, eljh = 0, eel = 0, qqs = 0;
+  float vl0 = 0, vl1 = 0, vl2 = 0, vl4 = 0, vl5 = 0, vl8 = 0;
+  float ve0 = 0, ve1 = 0, ve2 = 0, ve4 = 0, ve5 = 0, ve8 = 0;
+  unsigned under = 0;
+  if (active) {
+    const float4 xi = xq[t];
+    const int ti = styp[t];
+    const long long k0 = off[t], k1 = off[t + 1];
+    const uint32_t fl_lj = P.iflg == 1 ? ENT_LJ : ENT_LJS;
+    const uint32_t fl_el = P.iflg == 1 ? ENT_EL : ENT_ELS;
+    float fx = 0, fy = 0, fz = 0, sx = 0, sy = 0, sz = 0;
+    int cnt = 0;
+    for (long long k = k0 + g; k < k1; k += TPA) {
+      const uint32_t e = __ldg(nbr + k);
+      const int j = e & ENT_JMASK;
+      const float4 xj = xq[j];
+      const float4 sh = shift[(e >> ENT_CODE_SHIFT) & 31];
+      float dx = (xi.x - xj.x) + sh.x;
+      float dy = (xi.y - xj.y) + sh.y;
+      float dz = (xi.z - xj.z) + sh.z;
+      if (SMALLBOX) {
+        float s0 = P.hiF[0] * dx + P.hiF[1] * dy + P.hiF[2] * dz;
+        float s1 = P.hiF[3] * dx + P.hiF[4] * dy + P.hiF[5] * dz;
+        float s2 = P.hiF[6] * dx + P.hiF[7] * dy + P.hiF[8] * dz;
+        s0 -= rintf(s0);
+        s1 -= rintf(s1);
+        s2 -= rintf(s2);
+        dx = P.hF[0] * s0 + P.hF[1] * s1 + P.hF[2] * s2;
+        dy = P.hF[3] * s0 + P.hF[4] * s1 + P.hF[5] * s2;
+        dz = P.hF[6] * s0 + P.hF[7] * s1 + P.hF[8] * s2;
+      }
+      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      float ftot = 0.f, fsh = 0.f;
+      if ((e & fl_el) && (P.mask & 2) && r2 < P.rc2_el) {
+        float p = fmaf(r2, P.dx2c, -P.offc);
+        int kk = (int)p;
+        if (kk < 1) {
+          under++;
+          kk = 1;
+          p = 1.f;
+        }
+        p -= (float)kk;
+        const float4 c0 = te[2 * kk];
+        const float qq = xi.w * xj.w;
+        const float fe = qq * poly(p, c0.x, c0.y, c0.z);
+        ftot += fe;
+        if (P.iflg == 1) {
+          const float4 c1 = te[2 * kk + 1];
+          eel = fmaf(qq, poly(p, c0.w, c1.x, c1.y), eel);
+          qqs += qq;
+          const float fdx = fe * dx, fdy = fe * dy, fdz = fe * dz;
+          ve0 = fmaf(fdx, dx, ve0);
+          ve1 = fmaf(fdx, dy, ve1);
+          ve2 = fmaf(fdx, dz, ve2);
+          ve4 = fmaf(fdy, dy, ve4);
+          ve5 = fmaf(fdy, dz, ve5);
+          ve8 = fmaf(fdz, dz, ve8);
+          if (NEED_S) fsh += fe;           // force_e's switch is never engaged
+        }
+      }
+      if ((e & fl_lj) && (P.mask & 1)) {
+        const int in = map[ti * P.ntypes + styp[j]];
+        const float *fc = fcut + 8 * in;
+        const float rmax2 = P.iflg == 1 ? fc[0] : fc[4];
+        if (r2 < rmax2) {
+          float p = fmaf(r2, fc[2], -fc[1]);
+          int kk = (int)p;
+          if (kk < 1) {
+            under++;
+            kk = 1;
+            p = 1.f;
+          }
+          p -= (float)kk;
+          const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
+          const float4 a0 = T[0], a1 = T[1];
+          const float f = poly(p, a0.x, a0.y, a0.z);
+          float swv = 1.f;
+          if ((NEED_S || P.iflg == 0) && r2 > fc[3]) {
+            const float4 a2 = T[2];
+            swv = poly(p, a1.z, a1.w, a2.x);
+          }
+          if (P.iflg == 1) {
+            ftot += f;
+            const float v = poly(p, a0.w, a1.x, a1.y);
+            elj += v;
+            eljh += v - fc[5];
+            const float fdx = f * dx, fdy = f * dy, fdz = f * dz;
+            vl0 = fmaf(fdx, dx, vl0);
+            vl1 = fmaf(fdx, dy, vl1);
+            vl2 = fmaf(fdx, dz, vl2);
+            vl4 = fmaf(fdy, dy, vl4);
+            vl5 = fmaf(fdy, dz, vl5);
+            vl8 = fmaf(fdz, dz, vl8);
+            if (NEED_S) fsh += f * swv;
+          } else {
+            ftot += f * swv;
+          }
+        }
+      }
+      // F_i = -f d  (md_fnopol.c:227-229)
+      fx = fmaf(-ftot, dx, fx);
+      fy = fmaf(-ftot, dy, fy);
+      fz = fmaf(-ftot, dz, fz);
+      if (NEED_S) {
+        sx = fmaf(-fsh, dx, sx);
+        sy = fmaf(-fsh, dy, sy);
+        sz = fmaf(-fsh, dz, sz);
+      }
+      if (++cnt == 16) {
+        Fx += fx; Fy += fy; Fz += fz;
+        fx = fy = fz = 0.f;
+        if (NEED_S) {
+          Sx += sx; Sy += sy; Sz += sz;
+          sx = sy = sz = 0.f;
+        }
+        cnt = 0;
+      }
+    }
+    Fx += fx; Fy += fy; Fz += fz;
+    if (NEED_S) {
+      Sx += sx; Sy += sy; Sz += sz;
+    }
+  }
+  // reduce atom i's force over its TPA lanes (aligned lane groups)
+#pragma unroll
+  for (int o = TPA / 2; o > 0; o >>= 1) {
+    Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+    Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+    Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+    if (NEED_S) {
+      Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
+      Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
+      Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
+    }
+  }
+  if (active && g == 0) {
+    const int i = sorig[t], n = P.n;
+    fout[i] += Fx;
+    fout[n + i] += Fy;
+    fout[2 * n + i] += Fz;
+    if (NEED_S && P.iflg == 1) {
+      fshort[i] += Sx;
+      fshort[n + i] += Sy;
+      fshort[2 * n + i] += Sz;
+    }
+  }
+  if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), (unsigned long long)under);
+  if (P.iflg == 1) {
+    // every pair was visited from both ends: halve energies and virials
+    double v[18] = {0.5 * elj, 0.5 * eljh, 0.5 * -(double)(vl0 + vl4 + vl8),
+                    -0.5 * vl0, -0.5 * vl1, -0.5 * vl2, -0.5 * vl4, -0.5 * vl5, -0.5 * vl8,
+                    0.5 * eel, 0.5 * ((double)eel - (double)P.tablast_e * (double)qqs),
+                    0.5 * -(double)(ve0 + ve4 + ve8),
+                    -0.5 * ve0, -0.5 * ve1, -0.5 * ve2, -0.5 * ve4, -0.5 * ve5, -0.5 * ve8};
+    const int slots[18] = {ACC_SPOTL, ACC_SPOTHL, ACC_SPRSL, ACC_SPRSLT + 0, ACC_SPRSLT + 1,
+                           ACC_SPRSLT + 2, ACC_SPRSLT + 4, ACC_SPRSLT + 5, ACC_SPRSLT + 8,
+                           ACC_SPOTE, ACC_SPOTHE, ACC_SPRSE, ACC_SPRSET + 0, ACC_SPRSET + 1,
+                           ACC_SPRSET + 2, ACC_SPRSET + 4, ACC_SPRSET + 5, ACC_SPRSET + 8};
+    block_acc<18>(v, acc, slots);
+  }
+}
+
+// ------------------------------------------------------------------ host
+static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
+  size_t nf4 = (8 * (size_t)c->ninter + 3) / 4, nm4 = ((size_t)c->ntypes * c->ntypes + 3) / 4;
+  size_t b = (28 + nf4 + nm4) * sizeof(float4);
+  if (with_tables) {
+    b += (size_t)3 * c->ninter * c->ntable * sizeof(float4);
+    if (mask & 2) b += (size_t)2 * c->ntable * sizeof(float4);
+  }
+  return b;
+}
+
+template <int TPA, bool SB, bool NS>
+static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
+  const int B = 256;
+  long long threads = (long long)c->n * TPA;
+  int grid = grid_for(threads, B);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(k_pair_mixed<TPA, SB, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  k_pair_mixed<TPA, SB, NS><<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->off + 4 * ((size_t)c->n + 1),
+                                                      c->nbr, c->shift, c->map, c->fcut, c->ftab_lj, c->ftab_el,
+                                                      fout, c->fxs, c->acc, c->stat);
+}
+
+template <bool SB, bool NS>
+static int launch_tpa(Ctx *c, const MixedP &P, size_t smem, double *fout) {
+  switch (c->tpa) {
+    case 4: launch_t<4, SB, NS>(c, P, smem, fout); break;
+    case 8: launch_t<8, SB, NS>(c, P, smem, fout); break;
+    case 16: launch_t<16, SB, NS>(c, P, smem, fout); break;
+    case 32: launch_t<32, SB, NS>(c, P, smem, fout); break;
+    default: launch_t<8, SB, NS>(c, P, smem, fout); break;
+  }
+  return CM3D_NB_OK;
+}
+
+bool g_smallbox_warned = false;
+
+// mixed mode: which bit0 LJ, bit1 charges; iflg 1 -> fxl (+fxs), 0 -> fxs
+int mixed_pairs(Ctx *c, int iflg, int mask) {
+  if (c->ncharge == 0) mask &= 1;
+  if (c->ninter == 0) mask &= 2;
+  if (!mask || c->hcount[LT_FULL] == 0) return CM3D_NB_OK;
+  MixedP P;
+  P.n = c->n;
+  P.ntypes = c->ntypes;
+  P.ninter = c->ninter;
+  P.ntable = c->ntable;
+  P.iflg = iflg;
+  P.mask = mask;
+  P.rc2_el = (float)c->rmaxl_coul2;
+  P.dx2c = (float)c->dx2coul;
+  P.offc = (float)(c->rmins_coul2 * c->dx2coul);
+  P.tablast_e = (float)c->tablast_e;
+  for (int k = 0; k < 9; k++) {
+    P.hF[k] = (float)c->hmat[k];
+    P.hiF[k] = (float)c->hmati[k];
+  }
+  size_t full = smem_bytes(c, true, mask);
+  P.tab_smem = full <= 160 * 1024;
+  size_t smem = smem_bytes(c, P.tab_smem, mask);
+  bool ns = iflg == 1 && (c->need_short || c->nres_lrf > 1);
+  // boxes narrower than two list radii need the on-the-fly minimum image
+  bool sb = false;
+  for (int d = 0; d < 3; d++) {
+    double w = 1.0 / sqrt(c->hmati[3 * d] * c->hmati[3 * d] + c->hmati[3 * d + 1] * c->hmati[3 * d + 1] +
+                          c->hmati[3 * d + 2] * c->hmati[3 * d + 2]);
+    if (w < 2.0 * c->rlist_max) sb = true;
+  }
+  double *fout = iflg == 1 ? c->fxl : c->fxs;
+  const int B = 256;
+  k_xq_update<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, c->cell_atoms, c->pos, c->corner, c->q, c->xq);
+  cudaEvent_t e0;
+  tbegin(c, 0, &e0);
+  if (sb) {
+    if (ns) launch_tpa<true, true>(c, P, smem, fout);
+    else launch_tpa<true, false>(c, P, smem, fout);
+  } else {
+    if (ns) launch_tpa<false, true>(c, P, smem, fout);
+    else launch_tpa<false, false>(c, P, smem, fout);
+  }
+  tend(c, 0, e0);
+  c->launches += 2;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+// FP32 interpolation coefficients and the 27 cell shifts (mixed mode)
+int pair_setup(Ctx *c) {
+  if (c->mode != CM3D_NB_MIXED) return CM3D_NB_OK;
+  const int nt = c->ntable, ni = c->ninter;
+  std::vector<double> vt((size_t)ni * nt), dv((size_t)ni * nt), sw((size_t)ni * nt), cut(8 * (size_t)ni);
+  if (ni > 0) {
+    CK(cudaMemcpy(vt.data(), c->vtab, sizeof(double) * vt.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dv.data(), c->dvtab, sizeof(double) * dv.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sw.data(), c->switchs, sizeof(double) * sw.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cut.data(), c->icut, sizeof(double) * cut.size(), cudaMemcpyDeviceToHost));
+  }
+  auto coef = [](const double *t, int k, double &f0, double &a, double &b) {
+    if (k < 1) k = 1;
+    f0 = t[k];
+    a = 0.5 * (t[k + 1] - t[k - 1]);
+    b = 0.5 * (t[k - 1] - 2.0 * t[k] + t[k + 1]);
+  };
+  std::vector<float4> tl((size_t)3 * ni * nt), te((size_t)2 * nt);
+  for (int in = 0; in < ni; in++) {
+    for (int k = 0; k < nt; k++) {
+      double d0 = 0, da = 0, db = 0, v0 = 0, va = 0, vb = 0, s0 = 0, sa = 0, sb = 0;
+      if (k >= 1 && k <= nt - 2) {
+        coef(&dv[(size_t)in * nt], k, d0, da, db);
+        coef(&vt[(size_t)in * nt], k, v0, va, vb);
+        coef(&sw[(size_t)in * nt], k, s0, sa, sb);
+      }
+      size_t b = 3 * ((size_t)in * nt + k);
+      tl[b] = make_float4((float)d0, (float)da, (float)db, (float)v0);
+      tl[b + 1] = make_float4((float)va, (float)vb, (float)s0, (float)sa);
+      tl[b + 2] = make_float4((float)sb, 0.f, 0.f, 0.f);
+    }
+  }
+  if (c->ncharge > 0) {
+    std::vector<double> ct(nt), dct(nt);
+    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < nt; k++) {
+      double d0 = 0, da = 0, db = 0, v0 = 0, va = 0, vb = 0;
+      if (k >= 1 && k <= nt - 2) {
+        coef(dct.data(), k, d0, da, db);
+        coef(ct.data(), k, v0, va, vb);
+      }
+      te[2 * k] = make_float4((float)d0, (float)da, (float)db, (float)v0);
+      te[2 * k + 1] = make_float4((float)va, (float)vb, 0.f, 0.f);
+    }
+  }
+  // per interaction: rmaxl_cut2, rmins_cut2*dx2tab, dx2tab, rminl_cut2,
+  // rmaxs_cut2, vtab[ntable-4]
+  std::vector<float> fc(8 * (size_t)(ni > 0 ? ni : 1), 0.f);
+  for (int in = 0; in < ni; in++) {
+    const double *q = &cut[8 * (size_t)in];
+    fc[8 * in + 0] = (float)q[2];
+    fc[8 * in + 1] = (float)(q[1] * q[6]);
+    fc[8 * in + 2] = (float)q[6];
+    fc[8 * in + 3] = (float)q[3];
+    fc[8 * in + 4] = (float)q[0];
+    fc[8 * in + 5] = (float)q[7];
+  }
+  CK(cudaMalloc(&c->ftab_lj, sizeof(float4) * (tl.size() > 0 ? tl.size() : 1)));
+  CK(cudaMalloc(&c->ftab_el, sizeof(float4) * te.size()));
+  CK(cudaMalloc(&c->fcut, sizeof(float) * fc.size()));
+  if (!tl.empty()) CK(cudaMemcpy(c->ftab_lj, tl.data(), sizeof(float4) * tl.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->ftab_el, te.data(), sizeof(float4) * te.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->fcut, fc.data(), sizeof(float) * fc.size(), cudaMemcpyHostToDevice));
+  // cell shift for code (kx+1)*9 + (ky+1)*3 + (kz+1):  H (k / nc)
+  std::vector<float4> sh(27);
+  for (int a = -1; a <= 1; a++)
+    for (int b = -1; b <= 1; b++)
+      for (int d = -1; d <= 1; d++) {
+        double f0 = (double)a / c->nc[0], f1 = (double)b / c->nc[1], f2 = (double)d / c->nc[2];
+        const double *h = c->hmat;
+        sh[(a + 1) * 9 + (b + 1) * 3 + (d + 1)] =
+            make_float4((float)(h[0] * f0 + h[1] * f1 + h[2] * f2), (float)(h[3] * f0 + h[4] * f1 + h[5] * f2),
+                        (float)(h[6] * f0 + h[7] * f1 + h[8] * f2), 0.f);
+      }
+  CK(cudaMalloc(&c->shift, sizeof(float4) * 27));
+  CK(cudaMemcpy(c->shift, sh.data(), sizeof(float4) * 27, cudaMemcpyHostToDevice));
+  if (c->tpa == 0) {
+    // enough lane groups to fill the GPU, but at least 8 lanes per atom so a
+    // group reads a full 32-byte sector of the list
+    long long want = 148LL * 2048 * 2;
+    int tpa = 8;
+    while (tpa < 32 && (long long)c->n * tpa < want) tpa *= 2;
+    c->tpa = tpa;
+  }
+  return CM3D_NB_OK;
+}
+
+int pair_forces(Ctx *c, int iflg, int which) {
+  if (c->mode == CM3D_NB_PLAIN_FP64) {
+    if (which & 1) {
+      int rc = plain_pairs(c, iflg, 0);
+      if (rc) return rc;
+    }
+    if (which & 2) return plain_pairs(c, iflg, 1);
+    return CM3D_NB_OK;
+  }
+  return mixed_pairs(c, iflg, which);
+}
+
+}  // namespace cm3d

@@ -1,0 +1,636 @@
+// nb_step.cu -- the RESPA step on the device.
+//
+// Restates step() (integrate/md_step.c:62-159) for NVE with the level
+// structure ninter (nres_lrf) / ninrra (nres_tors) / ninnra (nres_intra), the
+// force levels of force() (energy/control/md_fcntr.c:44-134), nrefsh()
+// (energy/control/md_finter.c:43-108, with its RESETPOS pull-back) and the
+// harmonic fbond/fbend of the inner level (energy/intra/md_fbond.c:76-125,
+// md_fbend.c:126-260).
+//
+// Bonds, bends and excluded-pair corrections only couple atoms of one
+// molecule, so the atoms are partitioned into groups (connected components
+// of those terms) and one thread owns a group: the whole inner loop -- every
+// ninnra substep with its bonded forces -- runs in one kernel with no grid
+// synchronisation, followed by the displacement test of nrefsh.  The
+// excluded-pair correction (ecorr) and the bonded energies of getvireal are
+// likewise per-group.
+#include <math.h>
+
+#include <algorithm>
+#include <numeric>
+
+#include "nb_common.cuh"
+
+namespace cm3d {
+
+struct StepP {
+  int n, ngroups, ninrra, ninnra;
+  double dter, dter1, dts2, dtr2, dta2;
+  double skin2q;      // (skin/2)^2 = .25 skin^2  (md_finter.c:63)
+  double kappa, kappa2;
+  int use_fxs;
+};
+
+// bonded forces of one group into fxa (raw forces), fbond/fbend in CM3D's order
+__device__ __forceinline__ void group_bonded(int g, int n, const double *__restrict__ pos,
+                                             double *__restrict__ fxa, const int *__restrict__ gboff,
+                                             const int4 *__restrict__ bij, const double2 *__restrict__ bp,
+                                             const int *__restrict__ geoff, const int4 *__restrict__ eijk,
+                                             const double2 *__restrict__ ep) {
+  for (int b = gboff[g]; b < gboff[g + 1]; b++) {
+    const int i = bij[b].x, j = bij[b].y;
+    double dx = pos[i] - pos[j], dy = pos[n + i] - pos[n + j], dz = pos[2 * n + i] - pos[2 * n + j];
+    double r = sqrt(dx * dx + dy * dy + dz * dz);
+    double dr = r - bp[b].x;
+    double fr = bp[b].y * dr / r;
+    dx *= fr; dy *= fr; dz *= fr;
+    fxa[i] -= dx; fxa[n + i] -= dy; fxa[2 * n + i] -= dz;
+    fxa[j] += dx; fxa[n + j] += dy; fxa[2 * n + j] += dz;
+  }
+  for (int b = geoff[g]; b < geoff[g + 1]; b++) {
+    const int i = eijk[b].x, j = eijk[b].y, k = eijk[b].z;
+    double ax = pos[i] - pos[j], ay = pos[n + i] - pos[n + j], az = pos[2 * n + i] - pos[2 * n + j];
+    double al = ax * ax + ay * ay + az * az;
+    double bx = pos[k] - pos[j], by = pos[n + k] - pos[n + j], bz = pos[2 * n + k] - pos[2 * n + j];
+    double bl = bx * bx + by * by + bz * bz;
+    double adotb = ax * bx + ay * by + az * bz;
+    double r11 = 1. / sqrt(al * bl);
+    double costh = adotb * r11;
+    double dudth, dthdcos;
+    if (fabs(costh) >= 1.) {
+      dthdcos = -1.;
+      dudth = 0.;
+    } else {
+      double th = acos(costh);
+      double dth = th - ep[b].x;
+      dudth = ep[b].y * dth;
+      dthdcos = -1. / sqrt(1. - costh * costh);
+    }
+    double dudcos = dudth * dthdcos;
+    double d1x = costh * ax / al - bx * r11, d1y = costh * ay / al - by * r11, d1z = costh * az / al - bz * r11;
+    double d3x = costh * bx / bl - ax * r11, d3y = costh * by / bl - ay * r11, d3z = costh * bz / bl - az * r11;
+    fxa[i] += dudcos * d1x; fxa[n + i] += dudcos * d1y; fxa[2 * n + i] += dudcos * d1z;
+    fxa[j] += dudcos * (-d1x - d3x); fxa[n + j] += dudcos * (-d1y - d3y); fxa[2 * n + j] += dudcos * (-d1z - d3z);
+    fxa[k] += dudcos * d3x; fxa[n + k] += dudcos * d3y; fxa[2 * n + k] += dudcos * d3z;
+  }
+}
+
+// force(2) alone: bonds + bends of every group into fxa, then rmass
+__global__ void k_bonded(StepP P, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
+                         const double *__restrict__ pos, const double *__restrict__ mass, double *__restrict__ fxa,
+                         const int *__restrict__ gboff, const int4 *__restrict__ bij, const double2 *__restrict__ bp,
+                         const int *__restrict__ geoff, const int4 *__restrict__ eijk, const double2 *__restrict__ ep) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.ngroups) return;
+  const int n = P.n;
+  for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
+    int i = gatoms[a];
+    fxa[i] = fxa[n + i] = fxa[2 * n + i] = 0.;
+  }
+  group_bonded(g, n, pos, fxa, gboff, bij, bp, geoff, eijk, ep);
+  for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
+    int i = gatoms[a];
+    double r = 1. / mass[i];
+    fxa[i] *= r; fxa[n + i] *= r; fxa[2 * n + i] *= r;
+  }
+}
+
+// One pass of md_step.c:95-136 for level `intr`: the kick with the
+// nonbonded accelerations, the ninrra x ninnra inner loop with force(2) on
+// this group, then nrefsh's displacement test.
+__global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
+                        double *__restrict__ pos, double *__restrict__ vel, const double *__restrict__ mass,
+                        const double *__restrict__ fxl, const double *__restrict__ fxs, double *__restrict__ fxa,
+                        const double *__restrict__ dxn, const int *__restrict__ gboff,
+                        const int4 *__restrict__ bij, const double2 *__restrict__ bp,
+                        const int *__restrict__ geoff, const int4 *__restrict__ eijk,
+                        const double2 *__restrict__ ep, int *__restrict__ istate) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.ngroups) return;
+  const int n = P.n;
+  const int a0 = gaoff[g], a1 = gaoff[g + 1];
+  // long and short range intermolecular kick (md_step.c:97-103)
+  for (int a = a0; a < a1; a++) {
+    int i = gatoms[a];
+    for (int d = 0; d < 3; d++) {
+      int x = d * n + i;
+      if (intr == 0) vel[x] += P.dter * fxl[x] + (P.use_fxs ? P.dter1 * fxs[x] : 0.0);
+      else vel[x] += P.dts2 * fxs[x];
+    }
+  }
+  const bool bonded = gboff[g + 1] > gboff[g] || geoff[g + 1] > geoff[g];
+  for (int inrra = 0; inrra < P.ninrra; inrra++) {
+    // the torsion level (fxr) is empty in this engine
+    for (int intra = 0; intra < P.ninnra; intra++) {
+      for (int a = a0; a < a1; a++) {
+        int i = gatoms[a];
+        for (int d = 0; d < 3; d++) {
+          int x = d * n + i;
+          vel[x] += P.dta2 * fxa[x];
+          pos[x] += P.dta2 * vel[x];
+          pos[x] += P.dta2 * vel[x];
+        }
+      }
+      if (bonded) {
+        for (int a = a0; a < a1; a++) {
+          int i = gatoms[a];
+          fxa[i] = fxa[n + i] = fxa[2 * n + i] = 0.;
+        }
+        group_bonded(g, n, pos, fxa, gboff, bij, bp, geoff, eijk, ep);
+        for (int a = a0; a < a1; a++) {
+          int i = gatoms[a];
+          double r = 1. / mass[i];
+          fxa[i] *= r; fxa[n + i] *= r; fxa[2 * n + i] *= r;
+        }
+      }
+      for (int a = a0; a < a1; a++) {
+        int i = gatoms[a];
+        for (int d = 0; d < 3; d++) vel[d * n + i] += P.dta2 * fxa[d * n + i];
+      }
+    }
+  }
+  // nrefsh: any |r - r_last|^2 > skin^2/4 (md_finter.c:63-71)
+  bool far = false;
+  for (int a = a0; a < a1; a++) {
+    int i = gatoms[a];
+    double xc = dxn[i] - pos[i], yc = dxn[n + i] - pos[n + i], zc = dxn[2 * n + i] - pos[2 * n + i];
+    if (xc * xc + yc * yc + zc * zc > P.skin2q) far = true;
+  }
+  if (far) istate[IS_REBUILD] = 1;
+}
+
+// standalone displacement test (cm3d_nb_nrefsh)
+__global__ void k_disp(int n, double skin2q, const double *__restrict__ pos, const double *__restrict__ dxn,
+                       int *__restrict__ istate) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double xc = dxn[i] - pos[i], yc = dxn[n + i] - pos[n + i], zc = dxn[2 * n + i] - pos[2 * n + i];
+  if (xc * xc + yc * yc + zc * zc > skin2q) istate[IS_REBUILD] = 1;
+}
+
+// RESETPOS (md_finter.c:79-95): if a rebuild is due fewer than 3 steps after
+// the previous one, pull every atom that moved more than skin/2 back toward
+// its position at the last rebuild (by CM3D's factor skin2/d^2)
+__global__ void k_resetpos(int n, double skin2q, double *__restrict__ pos, const double *__restrict__ dxn,
+                           const int *__restrict__ istate, long long *__restrict__ stat) {
+  if (istate[IS_REBUILD] == 0) return;
+  if (istate[IS_ISTEP] - istate[IS_ISTEPLAST] >= 3) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) atomicAdd((unsigned long long *)(stat + ST_RESETS), 1ull);
+  if (i >= n) return;
+  double xc = pos[i] - dxn[i], yc = pos[n + i] - dxn[n + i], zc = pos[2 * n + i] - dxn[2 * n + i];
+  double d2 = xc * xc + yc * yc + zc * zc;
+  if (d2 > skin2q) {
+    double scale = skin2q / d2;
+    pos[i] = dxn[i] + scale * xc;
+    pos[n + i] = dxn[n + i] + scale * yc;
+    pos[2 * n + i] = dxn[2 * n + i] + scale * zc;
+  }
+}
+
+// start of force(1) (md_fcntr.c:64-73): zero fxl (and fxs), add the
+// excluded-pair correction of every group (ecorr, md_ewald.c:385-453), and
+// collect the group's bonded energies (getvbond / getvbend)
+__global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
+                             const double *__restrict__ pos, const double *__restrict__ q,
+                             double *__restrict__ fxl, double *__restrict__ fxs, const int *__restrict__ gcoff,
+                             const int2 *__restrict__ cij, const int *__restrict__ gboff,
+                             const int4 *__restrict__ bij, const double2 *__restrict__ bp,
+                             const int *__restrict__ geoff, const int4 *__restrict__ eijk,
+                             const double2 *__restrict__ ep, double *__restrict__ acc) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = P.n;
+  // ecorr: pot, prs, t0 t1 t2 t4 t5 t8 | bond: v, w, t0..t8 | bend: v
+  double v[20];
+#pragma unroll
+  for (int k = 0; k < 20; k++) v[k] = 0.;
+  if (g < P.ngroups) {
+    for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
+      int i = gatoms[a];
+      fxl[i] = fxl[n + i] = fxl[2 * n + i] = 0.;
+      if (zero_fxs) fxs[i] = fxs[n + i] = fxs[2 * n + i] = 0.;
+    }
+    const double sqrt_pi = 1. / sqrt(M_PI);
+    for (int c = gcoff[g]; c < gcoff[g + 1]; c++) {
+      int ii = cij[c].x, jj = cij[c].y;
+      double xd = pos[ii] - pos[jj], yd = pos[n + ii] - pos[n + jj], zd = pos[2 * n + ii] - pos[2 * n + jj];
+      double dis2 = xd * xd + yd * yd + zd * zd, dis = sqrt(dis2);
+      double qijr = q[ii] * q[jj] / dis;
+      double erfr = erf(dis * P.kappa);
+      v[0] += -qijr * erfr;
+      double dv = -qijr * (-2. * P.kappa * exp(-P.kappa2 * dis2) * sqrt_pi + erfr / dis);
+      v[1] += dis * dv;
+      dv /= dis;
+      v[2] += dv * xd * xd; v[3] += dv * xd * yd; v[4] += dv * xd * zd;
+      v[5] += dv * yd * yd; v[6] += dv * yd * zd; v[7] += dv * zd * zd;
+      xd *= dv; yd *= dv; zd *= dv;
+      fxl[ii] += xd; fxl[n + ii] += yd; fxl[2 * n + ii] += zd;
+      fxl[jj] -= xd; fxl[n + jj] -= yd; fxl[2 * n + jj] -= zd;
+    }
+    // getvbond (md_fbond.c:160-207), harmonic
+    for (int b = gboff[g]; b < gboff[g + 1]; b++) {
+      const int i = bij[b].x, j = bij[b].y;
+      double dx = pos[i] - pos[j], dy = pos[n + i] - pos[n + j], dz = pos[2 * n + i] - pos[2 * n + j];
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      double dr = r - bp[b].x;
+      double fk = bp[b].y;
+      v[8] += .5 * fk * dr * dr;
+      fk = fk * dr / r;
+      v[9] -= fk * r * r;
+      v[10] -= fk * dx * dx; v[11] -= fk * dy * dx; v[12] -= fk * dz * dx;
+      v[13] -= fk * dx * dy; v[14] -= fk * dy * dy; v[15] -= fk * dz * dy;
+      v[16] -= fk * dx * dz; v[17] -= fk * dy * dz; v[18] -= fk * dz * dz;
+    }
+    // getvbend (md_fbend.c:295-330), harmonic; its virial needs -DPRESSURE
+    for (int b = geoff[g]; b < geoff[g + 1]; b++) {
+      const int i = eijk[b].x, j = eijk[b].y, k = eijk[b].z;
+      double ax = pos[i] - pos[j], ay = pos[n + i] - pos[n + j], az = pos[2 * n + i] - pos[2 * n + j];
+      double al = ax * ax + ay * ay + az * az;
+      double bx = pos[k] - pos[j], by = pos[n + k] - pos[n + j], bz = pos[2 * n + k] - pos[2 * n + j];
+      double bl = bx * bx + by * by + bz * bz;
+      double r11 = 1. / sqrt(al * bl), costh = (ax * bx + ay * by + az * bz) * r11;
+      costh = costh < 1. ? costh : 1.;
+      costh = costh > -1. ? costh : -1.;
+      double th = fabs(costh) >= 1. ? 1. : acos(costh);
+      double dth = th - ep[b].x;
+      v[19] += .5 * ep[b].y * dth * dth;
+    }
+  }
+  const int slots[20] = {ACC_POT_ECORR, ACC_PRS_ECORR, ACC_PRS_ECORRT + 0, ACC_PRS_ECORRT + 1,
+                         ACC_PRS_ECORRT + 2, ACC_PRS_ECORRT + 4, ACC_PRS_ECORRT + 5, ACC_PRS_ECORRT + 8,
+                         ACC_VBOND, ACC_WBOND, ACC_WBONDT + 0, ACC_WBONDT + 1, ACC_WBONDT + 2,
+                         ACC_WBONDT + 3, ACC_WBONDT + 4, ACC_WBONDT + 5, ACC_WBONDT + 6, ACC_WBONDT + 7,
+                         ACC_WBONDT + 8, ACC_VBEND};
+  block_acc<20>(v, acc, slots);
+}
+
+// end of force(1) / force(0): rmass (utils/md_util.new.c:219) and, inside
+// step(), the closing kick of md_step.c:139-145; then the kinetic tensor of
+// get_p2mt (md_fcntr.c:332-354) for geteng
+__global__ void k_finish(int n, int level, int kick, int rm_l, int rm_s, double dk_l, double dk_s,
+                         const double *__restrict__ mass, double *__restrict__ fxl, double *__restrict__ fxs,
+                         double *__restrict__ vel, double *__restrict__ acc, int *__restrict__ istate,
+                         int advance_step) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  if (i < n) {
+    double r = 1. / mass[i];
+    for (int d = 0; d < 3; d++) {
+      int x = d * n + i;
+      if (rm_l) fxl[x] *= r;
+      if (rm_s) fxs[x] *= r;
+      if (kick) {
+        if (level == 1) vel[x] += dk_l * fxl[x] + (rm_s ? dk_s * fxs[x] : 0.0);
+        else vel[x] += dk_s * fxs[x];
+      }
+    }
+    double m = mass[i], vx = vel[i], vy = vel[n + i], vz = vel[2 * n + i];
+    v[0] = m * (vx * vx);
+    v[1] = m * (vy * vx);
+    v[2] = m * (vz * vx);
+    v[3] = m * (vy * vy);
+    v[4] = m * (vz * vy);
+    v[5] = m * (vz * vz);
+  }
+  if (i == 0 && advance_step) istate[IS_ISTEP] += 1;
+  if (level == 1) {
+    const int slots[6] = {ACC_P2MT + 0, ACC_P2MT + 1, ACC_P2MT + 2, ACC_P2MT + 4, ACC_P2MT + 5, ACC_P2MT + 8};
+    block_acc<6>(v, acc, slots);
+  }
+}
+
+// ------------------------------------------------------------------ host
+static StepP step_params(Ctx *c) {
+  StepP P;
+  P.n = c->n;
+  P.ngroups = c->ngroups;
+  P.ninrra = c->nres_tors;
+  P.ninnra = c->nres_intra;
+  // md_step.c:73-78
+  double dtl2 = .5 * c->dt;
+  P.dts2 = dtl2 / (double)c->nres_lrf;
+  P.dtr2 = P.dts2 / (double)c->nres_tors;
+  P.dta2 = P.dtr2 / (double)c->nres_intra;
+  P.dter = (double)c->nres_lrf * P.dts2;
+  P.dter1 = (double)(1 - c->nres_lrf) * P.dts2;
+  P.skin2q = .25 * c->skin * c->skin;
+  P.kappa = c->kappa;
+  P.kappa2 = c->kappa2;
+  P.use_fxs = c->nres_lrf > 1 || c->need_short;
+  return P;
+}
+
+struct UF {
+  std::vector<int> p;
+  explicit UF(int n) : p(n) { std::iota(p.begin(), p.end(), 0); }
+  int f(int x) {
+    while (p[x] != x) x = p[x] = p[p[x]];
+    return x;
+  }
+  void u(int a, int b) {
+    a = f(a);
+    b = f(b);
+    if (a != b) p[a < b ? b : a] = a < b ? a : b;
+  }
+};
+
+int step_setup(Ctx *c, const cm3d_nb_system *s) {
+  const int n = c->n;
+  UF uf(n);
+  for (int b = 0; b < s->nbonds; b++) uf.u(s->ibond[b], s->jbond[b]);
+  for (int b = 0; b < s->nbends; b++) {
+    uf.u(s->ibend[b], s->jbend[b]);
+    uf.u(s->jbend[b], s->kbend[b]);
+  }
+  for (int b = 0; b < s->necorr; b++) uf.u(s->iecorr[b], s->jecorr[b]);
+  // groups numbered by their lowest atom
+  std::vector<int> gid(n, -1), root_gid(n, -1);
+  int ng = 0;
+  for (int i = 0; i < n; i++) {
+    int r = uf.f(i);
+    if (root_gid[r] < 0) root_gid[r] = ng++;
+    gid[i] = root_gid[r];
+  }
+  c->ngroups = ng;
+  std::vector<int> aoff(ng + 1, 0), atoms(n);
+  for (int i = 0; i < n; i++) aoff[gid[i] + 1]++;
+  for (int g = 0; g < ng; g++) aoff[g + 1] += aoff[g];
+  {
+    std::vector<int> cur(aoff.begin(), aoff.end() - 1);
+    for (int i = 0; i < n; i++) atoms[cur[gid[i]]++] = i;
+  }
+  // bonds / bends / ecorr pairs grouped, CM3D's order kept inside a group
+  std::vector<int> boff(ng + 1, 0), eoff(ng + 1, 0), coff(ng + 1, 0);
+  for (int b = 0; b < s->nbonds; b++) boff[gid[s->ibond[b]] + 1]++;
+  for (int b = 0; b < s->nbends; b++) eoff[gid[s->jbend[b]] + 1]++;
+  for (int b = 0; b < s->necorr; b++) coff[gid[s->iecorr[b]] + 1]++;
+  for (int g = 0; g < ng; g++) {
+    boff[g + 1] += boff[g];
+    eoff[g + 1] += eoff[g];
+    coff[g + 1] += coff[g];
+  }
+  std::vector<int4> bij(s->nbonds > 0 ? s->nbonds : 1), eijk(s->nbends > 0 ? s->nbends : 1);
+  std::vector<double2> bp(bij.size()), ep(eijk.size());
+  std::vector<int2> cij(s->necorr > 0 ? s->necorr : 1), cpair(cij.size());
+  {
+    std::vector<int> cb(boff.begin(), boff.end() - 1), ce(eoff.begin(), eoff.end() - 1),
+        cc(coff.begin(), coff.end() - 1);
+    for (int b = 0; b < s->nbonds; b++) {
+      int t = s->idxbond[b];
+      if (s->itypbond[t] != 0) {
+        set_error("bond %d: only harmonic bonds are supported (itypbond %d)", b, s->itypbond[t]);
+        return CM3D_NB_ERR_ARG;
+      }
+      int slot = cb[gid[s->ibond[b]]]++;
+      bij[slot] = make_int4(s->ibond[b], s->jbond[b], 0, 0);
+      bp[slot] = make_double2(s->eqbond[t], s->fkbond[t]);
+    }
+    for (int b = 0; b < s->nbends; b++) {
+      int t = s->idxbend[b];
+      if (s->itypbend[t] != 0) {
+        set_error("bend %d: only harmonic bends are supported (itypbend %d)", b, s->itypbend[t]);
+        return CM3D_NB_ERR_ARG;
+      }
+      int slot = ce[gid[s->jbend[b]]]++;
+      eijk[slot] = make_int4(s->ibend[b], s->jbend[b], s->kbend[b], 0);
+      ep[slot] = make_double2(s->eqbend[t], s->fkbend[t]);
+    }
+    for (int b = 0; b < s->necorr; b++) {
+      int slot = cc[gid[s->iecorr[b]]]++;
+      cij[slot] = make_int2(s->iecorr[b], s->jecorr[b]);
+      cpair[b] = make_int2(s->iecorr[b], s->jecorr[b]);
+    }
+  }
+  CK(cudaMalloc(&c->grp_atom_off, sizeof(int) * (ng + 1)));
+  CK(cudaMalloc(&c->grp_atoms, sizeof(int) * (size_t)n));
+  CK(cudaMalloc(&c->grp_bond_off, sizeof(int) * (ng + 1)));
+  CK(cudaMalloc(&c->grp_bend_off, sizeof(int) * (ng + 1)));
+  CK(cudaMalloc(&c->grp_ecorr_off, sizeof(int) * (ng + 1)));
+  CK(cudaMalloc(&c->bond_ij, sizeof(int4) * bij.size()));
+  CK(cudaMalloc(&c->bond_p, sizeof(double2) * bp.size()));
+  CK(cudaMalloc(&c->bend_ijk, sizeof(int4) * eijk.size()));
+  CK(cudaMalloc(&c->bend_p, sizeof(double2) * ep.size()));
+  CK(cudaMalloc(&c->ecorr_ij, sizeof(int2) * cij.size()));
+  CK(cudaMalloc(&c->ecorr_pairs, sizeof(int2) * cpair.size()));
+  CK(cudaMemcpy(c->grp_atom_off, aoff.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->grp_atoms, atoms.data(), sizeof(int) * (size_t)n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->grp_bond_off, boff.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->grp_bend_off, eoff.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->grp_ecorr_off, coff.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->bond_ij, bij.data(), sizeof(int4) * bij.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->bond_p, bp.data(), sizeof(double2) * bp.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->bend_ijk, eijk.data(), sizeof(int4) * eijk.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->bend_p, ep.data(), sizeof(double2) * ep.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->ecorr_ij, cij.data(), sizeof(int2) * cij.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->ecorr_pairs, cpair.data(), sizeof(int2) * cpair.size(), cudaMemcpyHostToDevice));
+  return CM3D_NB_OK;
+}
+
+static const int SLOTS_NONBONDED[] = {ACC_SPOTL, ACC_SPOTE, ACC_VK, ACC_POT_ECORR};
+
+int run_bonded(Ctx *c) {
+  StepP P = step_params(c);
+  const int B = 128;
+  k_bonded<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, c->grp_atom_off, c->grp_atoms, c->pos, c->mass, c->fxa,
+                                                     c->grp_bond_off, c->bond_ij, c->bond_p, c->grp_bend_off,
+                                                     c->bend_ijk, c->bend_p);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int group_init(Ctx *c, bool zero_fxs) {
+  StepP P = step_params(c);
+  const int B = 128;
+  cudaEvent_t e0;
+  tbegin(c, 3, &e0);
+  k_group_init<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, zero_fxs ? 1 : 0, c->grp_atom_off, c->grp_atoms,
+                                                         c->pos, c->q, c->fxl, c->fxs, c->grp_ecorr_off,
+                                                         c->ecorr_ij, c->grp_bond_off, c->bond_ij, c->bond_p,
+                                                         c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc);
+  tend(c, 3, e0);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int finish_level1(Ctx *c, double dter, double dter1, bool kick) {
+  const int B = 256;
+  bool rs = c->need_short || c->nres_lrf > 1;
+  k_finish<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, 1, kick ? 1 : 0, 1, rs ? 1 : 0, dter, dter1, c->mass, c->fxl,
+                                               c->fxs, c->vel, c->acc, c->istate, kick ? 1 : 0);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int check_displacement(Ctx *c) {
+  CK(cudaMemsetAsync(c->istate + IS_REBUILD, 0, sizeof(int), c->st));
+  k_disp<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, .25 * c->skin * c->skin, c->pos, c->dxn, c->istate);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int reset_positions(Ctx *c) {
+  k_resetpos<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, .25 * c->skin * c->skin, c->pos, c->dxn, c->istate,
+                                                      c->stat);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+// zero the accumulators force(1) owns (everything but nothing persistent)
+static int zero_acc(Ctx *c) {
+  CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * ACC_COUNT, c->st));
+  return CM3D_NB_OK;
+}
+
+// force(iflg) of md_fcntr.c:44-134 (levels 0, 1, 2)
+int run_force(Ctx *c, int iflg) {
+  int rc;
+  if (iflg == 2) return run_bonded(c);
+  if (!c->lists_built) {
+    set_error("force(%d) before get_ngbr(): the pair lists do not exist yet", iflg);
+    return CM3D_NB_ERR_STATE;
+  }
+  if (iflg == 1) {
+    if ((rc = zero_acc(c))) return rc;
+    if ((rc = group_init(c, true))) return rc;
+    if ((rc = pair_forces(c, 1, 3))) return rc;
+    if ((rc = kspace_forces(c))) return rc;
+    return finish_level1(c, 0, 0, false);
+  }
+  if (iflg == 0) {
+    CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+    if ((rc = pair_forces(c, 0, 3))) return rc;
+    k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, 0, 0, 1, 0, 0, c->mass, c->fxl, c->fxs, c->vel,
+                                                     c->acc, c->istate, 0);
+    c->launches++;
+    CKL(c);
+    return CM3D_NB_OK;
+  }
+  set_error("force(): unknown level %d", iflg);
+  return CM3D_NB_ERR_ARG;
+}
+
+// one outer step; with `gated` the rebuild kernels are gated on the device
+// flag (graph capture), otherwise the host reads the flag and rebuilds
+static int one_step(Ctx *c, bool gated) {
+  int rc;
+  StepP P = step_params(c);
+  const int B = 128;
+  const int ninter = c->nres_lrf;
+  for (int intr = 0; intr < ninter; intr++) {
+    CK(cudaMemsetAsync(c->istate + IS_REBUILD, 0, sizeof(int), c->st));
+    cudaEvent_t e0;
+    tbegin(c, 3, &e0);
+    k_inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
+                                                      c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
+                                                      c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
+                                                      c->bend_p, c->istate);
+    tend(c, 3, e0);
+    c->launches++;
+    CKL(c);
+    if ((rc = reset_positions(c))) return rc;
+    if (gated) {
+      if ((rc = build_lists(c, true))) return rc;
+    } else {
+      CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      if (c->h_istate[IS_REBUILD]) {
+        if ((rc = build_lists(c, false))) return rc;
+      }
+    }
+    if (intr == ninter - 1) {
+      if ((rc = zero_acc(c))) return rc;
+      if ((rc = group_init(c, P.use_fxs))) return rc;
+      if ((rc = pair_forces(c, 1, 3))) return rc;
+      if ((rc = kspace_forces(c))) return rc;
+      if ((rc = finish_level1(c, P.dter, P.dter1, true))) return rc;
+    } else {
+      CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+      if ((rc = pair_forces(c, 0, 3))) return rc;
+      k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, 1, 0, 1, 0, P.dts2, c->mass, c->fxl, c->fxs,
+                                                       c->vel, c->acc, c->istate, 0);
+      c->launches++;
+      CKL(c);
+    }
+  }
+  return CM3D_NB_OK;
+}
+
+static int snapshot(Ctx *c, bool restore) {
+  const size_t n3 = 3 * (size_t)c->n;
+  double *bufs[6] = {c->pos, c->vel, c->fxl, c->fxs, c->fxa, c->dxn};
+  for (int k = 0; k < 6; k++) {
+    if (restore) CK(cudaMemcpyAsync(bufs[k], c->snap + k * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+    else CK(cudaMemcpyAsync(c->snap + k * n3, bufs[k], sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
+  }
+  int *is = reinterpret_cast<int *>(c->snap + 6 * n3);
+  if (restore) CK(cudaMemcpyAsync(c->istate, is, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToDevice, c->st));
+  else CK(cudaMemcpyAsync(is, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToDevice, c->st));
+  return CM3D_NB_OK;
+}
+
+int run_step(Ctx *c, int istep0, int nsteps) {
+  int rc;
+  if (!c->lists_built || !c->forces_valid) {
+    set_error("step() before step_init(): forces and lists are not set up");
+    return CM3D_NB_ERR_STATE;
+  }
+  if (nsteps <= 0) return CM3D_NB_OK;
+  c->h_istate[IS_ISTEP] = istep0;
+  CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  if (!c->use_graph || c->timing.on) {
+    for (int s = 0; s < nsteps; s++)
+      if ((rc = one_step(c, false))) return rc;
+    return CM3D_NB_OK;
+  }
+  // graph replay: one captured step, the rebuild gated on the device flag
+  if (!c->graph) {
+    cudaGraph_t g;
+    long long l0 = c->launches;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    rc = one_step(c, true);
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    CK(cudaGraphInstantiate(&c->graph, g, 0));
+    cudaGraphDestroy(g);
+    c->graph_launches = c->launches - l0;
+    c->launches = l0;
+  }
+  CK(cudaMemsetAsync(c->stat + ST_OVERFLOW, 0, sizeof(long long), c->st));
+  if ((rc = snapshot(c, false))) return rc;
+  for (int s = 0; s < nsteps; s++) {
+    CK(cudaGraphLaunch(c->graph, c->st));
+    c->launches += c->graph_launches;
+  }
+  long long ovf = 0;
+  CK(cudaMemcpyAsync(&c->h_stat[ST_OVERFLOW], c->stat + ST_OVERFLOW, sizeof(long long), cudaMemcpyDeviceToHost,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  ovf = c->h_stat[ST_OVERFLOW];
+  if (ovf) {
+    // a rebuild inside the graph outgrew a list: rewind and redo these steps
+    // with host-driven rebuilds (which grow the buffers), then re-capture
+    c->overflows_host++;
+    if ((rc = snapshot(c, true))) return rc;
+    CK(cudaMemsetAsync(c->stat + ST_OVERFLOW, 0, sizeof(long long), c->st));
+    c->h_istate[IS_ISTEP] = istep0;
+    CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
+    // rebuild at the restored positions (this grows the buffers); keep the
+    // restored isteplast so RESETPOS sees CM3D's step history
+    if ((rc = build_lists(c, false))) return rc;
+    CK(cudaMemcpyAsync(c->istate + IS_ISTEPLAST, reinterpret_cast<int *>(c->snap + 18 * (size_t)c->n) + IS_ISTEPLAST,
+                       sizeof(int), cudaMemcpyDeviceToDevice, c->st));
+    for (int s = 0; s < nsteps; s++)
+      if ((rc = one_step(c, false))) return rc;
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return CM3D_NB_OK;
+}
+
+}  // namespace cm3d

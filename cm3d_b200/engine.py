@@ -1,0 +1,311 @@
+"""Python host mirror of CM3D's nonbonded entry points over the C ABI.
+
+`Engine` wraps one device-resident system (libcm3d_nb.so, include/cm3d_nb.h)
+and exposes CM3D's routines under CM3D's names:
+
+    get_ngbr()            energy/control/ngbr_list.c:297
+    nrefsh(istep)         energy/control/md_finter.c:43
+    force(iflg)           energy/control/md_fcntr.c:44   (levels 0, 1, 2)
+    force_ter(iflg)       energy/control/md_finter.c:110
+    force_ter_e(iflg)     energy/control/md_finter_e.c:78
+    fk_ewald()            energy/inter/md_ewald.c:185
+    ecorr()               energy/inter/md_ewald.c:385
+    getsvirter()          energy/inter/md_fnopol.c:386
+    getsvirter_e()        energy/inter/finter_e.c:410
+    getvewald()           energy/inter/md_ewald.c:364
+    step_init(), step()   integrate/md_step.c:32, 62
+
+Errors surface as `EngineError` carrying the library's message, where CM3D
+would have called md_error().  There is no CPU fallback: without the built
+library or a CUDA device the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from .system import System
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcm3d_nb.so")
+
+_lib = None
+
+
+class EngineError(RuntimeError):
+    pass
+
+
+def load_library() -> C.CDLL:
+    """Load the in-tree engine library (build it first with
+    `python -m cm3d_b200.build`); raises when it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise EngineError(f"{LIB_PATH} is missing: run `python -m cm3d_b200.build` "
+                          "(the engine has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, dp, ip = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int)
+    ll = C.c_longlong
+    sig = {
+        "cm3d_nb_version": (C.c_int, []),
+        "cm3d_nb_last_error": (C.c_char_p, []),
+        "cm3d_nb_device_count": (C.c_int, [ip]),
+        "cm3d_nb_default_options": (None, [C.POINTER(_abi.Options)]),
+        "cm3d_nb_create": (C.c_int, [C.POINTER(_abi.SystemDesc), C.POINTER(_abi.Options), C.POINTER(vp)]),
+        "cm3d_nb_destroy": (None, [vp]),
+        "cm3d_nb_set_positions": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_get_positions": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_set_velocities": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_get_velocities": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_get_forces": (C.c_int, [vp, C.c_int, dp, dp, dp]),
+        "cm3d_nb_set_forces": (C.c_int, [vp, C.c_int, dp, dp, dp]),
+        "cm3d_nb_get_ngbr": (C.c_int, [vp]),
+        "cm3d_nb_nrefsh": (C.c_int, [vp, C.c_int, ip]),
+        "cm3d_nb_force": (C.c_int, [vp, C.c_int]),
+        "cm3d_nb_force_ter": (C.c_int, [vp, C.c_int]),
+        "cm3d_nb_force_ter_e": (C.c_int, [vp, C.c_int]),
+        "cm3d_nb_fk_ewald": (C.c_int, [vp]),
+        "cm3d_nb_ecorr": (C.c_int, [vp]),
+        "cm3d_nb_zero_forces": (C.c_int, [vp, C.c_int]),
+        "cm3d_nb_rmass": (C.c_int, [vp, C.c_int]),
+        "cm3d_nb_getsvirter": (C.c_int, [vp, dp, dp, dp, dp]),
+        "cm3d_nb_getsvirter_e": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_getvewald": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_step_init": (C.c_int, [vp]),
+        "cm3d_nb_step": (C.c_int, [vp, C.c_int, C.c_int]),
+        "cm3d_nb_get_energies": (C.c_int, [vp, C.POINTER(_abi.Energies)]),
+        "cm3d_nb_list_count": (C.c_int, [vp, C.c_int, C.POINTER(ll)]),
+        "cm3d_nb_get_list": (C.c_int, [vp, C.c_int, ip, ip, ll, C.POINTER(ll)]),
+        "cm3d_nb_get_status": (C.c_int, [vp, C.POINTER(_abi.Status)]),
+        "cm3d_nb_synchronize": (C.c_int, [vp]),
+        "cm3d_nb_stream": (vp, [vp]),
+        "cm3d_nb_enable_timing": (C.c_int, [vp, C.c_int]),
+        "cm3d_nb_kernel_time": (C.c_int, [vp, C.c_int, dp, C.POINTER(ll)]),
+        "cm3d_nb_launch_count": (ll, [vp]),
+        "cm3d_nb_lj_table": (C.c_int, [C.c_double] * 7 + [C.c_int, C.c_int, dp, dp, dp, dp]),
+        "cm3d_nb_coul_table": (C.c_int, [C.c_double] * 6 + [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]),
+        "cm3d_nb_ewald_kvectors": (C.c_int, [C.c_int, ip, ip, ip, ip, ip]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def last_error() -> str:
+    return load_library().cm3d_nb_last_error().decode(errors="replace")
+
+
+def check(rc: int, what: str) -> None:
+    if rc != _abi.OK:
+        raise EngineError(f"{what}: {last_error()} (code {rc})")
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    load_library().cm3d_nb_device_count(C.byref(n))
+    return int(n.value)
+
+
+def _p(a: np.ndarray, t=C.c_double):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class Engine:
+    """One CM3D system resident on one GPU."""
+
+    def __init__(self, system: System, mode: int = _abi.MIXED, device: int = 0,
+                 need_short: bool = False, tpa: int = 0, use_graph: bool = True):
+        L = load_library()
+        self.sys = system
+        self.n = system.natoms
+        self.mode = mode
+        opt = _abi.Options(device=device, mode=mode, need_short=int(need_short), tpa=tpa,
+                           use_graph=int(use_graph))
+        h = C.c_void_p()
+        check(L.cm3d_nb_create(C.byref(system.desc()), C.byref(opt), C.byref(h)), "cm3d_nb_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load_library().cm3d_nb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --------------------------------------------------------- transfers
+    def _get3(self, fn, *lead) -> np.ndarray:
+        x, y, z = (np.empty(self.n) for _ in range(3))
+        check(fn(self._h, *lead, _p(x), _p(y), _p(z)), fn.__name__)
+        return np.stack([x, y, z])
+
+    def _set3(self, fn, a, *lead) -> None:
+        a = np.asarray(a, dtype=np.float64)
+        x, y, z = (np.ascontiguousarray(a[k]) for k in range(3))
+        check(fn(self._h, *lead, _p(x), _p(y), _p(z)), fn.__name__)
+
+    def positions(self) -> np.ndarray:
+        return self._get3(load_library().cm3d_nb_get_positions)
+
+    def set_positions(self, p) -> None:
+        self._set3(load_library().cm3d_nb_set_positions, p)
+
+    def velocities(self) -> np.ndarray:
+        return self._get3(load_library().cm3d_nb_get_velocities)
+
+    def set_velocities(self, v) -> None:
+        self._set3(load_library().cm3d_nb_set_velocities, v)
+
+    def forces(self, which: int = _abi.FXL) -> np.ndarray:
+        """The stored force block (accelerations after rmass, raw forces after
+        force_ter/force_ter_e/fk_ewald/ecorr alone)."""
+        return self._get3(load_library().cm3d_nb_get_forces, which)
+
+    def set_forces(self, f, which: int = _abi.FXL) -> None:
+        L = load_library()
+        a = np.asarray(f, dtype=np.float64)
+        x, y, z = (np.ascontiguousarray(a[k]) for k in range(3))
+        check(L.cm3d_nb_set_forces(self._h, which, _p(x), _p(y), _p(z)), "set_forces")
+
+    # ---------------------------------------------------- CM3D routines
+    def get_ngbr(self) -> None:
+        check(load_library().cm3d_nb_get_ngbr(self._h), "get_ngbr")
+
+    def nrefsh(self, istep: int) -> bool:
+        r = C.c_int(0)
+        check(load_library().cm3d_nb_nrefsh(self._h, istep, C.byref(r)), "nrefsh")
+        return bool(r.value)
+
+    def force(self, iflg: int) -> None:
+        check(load_library().cm3d_nb_force(self._h, iflg), f"force({iflg})")
+
+    def force_ter(self, iflg: int) -> None:
+        check(load_library().cm3d_nb_force_ter(self._h, iflg), f"force_ter({iflg})")
+
+    def force_ter_e(self, iflg: int) -> None:
+        check(load_library().cm3d_nb_force_ter_e(self._h, iflg), f"force_ter_e({iflg})")
+
+    def fk_ewald(self) -> None:
+        check(load_library().cm3d_nb_fk_ewald(self._h), "fk_ewald")
+
+    def ecorr(self) -> None:
+        check(load_library().cm3d_nb_ecorr(self._h), "ecorr")
+
+    def zero_forces(self, which: int) -> None:
+        check(load_library().cm3d_nb_zero_forces(self._h, which), "zero_forces")
+
+    def rmass(self, which: int) -> None:
+        check(load_library().cm3d_nb_rmass(self._h, which), "rmass")
+
+    def getsvirter(self) -> dict:
+        vh, v, w = C.c_double(0), C.c_double(0), C.c_double(0)
+        t = np.zeros(9)
+        check(load_library().cm3d_nb_getsvirter(self._h, C.byref(vh), C.byref(v), C.byref(w), _p(t)),
+              "getsvirter")
+        return {"vhinter": vh.value, "vinter": v.value, "winter": w.value, "wintertensor": t}
+
+    def getsvirter_e(self) -> dict:
+        v, w = C.c_double(0), C.c_double(0)
+        t = np.zeros(9)
+        check(load_library().cm3d_nb_getsvirter_e(self._h, C.byref(v), C.byref(w), _p(t)), "getsvirter_e")
+        return {"velec": v.value, "welec": w.value, "welectensor": t}
+
+    def getvewald(self) -> dict:
+        p, w = C.c_double(0), C.c_double(0)
+        t = np.zeros(9)
+        check(load_library().cm3d_nb_getvewald(self._h, C.byref(p), C.byref(w), _p(t)), "getvewald")
+        return {"vewald": p.value, "wewald": w.value, "wewaldtensor": t}
+
+    def step_init(self) -> None:
+        check(load_library().cm3d_nb_step_init(self._h), "step_init")
+
+    def step(self, istep0: int, nsteps: int = 1) -> None:
+        check(load_library().cm3d_nb_step(self._h, istep0, nsteps), "step")
+
+    def energies(self) -> dict:
+        e = _abi.Energies()
+        check(load_library().cm3d_nb_get_energies(self._h, C.byref(e)), "get_energies")
+        return e.as_dict()
+
+    def pair_list(self, which: int) -> tuple[np.ndarray, np.ndarray]:
+        L = load_library()
+        n = C.c_longlong(0)
+        check(L.cm3d_nb_list_count(self._h, which, C.byref(n)), "list_count")
+        i = np.empty(max(n.value, 1), np.int32)
+        j = np.empty(max(n.value, 1), np.int32)
+        got = C.c_longlong(0)
+        check(L.cm3d_nb_get_list(self._h, which, _p(i, C.c_int), _p(j, C.c_int), n.value, C.byref(got)),
+              "get_list")
+        return i[:got.value], j[:got.value]
+
+    def status(self) -> dict:
+        s = _abi.Status()
+        check(load_library().cm3d_nb_get_status(self._h, C.byref(s)), "get_status")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def synchronize(self) -> None:
+        check(load_library().cm3d_nb_synchronize(self._h), "synchronize")
+
+    def enable_timing(self, on: bool = True) -> None:
+        check(load_library().cm3d_nb_enable_timing(self._h, int(on)), "enable_timing")
+
+    def kernel_time(self, cls: int) -> tuple[float, int]:
+        ms, n = C.c_double(0), C.c_longlong(0)
+        check(load_library().cm3d_nb_kernel_time(self._h, cls, C.byref(ms), C.byref(n)), "kernel_time")
+        return ms.value, n.value
+
+    def launch_count(self) -> int:
+        return int(load_library().cm3d_nb_launch_count(self._h))
+
+    def stream(self) -> int:
+        return int(load_library().cm3d_nb_stream(self._h) or 0)
+
+
+# ----------------------------------------------------- host set-up helpers
+def lj_table(eps, sig, rmin, rmax, rres, rheal, skin, ntable, shift):
+    """get_ter_parm's LJ table (input/md_getparm.c:236-366) via the C ABI."""
+    L = load_library()
+    v, dv, sw = np.empty(ntable), np.empty(ntable), np.empty(ntable)
+    dx2 = C.c_double(0)
+    check(L.cm3d_nb_lj_table(eps, sig, rmin, rmax, rres, rheal, skin, ntable, int(shift), _p(v), _p(dv),
+                             _p(sw), C.byref(dx2)), "lj_table")
+    return v, dv, sw, dx2.value
+
+
+def coul_table(alpha, rmin, rresp, rmax, rheal, skin, ntable, iperd=3, shift=0):
+    """set_charges' erfc table (energy/control/elec_ngbr.c:51-103) via the C ABI."""
+    L = load_library()
+    c, dc, sw = np.empty(ntable), np.empty(ntable), np.empty(ntable)
+    dx2 = C.c_double(0)
+    check(L.cm3d_nb_coul_table(alpha, rmin, rresp, rmax, rheal, skin, ntable, iperd, int(shift), _p(c),
+                               _p(dc), _p(sw), C.byref(dx2)), "coul_table")
+    return c, dc, sw, dx2.value
+
+
+def ewald_kvectors(kmax: int):
+    """ewald_setup's half-space spherical k set (energy/inter/md_ewald.c:93-114)."""
+    L = load_library()
+    n = C.c_int(0)
+    null = C.POINTER(C.c_int)()
+    check(L.cm3d_nb_ewald_kvectors(kmax, null, null, null, null, C.byref(n)), "ewald_kvectors")
+    ka, kb, kc, kup = (np.empty(n.value + 1, np.int32) for _ in range(4))
+    check(L.cm3d_nb_ewald_kvectors(kmax, _p(ka, C.c_int), _p(kb, C.c_int), _p(kc, C.c_int),
+                                   _p(kup, C.c_int), C.byref(n)), "ewald_kvectors")
+    return ka[:n.value], kb[:n.value], kc[:n.value], kup[:n.value + 1]

@@ -1,0 +1,179 @@
+"""GPU engine against CM3D (golden fixtures dumped from the reference) and the
+CPU oracle.  Every call goes through the C ABI (libcm3d_nb.so) via Engine.
+
+Tolerances
+  pair lists          bit-exact (sorted (min, max) pairs hashed), both modes
+  plain FP64 engine   relative RMS force error <= 1e-11 (only the summation
+                      order differs from CM3D), energies relative <= 1e-10
+  mixed engine        relative RMS force error <= 1e-5 against CM3D's FP64
+                      energies relative <= 1e-5
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import golden, rel_rms, xyz
+from cm3d_b200 import _abi
+from cm3d_b200.engine import Engine, EngineError
+from cm3d_b200.system import System
+from tests.golden.make_golden import pair_key
+
+pytestmark = pytest.mark.gpu
+
+MODES = [_abi.PLAIN_FP64, _abi.MIXED]
+MODE_ID = {_abi.PLAIN_FP64: "plain", _abi.MIXED: "mixed"}
+FTOL = {_abi.PLAIN_FP64: 1e-11, _abi.MIXED: 1e-5}
+ETOL = {_abi.PLAIN_FP64: 1e-10, _abi.MIXED: 1e-5}
+ALL = ["lj2", "lj256", "abutane", "argon864", "water216", "binary256", "water4096"]
+DYN = ["lj2", "lj256", "argon864", "water216", "binary256", "water4096"]   # no frozen atoms / torsions
+
+
+def engine(name, mode, **kw):
+    d = golden(name)
+    return d, Engine(System.from_arrays(d), mode=mode, **kw)
+
+
+def close(a, b, tol):
+    return abs(a - b) <= tol * max(abs(b), 1e-300) or abs(a - b) <= 1e-9
+
+
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+@pytest.mark.parametrize("name", ALL)
+def test_pair_lists_bit_exact(engine_lib, name, mode):
+    d, e = engine(name, mode)
+    e.get_ngbr()
+    n = int(d["natoms"][0])
+    for tag, w in (("t", _abi.LIST_T), ("s", _abi.LIST_S), ("te", _abi.LIST_TE), ("se", _abi.LIST_SE)):
+        i, j = e.pair_list(w)
+        assert len(i) == int(d[f"npr{tag}"][0]), tag
+        if len(i):
+            h = hashlib.sha256(pair_key(i, j, n).tobytes()).hexdigest()
+            assert h == str(d[f"list_{tag}_hash"]), tag
+    e.close()
+
+
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+@pytest.mark.parametrize("name", ALL)
+def test_force_terms(engine_lib, name, mode):
+    d, e = engine(name, mode, need_short=True)
+    e.get_ngbr()
+    tol = FTOL[mode]
+    # LJ: force_ter(1) adds the full force to fxl and the switched part to fxs
+    e.zero_forces(_abi.FXL)
+    e.zero_forces(_abi.FXS)
+    e.force_ter(1)
+    assert rel_rms(e.forces(_abi.FXL), xyz(d, "f_lj_l")) <= tol
+    assert rel_rms(e.forces(_abi.FXS), xyz(d, "f_lj_s")) <= tol
+    v = e.getsvirter()
+    assert close(v["vinter"], d["lj_vinter"][0], ETOL[mode])
+    assert close(v["vhinter"], d["lj_vhinter"][0], ETOL[mode])
+    assert close(v["winter"], d["lj_winter"][0], ETOL[mode])
+    # real-space Ewald: force_ter_e(1)
+    e.zero_forces(_abi.FXL)
+    e.zero_forces(_abi.FXS)
+    e.force_ter_e(1)
+    assert rel_rms(e.forces(_abi.FXL), xyz(d, "f_el_l")) <= tol
+    assert rel_rms(e.forces(_abi.FXS), xyz(d, "f_el_s")) <= tol
+    v = e.getsvirter_e()
+    assert close(v["velec"], d["el_velec"][0], ETOL[mode])
+    assert close(v["welec"], d["el_welec"][0], ETOL[mode])
+    if int(d["ncharge"][0]) > 0:
+        e.zero_forces(_abi.FXL)
+        e.fk_ewald()
+        assert rel_rms(e.forces(_abi.FXL), xyz(d, "f_k")) <= tol
+        e.zero_forces(_abi.FXL)
+        e.ecorr()
+        assert rel_rms(e.forces(_abi.FXL), xyz(d, "f_ecorr")) <= FTOL[_abi.PLAIN_FP64]
+    e.close()
+
+
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+@pytest.mark.parametrize("name", ALL)
+def test_short_level(engine_lib, name, mode):
+    """force_ter(...,0) over the s list with the RESPA switch, force_ter_e(...,0)
+    over the se list with CM3D's fall-through (no switch, full cutoff)"""
+    d, e = engine(name, mode)
+    e.get_ngbr()
+    for key, fn in (("f_lj_short", e.force_ter), ("f_el_short", e.force_ter_e)):
+        e.zero_forces(_abi.FXS)
+        fn(0)
+        assert rel_rms(e.forces(_abi.FXS), xyz(d, key)) <= FTOL[mode], key
+    e.close()
+
+
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+@pytest.mark.parametrize("name", DYN)
+def test_level1_forces_and_energies(engine_lib, name, mode):
+    d, e = engine(name, mode)
+    e.get_ngbr()
+    e.force(1)
+    assert rel_rms(e.forces(_abi.FXL), xyz(d, "acc_l")) <= FTOL[mode]
+    e.force(2)
+    en = e.energies()
+    for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke"):
+        assert close(en[k], float(d[f"e0_{k}"][0]), ETOL[mode]), k
+    e.close()
+
+
+@pytest.mark.parametrize("name", DYN)
+def test_bonded_level(engine_lib, name):
+    d, e = engine(name, _abi.MIXED)
+    e.force(2)
+    m = d["amass"]
+    want = (xyz(d, "f_bond") + xyz(d, "f_bend")) / m
+    assert rel_rms(e.forces(_abi.FXA), want) <= 1e-12
+    e.close()
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+@pytest.mark.parametrize("name", DYN)
+def test_trajectory(engine_lib, name, mode, graph):
+    """CM3D's step() for the dumped number of steps: per-step energies,
+    final positions and the rebuild count against the reference"""
+    d, e = engine(name, mode, use_graph=graph)
+    e.step_init()
+    eng = d["traj_eng"].reshape(-1, 8)
+    ns = int(d["nsteps"][0])
+    # plain FP64 tracks CM3D to round-off; mixed within its force tolerance,
+    # which a chaotic trajectory amplifies over the steps
+    ptol = 1e-9 if mode == _abi.PLAIN_FP64 else 2e-4
+    for k in range(ns):
+        e.step(1 + k, 1)
+        en = e.energies()
+        for c, key in enumerate(("poter", "potra", "zke")):
+            assert close(en[key], eng[k, c], ptol if c != 1 else 10 * ptol), (k, key)
+    pos = e.positions()
+    ref = np.stack([d["final_px"], d["final_py"], d["final_pz"]])
+    assert np.abs(pos - ref).max() <= (1e-9 if mode == _abi.PLAIN_FP64 else 1e-3)
+    st = e.status()
+    if mode == _abi.PLAIN_FP64:
+        assert st["rebuilds"] - 1 == int(eng[-1, 7])
+    e.close()
+
+
+def test_errors_are_reported(engine_lib):
+    d = golden("lj256")
+    e = Engine(System.from_arrays(d), mode=_abi.MIXED)
+    with pytest.raises(EngineError, match="get_ngbr"):
+        e.force(1)
+    with pytest.raises(EngineError):
+        e.force_ter(7)
+    e.close()
+    bad = System.from_arrays(d)
+    bad["iperd"] = 2
+    with pytest.raises(EngineError, match="iperd"):
+        Engine(bad)
+
+
+def test_status_counts_resets(engine_lib):
+    """water216 starts hot: CM3D's RESETPOS fires (reference log: 12 resets in
+    20 steps); the engine counts the same events in plain FP64"""
+    d, e = engine("water216", _abi.PLAIN_FP64)
+    e.step_init()
+    e.step(1, 20)
+    st = e.status()
+    assert st["resets"] == 12
+    assert st["rebuilds"] == 14      # step_init's build + 13 during the run
+    e.close()
