@@ -29,7 +29,7 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 void tbegin(Ctx *c, int cls, cudaEvent_t *e0) {
   *e0 = nullptr;
-  if (!c->timing.on) return;
+  if (cls == 4 ? !c->timing.steps : !c->timing.on) return;
   cudaEvent_t a, b;
   if (c->timing.pool.size() >= 1) {
     a = c->timing.pool.back().first;
@@ -45,14 +45,14 @@ void tbegin(Ctx *c, int cls, cudaEvent_t *e0) {
 }
 
 void tend(Ctx *c, int cls, cudaEvent_t e0) {
-  if (!c->timing.on || !e0) return;
+  if (!e0) return;
   cudaEventRecord(c->timing.pending[cls].back().second, c->st);
   c->timing.launches[cls]++;
 }
 
 static void collect_timing(Ctx *c) {
   cudaStreamSynchronize(c->st);
-  for (int k = 0; k < 4; k++) {
+  for (int k = 0; k < NTCLS; k++) {
     for (auto &pr : c->timing.pending[k]) {
       float ms = 0;
       cudaEventElapsedTime(&ms, pr.first, pr.second);
@@ -90,7 +90,7 @@ static void destroy(Ctx *c) {
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot};
   for (void *p : hp)
     if (p) cudaFreeHost(p);
-  for (int k = 0; k < 4; k++)
+  for (int k = 0; k < NTCLS; k++)
     for (auto &pr : c->timing.pending[k]) {
       cudaEventDestroy(pr.first);
       cudaEventDestroy(pr.second);
@@ -234,7 +234,6 @@ static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out
   if ((rc = upload<double>(&c->fxs, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->fxa, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->dxn, pos.data(), n3))) return rc;
-  if ((rc = upload<double>(&c->snap, nullptr, 6 * n3 + 8))) return rc;
   if ((rc = upload(&c->mass, s->amass, n))) return rc;
   if ((rc = upload(&c->q, s->qch, n))) return rc;
   if ((rc = upload(&c->itype, s->itype, n))) return rc;
@@ -275,6 +274,50 @@ static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out
   if (s->ntors > 0 || s->n14 > 0 || s->nbondx > 0) c->name = "has-torsions";
   CK(cudaDeviceSynchronize());
   return CM3D_NB_OK;
+}
+
+// FMA throughput probe: 8 independent dependency chains per thread
+template <typename T>
+__global__ void k_fma_peak(T *out, int iters, T a, T b) {
+  T x[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) x[k] = (T)(threadIdx.x + k);
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++) {
+#pragma unroll
+      for (int k = 0; k < 8; k++) x[k] = x[k] * a + b;
+    }
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) s += x[k];
+  if (s == (T)-12345.0) out[0] = s;   // keeps the chains alive
+}
+
+template <typename T>
+static double fma_peak(int blocks) {
+  T *out = nullptr;
+  if (cudaMalloc(&out, sizeof(T)) != cudaSuccess) return 0;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int threads = 256, iters = 4096;
+  double best = 0;
+  for (int rep = 0; rep < 6; rep++) {
+    cudaEventRecord(a);
+    k_fma_peak<T><<<blocks, threads>>>(out, iters, (T)0.999999, (T)1e-7);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    double flops = 2.0 * 8 * 16 * (double)iters * threads * blocks;
+    if (rep > 0 && ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(out);
+  return best;
 }
 
 __global__ void k_scale_rmass(int n, double *__restrict__ f, const double *__restrict__ mass) {
@@ -715,8 +758,9 @@ void *cm3d_nb_stream(cm3d_nb_ctx *ctx) {
 int cm3d_nb_enable_timing(cm3d_nb_ctx *ctx, int enable) {
   CTX;
   collect_timing(c);
-  c->timing.on = enable != 0;
-  for (int k = 0; k < 4; k++) {
+  c->timing.on = (enable & 1) != 0;
+  c->timing.steps = (enable & 2) != 0;
+  for (int k = 0; k < NTCLS; k++) {
     c->timing.ms[k] = 0;
     c->timing.launches[k] = 0;
   }
@@ -725,7 +769,7 @@ int cm3d_nb_enable_timing(cm3d_nb_ctx *ctx, int enable) {
 
 int cm3d_nb_kernel_time(cm3d_nb_ctx *ctx, int cls, double *ms, long long *launches) {
   CTX;
-  if (cls < 0 || cls > 3) {
+  if (cls < 0 || cls >= NTCLS) {
     set_error("kernel_time: unknown class %d", cls);
     return CM3D_NB_ERR_ARG;
   }
@@ -738,6 +782,16 @@ int cm3d_nb_kernel_time(cm3d_nb_ctx *ctx, int cls, double *ms, long long *launch
 long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   return c ? c->launches : 0;
+}
+
+int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops) {
+  CK(cudaSetDevice(device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  if (fp32_tflops) *fp32_tflops = fma_peak<float>(sms * 16);
+  if (fp64_tflops) *fp64_tflops = fma_peak<double>(sms * 16);
+  CKL(nullptr);
+  return CM3D_NB_OK;
 }
 
 // ------------------------------------------------- host set-up restatements

@@ -49,6 +49,7 @@ enum {
   ST_OVERFLOW = 2,        // a list fill ran past its capacity
   ST_RESETS = 3,          // RESETPOS events
   ST_REBUILDS = 4,
+  ST_BADSHIFT = 5,        // a pair's cell shift fell outside the 27-entry table
   ST_COUNT = 8
 };
 // device integer state
@@ -56,8 +57,19 @@ enum {
   IS_ISTEP = 0,           // SIMPARMS.istep of the step being taken
   IS_ISTEPLAST = 1,       // md_finter.c:48 static isteplast
   IS_REBUILD = 2,         // rebuild requested by the displacement check
+  IS_HALT = 3,            // a device-side rebuild outgrew a list: the rest
+                          // of the captured step does nothing, the host
+                          // grows the buffers and finishes the step
+  IS_INTR = 4,            // RESPA level (intr) the step is in
   IS_COUNT = 8
 };
+
+// Gate of kernels that run inside a captured step: with gs == nullptr (host
+// driven) never skip; otherwise skip once the step is halted, and list-build
+// kernels (need_rebuild) also when no rebuild was requested.
+__device__ __forceinline__ bool gated_off(const int *gs, int need_rebuild) {
+  return gs && (gs[IS_HALT] != 0 || (need_rebuild && gs[IS_REBUILD] == 0));
+}
 // list totals (long long) written by the list builder
 enum { LT_T = 0, LT_S = 1, LT_TE = 2, LT_SE = 3, LT_FULL = 4, LT_COUNT = 5 };
 
@@ -71,11 +83,15 @@ constexpr uint32_t ENT_LJS = 1u << 29;      // pair is in CM3D's s list
 constexpr uint32_t ENT_ELS = 1u << 30;      // pair is in CM3D's se list
 constexpr int MAX_ATOMS_MIXED = 1 << ENT_JBITS;
 
+// classes 0 pair, 1 k-space, 2 list build, 3 integrate (per kernel, eager
+// launches only); 4 whole steps (around graph replays too)
+constexpr int NTCLS = 5;
 struct Timing {
-  bool on = false;
-  double ms[4] = {0, 0, 0, 0};
-  long long launches[4] = {0, 0, 0, 0};
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[4];
+  bool on = false;          // per-kernel classes 0-3
+  bool steps = false;       // class 4
+  double ms[NTCLS] = {0, 0, 0, 0, 0};
+  long long launches[NTCLS] = {0, 0, 0, 0, 0};
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending[NTCLS];
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
 };
 
@@ -173,6 +189,7 @@ struct Ctx {
   Timing timing;
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
+  const int *gate = nullptr;            // istate while a step is being captured
   std::string name;
 };
 

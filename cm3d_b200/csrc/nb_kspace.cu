@@ -35,7 +35,8 @@ constexpr int MAX_ROWLEN = 128;    // 2 kmax + 1 <= 128
 // ------------------------------------------------------------ mixed mode
 __global__ void k_kprep(int nq, const int *__restrict__ icharge, int n, const double *__restrict__ pos,
                         const double *__restrict__ q, const double *__restrict__ hmati, uint4 *__restrict__ kfrac,
-                        double4 *__restrict__ kposd) {
+                        double4 *__restrict__ kposd, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   int jq = blockIdx.x * blockDim.x + threadIdx.x;
   if (jq >= nq) return;
   int i = icharge[jq];
@@ -61,7 +62,9 @@ __device__ __forceinline__ float phase_rad(unsigned phi) {
 __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *__restrict__ kfrac, int nrows,
                                                            const int4 *__restrict__ rows,
                                                            const int *__restrict__ row_k0, int rows_per_block,
-                                                           int ktot, double2 *__restrict__ spart) {
+                                                           int ktot, double2 *__restrict__ spart,
+                                                           const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   __shared__ float2 red[KS_THREADS / 32][MAX_ROWLEN];
   const int tile = blockIdx.x;
   const int r0 = blockIdx.y * rows_per_block;
@@ -126,7 +129,8 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
 __global__ void k_sred(int ktot, int ntiles, const double2 *__restrict__ spart, const int *__restrict__ ka,
                        const int *__restrict__ kb, const int *__restrict__ kc, const double *__restrict__ hmati,
                        double rvol, double falp2, double2 *__restrict__ sk, float2 *__restrict__ akf,
-                       double2 *__restrict__ akd, double *__restrict__ acc) {
+                       double2 *__restrict__ akd, double *__restrict__ acc, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   double v[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   const double TPI = 2.0 * M_PI;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ktot; k += gridDim.x * blockDim.x) {
@@ -165,7 +169,9 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
                                                              const int *__restrict__ row_k0, int rows_per_split,
                                                              const float2 *__restrict__ akf, int ktot,
                                                              const double *__restrict__ hmati, int atomic,
-                                                             double *__restrict__ fxl) {
+                                                             double *__restrict__ fxl,
+                                                             const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   extern __shared__ float2 ak_s[];
   const int r0 = blockIdx.y * rows_per_split;
   const int r1 = min(nrows, r0 + rows_per_split);
@@ -252,7 +258,9 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_plain(int nq, const double4
                                                            const int4 *__restrict__ rows,
                                                            const int *__restrict__ row_k0, int rows_per_block,
                                                            int ktot, const double *__restrict__ hmati,
-                                                           double2 *__restrict__ spart) {
+                                                           double2 *__restrict__ spart,
+                                                           const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   __shared__ double2 red[KS_THREADS / 32][MAX_ROWLEN];
   const int tile = blockIdx.x;
   const int r0 = blockIdx.y * rows_per_block;
@@ -296,7 +304,9 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_plain(int nq, const double4
 __global__ void k_kforce_plain(int nq, const double4 *__restrict__ kp, const int *__restrict__ icharge, int n,
                                int nrows, const int4 *__restrict__ rows, const int *__restrict__ row_k0,
                                int rows_per_split, const double2 *__restrict__ akd, int ktot,
-                               const double *__restrict__ hmati, int atomic, double *__restrict__ fxl) {
+                               const double *__restrict__ hmati, int atomic, double *__restrict__ fxl,
+                               const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   const int jq = blockIdx.x * blockDim.x + threadIdx.x;
   const int r0 = blockIdx.y * rows_per_split;
   const int r1 = min(nrows, r0 + rows_per_split);
@@ -418,21 +428,22 @@ int kspace_forces(Ctx *c) {
   tbegin(c, 1, &e0);
   const bool mixed = c->mode == CM3D_NB_MIXED;
   k_kprep<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, dhmati,
-                                                         mixed ? c->kfrac : nullptr, c->kposd);
+                                                         mixed ? c->kfrac : nullptr, c->kposd, c->gate);
   // structure factors: enough row chunks per tile to fill the machine
   int rpb = c->nrows;
   while (rpb > 1 && (long long)c->ks_tiles * ((c->nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
-  dim3 gs(c->ks_tiles, (c->nrows + rpb - 1) / rpb);
+  dim3 gsf(c->ks_tiles, (c->nrows + rpb - 1) / rpb);
   if (mixed)
-    k_sfac_mixed<<<gs, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
-                                               c->spart);
+    k_sfac_mixed<<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
+                                                c->spart, c->gate);
   else
-    k_sfac_plain<<<gs, KS_THREADS, 0, c->st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
-                                               dhmati, c->spart);
+    k_sfac_plain<<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
+                                                dhmati, c->spart, c->gate);
   int ib = 256, gb = grid_for(c->ktot, ib);
   if (gb > 148 * 4) gb = 148 * 4;
   k_sred<<<gb, ib, 0, c->st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
-                               c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc);
+                               c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc,
+                               c->gate);
   int split = c->kf_split;
   int rps = (c->nrows + split - 1) / split;
   if (mixed) {
@@ -446,11 +457,12 @@ int kspace_forces(Ctx *c) {
       attr = true;
     }
     k_kforce_mixed<<<gf, KS_THREADS, smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows, c->rows,
-                                                     c->row_k0, rps, c->akf, c->ktot, dhmati, split > 1, c->fxl);
+                                                     c->row_k0, rps, c->akf, c->ktot, dhmati, split > 1, c->fxl,
+                                                     c->gate);
   } else {
     dim3 gf((c->ncharge + 255) / 256, split);
     k_kforce_plain<<<gf, 256, 0, c->st>>>(c->ncharge, c->kposd, c->icharge, c->n, c->nrows, c->rows, c->row_k0,
-                                          rps, c->akd, c->ktot, dhmati, split > 1, c->fxl);
+                                          rps, c->akd, c->ktot, dhmati, split > 1, c->fxl, c->gate);
   }
   c->launches += 4;
   tend(c, 1, e0);

@@ -36,7 +36,7 @@ __global__ void k_cell_assign(int n, const double *__restrict__ pos, const doubl
                               int ncx, int ncy, int ncz, int *__restrict__ cell_of,
                               int *__restrict__ cell_count, int4 *__restrict__ cimg,
                               const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double x = pos[i], y = pos[n + i], z = pos[2 * n + i];
@@ -66,7 +66,7 @@ __global__ void k_cell_assign(int n, const double *__restrict__ pos, const doubl
 template <typename TI, typename TO>
 __global__ void k_scan(const TI *__restrict__ in, TO *__restrict__ out, long long *__restrict__ tot,
                        int m, const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   const TI *a = in + (size_t)blockIdx.y * m;
   TO *o = out + (size_t)blockIdx.y * (m + 1);
   __shared__ TO part[1024];
@@ -97,7 +97,7 @@ __global__ void k_scan(const TI *__restrict__ in, TO *__restrict__ out, long lon
 __global__ void k_cell_fill(int n, const int *__restrict__ cell_of, const int *__restrict__ cell_start,
                             int *__restrict__ cursor, int *__restrict__ cell_atoms,
                             const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int c = cell_of[i];
@@ -108,7 +108,7 @@ __global__ void k_cell_fill(int n, const int *__restrict__ cell_of, const int *_
 // order every cell's atoms by atom index (deterministic lists)
 __global__ void k_cell_sort(int ncells, const int *__restrict__ cell_start, int *__restrict__ cell_atoms,
                             const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
   int lo = cell_start[c], hi = cell_start[c + 1];
@@ -201,7 +201,14 @@ __device__ __forceinline__ void for_pairs(const ListParams &P, int t, const int 
           int kx = (ci.y - cj.y - (int)mx) * P.ncx + (cx - (cj.x & 1023));
           int ky = (ci.z - cj.z - (int)my) * P.ncy + (cy - ((cj.x >> 10) & 1023));
           int kz = (ci.w - cj.w - (int)mz) * P.ncz + (cz - ((cj.x >> 20) & 1023));
+          // |k| <= 1 per dimension whenever r < rlist <= cell width; any
+          // other value would mean the geometry assumption broke: count it
+          // and use the zero shift rather than index past the shift table
           int code = (kx + 1) * 9 + (ky + 1) * 3 + (kz + 1);
+          if (kx < -1 || kx > 1 || ky < -1 || ky > 1 || kz < -1 || kz > 1) {
+            code = 13;
+            flags |= 16;
+          }
           f(i, j, flags, code);
         }
       }
@@ -216,7 +223,7 @@ __global__ void k_list_count(ListParams P, const int *__restrict__ cell_atoms, c
                              const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
                              const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, int ninter,
                              int *__restrict__ cnt, const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= P.n) return;
   int c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
@@ -246,15 +253,22 @@ __global__ void k_list_fill(ListParams P, const int *__restrict__ cell_atoms, co
                             const long long *__restrict__ off, const long long *__restrict__ tot,
                             const int *__restrict__ rank, int2 *__restrict__ l0, int2 *__restrict__ l1,
                             int2 *__restrict__ l2, int2 *__restrict__ l3, uint32_t *__restrict__ nbr,
-                            long long *__restrict__ stat, const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+                            long long *__restrict__ stat, int *__restrict__ halt,
+                            const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= P.n) return;
-  // a list that outgrew its capacity is not written at all; the host sees
-  // ST_OVERFLOW, grows the buffers and rebuilds
+  // if any list outgrew its capacity nothing is written and the step halts:
+  // the host grows the buffers and finishes the step (see run_step)
   bool ok0 = tot[0] <= P.cap[0], ok1 = tot[1] <= P.cap[1], ok2 = tot[2] <= P.cap[2],
        ok3 = tot[3] <= P.cap[3], ok4 = tot[4] <= P.cap[4];
-  if (t == 0 && !(ok0 && ok1 && ok2 && ok3 && ok4)) atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
+  if (!(ok0 && ok1 && ok2 && ok3 && ok4)) {
+    if (t == 0) {
+      atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
+      if (halt) *halt = 1;
+    }
+    return;
+  }
   long long p0 = off[t], p1 = off[(P.n + 1) + t], p2 = off[2 * (P.n + 1) + t],
             p3 = off[3 * (P.n + 1) + t], p4 = off[4 * (P.n + 1) + t];
   for_pairs(P, t, cell_atoms, cell_start, pos, itype, map, icut, q, excl_off, excl_idx, cexcl_off,
@@ -266,6 +280,7 @@ __global__ void k_list_fill(ListParams P, const int *__restrict__ cell_atoms, co
                 if ((fl & 4) && ok2) l2[p2++] = pr;
                 if ((fl & 8) && ok3) l3[p3++] = pr;
               }
+              if (fl & 16) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
               if (P.want_full && (fl & 5) && ok4) {
                 uint32_t e = (uint32_t)rank[j] | ((uint32_t)code << ENT_CODE_SHIFT);
                 if (fl & 1) e |= ENT_LJ;
@@ -285,7 +300,7 @@ __global__ void k_sorted_init(int n, const int *__restrict__ cell_atoms, const i
                               const int *__restrict__ itype, int *__restrict__ rank,
                               int *__restrict__ styp, double *__restrict__ corner,
                               const int *__restrict__ gate) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   int i = cell_atoms[t];
@@ -303,7 +318,7 @@ __global__ void k_sorted_init(int n, const int *__restrict__ cell_atoms, const i
 __global__ void k_snapshot(int n3, const double *__restrict__ pos, double *__restrict__ dxn,
                            const int *__restrict__ gate, int *__restrict__ istate,
                            long long *__restrict__ stat) {
-  if (gate && *gate == 0) return;
+  if (gated_off(gate, 1)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n3) dxn[i] = pos[i];
   if (i == 0) {
@@ -398,7 +413,7 @@ static ListParams params(Ctx *c) {
 int build_lists(Ctx *c, bool device_flag) {
   const int n = c->n;
   const int B = 256;
-  const int *gate = device_flag ? c->istate + IS_REBUILD : nullptr;
+  const int *gate = device_flag ? c->istate : nullptr;
   cudaEvent_t e0;
   tbegin(c, 2, &e0);
   int4 *cimg = c->cimg;
@@ -439,7 +454,7 @@ int build_lists(Ctx *c, bool device_flag) {
                                                     c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off,
                                                     c->cexcl_idx, cimg, c->ninter, c->off, c->ltot, c->rank,
                                                     c->lst[0], c->lst[1], c->lst[2], c->lst[3], c->nbr,
-                                                    c->stat, gate);
+                                                    c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
   k_snapshot<<<grid_for(3LL * n, B), B, 0, c->st>>>(3 * n, c->pos, c->dxn, gate, c->istate, c->stat);
   c->launches += 2;
   CKL(c);

@@ -30,7 +30,8 @@ struct MixedP {
 
 __global__ void k_xq_update(int n, const int *__restrict__ sorig, const double *__restrict__ pos,
                             const double *__restrict__ corner, const double *__restrict__ q,
-                            float4 *__restrict__ xq) {
+                            float4 *__restrict__ xq, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   int i = sorig[t];
@@ -48,7 +49,8 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
     const long long *__restrict__ off, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
     const float4 *__restrict__ gte, double *__restrict__ fout, double *__restrict__ fshort,
-    double *__restrict__ acc, long long *__restrict__ stat) {
+    double *__restrict__ acc, long long *__restrict__ stat, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
   float4 *shift = sm;                                   // 27
   float *fcut = reinterpret_cast<float *>(sm + 28);     // 8 * ninter
@@ -260,7 +262,7 @@ static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   }
   k_pair_mixed<TPA, SB, NS><<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->off + 4 * ((size_t)c->n + 1),
                                                       c->nbr, c->shift, c->map, c->fcut, c->ftab_lj, c->ftab_el,
-                                                      fout, c->fxs, c->acc, c->stat);
+                                                      fout, c->fxs, c->acc, c->stat, c->gate);
 }
 
 template <bool SB, bool NS>
@@ -281,7 +283,7 @@ bool g_smallbox_warned = false;
 int mixed_pairs(Ctx *c, int iflg, int mask) {
   if (c->ncharge == 0) mask &= 1;
   if (c->ninter == 0) mask &= 2;
-  if (!mask || c->hcount[LT_FULL] == 0) return CM3D_NB_OK;
+  if (!mask || !c->lists_built) return CM3D_NB_OK;
   MixedP P;
   P.n = c->n;
   P.ntypes = c->ntypes;
@@ -310,7 +312,8 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   }
   double *fout = iflg == 1 ? c->fxl : c->fxs;
   const int B = 256;
-  k_xq_update<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, c->cell_atoms, c->pos, c->corner, c->q, c->xq);
+  k_xq_update<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, c->cell_atoms, c->pos, c->corner, c->q, c->xq,
+                                                  c->gate);
   cudaEvent_t e0;
   tbegin(c, 0, &e0);
   if (sb) {

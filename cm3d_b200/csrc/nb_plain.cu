@@ -23,15 +23,18 @@ __device__ __forceinline__ double interp_ref(const double *t, int k, double p) {
 }
 
 // LJ over a half list (t at iflg 1, s at iflg 0)
-__global__ void k_lj_plain(long long np, const int2 *__restrict__ lst, PlainP P, int n,
+__global__ void k_lj_plain(const long long *__restrict__ npd, const int2 *__restrict__ lst, PlainP P, int n,
                            const double *__restrict__ pos, const int *__restrict__ itype,
                            const int *__restrict__ map, const double *__restrict__ icut,
                            const double *__restrict__ dvtab, const double *__restrict__ vtab,
                            const double *__restrict__ switchs, double *__restrict__ fl,
-                           double *__restrict__ fs, double *__restrict__ acc, long long *__restrict__ stat) {
+                           double *__restrict__ fs, double *__restrict__ acc, long long *__restrict__ stat,
+                           const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   // v: spotl spothl sprsl t0 t1 t2 t4 t5 t8
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   long long under = 0;
+  const long long np = *npd;   // device count: valid after device-side rebuilds
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
        p += (long long)gridDim.x * blockDim.x) {
     int2 pr = lst[p];
@@ -94,14 +97,16 @@ __global__ void k_lj_plain(long long np, const int2 *__restrict__ lst, PlainP P,
 // real-space Ewald over a half list (te at iflg 1, se at iflg 0); CM3D's
 // force_e falls through from level 0 into level 1 (finter_e.c:72-83), so
 // both levels use the full cutoff rmaxl_coul2 and the switch never engages
-__global__ void k_el_plain(long long np, const int2 *__restrict__ lst, PlainP P, int n,
+__global__ void k_el_plain(const long long *__restrict__ npd, const int2 *__restrict__ lst, PlainP P, int n,
                            const double *__restrict__ pos, const double *__restrict__ q,
                            const double *__restrict__ dcoultab, const double *__restrict__ coultab,
                            double *__restrict__ fl, double *__restrict__ fs, double *__restrict__ acc,
-                           long long *__restrict__ stat) {
+                           long long *__restrict__ stat, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   // v: spote spothe sprse t0 t1 t2 t4 t5 t8
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   long long under = 0;
+  const long long np = *npd;   // device count: valid after device-side rebuilds
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < np;
        p += (long long)gridDim.x * blockDim.x) {
     int2 pr = lst[p];
@@ -202,20 +207,24 @@ int plain_pairs(Ctx *c, int iflg, int which) {
   double *fl = iflg == 1 ? c->fxl : c->fxs;
   const int B = 256;
   int list = which == 0 ? (iflg == 1 ? LT_T : LT_S) : (iflg == 1 ? LT_TE : LT_SE);
-  long long np = c->hcount[list];
-  if (np <= 0) return CM3D_NB_OK;
+  // the grid is sized from the host's latest count (grid-stride loop); the
+  // kernel reads the exact count from the device, which a device-side
+  // rebuild inside a CUDA graph may have changed
+  long long np = c->hcount[list] > 0 ? c->hcount[list] : 1;
   int grid = grid_for(np, B);
+  if (grid < 148 * 8) grid = 148 * 8;
   if (grid > 148 * 16) grid = 148 * 16;
+  const long long *npd = c->ltot + list;
   cudaEvent_t e0;
   tbegin(c, 0, &e0);
   if (which == 0) {
-    k_lj_plain<<<grid, B, 0, c->st>>>(np, c->lst[list], P, c->n, c->pos, c->itype, c->map, c->icut, c->dvtab,
-                                      c->vtab, c->switchs, fl, c->fxs, c->acc, c->stat);
+    k_lj_plain<<<grid, B, 0, c->st>>>(npd, c->lst[list], P, c->n, c->pos, c->itype, c->map, c->icut, c->dvtab,
+                                      c->vtab, c->switchs, fl, c->fxs, c->acc, c->stat, c->gate);
   } else {
     if (c->ncharge == 0) return CM3D_NB_OK;
     P.tablast = c->tablast_e;
-    k_el_plain<<<grid, B, 0, c->st>>>(np, c->lst[list], P, c->n, c->pos, c->q, c->dcoultab, c->coultab, fl,
-                                      c->fxs, c->acc, c->stat);
+    k_el_plain<<<grid, B, 0, c->st>>>(npd, c->lst[list], P, c->n, c->pos, c->q, c->dcoultab, c->coultab, fl,
+                                      c->fxs, c->acc, c->stat, c->gate);
   }
   c->launches++;
   tend(c, 0, e0);

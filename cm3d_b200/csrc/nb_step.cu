@@ -104,8 +104,10 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
                         const double *__restrict__ dxn, const int *__restrict__ gboff,
                         const int4 *__restrict__ bij, const double2 *__restrict__ bp,
                         const int *__restrict__ geoff, const int4 *__restrict__ eijk,
-                        const double2 *__restrict__ ep, int *__restrict__ istate) {
+                        const double2 *__restrict__ ep, int *__restrict__ istate, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g == 0) istate[IS_INTR] = intr;
   if (g >= P.ngroups) return;
   const int n = P.n;
   const int a0 = gaoff[g], a1 = gaoff[g + 1];
@@ -173,7 +175,7 @@ __global__ void k_disp(int n, double skin2q, const double *__restrict__ pos, con
 // its position at the last rebuild (by CM3D's factor skin2/d^2)
 __global__ void k_resetpos(int n, double skin2q, double *__restrict__ pos, const double *__restrict__ dxn,
                            const int *__restrict__ istate, long long *__restrict__ stat) {
-  if (istate[IS_REBUILD] == 0) return;
+  if (istate[IS_REBUILD] == 0 || istate[IS_HALT] != 0) return;
   if (istate[IS_ISTEP] - istate[IS_ISTEPLAST] >= 3) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) atomicAdd((unsigned long long *)(stat + ST_RESETS), 1ull);
@@ -197,7 +199,9 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
                              const int2 *__restrict__ cij, const int *__restrict__ gboff,
                              const int4 *__restrict__ bij, const double2 *__restrict__ bp,
                              const int *__restrict__ geoff, const int4 *__restrict__ eijk,
-                             const double2 *__restrict__ ep, double *__restrict__ acc) {
+                             const double2 *__restrict__ ep, double *__restrict__ acc,
+                             const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = P.n;
   // ecorr: pot, prs, t0 t1 t2 t4 t5 t8 | bond: v, w, t0..t8 | bend: v
@@ -270,7 +274,8 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
 __global__ void k_finish(int n, int level, int kick, int rm_l, int rm_s, double dk_l, double dk_s,
                          const double *__restrict__ mass, double *__restrict__ fxl, double *__restrict__ fxs,
                          double *__restrict__ vel, double *__restrict__ acc, int *__restrict__ istate,
-                         int advance_step) {
+                         int advance_step, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[6] = {0, 0, 0, 0, 0, 0};
   if (i < n) {
@@ -426,8 +431,6 @@ int step_setup(Ctx *c, const cm3d_nb_system *s) {
   return CM3D_NB_OK;
 }
 
-static const int SLOTS_NONBONDED[] = {ACC_SPOTL, ACC_SPOTE, ACC_VK, ACC_POT_ECORR};
-
 int run_bonded(Ctx *c) {
   StepP P = step_params(c);
   const int B = 128;
@@ -447,7 +450,7 @@ int group_init(Ctx *c, bool zero_fxs) {
   k_group_init<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, zero_fxs ? 1 : 0, c->grp_atom_off, c->grp_atoms,
                                                          c->pos, c->q, c->fxl, c->fxs, c->grp_ecorr_off,
                                                          c->ecorr_ij, c->grp_bond_off, c->bond_ij, c->bond_p,
-                                                         c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc);
+                                                         c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc, c->gate);
   tend(c, 3, e0);
   c->launches++;
   CKL(c);
@@ -458,7 +461,15 @@ int finish_level1(Ctx *c, double dter, double dter1, bool kick) {
   const int B = 256;
   bool rs = c->need_short || c->nres_lrf > 1;
   k_finish<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, 1, kick ? 1 : 0, 1, rs ? 1 : 0, dter, dter1, c->mass, c->fxl,
-                                               c->fxs, c->vel, c->acc, c->istate, kick ? 1 : 0);
+                                               c->fxs, c->vel, c->acc, c->istate, kick ? 1 : 0, c->gate);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+static int finish_level0(Ctx *c, double dts2, bool kick) {
+  k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, kick ? 1 : 0, 0, 1, 0, dts2, c->mass, c->fxl, c->fxs,
+                                                   c->vel, c->acc, c->istate, 0, c->gate);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
@@ -480,7 +491,7 @@ int reset_positions(Ctx *c) {
   return CM3D_NB_OK;
 }
 
-// zero the accumulators force(1) owns (everything but nothing persistent)
+// zero every accumulator force(1) and getvireal fill
 static int zero_acc(Ctx *c) {
   CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * ACC_COUNT, c->st));
   return CM3D_NB_OK;
@@ -504,72 +515,70 @@ int run_force(Ctx *c, int iflg) {
   if (iflg == 0) {
     CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
     if ((rc = pair_forces(c, 0, 3))) return rc;
-    k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, 0, 0, 1, 0, 0, c->mass, c->fxl, c->fxs, c->vel,
-                                                     c->acc, c->istate, 0);
-    c->launches++;
-    CKL(c);
-    return CM3D_NB_OK;
+    return finish_level0(c, 0, false);
   }
   set_error("force(): unknown level %d", iflg);
   return CM3D_NB_ERR_ARG;
 }
 
-// one outer step; with `gated` the rebuild kernels are gated on the device
-// flag (graph capture), otherwise the host reads the flag and rebuilds
-static int one_step(Ctx *c, bool gated) {
+// the nonbonded level that closes RESPA level `intr` (md_step.c:138-146):
+// force(1) + kick on the last level, force(0) + kick otherwise
+static int close_level(Ctx *c, int intr) {
+  int rc;
+  StepP P = step_params(c);
+  if (intr == c->nres_lrf - 1) {
+    if ((rc = zero_acc(c))) return rc;
+    if ((rc = group_init(c, P.use_fxs))) return rc;
+    if ((rc = pair_forces(c, 1, 3))) return rc;
+    if ((rc = kspace_forces(c))) return rc;
+    return finish_level1(c, P.dter, P.dter1, true);
+  }
+  CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+  if ((rc = pair_forces(c, 0, 3))) return rc;
+  return finish_level0(c, P.dts2, true);
+}
+
+// RESPA level `intr` of one outer step (md_step.c:95-146); with `gated` the
+// rebuild kernels are gated on the device flag (graph capture), otherwise
+// the host reads the flag and rebuilds
+static int one_level(Ctx *c, int intr, bool gated) {
   int rc;
   StepP P = step_params(c);
   const int B = 128;
-  const int ninter = c->nres_lrf;
-  for (int intr = 0; intr < ninter; intr++) {
-    CK(cudaMemsetAsync(c->istate + IS_REBUILD, 0, sizeof(int), c->st));
-    cudaEvent_t e0;
-    tbegin(c, 3, &e0);
-    k_inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
-                                                      c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
-                                                      c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
-                                                      c->bend_p, c->istate);
-    tend(c, 3, e0);
-    c->launches++;
-    CKL(c);
-    if ((rc = reset_positions(c))) return rc;
-    if (gated) {
-      if ((rc = build_lists(c, true))) return rc;
-    } else {
-      CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
-      CK(cudaStreamSynchronize(c->st));
-      if (c->h_istate[IS_REBUILD]) {
-        if ((rc = build_lists(c, false))) return rc;
-      }
+  CK(cudaMemsetAsync(c->istate + IS_REBUILD, 0, sizeof(int), c->st));
+  cudaEvent_t e0;
+  tbegin(c, 3, &e0);
+  k_inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
+                                                    c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
+                                                    c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
+                                                    c->bend_p, c->istate, c->gate);
+  tend(c, 3, e0);
+  c->launches++;
+  CKL(c);
+  if ((rc = reset_positions(c))) return rc;
+  if (gated) {
+    if ((rc = build_lists(c, true))) return rc;
+  } else {
+    CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_istate[IS_REBUILD]) {
+      if ((rc = build_lists(c, false))) return rc;
     }
-    if (intr == ninter - 1) {
-      if ((rc = zero_acc(c))) return rc;
-      if ((rc = group_init(c, P.use_fxs))) return rc;
-      if ((rc = pair_forces(c, 1, 3))) return rc;
-      if ((rc = kspace_forces(c))) return rc;
-      if ((rc = finish_level1(c, P.dter, P.dter1, true))) return rc;
-    } else {
-      CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
-      if ((rc = pair_forces(c, 0, 3))) return rc;
-      k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, 1, 0, 1, 0, P.dts2, c->mass, c->fxl, c->fxs,
-                                                       c->vel, c->acc, c->istate, 0);
-      c->launches++;
-      CKL(c);
-    }
+  }
+  return close_level(c, intr);
+}
+
+static int one_step(Ctx *c, bool gated) {
+  for (int intr = 0; intr < c->nres_lrf; intr++) {
+    int rc = one_level(c, intr, gated);
+    if (rc) return rc;
   }
   return CM3D_NB_OK;
 }
 
-static int snapshot(Ctx *c, bool restore) {
-  const size_t n3 = 3 * (size_t)c->n;
-  double *bufs[6] = {c->pos, c->vel, c->fxl, c->fxs, c->fxa, c->dxn};
-  for (int k = 0; k < 6; k++) {
-    if (restore) CK(cudaMemcpyAsync(bufs[k], c->snap + k * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
-    else CK(cudaMemcpyAsync(c->snap + k * n3, bufs[k], sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->st));
-  }
-  int *is = reinterpret_cast<int *>(c->snap + 6 * n3);
-  if (restore) CK(cudaMemcpyAsync(c->istate, is, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToDevice, c->st));
-  else CK(cudaMemcpyAsync(is, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToDevice, c->st));
+static int set_istep(Ctx *c, int istep) {
+  c->h_istate[IS_ISTEP] = istep;
+  CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
   return CM3D_NB_OK;
 }
 
@@ -580,19 +589,24 @@ int run_step(Ctx *c, int istep0, int nsteps) {
     return CM3D_NB_ERR_STATE;
   }
   if (nsteps <= 0) return CM3D_NB_OK;
-  c->h_istate[IS_ISTEP] = istep0;
-  CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  if ((rc = set_istep(c, istep0))) return rc;
+  cudaEvent_t e4;
   if (!c->use_graph || c->timing.on) {
+    tbegin(c, 4, &e4);
     for (int s = 0; s < nsteps; s++)
       if ((rc = one_step(c, false))) return rc;
+    tend(c, 4, e4);
     return CM3D_NB_OK;
   }
-  // graph replay: one captured step, the rebuild gated on the device flag
+  // graph replay: one captured step, every kernel gated on the device state
+  // (rebuild flag; halt after a list overflow)
   if (!c->graph) {
     cudaGraph_t g;
     long long l0 = c->launches;
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    c->gate = c->istate;
     rc = one_step(c, true);
+    c->gate = nullptr;
     cudaError_t e = cudaStreamEndCapture(c->st, &g);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
@@ -601,35 +615,29 @@ int run_step(Ctx *c, int istep0, int nsteps) {
     c->graph_launches = c->launches - l0;
     c->launches = l0;
   }
-  CK(cudaMemsetAsync(c->stat + ST_OVERFLOW, 0, sizeof(long long), c->st));
-  if ((rc = snapshot(c, false))) return rc;
+  tbegin(c, 4, &e4);
   for (int s = 0; s < nsteps; s++) {
     CK(cudaGraphLaunch(c->graph, c->st));
     c->launches += c->graph_launches;
   }
-  long long ovf = 0;
-  CK(cudaMemcpyAsync(&c->h_stat[ST_OVERFLOW], c->stat + ST_OVERFLOW, sizeof(long long), cudaMemcpyDeviceToHost,
-                     c->st));
+  tend(c, 4, e4);
+  CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  ovf = c->h_stat[ST_OVERFLOW];
-  if (ovf) {
-    // a rebuild inside the graph outgrew a list: rewind and redo these steps
-    // with host-driven rebuilds (which grow the buffers), then re-capture
-    c->overflows_host++;
-    if ((rc = snapshot(c, true))) return rc;
-    CK(cudaMemsetAsync(c->stat + ST_OVERFLOW, 0, sizeof(long long), c->st));
-    c->h_istate[IS_ISTEP] = istep0;
-    CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
-    // rebuild at the restored positions (this grows the buffers); keep the
-    // restored isteplast so RESETPOS sees CM3D's step history
-    if ((rc = build_lists(c, false))) return rc;
-    CK(cudaMemcpyAsync(c->istate + IS_ISTEPLAST, reinterpret_cast<int *>(c->snap + 18 * (size_t)c->n) + IS_ISTEPLAST,
-                       sizeof(int), cudaMemcpyDeviceToDevice, c->st));
-    for (int s = 0; s < nsteps; s++)
-      if ((rc = one_step(c, false))) return rc;
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  if (!c->h_istate[IS_HALT]) return CM3D_NB_OK;
+  // A device-side rebuild outgrew a list: that step stopped right after its
+  // list count and every later kernel did nothing.  Grow the buffers, finish
+  // the step on the host-driven path and run the remaining steps.
+  c->overflows_host++;
+  const int failed = c->h_istate[IS_ISTEP], intr = c->h_istate[IS_INTR];
+  CK(cudaMemsetAsync(c->istate + IS_HALT, 0, sizeof(int), c->st));
+  if ((rc = build_lists(c, false))) return rc;
+  if ((rc = close_level(c, intr))) return rc;
+  for (int lv = intr + 1; lv < c->nres_lrf; lv++)
+    if ((rc = one_level(c, lv, false))) return rc;
+  cudaGraphExecDestroy(c->graph);   // it holds the old buffer addresses
+  c->graph = nullptr;
+  int done = failed + 1 - istep0;
+  if (done < nsteps) return run_step(c, failed + 1, nsteps - done);
   return CM3D_NB_OK;
 }
 

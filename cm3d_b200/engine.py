@@ -87,6 +87,7 @@ def load_library() -> C.CDLL:
         "cm3d_nb_enable_timing": (C.c_int, [vp, C.c_int]),
         "cm3d_nb_kernel_time": (C.c_int, [vp, C.c_int, dp, C.POINTER(ll)]),
         "cm3d_nb_launch_count": (ll, [vp]),
+        "cm3d_nb_measure_peaks": (C.c_int, [C.c_int, dp, dp]),
         "cm3d_nb_lj_table": (C.c_int, [C.c_double] * 7 + [C.c_int, C.c_int, dp, dp, dp, dp]),
         "cm3d_nb_coul_table": (C.c_int, [C.c_double] * 6 + [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]),
         "cm3d_nb_ewald_kvectors": (C.c_int, [C.c_int, ip, ip, ip, ip, ip]),
@@ -116,6 +117,13 @@ def device_count() -> int:
 
 def _p(a: np.ndarray, t=C.c_double):
     return a.ctypes.data_as(C.POINTER(t))
+
+
+def measure_peaks(device: int = 0) -> tuple[float, float]:
+    """(FP32, FP64) FMA throughput of the device in TFLOP/s, measured now."""
+    f32, f64 = C.c_double(0), C.c_double(0)
+    check(load_library().cm3d_nb_measure_peaks(device, C.byref(f32), C.byref(f64)), "measure_peaks")
+    return f32.value, f64.value
 
 
 class Engine:

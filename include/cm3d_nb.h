@@ -237,11 +237,17 @@ void *cm3d_nb_stream(cm3d_nb_ctx *ctx);
 /* Bracket every launch of kernel class `cls` with CUDA events on the
    context's stream; cm3d_nb_kernel_time returns the summed device time in
    ms and the number of launches since timing was enabled.
-   cls: 0 = pair kernel(s), 1 = k-space, 2 = list build, 3 = integrate. */
+   cls: 0 = pair kernel(s), 1 = k-space, 2 = list build, 3 = integrate
+   (enable bit 0; these launches then run eagerly, outside CUDA graphs),
+   4 = whole steps of cm3d_nb_step (enable bit 1; graph replays included). */
 int cm3d_nb_enable_timing(cm3d_nb_ctx *ctx, int enable);
 int cm3d_nb_kernel_time(cm3d_nb_ctx *ctx, int cls, double *ms, long long *launches);
 /* number of kernel launches this context issued so far */
 long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx);
+/* FMA throughput of `device` measured with a dependency-chain probe
+   (TFLOP/s, an FMA counted as 2 flops): the roofline denominators of the
+   CUDA-core pair and k-space kernels.  No CM3D counterpart. */
+int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops);
 
 /* ------------------------------------------ host set-up restatements */
 /* One interaction's LJ table, as get_ter_parm() builds it
