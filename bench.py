@@ -119,15 +119,15 @@ def measured_peaks() -> dict:
         return {}
 
 
-def l2_flusher(device: int, stream_ptr: int):
-    """Write a buffer larger than L2 (126 MB) on the engine's stream."""
+def l2_flusher(device: int):
+    """Write a buffer larger than L2 (126 MB) and wait for it, so the next
+    step starts with a cold L2 (the write is outside the step's events)."""
     import torch
     buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")
-    ext = torch.cuda.ExternalStream(stream_ptr, device=f"cuda:{device}")
 
     def flush():
-        with torch.cuda.stream(ext):
-            buf.fill_(1.0)
+        buf.fill_(1.0)
+        torch.cuda.synchronize(device)
     return flush
 
 
@@ -325,7 +325,7 @@ def main() -> None:
 
     eng = Engine(sysm, mode=_abi.MIXED, device=local)
     eng.step_init()
-    flush = l2_flusher(local, eng.stream())
+    flush = l2_flusher(local)
     if dist:
         dist.barrier()
     torch.cuda.synchronize(local)

@@ -83,7 +83,8 @@ static void destroy(Ctx *c) {
                   c->ecorr_pairs, c->grp_atom_off, c->grp_atoms, c->grp_bond_off, c->grp_bend_off,
                   c->grp_ecorr_off, c->bond_ij, c->bond_p, c->bend_ijk, c->bend_p, c->ecorr_ij, c->cell_of,
                   c->cell_start, c->cell_cursor, c->cell_atoms, c->rank, c->cnt, c->off, c->ltot, c->lst[0],
-                  c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->styp, c->shift, c->corner, c->cimg, c->acc,
+                  c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
+                  c->cimg, c->acc,
                   c->stat, c->istate};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -137,6 +138,7 @@ static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out
   *out = c;
   c->dev = o.device;
   CK(cudaSetDevice(c->dev));
+  CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->dev));
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   c->mode = o.mode;
   c->need_short = o.need_short;
@@ -692,14 +694,32 @@ int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e) {
   return CM3D_NB_OK;
 }
 
+// The mixed engine's rebuilds write only its full list.  CM3D's half lists
+// are produced on request by rebuilding from the positions of the last
+// rebuild (dxn): the same cells and the same pairs, without touching the
+// live state or the snapshot.
+static int ensure_half_lists(Ctx *c) {
+  if (c->mode != CM3D_NB_MIXED || !c->lists_built) return CM3D_NB_OK;
+  std::swap(c->pos, c->dxn);
+  c->want_half = true;
+  c->no_snapshot = true;
+  int rc = build_lists(c, false);
+  std::swap(c->pos, c->dxn);
+  c->want_half = false;
+  c->no_snapshot = false;
+  return rc;
+}
+
 int cm3d_nb_list_count(cm3d_nb_ctx *ctx, int which, long long *npairs) {
   CTX;
   if (which < 0 || which > 3) {
     set_error("list_count: unknown list %d", which);
     return CM3D_NB_ERR_ARG;
   }
+  int rc = ensure_half_lists(c);
+  if (rc) return rc;
   *npairs = c->lists_built ? c->hcount[which] : 0;
-  if (c->lists_built && c->use_graph) {
+  if (c->lists_built && c->use_graph && c->mode == CM3D_NB_PLAIN_FP64) {
     // device-gated rebuilds may have changed the counts since the host looked
     CK(cudaMemcpyAsync(c->h_ltot, c->ltot, sizeof(long long) * LT_COUNT, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));

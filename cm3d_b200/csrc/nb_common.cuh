@@ -98,6 +98,7 @@ struct Timing {
 struct Ctx {
   // ---- configuration
   int dev = 0;
+  int num_sms = 148;
   cudaStream_t st = nullptr;
   int mode = CM3D_NB_MIXED;
   int need_short = 0;
@@ -168,6 +169,7 @@ struct Ctx {
   int2 *lst[4] = {nullptr, nullptr, nullptr, nullptr};   // t s te se half lists
   uint32_t *nbr = nullptr;              // full list (mixed)
   float4 *xq = nullptr;                 // sorted: cell-relative FP32 pos + q
+  float *epart = nullptr;               // mixed: per-atom energy/virial partials
   int *styp = nullptr;                  // sorted type
   int *sorig = nullptr;                 // sorted -> original (== cell_atoms)
   float4 *shift = nullptr;              // 27 FP32 cell-shift vectors
@@ -184,6 +186,8 @@ struct Ctx {
   // ---- host bookkeeping
   bool lists_built = false;
   bool forces_valid = false;
+  bool want_half = false;               // mixed mode: also write the half lists
+  bool no_snapshot = false;             // a rebuild that must not touch dxn
   long long launches = 0;
   long long rebuilds_host = 0, overflows_host = 0;
   Timing timing;

@@ -105,20 +105,35 @@ __global__ void k_cell_fill(int n, const int *__restrict__ cell_of, const int *_
   cell_atoms[cell_start[c] + slot] = i;
 }
 
-// order every cell's atoms by atom index (deterministic lists)
+// order every cell's atoms by atom index (deterministic lists): one block
+// per cell ranks each atom among its cell's atoms (indices are distinct)
 __global__ void k_cell_sort(int ncells, const int *__restrict__ cell_start, int *__restrict__ cell_atoms,
                             const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= ncells) return;
-  int lo = cell_start[c], hi = cell_start[c + 1];
-  for (int a = lo + 1; a < hi; a++) {
-    int v = cell_atoms[a], b = a - 1;
-    while (b >= lo && cell_atoms[b] > v) {
-      cell_atoms[b + 1] = cell_atoms[b];
-      b--;
+  __shared__ int s[1024];
+  const int c = blockIdx.x;
+  const int lo = cell_start[c], hi = cell_start[c + 1], m = hi - lo;
+  if (m <= 1) return;
+  if (m <= 1024) {
+    for (int k = threadIdx.x; k < m; k += blockDim.x) s[k] = cell_atoms[lo + k];
+    __syncthreads();
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+      int v = s[k], r = 0;
+      for (int u = 0; u < m; u++) r += s[u] < v;
+      cell_atoms[lo + r] = v;
     }
-    cell_atoms[b + 1] = v;
+    return;
+  }
+  // a cell with more than 1024 atoms: odd-even transposition sort in place
+  for (int pass = 0; pass < m; pass++) {
+    for (int k = lo + (pass & 1) + 2 * threadIdx.x; k + 1 < hi; k += 2 * blockDim.x) {
+      int a0 = cell_atoms[k], a1 = cell_atoms[k + 1];
+      if (a0 > a1) {
+        cell_atoms[k] = a1;
+        cell_atoms[k + 1] = a0;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -128,28 +143,116 @@ struct ListParams {
   int nsx, nsy, nsz;
   double h[9], hi[9];
   double rmaxl_skin2_e, rmaxs_skin2_e;
-  int want_full;                    // mixed: build the full list too
+  float lim2;                       // FP32 prefilter radius^2 (inf = off)
+  int want_full;                    // mixed: build the full list
+  int want_half;                    // build CM3D's four half lists
   long long cap[LT_COUNT];
 };
 
-// Visit every candidate j of sorted atom t, call f(i, j, flags, code) for
-// each pair that belongs to at least one list.  flags: bit0 t, bit1 s,
-// bit2 te, bit3 se.  code: cell-shift code for the full list.
-template <typename F>
-__device__ __forceinline__ void for_pairs(const ListParams &P, int t, const int *__restrict__ cell_atoms,
-                                          const int *__restrict__ cell_start, const double *__restrict__ pos,
-                                          const int *__restrict__ itype, const int *__restrict__ map,
-                                          const double *__restrict__ icut, const double *__restrict__ q,
-                                          const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
-                                          const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx,
-                                          const int4 *__restrict__ cimg, int ninter, F f) {
+// Exact membership test of one candidate pair, in CM3D's FP64 operation
+// order.  Returns flags (bit0 t, bit1 s, bit2 te, bit3 se, bit4 bad shift)
+// and the cell-shift code of the pair for the full list.
+__device__ __forceinline__ int exact_flags(const ListParams &P, int i, int j, int4 ci, const double *__restrict__ pos,
+                                           double xi, double yi, double zi, int ti, bool qi,
+                                           const int *__restrict__ itype, const int *__restrict__ map,
+                                           const double *__restrict__ icut, const double *__restrict__ q,
+                                           const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
+                                           const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx,
+                                           const int4 *__restrict__ cimg, int &code) {
   const int n = P.n;
-  int i = cell_atoms[t];
-  int4 ci = cimg[i];
-  int cx = ci.x & 1023, cy = (ci.x >> 10) & 1023, cz = (ci.x >> 20) & 1023;
-  double xi = pos[i], yi = pos[n + i], zi = pos[2 * n + i];
-  int ti = itype[i];
-  bool qi = q[i] != 0.0;
+  const int intr = map[ti * P.ntypes + itype[j]];
+  const bool lj_ok = intr >= 0;
+  const bool el_ok = qi && q[j] != 0.0;
+  if (!lj_ok && !el_ok) return 0;
+  double dx = xi - pos[j], dy = yi - pos[n + j], dz = zi - pos[2 * n + j];
+  double sx = __dadd_rn(__dadd_rn(__dmul_rn(dx, P.hi[0]), __dmul_rn(dy, P.hi[1])), __dmul_rn(dz, P.hi[2]));
+  double sy = __dadd_rn(__dadd_rn(__dmul_rn(dx, P.hi[3]), __dmul_rn(dy, P.hi[4])), __dmul_rn(dz, P.hi[5]));
+  double sz = __dadd_rn(__dadd_rn(__dmul_rn(dx, P.hi[6]), __dmul_rn(dy, P.hi[7])), __dmul_rn(dz, P.hi[8]));
+  const double mx = anint_ref(sx), my = anint_ref(sy), mz = anint_ref(sz);
+  sx = __dsub_rn(sx, mx);
+  sy = __dsub_rn(sy, my);
+  sz = __dsub_rn(sz, mz);
+  const double ex = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[0]), __dmul_rn(sy, P.h[1])), __dmul_rn(sz, P.h[2]));
+  const double ey = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[3]), __dmul_rn(sy, P.h[4])), __dmul_rn(sz, P.h[5]));
+  const double ez = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[6]), __dmul_rn(sy, P.h[7])), __dmul_rn(sz, P.h[8]));
+  const double r2 = r2_ref(ex, ey, ez);
+  int flags = 0;
+  if (lj_ok && r2 < icut[8 * intr + 5] && !excluded(i, j, excl_off, excl_idx)) {
+    flags |= 1;
+    if (r2 < icut[8 * intr + 4]) flags |= 2;
+  }
+  if (el_ok && r2 < P.rmaxl_skin2_e && !excluded(i, j, cexcl_off, cexcl_idx)) {
+    flags |= 4;
+    if (r2 < P.rmaxs_skin2_e) flags |= 8;
+  }
+  if (!flags) return 0;
+  // shift code: k = (n_i - n_j - m) nc + (c_i - c_j) per dimension; |k| <= 1
+  // whenever r < rlist <= cell width.  Anything else means the geometry
+  // assumption broke: flag it and use the zero shift rather than index past
+  // the shift table.
+  const int4 cj = cimg[j];
+  const int kx = (ci.y - cj.y - (int)mx) * P.ncx + ((ci.x & 1023) - (cj.x & 1023));
+  const int ky = (ci.z - cj.z - (int)my) * P.ncy + (((ci.x >> 10) & 1023) - ((cj.x >> 10) & 1023));
+  const int kz = (ci.w - cj.w - (int)mz) * P.ncz + (((ci.x >> 20) & 1023) - ((cj.x >> 20) & 1023));
+  code = (kx + 1) * 9 + (ky + 1) * 3 + (kz + 1);
+  if (kx < -1 || kx > 1 || ky < -1 || ky > 1 || kz < -1 || kz > 1) {
+    code = 13;
+    flags |= 16;
+  }
+  return flags;
+}
+
+// One warp per cell-sorted atom t: the lanes walk the candidates of the
+// stencil cells 32 at a time (consecutive sorted atoms, coalesced FP32
+// loads), drop those clearly beyond the largest list radius with an FP32
+// distance from cell-relative coordinates (margin 1e-3 A, far above FP32
+// rounding), and decide the rest exactly in FP64.  FILL = false counts the
+// pairs of every list per atom; FILL = true writes them, compacted with warp
+// ballots in candidate order (deterministic).
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_list_warp(
+    ListParams P, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    const float4 *__restrict__ xq, const float4 *__restrict__ shift, const double *__restrict__ pos,
+    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
+    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
+    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
+    int *__restrict__ cnt, const long long *__restrict__ off, const long long *__restrict__ tot,
+    const int *__restrict__ rank, int2 *__restrict__ l0, int2 *__restrict__ l1, int2 *__restrict__ l2,
+    int2 *__restrict__ l3, uint32_t *__restrict__ nbr, long long *__restrict__ stat, int *__restrict__ halt,
+    const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= P.n) return;                                   // whole warps
+  const unsigned lt_mask = (1u << lane) - 1u;
+  bool ok[5] = {true, true, true, true, true};
+  long long p[5] = {0, 0, 0, 0, 0};
+  if (FILL) {
+    bool all = true;
+    for (int k = 0; k < 5; k++) {
+      ok[k] = tot[k] <= P.cap[k];
+      all = all && ok[k];
+      p[k] = off[(size_t)k * (P.n + 1) + t];
+    }
+    if (!all) {
+      // a list outgrew its buffer: write nothing, halt the step (the host
+      // grows the buffers and finishes it, see run_step)
+      if (t == 0 && lane == 0) {
+        atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
+        if (halt) *halt = 1;
+      }
+      return;
+    }
+  }
+  const int i = cell_atoms[t];
+  const int4 ci = cimg[i];
+  const int cx = ci.x & 1023, cy = (ci.x >> 10) & 1023, cz = (ci.x >> 20) & 1023;
+  const float4 xi4 = xq[t];
+  const double xi = pos[i], yi = pos[P.n + i], zi = pos[2 * P.n + i];
+  const int ti = itype[i];
+  const bool qi = q[i] != 0.0;
+  int c[5] = {0, 0, 0, 0, 0};
+  unsigned bad = 0;
   for (int a = 0; a < P.nsx; a++) {
     int jx = cx + P.sx[a];
     jx = jx < 0 ? jx + P.ncx : (jx >= P.ncx ? jx - P.ncx : jx);
@@ -159,147 +262,66 @@ __device__ __forceinline__ void for_pairs(const ListParams &P, int t, const int 
       for (int cc = 0; cc < P.nsz; cc++) {
         int jz = cz + P.sz[cc];
         jz = jz < 0 ? jz + P.ncz : (jz >= P.ncz ? jz - P.ncz : jz);
-        int cell = (jx * P.ncy + jy) * P.ncz + jz;
-        int lo = cell_start[cell], hi = cell_start[cell + 1];
-        for (int u = lo; u < hi; u++) {
-          int j = cell_atoms[u];
-          if (j == i) continue;
-          if (!P.want_full && j < i) continue;
-          int intr = map[ti * P.ntypes + itype[j]];
-          bool qj = q[j] != 0.0;
-          bool lj_ok = intr >= 0;
-          bool el_ok = qi && qj;
-          if (!lj_ok && !el_ok) continue;
-          double dx = xi - pos[j], dy = yi - pos[n + j], dz = zi - pos[2 * n + j];
-          // image of CM3D's min image (needed for the shift code)
-          double sx = __dadd_rn(__dadd_rn(__dmul_rn(dx, P.hi[0]), __dmul_rn(dy, P.hi[1])), __dmul_rn(dz, P.hi[2]));
-          double sy = __dadd_rn(__dadd_rn(__dmul_rn(dx, P.hi[3]), __dmul_rn(dy, P.hi[4])), __dmul_rn(dz, P.hi[5]));
-          double sz = __dadd_rn(__dadd_rn(__dmul_rn(dx, P.hi[6]), __dmul_rn(dy, P.hi[7])), __dmul_rn(dz, P.hi[8]));
-          double mx = anint_ref(sx), my = anint_ref(sy), mz = anint_ref(sz);
-          sx = __dsub_rn(sx, mx);
-          sy = __dsub_rn(sy, my);
-          sz = __dsub_rn(sz, mz);
-          double ex = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[0]), __dmul_rn(sy, P.h[1])), __dmul_rn(sz, P.h[2]));
-          double ey = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[3]), __dmul_rn(sy, P.h[4])), __dmul_rn(sz, P.h[5]));
-          double ez = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[6]), __dmul_rn(sy, P.h[7])), __dmul_rn(sz, P.h[8]));
-          double r2 = r2_ref(ex, ey, ez);
-          int flags = 0;
-          if (lj_ok) {
-            if (r2 < icut[8 * intr + 5] && !excluded(i, j, excl_off, excl_idx)) {
-              flags |= 1;
-              if (r2 < icut[8 * intr + 4]) flags |= 2;
+        const int cell = (jx * P.ncy + jy) * P.ncz + jz;
+        // cell-corner shift of this stencil offset (k = -offset)
+        const float4 S = shift[(1 - P.sx[a]) * 9 + (1 - P.sy[b]) * 3 + (1 - P.sz[cc])];
+        const int lo = cell_start[cell], hi = cell_start[cell + 1];
+        for (int u0 = lo; u0 < hi; u0 += 32) {
+          const int u = u0 + lane;
+          int fl = 0, code = 13, j = -1;
+          if (u < hi) {
+            j = cell_atoms[u];
+            const float4 xj = xq[u];
+            const float dx = (xi4.x - xj.x) + S.x, dy = (xi4.y - xj.y) + S.y, dz = (xi4.z - xj.z) + S.z;
+            const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (j != i && r2f < P.lim2 && (P.want_full || j > i))
+              fl = exact_flags(P, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
+                               cexcl_off, cexcl_idx, cimg, code);
+          }
+          bad |= (fl >> 4) & 1;
+          const bool half = j > i;
+          const bool f0 = P.want_half && half && (fl & 1), f1 = P.want_half && half && (fl & 2);
+          const bool f2 = P.want_half && half && (fl & 4), f3 = P.want_half && half && (fl & 8);
+          const bool f4 = P.want_full && (fl & 5);
+          const unsigned b0 = __ballot_sync(0xffffffffu, f0), b1 = __ballot_sync(0xffffffffu, f1);
+          const unsigned b2 = __ballot_sync(0xffffffffu, f2), b3 = __ballot_sync(0xffffffffu, f3);
+          const unsigned b4 = __ballot_sync(0xffffffffu, f4);
+          if (!FILL) {
+            c[0] += __popc(b0); c[1] += __popc(b1); c[2] += __popc(b2); c[3] += __popc(b3); c[4] += __popc(b4);
+          } else {
+            const int2 pr = make_int2(i, j);
+            if (f0) l0[p[0] + __popc(b0 & lt_mask)] = pr;
+            if (f1) l1[p[1] + __popc(b1 & lt_mask)] = pr;
+            if (f2) l2[p[2] + __popc(b2 & lt_mask)] = pr;
+            if (f3) l3[p[3] + __popc(b3 & lt_mask)] = pr;
+            if (f4) {
+              uint32_t e = (uint32_t)rank[j] | ((uint32_t)code << ENT_CODE_SHIFT);
+              if (fl & 1) e |= ENT_LJ;
+              if (fl & 2) e |= ENT_LJS;
+              if (fl & 4) e |= ENT_EL;
+              if (fl & 8) e |= ENT_ELS;
+              nbr[p[4] + __popc(b4 & lt_mask)] = e;
             }
+            p[0] += __popc(b0); p[1] += __popc(b1); p[2] += __popc(b2); p[3] += __popc(b3); p[4] += __popc(b4);
           }
-          if (el_ok) {
-            if (r2 < P.rmaxl_skin2_e && !excluded(i, j, cexcl_off, cexcl_idx)) {
-              flags |= 4;
-              if (r2 < P.rmaxs_skin2_e) flags |= 8;
-            }
-          }
-          if (!flags) continue;
-          int4 cj = cimg[j];
-          int kx = (ci.y - cj.y - (int)mx) * P.ncx + (cx - (cj.x & 1023));
-          int ky = (ci.z - cj.z - (int)my) * P.ncy + (cy - ((cj.x >> 10) & 1023));
-          int kz = (ci.w - cj.w - (int)mz) * P.ncz + (cz - ((cj.x >> 20) & 1023));
-          // |k| <= 1 per dimension whenever r < rlist <= cell width; any
-          // other value would mean the geometry assumption broke: count it
-          // and use the zero shift rather than index past the shift table
-          int code = (kx + 1) * 9 + (ky + 1) * 3 + (kz + 1);
-          if (kx < -1 || kx > 1 || ky < -1 || ky > 1 || kz < -1 || kz > 1) {
-            code = 13;
-            flags |= 16;
-          }
-          f(i, j, flags, code);
         }
       }
     }
   }
-}
-
-__global__ void k_list_count(ListParams P, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
-                             const double *__restrict__ pos, const int *__restrict__ itype,
-                             const int *__restrict__ map, const double *__restrict__ icut,
-                             const double *__restrict__ q, const int *__restrict__ excl_off,
-                             const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
-                             const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, int ninter,
-                             int *__restrict__ cnt, const int *__restrict__ gate) {
-  if (gated_off(gate, 1)) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.n) return;
-  int c0 = 0, c1 = 0, c2 = 0, c3 = 0, c4 = 0;
-  for_pairs(P, t, cell_atoms, cell_start, pos, itype, map, icut, q, excl_off, excl_idx, cexcl_off,
-            cexcl_idx, cimg, ninter, [&](int i, int j, int fl, int) {
-              if (j > i) {
-                c0 += fl & 1;
-                c1 += (fl >> 1) & 1;
-                c2 += (fl >> 2) & 1;
-                c3 += (fl >> 3) & 1;
-              }
-              if (fl & 5) c4++;
-            });
-  cnt[t] = c0;
-  cnt[P.n + t] = c1;
-  cnt[2 * P.n + t] = c2;
-  cnt[3 * P.n + t] = c3;
-  cnt[4 * P.n + t] = P.want_full ? c4 : 0;
-}
-
-__global__ void k_list_fill(ListParams P, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
-                            const double *__restrict__ pos, const int *__restrict__ itype,
-                            const int *__restrict__ map, const double *__restrict__ icut,
-                            const double *__restrict__ q, const int *__restrict__ excl_off,
-                            const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
-                            const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, int ninter,
-                            const long long *__restrict__ off, const long long *__restrict__ tot,
-                            const int *__restrict__ rank, int2 *__restrict__ l0, int2 *__restrict__ l1,
-                            int2 *__restrict__ l2, int2 *__restrict__ l3, uint32_t *__restrict__ nbr,
-                            long long *__restrict__ stat, int *__restrict__ halt,
-                            const int *__restrict__ gate) {
-  if (gated_off(gate, 1)) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= P.n) return;
-  // if any list outgrew its capacity nothing is written and the step halts:
-  // the host grows the buffers and finishes the step (see run_step)
-  bool ok0 = tot[0] <= P.cap[0], ok1 = tot[1] <= P.cap[1], ok2 = tot[2] <= P.cap[2],
-       ok3 = tot[3] <= P.cap[3], ok4 = tot[4] <= P.cap[4];
-  if (!(ok0 && ok1 && ok2 && ok3 && ok4)) {
-    if (t == 0) {
-      atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
-      if (halt) *halt = 1;
-    }
-    return;
+  if (FILL) {
+    if (bad) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
+  } else if (lane == 0) {
+    for (int k = 0; k < 5; k++) cnt[(size_t)k * P.n + t] = c[k];
   }
-  long long p0 = off[t], p1 = off[(P.n + 1) + t], p2 = off[2 * (P.n + 1) + t],
-            p3 = off[3 * (P.n + 1) + t], p4 = off[4 * (P.n + 1) + t];
-  for_pairs(P, t, cell_atoms, cell_start, pos, itype, map, icut, q, excl_off, excl_idx, cexcl_off,
-            cexcl_idx, cimg, ninter, [&](int i, int j, int fl, int code) {
-              if (j > i) {
-                int2 pr = make_int2(i, j);
-                if ((fl & 1) && ok0) l0[p0++] = pr;
-                if ((fl & 2) && ok1) l1[p1++] = pr;
-                if ((fl & 4) && ok2) l2[p2++] = pr;
-                if ((fl & 8) && ok3) l3[p3++] = pr;
-              }
-              if (fl & 16) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
-              if (P.want_full && (fl & 5) && ok4) {
-                uint32_t e = (uint32_t)rank[j] | ((uint32_t)code << ENT_CODE_SHIFT);
-                if (fl & 1) e |= ENT_LJ;
-                if (fl & 2) e |= ENT_LJS;
-                if (fl & 4) e |= ENT_EL;
-                if (fl & 8) e |= ENT_ELS;
-                nbr[p4++] = e;
-              }
-            });
 }
 
-// sorted-order arrays of the mixed engine: rank, type, FP64 cell corner
-// (the cell origin in Cartesian coordinates, held fixed until the next
-// rebuild) and the first FP32 cell-relative coordinates
+// sorted-order arrays: rank, type, the FP64 corner of the atom's cell (held
+// fixed until the next rebuild) and FP32 cell-relative coordinates + charge
 __global__ void k_sorted_init(int n, const int *__restrict__ cell_atoms, const int4 *__restrict__ cimg,
                               const double *__restrict__ h, int ncx, int ncy, int ncz,
-                              const int *__restrict__ itype, int *__restrict__ rank,
-                              int *__restrict__ styp, double *__restrict__ corner,
-                              const int *__restrict__ gate) {
+                              const int *__restrict__ itype, const double *__restrict__ pos,
+                              const double *__restrict__ q, int *__restrict__ rank, int *__restrict__ styp,
+                              double *__restrict__ corner, float4 *__restrict__ xq, const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -308,9 +330,13 @@ __global__ void k_sorted_init(int n, const int *__restrict__ cell_atoms, const i
   double o0 = (double)ci.y + (double)(ci.x & 1023) / ncx;
   double o1 = (double)ci.z + (double)((ci.x >> 10) & 1023) / ncy;
   double o2 = (double)ci.w + (double)((ci.x >> 20) & 1023) / ncz;
-  corner[t] = h[0] * o0 + h[1] * o1 + h[2] * o2;
-  corner[n + t] = h[3] * o0 + h[4] * o1 + h[5] * o2;
-  corner[2 * n + t] = h[6] * o0 + h[7] * o1 + h[8] * o2;
+  double c0 = h[0] * o0 + h[1] * o1 + h[2] * o2;
+  double c1 = h[3] * o0 + h[4] * o1 + h[5] * o2;
+  double c2 = h[6] * o0 + h[7] * o1 + h[8] * o2;
+  corner[t] = c0;
+  corner[n + t] = c1;
+  corner[2 * n + t] = c2;
+  xq[t] = make_float4((float)(pos[i] - c0), (float)(pos[n + i] - c1), (float)(pos[2 * n + i] - c2), (float)q[i]);
   rank[i] = t;
   styp[t] = itype[i];
 }
@@ -365,13 +391,32 @@ int list_setup(Ctx *c) {
   CK(cudaMalloc(&c->corner, sizeof(double) * 3 * (size_t)c->n));
   CK(cudaMalloc(&c->xq, sizeof(float4) * (size_t)c->n));
   CK(cudaMalloc(&c->cimg, sizeof(int4) * (size_t)c->n));
+  // the 27 cell-corner shifts H k / nc, k in {-1, 0, 1}^3 (also used by the
+  // mixed pair kernel)
+  std::vector<float4> sh(27);
+  for (int a = -1; a <= 1; a++)
+    for (int b = -1; b <= 1; b++)
+      for (int d = -1; d <= 1; d++) {
+        double f0 = (double)a / c->nc[0], f1 = (double)b / c->nc[1], f2 = (double)d / c->nc[2];
+        const double *h = c->hmat;
+        sh[(a + 1) * 9 + (b + 1) * 3 + (d + 1)] =
+            make_float4((float)(h[0] * f0 + h[1] * f1 + h[2] * f2), (float)(h[3] * f0 + h[4] * f1 + h[5] * f2),
+                        (float)(h[6] * f0 + h[7] * f1 + h[8] * f2), 0.f);
+      }
+  CK(cudaMalloc(&c->shift, sizeof(float4) * 27));
+  CK(cudaMemcpy(c->shift, sh.data(), sizeof(float4) * 27, cudaMemcpyHostToDevice));
   return CM3D_NB_OK;
 }
 
-// grow list buffers to hold at least `need` entries (with 30% headroom)
+// grow list buffers to hold at least `need` entries (with 50% headroom)
 static int grow(Ctx *c, int which, long long need) {
   if (need <= c->lcap[which]) return CM3D_NB_OK;
-  long long cap = need + need / 3 + 1024;
+  long long cap = need + need / 2 + 4096;
+  if (c->graph) {
+    // a captured step holds the old buffer addresses
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
   if (which < 4) {
     if (c->lst[which]) cudaFree(c->lst[which]);
     c->lst[which] = nullptr;
@@ -387,7 +432,7 @@ static int grow(Ctx *c, int which, long long need) {
   return CM3D_NB_OK;
 }
 
-static ListParams params(Ctx *c) {
+static ListParams params(Ctx *c, bool want_half) {
   ListParams P;
   P.n = c->n;
   P.ntypes = c->ntypes;
@@ -403,17 +448,28 @@ static ListParams params(Ctx *c) {
   }
   P.rmaxl_skin2_e = c->ncharge > 0 ? c->rmaxl_skin2_e : -1.0;
   P.rmaxs_skin2_e = c->ncharge > 0 ? c->rmaxs_skin2_e : -1.0;
+  // with three or more cells per direction the stencil neighbour's image is
+  // the minimum image of every pair in range, so the FP32 prefilter is exact
+  // up to rounding; with fewer cells every candidate goes to the FP64 test
+  const bool pre = c->nc[0] >= 3 && c->nc[1] >= 3 && c->nc[2] >= 3;
+  const double rl = c->rlist_max + 1e-3;
+  P.lim2 = pre ? (float)(rl * rl) : INFINITY;
   P.want_full = c->mode == CM3D_NB_MIXED;
+  P.want_half = want_half;
   for (int k = 0; k < LT_COUNT; k++) P.cap[k] = c->lcap[k];
   return P;
 }
 
-// Build all lists.  With device_flag the kernels are gated on the device
-// rebuild flag (for graph replay) and capacity is not re-checked on the host.
+// Build the lists from the current positions.  With device_flag the kernels
+// are gated on the device rebuild flag (graph replay) and the capacities are
+// not re-checked on the host.  The plain engine always builds CM3D's half
+// lists (its pair kernels walk them); the mixed engine builds its full list
+// and the half lists only when asked (export / parity checks).
 int build_lists(Ctx *c, bool device_flag) {
   const int n = c->n;
   const int B = 256;
   const int *gate = device_flag ? c->istate : nullptr;
+  const bool want_half = c->mode == CM3D_NB_PLAIN_FP64 || c->want_half;
   cudaEvent_t e0;
   tbegin(c, 2, &e0);
   int4 *cimg = c->cimg;
@@ -426,17 +482,17 @@ int build_lists(Ctx *c, bool device_flag) {
   k_scan<int, int><<<dim3(1, 1), 1024, 0, c->st>>>(c->cell_cursor, c->cell_start, nullptr, c->ncells, gate);
   CK(cudaMemsetAsync(c->cell_cursor, 0, sizeof(int) * ((size_t)c->ncells + 1), c->st));
   k_cell_fill<<<grid_for(n, B), B, 0, c->st>>>(n, c->cell_of, c->cell_start, c->cell_cursor, c->cell_atoms, gate);
-  k_cell_sort<<<grid_for(c->ncells, 128), 128, 0, c->st>>>(c->ncells, c->cell_start, c->cell_atoms, gate);
-  c->launches += 4;
-  if (c->mode == CM3D_NB_MIXED) {
-    k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->cell_atoms, cimg, dhmat, c->nc[0], c->nc[1],
-                                                    c->nc[2], c->itype, c->rank, c->styp, c->corner, gate);
-    c->launches++;
-  }
-  ListParams P = params(c);
-  k_list_count<<<grid_for(n, 128), 128, 0, c->st>>>(P, c->cell_atoms, c->cell_start, c->pos, c->itype, c->map,
-                                                     c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off,
-                                                     c->cexcl_idx, cimg, c->ninter, c->cnt, gate);
+  k_cell_sort<<<c->ncells, 256, 0, c->st>>>(c->ncells, c->cell_start, c->cell_atoms, gate);
+  k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->cell_atoms, cimg, dhmat, c->nc[0], c->nc[1], c->nc[2],
+                                                  c->itype, c->pos, c->q, c->rank, c->styp, c->corner, c->xq,
+                                                  gate);
+  c->launches += 5;
+  ListParams P = params(c, want_half);
+  const long long warps_threads = 32LL * n;
+  k_list_warp<false><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
+      P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
+      c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->cnt, nullptr, nullptr, c->rank, nullptr, nullptr,
+      nullptr, nullptr, nullptr, c->stat, nullptr, gate);
   k_scan<int, long long><<<dim3(1, 5), 1024, 0, c->st>>>(c->cnt, c->off, c->ltot, n, gate);
   c->launches += 2;
   CKL(c);
@@ -448,15 +504,17 @@ int build_lists(Ctx *c, bool device_flag) {
       if (rc) return rc;
       c->hcount[k] = c->h_ltot[k];
     }
-    P = params(c);
+    P = params(c, want_half);
   }
-  k_list_fill<<<grid_for(n, 128), 128, 0, c->st>>>(P, c->cell_atoms, c->cell_start, c->pos, c->itype, c->map,
-                                                    c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off,
-                                                    c->cexcl_idx, cimg, c->ninter, c->off, c->ltot, c->rank,
-                                                    c->lst[0], c->lst[1], c->lst[2], c->lst[3], c->nbr,
-                                                    c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
-  k_snapshot<<<grid_for(3LL * n, B), B, 0, c->st>>>(3 * n, c->pos, c->dxn, gate, c->istate, c->stat);
-  c->launches += 2;
+  k_list_warp<true><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
+      P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
+      c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, nullptr, c->off, c->ltot, c->rank, c->lst[0], c->lst[1],
+      c->lst[2], c->lst[3], c->nbr, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+  if (!c->no_snapshot) {
+    k_snapshot<<<grid_for(3LL * n, B), B, 0, c->st>>>(3 * n, c->pos, c->dxn, gate, c->istate, c->stat);
+    c->launches++;
+  }
+  c->launches++;
   CKL(c);
   tend(c, 2, e0);
   if (!device_flag) {

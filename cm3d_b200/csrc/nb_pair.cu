@@ -14,9 +14,12 @@
 //   * the list is full (both directions), so a group of TPA lanes owns atom i
 //     and reduces its force with warp shuffles: no atomics, every force is
 //     written exactly once;
-//   * interpolation coefficients are FP32 float4 tables held in shared memory;
+//   * interpolation coefficients are FP32 float4 tables held in shared memory,
+//     loaded once per block: the grid is persistent (resident blocks walk
+//     the atoms), so the table load is paid once per SM, not per atom group;
 //   * forces are summed per lane in FP32 over chunks of 16 pairs and then in
-//     FP64; energies and virials are reduced in FP64 across lanes.
+//     FP64; energies and virials are summed per atom in FP32 and written as
+//     per-atom partials that k_ereduce adds up in FP64 in a fixed order.
 #include "nb_common.cuh"
 
 namespace cm3d {
@@ -43,13 +46,18 @@ __device__ __forceinline__ float poly(float p, float c0, float a, float b) {
   return fmaf(p, fmaf(p, b, a), c0);
 }
 
+// Per-atom energy/virial partials (EP_* rows of epart, FP32, half-weighted
+// because every pair is seen from both ends), summed by k_ereduce in FP64.
+enum { EP_ELJ = 0, EP_ELJH, EP_VL0, EP_VL1, EP_VL2, EP_VL4, EP_VL5, EP_VL8,
+       EP_EEL, EP_QQ, EP_VE0, EP_VE1, EP_VE2, EP_VE4, EP_VE5, EP_VE8, EP_COUNT };
+
 template <int TPA, bool SMALLBOX, bool NEED_S>
 __global__ void __launch_bounds__(256) k_pair_mixed(
     MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const long long *__restrict__ off, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
     const float4 *__restrict__ gte, double *__restrict__ fout, double *__restrict__ fshort,
-    double *__restrict__ acc, long long *__restrict__ stat, const int *__restrict__ gs) {
+    float *__restrict__ epart, long long *__restrict__ stat, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
   float4 *shift = sm;                                   // 27
@@ -74,75 +82,47 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
   __syncthreads();
 
   const int g = threadIdx.x % TPA;
-  const int t = (blockIdx.x * blockDim.x + threadIdx.x) / TPA;
-  const bool active = t < P.n;
-  double Fx = 0, Fy = 0, Fz = 0, Sx = 0, Sy = 0, Sz = 0;
-  float elj = 0, eljh = 0, eel = 0, qqs = 0;
-  float vl0 = 0, vl1 = 0, vl2 = 0, vl4 = 0, vl5 = 0, vl8 = 0;
-  float ve0 = 0, ve1 = 0, ve2 = 0, ve4 = 0, ve5 = 0, ve8 = 0;
+  const int groups = blockDim.x / TPA;
+  const uint32_t fl_lj = P.iflg == 1 ? ENT_LJ : ENT_LJS;
+  const uint32_t fl_el = P.iflg == 1 ? ENT_EL : ENT_ELS;
   unsigned under = 0;
-  if (active) {
-    const float4 xi = xq[t];
-    const int ti = styp[t];
-    const long long k0 = off[t], k1 = off[t + 1];
-    const uint32_t fl_lj = P.iflg == 1 ? ENT_LJ : ENT_LJS;
-    const uint32_t fl_el = P.iflg == 1 ? ENT_EL : ENT_ELS;
-    float fx = 0, fy = 0, fz = 0, sx = 0, sy = 0, sz = 0;
-    int cnt = 0;
-    for (long long k = k0 + g; k < k1; k += TPA) {
-      const uint32_t e = __ldg(nbr + k);
-      const int j = e & ENT_JMASK;
-      const float4 xj = xq[j];
-      const float4 sh = shift[(e >> ENT_CODE_SHIFT) & 31];
-      float dx = (xi.x - xj.x) + sh.x;
-      float dy = (xi.y - xj.y) + sh.y;
-      float dz = (xi.z - xj.z) + sh.z;
-      if (SMALLBOX) {
-        float s0 = P.hiF[0] * dx + P.hiF[1] * dy + P.hiF[2] * dz;
-        float s1 = P.hiF[3] * dx + P.hiF[4] * dy + P.hiF[5] * dz;
-        float s2 = P.hiF[6] * dx + P.hiF[7] * dy + P.hiF[8] * dz;
-        s0 -= rintf(s0);
-        s1 -= rintf(s1);
-        s2 -= rintf(s2);
-        dx = P.hF[0] * s0 + P.hF[1] * s1 + P.hF[2] * s2;
-        dy = P.hF[3] * s0 + P.hF[4] * s1 + P.hF[5] * s2;
-        dz = P.hF[6] * s0 + P.hF[7] * s1 + P.hF[8] * s2;
-      }
-      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      float ftot = 0.f, fsh = 0.f;
-      if ((e & fl_el) && (P.mask & 2) && r2 < P.rc2_el) {
-        float p = fmaf(r2, P.dx2c, -P.offc);
-        int kk = (int)p;
-        if (kk < 1) {
-          under++;
-          kk = 1;
-          p = 1.f;
+  // persistent: every lane group walks atoms blockIdx-strided
+  for (int tb = blockIdx.x * groups; tb < P.n; tb += gridDim.x * groups) {
+    const int t = tb + threadIdx.x / TPA;
+    const bool active = t < P.n;
+    double Fx = 0, Fy = 0, Fz = 0, Sx = 0, Sy = 0, Sz = 0;
+    float e[EP_COUNT];
+#pragma unroll
+    for (int k = 0; k < EP_COUNT; k++) e[k] = 0.f;
+    if (active) {
+      const float4 xi = xq[t];
+      const int ti = styp[t];
+      const long long k0 = off[t], k1 = off[t + 1];
+      float fx = 0, fy = 0, fz = 0, sx = 0, sy = 0, sz = 0;
+      int cnt = 0;
+      for (long long k = k0 + g; k < k1; k += TPA) {
+        const uint32_t en = __ldg(nbr + k);
+        const int j = en & ENT_JMASK;
+        const float4 xj = xq[j];
+        const float4 sh = shift[(en >> ENT_CODE_SHIFT) & 31];
+        float dx = (xi.x - xj.x) + sh.x;
+        float dy = (xi.y - xj.y) + sh.y;
+        float dz = (xi.z - xj.z) + sh.z;
+        if (SMALLBOX) {
+          float s0 = P.hiF[0] * dx + P.hiF[1] * dy + P.hiF[2] * dz;
+          float s1 = P.hiF[3] * dx + P.hiF[4] * dy + P.hiF[5] * dz;
+          float s2 = P.hiF[6] * dx + P.hiF[7] * dy + P.hiF[8] * dz;
+          s0 -= rintf(s0);
+          s1 -= rintf(s1);
+          s2 -= rintf(s2);
+          dx = P.hF[0] * s0 + P.hF[1] * s1 + P.hF[2] * s2;
+          dy = P.hF[3] * s0 + P.hF[4] * s1 + P.hF[5] * s2;
+          dz = P.hF[6] * s0 + P.hF[7] * s1 + P.hF[8] * s2;
         }
-        p -= (float)kk;
-        const float4 c0 = te[2 * kk];
-        const float qq = xi.w * xj.w;
-        const float fe = qq * poly(p, c0.x, c0.y, c0.z);
-        ftot += fe;
-        if (P.iflg == 1) {
-          const float4 c1 = te[2 * kk + 1];
-          eel = fmaf(qq, poly(p, c0.w, c1.x, c1.y), eel);
-          qqs += qq;
-          const float fdx = fe * dx, fdy = fe * dy, fdz = fe * dz;
-          ve0 = fmaf(fdx, dx, ve0);
-          ve1 = fmaf(fdx, dy, ve1);
-          ve2 = fmaf(fdx, dz, ve2);
-          ve4 = fmaf(fdy, dy, ve4);
-          ve5 = fmaf(fdy, dz, ve5);
-          ve8 = fmaf(fdz, dz, ve8);
-          if (NEED_S) fsh += fe;           // force_e's switch is never engaged
-        }
-      }
-      if ((e & fl_lj) && (P.mask & 1)) {
-        const int in = map[ti * P.ntypes + styp[j]];
-        const float *fc = fcut + 8 * in;
-        const float rmax2 = P.iflg == 1 ? fc[0] : fc[4];
-        if (r2 < rmax2) {
-          float p = fmaf(r2, fc[2], -fc[1]);
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        float ftot = 0.f, fsh = 0.f;
+        if ((en & fl_el) && (P.mask & 2) && r2 < P.rc2_el) {
+          float p = fmaf(r2, P.dx2c, -P.offc);
           int kk = (int)p;
           if (kk < 1) {
             under++;
@@ -150,92 +130,158 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
             p = 1.f;
           }
           p -= (float)kk;
-          const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
-          const float4 a0 = T[0], a1 = T[1];
-          const float f = poly(p, a0.x, a0.y, a0.z);
-          float swv = 1.f;
-          if ((NEED_S || P.iflg == 0) && r2 > fc[3]) {
-            const float4 a2 = T[2];
-            swv = poly(p, a1.z, a1.w, a2.x);
-          }
+          const float4 c0 = te[2 * kk];
+          const float qq = xi.w * xj.w;
+          const float fe = qq * poly(p, c0.x, c0.y, c0.z);
+          ftot += fe;
           if (P.iflg == 1) {
-            ftot += f;
-            const float v = poly(p, a0.w, a1.x, a1.y);
-            elj += v;
-            eljh += v - fc[5];
-            const float fdx = f * dx, fdy = f * dy, fdz = f * dz;
-            vl0 = fmaf(fdx, dx, vl0);
-            vl1 = fmaf(fdx, dy, vl1);
-            vl2 = fmaf(fdx, dz, vl2);
-            vl4 = fmaf(fdy, dy, vl4);
-            vl5 = fmaf(fdy, dz, vl5);
-            vl8 = fmaf(fdz, dz, vl8);
-            if (NEED_S) fsh += f * swv;
-          } else {
-            ftot += f * swv;
+            const float4 c1 = te[2 * kk + 1];
+            e[EP_EEL] = fmaf(qq, poly(p, c0.w, c1.x, c1.y), e[EP_EEL]);
+            e[EP_QQ] += qq;
+            const float fdx = fe * dx, fdy = fe * dy, fdz = fe * dz;
+            e[EP_VE0] = fmaf(fdx, dx, e[EP_VE0]);
+            e[EP_VE1] = fmaf(fdx, dy, e[EP_VE1]);
+            e[EP_VE2] = fmaf(fdx, dz, e[EP_VE2]);
+            e[EP_VE4] = fmaf(fdy, dy, e[EP_VE4]);
+            e[EP_VE5] = fmaf(fdy, dz, e[EP_VE5]);
+            e[EP_VE8] = fmaf(fdz, dz, e[EP_VE8]);
+            if (NEED_S) fsh += fe;           // force_e's switch is never engaged
           }
         }
-      }
-      // F_i = -f d  (md_fnopol.c:227-229)
-      fx = fmaf(-ftot, dx, fx);
-      fy = fmaf(-ftot, dy, fy);
-      fz = fmaf(-ftot, dz, fz);
-      if (NEED_S) {
-        sx = fmaf(-fsh, dx, sx);
-        sy = fmaf(-fsh, dy, sy);
-        sz = fmaf(-fsh, dz, sz);
-      }
-      if (++cnt == 16) {
-        Fx += fx; Fy += fy; Fz += fz;
-        fx = fy = fz = 0.f;
-        if (NEED_S) {
-          Sx += sx; Sy += sy; Sz += sz;
-          sx = sy = sz = 0.f;
+        if ((en & fl_lj) && (P.mask & 1)) {
+          const int in = map[ti * P.ntypes + styp[j]];
+          const float *fc = fcut + 8 * in;
+          const float rmax2 = P.iflg == 1 ? fc[0] : fc[4];
+          if (r2 < rmax2) {
+            float p = fmaf(r2, fc[2], -fc[1]);
+            int kk = (int)p;
+            if (kk < 1) {
+              under++;
+              kk = 1;
+              p = 1.f;
+            }
+            p -= (float)kk;
+            const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
+            const float4 a0 = T[0], a1 = T[1];
+            const float f = poly(p, a0.x, a0.y, a0.z);
+            float swv = 1.f;
+            if ((NEED_S || P.iflg == 0) && r2 > fc[3]) {
+              const float4 a2 = T[2];
+              swv = poly(p, a1.z, a1.w, a2.x);
+            }
+            if (P.iflg == 1) {
+              ftot += f;
+              const float v = poly(p, a0.w, a1.x, a1.y);
+              e[EP_ELJ] += v;
+              e[EP_ELJH] += v - fc[5];
+              const float fdx = f * dx, fdy = f * dy, fdz = f * dz;
+              e[EP_VL0] = fmaf(fdx, dx, e[EP_VL0]);
+              e[EP_VL1] = fmaf(fdx, dy, e[EP_VL1]);
+              e[EP_VL2] = fmaf(fdx, dz, e[EP_VL2]);
+              e[EP_VL4] = fmaf(fdy, dy, e[EP_VL4]);
+              e[EP_VL5] = fmaf(fdy, dz, e[EP_VL5]);
+              e[EP_VL8] = fmaf(fdz, dz, e[EP_VL8]);
+              if (NEED_S) fsh += f * swv;
+            } else {
+              ftot += f * swv;
+            }
+          }
         }
-        cnt = 0;
+        // F_i = -f d  (md_fnopol.c:227-229)
+        fx = fmaf(-ftot, dx, fx);
+        fy = fmaf(-ftot, dy, fy);
+        fz = fmaf(-ftot, dz, fz);
+        if (NEED_S) {
+          sx = fmaf(-fsh, dx, sx);
+          sy = fmaf(-fsh, dy, sy);
+          sz = fmaf(-fsh, dz, sz);
+        }
+        if (++cnt == 16) {
+          Fx += fx; Fy += fy; Fz += fz;
+          fx = fy = fz = 0.f;
+          if (NEED_S) {
+            Sx += sx; Sy += sy; Sz += sz;
+            sx = sy = sz = 0.f;
+          }
+          cnt = 0;
+        }
+      }
+      Fx += fx; Fy += fy; Fz += fz;
+      if (NEED_S) {
+        Sx += sx; Sy += sy; Sz += sz;
       }
     }
-    Fx += fx; Fy += fy; Fz += fz;
-    if (NEED_S) {
-      Sx += sx; Sy += sy; Sz += sz;
-    }
-  }
-  // reduce atom i's force over its TPA lanes (aligned lane groups)
+    // reduce atom i's sums over its TPA lanes (aligned lane groups)
 #pragma unroll
-  for (int o = TPA / 2; o > 0; o >>= 1) {
-    Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
-    Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
-    Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
-    if (NEED_S) {
-      Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
-      Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
-      Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
+    for (int o = TPA / 2; o > 0; o >>= 1) {
+      Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+      Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+      Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+      if (NEED_S) {
+        Sx += __shfl_xor_sync(0xffffffffu, Sx, o);
+        Sy += __shfl_xor_sync(0xffffffffu, Sy, o);
+        Sz += __shfl_xor_sync(0xffffffffu, Sz, o);
+      }
+      if (P.iflg == 1) {
+#pragma unroll
+        for (int k = 0; k < EP_COUNT; k++) e[k] += __shfl_xor_sync(0xffffffffu, e[k], o);
+      }
     }
-  }
-  if (active && g == 0) {
-    const int i = sorig[t], n = P.n;
-    fout[i] += Fx;
-    fout[n + i] += Fy;
-    fout[2 * n + i] += Fz;
-    if (NEED_S && P.iflg == 1) {
-      fshort[i] += Sx;
-      fshort[n + i] += Sy;
-      fshort[2 * n + i] += Sz;
+    if (active && g == 0) {
+      const int i = sorig[t], n = P.n;
+      fout[i] += Fx;
+      fout[n + i] += Fy;
+      fout[2 * n + i] += Fz;
+      if (NEED_S && P.iflg == 1) {
+        fshort[i] += Sx;
+        fshort[n + i] += Sy;
+        fshort[2 * n + i] += Sz;
+      }
+      if (P.iflg == 1) {
+#pragma unroll
+        for (int k = 0; k < EP_COUNT; k++) epart[(size_t)k * n + t] = e[k];
+      }
     }
   }
   if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), (unsigned long long)under);
-  if (P.iflg == 1) {
-    // every pair was visited from both ends: halve energies and virials
-    double v[18] = {0.5 * elj, 0.5 * eljh, 0.5 * -(double)(vl0 + vl4 + vl8),
-                    -0.5 * vl0, -0.5 * vl1, -0.5 * vl2, -0.5 * vl4, -0.5 * vl5, -0.5 * vl8,
-                    0.5 * eel, 0.5 * ((double)eel - (double)P.tablast_e * (double)qqs),
-                    0.5 * -(double)(ve0 + ve4 + ve8),
-                    -0.5 * ve0, -0.5 * ve1, -0.5 * ve2, -0.5 * ve4, -0.5 * ve5, -0.5 * ve8};
-    const int slots[18] = {ACC_SPOTL, ACC_SPOTHL, ACC_SPRSL, ACC_SPRSLT + 0, ACC_SPRSLT + 1,
-                           ACC_SPRSLT + 2, ACC_SPRSLT + 4, ACC_SPRSLT + 5, ACC_SPRSLT + 8,
-                           ACC_SPOTE, ACC_SPOTHE, ACC_SPRSE, ACC_SPRSET + 0, ACC_SPRSET + 1,
-                           ACC_SPRSET + 2, ACC_SPRSET + 4, ACC_SPRSET + 5, ACC_SPRSET + 8};
-    block_acc<18>(v, acc, slots);
+}
+
+// FP64 sums of the per-atom partials into CM3D's accumulators (one block per
+// quantity, fixed order: deterministic).  Every pair was seen from both ends,
+// hence the factor 1/2; CM3D's virials are -sum d_a d_b f.
+__global__ void k_ereduce(int n, int mask, float tablast_e, const float *__restrict__ epart,
+                          double *__restrict__ acc, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  __shared__ double red[32];
+  const int q = blockIdx.x;
+  if (!((q < EP_EEL && (mask & 1)) || (q >= EP_EEL && (mask & 2)))) return;
+  double s = 0;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) s += (double)epart[(size_t)q * n + t];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+  s = warp_sum(s);
+  if (threadIdx.x != 0) return;
+  s *= 0.5;
+  switch (q) {
+    case EP_ELJ: atomicAdd(acc + ACC_SPOTL, s); break;
+    case EP_ELJH: atomicAdd(acc + ACC_SPOTHL, s); break;
+    case EP_VL0: atomicAdd(acc + ACC_SPRSLT + 0, -s); atomicAdd(acc + ACC_SPRSL, -s); break;
+    case EP_VL1: atomicAdd(acc + ACC_SPRSLT + 1, -s); break;
+    case EP_VL2: atomicAdd(acc + ACC_SPRSLT + 2, -s); break;
+    case EP_VL4: atomicAdd(acc + ACC_SPRSLT + 4, -s); atomicAdd(acc + ACC_SPRSL, -s); break;
+    case EP_VL5: atomicAdd(acc + ACC_SPRSLT + 5, -s); break;
+    case EP_VL8: atomicAdd(acc + ACC_SPRSLT + 8, -s); atomicAdd(acc + ACC_SPRSL, -s); break;
+    case EP_EEL: atomicAdd(acc + ACC_SPOTE, s); atomicAdd(acc + ACC_SPOTHE, s); break;
+    case EP_QQ: atomicAdd(acc + ACC_SPOTHE, -(double)tablast_e * s); break;
+    case EP_VE0: atomicAdd(acc + ACC_SPRSET + 0, -s); atomicAdd(acc + ACC_SPRSE, -s); break;
+    case EP_VE1: atomicAdd(acc + ACC_SPRSET + 1, -s); break;
+    case EP_VE2: atomicAdd(acc + ACC_SPRSET + 2, -s); break;
+    case EP_VE4: atomicAdd(acc + ACC_SPRSET + 4, -s); atomicAdd(acc + ACC_SPRSE, -s); break;
+    case EP_VE5: atomicAdd(acc + ACC_SPRSET + 5, -s); break;
+    case EP_VE8: atomicAdd(acc + ACC_SPRSET + 8, -s); atomicAdd(acc + ACC_SPRSE, -s); break;
   }
 }
 
@@ -253,16 +299,23 @@ static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
 template <int TPA, bool SB, bool NS>
 static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   const int B = 256;
-  long long threads = (long long)c->n * TPA;
-  int grid = grid_for(threads, B);
   static bool attr_set = false;
+  static int per_sm = 1;
   if (!attr_set) {
     cudaFuncSetAttribute(k_pair_mixed<TPA, SB, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
+  // persistent grid: as many resident blocks as the SMs hold, no more than
+  // the atoms need
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_mixed<TPA, SB, NS>, B, smem);
+  if (per_sm < 1) per_sm = 1;
+  long long need = ((long long)c->n * TPA + B - 1) / B;
+  long long grid = (long long)c->num_sms * per_sm;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
   k_pair_mixed<TPA, SB, NS><<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->off + 4 * ((size_t)c->n + 1),
                                                       c->nbr, c->shift, c->map, c->fcut, c->ftab_lj, c->ftab_el,
-                                                      fout, c->fxs, c->acc, c->stat, c->gate);
+                                                      fout, c->fxs, c->epart, c->stat, c->gate);
 }
 
 template <bool SB, bool NS>
@@ -325,6 +378,10 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   }
   tend(c, 0, e0);
   c->launches += 2;
+  if (iflg == 1) {
+    k_ereduce<<<EP_COUNT, 1024, 0, c->st>>>(c->n, mask, (float)c->tablast_e, c->epart, c->acc, c->gate);
+    c->launches++;
+  }
   CKL(c);
   return CM3D_NB_OK;
 }
@@ -393,23 +450,12 @@ int pair_setup(Ctx *c) {
   if (!tl.empty()) CK(cudaMemcpy(c->ftab_lj, tl.data(), sizeof(float4) * tl.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ftab_el, te.data(), sizeof(float4) * te.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->fcut, fc.data(), sizeof(float) * fc.size(), cudaMemcpyHostToDevice));
-  // cell shift for code (kx+1)*9 + (ky+1)*3 + (kz+1):  H (k / nc)
-  std::vector<float4> sh(27);
-  for (int a = -1; a <= 1; a++)
-    for (int b = -1; b <= 1; b++)
-      for (int d = -1; d <= 1; d++) {
-        double f0 = (double)a / c->nc[0], f1 = (double)b / c->nc[1], f2 = (double)d / c->nc[2];
-        const double *h = c->hmat;
-        sh[(a + 1) * 9 + (b + 1) * 3 + (d + 1)] =
-            make_float4((float)(h[0] * f0 + h[1] * f1 + h[2] * f2), (float)(h[3] * f0 + h[4] * f1 + h[5] * f2),
-                        (float)(h[6] * f0 + h[7] * f1 + h[8] * f2), 0.f);
-      }
-  CK(cudaMalloc(&c->shift, sizeof(float4) * 27));
-  CK(cudaMemcpy(c->shift, sh.data(), sizeof(float4) * 27, cudaMemcpyHostToDevice));
+  // (the 27 cell shifts H k / nc are set up with the cell grid, list_setup)
+  CK(cudaMalloc(&c->epart, sizeof(float) * EP_COUNT * (size_t)c->n));
   if (c->tpa == 0) {
-    // enough lane groups to fill the GPU, but at least 8 lanes per atom so a
-    // group reads a full 32-byte sector of the list
-    long long want = 148LL * 2048 * 2;
+    // 8 lanes per atom: a group reads a full 32-byte sector of the list; more
+    // lanes only for systems too small to fill the GPU
+    long long want = (long long)c->num_sms * 1024;
     int tpa = 8;
     while (tpa < 32 && (long long)c->n * tpa < want) tpa *= 2;
     c->tpa = tpa;

@@ -6,7 +6,11 @@ Tolerances
   plain FP64 engine   relative RMS force error <= 1e-11 (only the summation
                       order differs from CM3D), energies relative <= 1e-10
   mixed engine        relative RMS force error <= 1e-5 against CM3D's FP64
-                      energies relative <= 1e-5
+                      energies relative <= 1e-5,
+                      virials (and the pressure) relative <= 5e-5: a virial
+                      sums -r^2 f over ~1e5 pairs of both signs, so the FP32
+                      rounding of each pair term (~5e-7) is amplified by the
+                      cancellation more than in a per-atom force
 """
 import hashlib
 
@@ -25,6 +29,8 @@ MODES = [_abi.PLAIN_FP64, _abi.MIXED]
 MODE_ID = {_abi.PLAIN_FP64: "plain", _abi.MIXED: "mixed"}
 FTOL = {_abi.PLAIN_FP64: 1e-11, _abi.MIXED: 1e-5}
 ETOL = {_abi.PLAIN_FP64: 1e-10, _abi.MIXED: 1e-5}
+VTOL = {_abi.PLAIN_FP64: 1e-10, _abi.MIXED: 5e-5}
+VIRIAL_KEYS = {"winter", "welec", "W", "prsi"}
 ALL = ["lj2", "lj256", "abutane", "argon864", "water216", "binary256", "water4096"]
 DYN = ["lj2", "lj256", "argon864", "water216", "binary256", "water4096"]   # no frozen atoms / torsions
 
@@ -76,20 +82,22 @@ def test_force_terms(engine_lib, name, mode):
     e.zero_forces(_abi.FXS)
     e.force_ter(1)
     assert rel_rms(e.forces(_abi.FXL), xyz(d, "f_lj_l"), fs) <= tol
-    assert rel_rms(e.forces(_abi.FXS), xyz(d, "f_lj_s"), fs) <= tol
+    if "f_lj_s" in d:                  # not stored for the large fixtures
+        assert rel_rms(e.forces(_abi.FXS), xyz(d, "f_lj_s"), fs) <= tol
     v = e.getsvirter()
     assert close(v["vinter"], d["lj_vinter"][0], ETOL[mode])
     assert close(v["vhinter"], d["lj_vhinter"][0], ETOL[mode])
-    assert close(v["winter"], d["lj_winter"][0], ETOL[mode])
+    assert close(v["winter"], d["lj_winter"][0], VTOL[mode])
     # real-space Ewald: force_ter_e(1)
     e.zero_forces(_abi.FXL)
     e.zero_forces(_abi.FXS)
     e.force_ter_e(1)
     assert rel_rms(e.forces(_abi.FXL), xyz(d, "f_el_l"), fs) <= tol
-    assert rel_rms(e.forces(_abi.FXS), xyz(d, "f_el_s"), fs) <= tol
+    if "f_el_s" in d:
+        assert rel_rms(e.forces(_abi.FXS), xyz(d, "f_el_s"), fs) <= tol
     v = e.getsvirter_e()
     assert close(v["velec"], d["el_velec"][0], ETOL[mode])
-    assert close(v["welec"], d["el_welec"][0], ETOL[mode])
+    assert close(v["welec"], d["el_welec"][0], VTOL[mode])
     if int(d["ncharge"][0]) > 0:
         e.zero_forces(_abi.FXL)
         e.fk_ewald()
@@ -128,7 +136,8 @@ def test_level1_forces_and_energies(engine_lib, name, mode):
     e.force(2)
     en = e.energies()
     for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke"):
-        assert close(en[k], float(d[f"e0_{k}"][0]), ETOL[mode]), k
+        tol = VTOL[mode] if k in VIRIAL_KEYS else ETOL[mode]
+        assert close(en[k], float(d[f"e0_{k}"][0]), tol), k
     e.close()
 
 
