@@ -23,6 +23,10 @@
 // the only FP32 error is that of the sin/cos of a number in [-pi, pi) and of
 // the recurrence along one row.  The plain mode does everything in FP64 with
 // CM3D's expressions (rk = x aka + y akb + z akc, md_ewald.c:264).
+#include <math.h>
+
+#include <mutex>
+
 #include "nb_common.cuh"
 
 namespace cm3d {
@@ -470,4 +474,288 @@ int kspace_forces(Ctx *c) {
   return CM3D_NB_OK;
 }
 
+// ------------------------------------------------- no-allocation variant
+// cm3d_nb_fk_ewald_noalloc runs the mixed-mode kernels above on one fixed
+// scratch area in the library's static device memory instead of the buffers
+// of an engine context, so a call allocates nothing.  Its size is set by the
+// limits below (about 2.9 MiB in all).
+constexpr int NA_MAX_CHARGES = CM3D_NB_NOALLOC_MAX_CHARGES;
+constexpr int NA_MAX_KMAX = CM3D_NB_NOALLOC_MAX_KMAX;
+constexpr int NA_MAX_K = 7073;                   // k-vectors of ewald_setup at kmax 15
+constexpr int NA_MAX_ROWS = (NA_MAX_KMAX + 1) * (2 * NA_MAX_KMAX + 1);
+constexpr int NA_MAX_TILES = (NA_MAX_CHARGES + KS_THREADS * KS_A - 1) / (KS_THREADS * KS_A);
+constexpr int NA_MAX_DEVICES = 64;
+static_assert(2 * NA_MAX_KMAX + 1 <= MAX_ROWLEN, "a k row must fit the structure-factor kernel");
+
+constexpr size_t na_align(size_t b) { return (b + 255) & ~(size_t)255; }
+constexpr size_t NA_OFF_KFRAC = 0;
+constexpr size_t NA_OFF_SPART = NA_OFF_KFRAC + na_align(sizeof(uint4) * NA_MAX_CHARGES);
+constexpr size_t NA_OFF_SK = NA_OFF_SPART + na_align(sizeof(double2) * NA_MAX_TILES * NA_MAX_K);
+constexpr size_t NA_OFF_AKF = NA_OFF_SK + na_align(sizeof(double2) * NA_MAX_K);
+constexpr size_t NA_OFF_KABC = NA_OFF_AKF + na_align(sizeof(float2) * NA_MAX_K);
+constexpr size_t NA_OFF_ROWS = NA_OFF_KABC + na_align(sizeof(int) * 3 * NA_MAX_K);
+constexpr size_t NA_OFF_ROWK0 = NA_OFF_ROWS + na_align(sizeof(int4) * NA_MAX_ROWS);
+constexpr size_t NA_OFF_ACC = NA_OFF_ROWK0 + na_align(sizeof(int) * NA_MAX_ROWS);
+constexpr size_t NA_BYTES = NA_OFF_ACC + na_align(sizeof(double) * (ACC_COUNT + 9));
+
+// the scratch area: per-atom fixed-point phases, per-tile partial S(k), S(k),
+// A(k), the k-vectors and rows of ewald_setup's set, and the accumulators
+// (+ H^-1 at ACC_COUNT, where the k-space kernels read it)
+static __device__ __align__(256) unsigned char g_na_scratch[NA_BYTES];
+
+struct Mat9 {
+  double m[9];
+};
+
+__host__ __device__ inline int na_isqrt(int r) {
+  int m = (int)sqrt((double)r);
+  while (m * m > r) m--;
+  while ((m + 1) * (m + 1) <= r) m++;
+  return m;
+}
+
+// ewald_setup's loops (md_ewald.c:93-114) as rows: candidate c is the pair
+// (i, j) = (c / (2 kmax + 1), c % (2 kmax + 1) - kmax) of the two outer
+// loops; its k's are the consecutive kc with i^2 + j^2 + kc^2 <= kmax^2
+// (kc >= 1 when i = j = 0).  Returns the row length, 0 for an empty row.
+__host__ __device__ inline int na_row(int kmax, int c, int *i, int *j, int *kc0) {
+  const int w = 2 * kmax + 1;
+  *i = c / w;
+  *j = c % w - kmax;
+  *kc0 = 0;
+  if (*i == 0 && *j < 0) return 0;
+  const int r2 = kmax * kmax - *i * *i - *j * *j;
+  if (r2 < 0) return 0;
+  const int m = na_isqrt(r2);
+  if (*i == 0 && *j == 0) {
+    *kc0 = 1;
+    return m;
+  }
+  *kc0 = -m;
+  return 2 * m + 1;
+}
+
+// one block: the rows, row offsets and per-k (ka, kb, kc) of the k set in
+// CM3D's order (a block-wide scan over the candidates), H^-1, and zeroed
+// reciprocal-space accumulators
+constexpr int NA_SETUP_THREADS = 512;
+__global__ void __launch_bounds__(NA_SETUP_THREADS) k_na_setup(int kmax, Mat9 hmati, int4 *__restrict__ rows,
+                                                               int *__restrict__ row_k0, int *__restrict__ ka,
+                                                               int *__restrict__ kb, int *__restrict__ kc,
+                                                               double *__restrict__ acc) {
+  __shared__ int wsum[2][NA_SETUP_THREADS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ncand = (kmax + 1) * (2 * kmax + 1);
+  int rbase = 0, kbase = 0;
+  for (int base = 0; base < ncand; base += NA_SETUP_THREADS) {
+    const int c = base + threadIdx.x;
+    int i = 0, j = 0, kc0 = 0, len = 0;
+    if (c < ncand) len = na_row(kmax, c, &i, &j, &kc0);
+    int fr = len > 0 ? 1 : 0, fk = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int a = __shfl_up_sync(0xffffffffu, fr, o), b = __shfl_up_sync(0xffffffffu, fk, o);
+      if (lane >= o) {
+        fr += a;
+        fk += b;
+      }
+    }
+    if (lane == 31) {
+      wsum[0][w] = fr;
+      wsum[1][w] = fk;
+    }
+    __syncthreads();
+    int pr = 0, pk = 0, tr = 0, tk = 0;
+    for (int q2 = 0; q2 < NA_SETUP_THREADS / 32; q2++) {
+      if (q2 < w) {
+        pr += wsum[0][q2];
+        pk += wsum[1][q2];
+      }
+      tr += wsum[0][q2];
+      tk += wsum[1][q2];
+    }
+    if (len > 0) {
+      const int r = rbase + pr + fr - 1;
+      const int k0 = kbase + pk + fk - len;
+      rows[r] = make_int4(i, j, kc0, len);
+      row_k0[r] = k0;
+      for (int t = 0; t < len; t++) {
+        ka[k0 + t] = i;
+        kb[k0 + t] = j;
+        kc[k0 + t] = kc0 + t;
+      }
+    }
+    rbase += tr;
+    kbase += tk;
+    __syncthreads();
+  }
+  if (threadIdx.x < 9) acc[ACC_COUNT + threadIdx.x] = hmati.m[threadIdx.x];
+  if (threadIdx.x < 11) acc[ACC_VK + threadIdx.x] = 0.0;
+}
+
+// fk_ewald's totals (md_ewald.c:336-348) into the caller's 11 doubles
+__global__ void k_na_finish(const double *__restrict__ acc, double six, double self, double *__restrict__ out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const double vk = acc[ACC_VK], vp = acc[ACC_VP];
+  out[0] = vk + six + self;
+  out[1] = vp + 3. * (vk + six);
+  for (int k = 0; k < 9; k++) out[2 + k] = acc[ACC_VPT + k] + (k % 4 == 0 ? vk + six : 0.0);
+}
+
+// per-device set-up, once: the scratch area's address (cudaGetSymbolAddress
+// with the device current) and the force kernel's shared-memory limit
+static std::once_flag g_na_once[NA_MAX_DEVICES];
+static cudaError_t g_na_err[NA_MAX_DEVICES];
+static const char *g_na_what[NA_MAX_DEVICES];
+static unsigned char *g_na_ptr[NA_MAX_DEVICES];
+
+static void na_device_setup(int dev) {
+  void *p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
+  g_na_what[dev] = "cudaGetSymbolAddress(scratch)";
+  if (e == cudaSuccess) {
+    // the same limit kspace_forces sets, so that neither caller lowers it
+    e = cudaFuncSetAttribute(k_kforce_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    g_na_what[dev] = "cudaFuncSetAttribute(k_kforce_mixed)";
+  }
+  g_na_err[dev] = e;
+  g_na_ptr[dev] = e == cudaSuccess ? (unsigned char *)p : nullptr;
+}
+
+struct NaDeviceGuard {
+  int prev = -1;
+  bool switched = false;
+  ~NaDeviceGuard() {
+    if (switched) cudaSetDevice(prev);
+  }
+};
+
+static int fk_ewald_noalloc(int device, cudaStream_t st, int natoms, const double *pos, const double *q,
+                            int ncharge, const int *icharge, const double *hmat, int kmax, double falp2,
+                            double ewald_self, double ewald_bkg, double *fxl, double *out) {
+  if (!hmat || !out || (ncharge > 0 && (!pos || !q || !icharge || !fxl))) {
+    set_error("fk_ewald_noalloc: null argument");
+    return CM3D_NB_ERR_ARG;
+  }
+  if (natoms < 1 || natoms > (1 << 28) || ncharge < 0 || ncharge > natoms) {
+    set_error("fk_ewald_noalloc: natoms = %d, ncharge = %d", natoms, ncharge);
+    return CM3D_NB_ERR_ARG;
+  }
+  if (ncharge > NA_MAX_CHARGES) {
+    set_error("fk_ewald_noalloc: %d charged atoms exceed the fixed scratch limit of %d "
+              "(CM3D_NB_NOALLOC_MAX_CHARGES); use cm3d_nb_fk_ewald",
+              ncharge, NA_MAX_CHARGES);
+    return CM3D_NB_ERR_ARG;
+  }
+  if (kmax < 0 || kmax > NA_MAX_KMAX) {
+    set_error("fk_ewald_noalloc: kmax = %d is outside the fixed scratch limit 0..%d "
+              "(CM3D_NB_NOALLOC_MAX_KMAX); use cm3d_nb_fk_ewald",
+              kmax, NA_MAX_KMAX);
+    return CM3D_NB_ERR_ARG;
+  }
+  const double *h = hmat;
+  const double vol = h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                     h[2] * (h[3] * h[7] - h[4] * h[6]);
+  if (!(vol != 0.0) || !isfinite(vol)) {
+    set_error("fk_ewald_noalloc: singular cell matrix (det = %g)", vol);
+    return CM3D_NB_ERR_ARG;
+  }
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev || device >= NA_MAX_DEVICES) {
+    set_error("fk_ewald_noalloc: device %d (the process sees %d)", device, ndev);
+    return CM3D_NB_ERR_ARG;
+  }
+  NaDeviceGuard guard;
+  CK(cudaGetDevice(&guard.prev));
+  if (guard.prev != device) {
+    CK(cudaSetDevice(device));
+    guard.switched = true;
+  }
+  std::call_once(g_na_once[device], na_device_setup, device);
+  if (g_na_err[device] != cudaSuccess) return cuda_fail(g_na_err[device], g_na_what[device]);
+  unsigned char *base = g_na_ptr[device];
+  uint4 *kfrac = (uint4 *)(base + NA_OFF_KFRAC);
+  double2 *spart = (double2 *)(base + NA_OFF_SPART);
+  double2 *sk = (double2 *)(base + NA_OFF_SK);
+  float2 *akf = (float2 *)(base + NA_OFF_AKF);
+  int *ka = (int *)(base + NA_OFF_KABC);
+  int *kb = ka + NA_MAX_K, *kc = ka + 2 * NA_MAX_K;
+  int4 *rows = (int4 *)(base + NA_OFF_ROWS);
+  int *row_k0 = (int *)(base + NA_OFF_ROWK0);
+  double *acc = (double *)(base + NA_OFF_ACC);
+  const double *dhmati = acc + ACC_COUNT;
+
+  // H^-1 as cm3d_nb_create forms it
+  const double rvol = 1. / vol;
+  Mat9 hi;
+  hi.m[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
+  hi.m[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
+  hi.m[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
+  hi.m[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
+  hi.m[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
+  hi.m[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
+  hi.m[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
+  hi.m[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
+  hi.m[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
+  // the same rows on the host (sizes and the force kernel's shared memory)
+  int hk0[NA_MAX_ROWS + 1];
+  int nrows = 0, ktot = 0;
+  for (int c = 0; c < (kmax + 1) * (2 * kmax + 1); c++) {
+    int i, j, kc0;
+    const int len = na_row(kmax, c, &i, &j, &kc0);
+    if (len == 0) continue;
+    hk0[nrows++] = ktot;
+    ktot += len;
+  }
+  hk0[nrows] = ktot;
+  if (ktot > NA_MAX_K || nrows > NA_MAX_ROWS) {
+    set_error("fk_ewald_noalloc: internal size check failed (ktot %d, rows %d)", ktot, nrows);
+    return CM3D_NB_ERR_ARG;
+  }
+
+  k_na_setup<<<1, NA_SETUP_THREADS, 0, st>>>(kmax, hi, rows, row_k0, ka, kb, kc, acc);
+  if (ncharge > 0 && ktot > 0) {
+    k_kprep<<<grid_for(ncharge, 256), 256, 0, st>>>(ncharge, icharge, natoms, pos, q, dhmati, kfrac, nullptr,
+                                                    nullptr);
+    // grids chosen as kspace_setup/kspace_forces choose them
+    const int ks_tiles = (ncharge + KS_THREADS * KS_A - 1) / (KS_THREADS * KS_A);
+    int rpb = nrows;
+    while (rpb > 1 && (long long)ks_tiles * ((nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
+    dim3 gsf(ks_tiles, (nrows + rpb - 1) / rpb);
+    k_sfac_mixed<<<gsf, KS_THREADS, 0, st>>>(ncharge, kfrac, nrows, rows, row_k0, rpb, ktot, spart, nullptr);
+    int gb = grid_for(ktot, 256);
+    if (gb > 148 * 4) gb = 148 * 4;
+    k_sred<<<gb, 256, 0, st>>>(ktot, ks_tiles, spart, ka, kb, kc, dhmati, rvol, falp2, sk, akf, nullptr, acc,
+                               nullptr);
+    const int per_block = KS_THREADS * KF_A;
+    const int tiles = (ncharge + per_block - 1) / per_block;
+    int split = 1;
+    while (tiles * split < 148 * 4 && split < nrows) split *= 2;
+    if (split > nrows) split = nrows;
+    const int rps = (nrows + split - 1) / split;
+    size_t smem = 0;
+    for (int r0 = 0; r0 < nrows; r0 += rps) {
+      const int r1 = r0 + rps < nrows ? r0 + rps : nrows;
+      const size_t nk = (size_t)(hk0[r1] - hk0[r0]) * sizeof(float2);
+      if (nk > smem) smem = nk;
+    }
+    dim3 gf(tiles, split);
+    k_kforce_mixed<<<gf, KS_THREADS, smem, st>>>(ncharge, kfrac, icharge, natoms, nrows, rows, row_k0, rps, akf,
+                                                 ktot, dhmati, split > 1, fxl, nullptr);
+  }
+  const double six = ncharge > 0 ? ewald_bkg / vol : 0.0;
+  k_na_finish<<<1, 32, 0, st>>>(acc, six, ncharge > 0 ? ewald_self : 0.0, out);
+  CK(cudaPeekAtLastError());
+  return CM3D_NB_OK;
+}
+
 }  // namespace cm3d
+
+extern "C" int cm3d_nb_fk_ewald_noalloc(int device, void *stream, int natoms, const double *pos,
+                                        const double *q, int ncharge, const int *icharge, const double hmat[9],
+                                        int kmax, double falp2, double ewald_self, double ewald_bkg,
+                                        double *fxl, double *out) {
+  return cm3d::fk_ewald_noalloc(device, (cudaStream_t)stream, natoms, pos, q, ncharge, icharge, hmat, kmax,
+                                falp2, ewald_self, ewald_bkg, fxl, out);
+}

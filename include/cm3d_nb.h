@@ -249,6 +249,59 @@ long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx);
    CUDA-core pair and k-space kernels.  No CM3D counterpart. */
 int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops);
 
+/* ------------------------------------------- no-allocation variant */
+#define CM3D_NB_NOALLOC_MAX_CHARGES 32768   /* charged atoms per call */
+#define CM3D_NB_NOALLOC_MAX_KMAX 15         /* kmax per call (7073 k-vectors) */
+/* fk_ewald() (energy/inter/md_ewald.c:185-348) in one call that allocates no
+   device memory.  It has no counterpart in the reference, whose fk_ewald
+   works on the COORDS arrays that CM3D's set-up allocated; it is for callers
+   that cannot allocate device memory at the point where they need the
+   reciprocal-space forces: a host program whose own memory pool has already
+   reserved the device (several systems packed on one GPU, each in its own
+   slice), or one that must not let an allocation stall the device in the
+   middle of a time step.  Such a caller owns every input and output buffer;
+   no engine context (cm3d_nb_create, which allocates) is involved.
+
+   The call runs the mixed-precision k-space kernels of cm3d_nb_fk_ewald (FP32
+   phases from fixed-point fractional coordinates, FP64 sums) on a scratch
+   area of about 2.9 MiB that is part of the library's static device memory,
+   one per device.  Limits: ncharge <= CM3D_NB_NOALLOC_MAX_CHARGES and
+   kmax <= CM3D_NB_NOALLOC_MAX_KMAX; larger inputs return CM3D_NB_ERR_ARG
+   (cm3d_nb_fk_ewald has no such limit).
+
+   The first call on a device does a one-time set-up: it looks the scratch
+   area up (the CUDA runtime may load the library's device code at that
+   moment, which is when the static area itself is reserved) and raises the
+   force kernel's shared-memory limit.  Make that first call before any stream
+   capture and where a one-time cost is acceptable.  Every call launches six
+   kernels on `stream` and returns without waiting for them.
+
+   The call clears the scratch accumulators itself; nothing has to start at
+   zero except what the caller wants in fxl, to which the forces are added.
+   Two calls on one device whose work overlaps in time (different streams,
+   or different host threads) share the scratch area and race: serialise
+   them, e.g. on one stream.
+
+   device         CUDA ordinal; made current for the call, the caller's
+                  current device is restored before returning
+   stream         cudaStream_t to launch on (NULL: the default stream)
+   natoms, pos    device, 3*natoms doubles: px | py | pz (COORDS.px ...)
+   q              device, natoms charges (COORDS.qch)
+   ncharge, icharge  device, the charged atoms' indices (COUL.icharge)
+   hmat           host, the cell matrix (COORDS.hmat)
+   kmax           ewald_setup's k-vector set (md_ewald.c:93-114)
+   falp2, ewald_self, ewald_bkg   COUL.falp2 / ewald_self / ewald_bkg
+                  (md_ewald.c:59-76)
+   fxl            device, 3*natoms doubles: the forces are ADDED, as fk_ewald
+                  adds them to COORDS.fxl
+   out            device, 11 doubles, overwritten: vk_ewald, vp_ewald,
+                  vp_ewald_tensor[9] (md_ewald.c:336-348) */
+int cm3d_nb_fk_ewald_noalloc(int device, void *stream, int natoms,
+                             const double *pos, const double *q, int ncharge,
+                             const int *icharge, const double hmat[9],
+                             int kmax, double falp2, double ewald_self,
+                             double ewald_bkg, double *fxl, double *out);
+
 /* ------------------------------------------ host set-up restatements */
 /* One interaction's LJ table, as get_ter_parm() builds it
    (input/md_getparm.c:236-237, 321-366 with func_lj md_funcvdw.c:40):
