@@ -84,7 +84,7 @@ static void destroy(Ctx *c) {
                   c->grp_ecorr_off, c->bond_ij, c->bond_p, c->bend_ijk, c->bend_p, c->ecorr_ij, c->cell_of,
                   c->cell_start, c->cell_cursor, c->cell_atoms, c->rank, c->cnt, c->off, c->ltot, c->lst[0],
                   c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
-                  c->cimg, c->acc,
+                  c->cimg, c->nlen, c->acc,
                   c->stat, c->istate};
   for (void *p : ptrs)
     if (p) cudaFree(p);

@@ -50,6 +50,7 @@ enum {
   ST_RESETS = 3,          // RESETPOS events
   ST_REBUILDS = 4,
   ST_BADSHIFT = 5,        // a pair's cell shift fell outside the 27-entry table
+  ST_NEED_STRIDE = 6,     // longest full list that did not fit its slot
   ST_COUNT = 8
 };
 // device integer state
@@ -167,7 +168,9 @@ struct Ctx {
   long long lcap[LT_COUNT] = {0, 0, 0, 0, 0};
   long long hcount[LT_COUNT] = {0, 0, 0, 0, 0};
   int2 *lst[4] = {nullptr, nullptr, nullptr, nullptr};   // t s te se half lists
-  uint32_t *nbr = nullptr;              // full list (mixed)
+  uint32_t *nbr = nullptr;              // full list (mixed): n slots of nbr_stride entries
+  int *nlen = nullptr;                  // full-list length per sorted atom
+  int nbr_stride = 0;
   float4 *xq = nullptr;                 // sorted: cell-relative FP32 pos + q
   float *epart = nullptr;               // mixed: per-atom energy/virial partials
   int *styp = nullptr;                  // sorted type

@@ -144,8 +144,6 @@ struct ListParams {
   double h[9], hi[9];
   double rmaxl_skin2_e, rmaxs_skin2_e;
   float lim2;                       // FP32 prefilter radius^2 (inf = off)
-  int want_full;                    // mixed: build the full list
-  int want_half;                    // build CM3D's four half lists
   long long cap[LT_COUNT];
 };
 
@@ -202,57 +200,27 @@ __device__ __forceinline__ int exact_flags(const ListParams &P, int i, int j, in
   return flags;
 }
 
-// One warp per cell-sorted atom t: the lanes walk the candidates of the
-// stencil cells 32 at a time (consecutive sorted atoms, coalesced FP32
-// loads), drop those clearly beyond the largest list radius with an FP32
-// distance from cell-relative coordinates (margin 1e-3 A, far above FP32
-// rounding), and decide the rest exactly in FP64.  FILL = false counts the
-// pairs of every list per atom; FILL = true writes them, compacted with warp
-// ballots in candidate order (deterministic).
-template <bool FILL>
-__global__ void __launch_bounds__(256) k_list_warp(
-    ListParams P, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
-    const float4 *__restrict__ xq, const float4 *__restrict__ shift, const double *__restrict__ pos,
-    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
-    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
-    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
-    int *__restrict__ cnt, const long long *__restrict__ off, const long long *__restrict__ tot,
-    const int *__restrict__ rank, int2 *__restrict__ l0, int2 *__restrict__ l1, int2 *__restrict__ l2,
-    int2 *__restrict__ l3, uint32_t *__restrict__ nbr, long long *__restrict__ stat, int *__restrict__ halt,
-    const int *__restrict__ gate) {
-  if (gated_off(gate, 1)) return;
-  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// The candidate walk shared by both list kernels.  One warp owns the
+// cell-sorted atom t; its lanes walk the stencil cells 32 candidates at a
+// time (consecutive sorted atoms: coalesced FP32 loads) and drop those
+// clearly beyond the largest list radius with an FP32 distance from
+// cell-relative coordinates (margin 1e-3 A, far above FP32 rounding).  The
+// survivors -- typically a few of every 32 -- are queued in shared memory in
+// candidate order, and whenever 32 are waiting the whole warp runs the exact
+// FP64 test on them at once (`decide(first, m)`: lane l < m takes queue entry
+// first + l), so the expensive test runs on full warps.
+constexpr int LQ = 64;                     // queue entries per warp (> 2 * 32 - 1)
+
+template <class Decide>
+__device__ __forceinline__ void walk_candidates(const ListParams &P, int i, int4 ci, float4 xi4, bool half_only,
+                                                const int *__restrict__ cell_atoms,
+                                                const int *__restrict__ cell_start,
+                                                const float4 *__restrict__ xq, const float4 *__restrict__ shift,
+                                                int *qbuf, Decide &decide) {
   const int lane = threadIdx.x & 31;
-  if (t >= P.n) return;                                   // whole warps
   const unsigned lt_mask = (1u << lane) - 1u;
-  bool ok[5] = {true, true, true, true, true};
-  long long p[5] = {0, 0, 0, 0, 0};
-  if (FILL) {
-    bool all = true;
-    for (int k = 0; k < 5; k++) {
-      ok[k] = tot[k] <= P.cap[k];
-      all = all && ok[k];
-      p[k] = off[(size_t)k * (P.n + 1) + t];
-    }
-    if (!all) {
-      // a list outgrew its buffer: write nothing, halt the step (the host
-      // grows the buffers and finishes it, see run_step)
-      if (t == 0 && lane == 0) {
-        atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
-        if (halt) *halt = 1;
-      }
-      return;
-    }
-  }
-  const int i = cell_atoms[t];
-  const int4 ci = cimg[i];
   const int cx = ci.x & 1023, cy = (ci.x >> 10) & 1023, cz = (ci.x >> 20) & 1023;
-  const float4 xi4 = xq[t];
-  const double xi = pos[i], yi = pos[P.n + i], zi = pos[2 * P.n + i];
-  const int ti = itype[i];
-  const bool qi = q[i] != 0.0;
-  int c[5] = {0, 0, 0, 0, 0};
-  unsigned bad = 0;
+  int head = 0, tail = 0;
   for (int a = 0; a < P.nsx; a++) {
     int jx = cx + P.sx[a];
     jx = jx < 0 ? jx + P.ncx : (jx >= P.ncx ? jx - P.ncx : jx);
@@ -268,50 +236,168 @@ __global__ void __launch_bounds__(256) k_list_warp(
         const int lo = cell_start[cell], hi = cell_start[cell + 1];
         for (int u0 = lo; u0 < hi; u0 += 32) {
           const int u = u0 + lane;
-          int fl = 0, code = 13, j = -1;
+          bool keep = false;
           if (u < hi) {
-            j = cell_atoms[u];
+            const int j = cell_atoms[u];
             const float4 xj = xq[u];
             const float dx = (xi4.x - xj.x) + S.x, dy = (xi4.y - xj.y) + S.y, dz = (xi4.z - xj.z) + S.z;
             const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            if (j != i && r2f < P.lim2 && (P.want_full || j > i))
-              fl = exact_flags(P, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
-                               cexcl_off, cexcl_idx, cimg, code);
+            keep = j != i && r2f < P.lim2 && (!half_only || j > i);
           }
-          bad |= (fl >> 4) & 1;
-          const bool half = j > i;
-          const bool f0 = P.want_half && half && (fl & 1), f1 = P.want_half && half && (fl & 2);
-          const bool f2 = P.want_half && half && (fl & 4), f3 = P.want_half && half && (fl & 8);
-          const bool f4 = P.want_full && (fl & 5);
-          const unsigned b0 = __ballot_sync(0xffffffffu, f0), b1 = __ballot_sync(0xffffffffu, f1);
-          const unsigned b2 = __ballot_sync(0xffffffffu, f2), b3 = __ballot_sync(0xffffffffu, f3);
-          const unsigned b4 = __ballot_sync(0xffffffffu, f4);
-          if (!FILL) {
-            c[0] += __popc(b0); c[1] += __popc(b1); c[2] += __popc(b2); c[3] += __popc(b3); c[4] += __popc(b4);
-          } else {
-            const int2 pr = make_int2(i, j);
-            if (f0) l0[p[0] + __popc(b0 & lt_mask)] = pr;
-            if (f1) l1[p[1] + __popc(b1 & lt_mask)] = pr;
-            if (f2) l2[p[2] + __popc(b2 & lt_mask)] = pr;
-            if (f3) l3[p[3] + __popc(b3 & lt_mask)] = pr;
-            if (f4) {
-              uint32_t e = (uint32_t)rank[j] | ((uint32_t)code << ENT_CODE_SHIFT);
-              if (fl & 1) e |= ENT_LJ;
-              if (fl & 2) e |= ENT_LJS;
-              if (fl & 4) e |= ENT_EL;
-              if (fl & 8) e |= ENT_ELS;
-              nbr[p[4] + __popc(b4 & lt_mask)] = e;
-            }
-            p[0] += __popc(b0); p[1] += __popc(b1); p[2] += __popc(b2); p[3] += __popc(b3); p[4] += __popc(b4);
+          const unsigned bk = __ballot_sync(0xffffffffu, keep);
+          if (keep) qbuf[(tail + __popc(bk & lt_mask)) & (LQ - 1)] = u;
+          tail += __popc(bk);
+          __syncwarp();
+          if (tail - head >= 32) {
+            decide(head, 32);
+            head += 32;
+            __syncwarp();
           }
         }
       }
     }
   }
+  while (tail > head) {
+    const int m = tail - head < 32 ? tail - head : 32;
+    decide(head, m);
+    head += m;
+  }
+}
+
+// CM3D's four half lists (i < j): FILL = false counts the pairs of every
+// list per atom, FILL = true writes them at the scanned offsets, compacted
+// with warp ballots in candidate order (deterministic).
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_list_half(
+    ListParams P, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    const float4 *__restrict__ xq, const float4 *__restrict__ shift, const double *__restrict__ pos,
+    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
+    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
+    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
+    int *__restrict__ cnt, const long long *__restrict__ off, const long long *__restrict__ tot,
+    int2 *__restrict__ l0, int2 *__restrict__ l1, int2 *__restrict__ l2, int2 *__restrict__ l3,
+    long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  __shared__ int qs[256 / 32][LQ];
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= P.n) return;                                   // whole warps
+  const unsigned lt_mask = (1u << lane) - 1u;
+  long long p[4] = {0, 0, 0, 0};
   if (FILL) {
-    if (bad) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
+    bool all = true;
+    for (int k = 0; k < 4; k++) {
+      all = all && tot[k] <= P.cap[k];
+      p[k] = off[(size_t)k * (P.n + 1) + t];
+    }
+    if (!all) {
+      // a list outgrew its buffer: write nothing, halt the step (the host
+      // grows the buffers and finishes it, see run_step)
+      if (t == 0 && lane == 0) {
+        atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
+        if (halt) *halt = 1;
+      }
+      return;
+    }
+  }
+  int *qbuf = qs[threadIdx.x >> 5];
+  const int i = cell_atoms[t];
+  const int4 ci = cimg[i];
+  const double xi = pos[i], yi = pos[P.n + i], zi = pos[2 * P.n + i];
+  const int ti = itype[i];
+  const bool qi = q[i] != 0.0;
+  int c[4] = {0, 0, 0, 0};
+  unsigned bad = 0;
+  auto decide = [&](int first, int m) {
+    int fl = 0, code = 13, j = -1;
+    if (lane < m) {
+      j = cell_atoms[qbuf[(first + lane) & (LQ - 1)]];
+      fl = exact_flags(P, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx, cexcl_off,
+                       cexcl_idx, cimg, code);
+    }
+    bad |= (fl >> 4) & 1;
+    const unsigned b0 = __ballot_sync(0xffffffffu, fl & 1), b1 = __ballot_sync(0xffffffffu, fl & 2);
+    const unsigned b2 = __ballot_sync(0xffffffffu, fl & 4), b3 = __ballot_sync(0xffffffffu, fl & 8);
+    if (!FILL) {
+      c[0] += __popc(b0); c[1] += __popc(b1); c[2] += __popc(b2); c[3] += __popc(b3);
+    } else {
+      const int2 pr = make_int2(i, j);
+      if (fl & 1) l0[p[0] + __popc(b0 & lt_mask)] = pr;
+      if (fl & 2) l1[p[1] + __popc(b1 & lt_mask)] = pr;
+      if (fl & 4) l2[p[2] + __popc(b2 & lt_mask)] = pr;
+      if (fl & 8) l3[p[3] + __popc(b3 & lt_mask)] = pr;
+      p[0] += __popc(b0); p[1] += __popc(b1); p[2] += __popc(b2); p[3] += __popc(b3);
+    }
+  };
+  walk_candidates(P, i, ci, xq[t], true, cell_atoms, cell_start, xq, shift, qbuf, decide);
+  if (FILL) {
+    if (bad && lane == 0) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
   } else if (lane == 0) {
-    for (int k = 0; k < 5; k++) cnt[(size_t)k * P.n + t] = c[k];
+    for (int k = 0; k < 4; k++) cnt[(size_t)k * P.n + t] = c[k];
+  }
+}
+
+// Mixed mode, one pass: the full list of sorted atom t (both directions,
+// every pair in CM3D's t or te list) written straight into its fixed slot
+// nbr[t * stride ...], in candidate order, its length into nlen[t].  An atom
+// with more than `stride` pairs writes the first `stride`, records the
+// length it needed (ST_NEED_STRIDE) and halts a captured step; the host then
+// widens the slots and builds again.
+__global__ void __launch_bounds__(256) k_list_full(
+    ListParams P, int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    const float4 *__restrict__ xq, const float4 *__restrict__ shift, const double *__restrict__ pos,
+    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
+    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
+    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
+    uint32_t *__restrict__ nbr, int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt,
+    const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  __shared__ int qs[256 / 32][LQ];
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= P.n) return;                                   // whole warps
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int *qbuf = qs[threadIdx.x >> 5];
+  const int i = cell_atoms[t];
+  const int4 ci = cimg[i];
+  const double xi = pos[i], yi = pos[P.n + i], zi = pos[2 * P.n + i];
+  const int ti = itype[i];
+  const bool qi = q[i] != 0.0;
+  uint32_t *out = nbr + (size_t)t * stride;
+  int count = 0;
+  unsigned bad = 0;
+  auto decide = [&](int first, int m) {
+    int fl = 0, code = 13, u = 0;
+    if (lane < m) {
+      u = qbuf[(first + lane) & (LQ - 1)];
+      fl = exact_flags(P, i, cell_atoms[u], ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
+                       cexcl_off, cexcl_idx, cimg, code);
+    }
+    bad |= (fl >> 4) & 1;
+    const bool f = (fl & 5) != 0;
+    const unsigned bf = __ballot_sync(0xffffffffu, f);
+    if (f) {
+      const int slot = count + __popc(bf & lt_mask);
+      uint32_t e = (uint32_t)u | ((uint32_t)code << ENT_CODE_SHIFT);
+      if (fl & 1) e |= ENT_LJ;
+      if (fl & 2) e |= ENT_LJS;
+      if (fl & 4) e |= ENT_EL;
+      if (fl & 8) e |= ENT_ELS;
+      if (slot < stride) out[slot] = e;
+    }
+    count += __popc(bf);
+  };
+  walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, shift, qbuf, decide);
+  if (lane == 0) {
+    nlen[t] = count < stride ? count : stride;
+    if (count > stride) {
+      atomicMax((unsigned long long *)(stat + ST_NEED_STRIDE), (unsigned long long)count);
+      if (halt) {
+        atomicAdd((unsigned long long *)(stat + ST_OVERFLOW), 1ull);
+        *halt = 1;
+      }
+    }
+    if (bad) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
   }
 }
 
@@ -383,8 +469,26 @@ int list_setup(Ctx *c) {
   CK(cudaMalloc(&c->cell_cursor, sizeof(int) * ((size_t)tot + 1)));
   CK(cudaMalloc(&c->cell_atoms, sizeof(int) * (size_t)c->n));
   CK(cudaMalloc(&c->rank, sizeof(int) * (size_t)c->n));
-  CK(cudaMalloc(&c->cnt, sizeof(int) * 5 * (size_t)c->n));
-  CK(cudaMalloc(&c->off, sizeof(long long) * 5 * ((size_t)c->n + 1)));
+  CK(cudaMalloc(&c->cnt, sizeof(int) * 4 * (size_t)c->n));
+  CK(cudaMalloc(&c->off, sizeof(long long) * 4 * ((size_t)c->n + 1)));
+  if (c->mode == CM3D_NB_MIXED) {
+    CK(cudaMalloc(&c->nlen, sizeof(int) * (size_t)c->n));
+    // first guess of the full-list slot: 1.3 x the mean number of atoms in
+    // a list sphere, plus 64, in whole 32-entry (128-byte) units; a build
+    // that finds a longer list widens it (grow_full)
+    const double *h = c->hmat;
+    double vol = fabs(h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                      h[2] * (h[3] * h[7] - h[4] * h[6]));
+    double r = c->rlist_max;
+    double est = 1.3 * (double)c->n / vol * (4.0 / 3.0) * M_PI * r * r * r + 64.0;
+    long long cap_n = ((long long)c->n + 31) / 32 * 32;
+    long long s = ((long long)est + 31) / 32 * 32;
+    if (s > cap_n) s = cap_n;
+    if (s < 32) s = 32;
+    c->nbr_stride = (int)s;
+    CK(cudaMalloc(&c->nbr, sizeof(uint32_t) * (size_t)c->n * (size_t)s));
+    c->lcap[LT_FULL] = (long long)c->n * s;
+  }
   CK(cudaMalloc(&c->ltot, sizeof(long long) * LT_COUNT));
   CK(cudaMallocHost(&c->h_ltot, sizeof(long long) * LT_COUNT));
   CK(cudaMalloc(&c->styp, sizeof(int) * (size_t)c->n));
@@ -417,22 +521,35 @@ static int grow(Ctx *c, int which, long long need) {
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
   }
-  if (which < 4) {
-    if (c->lst[which]) cudaFree(c->lst[which]);
-    c->lst[which] = nullptr;
-    cudaError_t e = cudaMalloc(&c->lst[which], sizeof(int2) * (size_t)cap);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(list)");
-  } else {
-    if (c->nbr) cudaFree(c->nbr);
-    c->nbr = nullptr;
-    cudaError_t e = cudaMalloc(&c->nbr, sizeof(uint32_t) * (size_t)cap);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(full list)");
-  }
+  if (c->lst[which]) cudaFree(c->lst[which]);
+  c->lst[which] = nullptr;
+  cudaError_t e = cudaMalloc(&c->lst[which], sizeof(int2) * (size_t)cap);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(list)");
   c->lcap[which] = cap;
   return CM3D_NB_OK;
 }
 
-static ListParams params(Ctx *c, bool want_half) {
+// widen the full-list slots to hold `need` entries (+1/8 and 32 spare)
+static int grow_full(Ctx *c, long long need) {
+  long long cap_n = ((long long)c->n + 31) / 32 * 32;
+  long long s = (need + need / 8 + 32 + 31) / 32 * 32;
+  if (s > cap_n) s = cap_n;
+  if (s <= c->nbr_stride) s = c->nbr_stride + 32;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  if (c->nbr) cudaFree(c->nbr);
+  c->nbr = nullptr;
+  cudaError_t e = cudaMalloc(&c->nbr, sizeof(uint32_t) * (size_t)c->n * (size_t)s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(full list)");
+  c->nbr_stride = (int)s;
+  c->lcap[LT_FULL] = (long long)c->n * s;
+  return CM3D_NB_OK;
+}
+
+static ListParams params(Ctx *c) {
   ListParams P;
   P.n = c->n;
   P.ntypes = c->ntypes;
@@ -454,8 +571,6 @@ static ListParams params(Ctx *c, bool want_half) {
   const bool pre = c->nc[0] >= 3 && c->nc[1] >= 3 && c->nc[2] >= 3;
   const double rl = c->rlist_max + 1e-3;
   P.lim2 = pre ? (float)(rl * rl) : INFINITY;
-  P.want_full = c->mode == CM3D_NB_MIXED;
-  P.want_half = want_half;
   for (int k = 0; k < LT_COUNT; k++) P.cap[k] = c->lcap[k];
   return P;
 }
@@ -487,34 +602,53 @@ int build_lists(Ctx *c, bool device_flag) {
                                                   c->itype, c->pos, c->q, c->rank, c->styp, c->corner, c->xq,
                                                   gate);
   c->launches += 5;
-  ListParams P = params(c, want_half);
+  ListParams P = params(c);
   const long long warps_threads = 32LL * n;
-  k_list_warp<false><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
-      P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
-      c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->cnt, nullptr, nullptr, c->rank, nullptr, nullptr,
-      nullptr, nullptr, nullptr, c->stat, nullptr, gate);
-  k_scan<int, long long><<<dim3(1, 5), 1024, 0, c->st>>>(c->cnt, c->off, c->ltot, n, gate);
-  c->launches += 2;
-  CKL(c);
-  if (!device_flag) {
-    CK(cudaMemcpyAsync(c->h_ltot, c->ltot, sizeof(long long) * LT_COUNT, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    for (int k = 0; k < LT_COUNT; k++) {
-      int rc = grow(c, k, c->h_ltot[k] > 0 ? c->h_ltot[k] : 1);
+  if (c->mode == CM3D_NB_MIXED) {
+    for (;;) {
+      k_list_full<<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
+          P, c->nbr_stride, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut,
+          c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->nbr, c->nlen, c->stat,
+          device_flag ? c->istate + IS_HALT : nullptr, gate);
+      c->launches++;
+      CKL(c);
+      if (device_flag) break;
+      // host-driven build: widen the slots and build again if a list did not fit
+      CK(cudaMemcpyAsync(c->h_stat, c->stat, sizeof(long long) * ST_COUNT, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      if (c->h_stat[ST_NEED_STRIDE] <= c->nbr_stride) break;
+      int rc = grow_full(c, c->h_stat[ST_NEED_STRIDE]);
       if (rc) return rc;
-      c->hcount[k] = c->h_ltot[k];
     }
-    P = params(c, want_half);
   }
-  k_list_warp<true><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
-      P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
-      c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, nullptr, c->off, c->ltot, c->rank, c->lst[0], c->lst[1],
-      c->lst[2], c->lst[3], c->nbr, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+  if (want_half) {
+    k_list_half<false><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
+        P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
+        c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->cnt, nullptr, nullptr, nullptr, nullptr, nullptr,
+        nullptr, c->stat, nullptr, gate);
+    k_scan<int, long long><<<dim3(1, 4), 1024, 0, c->st>>>(c->cnt, c->off, c->ltot, n, gate);
+    c->launches += 2;
+    CKL(c);
+    if (!device_flag) {
+      CK(cudaMemcpyAsync(c->h_ltot, c->ltot, sizeof(long long) * 4, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      for (int k = 0; k < 4; k++) {
+        int rc = grow(c, k, c->h_ltot[k] > 0 ? c->h_ltot[k] : 1);
+        if (rc) return rc;
+        c->hcount[k] = c->h_ltot[k];
+      }
+      P = params(c);
+    }
+    k_list_half<true><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
+        P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
+        c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, nullptr, c->off, c->ltot, c->lst[0], c->lst[1], c->lst[2],
+        c->lst[3], c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+    c->launches++;
+  }
   if (!c->no_snapshot) {
     k_snapshot<<<grid_for(3LL * n, B), B, 0, c->st>>>(3 * n, c->pos, c->dxn, gate, c->istate, c->stat);
     c->launches++;
   }
-  c->launches++;
   CKL(c);
   tend(c, 2, e0);
   if (!device_flag) {

@@ -54,7 +54,7 @@ enum { EP_ELJ = 0, EP_ELJH, EP_VL0, EP_VL1, EP_VL2, EP_VL4, EP_VL5, EP_VL8,
 template <int TPA, bool SMALLBOX, bool NEED_S>
 __global__ void __launch_bounds__(256) k_pair_mixed(
     MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
-    const long long *__restrict__ off, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
+    const int *__restrict__ nlen, int stride, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
     const float4 *__restrict__ gte, double *__restrict__ fout, double *__restrict__ fshort,
     float *__restrict__ epart, long long *__restrict__ stat, const int *__restrict__ gs) {
@@ -97,13 +97,12 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
     if (active) {
       const float4 xi = xq[t];
       const int ti = styp[t];
-      const long long k0 = off[t], k1 = off[t + 1];
+      const long long k0 = (long long)t * stride, k1 = k0 + nlen[t];
       float fx = 0, fy = 0, fz = 0, sx = 0, sy = 0, sz = 0;
       int cnt = 0;
-      for (long long k = k0 + g; k < k1; k += TPA) {
-        const uint32_t en = __ldg(nbr + k);
-        const int j = en & ENT_JMASK;
-        const float4 xj = xq[j];
+      // one pair; xj and tj (j's type, needed only by LJ pairs) come from the
+      // batched loads below
+      auto pair = [&](const uint32_t en, const float4 xj, const int tj) {
         const float4 sh = shift[(en >> ENT_CODE_SHIFT) & 31];
         float dx = (xi.x - xj.x) + sh.x;
         float dy = (xi.y - xj.y) + sh.y;
@@ -149,7 +148,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
           }
         }
         if ((en & fl_lj) && (P.mask & 1)) {
-          const int in = map[ti * P.ntypes + styp[j]];
+          const int in = map[ti * P.ntypes + tj];
           const float *fc = fcut + 8 * in;
           const float rmax2 = P.iflg == 1 ? fc[0] : fc[4];
           if (r2 < rmax2) {
@@ -196,7 +195,32 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
           sy = fmaf(-fsh, dy, sy);
           sz = fmaf(-fsh, dz, sz);
         }
-        if (++cnt == 16) {
+      };
+      // the lane's pairs k0+g, k0+g+TPA, ... in batches of PU: the batch's
+      // list entries, then its coordinates and types, are loaded together so
+      // that PU independent loads are in flight; FP32 sums go to FP64 every
+      // 16 pairs.  Entry 0 marks the end (a real entry has a list flag set).
+      constexpr int PU = 4;
+      for (long long kb = k0 + g; kb < k1; kb += PU * TPA) {
+        uint32_t en[PU];
+        float4 xj[PU];
+        int tj[PU];
+#pragma unroll
+        for (int u = 0; u < PU; u++) {
+          const long long k = kb + (long long)u * TPA;
+          en[u] = k < k1 ? __ldg(nbr + k) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < PU; u++) {
+          const int j = en[u] & ENT_JMASK;
+          xj[u] = xq[j];
+          tj[u] = (en[u] & fl_lj) ? styp[j] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < PU; u++)
+          if (en[u] != 0u) pair(en[u], xj[u], tj[u]);
+        cnt += PU;
+        if (cnt == 16) {
           Fx += fx; Fy += fy; Fz += fz;
           fx = fy = fz = 0.f;
           if (NEED_S) {
@@ -313,7 +337,7 @@ static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   long long grid = (long long)c->num_sms * per_sm;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  k_pair_mixed<TPA, SB, NS><<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->off + 4 * ((size_t)c->n + 1),
+  k_pair_mixed<TPA, SB, NS><<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->nlen, c->nbr_stride,
                                                       c->nbr, c->shift, c->map, c->fcut, c->ftab_lj, c->ftab_el,
                                                       fout, c->fxs, c->epart, c->stat, c->gate);
 }

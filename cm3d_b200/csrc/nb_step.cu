@@ -634,7 +634,7 @@ int run_step(Ctx *c, int istep0, int nsteps) {
   if ((rc = close_level(c, intr))) return rc;
   for (int lv = intr + 1; lv < c->nres_lrf; lv++)
     if ((rc = one_level(c, lv, false))) return rc;
-  cudaGraphExecDestroy(c->graph);   // it holds the old buffer addresses
+  if (c->graph) cudaGraphExecDestroy(c->graph);   // it holds the old buffer addresses
   c->graph = nullptr;
   int done = failed + 1 - istep0;
   if (done < nsteps) return run_step(c, failed + 1, nsteps - done);
