@@ -85,10 +85,11 @@ static void destroy(Ctx *c) {
                   c->cell_start, c->cell_cursor, c->cell_atoms, c->rank, c->cnt, c->off, c->ltot, c->lst[0],
                   c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
                   c->cimg, c->nlen, c->acc,
-                  c->stat, c->istate};
+                  c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
+                  c->ktile_sys, c->ftile_sys, c->k_sys};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot};
+  void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
   for (void *p : hp)
     if (p) cudaFreeHost(p);
   for (int k = 0; k < NTCLS; k++)
@@ -104,34 +105,57 @@ static void destroy(Ctx *c) {
   delete c;
 }
 
-static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out) {
-  if (!s || !out) {
-    set_error("cm3d_nb_create: null argument");
-    return CM3D_NB_ERR_ARG;
-  }
-  if (s->natoms <= 0) {
-    set_error("cm3d_nb_create: natoms = %d", s->natoms);
-    return CM3D_NB_ERR_ARG;
-  }
-  if (s->iperd != 3) {
-    set_error("cm3d_nb_create: only iperd 3 (three-dimensional periodicity) is supported, got %d", s->iperd);
-    return CM3D_NB_ERR_ARG;
-  }
-  if (s->ntable < 5) {
-    set_error("cm3d_nb_create: ntable = %d is too small", s->ntable);
+// One context over `nsys` systems (a batch; one system is a batch of one).
+// The systems' atoms are concatenated in order; every per-system parameter
+// goes to SysP / SysH.  Batches need the mixed engine and the same ntable,
+// time step and RESPA levels in every system.
+static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options *opt, Ctx **out) {
+  if (!systems || !out || nsys < 1) {
+    set_error("cm3d_nb_create: null argument or no systems");
     return CM3D_NB_ERR_ARG;
   }
   cm3d_nb_options o;
   cm3d_nb_default_options(&o);
   if (opt) o = *opt;
+  if (nsys > 1 && o.mode != CM3D_NB_MIXED) {
+    set_error("cm3d_nb_create_batch: batches run in the mixed engine only (the plain FP64 engine is one system "
+              "per context)");
+    return CM3D_NB_ERR_ARG;
+  }
+  long long ntot = 0;
+  for (int sy = 0; sy < nsys; sy++) {
+    const cm3d_nb_system *s = systems + sy;
+    if (s->natoms <= 0) {
+      set_error("cm3d_nb_create: system %d: natoms = %d", sy, s->natoms);
+      return CM3D_NB_ERR_ARG;
+    }
+    if (s->iperd != 3) {
+      set_error("cm3d_nb_create: system %d: only iperd 3 (three-dimensional periodicity) is supported, got %d", sy,
+                s->iperd);
+      return CM3D_NB_ERR_ARG;
+    }
+    if (s->ntable < 5) {
+      set_error("cm3d_nb_create: system %d: ntable = %d is too small", sy, s->ntable);
+      return CM3D_NB_ERR_ARG;
+    }
+    const cm3d_nb_system *s0 = systems;
+    if (s->ntable != s0->ntable || s->dt != s0->dt || s->nres_lrf != s0->nres_lrf ||
+        s->nres_intra != s0->nres_intra || s->nres_tors != s0->nres_tors) {
+      set_error("cm3d_nb_create_batch: system %d differs from system 0 in ntable, dt or the RESPA levels; a batch "
+                "steps all its systems together",
+                sy);
+      return CM3D_NB_ERR_ARG;
+    }
+    ntot += s->natoms;
+  }
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0) {
     set_error("cm3d_nb_create: no CUDA device (%s)", e != cudaSuccess ? cudaGetErrorString(e) : "count 0");
     return CM3D_NB_ERR_NODEV;
   }
-  if (o.mode == CM3D_NB_MIXED && s->natoms > MAX_ATOMS_MIXED) {
-    set_error("cm3d_nb_create: the mixed engine holds at most %d atoms per system", MAX_ATOMS_MIXED);
+  if (o.mode == CM3D_NB_MIXED && ntot > MAX_ATOMS_MIXED) {
+    set_error("cm3d_nb_create: the mixed engine holds at most %d atoms per context", MAX_ATOMS_MIXED);
     return CM3D_NB_ERR_ARG;
   }
   Ctx *c = new Ctx();
@@ -144,91 +168,191 @@ static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out
   c->need_short = o.need_short;
   c->tpa = o.tpa;
   c->use_graph = o.use_graph;
-  const int n = s->natoms;
+  c->nsys = nsys;
+  c->h_sp.assign(nsys, SysP());
+  c->hs.assign(nsys, SysH());
+  const cm3d_nb_system *s0 = systems;
+  const int n = (int)ntot;
   c->n = n;
-  c->ntypes = s->ntypes;
-  c->ninter = s->ninter;
-  c->ntable = s->ntable;
-  c->iperd = s->iperd;
-  c->nres_lrf = s->nres_lrf > 0 ? s->nres_lrf : 1;
-  c->nres_intra = s->nres_intra > 0 ? s->nres_intra : 1;
-  c->nres_tors = s->nres_tors > 0 ? s->nres_tors : 1;
-  c->ndof = s->ndof > 0 ? s->ndof : 1;
-  c->dt = s->dt;
-  c->vlrc = s->vlrc;
-  c->wlrc = s->wlrc;
-  c->skin = s->skin_ter;
-  c->rheal = s->rheal;
-  memcpy(c->hmat, s->hmat, sizeof c->hmat);
-  {
-    const double *h = c->hmat;
-    double *hi = c->hmati;
-    double rvol = 1. / (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
-                        h[2] * (h[3] * h[7] - h[4] * h[6]));
-    hi[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
-    hi[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
-    hi[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
-    hi[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
-    hi[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
-    hi[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
-    hi[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
-    hi[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
-    hi[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
-  }
-  c->kappa = s->kappa;
-  c->kappa2 = s->kappa * s->kappa;
-  c->falp2 = s->falp2;
-  c->ewald_self = s->ewald_self;
-  c->ewald_bkg = s->ewald_bkg;
-  c->dx2coul = s->dx2coul;
-  c->rmins_coul2 = s->rmins_coul2;
-  c->rmaxs_coul2 = s->rmaxs_coul2;
-  c->rminl_coul2 = s->rminl_coul2;
-  c->rmaxl_coul2 = s->rmaxl_coul2;
-  c->rmaxs_skin2_e = s->rmaxs_skin2_e;
-  c->rmaxl_skin2_e = s->rmaxl_skin2_e;
-  c->ktot = s->ktot;
-  c->necorr = s->necorr;
-  c->nbonds = s->nbonds;
-  c->nbends = s->nbends;
-  // charged atoms (set_charges, elec_ngbr.c:115-121)
-  std::vector<int> ich;
-  for (int i = 0; i < n; i++)
-    if (s->qch[i] != 0.) ich.push_back(i);
-  c->ncharge = (int)ich.size();
-  if (c->ncharge > 0 && (!s->coultab || !s->dcoultab)) {
-    set_error("cm3d_nb_create: charged atoms but no coultab/dcoultab");
-    return CM3D_NB_ERR_ARG;
-  }
-  c->tablast_e = c->ncharge > 0 ? s->coultab[s->ntable - 4] : 0.0;
-  // largest list radius
-  double r2 = 0;
-  std::vector<double> icut(8 * (size_t)(s->ninter > 0 ? s->ninter : 1), 0.0);
-  for (int in = 0; in < s->ninter; in++) {
-    icut[8 * in + 0] = s->rmaxs_cut2[in];
-    icut[8 * in + 1] = s->rmins_cut2[in];
-    icut[8 * in + 2] = s->rmaxl_cut2[in];
-    icut[8 * in + 3] = s->rminl_cut2[in];
-    icut[8 * in + 4] = s->rmaxs_skin2[in];
-    icut[8 * in + 5] = s->rmaxl_skin2[in];
-    icut[8 * in + 6] = s->dx2tab[in];
-    icut[8 * in + 7] = s->vtab[(size_t)in * s->ntable + s->ntable - 4];
-    r2 = std::max(r2, s->rmaxl_skin2[in]);
-    c->rc_lj_max = std::max(c->rc_lj_max, sqrt(s->rmaxl_cut2[in]));
-  }
-  if (c->ncharge > 0) r2 = std::max(r2, s->rmaxl_skin2_e);
-  c->rlist_max = sqrt(r2);
-  // device arrays
+  c->ntable = s0->ntable;
+  c->iperd = 3;
+  c->nres_lrf = s0->nres_lrf > 0 ? s0->nres_lrf : 1;
+  c->nres_intra = s0->nres_intra > 0 ? s0->nres_intra : 1;
+  c->nres_tors = s0->nres_tors > 0 ? s0->nres_tors : 1;
+  c->dt = s0->dt;
+  const int nt = s0->ntable;
+  // concatenated host arrays
   const size_t n3 = 3 * (size_t)n;
-  std::vector<double> pos(n3), vel(n3);
-  for (int i = 0; i < n; i++) {
-    pos[i] = s->px[i];
-    pos[n + i] = s->py[i];
-    pos[2 * n + i] = s->pz[i];
-    vel[i] = s->vx ? s->vx[i] : 0.;
-    vel[n + i] = s->vy ? s->vy[i] : 0.;
-    vel[2 * n + i] = s->vz ? s->vz[i] : 0.;
+  std::vector<double> pos(n3), vel(n3), mass(n), q(n);
+  std::vector<int> itype(n), sys_of(n), map, ich, eoff(n + 1, 0), eidx, coff(n + 1, 0), cidx;
+  std::vector<double> vtab, dvtab, swt, icut, coultab, dcoultab, switchse;
+  int a0 = 0, inter0 = 0, ncoul = 0;
+  for (int sy = 0; sy < nsys; sy++) {
+    const cm3d_nb_system *s = systems + sy;
+    SysP &P = c->h_sp[sy];
+    SysH &H = c->hs[sy];
+    const int ns = s->natoms;
+    P.a0 = a0;
+    P.n = ns;
+    H.n = ns;
+    H.ndof = s->ndof > 0 ? s->ndof : 1;
+    H.ntypes = s->ntypes;
+    H.ninter = s->ninter;
+    H.vlrc = s->vlrc;
+    H.wlrc = s->wlrc;
+    H.iperd = s->iperd;
+    memcpy(H.hmat, s->hmat, sizeof H.hmat);
+    {
+      const double *h = H.hmat;
+      double *hi = H.hmati;
+      double rvol = 1. / (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                          h[2] * (h[3] * h[7] - h[4] * h[6]));
+      hi[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
+      hi[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
+      hi[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
+      hi[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
+      hi[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
+      hi[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
+      hi[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
+      hi[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
+      hi[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
+      P.rvol = rvol;
+    }
+    for (int k = 0; k < 9; k++) {
+      P.h[k] = H.hmat[k];
+      P.hi[k] = H.hmati[k];
+      P.hF[k] = (float)H.hmat[k];
+      P.hiF[k] = (float)H.hmati[k];
+    }
+    P.kappa = s->kappa;
+    P.kappa2 = s->kappa * s->kappa;
+    P.falp2 = s->falp2;
+    H.ewald_self = s->ewald_self;
+    H.ewald_bkg = s->ewald_bkg;
+    P.skin2q = .25 * s->skin_ter * s->skin_ter;
+    // atoms
+    for (int i = 0; i < ns; i++) {
+      const int g = a0 + i;
+      pos[g] = s->px[i];
+      pos[n + g] = s->py[i];
+      pos[2 * (size_t)n + g] = s->pz[i];
+      vel[g] = s->vx ? s->vx[i] : 0.;
+      vel[n + g] = s->vy ? s->vy[i] : 0.;
+      vel[2 * (size_t)n + g] = s->vz ? s->vz[i] : 0.;
+      mass[g] = s->amass[i];
+      q[g] = s->qch[i];
+      itype[g] = s->itype[i];
+      sys_of[g] = sy;
+      // charged atoms (set_charges, elec_ngbr.c:115-121)
+      if (s->qch[i] != 0.) {
+        ich.push_back(g);
+        H.ncharge++;
+      }
+    }
+    if (H.ncharge > 0 && (!s->coultab || !s->dcoultab)) {
+      set_error("cm3d_nb_create: system %d: charged atoms but no coultab/dcoultab", sy);
+      return CM3D_NB_ERR_ARG;
+    }
+    // exclusion lists (CSR over global atom indices)
+    for (int i = 0; i < ns; i++) {
+      const int e0 = s->excl_off ? s->excl_off[i] : 0, e1 = s->excl_off ? s->excl_off[i + 1] : 0;
+      for (int k = e0; k < e1; k++) eidx.push_back(a0 + s->excl_idx[k]);
+      eoff[a0 + i + 1] = (int)eidx.size();
+      const int c0 = s->cexcl_off ? s->cexcl_off[i] : 0, c1 = s->cexcl_off ? s->cexcl_off[i + 1] : 0;
+      for (int k = c0; k < c1; k++) cidx.push_back(a0 + s->cexcl_idx[k]);
+      coff[a0 + i + 1] = (int)cidx.size();
+    }
+    // interactions: global indices inter0 + local, type map per system
+    P.ntypes = s->ntypes;
+    P.map0 = (int)map.size();
+    for (int k = 0; k < s->ntypes * s->ntypes; k++) map.push_back(s->map[k] >= 0 ? inter0 + s->map[k] : -1);
+    double r2 = 0;
+    for (int in = 0; in < s->ninter; in++) {
+      icut.push_back(s->rmaxs_cut2[in]);
+      icut.push_back(s->rmins_cut2[in]);
+      icut.push_back(s->rmaxl_cut2[in]);
+      icut.push_back(s->rminl_cut2[in]);
+      icut.push_back(s->rmaxs_skin2[in]);
+      icut.push_back(s->rmaxl_skin2[in]);
+      icut.push_back(s->dx2tab[in]);
+      icut.push_back(s->vtab[(size_t)in * nt + nt - 4]);
+      r2 = std::max(r2, s->rmaxl_skin2[in]);
+      for (int k = 0; k < nt; k++) {
+        vtab.push_back(s->vtab[(size_t)in * nt + k]);
+        dvtab.push_back(s->dvtab[(size_t)in * nt + k]);
+        swt.push_back(s->switchs ? s->switchs[(size_t)in * nt + k] : 0.0);
+      }
+    }
+    inter0 += s->ninter;
+    // charges: this system's erfc table and radii
+    if (H.ncharge > 0) {
+      P.coul = ncoul++;
+      for (int k = 0; k < nt; k++) {
+        coultab.push_back(s->coultab[k]);
+        dcoultab.push_back(s->dcoultab[k]);
+        switchse.push_back(s->switchse ? s->switchse[k] : 0.0);
+      }
+      P.rmaxl_skin2_e = s->rmaxl_skin2_e;
+      P.rmaxs_skin2_e = s->rmaxs_skin2_e;
+      P.rc2_el = (float)s->rmaxl_coul2;
+      P.dx2c = (float)s->dx2coul;
+      P.offc = (float)(s->rmins_coul2 * s->dx2coul);
+      P.tablast_e = (float)s->coultab[nt - 4];
+      r2 = std::max(r2, s->rmaxl_skin2_e);
+      H.ktot = s->ktot;
+      H.ka.assign(s->ka, s->ka + s->ktot);
+      H.kb.assign(s->kb, s->kb + s->ktot);
+      H.kc.assign(s->kc, s->kc + s->ktot);
+    } else {
+      P.coul = -1;
+      P.rmaxl_skin2_e = P.rmaxs_skin2_e = -1.0;
+    }
+    H.rlist = sqrt(r2);
+    // boxes narrower than two list radii need the on-the-fly minimum image
+    P.smallbox = 0;
+    for (int d = 0; d < 3; d++) {
+      double w = 1.0 / sqrt(H.hmati[3 * d] * H.hmati[3 * d] + H.hmati[3 * d + 1] * H.hmati[3 * d + 1] +
+                            H.hmati[3 * d + 2] * H.hmati[3 * d + 2]);
+      if (w < 2.0 * H.rlist) P.smallbox = 1;
+    }
+    a0 += ns;
   }
+  c->ncoul = ncoul;
+  c->ncharge = (int)ich.size();
+  c->ninter = inter0;
+  // the scalar fields describe system 0 (the plain engine and the single-system
+  // paths read them)
+  {
+    const cm3d_nb_system *s = s0;
+    const SysH &H = c->hs[0];
+    c->ntypes = s->ntypes;
+    c->ndof = H.ndof;
+    c->vlrc = s->vlrc;
+    c->wlrc = s->wlrc;
+    c->skin = s->skin_ter;
+    c->rheal = s->rheal;
+    memcpy(c->hmat, H.hmat, sizeof c->hmat);
+    memcpy(c->hmati, H.hmati, sizeof c->hmati);
+    c->kappa = s->kappa;
+    c->kappa2 = s->kappa * s->kappa;
+    c->falp2 = s->falp2;
+    c->ewald_self = s->ewald_self;
+    c->ewald_bkg = s->ewald_bkg;
+    c->dx2coul = s->dx2coul;
+    c->rmins_coul2 = s->rmins_coul2;
+    c->rmaxs_coul2 = s->rmaxs_coul2;
+    c->rminl_coul2 = s->rminl_coul2;
+    c->rmaxl_coul2 = s->rmaxl_coul2;
+    c->rmaxs_skin2_e = s->rmaxs_skin2_e;
+    c->rmaxl_skin2_e = s->rmaxl_skin2_e;
+    c->necorr = s->necorr;
+    c->nbonds = s->nbonds;
+    c->nbends = s->nbends;
+    c->tablast_e = H.ncharge > 0 ? s->coultab[nt - 4] : 0.0;
+    c->rlist_max = H.rlist;
+    for (int in = 0; in < s->ninter; in++) c->rc_lj_max = std::max(c->rc_lj_max, sqrt(s->rmaxl_cut2[in]));
+  }
+  // device arrays
   int rc;
   if ((rc = upload(&c->pos, pos.data(), n3))) return rc;
   if ((rc = upload(&c->vel, vel.data(), n3))) return rc;
@@ -236,44 +360,50 @@ static int create(const cm3d_nb_system *s, const cm3d_nb_options *opt, Ctx **out
   if ((rc = upload<double>(&c->fxs, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->fxa, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->dxn, pos.data(), n3))) return rc;
-  if ((rc = upload(&c->mass, s->amass, n))) return rc;
-  if ((rc = upload(&c->q, s->qch, n))) return rc;
-  if ((rc = upload(&c->itype, s->itype, n))) return rc;
-  if ((rc = upload(&c->map, s->map, (size_t)s->ntypes * s->ntypes))) return rc;
-  const size_t nt = (size_t)s->ninter * s->ntable;
-  if ((rc = upload(&c->vtab, s->vtab, nt))) return rc;
-  if ((rc = upload(&c->dvtab, s->dvtab, nt))) return rc;
-  if ((rc = upload(&c->switchs, s->switchs, nt))) return rc;
+  if ((rc = upload(&c->mass, mass.data(), n))) return rc;
+  if ((rc = upload(&c->q, q.data(), n))) return rc;
+  if ((rc = upload(&c->itype, itype.data(), n))) return rc;
+  if ((rc = upload(&c->sys_of, sys_of.data(), n))) return rc;
+  if ((rc = upload(&c->map, map.data(), map.size()))) return rc;
+  if ((rc = upload(&c->vtab, vtab.data(), vtab.size()))) return rc;
+  if ((rc = upload(&c->dvtab, dvtab.data(), dvtab.size()))) return rc;
+  if ((rc = upload(&c->switchs, swt.data(), swt.size()))) return rc;
   if ((rc = upload(&c->icut, icut.data(), icut.size()))) return rc;
-  if ((rc = upload(&c->coultab, c->ncharge ? s->coultab : nullptr, s->ntable))) return rc;
-  if ((rc = upload(&c->dcoultab, c->ncharge ? s->dcoultab : nullptr, s->ntable))) return rc;
-  if ((rc = upload(&c->switchse, c->ncharge && s->switchse ? s->switchse : nullptr, s->ntable))) return rc;
-  std::vector<int> zoff(n + 1, 0);
-  const int *eo = s->excl_off ? s->excl_off : zoff.data();
-  const int *co = s->cexcl_off ? s->cexcl_off : zoff.data();
-  if ((rc = upload(&c->excl_off, eo, n + 1))) return rc;
-  if ((rc = upload(&c->excl_idx, s->excl_idx, (size_t)eo[n]))) return rc;
-  if ((rc = upload(&c->cexcl_off, co, n + 1))) return rc;
-  if ((rc = upload(&c->cexcl_idx, s->cexcl_idx, (size_t)co[n]))) return rc;
+  if ((rc = upload(&c->coultab, coultab.data(), coultab.size()))) return rc;
+  if ((rc = upload(&c->dcoultab, dcoultab.data(), dcoultab.size()))) return rc;
+  if ((rc = upload(&c->switchse, switchse.data(), switchse.size()))) return rc;
+  if ((rc = upload(&c->excl_off, eoff.data(), eoff.size()))) return rc;
+  if ((rc = upload(&c->excl_idx, eidx.data(), eidx.size()))) return rc;
+  if ((rc = upload(&c->cexcl_off, coff.data(), coff.size()))) return rc;
+  if ((rc = upload(&c->cexcl_idx, cidx.data(), cidx.size()))) return rc;
   if ((rc = upload(&c->icharge, ich.data(), ich.size()))) return rc;
-  // accumulators + device copies of hmati (ACC_COUNT..+9) and hmat (+9..+18)
-  std::vector<double> acc0(ACC_COUNT + 18, 0.0);
-  for (int k = 0; k < 9; k++) {
-    acc0[ACC_COUNT + k] = c->hmati[k];
-    acc0[ACC_COUNT + 9 + k] = c->hmat[k];
-  }
+  // accumulators: per system ACC_COUNT sums + device copies of hmati and hmat
+  std::vector<double> acc0((size_t)nsys * ACC_STRIDE, 0.0);
+  for (int sy = 0; sy < nsys; sy++)
+    for (int k = 0; k < 9; k++) {
+      acc0[(size_t)sy * ACC_STRIDE + ACC_COUNT + k] = c->hs[sy].hmati[k];
+      acc0[(size_t)sy * ACC_STRIDE + ACC_COUNT + 9 + k] = c->hs[sy].hmat[k];
+    }
   if ((rc = upload(&c->acc, acc0.data(), acc0.size()))) return rc;
   if ((rc = upload<long long>(&c->stat, nullptr, ST_COUNT))) return rc;
   if ((rc = upload<int>(&c->istate, nullptr, IS_COUNT))) return rc;
-  CK(cudaMallocHost(&c->h_acc, sizeof(double) * (ACC_COUNT + 18)));
+  if ((rc = upload<int>(&c->sreb, nullptr, (size_t)nsys))) return rc;
+  if ((rc = upload<int>(&c->slast, nullptr, (size_t)nsys))) return rc;
+  if ((rc = upload<long long>(&c->sstat, nullptr, (size_t)nsys * SS_COUNT))) return rc;
+  CK(cudaMallocHost(&c->h_acc, sizeof(double) * (size_t)nsys * ACC_STRIDE));
   CK(cudaMallocHost(&c->h_stat, sizeof(long long) * ST_COUNT));
   CK(cudaMallocHost(&c->h_istate, sizeof(int) * IS_COUNT));
+  CK(cudaMallocHost(&c->h_sstat, sizeof(long long) * (size_t)nsys * SS_COUNT));
   memset(c->h_istate, 0, sizeof(int) * IS_COUNT);
   if ((rc = list_setup(c))) return rc;
   if ((rc = pair_setup(c))) return rc;
-  if ((rc = kspace_setup(c, s))) return rc;
-  if ((rc = step_setup(c, s))) return rc;
-  if (s->ntors > 0 || s->n14 > 0 || s->nbondx > 0) c->name = "has-torsions";
+  if ((rc = kspace_setup(c))) return rc;
+  if ((rc = step_setup(c, systems, nsys))) return rc;
+  if ((rc = upload(&c->sp, c->h_sp.data(), c->h_sp.size()))) return rc;
+  for (int sy = 0; sy < nsys; sy++) {
+    const cm3d_nb_system *s = systems + sy;
+    if (s->ntors > 0 || s->n14 > 0 || s->nbondx > 0) c->name = "has-torsions";
+  }
   CK(cudaDeviceSynchronize());
   return CM3D_NB_OK;
 }
@@ -336,7 +466,8 @@ static double *block_of(Ctx *c, int which) {
 }
 
 static int pull_acc(Ctx *c) {
-  CK(cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * ACC_COUNT, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(c->h_acc, c->acc, sizeof(double) * (size_t)c->nsys * ACC_STRIDE, cudaMemcpyDeviceToHost,
+                     c->st));
   CK(cudaStreamSynchronize(c->st));
   return CM3D_NB_OK;
 }
@@ -389,8 +520,12 @@ void cm3d_nb_default_options(cm3d_nb_options *opt) {
 }
 
 int cm3d_nb_create(const cm3d_nb_system *sys, const cm3d_nb_options *opt, cm3d_nb_ctx **out) {
+  return cm3d_nb_create_batch(sys, 1, opt, out);
+}
+
+int cm3d_nb_create_batch(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options *opt, cm3d_nb_ctx **out) {
   Ctx *c = nullptr;
-  int rc = create(sys, opt, &c);
+  int rc = create(systems, nsys, opt, &c);
   if (rc) {
     destroy(c);
     if (out) *out = nullptr;
@@ -468,7 +603,7 @@ int cm3d_nb_set_forces(cm3d_nb_ctx *ctx, int which, const double *fx, const doub
 
 int cm3d_nb_get_ngbr(cm3d_nb_ctx *ctx) {
   CTX;
-  return build_lists(c, false);
+  return build_lists(c, false, true);
 }
 
 int cm3d_nb_nrefsh(cm3d_nb_ctx *ctx, int istep, int *rebuilt) {
@@ -486,7 +621,7 @@ int cm3d_nb_nrefsh(cm3d_nb_ctx *ctx, int istep, int *rebuilt) {
   CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (c->h_istate[IS_REBUILD]) {
-    if ((rc = build_lists(c, false))) return rc;
+    if ((rc = build_lists(c, false, false))) return rc;
     if (rebuilt) *rebuilt = 1;
   }
   return CM3D_NB_OK;
@@ -497,8 +632,10 @@ int cm3d_nb_force(cm3d_nb_ctx *ctx, int iflg) {
   return run_force(c, iflg);
 }
 
+// zero accumulator slots [first, first + count) of every system
 static int zero_slots(Ctx *c, int first, int count) {
-  CK(cudaMemsetAsync(c->acc + first, 0, sizeof(double) * count, c->st));
+  CK(cudaMemset2DAsync(c->acc + first, sizeof(double) * ACC_STRIDE, 0, sizeof(double) * count, (size_t)c->nsys,
+                       c->st));
   return CM3D_NB_OK;
 }
 
@@ -595,14 +732,16 @@ int cm3d_nb_getsvirter_e(cm3d_nb_ctx *ctx, double *velec, double *welec, double 
   return CM3D_NB_OK;
 }
 
-// fk_ewald's totals (md_ewald.c:336-348) plus ecorr, as getvewald adds them
-static void ewald_totals(Ctx *c, double *pot, double *prs, double tens[9]) {
-  const double *a = c->h_acc;
-  double six = c->ncharge > 0 ? c->ewald_bkg / deth(c->hmat) : 0.0;
+// fk_ewald's totals (md_ewald.c:336-348) plus ecorr, as getvewald adds
+// them, for system `sy` (pulled accumulators)
+static void ewald_totals(Ctx *c, int sy, double *pot, double *prs, double tens[9]) {
+  const SysH &H = c->hs[sy];
+  const double *a = c->h_acc + (size_t)sy * ACC_STRIDE;
+  double six = H.ncharge > 0 ? H.ewald_bkg / deth(H.hmat) : 0.0;
   double vk = a[ACC_VK], vp = a[ACC_VP];
   double vk_ewald = 0, vp_ewald = 0, vpt[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (c->iperd == 3) {
-    vk_ewald = vk + six + (c->ncharge > 0 ? c->ewald_self : 0.0);
+  if (H.iperd == 3) {
+    vk_ewald = vk + six + (H.ncharge > 0 ? H.ewald_self : 0.0);
     vp_ewald = vp + 3. * (vk + six);
     for (int k = 0; k < 9; k++) vpt[k] = a[ACC_VPT + k];
     vpt[0] += vk + six;
@@ -621,7 +760,7 @@ int cm3d_nb_getvewald(cm3d_nb_ctx *ctx, double *pot_ewald, double *prs_ewald, do
   int rc;
   if ((rc = pull_acc(c))) return rc;
   double p, w, t[9];
-  ewald_totals(c, &p, &w, t);
+  ewald_totals(c, 0, &p, &w, t);
   *pot_ewald += p;
   *prs_ewald += w;
   for (int k = 0; k < 9; k++) prs_ewald_tensor[k] += t[k];
@@ -638,7 +777,7 @@ int cm3d_nb_step_init(cm3d_nb_ctx *ctx) {
   c->h_istate[IS_ISTEP] = 0;
   c->h_istate[IS_ISTEPLAST] = 0;
   CK(cudaMemcpyAsync(c->istate, c->h_istate, sizeof(int) * 2, cudaMemcpyHostToDevice, c->st));
-  if ((rc = build_lists(c, false))) return rc;
+  if ((rc = build_lists(c, false, true))) return rc;
   if ((rc = run_force(c, 1))) return rc;
   if ((rc = run_force(c, 2))) return rc;
   c->forces_valid = true;
@@ -654,11 +793,10 @@ int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
   return run_step(c, istep0, nsteps);
 }
 
-int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e) {
-  CTX;
-  int rc;
-  if ((rc = pull_acc(c))) return rc;
-  const double *a = c->h_acc;
+// getvireal(...,1)+geteng() of system `sy` from the pulled accumulators
+static void energies_of(Ctx *c, int sy, cm3d_nb_energies *e) {
+  const SysH &H = c->hs[sy];
+  const double *a = c->h_acc + (size_t)sy * ACC_STRIDE;
   memset(e, 0, sizeof *e);
   e->vinter = a[ACC_SPOTL];
   e->vhinter = a[ACC_SPOTHL];
@@ -667,30 +805,82 @@ int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e) {
   e->velec = a[ACC_SPOTE];
   e->welec = a[ACC_SPRSE];
   sym9(a, ACC_SPRSET, e->welectensor);
-  ewald_totals(c, &e->vewald, &e->wewald, e->wewaldtensor);
+  ewald_totals(c, sy, &e->vewald, &e->wewald, e->wewaldtensor);
   e->vbond = a[ACC_VBOND];
   e->wbond = a[ACC_WBOND];
   e->vbend = a[ACC_VBEND];
   e->wbend = 0.;
-  double vol = deth(c->hmat), rvol = 1. / vol;
+  double vol = deth(H.hmat), rvol = 1. / vol;
   e->US = e->vhinter + e->velec + e->vewald;
   e->U = e->vinter + e->velec + e->vewald;
   e->W = e->winter + e->welec + e->wewald;
   for (int k = 0; k < 9; k++) e->Wtensor[k] = e->wintertensor[k] + e->welectensor[k] + e->wewaldtensor[k];
-  e->W -= 3 * c->wlrc * rvol;
-  e->Wtensor[0] -= c->wlrc * rvol;
-  e->Wtensor[4] -= c->wlrc * rvol;
-  e->Wtensor[8] -= c->wlrc * rvol;
+  e->W -= 3 * H.wlrc * rvol;
+  e->Wtensor[0] -= H.wlrc * rvol;
+  e->Wtensor[4] -= H.wlrc * rvol;
+  e->Wtensor[8] -= H.wlrc * rvol;
   sym9(a, ACC_P2MT, e->p2m_tensor);
   double p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
   double UI = e->vbond + e->vbend, WI = e->wbond;
-  e->poth = e->US + c->vlrc / vol;
-  e->poter = e->U + c->vlrc / vol;
+  e->poth = e->US + H.vlrc / vol;
+  e->poter = e->U + H.vlrc / vol;
   e->potra = UI;
   e->prsi = (p2m + e->W + WI) / (3 * vol);
   for (int k = 0; k < 9; k++) e->prs_tensor[k] = (e->p2m_tensor[k] + e->Wtensor[k] + a[ACC_WBONDT + k]) / vol;
   e->zke = .5 * p2m;
-  e->tiout = p2m / (double)c->ndof;
+  e->tiout = p2m / (double)H.ndof;
+}
+
+int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e) {
+  return cm3d_nb_get_system_energies(ctx, 0, e);
+}
+
+int cm3d_nb_get_system_energies(cm3d_nb_ctx *ctx, int sys, cm3d_nb_energies *e) {
+  CTX;
+  int rc;
+  if (sys < 0 || sys >= c->nsys) {
+    set_error("get_system_energies: system %d of %d", sys, c->nsys);
+    return CM3D_NB_ERR_ARG;
+  }
+  if ((rc = pull_acc(c))) return rc;
+  energies_of(c, sys, e);
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_get_all_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e) {
+  CTX;
+  int rc;
+  if ((rc = pull_acc(c))) return rc;
+  for (int s = 0; s < c->nsys; s++) energies_of(c, s, e + s);
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_num_systems(cm3d_nb_ctx *ctx, int *nsys) {
+  CTX;
+  *nsys = c->nsys;
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_system_atoms(cm3d_nb_ctx *ctx, int sys, int *first, int *natoms) {
+  CTX;
+  if (sys < 0 || sys >= c->nsys) {
+    set_error("system_atoms: system %d of %d", sys, c->nsys);
+    return CM3D_NB_ERR_ARG;
+  }
+  *first = c->h_sp[sys].a0;
+  *natoms = c->h_sp[sys].n;
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_system_counts(cm3d_nb_ctx *ctx, long long *rebuilds, long long *resets) {
+  CTX;
+  CK(cudaMemcpyAsync(c->h_sstat, c->sstat, sizeof(long long) * (size_t)c->nsys * SS_COUNT, cudaMemcpyDeviceToHost,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  for (int s = 0; s < c->nsys; s++) {
+    if (rebuilds) rebuilds[s] = c->h_sstat[(size_t)s * SS_COUNT + SS_REBUILDS];
+    if (resets) resets[s] = c->h_sstat[(size_t)s * SS_COUNT + SS_RESETS];
+  }
   return CM3D_NB_OK;
 }
 
@@ -703,7 +893,7 @@ static int ensure_half_lists(Ctx *c) {
   std::swap(c->pos, c->dxn);
   c->want_half = true;
   c->no_snapshot = true;
-  int rc = build_lists(c, false);
+  int rc = build_lists(c, false, true);
   std::swap(c->pos, c->dxn);
   c->want_half = false;
   c->no_snapshot = false;

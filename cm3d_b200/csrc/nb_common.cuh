@@ -40,7 +40,37 @@ enum {
   ACC_WBONDT = 48,        // 9
   ACC_VBEND = 57,         // getvbend energy
   ACC_P2MT = 58,          // 9: get_p2mt kinetic tensor
-  ACC_COUNT = 72
+  ACC_COUNT = 72,
+  // each system owns ACC_STRIDE doubles of acc[]: its accumulators, then
+  // device copies of its H^-1 (ACC_COUNT..+9) and H (+9..+18)
+  ACC_STRIDE = 96
+};
+
+// Per-system parameters of a context that holds several independent systems
+// (a batch), one entry per system in a device array.  The systems' atoms are
+// concatenated: system s owns atoms [a0, a0 + n), in original order and in
+// cell-sorted order alike, cells [c0, c0 + ncells), charged atoms
+// icharge[q0 .. q0 + nq) and k rows / k-vectors / tiles as below.
+struct SysP {
+  int a0, n;
+  int c0, ncells, nc[3];
+  int nsx, nsy, nsz, sx[3], sy[3], sz[3];   // unique stencil offsets per axis
+  int ntypes, map0;          // type map at map[map0 ...], ntypes^2 global interaction indices
+  int coul;                  // Coulomb table index (tables at coul * ntable), -1: no charges
+  int smallbox;              // box narrower than two list radii: minimum image per pair
+  int q0, nq;
+  int krow0, nrows, kk0, ktot;   // k rows and k-vectors (global indices)
+  int ktile0, ktiles;        // structure-factor tiles (global tile ids)
+  int ftile0, ftiles;        // reciprocal-force tiles (global tile ids)
+  long long spart0;          // first per-tile partial S(k) of the system
+  float lim2;                // FP32 list prefilter radius^2 (inf = off)
+  float rc2_el, dx2c, offc, tablast_e;
+  float hF[9], hiF[9];
+  double h[9], hi[9];
+  double rmaxl_skin2_e, rmaxs_skin2_e;   // -1 without charges
+  double skin2q;             // (skin / 2)^2
+  double falp2, rvol, kappa, kappa2;
+  float4 shift[27];          // cell-corner shifts H k / nc, k in {-1, 0, 1}^3
 };
 // device status words (long long)
 enum {
@@ -71,6 +101,32 @@ enum {
 __device__ __forceinline__ bool gated_off(const int *gs, int need_rebuild) {
   return gs && (gs[IS_HALT] != 0 || (need_rebuild && gs[IS_REBUILD] == 0));
 }
+// per-system counters (sstat[s * SS_COUNT + ...])
+enum { SS_REBUILDS = 0, SS_RESETS = 1, SS_COUNT = 2 };
+
+// Sum NV per-thread values into the accumulators of each thread's system
+// (acc + sys * ACC_STRIDE + slots[k]).  A warp whose threads all belong to
+// one system reduces first and adds once; a mixed warp adds per thread.
+// Threads with sys < 0 contribute nothing.  Every thread of the warp calls it.
+template <int NV>
+__device__ __forceinline__ void sys_acc(double (&v)[NV], int sys, double *acc, const int *slots) {
+  const unsigned full = 0xffffffffu;
+  const int s0 = __shfl_sync(full, sys, 0);
+  if (__all_sync(full, sys == s0 || sys < 0)) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double s = sys < 0 ? 0.0 : v[k];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
+      if ((threadIdx.x & 31) == 0 && s != 0.0 && s0 >= 0) atomicAdd(acc + (size_t)s0 * ACC_STRIDE + slots[k], s);
+    }
+  } else if (sys >= 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+      if (v[k] != 0.0) atomicAdd(acc + (size_t)sys * ACC_STRIDE + slots[k], v[k]);
+  }
+}
+
 // list totals (long long) written by the list builder
 enum { LT_T = 0, LT_S = 1, LT_TE = 2, LT_SE = 3, LT_FULL = 4, LT_COUNT = 5 };
 
@@ -96,9 +152,35 @@ struct Timing {
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
 };
 
+// host-side facts of one system of a batch (energies, set-up)
+struct SysH {
+  int n = 0, ncharge = 0, ndof = 1, ntypes = 0, ninter = 0, ktot = 0, iperd = 3;
+  double hmat[9], hmati[9];
+  double vlrc = 0, wlrc = 0, ewald_self = 0, ewald_bkg = 0;
+  double rlist = 0;          // largest list radius (LJ or charges, with skin)
+  std::vector<int4> krows;   // k rows {ka, kb, kc0, len} of the system's k set
+  std::vector<int> krow_k0;  // first k of each row (system-local)
+  std::vector<int> ka, kb, kc;
+};
+
 struct Ctx {
   // ---- configuration
   int dev = 0;
+  // ---- systems (a single system is a batch of one)
+  int nsys = 1;
+  std::vector<SysP> h_sp;              // per-system parameters, host copy
+  std::vector<SysH> hs;
+  SysP *sp = nullptr;                  // device copy
+  int *sys_of = nullptr;               // per atom: its system
+  int *cell_sys = nullptr;             // per cell: its system
+  int *sreb = nullptr;                 // per system: rebuild requested (nrefsh)
+  int *slast = nullptr;                // per system: md_finter.c's isteplast
+  long long *sstat = nullptr;          // per system: SS_* counters
+  long long *h_sstat = nullptr;
+  int *ktile_sys = nullptr, *ftile_sys = nullptr, *k_sys = nullptr;   // k-space tiles / k -> system
+  int ktiles_tot = 0, ftiles_tot = 0, nrows_max = 0;
+  int ncoul = 0;                       // erfc tables (one per system with charges)
+  int all_rebuild = 1;                 // list kernels: rebuild every system (host-driven builds)
   int num_sms = 148;
   cudaStream_t st = nullptr;
   int mode = CM3D_NB_MIXED;
@@ -291,14 +373,13 @@ __device__ __forceinline__ void block_acc(double (&v)[NV], double *acc, const in
 int plain_pairs(Ctx *c, int iflg, int which);   // nb_plain.cu
 int plain_ecorr(Ctx *c, const int2 *ij);        // nb_plain.cu
 int mixed_pairs(Ctx *c, int iflg, int mask);    // nb_pair.cu
-int build_lists(Ctx *c, bool device_flag);      // nb_list.cu
+int build_lists(Ctx *c, bool device_flag, bool all);   // nb_list.cu
 int list_setup(Ctx *c);                         // nb_list.cu
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused
 int pair_setup(Ctx *c);                         // nb_pair.cu
 int kspace_forces(Ctx *c);                      // nb_kspace.cu
-int kspace_setup(Ctx *c, const cm3d_nb_system *s);
-int ecorr_forces(Ctx *c);                       // nb_kspace.cu (plain, atomic)
-int step_setup(Ctx *c, const cm3d_nb_system *s);// nb_step.cu
+int kspace_setup(Ctx *c);                       // nb_kspace.cu
+int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys);   // nb_step.cu
 int run_step(Ctx *c, int istep0, int nsteps);   // nb_step.cu
 int run_force(Ctx *c, int iflg);                // nb_step.cu
 int run_bonded(Ctx *c);                         // nb_step.cu

@@ -37,13 +37,19 @@ constexpr int KF_A = 2;            // atoms per thread, forces
 constexpr int MAX_ROWLEN = 128;    // 2 kmax + 1 <= 128
 
 // ------------------------------------------------------------ mixed mode
+// BATCH = true (every kernel below): the context holds several systems and
+// each tile / k / atom takes its box, rows and tiles from its system's SysP;
+// BATCH = false: one system described by the scalar arguments.
+template <bool BATCH>
 __global__ void k_kprep(int nq, const int *__restrict__ icharge, int n, const double *__restrict__ pos,
-                        const double *__restrict__ q, const double *__restrict__ hmati, uint4 *__restrict__ kfrac,
+                        const double *__restrict__ q, const double *__restrict__ hmati_one,
+                        const SysP *__restrict__ sp, const int *__restrict__ sys_of, uint4 *__restrict__ kfrac,
                         double4 *__restrict__ kposd, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   int jq = blockIdx.x * blockDim.x + threadIdx.x;
   if (jq >= nq) return;
   int i = icharge[jq];
+  const double *hmati = BATCH ? sp[sys_of[i]].hi : hmati_one;
   double x = pos[i], y = pos[n + i], z = pos[2 * n + i];
   const double fact = sqrt(4.0 * M_PI);   // md_ewald.c:202
   double tq = q[i] * fact;
@@ -63,23 +69,37 @@ __device__ __forceinline__ float phase_rad(unsigned phi) {
   return (float)(int)phi * 1.4629180792671596e-09f;   // 2 pi / 2^32
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *__restrict__ kfrac, int nrows,
                                                            const int4 *__restrict__ rows,
                                                            const int *__restrict__ row_k0, int rows_per_block,
                                                            int ktot, double2 *__restrict__ spart,
+                                                           const SysP *__restrict__ sp,
+                                                           const int *__restrict__ tile_sys,
                                                            const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   __shared__ float2 red[KS_THREADS / 32][MAX_ROWLEN];
-  const int tile = blockIdx.x;
-  const int r0 = blockIdx.y * rows_per_block;
-  const int r1 = min(nrows, r0 + rows_per_block);
+  // this block's atoms [abase, aend), rows [rbeg, rend) and partial-S(k) base
+  int abase = blockIdx.x * (KS_THREADS * KS_A), aend = nq, rbeg = 0, rend = nrows;
+  long long sbase = (long long)blockIdx.x * ktot;
+  if (BATCH) {
+    const SysP &S = sp[tile_sys[blockIdx.x]];
+    const int lt = blockIdx.x - S.ktile0;
+    abase = S.q0 + lt * (KS_THREADS * KS_A);
+    aend = S.q0 + S.nq;
+    rbeg = S.krow0;
+    rend = S.krow0 + S.nrows;
+    sbase = S.spart0 + (long long)lt * S.ktot - S.kk0;
+  }
+  const int r0 = rbeg + blockIdx.y * rows_per_block;
+  const int r1 = min(rend, r0 + rows_per_block);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned u0[KS_A], u1[KS_A], u2[KS_A];
   float tq[KS_A], cs[KS_A], sn[KS_A];
 #pragma unroll
   for (int m = 0; m < KS_A; m++) {
-    int a = tile * (KS_THREADS * KS_A) + m * KS_THREADS + threadIdx.x;
-    if (a < nq) {
+    int a = abase + m * KS_THREADS + threadIdx.x;
+    if (a < aend) {
       uint4 v = kfrac[a];
       u0[m] = v.x; u1[m] = v.y; u2[m] = v.z;
       tq[m] = __uint_as_float(v.w);
@@ -123,24 +143,43 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
         ar += red[q2][kk].x;
         ai += red[q2][kk].y;
       }
-      spart[(size_t)tile * ktot + k0 + kk] = make_double2(ar, ai);
+      spart[sbase + k0 + kk] = make_double2(ar, ai);
     }
     __syncthreads();
   }
 }
 
-// per-k totals; every k of CM3D's list is one thread (md_ewald.c:247-305)
+// per-k totals; every k of CM3D's list is one thread (md_ewald.c:247-305).
+// BATCH: exactly one k per thread (ktot = all systems' k-vectors), so that
+// each thread's sums belong to one system.
+template <bool BATCH>
 __global__ void k_sred(int ktot, int ntiles, const double2 *__restrict__ spart, const int *__restrict__ ka,
-                       const int *__restrict__ kb, const int *__restrict__ kc, const double *__restrict__ hmati,
-                       double rvol, double falp2, double2 *__restrict__ sk, float2 *__restrict__ akf,
-                       double2 *__restrict__ akd, double *__restrict__ acc, const int *__restrict__ gs) {
+                       const int *__restrict__ kb, const int *__restrict__ kc, const double *__restrict__ hmati_one,
+                       double rvol_one, double falp2_one, double2 *__restrict__ sk, float2 *__restrict__ akf,
+                       double2 *__restrict__ akd, double *__restrict__ acc, const SysP *__restrict__ sp,
+                       const int *__restrict__ k_sys, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   double v[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   const double TPI = 2.0 * M_PI;
+  int sys = -1;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ktot; k += gridDim.x * blockDim.x) {
+    const double *hmati = hmati_one;
+    double rvol = rvol_one, falp2 = falp2_one;
+    int nt = ntiles, kstride = ktot;
+    long long sb = k;
+    if (BATCH) {
+      sys = k_sys[k];
+      const SysP &S = sp[sys];
+      hmati = S.hi;
+      rvol = S.rvol;
+      falp2 = S.falp2;
+      nt = S.ktiles;
+      kstride = S.ktot;
+      sb = S.spart0 + (k - S.kk0);
+    }
     double sr = 0, si = 0;
-    for (int t = 0; t < ntiles; t++) {
-      double2 p = spart[(size_t)t * ktot + k];
+    for (int t = 0; t < nt; t++) {
+      double2 p = spart[sb + (long long)t * kstride];
       sr += p.x;
       si += p.y;
     }
@@ -164,24 +203,45 @@ __global__ void k_sred(int ktot, int ntiles, const double2 *__restrict__ spart, 
   }
   const int slots[11] = {ACC_VK, ACC_VP, ACC_VPT + 0, ACC_VPT + 1, ACC_VPT + 2, ACC_VPT + 3,
                          ACC_VPT + 4, ACC_VPT + 5, ACC_VPT + 6, ACC_VPT + 7, ACC_VPT + 8};
-  block_acc<11>(v, acc, slots);
+  if (BATCH) sys_acc<11>(v, sys, acc, slots);
+  else block_acc<11>(v, acc, slots);
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4 *__restrict__ kfrac,
                                                              const int *__restrict__ icharge, int n, int nrows,
                                                              const int4 *__restrict__ rows,
                                                              const int *__restrict__ row_k0, int rows_per_split,
                                                              const float2 *__restrict__ akf, int ktot,
-                                                             const double *__restrict__ hmati, int atomic,
+                                                             const double *__restrict__ hmati_one, int atomic,
                                                              double *__restrict__ fxl,
+                                                             const SysP *__restrict__ sp,
+                                                             const int *__restrict__ tile_sys,
                                                              const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   extern __shared__ float2 ak_s[];
-  const int r0 = blockIdx.y * rows_per_split;
-  const int r1 = min(nrows, r0 + rows_per_split);
+  // this block's charged atoms [abase, aend), rows [r0, r1) and k range
+  int r0, r1, kend, abase, aend;
+  const double *hmati = hmati_one;
+  if (BATCH) {
+    const SysP &S = sp[tile_sys[blockIdx.x]];
+    const int rps = (S.nrows + gridDim.y - 1) / gridDim.y;
+    const int rend = S.krow0 + S.nrows;
+    r0 = S.krow0 + blockIdx.y * rps;
+    r1 = min(rend, r0 + rps);
+    kend = r1 < rend ? (r1 > r0 ? row_k0[r1] : 0) : S.kk0 + S.ktot;
+    abase = S.q0 + (blockIdx.x - S.ftile0) * (blockDim.x * KF_A);
+    aend = S.q0 + S.nq;
+    hmati = S.hi;
+  } else {
+    r0 = blockIdx.y * rows_per_split;
+    r1 = min(nrows, r0 + rows_per_split);
+    kend = (r1 < nrows) ? row_k0[r1] : ktot;
+    abase = blockIdx.x * (blockDim.x * KF_A);
+    aend = nq;
+  }
   if (r0 >= r1) return;
   const int kbase = row_k0[r0];
-  const int kend = (r1 < nrows) ? row_k0[r1] : ktot;
   for (int k = threadIdx.x; k < kend - kbase; k += blockDim.x) ak_s[k] = akf[kbase + k];
   __syncthreads();
   unsigned u0[KF_A], u1[KF_A], u2[KF_A];
@@ -190,9 +250,9 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
   int jq[KF_A];
 #pragma unroll
   for (int m = 0; m < KF_A; m++) {
-    jq[m] = blockIdx.x * (blockDim.x * KF_A) + m * blockDim.x + threadIdx.x;
+    jq[m] = abase + m * blockDim.x + threadIdx.x;
     U0[m] = U1[m] = U2[m] = 0.0;
-    if (jq[m] < nq) {
+    if (jq[m] < aend) {
       uint4 v = kfrac[jq[m]];
       u0[m] = v.x; u1[m] = v.y; u2[m] = v.z;
       tq[m] = __uint_as_float(v.w);
@@ -238,7 +298,7 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
   const double TPI = 2.0 * M_PI;
 #pragma unroll
   for (int m = 0; m < KF_A; m++) {
-    if (jq[m] >= nq) continue;
+    if (jq[m] >= aend) continue;
     int i = icharge[jq[m]];
     double t = TPI * (double)tq[m];
     // F = tq 2 pi H^-T U  (k = 2 pi H^-T n, md_ewald.c:248-251)
@@ -363,67 +423,146 @@ __global__ void k_kforce_plain(int nq, const double4 *__restrict__ kp, const int
 }
 
 // ------------------------------------------------------------------ host
-int kspace_setup(Ctx *c, const cm3d_nb_system *s) {
-  if (c->ncharge == 0 || c->ktot == 0) return CM3D_NB_OK;
+// k rows, tiles and partial-S(k) layout of every system (SysP fields q0 ..
+// spart0), all systems' rows / k-vectors concatenated
+int kspace_setup(Ctx *c) {
   std::vector<int4> rows;
-  std::vector<int> k0;
-  for (int k = 0; k < s->ktot;) {
-    int e = k + 1;
-    while (e < s->ktot && s->ka[e] == s->ka[k] && s->kb[e] == s->kb[k] && s->kc[e] == s->kc[e - 1] + 1 &&
-           e - k < MAX_ROWLEN)
-      e++;
-    rows.push_back(make_int4(s->ka[k], s->kb[k], s->kc[k], e - k));
-    k0.push_back(k);
-    k = e;
+  std::vector<int> k0, ka, kb, kc, k_sys, ktile_sys, ftile_sys;
+  const bool mixed = c->mode == CM3D_NB_MIXED;
+  const int per_tile = mixed ? KS_THREADS * KS_A : KS_THREADS;
+  const int per_ftile = mixed ? KS_THREADS * KF_A : KS_THREADS;
+  int qoff = 0, nrows_max = 0;
+  long long spart_tot = 0;
+  for (int sy = 0; sy < c->nsys; sy++) {
+    SysP &P = c->h_sp[sy];
+    const SysH &H = c->hs[sy];
+    P.q0 = qoff;
+    P.nq = H.ncharge;
+    qoff += H.ncharge;
+    P.krow0 = (int)rows.size();
+    P.kk0 = (int)ka.size();
+    P.ktot = H.ncharge > 0 ? H.ktot : 0;
+    // CM3D's k set (ewald_setup, md_ewald.c:93-114) as rows of constant
+    // (ka, kb) and consecutive kc
+    for (int k = 0; k < P.ktot;) {
+      int e = k + 1;
+      while (e < P.ktot && H.ka[e] == H.ka[k] && H.kb[e] == H.kb[k] && H.kc[e] == H.kc[e - 1] + 1 &&
+             e - k < MAX_ROWLEN)
+        e++;
+      rows.push_back(make_int4(H.ka[k], H.kb[k], H.kc[k], e - k));
+      k0.push_back(P.kk0 + k);
+      k = e;
+    }
+    for (int k = 0; k < P.ktot; k++) {
+      ka.push_back(H.ka[k]);
+      kb.push_back(H.kb[k]);
+      kc.push_back(H.kc[k]);
+      k_sys.push_back(sy);
+    }
+    P.nrows = (int)rows.size() - P.krow0;
+    nrows_max = std::max(nrows_max, P.nrows);
+    P.ktile0 = (int)ktile_sys.size();
+    P.ktiles = P.ktot > 0 ? (P.nq + per_tile - 1) / per_tile : 0;
+    for (int t = 0; t < P.ktiles; t++) ktile_sys.push_back(sy);
+    P.ftile0 = (int)ftile_sys.size();
+    P.ftiles = P.ktot > 0 ? (P.nq + per_ftile - 1) / per_ftile : 0;
+    for (int t = 0; t < P.ftiles; t++) ftile_sys.push_back(sy);
+    P.spart0 = spart_tot;
+    spart_tot += (long long)P.ktiles * P.ktot;
   }
+  c->ktot = (int)ka.size();
   c->nrows = (int)rows.size();
-  CK(cudaMalloc(&c->rows, sizeof(int4) * rows.size()));
-  CK(cudaMalloc(&c->row_k0, sizeof(int) * k0.size()));
-  CK(cudaMemcpy(c->rows, rows.data(), sizeof(int4) * rows.size(), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->row_k0, k0.data(), sizeof(int) * k0.size(), cudaMemcpyHostToDevice));
-  int per_tile = c->mode == CM3D_NB_MIXED ? KS_THREADS * KS_A : KS_THREADS;
-  c->ks_tiles = (c->ncharge + per_tile - 1) / per_tile;
+  c->nrows_max = nrows_max;
+  c->ktiles_tot = (int)ktile_sys.size();
+  c->ftiles_tot = (int)ftile_sys.size();
+  if (c->ncharge == 0 || c->ktot == 0) return CM3D_NB_OK;
+  c->ks_tiles = c->h_sp[0].ktiles;
   c->ks_tile_atoms = per_tile;
-  CK(cudaMalloc(&c->spart, sizeof(double2) * (size_t)c->ks_tiles * c->ktot));
+  auto up = [&](int **dst, const std::vector<int> &v) -> int {
+    CK(cudaMalloc(dst, sizeof(int) * (v.empty() ? 1 : v.size())));
+    if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), sizeof(int) * v.size(), cudaMemcpyHostToDevice));
+    return CM3D_NB_OK;
+  };
+  int rc;
+  CK(cudaMalloc(&c->rows, sizeof(int4) * rows.size()));
+  CK(cudaMemcpy(c->rows, rows.data(), sizeof(int4) * rows.size(), cudaMemcpyHostToDevice));
+  if ((rc = up(&c->row_k0, k0)) || (rc = up(&c->ka_d, ka)) || (rc = up(&c->kb_d, kb)) || (rc = up(&c->kc_d, kc)) ||
+      (rc = up(&c->k_sys, k_sys)) || (rc = up(&c->ktile_sys, ktile_sys)) || (rc = up(&c->ftile_sys, ftile_sys)))
+    return rc;
+  CK(cudaMalloc(&c->spart, sizeof(double2) * (size_t)(spart_tot > 0 ? spart_tot : 1)));
   CK(cudaMalloc(&c->sk, sizeof(double2) * (size_t)c->ktot));
-  if (c->mode == CM3D_NB_MIXED) {
+  if (mixed) {
     CK(cudaMalloc(&c->akf, sizeof(float2) * (size_t)c->ktot));
     CK(cudaMalloc(&c->kfrac, sizeof(uint4) * (size_t)c->ncharge));
   } else {
     CK(cudaMalloc(&c->akd, sizeof(double2) * (size_t)c->ktot));
   }
   CK(cudaMalloc(&c->kposd, sizeof(double4) * (size_t)c->ncharge));
-  CK(cudaMalloc(&c->ka_d, sizeof(int) * (size_t)c->ktot));
-  CK(cudaMalloc(&c->kb_d, sizeof(int) * (size_t)c->ktot));
-  CK(cudaMalloc(&c->kc_d, sizeof(int) * (size_t)c->ktot));
-  CK(cudaMemcpy(c->ka_d, s->ka, sizeof(int) * (size_t)c->ktot, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->kb_d, s->kb, sizeof(int) * (size_t)c->ktot, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(c->kc_d, s->kc, sizeof(int) * (size_t)c->ktot, cudaMemcpyHostToDevice));
   // split the rows over enough blocks to fill the machine in the force pass
-  int per_block = c->mode == CM3D_NB_MIXED ? KS_THREADS * KF_A : KS_THREADS;
-  int tiles = (c->ncharge + per_block - 1) / per_block;
   int split = 1;
-  while (tiles * split < 148 * 4 && split < c->nrows) split *= 2;
+  while ((long long)c->ftiles_tot * split < 148 * 4 && split < nrows_max) split *= 2;
   // every split's A(k) must fit in shared memory
   for (;;) {
-    int rps = (c->nrows + split - 1) / split;
     size_t mx = 0;
-    for (int r0 = 0; r0 < c->nrows; r0 += rps) {
-      int r1 = r0 + rps < c->nrows ? r0 + rps : c->nrows;
-      size_t nk = (size_t)((r1 < c->nrows ? k0[r1] : c->ktot) - k0[r0]);
-      if (nk > mx) mx = nk;
+    for (int sy = 0; sy < c->nsys; sy++) {
+      const SysP &P = c->h_sp[sy];
+      if (P.nrows == 0) continue;
+      const int rps = (P.nrows + split - 1) / split;
+      for (int r0 = 0; r0 < P.nrows; r0 += rps) {
+        const int r1 = r0 + rps < P.nrows ? r0 + rps : P.nrows;
+        const int kb1 = r1 < P.nrows ? k0[P.krow0 + r1] : P.kk0 + P.ktot;
+        const size_t nk = (size_t)(kb1 - k0[P.krow0 + r0]);
+        if (nk > mx) mx = nk;
+      }
     }
     c->kf_smem = mx * sizeof(float2);
-    if (c->kf_smem <= 180 * 1024 || split >= c->nrows) break;
+    if (c->kf_smem <= 180 * 1024 || split >= nrows_max) break;
     split *= 2;
   }
-  if (split > c->nrows) split = c->nrows;
+  if (split > nrows_max) split = nrows_max;
   c->kf_split = split;
+  return CM3D_NB_OK;
+}
+
+// the force kernels' shared-memory limit, once per device
+static void kforce_attr(int dev) {
+  static unsigned long long done = 0;
+  if (dev < 64 && (done & (1ull << dev))) return;
+  cudaFuncSetAttribute(k_kforce_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_kforce_mixed<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (dev < 64) done |= 1ull << dev;
+}
+
+// several systems (mixed mode): every system's structure factors, totals
+// and forces in one launch per stage
+static int kspace_forces_batch(Ctx *c) {
+  cudaEvent_t e0;
+  tbegin(c, 1, &e0);
+  k_kprep<true><<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, nullptr,
+                                                               c->sp, c->sys_of, c->kfrac, nullptr, c->gate);
+  int ych = 1;
+  while ((long long)c->ktiles_tot * ych < 148 * 4 && ych < c->nrows_max) ych *= 2;
+  const int rpb = (c->nrows_max + ych - 1) / ych;
+  dim3 gsf(c->ktiles_tot, (c->nrows_max + rpb - 1) / rpb);
+  k_sfac_mixed<true><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0, c->spart,
+                                                    c->sp, c->ktile_sys, c->gate);
+  k_sred<true><<<grid_for(c->ktot, 256), 256, 0, c->st>>>(c->ktot, 0, c->spart, c->ka_d, c->kb_d, c->kc_d, nullptr,
+                                                           0.0, 0.0, c->sk, c->akf, nullptr, c->acc, c->sp,
+                                                           c->k_sys, c->gate);
+  kforce_attr(c->dev);
+  dim3 gf(c->ftiles_tot, c->kf_split);
+  k_kforce_mixed<true><<<gf, KS_THREADS, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0, c->rows,
+                                                               c->row_k0, 0, c->akf, 0, nullptr, c->kf_split > 1,
+                                                               c->fxl, c->sp, c->ftile_sys, c->gate);
+  c->launches += 4;
+  tend(c, 1, e0);
+  CKL(c);
   return CM3D_NB_OK;
 }
 
 int kspace_forces(Ctx *c) {
   if (c->ncharge == 0 || c->ktot == 0) return CM3D_NB_OK;
+  if (c->nsys > 1) return kspace_forces_batch(c);
   const double *dhmati = c->acc + ACC_COUNT;
   double vol = c->hmat[0] * (c->hmat[4] * c->hmat[8] - c->hmat[5] * c->hmat[7]) +
                c->hmat[1] * (c->hmat[5] * c->hmat[6] - c->hmat[3] * c->hmat[8]) +
@@ -431,23 +570,24 @@ int kspace_forces(Ctx *c) {
   cudaEvent_t e0;
   tbegin(c, 1, &e0);
   const bool mixed = c->mode == CM3D_NB_MIXED;
-  k_kprep<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, dhmati,
-                                                         mixed ? c->kfrac : nullptr, c->kposd, c->gate);
+  k_kprep<false><<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, dhmati,
+                                                                nullptr, nullptr, mixed ? c->kfrac : nullptr,
+                                                                c->kposd, c->gate);
   // structure factors: enough row chunks per tile to fill the machine
   int rpb = c->nrows;
   while (rpb > 1 && (long long)c->ks_tiles * ((c->nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
   dim3 gsf(c->ks_tiles, (c->nrows + rpb - 1) / rpb);
   if (mixed)
-    k_sfac_mixed<<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
-                                                c->spart, c->gate);
+    k_sfac_mixed<false><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb,
+                                                       c->ktot, c->spart, nullptr, nullptr, c->gate);
   else
     k_sfac_plain<<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
                                                 dhmati, c->spart, c->gate);
   int ib = 256, gb = grid_for(c->ktot, ib);
   if (gb > 148 * 4) gb = 148 * 4;
-  k_sred<<<gb, ib, 0, c->st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
-                               c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc,
-                               c->gate);
+  k_sred<false><<<gb, ib, 0, c->st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
+                                      c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc,
+                                      nullptr, nullptr, c->gate);
   int split = c->kf_split;
   int rps = (c->nrows + split - 1) / split;
   if (mixed) {
@@ -455,14 +595,10 @@ int kspace_forces(Ctx *c) {
     dim3 gf((c->ncharge + per - 1) / per, split);
     // shared memory: the A(k) of one split's rows
     size_t smem = c->kf_smem;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_kforce_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      attr = true;
-    }
-    k_kforce_mixed<<<gf, KS_THREADS, smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows, c->rows,
-                                                     c->row_k0, rps, c->akf, c->ktot, dhmati, split > 1, c->fxl,
-                                                     c->gate);
+    kforce_attr(c->dev);
+    k_kforce_mixed<false><<<gf, KS_THREADS, smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows,
+                                                            c->rows, c->row_k0, rps, c->akf, c->ktot, dhmati,
+                                                            split > 1, c->fxl, nullptr, nullptr, c->gate);
   } else {
     dim3 gf((c->ncharge + 255) / 256, split);
     k_kforce_plain<<<gf, 256, 0, c->st>>>(c->ncharge, c->kposd, c->icharge, c->n, c->nrows, c->rows, c->row_k0,
@@ -615,7 +751,7 @@ static void na_device_setup(int dev) {
   g_na_what[dev] = "cudaGetSymbolAddress(scratch)";
   if (e == cudaSuccess) {
     // the same limit kspace_forces sets, so that neither caller lowers it
-    e = cudaFuncSetAttribute(k_kforce_mixed, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    e = cudaFuncSetAttribute(k_kforce_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     g_na_what[dev] = "cudaFuncSetAttribute(k_kforce_mixed)";
   }
   g_na_err[dev] = e;
@@ -716,18 +852,19 @@ static int fk_ewald_noalloc(int device, cudaStream_t st, int natoms, const doubl
 
   k_na_setup<<<1, NA_SETUP_THREADS, 0, st>>>(kmax, hi, rows, row_k0, ka, kb, kc, acc);
   if (ncharge > 0 && ktot > 0) {
-    k_kprep<<<grid_for(ncharge, 256), 256, 0, st>>>(ncharge, icharge, natoms, pos, q, dhmati, kfrac, nullptr,
-                                                    nullptr);
+    k_kprep<false><<<grid_for(ncharge, 256), 256, 0, st>>>(ncharge, icharge, natoms, pos, q, dhmati, nullptr,
+                                                           nullptr, kfrac, nullptr, nullptr);
     // grids chosen as kspace_setup/kspace_forces choose them
     const int ks_tiles = (ncharge + KS_THREADS * KS_A - 1) / (KS_THREADS * KS_A);
     int rpb = nrows;
     while (rpb > 1 && (long long)ks_tiles * ((nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
     dim3 gsf(ks_tiles, (nrows + rpb - 1) / rpb);
-    k_sfac_mixed<<<gsf, KS_THREADS, 0, st>>>(ncharge, kfrac, nrows, rows, row_k0, rpb, ktot, spart, nullptr);
+    k_sfac_mixed<false><<<gsf, KS_THREADS, 0, st>>>(ncharge, kfrac, nrows, rows, row_k0, rpb, ktot, spart, nullptr,
+                                                    nullptr, nullptr);
     int gb = grid_for(ktot, 256);
     if (gb > 148 * 4) gb = 148 * 4;
-    k_sred<<<gb, 256, 0, st>>>(ktot, ks_tiles, spart, ka, kb, kc, dhmati, rvol, falp2, sk, akf, nullptr, acc,
-                               nullptr);
+    k_sred<false><<<gb, 256, 0, st>>>(ktot, ks_tiles, spart, ka, kb, kc, dhmati, rvol, falp2, sk, akf, nullptr, acc,
+                                      nullptr, nullptr, nullptr);
     const int per_block = KS_THREADS * KF_A;
     const int tiles = (ncharge + per_block - 1) / per_block;
     int split = 1;
@@ -741,8 +878,8 @@ static int fk_ewald_noalloc(int device, cudaStream_t st, int natoms, const doubl
       if (nk > smem) smem = nk;
     }
     dim3 gf(tiles, split);
-    k_kforce_mixed<<<gf, KS_THREADS, smem, st>>>(ncharge, kfrac, icharge, natoms, nrows, rows, row_k0, rps, akf,
-                                                 ktot, dhmati, split > 1, fxl, nullptr);
+    k_kforce_mixed<false><<<gf, KS_THREADS, smem, st>>>(ncharge, kfrac, icharge, natoms, nrows, rows, row_k0, rps,
+                                                        akf, ktot, dhmati, split > 1, fxl, nullptr, nullptr, nullptr);
   }
   const double six = ncharge > 0 ? ewald_bkg / vol : 0.0;
   k_na_finish<<<1, 32, 0, st>>>(acc, six, ncharge > 0 ? ewald_self : 0.0, out);

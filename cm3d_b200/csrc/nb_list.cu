@@ -6,10 +6,10 @@
 // get_lnklist_e (energy/control/set_link.c:203-300).
 //
 // Pair membership is decided exactly as CM3D decides it: the displacement is
-// taken in FP64, folded with period_ref() (md_period.new.c:39-52, CM3D's
-// anint and operation order, no FMA contraction -- this file is compiled with
-// -fmad=false as well) and compared with the per-interaction radius
-// rmaxl_skin2[map[ti][tj]] / rmaxs_skin2 (LJ, after the map == -1 and
+// taken in FP64, folded with CM3D's period() arithmetic (md_period.new.c:39-52,
+// CM3D's anint and operation order, no FMA contraction -- this file is
+// compiled with -fmad=false as well) and compared with the per-interaction
+// radius rmaxl_skin2[map[ti][tj]] / rmaxs_skin2 (LJ, after the map == -1 and
 // exclusion tests) or rmaxl_skin2_e / rmaxs_skin2_e (charged atoms, after the
 // charge-exclusion test).  The resulting pair sets are bit-identical to
 // CM3D's.  The cell grid itself is our own: cells at least one list radius
@@ -17,12 +17,17 @@
 // a stencil of unique neighbour cells, so every pair within range is seen
 // exactly once per direction whatever CM3D's ncell_div is.
 //
+// A context may hold several independent systems (SysP, nb_common.cuh): each
+// has its own box, cell grid and parameters, its cells and atoms occupy
+// contiguous ranges, and a system is rebuilt only when its own displacement
+// test asked for it (sreb[s]) unless the build covers every system (`all`).
+//
 // Outputs
 //   lst[0..3]  CM3D's four half lists t, s, te, se as (i, j) with i < j
 //   nbr        (mixed mode) a full list per atom in cell-sorted order; each
 //              32-bit entry holds j's sorted index, the code of the cell shift
 //              that turns cell-relative coordinates into the minimum-image
-//              displacement, and whether the pair is in the t and/or te list
+//              displacement, and whether the pair is in the t/s/te/se lists
 //   xq, styp   cell-relative FP32 coordinates + charge and type, sorted order
 #include <math.h>
 #include <stdio.h>
@@ -31,38 +36,86 @@
 
 namespace cm3d {
 
+__device__ __forceinline__ bool sys_skip(int s, const int *__restrict__ sreb, int all) {
+  return !all && sreb[s] == 0;
+}
+
 // ----------------------------------------------------------------- binning
-__global__ void k_cell_assign(int n, const double *__restrict__ pos, const double *__restrict__ hmati,
-                              int ncx, int ncy, int ncz, int *__restrict__ cell_of,
-                              int *__restrict__ cell_count, int4 *__restrict__ cimg,
+// zero the cell counters of the systems being rebuilt
+__global__ void k_cell_zero(int ncells, const int *__restrict__ cell_sys, const int *__restrict__ sreb, int all,
+                            int *__restrict__ cell_count, const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells || sys_skip(cell_sys[c], sreb, all)) return;
+  cell_count[c] = 0;
+}
+
+__global__ void k_cell_assign(int n, const double *__restrict__ pos, const SysP *__restrict__ sp,
+                              const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
+                              int *__restrict__ cell_of, int *__restrict__ cell_count, int4 *__restrict__ cimg,
                               const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int s = sys_of[i];
+  if (sys_skip(s, sreb, all)) return;
+  const SysP &P = sp[s];
   double x = pos[i], y = pos[n + i], z = pos[2 * n + i];
-  double s[3];
+  double sv[3];
   for (int d = 0; d < 3; d++)
-    s[d] = __dadd_rn(__dadd_rn(__dmul_rn(x, hmati[3 * d]), __dmul_rn(y, hmati[3 * d + 1])),
-                     __dmul_rn(z, hmati[3 * d + 2]));
+    sv[d] = __dadd_rn(__dadd_rn(__dmul_rn(x, P.hi[3 * d]), __dmul_rn(y, P.hi[3 * d + 1])),
+                      __dmul_rn(z, P.hi[3 * d + 2]));
   int img[3], cc[3];
-  int ncd[3] = {ncx, ncy, ncz};
   for (int d = 0; d < 3; d++) {
-    double fl = floor(s[d]);
-    double fr = s[d] - fl;                       // [0, 1]
-    int c = (int)(fr * ncd[d]);
-    c = c < 0 ? 0 : (c >= ncd[d] ? ncd[d] - 1 : c);
+    const int ncd = P.nc[d];
+    double fl = floor(sv[d]);
+    double fr = sv[d] - fl;                      // [0, 1]
+    int c = (int)(fr * ncd);
+    c = c < 0 ? 0 : (c >= ncd ? ncd - 1 : c);
     img[d] = (int)fl;
     cc[d] = c;
   }
-  int cell = (cc[0] * ncy + cc[1]) * ncz + cc[2];
+  int cell = P.c0 + (cc[0] * P.nc[1] + cc[1]) * P.nc[2] + cc[2];
   cell_of[i] = cell;
   cimg[i] = make_int4(cc[0] | (cc[1] << 10) | (cc[2] << 20), img[0], img[1], img[2]);
   atomicAdd(cell_count + cell, 1);
 }
 
-// exclusive scan of `m` ints (or long longs) in one block; `nseg` independent
-// segments laid out back to back, one per blockIdx.y; segment totals go to
-// tot[blockIdx.y]
+// one block per system: cell_start[c0 ..] = a0 + exclusive scan of the
+// system's cell counts; the counters are then reset for the fill
+__global__ void __launch_bounds__(256) k_cell_scan(const SysP *__restrict__ sp, const int *__restrict__ sreb,
+                                                   int all, int *__restrict__ cell_count,
+                                                   int *__restrict__ cell_start, const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  const int s = blockIdx.x;
+  if (sys_skip(s, sreb, all)) return;
+  const int c0 = sp[s].c0, m = sp[s].ncells, a0 = sp[s].a0;
+  __shared__ int part[256];
+  const int t = threadIdx.x, nt = blockDim.x;
+  const int chunk = (m + nt - 1) / nt;
+  const int lo = t * chunk, hi = min(m, lo + chunk);
+  int sum = 0;
+  for (int k = lo; k < hi; k++) sum += cell_count[c0 + k];
+  part[t] = sum;
+  __syncthreads();
+  for (int d = 1; d < nt; d <<= 1) {
+    int v = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int run = a0 + (t > 0 ? part[t - 1] : 0);
+  for (int k = lo; k < hi; k++) {
+    const int cnt = cell_count[c0 + k];
+    cell_start[c0 + k] = run;
+    cell_count[c0 + k] = 0;
+    run += cnt;
+  }
+  if (t == nt - 1) cell_start[c0 + m] = a0 + part[nt - 1];
+}
+
+// exclusive scan of `m` ints in one block; `nseg` independent segments laid
+// out back to back, one per blockIdx.y; segment totals go to tot[blockIdx.y]
 template <typename TI, typename TO>
 __global__ void k_scan(const TI *__restrict__ in, TO *__restrict__ out, long long *__restrict__ tot,
                        int m, const int *__restrict__ gate) {
@@ -94,12 +147,12 @@ __global__ void k_scan(const TI *__restrict__ in, TO *__restrict__ out, long lon
   }
 }
 
-__global__ void k_cell_fill(int n, const int *__restrict__ cell_of, const int *__restrict__ cell_start,
-                            int *__restrict__ cursor, int *__restrict__ cell_atoms,
-                            const int *__restrict__ gate) {
+__global__ void k_cell_fill(int n, const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
+                            const int *__restrict__ cell_of, const int *__restrict__ cell_start,
+                            int *__restrict__ cursor, int *__restrict__ cell_atoms, const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || sys_skip(sys_of[i], sreb, all)) return;
   int c = cell_of[i];
   int slot = atomicAdd(cursor + c, 1);
   cell_atoms[cell_start[c] + slot] = i;
@@ -107,11 +160,13 @@ __global__ void k_cell_fill(int n, const int *__restrict__ cell_of, const int *_
 
 // order every cell's atoms by atom index (deterministic lists): one block
 // per cell ranks each atom among its cell's atoms (indices are distinct)
-__global__ void k_cell_sort(int ncells, const int *__restrict__ cell_start, int *__restrict__ cell_atoms,
+__global__ void k_cell_sort(int ncells, const int *__restrict__ cell_sys, const int *__restrict__ sreb, int all,
+                            const int *__restrict__ cell_start, int *__restrict__ cell_atoms,
                             const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   __shared__ int s[1024];
   const int c = blockIdx.x;
+  if (sys_skip(cell_sys[c], sreb, all)) return;
   const int lo = cell_start[c], hi = cell_start[c + 1], m = hi - lo;
   if (m <= 1) return;
   if (m <= 1024) {
@@ -137,28 +192,17 @@ __global__ void k_cell_sort(int ncells, const int *__restrict__ cell_start, int 
   }
 }
 
-struct ListParams {
-  int n, ntypes, ncx, ncy, ncz;
-  int sx[3], sy[3], sz[3];          // unique stencil offsets per dimension
-  int nsx, nsy, nsz;
-  double h[9], hi[9];
-  double rmaxl_skin2_e, rmaxs_skin2_e;
-  float lim2;                       // FP32 prefilter radius^2 (inf = off)
-  long long cap[LT_COUNT];
-};
-
 // Exact membership test of one candidate pair, in CM3D's FP64 operation
 // order.  Returns flags (bit0 t, bit1 s, bit2 te, bit3 se, bit4 bad shift)
 // and the cell-shift code of the pair for the full list.
-__device__ __forceinline__ int exact_flags(const ListParams &P, int i, int j, int4 ci, const double *__restrict__ pos,
-                                           double xi, double yi, double zi, int ti, bool qi,
-                                           const int *__restrict__ itype, const int *__restrict__ map,
+__device__ __forceinline__ int exact_flags(const SysP &P, int n, int i, int j, int4 ci,
+                                           const double *__restrict__ pos, double xi, double yi, double zi, int ti,
+                                           bool qi, const int *__restrict__ itype, const int *__restrict__ map,
                                            const double *__restrict__ icut, const double *__restrict__ q,
                                            const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
                                            const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx,
                                            const int4 *__restrict__ cimg, int &code) {
-  const int n = P.n;
-  const int intr = map[ti * P.ntypes + itype[j]];
+  const int intr = map[P.map0 + ti * P.ntypes + itype[j]];
   const bool lj_ok = intr >= 0;
   const bool el_ok = qi && q[j] != 0.0;
   if (!lj_ok && !el_ok) return 0;
@@ -189,9 +233,9 @@ __device__ __forceinline__ int exact_flags(const ListParams &P, int i, int j, in
   // assumption broke: flag it and use the zero shift rather than index past
   // the shift table.
   const int4 cj = cimg[j];
-  const int kx = (ci.y - cj.y - (int)mx) * P.ncx + ((ci.x & 1023) - (cj.x & 1023));
-  const int ky = (ci.z - cj.z - (int)my) * P.ncy + (((ci.x >> 10) & 1023) - ((cj.x >> 10) & 1023));
-  const int kz = (ci.w - cj.w - (int)mz) * P.ncz + (((ci.x >> 20) & 1023) - ((cj.x >> 20) & 1023));
+  const int kx = (ci.y - cj.y - (int)mx) * P.nc[0] + ((ci.x & 1023) - (cj.x & 1023));
+  const int ky = (ci.z - cj.z - (int)my) * P.nc[1] + (((ci.x >> 10) & 1023) - ((cj.x >> 10) & 1023));
+  const int kz = (ci.w - cj.w - (int)mz) * P.nc[2] + (((ci.x >> 20) & 1023) - ((cj.x >> 20) & 1023));
   code = (kx + 1) * 9 + (ky + 1) * 3 + (kz + 1);
   if (kx < -1 || kx > 1 || ky < -1 || ky > 1 || kz < -1 || kz > 1) {
     code = 13;
@@ -212,27 +256,31 @@ __device__ __forceinline__ int exact_flags(const ListParams &P, int i, int j, in
 constexpr int LQ = 64;                     // queue entries per warp (> 2 * 32 - 1)
 
 template <class Decide>
-__device__ __forceinline__ void walk_candidates(const ListParams &P, int i, int4 ci, float4 xi4, bool half_only,
+__device__ __forceinline__ void walk_candidates(const SysP &P, int i, int4 ci, float4 xi4, bool half_only,
                                                 const int *__restrict__ cell_atoms,
                                                 const int *__restrict__ cell_start,
-                                                const float4 *__restrict__ xq, const float4 *__restrict__ shift,
-                                                int *qbuf, Decide &decide) {
+                                                const float4 *__restrict__ xq, int *qbuf, Decide &decide) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int cx = ci.x & 1023, cy = (ci.x >> 10) & 1023, cz = (ci.x >> 20) & 1023;
+  const int ncx = P.nc[0], ncy = P.nc[1], ncz = P.nc[2];
+  const float lim2 = P.lim2;
   int head = 0, tail = 0;
   for (int a = 0; a < P.nsx; a++) {
-    int jx = cx + P.sx[a];
-    jx = jx < 0 ? jx + P.ncx : (jx >= P.ncx ? jx - P.ncx : jx);
+    const int ox = P.sx[a];
+    int jx = cx + ox;
+    jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
     for (int b = 0; b < P.nsy; b++) {
-      int jy = cy + P.sy[b];
-      jy = jy < 0 ? jy + P.ncy : (jy >= P.ncy ? jy - P.ncy : jy);
+      const int oy = P.sy[b];
+      int jy = cy + oy;
+      jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
       for (int cc = 0; cc < P.nsz; cc++) {
-        int jz = cz + P.sz[cc];
-        jz = jz < 0 ? jz + P.ncz : (jz >= P.ncz ? jz - P.ncz : jz);
-        const int cell = (jx * P.ncy + jy) * P.ncz + jz;
+        const int oz = P.sz[cc];
+        int jz = cz + oz;
+        jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
+        const int cell = P.c0 + (jx * ncy + jy) * ncz + jz;
         // cell-corner shift of this stencil offset (k = -offset)
-        const float4 S = shift[(1 - P.sx[a]) * 9 + (1 - P.sy[b]) * 3 + (1 - P.sz[cc])];
+        const float4 S = P.shift[(1 - ox) * 9 + (1 - oy) * 3 + (1 - oz)];
         const int lo = cell_start[cell], hi = cell_start[cell + 1];
         for (int u0 = lo; u0 < hi; u0 += 32) {
           const int u = u0 + lane;
@@ -242,7 +290,7 @@ __device__ __forceinline__ void walk_candidates(const ListParams &P, int i, int4
             const float4 xj = xq[u];
             const float dx = (xi4.x - xj.x) + S.x, dy = (xi4.y - xj.y) + S.y, dz = (xi4.z - xj.z) + S.z;
             const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            keep = j != i && r2f < P.lim2 && (!half_only || j > i);
+            keep = j != i && r2f < lim2 && (!half_only || j > i);
           }
           const unsigned bk = __ballot_sync(0xffffffffu, keep);
           if (keep) qbuf[(tail + __popc(bk & lt_mask)) & (LQ - 1)] = u;
@@ -264,33 +312,38 @@ __device__ __forceinline__ void walk_candidates(const ListParams &P, int i, int4
   }
 }
 
+struct ListCaps {
+  long long cap[4];
+};
+
 // CM3D's four half lists (i < j): FILL = false counts the pairs of every
 // list per atom, FILL = true writes them at the scanned offsets, compacted
-// with warp ballots in candidate order (deterministic).
+// with warp ballots in candidate order (deterministic).  Always built for
+// every system (host-driven builds and the single-system plain engine).
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_list_half(
-    ListParams P, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
-    const float4 *__restrict__ xq, const float4 *__restrict__ shift, const double *__restrict__ pos,
-    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
-    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
-    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
-    int *__restrict__ cnt, const long long *__restrict__ off, const long long *__restrict__ tot,
-    int2 *__restrict__ l0, int2 *__restrict__ l1, int2 *__restrict__ l2, int2 *__restrict__ l3,
-    long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
+    int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of, ListCaps C,
+    const int *__restrict__ cell_atoms, const int *__restrict__ cell_start, const float4 *__restrict__ xq,
+    const double *__restrict__ pos, const int *__restrict__ itype, const int *__restrict__ map,
+    const double *__restrict__ icut, const double *__restrict__ q, const int *__restrict__ excl_off,
+    const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx,
+    const int4 *__restrict__ cimg, int *__restrict__ cnt, const long long *__restrict__ off,
+    const long long *__restrict__ tot, int2 *__restrict__ l0, int2 *__restrict__ l1, int2 *__restrict__ l2,
+    int2 *__restrict__ l3, long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   __shared__ int qs[256 / 32][LQ];
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (t >= P.n) return;                                   // whole warps
+  if (t >= n) return;                                     // whole warps
   const unsigned lt_mask = (1u << lane) - 1u;
   long long p[4] = {0, 0, 0, 0};
   if (FILL) {
-    bool all = true;
+    bool fits = true;
     for (int k = 0; k < 4; k++) {
-      all = all && tot[k] <= P.cap[k];
-      p[k] = off[(size_t)k * (P.n + 1) + t];
+      fits = fits && tot[k] <= C.cap[k];
+      p[k] = off[(size_t)k * (n + 1) + t];
     }
-    if (!all) {
+    if (!fits) {
       // a list outgrew its buffer: write nothing, halt the step (the host
       // grows the buffers and finishes it, see run_step)
       if (t == 0 && lane == 0) {
@@ -301,9 +354,10 @@ __global__ void __launch_bounds__(256) k_list_half(
     }
   }
   int *qbuf = qs[threadIdx.x >> 5];
+  const SysP &P = sp[sys_of[t]];
   const int i = cell_atoms[t];
   const int4 ci = cimg[i];
-  const double xi = pos[i], yi = pos[P.n + i], zi = pos[2 * P.n + i];
+  const double xi = pos[i], yi = pos[n + i], zi = pos[2 * n + i];
   const int ti = itype[i];
   const bool qi = q[i] != 0.0;
   int c[4] = {0, 0, 0, 0};
@@ -312,8 +366,8 @@ __global__ void __launch_bounds__(256) k_list_half(
     int fl = 0, code = 13, j = -1;
     if (lane < m) {
       j = cell_atoms[qbuf[(first + lane) & (LQ - 1)]];
-      fl = exact_flags(P, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx, cexcl_off,
-                       cexcl_idx, cimg, code);
+      fl = exact_flags(P, n, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
+                       cexcl_off, cexcl_idx, cimg, code);
     }
     bad |= (fl >> 4) & 1;
     const unsigned b0 = __ballot_sync(0xffffffffu, fl & 1), b1 = __ballot_sync(0xffffffffu, fl & 2);
@@ -329,11 +383,11 @@ __global__ void __launch_bounds__(256) k_list_half(
       p[0] += __popc(b0); p[1] += __popc(b1); p[2] += __popc(b2); p[3] += __popc(b3);
     }
   };
-  walk_candidates(P, i, ci, xq[t], true, cell_atoms, cell_start, xq, shift, qbuf, decide);
+  walk_candidates(P, i, ci, xq[t], true, cell_atoms, cell_start, xq, qbuf, decide);
   if (FILL) {
     if (bad && lane == 0) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
   } else if (lane == 0) {
-    for (int k = 0; k < 4; k++) cnt[(size_t)k * P.n + t] = c[k];
+    for (int k = 0; k < 4; k++) cnt[(size_t)k * n + t] = c[k];
   }
 }
 
@@ -344,23 +398,26 @@ __global__ void __launch_bounds__(256) k_list_half(
 // length it needed (ST_NEED_STRIDE) and halts a captured step; the host then
 // widens the slots and builds again.
 __global__ void __launch_bounds__(256) k_list_full(
-    ListParams P, int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
-    const float4 *__restrict__ xq, const float4 *__restrict__ shift, const double *__restrict__ pos,
-    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
-    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
-    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
-    uint32_t *__restrict__ nbr, int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt,
-    const int *__restrict__ gate) {
+    int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
+    int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    const float4 *__restrict__ xq, const double *__restrict__ pos, const int *__restrict__ itype,
+    const int *__restrict__ map, const double *__restrict__ icut, const double *__restrict__ q,
+    const int *__restrict__ excl_off, const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
+    const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, uint32_t *__restrict__ nbr,
+    int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   __shared__ int qs[256 / 32][LQ];
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (t >= P.n) return;                                   // whole warps
+  if (t >= n) return;                                     // whole warps
+  const int s = sys_of[t];
+  if (sys_skip(s, sreb, all)) return;                     // whole warps
+  const SysP &P = sp[s];
   const unsigned lt_mask = (1u << lane) - 1u;
   int *qbuf = qs[threadIdx.x >> 5];
   const int i = cell_atoms[t];
   const int4 ci = cimg[i];
-  const double xi = pos[i], yi = pos[P.n + i], zi = pos[2 * P.n + i];
+  const double xi = pos[i], yi = pos[n + i], zi = pos[2 * n + i];
   const int ti = itype[i];
   const bool qi = q[i] != 0.0;
   uint32_t *out = nbr + (size_t)t * stride;
@@ -370,8 +427,8 @@ __global__ void __launch_bounds__(256) k_list_full(
     int fl = 0, code = 13, u = 0;
     if (lane < m) {
       u = qbuf[(first + lane) & (LQ - 1)];
-      fl = exact_flags(P, i, cell_atoms[u], ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
-                       cexcl_off, cexcl_idx, cimg, code);
+      fl = exact_flags(P, n, i, cell_atoms[u], ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off,
+                       excl_idx, cexcl_off, cexcl_idx, cimg, code);
     }
     bad |= (fl >> 4) & 1;
     const bool f = (fl & 5) != 0;
@@ -387,7 +444,7 @@ __global__ void __launch_bounds__(256) k_list_full(
     }
     count += __popc(bf);
   };
-  walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, shift, qbuf, decide);
+  walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide);
   if (lane == 0) {
     nlen[t] = count < stride ? count : stride;
     if (count > stride) {
@@ -403,19 +460,24 @@ __global__ void __launch_bounds__(256) k_list_full(
 
 // sorted-order arrays: rank, type, the FP64 corner of the atom's cell (held
 // fixed until the next rebuild) and FP32 cell-relative coordinates + charge
-__global__ void k_sorted_init(int n, const int *__restrict__ cell_atoms, const int4 *__restrict__ cimg,
-                              const double *__restrict__ h, int ncx, int ncy, int ncz,
-                              const int *__restrict__ itype, const double *__restrict__ pos,
-                              const double *__restrict__ q, int *__restrict__ rank, int *__restrict__ styp,
-                              double *__restrict__ corner, float4 *__restrict__ xq, const int *__restrict__ gate) {
+__global__ void k_sorted_init(int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
+                              const int *__restrict__ sreb, int all, const int *__restrict__ cell_atoms,
+                              const int4 *__restrict__ cimg, const int *__restrict__ itype,
+                              const double *__restrict__ pos, const double *__restrict__ q, int *__restrict__ rank,
+                              int *__restrict__ styp, double *__restrict__ corner, float4 *__restrict__ xq,
+                              const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
+  const int s = sys_of[t];
+  if (sys_skip(s, sreb, all)) return;
+  const SysP &P = sp[s];
   int i = cell_atoms[t];
   int4 ci = cimg[i];
-  double o0 = (double)ci.y + (double)(ci.x & 1023) / ncx;
-  double o1 = (double)ci.z + (double)((ci.x >> 10) & 1023) / ncy;
-  double o2 = (double)ci.w + (double)((ci.x >> 20) & 1023) / ncz;
+  const double *h = P.h;
+  double o0 = (double)ci.y + (double)(ci.x & 1023) / P.nc[0];
+  double o1 = (double)ci.z + (double)((ci.x >> 10) & 1023) / P.nc[1];
+  double o2 = (double)ci.w + (double)((ci.x >> 20) & 1023) / P.nc[2];
   double c0 = h[0] * o0 + h[1] * o1 + h[2] * o2;
   double c1 = h[3] * o0 + h[4] * o1 + h[5] * o2;
   double c2 = h[6] * o0 + h[7] * o1 + h[8] * o2;
@@ -427,16 +489,25 @@ __global__ void k_sorted_init(int n, const int *__restrict__ cell_atoms, const i
   styp[t] = itype[i];
 }
 
-__global__ void k_snapshot(int n3, const double *__restrict__ pos, double *__restrict__ dxn,
-                           const int *__restrict__ gate, int *__restrict__ istate,
+// dxn = pos of the rebuilt systems (ngbr_list.c:577-580) and, per rebuilt
+// system, isteplast = istep (md_finter.c:98)
+__global__ void k_snapshot(int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
+                           const int *__restrict__ sreb, int all, const double *__restrict__ pos,
+                           double *__restrict__ dxn, int *__restrict__ slast, long long *__restrict__ sstat,
+                           const int *__restrict__ gate, const int *__restrict__ istate,
                            long long *__restrict__ stat) {
   if (gated_off(gate, 1)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n3) dxn[i] = pos[i];
-  if (i == 0) {
-    // md_finter.c:98: isteplast = istep after a rebuild
-    istate[IS_ISTEPLAST] = istate[IS_ISTEP];
-    atomicAdd((unsigned long long *)(stat + ST_REBUILDS), 1ull);
+  if (i == 0) atomicAdd((unsigned long long *)(stat + ST_REBUILDS), 1ull);
+  if (i >= n) return;
+  const int s = sys_of[i];
+  if (sys_skip(s, sreb, all)) return;
+  dxn[i] = pos[i];
+  dxn[n + i] = pos[n + i];
+  dxn[2 * n + i] = pos[2 * n + i];
+  if (i == sp[s].a0) {
+    slast[s] = istate[IS_ISTEP];
+    sstat[(size_t)s * SS_COUNT + SS_REBUILDS] += 1;
   }
 }
 
@@ -451,64 +522,91 @@ static void stencil(int nc, int *s, int *ns) {
   }
 }
 
+// Cell grids of every system (cells at least one list radius wide in every
+// fractional direction: plane spacing 1 / |row d of hmati|), their stencils,
+// the 27 cell-corner shifts and the FP32 prefilter radius; fills the cell
+// fields of c->h_sp and allocates the binning and list arrays.
 int list_setup(Ctx *c) {
-  // cells at least one list radius wide in every fractional direction
-  // (plane spacing 1/|row d of hmati|)
-  int tot = 1;
-  for (int d = 0; d < 3; d++) {
-    double w = 1.0 / sqrt(c->hmati[3 * d] * c->hmati[3 * d] + c->hmati[3 * d + 1] * c->hmati[3 * d + 1] +
-                          c->hmati[3 * d + 2] * c->hmati[3 * d + 2]);
-    int m = c->rlist_max > 0 ? (int)floor(w / c->rlist_max) : 1;
-    m = m < 1 ? 1 : (m > 1000 ? 1000 : m);
-    c->nc[d] = m;
-    tot *= m;
+  int c0 = 0;
+  double est_max = 32.0;
+  for (int s = 0; s < c->nsys; s++) {
+    SysP &P = c->h_sp[s];
+    const SysH &H = c->hs[s];
+    int tot = 1;
+    for (int d = 0; d < 3; d++) {
+      double w = 1.0 / sqrt(H.hmati[3 * d] * H.hmati[3 * d] + H.hmati[3 * d + 1] * H.hmati[3 * d + 1] +
+                            H.hmati[3 * d + 2] * H.hmati[3 * d + 2]);
+      int m = H.rlist > 0 ? (int)floor(w / H.rlist) : 1;
+      m = m < 1 ? 1 : (m > 1000 ? 1000 : m);
+      P.nc[d] = m;
+      tot *= m;
+    }
+    P.c0 = c0;
+    P.ncells = tot;
+    c0 += tot;
+    stencil(P.nc[0], P.sx, &P.nsx);
+    stencil(P.nc[1], P.sy, &P.nsy);
+    stencil(P.nc[2], P.sz, &P.nsz);
+    // with three or more cells per direction the stencil neighbour's image
+    // is the minimum image of every pair in range, so the FP32 prefilter is
+    // exact up to rounding; with fewer cells every candidate goes to the
+    // FP64 test
+    const bool pre = P.nc[0] >= 3 && P.nc[1] >= 3 && P.nc[2] >= 3;
+    const double rl = H.rlist + 1e-3;
+    P.lim2 = pre ? (float)(rl * rl) : INFINITY;
+    for (int a = -1; a <= 1; a++)
+      for (int b = -1; b <= 1; b++)
+        for (int d = -1; d <= 1; d++) {
+          double f0 = (double)a / P.nc[0], f1 = (double)b / P.nc[1], f2 = (double)d / P.nc[2];
+          const double *h = H.hmat;
+          P.shift[(a + 1) * 9 + (b + 1) * 3 + (d + 1)] =
+              make_float4((float)(h[0] * f0 + h[1] * f1 + h[2] * f2), (float)(h[3] * f0 + h[4] * f1 + h[5] * f2),
+                          (float)(h[6] * f0 + h[7] * f1 + h[8] * f2), 0.f);
+        }
+    // first guess of the full-list slot: 1.3 x the mean number of atoms in
+    // a list sphere, plus 64
+    double vol = fabs(H.hmat[0] * (H.hmat[4] * H.hmat[8] - H.hmat[5] * H.hmat[7]) +
+                      H.hmat[1] * (H.hmat[5] * H.hmat[6] - H.hmat[3] * H.hmat[8]) +
+                      H.hmat[2] * (H.hmat[3] * H.hmat[7] - H.hmat[4] * H.hmat[6]));
+    double r = H.rlist;
+    double est = 1.3 * (double)H.n / vol * (4.0 / 3.0) * M_PI * r * r * r + 64.0;
+    if (est > (double)H.n + 31.0) est = (double)H.n + 31.0;
+    if (est > est_max) est_max = est;
   }
-  c->ncells = tot;
+  c->ncells = c0;
+  c->nc[0] = c->h_sp[0].nc[0];
+  c->nc[1] = c->h_sp[0].nc[1];
+  c->nc[2] = c->h_sp[0].nc[2];
+  std::vector<int> cell_sys(c0);
+  for (int s = 0; s < c->nsys; s++)
+    for (int k = 0; k < c->h_sp[s].ncells; k++) cell_sys[c->h_sp[s].c0 + k] = s;
+  CK(cudaMalloc(&c->cell_sys, sizeof(int) * (size_t)c0));
+  CK(cudaMemcpy(c->cell_sys, cell_sys.data(), sizeof(int) * (size_t)c0, cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c->cell_of, sizeof(int) * (size_t)c->n));
-  CK(cudaMalloc(&c->cell_start, sizeof(int) * ((size_t)tot + 1)));
-  CK(cudaMalloc(&c->cell_cursor, sizeof(int) * ((size_t)tot + 1)));
+  CK(cudaMalloc(&c->cell_start, sizeof(int) * ((size_t)c0 + 1)));
+  CK(cudaMalloc(&c->cell_cursor, sizeof(int) * ((size_t)c0 + 1)));
+  CK(cudaMemset(c->cell_cursor, 0, sizeof(int) * ((size_t)c0 + 1)));
   CK(cudaMalloc(&c->cell_atoms, sizeof(int) * (size_t)c->n));
   CK(cudaMalloc(&c->rank, sizeof(int) * (size_t)c->n));
   CK(cudaMalloc(&c->cnt, sizeof(int) * 4 * (size_t)c->n));
   CK(cudaMalloc(&c->off, sizeof(long long) * 4 * ((size_t)c->n + 1)));
-  if (c->mode == CM3D_NB_MIXED) {
-    CK(cudaMalloc(&c->nlen, sizeof(int) * (size_t)c->n));
-    // first guess of the full-list slot: 1.3 x the mean number of atoms in
-    // a list sphere, plus 64, in whole 32-entry (128-byte) units; a build
-    // that finds a longer list widens it (grow_full)
-    const double *h = c->hmat;
-    double vol = fabs(h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
-                      h[2] * (h[3] * h[7] - h[4] * h[6]));
-    double r = c->rlist_max;
-    double est = 1.3 * (double)c->n / vol * (4.0 / 3.0) * M_PI * r * r * r + 64.0;
-    long long cap_n = ((long long)c->n + 31) / 32 * 32;
-    long long s = ((long long)est + 31) / 32 * 32;
-    if (s > cap_n) s = cap_n;
-    if (s < 32) s = 32;
-    c->nbr_stride = (int)s;
-    CK(cudaMalloc(&c->nbr, sizeof(uint32_t) * (size_t)c->n * (size_t)s));
-    c->lcap[LT_FULL] = (long long)c->n * s;
-  }
   CK(cudaMalloc(&c->ltot, sizeof(long long) * LT_COUNT));
   CK(cudaMallocHost(&c->h_ltot, sizeof(long long) * LT_COUNT));
   CK(cudaMalloc(&c->styp, sizeof(int) * (size_t)c->n));
   CK(cudaMalloc(&c->corner, sizeof(double) * 3 * (size_t)c->n));
   CK(cudaMalloc(&c->xq, sizeof(float4) * (size_t)c->n));
   CK(cudaMalloc(&c->cimg, sizeof(int4) * (size_t)c->n));
-  // the 27 cell-corner shifts H k / nc, k in {-1, 0, 1}^3 (also used by the
-  // mixed pair kernel)
-  std::vector<float4> sh(27);
-  for (int a = -1; a <= 1; a++)
-    for (int b = -1; b <= 1; b++)
-      for (int d = -1; d <= 1; d++) {
-        double f0 = (double)a / c->nc[0], f1 = (double)b / c->nc[1], f2 = (double)d / c->nc[2];
-        const double *h = c->hmat;
-        sh[(a + 1) * 9 + (b + 1) * 3 + (d + 1)] =
-            make_float4((float)(h[0] * f0 + h[1] * f1 + h[2] * f2), (float)(h[3] * f0 + h[4] * f1 + h[5] * f2),
-                        (float)(h[6] * f0 + h[7] * f1 + h[8] * f2), 0.f);
-      }
+  // system 0's shifts (the single-system pair kernel keeps them in shared memory)
   CK(cudaMalloc(&c->shift, sizeof(float4) * 27));
-  CK(cudaMemcpy(c->shift, sh.data(), sizeof(float4) * 27, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->shift, c->h_sp[0].shift, sizeof(float4) * 27, cudaMemcpyHostToDevice));
+  if (c->mode == CM3D_NB_MIXED) {
+    CK(cudaMalloc(&c->nlen, sizeof(int) * (size_t)c->n));
+    long long s = ((long long)est_max + 31) / 32 * 32;
+    if (s < 32) s = 32;
+    c->nbr_stride = (int)s;
+    CK(cudaMalloc(&c->nbr, sizeof(uint32_t) * (size_t)c->n * (size_t)s));
+    c->lcap[LT_FULL] = (long long)c->n * s;
+  }
   return CM3D_NB_OK;
 }
 
@@ -531,9 +629,7 @@ static int grow(Ctx *c, int which, long long need) {
 
 // widen the full-list slots to hold `need` entries (+1/8 and 32 spare)
 static int grow_full(Ctx *c, long long need) {
-  long long cap_n = ((long long)c->n + 31) / 32 * 32;
   long long s = (need + need / 8 + 32 + 31) / 32 * 32;
-  if (s > cap_n) s = cap_n;
   if (s <= c->nbr_stride) s = c->nbr_stride + 32;
   if (c->graph) {
     cudaGraphExecDestroy(c->graph);
@@ -549,67 +645,46 @@ static int grow_full(Ctx *c, long long need) {
   return CM3D_NB_OK;
 }
 
-static ListParams params(Ctx *c) {
-  ListParams P;
-  P.n = c->n;
-  P.ntypes = c->ntypes;
-  P.ncx = c->nc[0];
-  P.ncy = c->nc[1];
-  P.ncz = c->nc[2];
-  stencil(c->nc[0], P.sx, &P.nsx);
-  stencil(c->nc[1], P.sy, &P.nsy);
-  stencil(c->nc[2], P.sz, &P.nsz);
-  for (int k = 0; k < 9; k++) {
-    P.h[k] = c->hmat[k];
-    P.hi[k] = c->hmati[k];
-  }
-  P.rmaxl_skin2_e = c->ncharge > 0 ? c->rmaxl_skin2_e : -1.0;
-  P.rmaxs_skin2_e = c->ncharge > 0 ? c->rmaxs_skin2_e : -1.0;
-  // with three or more cells per direction the stencil neighbour's image is
-  // the minimum image of every pair in range, so the FP32 prefilter is exact
-  // up to rounding; with fewer cells every candidate goes to the FP64 test
-  const bool pre = c->nc[0] >= 3 && c->nc[1] >= 3 && c->nc[2] >= 3;
-  const double rl = c->rlist_max + 1e-3;
-  P.lim2 = pre ? (float)(rl * rl) : INFINITY;
-  for (int k = 0; k < LT_COUNT; k++) P.cap[k] = c->lcap[k];
-  return P;
+static ListCaps caps(Ctx *c) {
+  ListCaps C;
+  for (int k = 0; k < 4; k++) C.cap[k] = c->lcap[k];
+  return C;
 }
 
-// Build the lists from the current positions.  With device_flag the kernels
-// are gated on the device rebuild flag (graph replay) and the capacities are
-// not re-checked on the host.  The plain engine always builds CM3D's half
-// lists (its pair kernels walk them); the mixed engine builds its full list
-// and the half lists only when asked (export / parity checks).
-int build_lists(Ctx *c, bool device_flag) {
+// Build the lists from the current positions.  `all`: every system (set-up,
+// get_ngbr, export); otherwise only the systems whose displacement test
+// asked for it (sreb).  With device_flag the kernels are also gated on the
+// device rebuild flag (graph replay) and the capacities are not re-checked on
+// the host.  The plain engine always builds CM3D's half lists (its pair
+// kernels walk them); the mixed engine builds its full list and the half
+// lists only when asked (export / parity checks).
+int build_lists(Ctx *c, bool device_flag, bool all) {
   const int n = c->n;
   const int B = 256;
   const int *gate = device_flag ? c->istate : nullptr;
+  const int al = all ? 1 : 0;
   const bool want_half = c->mode == CM3D_NB_PLAIN_FP64 || c->want_half;
   cudaEvent_t e0;
   tbegin(c, 2, &e0);
   int4 *cimg = c->cimg;
-  CK(cudaMemsetAsync(c->cell_start, 0, sizeof(int) * ((size_t)c->ncells + 1), c->st));
-  CK(cudaMemsetAsync(c->cell_cursor, 0, sizeof(int) * ((size_t)c->ncells + 1), c->st));
-  double *dhmati = c->acc + ACC_COUNT;        // device copies of hmat/hmati
-  double *dhmat = c->acc + ACC_COUNT + 9;
-  k_cell_assign<<<grid_for(n, B), B, 0, c->st>>>(n, c->pos, dhmati, c->nc[0], c->nc[1], c->nc[2],
-                                                  c->cell_of, c->cell_cursor, cimg, gate);
-  k_scan<int, int><<<dim3(1, 1), 1024, 0, c->st>>>(c->cell_cursor, c->cell_start, nullptr, c->ncells, gate);
-  CK(cudaMemsetAsync(c->cell_cursor, 0, sizeof(int) * ((size_t)c->ncells + 1), c->st));
-  k_cell_fill<<<grid_for(n, B), B, 0, c->st>>>(n, c->cell_of, c->cell_start, c->cell_cursor, c->cell_atoms, gate);
-  k_cell_sort<<<c->ncells, 256, 0, c->st>>>(c->ncells, c->cell_start, c->cell_atoms, gate);
-  k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->cell_atoms, cimg, dhmat, c->nc[0], c->nc[1], c->nc[2],
-                                                  c->itype, c->pos, c->q, c->rank, c->styp, c->corner, c->xq,
-                                                  gate);
-  c->launches += 5;
-  ListParams P = params(c);
+  k_cell_zero<<<grid_for(c->ncells, B), B, 0, c->st>>>(c->ncells, c->cell_sys, c->sreb, al, c->cell_cursor, gate);
+  k_cell_assign<<<grid_for(n, B), B, 0, c->st>>>(n, c->pos, c->sp, c->sys_of, c->sreb, al, c->cell_of,
+                                                  c->cell_cursor, cimg, gate);
+  k_cell_scan<<<c->nsys, 256, 0, c->st>>>(c->sp, c->sreb, al, c->cell_cursor, c->cell_start, gate);
+  k_cell_fill<<<grid_for(n, B), B, 0, c->st>>>(n, c->sys_of, c->sreb, al, c->cell_of, c->cell_start,
+                                                c->cell_cursor, c->cell_atoms, gate);
+  k_cell_sort<<<c->ncells, 256, 0, c->st>>>(c->ncells, c->cell_sys, c->sreb, al, c->cell_start, c->cell_atoms,
+                                            gate);
+  k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->sp, c->sys_of, c->sreb, al, c->cell_atoms, cimg, c->itype,
+                                                  c->pos, c->q, c->rank, c->styp, c->corner, c->xq, gate);
+  c->launches += 6;
   const long long warps_threads = 32LL * n;
   if (c->mode == CM3D_NB_MIXED) {
     for (;;) {
       k_list_full<<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
-          P, c->nbr_stride, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut,
-          c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->nbr, c->nlen, c->stat,
-          device_flag ? c->istate + IS_HALT : nullptr, gate);
+          n, c->sp, c->sys_of, c->sreb, al, c->nbr_stride, c->cell_atoms, c->cell_start, c->xq, c->pos, c->itype,
+          c->map, c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->nbr, c->nlen,
+          c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
       c->launches++;
       CKL(c);
       if (device_flag) break;
@@ -623,9 +698,9 @@ int build_lists(Ctx *c, bool device_flag) {
   }
   if (want_half) {
     k_list_half<false><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
-        P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
-        c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->cnt, nullptr, nullptr, nullptr, nullptr, nullptr,
-        nullptr, c->stat, nullptr, gate);
+        n, c->sp, c->sys_of, caps(c), c->cell_atoms, c->cell_start, c->xq, c->pos, c->itype, c->map, c->icut,
+        c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->cnt, nullptr, nullptr, nullptr,
+        nullptr, nullptr, nullptr, c->stat, nullptr, gate);
     k_scan<int, long long><<<dim3(1, 4), 1024, 0, c->st>>>(c->cnt, c->off, c->ltot, n, gate);
     c->launches += 2;
     CKL(c);
@@ -637,16 +712,16 @@ int build_lists(Ctx *c, bool device_flag) {
         if (rc) return rc;
         c->hcount[k] = c->h_ltot[k];
       }
-      P = params(c);
     }
     k_list_half<true><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
-        P, c->cell_atoms, c->cell_start, c->xq, c->shift, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off,
-        c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, nullptr, c->off, c->ltot, c->lst[0], c->lst[1], c->lst[2],
-        c->lst[3], c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+        n, c->sp, c->sys_of, caps(c), c->cell_atoms, c->cell_start, c->xq, c->pos, c->itype, c->map, c->icut,
+        c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, nullptr, c->off, c->ltot, c->lst[0],
+        c->lst[1], c->lst[2], c->lst[3], c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
     c->launches++;
   }
   if (!c->no_snapshot) {
-    k_snapshot<<<grid_for(3LL * n, B), B, 0, c->st>>>(3 * n, c->pos, c->dxn, gate, c->istate, c->stat);
+    k_snapshot<<<grid_for(n, B), B, 0, c->st>>>(n, c->sp, c->sys_of, c->sreb, al, c->pos, c->dxn, c->slast,
+                                                 c->sstat, gate, c->istate, c->stat);
     c->launches++;
   }
   CKL(c);

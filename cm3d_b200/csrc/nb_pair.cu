@@ -51,13 +51,33 @@ __device__ __forceinline__ float poly(float p, float c0, float a, float b) {
 enum { EP_ELJ = 0, EP_ELJH, EP_VL0, EP_VL1, EP_VL2, EP_VL4, EP_VL5, EP_VL8,
        EP_EEL, EP_QQ, EP_VE0, EP_VE1, EP_VE2, EP_VE4, EP_VE5, EP_VE8, EP_COUNT };
 
-template <int TPA, bool SMALLBOX, bool NEED_S>
+// minimum image of a cell-shifted displacement for boxes narrower than two
+// list radii (fractional coordinates rounded to the nearest image)
+template <class Box>
+__device__ __forceinline__ void min_image(const Box &B, float &dx, float &dy, float &dz) {
+  float s0 = B.hiF[0] * dx + B.hiF[1] * dy + B.hiF[2] * dz;
+  float s1 = B.hiF[3] * dx + B.hiF[4] * dy + B.hiF[5] * dz;
+  float s2 = B.hiF[6] * dx + B.hiF[7] * dy + B.hiF[8] * dz;
+  s0 -= rintf(s0);
+  s1 -= rintf(s1);
+  s2 -= rintf(s2);
+  dx = B.hF[0] * s0 + B.hF[1] * s1 + B.hF[2] * s2;
+  dy = B.hF[3] * s0 + B.hF[4] * s1 + B.hF[5] * s2;
+  dz = B.hF[6] * s0 + B.hF[7] * s1 + B.hF[8] * s2;
+}
+
+// BATCH = false: one system, its parameters in P and its shifts, cut-offs,
+// type map and (when they fit) tables staged in shared memory.  BATCH = true:
+// several systems; each atom group reads its system's parameters, shifts and
+// tables (global interaction / Coulomb-table indices) from sp[sys_of[t]].
+template <int TPA, bool SMALLBOX, bool NEED_S, bool BATCH>
 __global__ void __launch_bounds__(256) k_pair_mixed(
     MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ nlen, int stride, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
-    const float4 *__restrict__ gte, double *__restrict__ fout, double *__restrict__ fshort,
-    float *__restrict__ epart, long long *__restrict__ stat, const int *__restrict__ gs) {
+    const float4 *__restrict__ gte, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
+    double *__restrict__ fout, double *__restrict__ fshort, float *__restrict__ epart,
+    long long *__restrict__ stat, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
   float4 *shift = sm;                                   // 27
@@ -67,10 +87,12 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
   int nm4 = (P.ntypes * P.ntypes + 3) / 4;
   float4 *tl_s = sm + 28 + nf4 + nm4;
   const float4 *tl = gtl, *te = gte;
-  for (int k = threadIdx.x; k < 27; k += blockDim.x) shift[k] = gshift[k];
-  for (int k = threadIdx.x; k < 8 * P.ninter; k += blockDim.x) fcut[k] = gfcut[k];
-  for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) map[k] = gmap[k];
-  if (P.tab_smem) {
+  if (!BATCH) {
+    for (int k = threadIdx.x; k < 27; k += blockDim.x) shift[k] = gshift[k];
+    for (int k = threadIdx.x; k < 8 * P.ninter; k += blockDim.x) fcut[k] = gfcut[k];
+    for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) map[k] = gmap[k];
+  }
+  if (!BATCH && P.tab_smem) {
     int nl = (P.mask & 1) ? 3 * P.ninter * P.ntable : 0;
     int ne = (P.mask & 2) ? 2 * P.ntable : 0;
     for (int k = threadIdx.x; k < nl; k += blockDim.x) tl_s[k] = gtl[k];
@@ -100,28 +122,34 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
       const long long k0 = (long long)t * stride, k1 = k0 + nlen[t];
       float fx = 0, fy = 0, fz = 0, sx = 0, sy = 0, sz = 0;
       int cnt = 0;
+      // this atom's system: shifts, type map, cut-offs and tables
+      const SysP *Sp = BATCH ? sp + sys_of[t] : nullptr;
+      const float4 *shp = BATCH ? Sp->shift : shift;
+      const int *mapp = BATCH ? gmap + Sp->map0 : map;
+      const float *fcp = BATCH ? gfcut : fcut;
+      const int ntyp = BATCH ? Sp->ntypes : P.ntypes;
+      const bool has_el = (P.mask & 2) && (!BATCH || Sp->coul >= 0);
+      const float4 *tep = BATCH ? gte + (size_t)2 * P.ntable * (Sp->coul > 0 ? Sp->coul : 0) : te;
+      const float rc2_el = BATCH ? Sp->rc2_el : P.rc2_el;
+      const float dx2c = BATCH ? Sp->dx2c : P.dx2c;
+      const float offc = BATCH ? Sp->offc : P.offc;
+      const bool sb = BATCH ? Sp->smallbox != 0 : SMALLBOX;
       // one pair; xj and tj (j's type, needed only by LJ pairs) come from the
       // batched loads below
       auto pair = [&](const uint32_t en, const float4 xj, const int tj) {
-        const float4 sh = shift[(en >> ENT_CODE_SHIFT) & 31];
+        const float4 sh = shp[(en >> ENT_CODE_SHIFT) & 31];
         float dx = (xi.x - xj.x) + sh.x;
         float dy = (xi.y - xj.y) + sh.y;
         float dz = (xi.z - xj.z) + sh.z;
-        if (SMALLBOX) {
-          float s0 = P.hiF[0] * dx + P.hiF[1] * dy + P.hiF[2] * dz;
-          float s1 = P.hiF[3] * dx + P.hiF[4] * dy + P.hiF[5] * dz;
-          float s2 = P.hiF[6] * dx + P.hiF[7] * dy + P.hiF[8] * dz;
-          s0 -= rintf(s0);
-          s1 -= rintf(s1);
-          s2 -= rintf(s2);
-          dx = P.hF[0] * s0 + P.hF[1] * s1 + P.hF[2] * s2;
-          dy = P.hF[3] * s0 + P.hF[4] * s1 + P.hF[5] * s2;
-          dz = P.hF[6] * s0 + P.hF[7] * s1 + P.hF[8] * s2;
+        if (BATCH) {
+          if (sb) min_image(*Sp, dx, dy, dz);
+        } else if (SMALLBOX) {
+          min_image(P, dx, dy, dz);
         }
         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
         float ftot = 0.f, fsh = 0.f;
-        if ((en & fl_el) && (P.mask & 2) && r2 < P.rc2_el) {
-          float p = fmaf(r2, P.dx2c, -P.offc);
+        if ((en & fl_el) && has_el && r2 < rc2_el) {
+          float p = fmaf(r2, dx2c, -offc);
           int kk = (int)p;
           if (kk < 1) {
             under++;
@@ -129,12 +157,12 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
             p = 1.f;
           }
           p -= (float)kk;
-          const float4 c0 = te[2 * kk];
+          const float4 c0 = tep[2 * kk];
           const float qq = xi.w * xj.w;
           const float fe = qq * poly(p, c0.x, c0.y, c0.z);
           ftot += fe;
           if (P.iflg == 1) {
-            const float4 c1 = te[2 * kk + 1];
+            const float4 c1 = tep[2 * kk + 1];
             e[EP_EEL] = fmaf(qq, poly(p, c0.w, c1.x, c1.y), e[EP_EEL]);
             e[EP_QQ] += qq;
             const float fdx = fe * dx, fdy = fe * dy, fdz = fe * dz;
@@ -148,8 +176,8 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
           }
         }
         if ((en & fl_lj) && (P.mask & 1)) {
-          const int in = map[ti * P.ntypes + tj];
-          const float *fc = fcut + 8 * in;
+          const int in = mapp[ti * ntyp + tj];
+          const float *fc = fcp + 8 * in;
           const float rmax2 = P.iflg == 1 ? fc[0] : fc[4];
           if (r2 < rmax2) {
             float p = fmaf(r2, fc[2], -fc[1]);
@@ -271,16 +299,19 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
 }
 
 // FP64 sums of the per-atom partials into CM3D's accumulators (one block per
-// quantity, fixed order: deterministic).  Every pair was seen from both ends,
-// hence the factor 1/2; CM3D's virials are -sum d_a d_b f.
-__global__ void k_ereduce(int n, int mask, float tablast_e, const float *__restrict__ epart,
-                          double *__restrict__ acc, const int *__restrict__ gs) {
+// quantity and system, fixed order: deterministic).  Every pair was seen from
+// both ends, hence the factor 1/2; CM3D's virials are -sum d_a d_b f.
+__global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const float *__restrict__ epart,
+                          double *__restrict__ accs, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   __shared__ double red[32];
-  const int q = blockIdx.x;
+  const int q = blockIdx.x, sy = blockIdx.y;
   if (!((q < EP_EEL && (mask & 1)) || (q >= EP_EEL && (mask & 2)))) return;
+  const int a0 = sp[sy].a0, a1 = a0 + sp[sy].n;
+  const float tablast_e = sp[sy].tablast_e;
+  double *acc = accs + (size_t)sy * ACC_STRIDE;
   double s = 0;
-  for (int t = threadIdx.x; t < n; t += blockDim.x) s += (double)epart[(size_t)q * n + t];
+  for (int t = a0 + threadIdx.x; t < a1; t += blockDim.x) s += (double)epart[(size_t)q * n + t];
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
@@ -320,36 +351,39 @@ static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
   return b;
 }
 
-template <int TPA, bool SB, bool NS>
+template <int TPA, bool SB, bool NS, bool BT>
 static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   const int B = 256;
-  static bool attr_set = false;
-  static int per_sm = 1;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_pair_mixed<TPA, SB, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
+  auto kern = k_pair_mixed<TPA, SB, NS, BT>;
+  // the shared-memory limit is a per-device attribute: set it for every
+  // device this process launches on
+  static unsigned long long attr_devs = 0;
+  if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_devs |= 1ull << c->dev;
   }
   // persistent grid: as many resident blocks as the SMs hold, no more than
   // the atoms need
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pair_mixed<TPA, SB, NS>, B, smem);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, B, smem);
   if (per_sm < 1) per_sm = 1;
   long long need = ((long long)c->n * TPA + B - 1) / B;
   long long grid = (long long)c->num_sms * per_sm;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
-  k_pair_mixed<TPA, SB, NS><<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->nlen, c->nbr_stride,
-                                                      c->nbr, c->shift, c->map, c->fcut, c->ftab_lj, c->ftab_el,
-                                                      fout, c->fxs, c->epart, c->stat, c->gate);
+  kern<<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->nlen, c->nbr_stride, c->nbr, c->shift,
+                                 c->map, c->fcut, c->ftab_lj, c->ftab_el, c->sp, c->sys_of, fout, c->fxs, c->epart,
+                                 c->stat, c->gate);
 }
 
-template <bool SB, bool NS>
+template <bool SB, bool NS, bool BT>
 static int launch_tpa(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   switch (c->tpa) {
-    case 4: launch_t<4, SB, NS>(c, P, smem, fout); break;
-    case 8: launch_t<8, SB, NS>(c, P, smem, fout); break;
-    case 16: launch_t<16, SB, NS>(c, P, smem, fout); break;
-    case 32: launch_t<32, SB, NS>(c, P, smem, fout); break;
-    default: launch_t<8, SB, NS>(c, P, smem, fout); break;
+    case 4: launch_t<4, SB, NS, BT>(c, P, smem, fout); break;
+    case 8: launch_t<8, SB, NS, BT>(c, P, smem, fout); break;
+    case 16: launch_t<16, SB, NS, BT>(c, P, smem, fout); break;
+    case 32: launch_t<32, SB, NS, BT>(c, P, smem, fout); break;
+    default: launch_t<8, SB, NS, BT>(c, P, smem, fout); break;
   }
   return CM3D_NB_OK;
 }
@@ -393,17 +427,23 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
                                                   c->gate);
   cudaEvent_t e0;
   tbegin(c, 0, &e0);
-  if (sb) {
-    if (ns) launch_tpa<true, true>(c, P, smem, fout);
-    else launch_tpa<true, false>(c, P, smem, fout);
+  if (c->nsys > 1) {
+    // several systems: per-system parameters and tables from global memory
+    P.tab_smem = 0;
+    if (ns) launch_tpa<false, true, true>(c, P, 0, fout);
+    else launch_tpa<false, false, true>(c, P, 0, fout);
+  } else if (sb) {
+    if (ns) launch_tpa<true, true, false>(c, P, smem, fout);
+    else launch_tpa<true, false, false>(c, P, smem, fout);
   } else {
-    if (ns) launch_tpa<false, true>(c, P, smem, fout);
-    else launch_tpa<false, false>(c, P, smem, fout);
+    if (ns) launch_tpa<false, true, false>(c, P, smem, fout);
+    else launch_tpa<false, false, false>(c, P, smem, fout);
   }
   tend(c, 0, e0);
   c->launches += 2;
   if (iflg == 1) {
-    k_ereduce<<<EP_COUNT, 1024, 0, c->st>>>(c->n, mask, (float)c->tablast_e, c->epart, c->acc, c->gate);
+    k_ereduce<<<dim3(EP_COUNT, c->nsys), c->nsys > 1 ? 256 : 1024, 0, c->st>>>(c->n, mask, c->sp, c->epart,
+                                                                                 c->acc, c->gate);
     c->launches++;
   }
   CKL(c);
@@ -427,7 +467,8 @@ int pair_setup(Ctx *c) {
     a = 0.5 * (t[k + 1] - t[k - 1]);
     b = 0.5 * (t[k - 1] - 2.0 * t[k] + t[k + 1]);
   };
-  std::vector<float4> tl((size_t)3 * ni * nt), te((size_t)2 * nt);
+  const int ncoul = c->ncoul > 0 ? c->ncoul : 1;
+  std::vector<float4> tl((size_t)3 * ni * nt), te((size_t)2 * nt * ncoul);
   for (int in = 0; in < ni; in++) {
     for (int k = 0; k < nt; k++) {
       double d0 = 0, da = 0, db = 0, v0 = 0, va = 0, vb = 0, s0 = 0, sa = 0, sb = 0;
@@ -443,18 +484,20 @@ int pair_setup(Ctx *c) {
     }
   }
   if (c->ncharge > 0) {
-    std::vector<double> ct(nt), dct(nt);
-    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
-    for (int k = 0; k < nt; k++) {
-      double d0 = 0, da = 0, db = 0, v0 = 0, va = 0, vb = 0;
-      if (k >= 1 && k <= nt - 2) {
-        coef(dct.data(), k, d0, da, db);
-        coef(ct.data(), k, v0, va, vb);
+    // one erfc table per charged system (back to back, ntable each)
+    std::vector<double> ct((size_t)nt * c->ncoul), dct((size_t)nt * c->ncoul);
+    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * ct.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * dct.size(), cudaMemcpyDeviceToHost));
+    for (int tb = 0; tb < c->ncoul; tb++)
+      for (int k = 0; k < nt; k++) {
+        double d0 = 0, da = 0, db = 0, v0 = 0, va = 0, vb = 0;
+        if (k >= 1 && k <= nt - 2) {
+          coef(dct.data() + (size_t)tb * nt, k, d0, da, db);
+          coef(ct.data() + (size_t)tb * nt, k, v0, va, vb);
+        }
+        te[(size_t)2 * nt * tb + 2 * k] = make_float4((float)d0, (float)da, (float)db, (float)v0);
+        te[(size_t)2 * nt * tb + 2 * k + 1] = make_float4((float)va, (float)vb, 0.f, 0.f);
       }
-      te[2 * k] = make_float4((float)d0, (float)da, (float)db, (float)v0);
-      te[2 * k + 1] = make_float4((float)va, (float)vb, 0.f, 0.f);
-    }
   }
   // per interaction: rmaxl_cut2, rmins_cut2*dx2tab, dx2tab, rminl_cut2,
   // rmaxs_cut2, vtab[ntable-4]

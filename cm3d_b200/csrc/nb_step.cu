@@ -104,7 +104,9 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
                         const double *__restrict__ dxn, const int *__restrict__ gboff,
                         const int4 *__restrict__ bij, const double2 *__restrict__ bp,
                         const int *__restrict__ geoff, const int4 *__restrict__ eijk,
-                        const double2 *__restrict__ ep, int *__restrict__ istate, const int *__restrict__ gs) {
+                        const double2 *__restrict__ ep, const SysP *__restrict__ sp,
+                        const int *__restrict__ sys_of, int *__restrict__ sreb, int *__restrict__ istate,
+                        const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g == 0) istate[IS_INTR] = intr;
@@ -151,35 +153,52 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
       }
     }
   }
-  // nrefsh: any |r - r_last|^2 > skin^2/4 (md_finter.c:63-71)
+  // nrefsh: any |r - r_last|^2 > skin^2/4 (md_finter.c:63-71), per system
+  const int sy = sys_of[gatoms[a0]];
+  const double skin2q = sp[sy].skin2q;
   bool far = false;
   for (int a = a0; a < a1; a++) {
     int i = gatoms[a];
     double xc = dxn[i] - pos[i], yc = dxn[n + i] - pos[n + i], zc = dxn[2 * n + i] - pos[2 * n + i];
-    if (xc * xc + yc * yc + zc * zc > P.skin2q) far = true;
+    if (xc * xc + yc * yc + zc * zc > skin2q) far = true;
   }
-  if (far) istate[IS_REBUILD] = 1;
+  if (far) {
+    sreb[sy] = 1;
+    istate[IS_REBUILD] = 1;
+  }
 }
 
 // standalone displacement test (cm3d_nb_nrefsh)
-__global__ void k_disp(int n, double skin2q, const double *__restrict__ pos, const double *__restrict__ dxn,
+__global__ void k_disp(int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
+                       const double *__restrict__ pos, const double *__restrict__ dxn, int *__restrict__ sreb,
                        int *__restrict__ istate) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int sy = sys_of[i];
   double xc = dxn[i] - pos[i], yc = dxn[n + i] - pos[n + i], zc = dxn[2 * n + i] - pos[2 * n + i];
-  if (xc * xc + yc * yc + zc * zc > skin2q) istate[IS_REBUILD] = 1;
+  if (xc * xc + yc * yc + zc * zc > sp[sy].skin2q) {
+    sreb[sy] = 1;
+    istate[IS_REBUILD] = 1;
+  }
 }
 
 // RESETPOS (md_finter.c:79-95): if a rebuild is due fewer than 3 steps after
-// the previous one, pull every atom that moved more than skin/2 back toward
-// its position at the last rebuild (by CM3D's factor skin2/d^2)
-__global__ void k_resetpos(int n, double skin2q, double *__restrict__ pos, const double *__restrict__ dxn,
-                           const int *__restrict__ istate, long long *__restrict__ stat) {
+// the system's previous one, pull every atom that moved more than skin/2
+// back toward its position at the last rebuild (by CM3D's factor skin2/d^2)
+__global__ void k_resetpos(int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
+                           const int *__restrict__ sreb, const int *__restrict__ slast, double *__restrict__ pos,
+                           const double *__restrict__ dxn, const int *__restrict__ istate,
+                           long long *__restrict__ stat, long long *__restrict__ sstat) {
   if (istate[IS_REBUILD] == 0 || istate[IS_HALT] != 0) return;
-  if (istate[IS_ISTEP] - istate[IS_ISTEPLAST] >= 3) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i == 0) atomicAdd((unsigned long long *)(stat + ST_RESETS), 1ull);
   if (i >= n) return;
+  const int sy = sys_of[i];
+  if (sreb[sy] == 0 || istate[IS_ISTEP] - slast[sy] >= 3) return;
+  if (i == sp[sy].a0) {
+    atomicAdd((unsigned long long *)(stat + ST_RESETS), 1ull);
+    sstat[(size_t)sy * SS_COUNT + SS_RESETS] += 1;
+  }
+  const double skin2q = sp[sy].skin2q;
   double xc = pos[i] - dxn[i], yc = pos[n + i] - dxn[n + i], zc = pos[2 * n + i] - dxn[2 * n + i];
   double d2 = xc * xc + yc * yc + zc * zc;
   if (d2 > skin2q) {
@@ -200,6 +219,7 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
                              const int4 *__restrict__ bij, const double2 *__restrict__ bp,
                              const int *__restrict__ geoff, const int4 *__restrict__ eijk,
                              const double2 *__restrict__ ep, double *__restrict__ acc,
+                             const SysP *__restrict__ sp, const int *__restrict__ sys_of,
                              const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -208,7 +228,10 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
   double v[20];
 #pragma unroll
   for (int k = 0; k < 20; k++) v[k] = 0.;
+  int sy = -1;
   if (g < P.ngroups) {
+    sy = sys_of[gatoms[gaoff[g]]];
+    const double kappa = sp[sy].kappa, kappa2 = sp[sy].kappa2;
     for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
       int i = gatoms[a];
       fxl[i] = fxl[n + i] = fxl[2 * n + i] = 0.;
@@ -220,9 +243,9 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
       double xd = pos[ii] - pos[jj], yd = pos[n + ii] - pos[n + jj], zd = pos[2 * n + ii] - pos[2 * n + jj];
       double dis2 = xd * xd + yd * yd + zd * zd, dis = sqrt(dis2);
       double qijr = q[ii] * q[jj] / dis;
-      double erfr = erf(dis * P.kappa);
+      double erfr = erf(dis * kappa);
       v[0] += -qijr * erfr;
-      double dv = -qijr * (-2. * P.kappa * exp(-P.kappa2 * dis2) * sqrt_pi + erfr / dis);
+      double dv = -qijr * (-2. * kappa * exp(-kappa2 * dis2) * sqrt_pi + erfr / dis);
       v[1] += dis * dv;
       dv /= dis;
       v[2] += dv * xd * xd; v[3] += dv * xd * yd; v[4] += dv * xd * zd;
@@ -265,7 +288,7 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
                          ACC_VBOND, ACC_WBOND, ACC_WBONDT + 0, ACC_WBONDT + 1, ACC_WBONDT + 2,
                          ACC_WBONDT + 3, ACC_WBONDT + 4, ACC_WBONDT + 5, ACC_WBONDT + 6, ACC_WBONDT + 7,
                          ACC_WBONDT + 8, ACC_VBEND};
-  block_acc<20>(v, acc, slots);
+  sys_acc<20>(v, sy, acc, slots);
 }
 
 // end of force(1) / force(0): rmass (utils/md_util.new.c:219) and, inside
@@ -274,11 +297,14 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
 __global__ void k_finish(int n, int level, int kick, int rm_l, int rm_s, double dk_l, double dk_s,
                          const double *__restrict__ mass, double *__restrict__ fxl, double *__restrict__ fxs,
                          double *__restrict__ vel, double *__restrict__ acc, int *__restrict__ istate,
-                         int advance_step, const int *__restrict__ gs) {
+                         int advance_step, const int *__restrict__ sys_of, int batch,
+                         const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[6] = {0, 0, 0, 0, 0, 0};
+  int sy = -1;
   if (i < n) {
+    sy = sys_of[i];
     double r = 1. / mass[i];
     for (int d = 0; d < 3; d++) {
       int x = d * n + i;
@@ -300,7 +326,8 @@ __global__ void k_finish(int n, int level, int kick, int rm_l, int rm_s, double 
   if (i == 0 && advance_step) istate[IS_ISTEP] += 1;
   if (level == 1) {
     const int slots[6] = {ACC_P2MT + 0, ACC_P2MT + 1, ACC_P2MT + 2, ACC_P2MT + 4, ACC_P2MT + 5, ACC_P2MT + 8};
-    block_acc<6>(v, acc, slots);
+    if (batch) sys_acc<6>(v, sy, acc, slots);
+    else block_acc<6>(v, acc, slots);
   }
 }
 
@@ -339,15 +366,44 @@ struct UF {
   }
 };
 
-int step_setup(Ctx *c, const cm3d_nb_system *s) {
+int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   const int n = c->n;
-  UF uf(n);
-  for (int b = 0; b < s->nbonds; b++) uf.u(s->ibond[b], s->jbond[b]);
-  for (int b = 0; b < s->nbends; b++) {
-    uf.u(s->ibend[b], s->jbend[b]);
-    uf.u(s->jbend[b], s->kbend[b]);
+  // every system's bonds, bends and excluded Ewald pairs with global atom
+  // indices, in system order (CM3D's order inside a system)
+  std::vector<int4> mb, me;            // {i, j, -, -} / {i, j, k, -}
+  std::vector<double2> mbp, mep;       // {eq, fk}
+  std::vector<int2> mc;
+  for (int sy = 0; sy < nsys; sy++) {
+    const cm3d_nb_system *s = systems + sy;
+    const int a0 = c->h_sp[sy].a0;
+    for (int b = 0; b < s->nbonds; b++) {
+      int t = s->idxbond[b];
+      if (s->itypbond[t] != 0) {
+        set_error("system %d bond %d: only harmonic bonds are supported (itypbond %d)", sy, b, s->itypbond[t]);
+        return CM3D_NB_ERR_ARG;
+      }
+      mb.push_back(make_int4(a0 + s->ibond[b], a0 + s->jbond[b], 0, 0));
+      mbp.push_back(make_double2(s->eqbond[t], s->fkbond[t]));
+    }
+    for (int b = 0; b < s->nbends; b++) {
+      int t = s->idxbend[b];
+      if (s->itypbend[t] != 0) {
+        set_error("system %d bend %d: only harmonic bends are supported (itypbend %d)", sy, b, s->itypbend[t]);
+        return CM3D_NB_ERR_ARG;
+      }
+      me.push_back(make_int4(a0 + s->ibend[b], a0 + s->jbend[b], a0 + s->kbend[b], 0));
+      mep.push_back(make_double2(s->eqbend[t], s->fkbend[t]));
+    }
+    for (int b = 0; b < s->necorr; b++) mc.push_back(make_int2(a0 + s->iecorr[b], a0 + s->jecorr[b]));
   }
-  for (int b = 0; b < s->necorr; b++) uf.u(s->iecorr[b], s->jecorr[b]);
+  const int nb = (int)mb.size(), ne = (int)me.size(), nc = (int)mc.size();
+  UF uf(n);
+  for (int b = 0; b < nb; b++) uf.u(mb[b].x, mb[b].y);
+  for (int b = 0; b < ne; b++) {
+    uf.u(me[b].x, me[b].y);
+    uf.u(me[b].y, me[b].z);
+  }
+  for (int b = 0; b < nc; b++) uf.u(mc[b].x, mc[b].y);
   // groups numbered by their lowest atom
   std::vector<int> gid(n, -1), root_gid(n, -1);
   int ng = 0;
@@ -366,44 +422,34 @@ int step_setup(Ctx *c, const cm3d_nb_system *s) {
   }
   // bonds / bends / ecorr pairs grouped, CM3D's order kept inside a group
   std::vector<int> boff(ng + 1, 0), eoff(ng + 1, 0), coff(ng + 1, 0);
-  for (int b = 0; b < s->nbonds; b++) boff[gid[s->ibond[b]] + 1]++;
-  for (int b = 0; b < s->nbends; b++) eoff[gid[s->jbend[b]] + 1]++;
-  for (int b = 0; b < s->necorr; b++) coff[gid[s->iecorr[b]] + 1]++;
+  for (int b = 0; b < nb; b++) boff[gid[mb[b].x] + 1]++;
+  for (int b = 0; b < ne; b++) eoff[gid[me[b].y] + 1]++;
+  for (int b = 0; b < nc; b++) coff[gid[mc[b].x] + 1]++;
   for (int g = 0; g < ng; g++) {
     boff[g + 1] += boff[g];
     eoff[g + 1] += eoff[g];
     coff[g + 1] += coff[g];
   }
-  std::vector<int4> bij(s->nbonds > 0 ? s->nbonds : 1), eijk(s->nbends > 0 ? s->nbends : 1);
+  std::vector<int4> bij(nb > 0 ? nb : 1), eijk(ne > 0 ? ne : 1);
   std::vector<double2> bp(bij.size()), ep(eijk.size());
-  std::vector<int2> cij(s->necorr > 0 ? s->necorr : 1), cpair(cij.size());
+  std::vector<int2> cij(nc > 0 ? nc : 1), cpair(cij.size());
   {
     std::vector<int> cb(boff.begin(), boff.end() - 1), ce(eoff.begin(), eoff.end() - 1),
         cc(coff.begin(), coff.end() - 1);
-    for (int b = 0; b < s->nbonds; b++) {
-      int t = s->idxbond[b];
-      if (s->itypbond[t] != 0) {
-        set_error("bond %d: only harmonic bonds are supported (itypbond %d)", b, s->itypbond[t]);
-        return CM3D_NB_ERR_ARG;
-      }
-      int slot = cb[gid[s->ibond[b]]]++;
-      bij[slot] = make_int4(s->ibond[b], s->jbond[b], 0, 0);
-      bp[slot] = make_double2(s->eqbond[t], s->fkbond[t]);
+    for (int b = 0; b < nb; b++) {
+      int slot = cb[gid[mb[b].x]]++;
+      bij[slot] = mb[b];
+      bp[slot] = mbp[b];
     }
-    for (int b = 0; b < s->nbends; b++) {
-      int t = s->idxbend[b];
-      if (s->itypbend[t] != 0) {
-        set_error("bend %d: only harmonic bends are supported (itypbend %d)", b, s->itypbend[t]);
-        return CM3D_NB_ERR_ARG;
-      }
-      int slot = ce[gid[s->jbend[b]]]++;
-      eijk[slot] = make_int4(s->ibend[b], s->jbend[b], s->kbend[b], 0);
-      ep[slot] = make_double2(s->eqbend[t], s->fkbend[t]);
+    for (int b = 0; b < ne; b++) {
+      int slot = ce[gid[me[b].y]]++;
+      eijk[slot] = me[b];
+      ep[slot] = mep[b];
     }
-    for (int b = 0; b < s->necorr; b++) {
-      int slot = cc[gid[s->iecorr[b]]]++;
-      cij[slot] = make_int2(s->iecorr[b], s->jecorr[b]);
-      cpair[b] = make_int2(s->iecorr[b], s->jecorr[b]);
+    for (int b = 0; b < nc; b++) {
+      int slot = cc[gid[mc[b].x]]++;
+      cij[slot] = mc[b];
+      cpair[b] = mc[b];
     }
   }
   CK(cudaMalloc(&c->grp_atom_off, sizeof(int) * (ng + 1)));
@@ -450,7 +496,8 @@ int group_init(Ctx *c, bool zero_fxs) {
   k_group_init<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, zero_fxs ? 1 : 0, c->grp_atom_off, c->grp_atoms,
                                                          c->pos, c->q, c->fxl, c->fxs, c->grp_ecorr_off,
                                                          c->ecorr_ij, c->grp_bond_off, c->bond_ij, c->bond_p,
-                                                         c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc, c->gate);
+                                                         c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc, c->sp,
+                                                         c->sys_of, c->gate);
   tend(c, 3, e0);
   c->launches++;
   CKL(c);
@@ -461,7 +508,8 @@ int finish_level1(Ctx *c, double dter, double dter1, bool kick) {
   const int B = 256;
   bool rs = c->need_short || c->nres_lrf > 1;
   k_finish<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, 1, kick ? 1 : 0, 1, rs ? 1 : 0, dter, dter1, c->mass, c->fxl,
-                                               c->fxs, c->vel, c->acc, c->istate, kick ? 1 : 0, c->gate);
+                                               c->fxs, c->vel, c->acc, c->istate, kick ? 1 : 0, c->sys_of,
+                                               c->nsys > 1, c->gate);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
@@ -469,31 +517,39 @@ int finish_level1(Ctx *c, double dter, double dter1, bool kick) {
 
 static int finish_level0(Ctx *c, double dts2, bool kick) {
   k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, kick ? 1 : 0, 0, 1, 0, dts2, c->mass, c->fxl, c->fxs,
-                                                   c->vel, c->acc, c->istate, 0, c->gate);
+                                                   c->vel, c->acc, c->istate, 0, c->sys_of, c->nsys > 1, c->gate);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
 }
 
-int check_displacement(Ctx *c) {
+// clear the rebuild requests (the any-system flag and every system's own)
+static int clear_rebuild(Ctx *c) {
   CK(cudaMemsetAsync(c->istate + IS_REBUILD, 0, sizeof(int), c->st));
-  k_disp<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, .25 * c->skin * c->skin, c->pos, c->dxn, c->istate);
+  CK(cudaMemsetAsync(c->sreb, 0, sizeof(int) * (size_t)c->nsys, c->st));
+  return CM3D_NB_OK;
+}
+
+int check_displacement(Ctx *c) {
+  int rc;
+  if ((rc = clear_rebuild(c))) return rc;
+  k_disp<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, c->sp, c->sys_of, c->pos, c->dxn, c->sreb, c->istate);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
 }
 
 int reset_positions(Ctx *c) {
-  k_resetpos<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, .25 * c->skin * c->skin, c->pos, c->dxn, c->istate,
-                                                      c->stat);
+  k_resetpos<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, c->sp, c->sys_of, c->sreb, c->slast, c->pos, c->dxn,
+                                                      c->istate, c->stat, c->sstat);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
 }
 
-// zero every accumulator force(1) and getvireal fill
+// zero every accumulator force(1) and getvireal fill, in every system
 static int zero_acc(Ctx *c) {
-  CK(cudaMemsetAsync(c->acc, 0, sizeof(double) * ACC_COUNT, c->st));
+  CK(cudaMemset2DAsync(c->acc, sizeof(double) * ACC_STRIDE, 0, sizeof(double) * ACC_COUNT, (size_t)c->nsys, c->st));
   return CM3D_NB_OK;
 }
 
@@ -545,24 +601,24 @@ static int one_level(Ctx *c, int intr, bool gated) {
   int rc;
   StepP P = step_params(c);
   const int B = 128;
-  CK(cudaMemsetAsync(c->istate + IS_REBUILD, 0, sizeof(int), c->st));
+  if ((rc = clear_rebuild(c))) return rc;
   cudaEvent_t e0;
   tbegin(c, 3, &e0);
   k_inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
                                                     c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
                                                     c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
-                                                    c->bend_p, c->istate, c->gate);
+                                                    c->bend_p, c->sp, c->sys_of, c->sreb, c->istate, c->gate);
   tend(c, 3, e0);
   c->launches++;
   CKL(c);
   if ((rc = reset_positions(c))) return rc;
   if (gated) {
-    if ((rc = build_lists(c, true))) return rc;
+    if ((rc = build_lists(c, true, false))) return rc;
   } else {
     CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     if (c->h_istate[IS_REBUILD]) {
-      if ((rc = build_lists(c, false))) return rc;
+      if ((rc = build_lists(c, false, false))) return rc;
     }
   }
   return close_level(c, intr);
@@ -630,7 +686,7 @@ int run_step(Ctx *c, int istep0, int nsteps) {
   c->overflows_host++;
   const int failed = c->h_istate[IS_ISTEP], intr = c->h_istate[IS_INTR];
   CK(cudaMemsetAsync(c->istate + IS_HALT, 0, sizeof(int), c->st));
-  if ((rc = build_lists(c, false))) return rc;
+  if ((rc = build_lists(c, false, false))) return rc;
   if ((rc = close_level(c, intr))) return rc;
   for (int lv = intr + 1; lv < c->nres_lrf; lv++)
     if ((rc = one_level(c, lv, false))) return rc;

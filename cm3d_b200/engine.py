@@ -58,6 +58,13 @@ def load_library() -> C.CDLL:
         "cm3d_nb_default_options": (None, [C.POINTER(_abi.Options)]),
         "cm3d_nb_create": (C.c_int, [C.POINTER(_abi.SystemDesc), C.POINTER(_abi.Options), C.POINTER(vp)]),
         "cm3d_nb_destroy": (None, [vp]),
+        "cm3d_nb_create_batch": (C.c_int, [C.POINTER(_abi.SystemDesc), C.c_int, C.POINTER(_abi.Options),
+                                           C.POINTER(vp)]),
+        "cm3d_nb_num_systems": (C.c_int, [vp, ip]),
+        "cm3d_nb_system_atoms": (C.c_int, [vp, C.c_int, ip, ip]),
+        "cm3d_nb_get_system_energies": (C.c_int, [vp, C.c_int, C.POINTER(_abi.Energies)]),
+        "cm3d_nb_get_all_energies": (C.c_int, [vp, C.POINTER(_abi.Energies)]),
+        "cm3d_nb_system_counts": (C.c_int, [vp, C.POINTER(ll), C.POINTER(ll)]),
         "cm3d_nb_set_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_get_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_velocities": (C.c_int, [vp, dp, dp, dp]),
@@ -127,19 +134,31 @@ def measure_peaks(device: int = 0) -> tuple[float, float]:
 
 
 class Engine:
-    """One CM3D system resident on one GPU."""
+    """CM3D systems resident on one GPU: one system, or a batch of independent
+    systems (a list) that every kernel of a step covers at once.  In a batch
+    the per-atom arrays (positions, velocities, forces) hold all systems'
+    atoms back to back; `ranges[s]` is system s's (first, natoms)."""
 
-    def __init__(self, system: System, mode: int = _abi.MIXED, device: int = 0,
+    def __init__(self, system, mode: int = _abi.MIXED, device: int = 0,
                  need_short: bool = False, tpa: int = 0, use_graph: bool = True):
         L = load_library()
-        self.sys = system
-        self.n = system.natoms
+        systems = list(system) if isinstance(system, (list, tuple)) else [system]
+        self.systems = systems
+        self.sys = systems[0]
+        self.nsys = len(systems)
+        self.n = sum(s.natoms for s in systems)
         self.mode = mode
         opt = _abi.Options(device=device, mode=mode, need_short=int(need_short), tpa=tpa,
                            use_graph=int(use_graph))
         h = C.c_void_p()
-        check(L.cm3d_nb_create(C.byref(system.desc()), C.byref(opt), C.byref(h)), "cm3d_nb_create")
+        descs = (_abi.SystemDesc * self.nsys)(*[s.desc() for s in systems])
+        check(L.cm3d_nb_create_batch(descs, self.nsys, C.byref(opt), C.byref(h)), "cm3d_nb_create_batch")
         self._h = h
+        self.ranges = []
+        a0 = 0
+        for s in systems:
+            self.ranges.append((a0, s.natoms))
+            a0 += s.natoms
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -234,6 +253,25 @@ class Engine:
         t = np.zeros(9)
         check(load_library().cm3d_nb_getsvirter_e(self._h, C.byref(v), C.byref(w), _p(t)), "getsvirter_e")
         return {"velec": v.value, "welec": w.value, "welectensor": t}
+
+    def system_energies(self, sys: int) -> dict:
+        """getvireal + geteng of one system of a batch"""
+        e = _abi.Energies()
+        check(load_library().cm3d_nb_get_system_energies(self._h, sys, C.byref(e)), "get_system_energies")
+        return e.as_dict()
+
+    def all_energies(self) -> list[dict]:
+        arr = (_abi.Energies * self.nsys)()
+        check(load_library().cm3d_nb_get_all_energies(self._h, arr), "get_all_energies")
+        return [arr[k].as_dict() for k in range(self.nsys)]
+
+    def system_counts(self) -> tuple[np.ndarray, np.ndarray]:
+        """per-system (list rebuilds, RESETPOS events)"""
+        rb = np.zeros(self.nsys, np.int64)
+        rs = np.zeros(self.nsys, np.int64)
+        check(load_library().cm3d_nb_system_counts(self._h, _p(rb, C.c_longlong), _p(rs, C.c_longlong)),
+              "system_counts")
+        return rb, rs
 
     def getvewald(self) -> dict:
         p, w = C.c_double(0), C.c_double(0)

@@ -161,6 +161,28 @@ int cm3d_nb_create(const cm3d_nb_system *sys, const cm3d_nb_options *opt,
                    cm3d_nb_ctx **out);
 void cm3d_nb_destroy(cm3d_nb_ctx *ctx);
 
+/* ------------------------------------------------------------ batches */
+/* Many independent systems in one context (no CM3D counterpart: CM3D runs one
+   system per process).  Each system keeps its own box, cell grid, tables,
+   k-vectors, neighbour lists, rebuild decisions (nrefsh with RESETPOS) and
+   energies, exactly as it would alone; every kernel of a step covers all
+   systems at once.  The systems' atoms are concatenated in array order, so
+   the per-atom calls below (positions, velocities, forces) see
+   sum(natoms) atoms and system s owns [first, first + natoms) of them.
+   Requirements: the mixed engine, and the same ntable, dt and RESPA levels
+   (nres_lrf / nres_tors / nres_intra) in every system.  cm3d_nb_create is
+   cm3d_nb_create_batch with nsys = 1; the single-system routines below
+   report system 0. */
+int cm3d_nb_create_batch(const cm3d_nb_system *systems, int nsys,
+                         const cm3d_nb_options *opt, cm3d_nb_ctx **out);
+int cm3d_nb_num_systems(cm3d_nb_ctx *ctx, int *nsys);
+int cm3d_nb_system_atoms(cm3d_nb_ctx *ctx, int sys, int *first, int *natoms);
+/* getvireal()+geteng() of one system / of every system (e[nsys]) */
+int cm3d_nb_get_system_energies(cm3d_nb_ctx *ctx, int sys, cm3d_nb_energies *e);
+int cm3d_nb_get_all_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e);
+/* per-system list rebuilds and RESETPOS events since creation (arrays of nsys) */
+int cm3d_nb_system_counts(cm3d_nb_ctx *ctx, long long *rebuilds, long long *resets);
+
 /* host <-> device state (COORDS.px..pz, vx..vz, hmat) */
 int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py,
                           const double *pz);

@@ -1,0 +1,131 @@
+"""Batches: several independent systems in one context (cm3d_nb_create_batch).
+
+Every system of a batch must come out as it does alone.  The checks:
+  - its pair lists, cut out of the batch's lists, are bit-exact with CM3D's;
+  - its forces and energies match the same system in its own context
+    (relative 1e-12 / 1e-10: the same kernels, only the order of FP64
+    atomic adds in the reciprocal-space force pass can differ) and CM3D's
+    within the mixed engine's stated bounds (forces 1e-5, energies 1e-5,
+    virials 5e-5);
+  - its trajectory tracks CM3D's per-step energies (2e-4, as for a single
+    system) and its own single-context run (positions within 1e-9 A), with
+    the same number of list rebuilds and RESETPOS events.
+
+Systems are grouped by time step and RESPA levels, which a batch shares.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import force_scale, golden, rel_rms, xyz
+from cm3d_b200 import _abi
+from cm3d_b200.engine import Engine, EngineError
+from cm3d_b200.system import System
+from tests.golden.make_golden import pair_key
+
+pytestmark = pytest.mark.gpu
+
+GROUPS = {
+    "dt5fs": ["argon864", "binary256"],
+    "dt1fs": ["lj256", "lj2"],
+    "water": ["water216", "water4096"],
+}
+ETOL, VTOL, FTOL = 1e-5, 5e-5, 1e-5
+VIRIAL_KEYS = {"winter", "welec", "W", "prsi"}
+
+
+TPA = 16          # lanes per atom, fixed so that a system sums its pairs alike alone and in a batch
+
+
+def batch(names, **kw):
+    ds = [golden(n) for n in names]
+    return ds, Engine([System.from_arrays(d) for d in ds], mode=_abi.MIXED, tpa=TPA, **kw)
+
+
+def close(a, b, tol):
+    return abs(a - b) <= tol * max(abs(b), 1e-300) or abs(a - b) <= 1e-9
+
+
+@pytest.mark.parametrize("group", list(GROUPS))
+def test_batch_lists_bit_exact(engine_lib, group):
+    ds, e = batch(GROUPS[group])
+    e.get_ngbr()
+    for tag, w in (("t", _abi.LIST_T), ("s", _abi.LIST_S), ("te", _abi.LIST_TE), ("se", _abi.LIST_SE)):
+        i, j = e.pair_list(w)
+        for s, d in enumerate(ds):
+            a0, n = e.ranges[s]
+            sel = (i >= a0) & (i < a0 + n)
+            assert ((j[sel] >= a0) & (j[sel] < a0 + n)).all(), "a pair crosses systems"
+            assert int(sel.sum()) == int(d[f"npr{tag}"][0]), (tag, s)
+            if sel.any():
+                h = hashlib.sha256(pair_key(i[sel] - a0, j[sel] - a0, n).tobytes()).hexdigest()
+                assert h == str(d[f"list_{tag}_hash"]), (tag, s)
+    e.close()
+
+
+@pytest.mark.parametrize("group", list(GROUPS))
+def test_batch_forces_and_energies(engine_lib, group):
+    names = GROUPS[group]
+    ds, e = batch(names)
+    e.get_ngbr()
+    e.force(1)
+    e.force(2)
+    fb = e.forces(_abi.FXL)
+    en = e.all_energies()
+    e.close()
+    for s, (name, d) in enumerate(zip(names, ds)):
+        a0, n = e.ranges[s]
+        one = Engine(System.from_arrays(d), mode=_abi.MIXED, tpa=TPA)
+        one.get_ngbr()
+        one.force(1)
+        one.force(2)
+        f1 = one.forces(_abi.FXL)
+        e1 = one.energies()
+        one.close()
+        fs = force_scale(d) / float(np.sqrt((d["amass"] ** 2).mean()))
+        assert rel_rms(fb[:, a0:a0 + n], f1, fs) <= 1e-12, name
+        assert rel_rms(fb[:, a0:a0 + n], xyz(d, "acc_l"), fs) <= FTOL, name
+        for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke", "vbond", "vbend"):
+            assert close(en[s][k], e1[k], 1e-10), (name, k, en[s][k], e1[k])
+        for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke"):
+            tol = VTOL if k in VIRIAL_KEYS else ETOL
+            assert close(en[s][k], float(d[f"e0_{k}"][0]), tol), (name, k)
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+@pytest.mark.parametrize("group", list(GROUPS))
+def test_batch_trajectory(engine_lib, group, graph):
+    names = GROUPS[group]
+    ds, e = batch(names, use_graph=graph)
+    nsteps = min(int(d["nsteps"][0]) for d in ds)
+    e.step_init()
+    for k in range(nsteps):
+        e.step(1 + k, 1)
+        en = e.all_energies()
+        for s, d in enumerate(ds):
+            ref = d["traj_eng"].reshape(-1, 8)
+            for c, key in enumerate(("poter", "potra", "zke")):
+                tol = 2e-4 if c != 1 else 2e-3
+                assert close(en[s][key], ref[k, c], tol), (names[s], k, key)
+    pos = e.positions()
+    rb, rs = e.system_counts()
+    e.close()
+    for s, d in enumerate(ds):
+        a0, n = e.ranges[s]
+        one = Engine(System.from_arrays(d), mode=_abi.MIXED, tpa=TPA, use_graph=graph)
+        one.step_init()
+        one.step(1, nsteps)
+        p1 = one.positions()
+        rb1, rs1 = one.system_counts()
+        one.close()
+        assert np.abs(pos[:, a0:a0 + n] - p1).max() <= 1e-9, names[s]
+        assert rb[s] == rb1[0] and rs[s] == rs1[0], (names[s], rb[s], rb1[0], rs[s], rs1[0])
+
+
+def test_batch_rejects_mismatched_steps(engine_lib):
+    with pytest.raises(EngineError, match="dt"):
+        batch(["argon864", "water216"])
+    d = golden("lj256")
+    with pytest.raises(EngineError, match="mixed"):
+        Engine([System.from_arrays(d), System.from_arrays(d)], mode=_abi.PLAIN_FP64)
