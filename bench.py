@@ -1,22 +1,27 @@
-"""Benchmark of the CM3D nonbonded engine on one B200 (or N replicas).
+"""Benchmark of the CM3D nonbonded engine on one B200 (or N ranks).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload water12288|argon864|water331776]
+                    [--workload ensemble1024|water12288|water331776|argon864]
 
-A step is one CM3D RESPA outer step (integrate/md_step.c:62: inner bonded
-levels, neighbour-list check/rebuild, full nonbonded + Ewald forces, kicks)
-of the workload on the GPU.  The default workload is the flexible-water box of
-4096 molecules (12,288 atoms, 16^3 grid, L = 49.66 A, Ewald alpha 0.31,
-kmax 7, rc 10 A, RESPA 0.5/2 fs) run for the 1000 outer steps the workload
-names; inputs are synthetic and seeded (cm3d_b200.configs).
+A step is one CM3D outer step (integrate/md_step.c:62: inner bonded levels,
+neighbour-list check/rebuild with RESETPOS, full nonbonded + Ewald forces,
+kicks) of every system of the workload.  Default workload: the uneven
+ensemble of 1024 independent boxes (N log-uniform in [64, 4096], reduced
+density U(0.6, 0.9), T* U(0.7, 1.5), 75% argon LJ, 25% charged +/-0.5 e
+binary with Ewald alpha = 3.2/rc and kmax 5, rc = min(2.5 sigma, 0.45 L), FCC
+start, dt 5 fs), run as one batch.  Inputs are synthetic and seeded
+(cm3d_b200.configs) and written in CM3D's own input formats.
 
 Printed: one JSON line (rank 0) with the contract's keys plus
-  plain_fp64   the same run through the plain FP64 one-system engine
-  roofline     the fused pair kernel against its FP32 / HBM roofline
-  cpu_baseline CM3D itself (oracle/_ref/ref_bench) on this host's cores
-  e2e          the same metric through the public API with host buffers
-Under torchrun (N > 1) every rank runs an independent replica (the path has
-no collective: "replicas only"); value = all ranks' atom-steps / max time.
+  plain_fp64      the same systems through the plain FP64 engine, one system
+                  per context and per launch (the comparator of the metric)
+  roofline        the fused pair kernel against its FP32 / HBM roofline
+  cpu_baseline    CM3D itself (oracle/_ref/ref_bench) on this host's cores
+  e2e             the same metric through the public API with host buffers
+  latency         per-step device time p50 / p99
+  other_workloads the water-12288 box, mixed and plain, in the same run
+Under torchrun (N > 1) every rank runs its own ensemble (seed + rank): the
+systems are independent and no collective touches the step path.
 """
 from __future__ import annotations
 
@@ -40,23 +45,32 @@ UNIT = "atom-steps/s"
 # per unique listed pair (i < j) of CM3D's te / t lists (algorithmic counts)
 FLOPS_ELEC_PAIR = 57.0
 FLOPS_LJ_EXTRA = 14.0
+FLOPS_LJ_ONLY = FLOPS_ELEC_PAIR - 16.0 + FLOPS_LJ_EXTRA   # no charge product / erfc tables
 BYTES_PAIR = 4.0                  # one 32-bit neighbour index
 BYTES_ATOM = 16.0 + 24.0          # float4 position/charge in, FP64 force out
 
 
 def workload(name: str, seed: int):
+    """(list of Workloads, description, default steps)"""
     from cm3d_b200 import configs
+    if name == "ensemble1024":
+        return configs.ensemble(1024, seed=2024 + seed - 1), \
+            "ensemble-1024: 1024 independent boxes, N log-uniform in [64, 4096] (953,101 atoms at seed 2024), " \
+            "rho* U(0.6,0.9), T* U(0.7,1.5), 75% argon LJ / 25% charged +/-0.5 e binary (Ewald alpha 3.2/rc, " \
+            "kmax 5), rc min(2.5 sigma, 0.45 L), skin 0.3 sigma, FCC start, dt 5 fs, one batch", 300
     if name == "water12288":
-        return configs.water_box(ngrid=16, seed=seed, ntime=1000), \
-            "water-12288: 4096 flexible 3-site waters on a 16^3 grid, L 49.66 A, alpha 0.31, kmax 7, " \
-            "rc 10 A, skin 0.5 A, RESPA 0.5/2 fs (nres_intra 4), 300 K"
+        return [configs.water_box(ngrid=16, seed=seed, ntime=1000, placement="octant")], \
+            "water-12288: 4096 flexible 3-site waters on a 16^3 grid (seeded orientations, no intermolecular " \
+            "contact under 1.9 A), L 49.66 A, alpha 0.31, kmax 7, rc 10 A, skin 0.5 A, RESPA 0.5/2 fs " \
+            "(nres_intra 4), 300 K", 1000
     if name == "water331776":
-        return configs.water_box(ngrid=48, seed=seed, skin=1.5, kmax=21, ntime=500), \
-            "water-331776: 110592 flexible 3-site waters on a 48^3 grid, L 148.98 A, alpha 0.31, kmax 21, " \
-            "rc 10 A, skin 1.5 A, RESPA 0.5/2 fs"
+        return [configs.water_box(ngrid=48, seed=seed, skin=1.5, kmax=21, ntime=500, placement="octant")], \
+            "water-331776: 110592 flexible 3-site waters on a 48^3 grid (seeded orientations, no " \
+            "intermolecular contact under 1.9 A), L 148.98 A, alpha 0.31, kmax 21, rc 10 A, skin 1.5 A, " \
+            "RESPA 0.5/2 fs", 100
     if name == "argon864":
-        return configs.argon_fcc(seed=seed, ntime=1000), \
-            "argon-864: LJ argon FCC 6^3x4, rho* 0.8442, rc 2.5 sigma, skin 0.3 sigma, dt 5 fs, 120 K"
+        return [configs.argon_fcc(seed=seed, ntime=1000)], \
+            "argon-864: LJ argon FCC 6^3x4, rho* 0.8442, rc 2.5 sigma, skin 0.3 sigma, dt 5 fs, 120 K", 1000
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -131,10 +145,11 @@ def l2_flusher(device: int):
     return flush
 
 
-def timed_run(eng, steps: int, warmup: int, istep0: int, flush) -> tuple[float, int]:
+def timed_run(eng, steps: int, warmup: int, istep0: int, flush) -> tuple[float, int, list]:
     """W untimed steps, then K steps each timed on the device (CUDA events
     around the step's graph replay on the engine's stream), with an L2 flush
-    between steps outside the timed events.  Returns (total ms, kernels)."""
+    between steps outside the timed events.  Returns (total ms, kernels
+    launched in the timed steps, per-step ms)."""
     istep = istep0
     for _ in range(warmup):
         eng.step(istep, 1)
@@ -142,14 +157,17 @@ def timed_run(eng, steps: int, warmup: int, istep0: int, flush) -> tuple[float, 
     eng.synchronize()
     eng.enable_timing(2)
     l0 = eng.launch_count()
+    per, prev = [], 0.0
     for _ in range(steps):
         flush()
         eng.step(istep, 1)
         istep += 1
-    ms, n = eng.kernel_time(4)
+        tot, _ = eng.kernel_time(4)
+        per.append(tot - prev)
+        prev = tot
     launches = eng.launch_count() - l0
     eng.enable_timing(0)
-    return ms, launches
+    return prev, launches, per
 
 
 def pinned(n: int):
@@ -163,7 +181,8 @@ def pinned(n: int):
 def e2e_run(eng, steps: int, istep0: int, n: int) -> tuple[float, int, int]:
     """The public API with host buffers: every step uploads positions and
     velocities from pinned host memory, runs one step, and reads positions,
-    velocities and the energies back (CM3D's host loop owning the state)."""
+    velocities and every system's energies back (CM3D's host loop owning the
+    state)."""
     px, vx = [pinned(3 * n).reshape(3, n) for _ in range(2)]
     px[:] = eng.positions()
     vx[:] = eng.velocities()
@@ -175,29 +194,34 @@ def e2e_run(eng, steps: int, istep0: int, n: int) -> tuple[float, int, int]:
         eng.step(istep0 + s, 1)
         px[:] = eng.positions()
         vx[:] = eng.velocities()
-        eng.energies()
+        eng.all_energies()
     dt = time.perf_counter() - t0
     h2d = 2 * 3 * n * 8
-    d2h = 2 * 3 * n * 8 + 72 * 8
+    d2h = 2 * 3 * n * 8 + 96 * 8 * eng.nsys
     return dt, h2d, d2h
 
 
-def roofline(eng, steps: int, istep0: int, n: int, fp32_tflops: float, hbm_gbs: float) -> dict:
+def roofline(eng, steps: int, istep0: int, fp32_tflops: float, hbm_gbs: float) -> dict:
     """Time the fused pair kernel with CUDA events around every launch (eager
     launches on the engine's stream) and compare with its roofline: the
     slower of its algorithmic bytes / HBM bandwidth and its algorithmic flops
-    / FP32 FMA throughput (both measured)."""
+    / FP32 FMA throughput (both measured).  Pairs are CM3D's unique listed
+    pairs (te for charged systems, t otherwise), counted from its own lists."""
     from cm3d_b200 import _abi
     eng.enable_timing(1)
     eng.step(istep0, steps)
     ms, launches = eng.kernel_time(0)
     eng.enable_timing(0)
-    pte = len(eng.pair_list(_abi.LIST_TE)[0])
-    pt = len(eng.pair_list(_abi.LIST_T)[0])
-    flops = pte * FLOPS_ELEC_PAIR + pt * FLOPS_LJ_EXTRA
-    if pte == 0:
-        flops = pt * (FLOPS_ELEC_PAIR - 16 + FLOPS_LJ_EXTRA)
-    nbytes = (pte if pte else pt) * BYTES_PAIR + n * BYTES_ATOM
+    ite, _ = eng.pair_list(_abi.LIST_TE)
+    it, _ = eng.pair_list(_abi.LIST_T)
+    starts = np.array([a for a, _ in eng.ranges] + [eng.n])
+    pte_s = np.bincount(np.searchsorted(starts, ite, side="right") - 1, minlength=eng.nsys)
+    pt_s = np.bincount(np.searchsorted(starts, it, side="right") - 1, minlength=eng.nsys)
+    charged = pte_s > 0
+    flops = float((pte_s * FLOPS_ELEC_PAIR + pt_s * FLOPS_LJ_EXTRA)[charged].sum()
+                  + (pt_s * FLOPS_LJ_ONLY)[~charged].sum())
+    pairs = float(pte_s[charged].sum() + pt_s[~charged].sum())
+    nbytes = pairs * BYTES_PAIR + eng.n * BYTES_ATOM
     t = ms / 1e3 / max(launches, 1)
     t_bw = nbytes / (hbm_gbs * 1e9)
     t_fl = flops / (fp32_tflops * 1e12)
@@ -205,7 +229,7 @@ def roofline(eng, steps: int, istep0: int, n: int, fp32_tflops: float, hbm_gbs: 
     try:
         with open(os.path.join(ROOT, "profiles", "pair_kernel_traffic.json")) as fh:
             tr = json.load(fh)
-        traffic = tr.get("dram_bytes_per_launch_scaled", tr.get("dram_bytes_per_launch"))
+        traffic = tr.get(eng.workload_name, {}).get("dram_bytes_per_launch")
     except Exception:
         pass
     if t_fl >= t_bw:
@@ -215,11 +239,13 @@ def roofline(eng, steps: int, istep0: int, n: int, fp32_tflops: float, hbm_gbs: 
         out = {"bound": "hbm", "achieved": nbytes / t / 1e9, "peak": hbm_gbs, "unit": "GB/s",
                "frac": (nbytes / t / 1e9) / hbm_gbs}
     out.update({"traffic": traffic, "kernel": "k_pair_mixed (fused LJ + real-space Ewald)",
-                "ms_per_launch": t * 1e3, "launches": launches, "pairs_te": pte, "pairs_t": pt,
+                "ms_per_launch": t * 1e3, "launches": launches, "unique_pairs": pairs,
+                "pairs_te": int(pte_s.sum()), "pairs_t": int(pt_s.sum()),
                 "algorithmic_flops": flops, "algorithmic_bytes": nbytes,
                 "hbm_frac": (nbytes / t / 1e9) / hbm_gbs,
                 "fp32_frac": (flops / t / 1e12) / fp32_tflops,
-                "peak_source": "fp32: cm3d_nb_measure_peaks (this run); hbm: MEASURED_PEAKS.json"})
+                "peak_source": "fp32: cm3d_nb_measure_peaks (this run, of measured); "
+                               "hbm: MEASURED_PEAKS.json (of measured)"})
     return out
 
 
@@ -229,15 +255,29 @@ def ref_bench_bin() -> str | None:
     return p if os.path.exists(p) else None
 
 
-def cpu_reference(wl, steps: int, procs: int) -> dict:
-    """CM3D itself on the host: `procs` independent replicas of the deck, each
-    timing `steps` of CM3D's step() after its own start-up."""
+def cpu_steps(natoms: int, charged: bool) -> int:
+    # ~10-20 s of CM3D on one core: LJ runs near 4e5 atom-steps/s, Ewald
+    # systems near 3.5e4
+    rate = 3.0e4 if charged else 3.0e5
+    return max(2, min(2000, int(12.0 * rate / max(natoms, 1))))
+
+
+def cpu_reference(wls, procs: int) -> dict:
+    """CM3D itself on the host: `procs` processes, each running one system of
+    the workload (a sample spread over the ensemble) for a bounded number of
+    steps of CM3D's step() after its own start-up; aggregate atom-steps/s over
+    the longest process time."""
     exe = ref_bench_bin()
+    pick = np.linspace(0, len(wls) - 1, num=min(procs, len(wls))).round().astype(int)
+    if len(wls) == 1:
+        pick = np.zeros(procs, int)
     with tempfile.TemporaryDirectory() as tmp:
         jobs = []
-        for p in range(procs):
+        for p, k in enumerate(pick):
+            wl = wls[int(k)]
             d = os.path.join(tmp, f"r{p}")
             inp = wl.write(d)
+            steps = cpu_steps(wl.natoms, "kmax" in wl.keywords)
             jobs.append(subprocess.Popen([exe, os.path.basename(inp), str(steps)], cwd=d,
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
         res = []
@@ -247,37 +287,94 @@ def cpu_reference(wl, steps: int, procs: int) -> dict:
             res.append(json.loads(line))
     tmax = max(r["seconds"] for r in res)
     total = sum(r["natoms"] * r["steps"] for r in res)
-    return {"value": total / tmax, "unit": UNIT, "cores": procs, "kind": "reference",
-            "sample": f"{procs} x CM3D step() (oracle/_ref/ref_bench, gcc -O2) for {steps} steps of the "
-                      f"same deck after start-up; single-process {res[0]['atom_steps_per_s']:.4g} atom-steps/s",
-            "single_process": res[0]["atom_steps_per_s"]}
+    natoms = sum(r["natoms"] for r in res)
+    return {"value": total / tmax, "unit": UNIT, "cores": len(res), "kind": "reference",
+            "sample": f"{len(res)} host processes, each CM3D step() (oracle/_ref/ref_bench, gcc -O2) on one "
+                      f"system of the workload ({natoms} atoms in all) for a bounded number of steps after "
+                      f"its start-up; value = their atom-steps / the longest process time",
+            "single_process_mean": float(np.mean([r["atom_steps_per_s"] for r in res]))}
 
 
-def cpu_port(sysm, steps: int) -> dict:
+def cpu_port(systems, steps: int) -> dict:
     from oracle import Oracle
-    o = Oracle(sysm)
+    o = Oracle(systems[0])
     o.step_init()
     t0 = time.perf_counter()
     o.step(1, steps)
     dt = time.perf_counter() - t0
-    return {"value": sysm.natoms * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"oracle (C restatement of CM3D) for {steps} steps"}
+    return {"value": systems[0].natoms * steps / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle (C restatement of CM3D) for {steps} steps of one system"}
 
 
-def cpu_sample_steps(natoms: int) -> int:
-    # ~10-20 s of CM3D on one core: water runs at ~3.5e4 atom-steps/s
-    return max(2, min(200, int(4.0e5 / max(natoms, 1))))
+# ------------------------------------------------------------ GPU arms
+def plain_arm(systems, device: int, steps: int, warmup: int, flush) -> dict:
+    """The plain FP64 engine, one system per context: each system's steps run
+    as their own launches (graph replays), one system after another, so the
+    ensemble's step time is the sum of its systems' step times."""
+    from cm3d_b200 import _abi
+    from cm3d_b200.engine import Engine
+    ms_tot, atoms = 0.0, 0
+    for sm in systems:
+        pe = Engine(sm, mode=_abi.PLAIN_FP64, device=device)
+        pe.step_init()
+        ms, _, _ = timed_run(pe, steps, warmup, 1, lambda: None)
+        pe.close()
+        ms_tot += ms
+        atoms += sm.natoms
+    flush()
+    return {"value": atoms * steps / (ms_tot / 1e3), "unit": UNIT, "ms_per_step": ms_tot / steps,
+            "steps": steps, "systems": len(systems),
+            "timing": "CUDA events around each system's step graph replay, summed over systems"}
+
+
+def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float, hbm: float, name: str,
+              e2e_steps: int, dist=None) -> dict:
+    import torch
+    from cm3d_b200 import _abi
+    from cm3d_b200.engine import Engine
+    eng = Engine(systems, mode=_abi.MIXED, device=device)
+    eng.workload_name = name
+    eng.step_init()
+    n = eng.n
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clk:
+        ms, launches, per = timed_run(eng, steps, warmup, 1, flush)
+    torch.cuda.synchronize(device)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    status = eng.status()
+    istep = 1 + warmup + steps
+    if dist:
+        dist.barrier()
+    dt_e2e, h2d, d2h = e2e_run(eng, e2e_steps, istep, n)
+    istep += e2e_steps
+    if dist:
+        t = torch.tensor([dt_e2e], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt_e2e = float(t.item())
+    roof = roofline(eng, 20, istep, fp32, hbm)
+    en = eng.all_energies()
+    eng.close()
+    return {"ms": ms, "launches": launches, "per_step_ms": per, "n": n, "status": status,
+            "e2e": (dt_e2e, h2d, d2h, e2e_steps), "roofline": roof, "energies": en,
+            "clocks": clk.summary()}
 
 
 # ------------------------------------------------------------------- main
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="water12288")
+    ap.add_argument("--workload", default="ensemble1024")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -286,20 +383,22 @@ def main() -> None:
     if args.impl == "reference":
         if rank != 0:
             return
-        wl, desc = workload(args.workload, seed=1)
-        steps = cpu_sample_steps(wl.natoms)
-        procs = max(1, min(os.cpu_count() or 1, 32))
+        wls, desc, dsteps = workload(args.workload, seed=1)
+        steps = args.steps if args.steps is not None else dsteps
+        warmup = args.warmup if args.warmup is not None else 20
+        procs = max(1, min(os.cpu_count() or 1, 64))
         if ref_bench_bin():
-            base = cpu_reference(wl, steps, procs)
+            base = cpu_reference(wls, procs)
         else:
             from cm3d_b200.setup import build_system
-            base = cpu_port(build_system(wl), steps)
+            base = cpu_port([build_system(wls[0])], 20)
+        natoms = sum(w.natoms for w in wls)
         line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": 1e3 * wl.natoms / base["value"] * base["cores"],
+                "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+                "ms_per_step": 1e3 * natoms / base["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": {"workload": desc, "natoms": wl.natoms,
-                                                "parallelism": f"{base['cores']} host processes (replicas)"},
+                "data": "synthetic", "config": {"workload": desc, "natoms": natoms,
+                                                "parallelism": f"{base['cores']} host processes"},
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -312,95 +411,81 @@ def main() -> None:
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    from cm3d_b200 import _abi
-    from cm3d_b200.engine import Engine, measure_peaks
+    from cm3d_b200.engine import measure_peaks
     from cm3d_b200.setup import build_system
 
-    wl, desc = workload(args.workload, seed=1 + rank)
-    sysm = build_system(wl)
-    n = sysm.natoms
+    wls, desc, dsteps = workload(args.workload, seed=1 + rank)
+    steps = args.steps if args.steps is not None else dsteps
+    warmup = args.warmup if args.warmup is not None else 20
+    systems = [build_system(w) for w in wls]
     peaks = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     fp32, fp64 = measure_peaks(local)
-
-    eng = Engine(sysm, mode=_abi.MIXED, device=local)
-    eng.step_init()
     flush = l2_flusher(local)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize(local)
-    with ClockSampler(local) as clk:
-        ms, launches = timed_run(eng, args.steps, args.warmup, 1, flush)
-    torch.cuda.synchronize(local)
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    value = world * n * args.steps / (ms / 1e3)
-    status = eng.status()
-    istep = 1 + args.warmup + args.steps
 
-    # end to end through the public API with host buffers
-    e2e_steps = min(args.steps, 300)
-    if dist:
-        dist.barrier()
-    dt_e2e, h2d, d2h = e2e_run(eng, e2e_steps, istep, n)
-    istep += e2e_steps
-    if dist:
-        t = torch.tensor([dt_e2e], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dt_e2e = float(t.item())
+    m = mixed_arm(systems, local, steps, warmup, flush, fp32, hbm, args.workload, min(steps, 100), dist)
+    n = m["n"]
+    ms = m["ms"]
+    value = world * n * steps / (ms / 1e3)
+    dt_e2e, h2d, d2h, e2e_steps = m["e2e"]
     e2e_value = world * n * e2e_steps / dt_e2e
-
-    roof = roofline(eng, 50, istep, n, fp32, hbm)
-    en = eng.energies()
-    eng.close()
 
     plain = None
     if not args.no_plain:
-        psteps = min(args.steps, 300)
-        pe = Engine(sysm, mode=_abi.PLAIN_FP64, device=local)
-        pe.step_init()
-        pms, _ = timed_run(pe, psteps, min(args.warmup, 10), 1, flush)
-        pe.close()
-        if dist:
-            t = torch.tensor([pms], dtype=torch.float64, device=f"cuda:{local}")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            pms = float(t.item())
-        pval = world * n * psteps / (pms / 1e3)
-        plain = {"value": pval, "unit": UNIT, "ms_per_step": pms / psteps, "steps": psteps,
-                 "speedup_mixed_vs_plain": value / pval}
+        psteps = 10 if len(systems) > 1 else min(steps, 300)
+        plain = plain_arm(systems, local, psteps, 3 if len(systems) > 1 else 10, flush)
+        plain["value"] *= world
+        plain["speedup_mixed_vs_plain"] = value / plain["value"]
+
+    other = {}
+    if not args.no_extra and args.workload != "water12288" and world == 1:
+        wwl, wdesc, _ = workload("water12288", seed=1)
+        wsys = [build_system(w) for w in wwl]
+        wm = mixed_arm(wsys, local, 500, 20, flush, fp32, hbm, "water12288", 100)
+        wval = wm["n"] * 500 / (wm["ms"] / 1e3)
+        wplain = None if args.no_plain else plain_arm(wsys, local, 300, 10, flush)
+        other["water12288"] = {
+            "workload": wdesc, "value": wval, "unit": UNIT, "ms_per_step": wm["ms"] / 500, "steps": 500,
+            "ns_per_day": (500 / (wm["ms"] / 1e3)) * float(wsys[0]["dt"]) * 86400.0 / 1e3,
+            "plain_fp64": wplain,
+            "speedup_mixed_vs_plain": (wval / wplain["value"]) if wplain else None,
+            "roofline": wm["roofline"], "status": {k: wm["status"][k] for k in ("rebuilds", "resets")}}
 
     cpu = None
     if rank == 0 and world == 1:
-        steps = cpu_sample_steps(n)
-        cpu = cpu_reference(wl, steps, 1) if ref_bench_bin() else cpu_port(sysm, steps)
+        cpu = (cpu_reference(wls, max(1, min(os.cpu_count() or 1, 64))) if ref_bench_bin()
+               else cpu_port(systems, 20))
 
     if rank == 0:
-        dt_ps = float(sysm["dt"])
-        ms_step = ms / args.steps
+        dt_ps = float(systems[0]["dt"])
+        per = np.array(m["per_step_ms"])
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": ms / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "accumulate": "f64",
             "data": "synthetic (seeded; CM3D input decks from cm3d_b200.configs)",
-            "config": {"workload": desc, "natoms": n, "mode": "mixed (FP32 compute, FP64 accumulation)",
-                       "parallelism": "replicas only" if world > 1 else "single system",
+            "config": {"workload": desc, "natoms": n, "systems": len(systems),
+                       "mode": "mixed (FP32 compute, FP64 accumulation), one batch",
+                       "parallelism": f"{world} ranks, each its own ensemble (seed + rank)" if world > 1
+                       else "one GPU",
                        "l2": "flushed between timed steps (256 MB write outside the step's events)",
                        "timing": "CUDA events around each step's graph replay on the engine stream; "
                                  "max over ranks"},
-            "ns_per_day": (args.steps / (ms / 1e3)) * dt_ps * 86400.0 / 1e3,
-            "gpu_launches": launches,
-            "roofline": roof,
+            "ns_per_day": (steps / (ms / 1e3)) * dt_ps * 86400.0 / 1e3,
+            "latency": {"unit": "ms per step (device)", "p50": float(np.percentile(per, 50)),
+                        "p99": float(np.percentile(per, 99))},
+            "gpu_launches": m["launches"],
+            "roofline": m["roofline"],
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},
             "plain_fp64": plain,
+            "other_workloads": other,
             "peaks": {"fp32_tflops": fp32, "fp64_tflops": fp64, "hbm_gbs": hbm},
-            "clocks": clk.summary(),
-            "status": {k: status[k] for k in ("rebuilds", "resets", "overflows", "table_underflow")},
-            "final_energy": {"poter": en["poter"], "zke": en["zke"]},
+            "clocks": m["clocks"],
+            "status": {k: m["status"][k] for k in ("rebuilds", "resets", "overflows", "table_underflow")},
+            "final_energy": {"poter_sum": float(sum(e["poter"] for e in m["energies"])),
+                             "zke_sum": float(sum(e["zke"] for e in m["energies"]))},
         }
         print(json.dumps(line))
     if dist:

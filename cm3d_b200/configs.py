@@ -197,10 +197,16 @@ def _random_rotations(n: int, rng) -> np.ndarray:
 def water_box(ngrid: int = 16, temp: float = 300.0, seed: int = 1,
               rc: float | None = None, alpha: float = 0.31, kmax: int = 7,
               skin: float = 0.5, dt_fs: float = 2.0, nres_intra: int = 4,
-              ntime: int = 1000, ntable: int = 500, name: str = "water") -> Workload:
+              ntime: int = 1000, ntable: int = 500, name: str = "water",
+              placement: str = "checkerboard") -> Workload:
     """Flexible 3-site water: ngrid^3 molecules on a cubic grid at 1.0 g/cm^3
     with seeded random orientations.  Ewald with `alpha` and a spherical
-    k-space cutoff `kmax` (CM3D's kmax keyword, md_ewald.c:93-114)."""
+    k-space cutoff `kmax` (CM3D's kmax keyword, md_ewald.c:93-114).
+    `placement` is how orientations with close intermolecular contacts are
+    re-drawn: "checkerboard" (half of the clashing molecules per sweep, at
+    most 200 sweeps; the decks of the test fixtures) or "octant" (one parity
+    class at a time until clear; converges in a few rounds, used for large
+    grids)."""
     w = WATER
     nmol = ngrid ** 3
     L = ngrid * WATER_SPACING
@@ -224,31 +230,77 @@ def water_box(ngrid: int = 16, temp: float = 300.0, seed: int = 1,
     # some H atoms within 1 A of each other)
     min_contact = 1.9
     g = pos.reshape(ngrid, ngrid, ngrid, 3, 3)
-    for _sweep in range(200):
-        bad = np.zeros((ngrid, ngrid, ngrid), dtype=bool)
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    if (dx, dy, dz) == (0, 0, 0):
-                        continue
-                    nb = np.roll(g, shift=(dx, dy, dz), axis=(0, 1, 2))
-                    d = g[:, :, :, :, None, :] - nb[:, :, :, None, :, :]
-                    d -= L * np.round(d / L)
-                    r = np.sqrt((d * d).sum(-1)).min(axis=(-1, -2))
-                    bad |= r < min_contact
-        nbad = int(bad.sum())
-        if nbad == 0:
-            break
-        idx = np.argwhere(bad)
-        # re-draw only a checkerboard subset per sweep so neighbours that
-        # clash with each other do not both move at once
-        sel = idx[(idx.sum(1) + _sweep) % 2 == 0]
-        if sel.shape[0] == 0:
-            sel = idx[:1]
+    offs = np.array([(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)
+                     if (dx, dy, dz) != (0, 0, 0)])
+
+    def clashes(cells: np.ndarray) -> np.ndarray:
+        # closest intermolecular contact of the molecules at grid `cells`
+        # (k, 3) with their 26 grid neighbours, below min_contact?
+        out = np.zeros(cells.shape[0], dtype=bool)
+        for k0 in range(0, cells.shape[0], 65536):
+            c = cells[k0:k0 + 65536]
+            mine = g[c[:, 0], c[:, 1], c[:, 2]]                   # (k, 3, 3)
+            r = np.full(c.shape[0], np.inf)
+            for o in offs:
+                nb = (c + o) % ngrid
+                d = mine[:, :, None, :] - g[nb[:, 0], nb[:, 1], nb[:, 2]][:, None, :, :]
+                d -= L * np.round(d / L)
+                r = np.minimum(r, np.sqrt((d * d).sum(-1)).min(axis=(-1, -2)))
+            out[k0:k0 + 65536] = r < min_contact
+        return out
+
+    stencil = np.vstack([np.zeros((1, 3), int), offs])
+
+    def redraw(sel: np.ndarray) -> None:
         Rn = _random_rotations(sel.shape[0], rng)
         oo = g[sel[:, 0], sel[:, 1], sel[:, 2], 0]
         g[sel[:, 0], sel[:, 1], sel[:, 2], 1] = oo + Rn @ h1
         g[sel[:, 0], sel[:, 1], sel[:, 2], 2] = oo + Rn @ h2
+
+    def around(sel: np.ndarray) -> np.ndarray:
+        # the molecules at `sel` and their grid neighbours, each once
+        near = ((sel[:, None, :] + stencil[None, :, :]) % ngrid).reshape(-1, 3)
+        key = np.unique((near[:, 0] * ngrid + near[:, 1]) * ngrid + near[:, 2])
+        return np.stack([key // (ngrid * ngrid), (key // ngrid) % ngrid, key % ngrid], axis=1)
+
+    every = np.argwhere(np.ones((ngrid, ngrid, ngrid), dtype=bool))
+    bad = clashes(every).reshape(ngrid, ngrid, ngrid)
+    if placement == "octant" and ngrid % 2 == 0:
+        # Neighbours differ in the parity of at least one coordinate, so the
+        # molecules of one parity class (x, y, z mod 2) can be re-drawn
+        # together against fixed neighbours; each class is re-drawn until it
+        # is clear, then the next, for a few rounds.
+        for _round in range(20):
+            if not bad.any():
+                break
+            for cls in range(8):
+                par = np.array([(cls >> 2) & 1, (cls >> 1) & 1, cls & 1])
+                moved = []
+                for _try in range(50):
+                    idx = np.argwhere(bad)
+                    sel = idx[(idx % 2 == par).all(axis=1)]
+                    if sel.shape[0] == 0:
+                        break
+                    redraw(sel)
+                    moved.append(sel)
+                    bad[sel[:, 0], sel[:, 1], sel[:, 2]] = clashes(sel)
+                if moved:
+                    near = around(np.concatenate(moved))
+                    bad[near[:, 0], near[:, 1], near[:, 2]] = clashes(near)
+    else:
+        for _sweep in range(200):
+            if not bad.any():
+                break
+            idx = np.argwhere(bad)
+            # re-draw only a checkerboard subset per sweep so neighbours that
+            # clash with each other do not both move at once
+            sel = idx[(idx.sum(1) + _sweep) % 2 == 0]
+            if sel.shape[0] == 0:
+                sel = idx[:1]
+            redraw(sel)
+            # only the re-drawn molecules and their neighbours can change state
+            near = around(sel)
+            bad[near[:, 0], near[:, 1], near[:, 2]] = clashes(near)
     pos = g.reshape(-1, 3)
     m = np.tile([w["m_o"], w["m_h"], w["m_h"]], nmol)
     vel = maxwell_boltzmann(m, temp, rng)
@@ -323,3 +375,104 @@ def charged_binary(natoms: int = 256, density: float = 0.75, tstar: float = 1.0,
                     species=[("cat", n // 2, topa), ("ani", n - n // 2, topb)],
                     inter_parms=inter, pos=pos, vel=vel, mass_amu=m, box=L,
                     temp=temp, dt_fs=dt_fs)
+
+
+# ------------------------------------------- uneven ensemble of small boxes
+def _fcc_sites(natoms: int, rng) -> tuple[np.ndarray, int]:
+    """`natoms` sites of the smallest FCC lattice (4 ncell^3 sites) that holds
+    them, as fractional coordinates; a seeded choice of sites when the lattice
+    has more than needed (vacancies spread through the box)."""
+    ncell = max(1, int(math.ceil((natoms / 4.0) ** (1.0 / 3.0) - 1e-9)))
+    basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    cells = np.array([(i, j, k) for i in range(ncell) for j in range(ncell)
+                      for k in range(ncell)], dtype=float)
+    sites = ((cells[:, None, :] + basis[None, :, :] + 0.25) / ncell).reshape(-1, 3)
+    if sites.shape[0] > natoms:
+        keep = np.sort(rng.choice(sites.shape[0], natoms, replace=False))
+        sites = sites[keep]
+    return sites, ncell
+
+
+def lj_box(natoms: int, density: float, tstar: float, seed: int, charged: bool = False,
+           charge: float = 0.5, kmax: int = 5, dt_fs: float = 5.0, ntime: int = 2000,
+           name: str = "ljbox") -> Workload:
+    """One box of the uneven ensemble: `natoms` argon-parameter LJ atoms at
+    reduced density `density` and reduced temperature `tstar` on an FCC start,
+    rc = min(2.5 sigma, 0.45 L) with a 0.3 sigma skin.  `charged`: an
+    equimolar binary mixture with charges +/- `charge` e (natoms rounded down
+    to even), Ewald alpha = 3.2 / rc and a spherical kmax."""
+    sig, eps, mass = ARGON["sig"], ARGON["eps"], ARGON["mass"]
+    if charged and natoms % 2:
+        natoms -= 1
+    rng = np.random.default_rng(seed)
+    L = (natoms / density) ** (1.0 / 3.0) * sig
+    frac, _ = _fcc_sites(natoms, rng)
+    pos = frac * L
+    temp = tstar * eps
+    m = np.full(natoms, mass)
+    vel = maxwell_boltzmann(m, temp, rng)
+    rc = min(2.5 * sig, 0.45 * L)
+    skin = 0.3 * sig
+    kw = _base_keywords(name, dt_fs, temp, ntime)
+    kw.update({"skin": skin, "shift": 1, "nres_lrf": 1, "nres_intra": 1,
+               "nres_tors": 1, "neighbor_list": "verlist"})
+    if not charged:
+        top = (f"~mol_name_def[\\mol_name{{argon}}\\natom{{1}}\\nbond{{0}}]\n"
+               f"~atom_def[\\atom_typ{{ar}}\\atom_ind{{1}}\\mass{{{mass!r}}}\\charge{{0}}]\n")
+        return Workload(name=name, keywords=kw, species=[("argon", natoms, top)],
+                        inter_parms=[_lj_parm("ar", "ar", eps, sig, 0.55 * sig, rc, rc)],
+                        pos=pos, vel=vel, mass_amu=m, box=L, temp=temp, dt_fs=dt_fs)
+    kw.update({"alp_ewald": 3.2 / rc, "kmax": kmax, "rcute_max": rc, "rcute_resp": rc,
+               "rcute_min": 1.0})
+    topa = (f"~mol_name_def[\\mol_name{{cat}}\\natom{{1}}\\nbond{{0}}]\n"
+            f"~atom_def[\\atom_typ{{ca}}\\atom_ind{{1}}\\mass{{{mass!r}}}"
+            f"\\charge{{{charge!r}}}]\n")
+    topb = (f"~mol_name_def[\\mol_name{{ani}}\\natom{{1}}\\nbond{{0}}]\n"
+            f"~atom_def[\\atom_typ{{an}}\\atom_ind{{1}}\\mass{{{mass!r}}}"
+            f"\\charge{{{-charge!r}}}]\n")
+    pos = pos[rng.permutation(natoms)]
+    inter = [_lj_parm("ca", "ca", eps, sig, 0.55 * sig, rc, rc),
+             _lj_parm("an", "an", eps, sig, 0.55 * sig, rc, rc),
+             _lj_parm("an", "ca", eps, sig, 0.55 * sig, rc, rc)]
+    return Workload(name=name, keywords=kw,
+                    species=[("cat", natoms // 2, topa), ("ani", natoms // 2, topb)],
+                    inter_parms=inter, pos=pos, vel=vel, mass_amu=m, box=L, temp=temp,
+                    dt_fs=dt_fs)
+
+
+@dataclass
+class EnsembleMember:
+    """One box of an ensemble, with the draws it was generated from."""
+    index: int
+    natoms: int
+    density: float
+    tstar: float
+    charged: bool
+    seed: int
+
+
+def ensemble_plan(nsys: int = 1024, seed: int = 2024, nmin: int = 64, nmax: int = 4096,
+                  frac_charged: float = 0.25) -> list[EnsembleMember]:
+    """The draws of the uneven ensemble: N log-uniform in [nmin, nmax],
+    reduced density U(0.6, 0.9), reduced temperature U(0.7, 1.5), a per-box
+    seed, and exactly round(frac_charged * nsys) charged binary boxes."""
+    rng = np.random.default_rng(seed)
+    ncharged = int(round(frac_charged * nsys))
+    charged = np.zeros(nsys, bool)
+    charged[rng.permutation(nsys)[:ncharged]] = True
+    out = []
+    for k in range(nsys):
+        n = int(round(math.exp(rng.uniform(math.log(nmin), math.log(nmax)))))
+        rho = float(rng.uniform(0.6, 0.9))
+        ts = float(rng.uniform(0.7, 1.5))
+        sd = int(rng.integers(1, 2 ** 31 - 1))
+        out.append(EnsembleMember(k, n, rho, ts, bool(charged[k]), sd))
+    return out
+
+
+def ensemble(nsys: int = 1024, seed: int = 2024, ntime: int = 2000, **kw) -> list[Workload]:
+    """The uneven ensemble as Workloads (argon-parameter LJ and charged binary
+    boxes, FCC start, dt 5 fs, kmax 5 for the charged ones)."""
+    return [lj_box(m.natoms, m.density, m.tstar, m.seed, charged=m.charged, ntime=ntime,
+                   name=f"box{m.index:04d}")
+            for m in ensemble_plan(nsys, seed, **kw)]

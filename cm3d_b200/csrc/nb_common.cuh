@@ -70,7 +70,8 @@ struct SysP {
   double rmaxl_skin2_e, rmaxs_skin2_e;   // -1 without charges
   double skin2q;             // (skin / 2)^2
   double falp2, rvol, kappa, kappa2;
-  float4 shift[27];          // cell-corner shifts H k / nc, k in {-1, 0, 1}^3
+  float4 shift[27];          // cell-corner shifts H k / nc, k in {-1, 0, 1}^3 (FP32 hi part)
+  float4 shift_lo[27];       // their FP32 residuals (shift + shift_lo = the FP64 shift)
 };
 // device status words (long long)
 enum {

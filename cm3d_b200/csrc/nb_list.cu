@@ -559,9 +559,12 @@ int list_setup(Ctx *c) {
         for (int d = -1; d <= 1; d++) {
           double f0 = (double)a / P.nc[0], f1 = (double)b / P.nc[1], f2 = (double)d / P.nc[2];
           const double *h = H.hmat;
-          P.shift[(a + 1) * 9 + (b + 1) * 3 + (d + 1)] =
-              make_float4((float)(h[0] * f0 + h[1] * f1 + h[2] * f2), (float)(h[3] * f0 + h[4] * f1 + h[5] * f2),
-                          (float)(h[6] * f0 + h[7] * f1 + h[8] * f2), 0.f);
+          const double v0 = h[0] * f0 + h[1] * f1 + h[2] * f2, v1 = h[3] * f0 + h[4] * f1 + h[5] * f2,
+                       v2 = h[6] * f0 + h[7] * f1 + h[8] * f2;
+          const int k = (a + 1) * 9 + (b + 1) * 3 + (d + 1);
+          P.shift[k] = make_float4((float)v0, (float)v1, (float)v2, 0.f);
+          P.shift_lo[k] = make_float4((float)(v0 - (double)(float)v0), (float)(v1 - (double)(float)v1),
+                                      (float)(v2 - (double)(float)v2), 0.f);
         }
     // first guess of the full-list slot: 1.3 x the mean number of atoms in
     // a list sphere, plus 64
@@ -597,8 +600,9 @@ int list_setup(Ctx *c) {
   CK(cudaMalloc(&c->xq, sizeof(float4) * (size_t)c->n));
   CK(cudaMalloc(&c->cimg, sizeof(int4) * (size_t)c->n));
   // system 0's shifts (the single-system pair kernel keeps them in shared memory)
-  CK(cudaMalloc(&c->shift, sizeof(float4) * 27));
+  CK(cudaMalloc(&c->shift, sizeof(float4) * 54));
   CK(cudaMemcpy(c->shift, c->h_sp[0].shift, sizeof(float4) * 27, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->shift + 27, c->h_sp[0].shift_lo, sizeof(float4) * 27, cudaMemcpyHostToDevice));
   if (c->mode == CM3D_NB_MIXED) {
     CK(cudaMalloc(&c->nlen, sizeof(int) * (size_t)c->n));
     long long s = ((long long)est_max + 31) / 32 * 32;

@@ -19,7 +19,10 @@
 //     the atoms), so the table load is paid once per SM, not per atom group;
 //   * forces are summed per lane in FP32 over chunks of 16 pairs and then in
 //     FP64; energies and virials are summed per atom in FP32 and written as
-//     per-atom partials that k_ereduce adds up in FP64 in a fixed order.
+//     per-atom partials that k_ereduce adds up in FP64 in a fixed order --
+//     except the table base values of the LJ energy, whose hi parts are
+//     summed in FP64 (an LJ energy is a sum of terms of both signs that can
+//     nearly cancel).
 #include "nb_common.cuh"
 
 namespace cm3d {
@@ -52,18 +55,18 @@ enum { EP_ELJ = 0, EP_ELJH, EP_VL0, EP_VL1, EP_VL2, EP_VL4, EP_VL5, EP_VL8,
        EP_EEL, EP_QQ, EP_VE0, EP_VE1, EP_VE2, EP_VE4, EP_VE5, EP_VE8, EP_COUNT };
 
 // minimum image of a cell-shifted displacement for boxes narrower than two
-// list radii (fractional coordinates rounded to the nearest image)
+// list radii: the nearest lattice vector m = rint(H^-1 d) is subtracted only
+// when it is not zero, so that d keeps its precision in the common case
 template <class Box>
 __device__ __forceinline__ void min_image(const Box &B, float &dx, float &dy, float &dz) {
-  float s0 = B.hiF[0] * dx + B.hiF[1] * dy + B.hiF[2] * dz;
-  float s1 = B.hiF[3] * dx + B.hiF[4] * dy + B.hiF[5] * dz;
-  float s2 = B.hiF[6] * dx + B.hiF[7] * dy + B.hiF[8] * dz;
-  s0 -= rintf(s0);
-  s1 -= rintf(s1);
-  s2 -= rintf(s2);
-  dx = B.hF[0] * s0 + B.hF[1] * s1 + B.hF[2] * s2;
-  dy = B.hF[3] * s0 + B.hF[4] * s1 + B.hF[5] * s2;
-  dz = B.hF[6] * s0 + B.hF[7] * s1 + B.hF[8] * s2;
+  const float m0 = rintf(B.hiF[0] * dx + B.hiF[1] * dy + B.hiF[2] * dz);
+  const float m1 = rintf(B.hiF[3] * dx + B.hiF[4] * dy + B.hiF[5] * dz);
+  const float m2 = rintf(B.hiF[6] * dx + B.hiF[7] * dy + B.hiF[8] * dz);
+  if (m0 != 0.f || m1 != 0.f || m2 != 0.f) {
+    dx -= B.hF[0] * m0 + B.hF[1] * m1 + B.hF[2] * m2;
+    dy -= B.hF[3] * m0 + B.hF[4] * m1 + B.hF[5] * m2;
+    dz -= B.hF[6] * m0 + B.hF[7] * m1 + B.hF[8] * m2;
+  }
 }
 
 // BATCH = false: one system, its parameters in P and its shifts, cut-offs,
@@ -77,18 +80,18 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
     const float4 *__restrict__ gte, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
     double *__restrict__ fout, double *__restrict__ fshort, float *__restrict__ epart,
-    long long *__restrict__ stat, const int *__restrict__ gs) {
+    double *__restrict__ epart64, long long *__restrict__ stat, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
-  float4 *shift = sm;                                   // 27
-  float *fcut = reinterpret_cast<float *>(sm + 28);     // 8 * ninter
+  float4 *shift = sm;                                   // 27 hi + 27 lo
+  float *fcut = reinterpret_cast<float *>(sm + 54);     // 8 * ninter
   int nf4 = (8 * P.ninter + 3) / 4;
-  int *map = reinterpret_cast<int *>(sm + 28 + nf4);    // ntypes^2
+  int *map = reinterpret_cast<int *>(sm + 54 + nf4);    // ntypes^2
   int nm4 = (P.ntypes * P.ntypes + 3) / 4;
-  float4 *tl_s = sm + 28 + nf4 + nm4;
+  float4 *tl_s = sm + 54 + nf4 + nm4;
   const float4 *tl = gtl, *te = gte;
   if (!BATCH) {
-    for (int k = threadIdx.x; k < 27; k += blockDim.x) shift[k] = gshift[k];
+    for (int k = threadIdx.x; k < 54; k += blockDim.x) shift[k] = gshift[k];
     for (int k = threadIdx.x; k < 8 * P.ninter; k += blockDim.x) fcut[k] = gfcut[k];
     for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) map[k] = gmap[k];
   }
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
   for (int tb = blockIdx.x * groups; tb < P.n; tb += gridDim.x * groups) {
     const int t = tb + threadIdx.x / TPA;
     const bool active = t < P.n;
-    double Fx = 0, Fy = 0, Fz = 0, Sx = 0, Sy = 0, Sz = 0;
+    double Fx = 0, Fy = 0, Fz = 0, Sx = 0, Sy = 0, Sz = 0, elj_hi = 0;
     float e[EP_COUNT];
 #pragma unroll
     for (int k = 0; k < EP_COUNT; k++) e[k] = 0.f;
@@ -125,6 +128,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
       // this atom's system: shifts, type map, cut-offs and tables
       const SysP *Sp = BATCH ? sp + sys_of[t] : nullptr;
       const float4 *shp = BATCH ? Sp->shift : shift;
+      const float4 *shlp = BATCH ? Sp->shift_lo : shift + 27;
       const int *mapp = BATCH ? gmap + Sp->map0 : map;
       const float *fcp = BATCH ? gfcut : fcut;
       const int ntyp = BATCH ? Sp->ntypes : P.ntypes;
@@ -137,10 +141,11 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
       // one pair; xj and tj (j's type, needed only by LJ pairs) come from the
       // batched loads below
       auto pair = [&](const uint32_t en, const float4 xj, const int tj) {
-        const float4 sh = shp[(en >> ENT_CODE_SHIFT) & 31];
-        float dx = (xi.x - xj.x) + sh.x;
-        float dy = (xi.y - xj.y) + sh.y;
-        float dz = (xi.z - xj.z) + sh.z;
+        const int code = (en >> ENT_CODE_SHIFT) & 31;
+        const float4 sh = shp[code], shl = shlp[code];
+        float dx = ((xi.x - xj.x) + sh.x) + shl.x;
+        float dy = ((xi.y - xj.y) + sh.y) + shl.y;
+        float dz = ((xi.z - xj.z) + sh.z) + shl.z;
         if (BATCH) {
           if (sb) min_image(*Sp, dx, dy, dz);
         } else if (SMALLBOX) {
@@ -189,18 +194,19 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
             }
             p -= (float)kk;
             const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
-            const float4 a0 = T[0], a1 = T[1];
+            const float4 a0 = T[0], a1 = T[1], a2 = T[2];
             const float f = poly(p, a0.x, a0.y, a0.z);
             float swv = 1.f;
-            if ((NEED_S || P.iflg == 0) && r2 > fc[3]) {
-              const float4 a2 = T[2];
-              swv = poly(p, a1.z, a1.w, a2.x);
-            }
+            if ((NEED_S || P.iflg == 0) && r2 > fc[3]) swv = poly(p, a1.z, a1.w, a2.x);
             if (P.iflg == 1) {
               ftot += f;
-              const float v = poly(p, a0.w, a1.x, a1.y);
-              e[EP_ELJ] += v;
-              e[EP_ELJH] += v - fc[5];
+              // V = v0 + p (vA + p vB) with v0 = hi (a0.w) + lo (a2.y): the
+              // hi parts are summed in FP64, so that an LJ energy whose pair
+              // terms cancel keeps FP64-like accuracy
+              elj_hi += (double)a0.w;
+              const float vlo = a2.y + p * fmaf(p, a1.y, a1.x);
+              e[EP_ELJ] += vlo;
+              e[EP_ELJH] += vlo - fc[5];
               const float fdx = f * dx, fdy = f * dy, fdz = f * dz;
               e[EP_VL0] = fmaf(fdx, dx, e[EP_VL0]);
               e[EP_VL1] = fmaf(fdx, dy, e[EP_VL1]);
@@ -277,6 +283,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
       if (P.iflg == 1) {
 #pragma unroll
         for (int k = 0; k < EP_COUNT; k++) e[k] += __shfl_xor_sync(0xffffffffu, e[k], o);
+        elj_hi += __shfl_xor_sync(0xffffffffu, elj_hi, o);
       }
     }
     if (active && g == 0) {
@@ -292,6 +299,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
       if (P.iflg == 1) {
 #pragma unroll
         for (int k = 0; k < EP_COUNT; k++) epart[(size_t)k * n + t] = e[k];
+        epart64[t] = elj_hi;
       }
     }
   }
@@ -302,7 +310,8 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
 // quantity and system, fixed order: deterministic).  Every pair was seen from
 // both ends, hence the factor 1/2; CM3D's virials are -sum d_a d_b f.
 __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const float *__restrict__ epart,
-                          double *__restrict__ accs, const int *__restrict__ gs) {
+                          const double *__restrict__ epart64, double *__restrict__ accs,
+                          const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   __shared__ double red[32];
   const int q = blockIdx.x, sy = blockIdx.y;
@@ -310,8 +319,11 @@ __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const fl
   const int a0 = sp[sy].a0, a1 = a0 + sp[sy].n;
   const float tablast_e = sp[sy].tablast_e;
   double *acc = accs + (size_t)sy * ACC_STRIDE;
+  // the LJ energies add the FP64 sums of the table's hi parts
+  const bool hi = q == EP_ELJ || q == EP_ELJH;
   double s = 0;
-  for (int t = a0 + threadIdx.x; t < a1; t += blockDim.x) s += (double)epart[(size_t)q * n + t];
+  for (int t = a0 + threadIdx.x; t < a1; t += blockDim.x)
+    s += (double)epart[(size_t)q * n + t] + (hi ? epart64[t] : 0.0);
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
@@ -343,13 +355,17 @@ __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const fl
 // ------------------------------------------------------------------ host
 static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
   size_t nf4 = (8 * (size_t)c->ninter + 3) / 4, nm4 = ((size_t)c->ntypes * c->ntypes + 3) / 4;
-  size_t b = (28 + nf4 + nm4) * sizeof(float4);
+  size_t b = (54 + nf4 + nm4) * sizeof(float4);
   if (with_tables) {
     b += (size_t)3 * c->ninter * c->ntable * sizeof(float4);
     if (mask & 2) b += (size_t)2 * c->ntable * sizeof(float4);
   }
   return b;
 }
+
+// per-atom FP64 partials of the LJ energy's table hi parts, stored after the
+// EP_COUNT FP32 rows of epart
+static double *epart_hi(Ctx *c) { return reinterpret_cast<double *>(c->epart + (size_t)EP_COUNT * c->n); }
 
 template <int TPA, bool SB, bool NS, bool BT>
 static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
@@ -373,7 +389,7 @@ static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   if (grid < 1) grid = 1;
   kern<<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->nlen, c->nbr_stride, c->nbr, c->shift,
                                  c->map, c->fcut, c->ftab_lj, c->ftab_el, c->sp, c->sys_of, fout, c->fxs, c->epart,
-                                 c->stat, c->gate);
+                                 epart_hi(c), c->stat, c->gate);
 }
 
 template <bool SB, bool NS, bool BT>
@@ -443,7 +459,7 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   c->launches += 2;
   if (iflg == 1) {
     k_ereduce<<<dim3(EP_COUNT, c->nsys), c->nsys > 1 ? 256 : 1024, 0, c->st>>>(c->n, mask, c->sp, c->epart,
-                                                                                 c->acc, c->gate);
+                                                                                 epart_hi(c), c->acc, c->gate);
     c->launches++;
   }
   CKL(c);
@@ -480,7 +496,8 @@ int pair_setup(Ctx *c) {
       size_t b = 3 * ((size_t)in * nt + k);
       tl[b] = make_float4((float)d0, (float)da, (float)db, (float)v0);
       tl[b + 1] = make_float4((float)va, (float)vb, (float)s0, (float)sa);
-      tl[b + 2] = make_float4((float)sb, 0.f, 0.f, 0.f);
+      // v0 as hi + lo: the kernel sums the hi parts of the LJ energy in FP64
+      tl[b + 2] = make_float4((float)sb, (float)(v0 - (double)(float)v0), 0.f, 0.f);
     }
   }
   if (c->ncharge > 0) {
@@ -518,7 +535,7 @@ int pair_setup(Ctx *c) {
   CK(cudaMemcpy(c->ftab_el, te.data(), sizeof(float4) * te.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->fcut, fc.data(), sizeof(float) * fc.size(), cudaMemcpyHostToDevice));
   // (the 27 cell shifts H k / nc are set up with the cell grid, list_setup)
-  CK(cudaMalloc(&c->epart, sizeof(float) * EP_COUNT * (size_t)c->n));
+  CK(cudaMalloc(&c->epart, (sizeof(float) * EP_COUNT + sizeof(double)) * (size_t)c->n));
   if (c->tpa == 0) {
     // 8 lanes per atom: a group reads a full 32-byte sector of the list; more
     // lanes only for systems too small to fill the GPU

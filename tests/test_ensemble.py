@@ -1,0 +1,102 @@
+"""The uneven ensemble (many small LJ and charged-binary boxes, one batch)
+against the CPU oracle, box by box.
+
+A slice of the benchmark's ensemble generator (16 boxes, N <= 600) covers
+the small-box paths: boxes narrower than three list radii (one or two cells
+per axis, no FP32 prefilter, minimum image per pair in the pair kernel) next
+to larger ones, charged boxes with Ewald next to LJ-only ones.
+
+Tolerances: pair lists bit-exact; forces relative RMS <= 1e-5; energies
+relative <= 1e-5; virials <= 5e-5 (the mixed engine's stated bounds).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_rms
+from cm3d_b200 import _abi
+from cm3d_b200.engine import Engine
+from tests.golden.make_golden import pair_key
+
+pytestmark = pytest.mark.gpu
+
+ETOL, VTOL, FTOL = 1e-5, 5e-5, 1e-5
+VIRIAL_KEYS = {"winter", "welec", "W", "prsi"}
+
+
+@pytest.fixture(scope="module")
+def boxes():
+    from cm3d_b200 import configs, setup
+    wls = configs.ensemble(16, seed=7, nmax=600)
+    return [setup.build_system(w) for w in wls]
+
+
+def close(a, b, tol, floor=1e-9):
+    return abs(a - b) <= tol * max(abs(b), 1e-300) or abs(a - b) <= floor
+
+
+def test_ensemble_matches_oracle(engine_lib, boxes):
+    """lists, forces and energies at positions the oracle reached after 10
+    steps from the FCC start (at the lattice itself every force is a
+    near-cancelling sum, which no relative error can be measured against)"""
+    from oracle import Oracle
+    pos = []
+    for sm in boxes:
+        o = Oracle(sm, nocell_all=1)
+        o.step_init()
+        o.step(1, 10)
+        pos.append(o.positions())
+    e = Engine(boxes, mode=_abi.MIXED)
+    e.set_positions(np.concatenate(pos, axis=1))
+    e.get_ngbr()
+    e.force(1)
+    e.force(2)
+    f = e.forces(_abi.FXL)
+    en = e.all_energies()
+    lists = {w: e.pair_list(w) for w in (_abi.LIST_T, _abi.LIST_S, _abi.LIST_TE, _abi.LIST_SE)}
+    e.close()
+    small = 0
+    for s, sm in enumerate(boxes):
+        a0, n = e.ranges[s]
+        o = Oracle(sm, nocell_all=1)
+        o.set_positions(pos[s])
+        o.get_ngbr()
+        for w, (i, j) in lists.items():
+            sel = (i >= a0) & (i < a0 + n)
+            oi, oj = o.pair_list(w)
+            got = np.sort(pair_key(i[sel] - a0, j[sel] - a0, n))
+            want = np.sort(pair_key(oi, oj, n))
+            assert got.shape == want.shape and (got == want).all(), (s, w)
+        o.force(1)
+        o.force(2)
+        fo = o.forces(_abi.FXL)
+        scale = float(np.sqrt((fo * fo).mean()))
+        assert rel_rms(f[:, a0:a0 + n], fo, scale) <= FTOL, s
+        eo = o.energies()
+        for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke"):
+            tol = VTOL if k in VIRIAL_KEYS else ETOL
+            assert close(en[s][k], eo[k], tol, floor=1e-6 * max(1.0, abs(eo["U"]))), (s, k, en[s][k], eo[k])
+        L = float(sm["hmat"][0])
+        small += L < 3 * (float(np.sqrt(sm["rmaxl_skin2"].max())))
+    assert small > 0, "the slice should contain boxes narrower than three list radii"
+
+
+def test_ensemble_steps_like_oracle(engine_lib, boxes):
+    """20 steps of the whole slice as one batch (graph) against each box's
+    oracle trajectory: energies within the mixed engine's trajectory bound,
+    same list rebuild and RESETPOS counts"""
+    from oracle import Oracle
+    nsteps = 20
+    e = Engine(boxes, mode=_abi.MIXED)
+    e.step_init()
+    e.step(1, nsteps)
+    en = e.all_energies()
+    rb, rs = e.system_counts()
+    e.close()
+    for s, sm in enumerate(boxes):
+        o = Oracle(sm, nocell_all=1)
+        o.step_init()
+        o.step(1, nsteps)
+        eo = o.energies()
+        for k in ("poter", "zke"):
+            assert close(en[s][k], eo[k], 2e-4, floor=1e-6 * max(1.0, abs(eo["poter"]))), (s, k)
+        assert rb[s] == o.rebuilds and rs[s] == o.resets, (s, rb[s], o.rebuilds, rs[s], o.resets)
