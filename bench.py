@@ -335,6 +335,7 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
     eng = Engine(systems, mode=_abi.MIXED, device=device)
     eng.workload_name = name
     eng.step_init()
+    tune = eng.autotune()
     n = eng.n
     if dist:
         dist.barrier()
@@ -362,7 +363,7 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
     eng.close()
     return {"ms": ms, "launches": launches, "per_step_ms": per, "n": n, "status": status,
             "e2e": (dt_e2e, h2d, d2h, e2e_steps), "roofline": roof, "energies": en,
-            "clocks": clk.summary()}
+            "clocks": clk.summary(), "autotune": tune}
 
 
 # ------------------------------------------------------------------- main
@@ -375,6 +376,7 @@ def main() -> None:
     ap.add_argument("--workload", default="ensemble1024")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -449,10 +451,11 @@ def main() -> None:
             "ns_per_day": (500 / (wm["ms"] / 1e3)) * float(wsys[0]["dt"]) * 86400.0 / 1e3,
             "plain_fp64": wplain,
             "speedup_mixed_vs_plain": (wval / wplain["value"]) if wplain else None,
-            "roofline": wm["roofline"], "status": {k: wm["status"][k] for k in ("rebuilds", "resets")}}
+            "roofline": wm["roofline"], "autotune": wm["autotune"],
+            "status": {k: wm["status"][k] for k in ("rebuilds", "resets")}}
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         cpu = (cpu_reference(wls, max(1, min(os.cpu_count() or 1, 64))) if ref_bench_bin()
                else cpu_port(systems, 20))
 
@@ -476,6 +479,7 @@ def main() -> None:
                         "p99": float(np.percentile(per, 99))},
             "gpu_launches": m["launches"],
             "roofline": m["roofline"],
+            "autotune": m["autotune"],
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": e2e_steps},

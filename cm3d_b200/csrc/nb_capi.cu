@@ -309,11 +309,13 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
     }
     H.rlist = sqrt(r2);
     // boxes narrower than two list radii need the on-the-fly minimum image
+    // (for the pairs near the image boundary, see near_s)
     P.smallbox = 0;
     for (int d = 0; d < 3; d++) {
       double w = 1.0 / sqrt(H.hmati[3 * d] * H.hmati[3 * d] + H.hmati[3 * d + 1] * H.hmati[3 * d + 1] +
                             H.hmati[3 * d + 2] * H.hmati[3 * d + 2]);
       if (w < 2.0 * H.rlist) P.smallbox = 1;
+      P.near_s[d] = 0.5 - 1.01 * s->skin_ter / w - 1e-6;
     }
     a0 += ns;
   }
@@ -992,6 +994,59 @@ int cm3d_nb_kernel_time(cm3d_nb_ctx *ctx, int cls, double *ms, long long *launch
 long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx) {
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   return c ? c->launches : 0;
+}
+
+int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]) {
+  CTX;
+  int rc;
+  if (c->mode != CM3D_NB_MIXED) {
+    set_error("autotune: the plain FP64 engine has nothing to tune");
+    return CM3D_NB_ERR_ARG;
+  }
+  if (!c->lists_built) {
+    set_error("autotune before get_ngbr()/step_init(): it times the live lists");
+    return CM3D_NB_ERR_STATE;
+  }
+  if (reps < 1) reps = 5;
+  const int cand[4] = {4, 8, 16, 32};
+  double best = 1e300;
+  int best_tpa = c->tpa;
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  const bool timing = c->timing.on;
+  c->timing.on = false;
+  for (int k = 0; k < 4; k++) {
+    c->tpa = cand[k];
+    if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
+    CK(cudaEventRecord(a, c->st));
+    for (int r = 0; r < reps; r++)
+      if ((rc = pair_forces(c, 1, 3))) return rc;
+    CK(cudaEventRecord(b, c->st));
+    CK(cudaEventSynchronize(b));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    const double per = ms / reps;
+    if (ms_per_launch) ms_per_launch[k] = per;
+    if (per < best) {
+      best = per;
+      best_tpa = cand[k];
+    }
+  }
+  c->timing.on = timing;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  c->tpa = best_tpa;
+  if (tpa_chosen) *tpa_chosen = best_tpa;
+  // a captured step holds the old launch configuration; the timing launches
+  // added to the force blocks and accumulators: recompute force(1)
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  if ((rc = run_force(c, 1))) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return CM3D_NB_OK;
 }
 
 int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops) {

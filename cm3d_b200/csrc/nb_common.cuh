@@ -69,6 +69,8 @@ struct SysP {
   double h[9], hi[9];
   double rmaxl_skin2_e, rmaxs_skin2_e;   // -1 without charges
   double skin2q;             // (skin / 2)^2
+  double near_s[3];          // small boxes: |fractional displacement| above which a listed pair
+                             // may change its nearest image before the next rebuild
   double falp2, rvol, kappa, kappa2;
   float4 shift[27];          // cell-corner shifts H k / nc, k in {-1, 0, 1}^3 (FP32 hi part)
   float4 shift_lo[27];       // their FP32 residuals (shift + shift_lo = the FP64 shift)
@@ -139,6 +141,7 @@ constexpr uint32_t ENT_LJ = 1u << 27;       // pair is in CM3D's t list
 constexpr uint32_t ENT_EL = 1u << 28;       // pair is in CM3D's te list
 constexpr uint32_t ENT_LJS = 1u << 29;      // pair is in CM3D's s list
 constexpr uint32_t ENT_ELS = 1u << 30;      // pair is in CM3D's se list
+constexpr uint32_t ENT_NEAR = 1u << 31;     // small box: the pair may change image, check it
 constexpr int MAX_ATOMS_MIXED = 1 << ENT_JBITS;
 
 // classes 0 pair, 1 k-space, 2 list build, 3 integrate (per kernel, eager

@@ -228,6 +228,10 @@ __device__ __forceinline__ int exact_flags(const SysP &P, int n, int i, int j, i
     if (r2 < P.rmaxs_skin2_e) flags |= 8;
   }
   if (!flags) return 0;
+  // small boxes: the atoms may move skin/2 each before the next rebuild, so a
+  // pair whose fractional displacement is within skin / plane spacing of 1/2
+  // may change its nearest image; the pair kernel checks those pairs
+  if (P.smallbox && (fabs(sx) > P.near_s[0] || fabs(sy) > P.near_s[1] || fabs(sz) > P.near_s[2])) flags |= 32;
   // shift code: k = (n_i - n_j - m) nc + (c_i - c_j) per dimension; |k| <= 1
   // whenever r < rlist <= cell width.  Anything else means the geometry
   // assumption broke: flag it and use the zero shift rather than index past
@@ -440,6 +444,7 @@ __global__ void __launch_bounds__(256) k_list_full(
       if (fl & 2) e |= ENT_LJS;
       if (fl & 4) e |= ENT_EL;
       if (fl & 8) e |= ENT_ELS;
+      if (fl & 32) e |= ENT_NEAR;
       if (slot < stride) out[slot] = e;
     }
     count += __popc(bf);

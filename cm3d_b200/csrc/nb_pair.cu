@@ -74,7 +74,7 @@ __device__ __forceinline__ void min_image(const Box &B, float &dx, float &dy, fl
 // several systems; each atom group reads its system's parameters, shifts and
 // tables (global interaction / Coulomb-table indices) from sp[sys_of[t]].
 template <int TPA, bool SMALLBOX, bool NEED_S, bool BATCH>
-__global__ void __launch_bounds__(256) k_pair_mixed(
+__global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
     MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ nlen, int stride, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
@@ -147,9 +147,9 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
         float dy = ((xi.y - xj.y) + sh.y) + shl.y;
         float dz = ((xi.z - xj.z) + sh.z) + shl.z;
         if (BATCH) {
-          if (sb) min_image(*Sp, dx, dy, dz);
+          if (sb && (en & ENT_NEAR)) min_image(*Sp, dx, dy, dz);
         } else if (SMALLBOX) {
-          min_image(P, dx, dy, dz);
+          if (en & ENT_NEAR) min_image(P, dx, dy, dz);
         }
         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
         float ftot = 0.f, fsh = 0.f;
@@ -182,10 +182,13 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
         }
         if ((en & fl_lj) && (P.mask & 1)) {
           const int in = mapp[ti * ntyp + tj];
-          const float *fc = fcp + 8 * in;
-          const float rmax2 = P.iflg == 1 ? fc[0] : fc[4];
+          // {rmaxl_cut2, rmins_cut2 dx2tab, dx2tab, vt} {rminl_cut2, rmaxs_cut2, -, -}
+          const float4 cA = reinterpret_cast<const float4 *>(fcp)[2 * in];
+          const bool needB = P.iflg == 0 || NEED_S;
+          const float4 cB = needB ? reinterpret_cast<const float4 *>(fcp)[2 * in + 1] : cA;
+          const float rmax2 = P.iflg == 1 ? cA.x : cB.y;
           if (r2 < rmax2) {
-            float p = fmaf(r2, fc[2], -fc[1]);
+            float p = fmaf(r2, cA.z, -cA.y);
             int kk = (int)p;
             if (kk < 1) {
               under++;
@@ -197,7 +200,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
             const float4 a0 = T[0], a1 = T[1], a2 = T[2];
             const float f = poly(p, a0.x, a0.y, a0.z);
             float swv = 1.f;
-            if ((NEED_S || P.iflg == 0) && r2 > fc[3]) swv = poly(p, a1.z, a1.w, a2.x);
+            if (needB && r2 > cB.x) swv = poly(p, a1.z, a1.w, a2.x);
             if (P.iflg == 1) {
               ftot += f;
               // V = v0 + p (vA + p vB) with v0 = hi (a0.w) + lo (a2.y): the
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(256) k_pair_mixed(
               elj_hi += (double)a0.w;
               const float vlo = a2.y + p * fmaf(p, a1.y, a1.x);
               e[EP_ELJ] += vlo;
-              e[EP_ELJH] += vlo - fc[5];
+              e[EP_ELJH] += vlo - cA.w;
               const float fdx = f * dx, fdy = f * dy, fdz = f * dz;
               e[EP_VL0] = fmaf(fdx, dx, e[EP_VL0]);
               e[EP_VL1] = fmaf(fdx, dy, e[EP_VL1]);
@@ -516,17 +519,17 @@ int pair_setup(Ctx *c) {
         te[(size_t)2 * nt * tb + 2 * k + 1] = make_float4((float)va, (float)vb, 0.f, 0.f);
       }
   }
-  // per interaction: rmaxl_cut2, rmins_cut2*dx2tab, dx2tab, rminl_cut2,
-  // rmaxs_cut2, vtab[ntable-4]
+  // per interaction, two float4: {rmaxl_cut2, rmins_cut2*dx2tab, dx2tab,
+  // vtab[ntable-4]} {rminl_cut2, rmaxs_cut2, -, -}
   std::vector<float> fc(8 * (size_t)(ni > 0 ? ni : 1), 0.f);
   for (int in = 0; in < ni; in++) {
     const double *q = &cut[8 * (size_t)in];
     fc[8 * in + 0] = (float)q[2];
     fc[8 * in + 1] = (float)(q[1] * q[6]);
     fc[8 * in + 2] = (float)q[6];
-    fc[8 * in + 3] = (float)q[3];
-    fc[8 * in + 4] = (float)q[0];
-    fc[8 * in + 5] = (float)q[7];
+    fc[8 * in + 3] = (float)q[7];
+    fc[8 * in + 4] = (float)q[3];
+    fc[8 * in + 5] = (float)q[0];
   }
   CK(cudaMalloc(&c->ftab_lj, sizeof(float4) * (tl.size() > 0 ? tl.size() : 1)));
   CK(cudaMalloc(&c->ftab_el, sizeof(float4) * te.size()));

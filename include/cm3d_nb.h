@@ -270,6 +270,13 @@ long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx);
    (TFLOP/s, an FMA counted as 2 flops): the roofline denominators of the
    CUDA-core pair and k-space kernels.  No CM3D counterpart. */
 int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops);
+/* Autotuner of the mixed pair kernel (no CM3D counterpart): times the fused
+   LJ + real-space Ewald kernel with 4, 8, 16 and 32 lanes per atom on the
+   context's current lists (reps launches each, CUDA events), keeps the
+   fastest, and recomputes force(1) so the state is as before.  Call after
+   cm3d_nb_get_ngbr or cm3d_nb_step_init.  ms_per_launch[4] (may be NULL)
+   receives the four timings. */
+int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]);
 
 /* ------------------------------------------- no-allocation variant */
 #define CM3D_NB_NOALLOC_MAX_CHARGES 32768   /* charged atoms per call */

@@ -1,0 +1,35 @@
+"""The pair-kernel autotuner (cm3d_nb_autotune): it picks one of the
+candidate lane counts, leaves forces and energies as they were (the lane
+count only reorders FP32 partial sums: relative 1e-6), and a trajectory
+continues after it exactly as the mixed engine's bound requires."""
+import numpy as np
+import pytest
+
+from conftest import force_scale, golden, rel_rms
+from cm3d_b200 import _abi
+from cm3d_b200.engine import Engine
+from cm3d_b200.system import System
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("names", [["water216"], ["argon864", "binary256"]], ids=["single", "batch"])
+def test_autotune_keeps_state(engine_lib, names):
+    ds = [golden(n) for n in names]
+    e = Engine([System.from_arrays(d) for d in ds], mode=_abi.MIXED)
+    e.step_init()
+    f0 = e.forces(_abi.FXL)
+    en0 = e.all_energies()
+    res = e.autotune(reps=3)
+    assert res["tpa"] in (4, 8, 16, 32)
+    assert all(v > 0 for v in res["ms_per_launch"].values())
+    f1 = e.forces(_abi.FXL)
+    en1 = e.all_energies()
+    fs = max(force_scale(d) / float(np.sqrt((d["amass"] ** 2).mean())) for d in ds)
+    assert rel_rms(f1, f0, fs) <= 1e-6
+    for a, b in zip(en0, en1):
+        for k in ("vinter", "velec", "vewald", "U", "W", "zke"):
+            assert abs(a[k] - b[k]) <= 1e-6 * max(abs(b[k]), 1.0), k
+    e.step(1, 5)                      # the step graph is recaptured with the new lane count
+    assert np.isfinite(e.positions()).all()
+    e.close()
