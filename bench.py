@@ -20,6 +20,9 @@ Printed: one JSON line (rank 0) with the contract's keys plus
   e2e             the same metric through the public API with host buffers
   latency         per-step device time p50 / p99
   other_workloads the water-12288 box, mixed and plain, in the same run
+  serving         the serving loop on a Poisson stream of water-box jobs
+                  (4 jobs/s over 5 s): job latency p50/p95/p99 and aggregate
+                  atom-steps/s, mixed against plain FP64 on the same jobs
 Under torchrun (N > 1) every rank runs its own ensemble (seed + rank): the
 systems are independent and no collective touches the step path.
 """
@@ -366,6 +369,33 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
             "clocks": clk.summary(), "autotune": tune}
 
 
+def serving_arm(rate: float, window: float, device: int, plain: bool) -> dict:
+    """The serving loop (cm3d_b200.serving) on a Poisson stream of water-box
+    jobs (configs.serving_plan: molecules log-uniform in [256, 16384], steps
+    U[500, 5000], RESPA 0.5/2 fs), mixed engine and -- on the same jobs --
+    the plain FP64 engine, one job per context and per launch."""
+    from cm3d_b200 import _abi, configs, setup
+    from cm3d_b200.serving import Job, Server, summarize
+    plan = configs.serving_plan(rate, window)
+    systems = [setup.build_system(configs.serving_workload(r)) for r in plan]
+    out = {"rate_jobs_per_s": rate, "arrival_window_s": window, "hbm_budget_gb": 150.0,
+           "jobs": len(plan), "natoms_total": int(sum(sm.natoms for sm in systems))}
+    for key, mode in (("mixed", _abi.MIXED), ("plain_fp64", _abi.PLAIN_FP64)):
+        if key == "plain_fp64" and not plain:
+            continue
+        srv = Server(device=device, mode=mode, chunk=100)
+        for r, sm in zip(plan, systems):
+            srv.submit(Job(r.index, sm, r.nsteps, arrival=r.arrival))
+        t0 = time.perf_counter()
+        done = srv.run()
+        res = summarize(done, time.perf_counter() - t0)
+        res["max_concurrent"] = srv.max_active
+        out[key] = res
+    if plain:
+        out["speedup_mixed_vs_plain"] = out["mixed"]["atom_steps_per_s"] / out["plain_fp64"]["atom_steps_per_s"]
+    return out
+
+
 # ------------------------------------------------------------------- main
 def main() -> None:
     ap = argparse.ArgumentParser()
@@ -377,6 +407,8 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--serving-sweep", action="store_true",
+                    help="serving at 0.5, 1, 2, 4, 8 jobs/s over 120 s windows (long)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -454,6 +486,13 @@ def main() -> None:
             "roofline": wm["roofline"], "autotune": wm["autotune"],
             "status": {k: wm["status"][k] for k in ("rebuilds", "resets")}}
 
+    serving = None
+    if not args.no_extra and world == 1:
+        if args.serving_sweep:
+            serving = [serving_arm(r, 120.0, local, not args.no_plain) for r in (0.5, 1.0, 2.0, 4.0, 8.0)]
+        else:
+            serving = serving_arm(4.0, 5.0, local, not args.no_plain)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = (cpu_reference(wls, max(1, min(os.cpu_count() or 1, 64))) if ref_bench_bin()
@@ -485,6 +524,7 @@ def main() -> None:
                     "steps": e2e_steps},
             "plain_fp64": plain,
             "other_workloads": other,
+            "serving": serving,
             "peaks": {"fp32_tflops": fp32, "fp64_tflops": fp64, "hbm_gbs": hbm},
             "clocks": m["clocks"],
             "status": {k: m["status"][k] for k in ("rebuilds", "resets", "overflows", "table_underflow")},

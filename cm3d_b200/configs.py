@@ -265,20 +265,26 @@ def water_box(ngrid: int = 16, temp: float = 300.0, seed: int = 1,
 
     every = np.argwhere(np.ones((ngrid, ngrid, ngrid), dtype=bool))
     bad = clashes(every).reshape(ngrid, ngrid, ngrid)
-    if placement == "octant" and ngrid % 2 == 0:
-        # Neighbours differ in the parity of at least one coordinate, so the
-        # molecules of one parity class (x, y, z mod 2) can be re-drawn
-        # together against fixed neighbours; each class is re-drawn until it
-        # is clear, then the next, for a few rounds.
+    if placement == "octant":
+        # Grid neighbours differ in the class of at least one coordinate --
+        # its parity, with the last layer of an odd grid a class of its own
+        # (it touches layer 0 through the periodic boundary) -- so the
+        # molecules of one class can be re-drawn together against fixed
+        # neighbours; each class is re-drawn until it is clear, then the
+        # next, for a few rounds.
+        nv = 2 if ngrid % 2 == 0 else 3
+        coord_cls = np.arange(ngrid) % 2
+        if nv == 3:
+            coord_cls[ngrid - 1] = 2
         for _round in range(20):
             if not bad.any():
                 break
-            for cls in range(8):
-                par = np.array([(cls >> 2) & 1, (cls >> 1) & 1, cls & 1])
+            for cls in range(nv ** 3):
+                par = np.array([cls // (nv * nv), (cls // nv) % nv, cls % nv])
                 moved = []
                 for _try in range(50):
                     idx = np.argwhere(bad)
-                    sel = idx[(idx % 2 == par).all(axis=1)]
+                    sel = idx[(coord_cls[idx] == par).all(axis=1)]
                     if sel.shape[0] == 0:
                         break
                     redraw(sel)
@@ -476,3 +482,42 @@ def ensemble(nsys: int = 1024, seed: int = 2024, ntime: int = 2000, **kw) -> lis
     return [lj_box(m.natoms, m.density, m.tstar, m.seed, charged=m.charged, ntime=ntime,
                    name=f"box{m.index:04d}")
             for m in ensemble_plan(nsys, seed, **kw)]
+
+
+# ------------------------------------------------------ serving job stream
+@dataclass
+class ServingRequest:
+    """One water-box MD request of the serving workload."""
+    index: int
+    arrival: float          # seconds
+    ngrid: int              # ngrid^3 molecules
+    nsteps: int
+    seed: int
+
+
+def serving_plan(rate: float, duration: float, seed: int = 11, mol_min: int = 256, mol_max: int = 16384,
+                 steps_min: int = 500, steps_max: int = 5000) -> list[ServingRequest]:
+    """Poisson arrivals at `rate` jobs/s over `duration` s; molecule count
+    log-uniform in [mol_min, mol_max] (rounded to a cubic grid), step count
+    uniform in [steps_min, steps_max]."""
+    rng = np.random.default_rng(seed)
+    out, t = [], 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t > duration:
+            break
+        nmol = math.exp(rng.uniform(math.log(mol_min), math.log(mol_max)))
+        ngrid = max(2, int(round(nmol ** (1.0 / 3.0))))
+        out.append(ServingRequest(len(out), t, ngrid, int(rng.integers(steps_min, steps_max + 1)),
+                                  int(rng.integers(1, 2 ** 31 - 1))))
+    return out
+
+
+def serving_workload(req: ServingRequest) -> Workload:
+    """The water box of a request: 1.0 g/cm^3, rc = min(10 A, 0.45 L),
+    Ewald alpha = 3.1 / rc, kmax = ceil(7 L / 49.66), RESPA 0.5/2 fs."""
+    L = req.ngrid * WATER_SPACING
+    rc = min(10.0, 0.45 * L)
+    return water_box(ngrid=req.ngrid, seed=req.seed, rc=rc, alpha=3.1 / rc,
+                     kmax=int(math.ceil(7.0 * L / 49.66)), ntime=req.nsteps, placement="octant",
+                     name=f"job{req.index:04d}")

@@ -86,7 +86,7 @@ static void destroy(Ctx *c) {
                   c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
                   c->cimg, c->nlen, c->acc,
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
-                  c->ktile_sys, c->ftile_sys, c->k_sys};
+                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -101,6 +101,7 @@ static void destroy(Ctx *c) {
     cudaEventDestroy(pr.first);
     cudaEventDestroy(pr.second);
   }
+  if (c->step_ev) cudaEventDestroy(c->step_ev);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -539,6 +540,7 @@ int cm3d_nb_create_batch(const cm3d_nb_system *systems, int nsys, const cm3d_nb_
 
 void cm3d_nb_destroy(cm3d_nb_ctx *ctx) { destroy(reinterpret_cast<Ctx *>(ctx)); }
 
+// every entry point first finishes asynchronously launched steps
 #define CTX                                         \
   Ctx *c = reinterpret_cast<Ctx *>(ctx);            \
   if (!c) {                                         \
@@ -548,6 +550,10 @@ void cm3d_nb_destroy(cm3d_nb_ctx *ctx) { destroy(reinterpret_cast<Ctx *>(ctx)); 
   do {                                              \
     cudaError_t _e = cudaSetDevice(c->dev);         \
     if (_e != cudaSuccess) return cuda_fail(_e, "cudaSetDevice"); \
+    if (c->pending) {                               \
+      int _rc = finish_steps(c);                    \
+      if (_rc) return _rc;                          \
+    }                                               \
   } while (0)
 
 static int put3(Ctx *c, double *dst, const double *x, const double *y, const double *z) {
@@ -793,6 +799,31 @@ int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
     return CM3D_NB_ERR_ARG;
   }
   return run_step(c, istep0, nsteps);
+}
+
+int cm3d_nb_step_async(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
+  CTX;
+  if (c->name == "has-torsions") {
+    set_error("step(): torsions, 1-4 terms and cross bonds are not part of the engine");
+    return CM3D_NB_ERR_ARG;
+  }
+  return launch_steps(c, istep0, nsteps);
+}
+
+int cm3d_nb_step_query(cm3d_nb_ctx *ctx, int *done) {
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c || !done) {
+    set_error("step_query: null argument");
+    return CM3D_NB_ERR_ARG;
+  }
+  cudaError_t e = cudaSetDevice(c->dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  return query_steps(c, done);
+}
+
+int cm3d_nb_step_wait(cm3d_nb_ctx *ctx) {
+  CTX;   // finishes the pending steps
+  return CM3D_NB_OK;
 }
 
 // getvireal(...,1)+geteng() of system `sy` from the pulled accumulators

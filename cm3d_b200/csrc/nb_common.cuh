@@ -234,6 +234,7 @@ struct Ctx {
   int *ka_d = nullptr, *kb_d = nullptr, *kc_d = nullptr;
   int ks_tiles = 0, ks_tile_atoms = 0, kf_split = 1;
   size_t kf_smem = 0;
+  double *kf_part = nullptr;            // per row split partial reciprocal forces (mixed, split > 1)
   int2 *ecorr_pairs = nullptr;          // CM3D's iecorr/jecorr order
   // ---- bonded groups (connected components of bonds/bends/ecorr)
   int ngroups = 0;
@@ -283,6 +284,9 @@ struct Ctx {
   cudaGraphExec_t graph = nullptr;
   long long graph_launches = 0;
   const int *gate = nullptr;            // istate while a step is being captured
+  cudaEvent_t step_ev = nullptr;        // end of asynchronously launched steps
+  bool pending = false;                 // steps launched and not finished yet
+  int pend_istep0 = 0, pend_nsteps = 0;
   std::string name;
 };
 
@@ -385,6 +389,9 @@ int kspace_forces(Ctx *c);                      // nb_kspace.cu
 int kspace_setup(Ctx *c);                       // nb_kspace.cu
 int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys);   // nb_step.cu
 int run_step(Ctx *c, int istep0, int nsteps);   // nb_step.cu
+int launch_steps(Ctx *c, int istep0, int nsteps);   // nb_step.cu
+int finish_steps(Ctx *c);                       // nb_step.cu
+int query_steps(Ctx *c, int *done);             // nb_step.cu
 int run_force(Ctx *c, int iflg);                // nb_step.cu
 int run_bonded(Ctx *c);                         // nb_step.cu
 int group_init(Ctx *c, bool zero_fxs);          // nb_step.cu

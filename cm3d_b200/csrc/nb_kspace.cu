@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
                                                              const int *__restrict__ row_k0, int rows_per_split,
                                                              const float2 *__restrict__ akf, int ktot,
                                                              const double *__restrict__ hmati_one, int atomic,
-                                                             double *__restrict__ fxl,
+                                                             double *__restrict__ fxl, double *__restrict__ part,
                                                              const SysP *__restrict__ sp,
                                                              const int *__restrict__ tile_sys,
                                                              const int *__restrict__ gs) {
@@ -240,7 +240,18 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
     abase = blockIdx.x * (blockDim.x * KF_A);
     aend = nq;
   }
-  if (r0 >= r1) return;
+  if (r0 >= r1) {
+    // no rows for this split: its share of the partial forces is zero
+    if (part)
+      for (int m = 0; m < KF_A; m++) {
+        const int jq = abase + m * blockDim.x + threadIdx.x;
+        if (jq < aend) {
+          const size_t o = ((size_t)blockIdx.y * nq + jq) * 3;
+          part[o] = part[o + 1] = part[o + 2] = 0.0;
+        }
+      }
+    return;
+  }
   const int kbase = row_k0[r0];
   for (int k = threadIdx.x; k < kend - kbase; k += blockDim.x) ak_s[k] = akf[kbase + k];
   __syncthreads();
@@ -305,7 +316,13 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
     double fx = t * (hmati[0] * U0[m] + hmati[3] * U1[m] + hmati[6] * U2[m]);
     double fy = t * (hmati[1] * U0[m] + hmati[4] * U1[m] + hmati[7] * U2[m]);
     double fz = t * (hmati[2] * U0[m] + hmati[5] * U1[m] + hmati[8] * U2[m]);
-    if (atomic) {
+    if (part) {
+      // one partial per row split, summed in a fixed order by k_kforce_sum
+      const size_t o = ((size_t)blockIdx.y * nq + jq[m]) * 3;
+      part[o] = fx;
+      part[o + 1] = fy;
+      part[o + 2] = fz;
+    } else if (atomic) {
       atomicAdd(fxl + i, fx);
       atomicAdd(fxl + n + i, fy);
       atomicAdd(fxl + 2 * n + i, fz);
@@ -315,6 +332,26 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
       fxl[2 * n + i] += fz;
     }
   }
+}
+
+// the row splits' partial reciprocal forces of every charged atom, summed in
+// split order (deterministic: the same result whatever else the device runs)
+__global__ void k_kforce_sum(int nq, int nsplit, const double *__restrict__ part, const int *__restrict__ icharge,
+                             int n, double *__restrict__ fxl, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  const int jq = blockIdx.x * blockDim.x + threadIdx.x;
+  if (jq >= nq) return;
+  double fx = 0, fy = 0, fz = 0;
+  for (int y = 0; y < nsplit; y++) {
+    const size_t o = ((size_t)y * nq + jq) * 3;
+    fx += part[o];
+    fy += part[o + 1];
+    fz += part[o + 2];
+  }
+  const int i = icharge[jq];
+  fxl[i] += fx;
+  fxl[n + i] += fy;
+  fxl[2 * n + i] += fz;
 }
 
 // ------------------------------------------------------------ plain FP64
@@ -521,6 +558,11 @@ int kspace_setup(Ctx *c) {
   }
   if (split > nrows_max) split = nrows_max;
   c->kf_split = split;
+  if (mixed && split > 1) {
+    // zeroed once: the charged atoms of systems without k-vectors keep zero partials
+    CK(cudaMalloc(&c->kf_part, sizeof(double) * 3 * (size_t)split * c->ncharge));
+    CK(cudaMemset(c->kf_part, 0, sizeof(double) * 3 * (size_t)split * c->ncharge));
+  }
   return CM3D_NB_OK;
 }
 
@@ -551,10 +593,16 @@ static int kspace_forces_batch(Ctx *c) {
                                                            c->k_sys, c->gate);
   kforce_attr(c->dev);
   dim3 gf(c->ftiles_tot, c->kf_split);
+  double *part = c->kf_split > 1 ? c->kf_part : nullptr;
   k_kforce_mixed<true><<<gf, KS_THREADS, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0, c->rows,
-                                                               c->row_k0, 0, c->akf, 0, nullptr, c->kf_split > 1,
-                                                               c->fxl, c->sp, c->ftile_sys, c->gate);
+                                                               c->row_k0, 0, c->akf, 0, nullptr, 0, c->fxl, part,
+                                                               c->sp, c->ftile_sys, c->gate);
   c->launches += 4;
+  if (part) {
+    k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->kf_split, part, c->icharge, c->n,
+                                                                c->fxl, c->gate);
+    c->launches++;
+  }
   tend(c, 1, e0);
   CKL(c);
   return CM3D_NB_OK;
@@ -598,7 +646,13 @@ int kspace_forces(Ctx *c) {
     kforce_attr(c->dev);
     k_kforce_mixed<false><<<gf, KS_THREADS, smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows,
                                                             c->rows, c->row_k0, rps, c->akf, c->ktot, dhmati,
-                                                            split > 1, c->fxl, nullptr, nullptr, c->gate);
+                                                            0, c->fxl, split > 1 ? c->kf_part : nullptr, nullptr,
+                                                            nullptr, c->gate);
+    if (split > 1) {
+      k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, split, c->kf_part, c->icharge,
+                                                                  c->n, c->fxl, c->gate);
+      c->launches++;
+    }
   } else {
     dim3 gf((c->ncharge + 255) / 256, split);
     k_kforce_plain<<<gf, 256, 0, c->st>>>(c->ncharge, c->kposd, c->icharge, c->n, c->nrows, c->rows, c->row_k0,
@@ -879,7 +933,8 @@ static int fk_ewald_noalloc(int device, cudaStream_t st, int natoms, const doubl
     }
     dim3 gf(tiles, split);
     k_kforce_mixed<false><<<gf, KS_THREADS, smem, st>>>(ncharge, kfrac, icharge, natoms, nrows, rows, row_k0, rps,
-                                                        akf, ktot, dhmati, split > 1, fxl, nullptr, nullptr, nullptr);
+                                                        akf, ktot, dhmati, split > 1, fxl, nullptr, nullptr, nullptr,
+                                                        nullptr);
   }
   const double six = ncharge > 0 ? ewald_bkg / vol : 0.0;
   k_na_finish<<<1, 32, 0, st>>>(acc, six, ncharge > 0 ? ewald_self : 0.0, out);

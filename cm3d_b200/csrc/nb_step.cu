@@ -638,10 +638,18 @@ static int set_istep(Ctx *c, int istep) {
   return CM3D_NB_OK;
 }
 
-int run_step(Ctx *c, int istep0, int nsteps) {
+// Launch `nsteps` outer steps from istep0.  Graph mode: the captured step is
+// replayed nsteps times on the context's stream, the device state is copied
+// back asynchronously and an event marks the end; nothing waits (finish_steps
+// completes the call).  Eager mode runs the steps to completion here.
+int launch_steps(Ctx *c, int istep0, int nsteps) {
   int rc;
   if (!c->lists_built || !c->forces_valid) {
     set_error("step() before step_init(): forces and lists are not set up");
+    return CM3D_NB_ERR_STATE;
+  }
+  if (c->pending) {
+    set_error("step: the previous asynchronous steps have not been finished (cm3d_nb_step_wait)");
     return CM3D_NB_ERR_STATE;
   }
   if (nsteps <= 0) return CM3D_NB_OK;
@@ -678,11 +686,25 @@ int run_step(Ctx *c, int istep0, int nsteps) {
   }
   tend(c, 4, e4);
   CK(cudaMemcpyAsync(c->h_istate, c->istate, sizeof(int) * IS_COUNT, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  if (!c->step_ev) CK(cudaEventCreateWithFlags(&c->step_ev, cudaEventDisableTiming));
+  CK(cudaEventRecord(c->step_ev, c->st));
+  c->pending = true;
+  c->pend_istep0 = istep0;
+  c->pend_nsteps = nsteps;
+  return CM3D_NB_OK;
+}
+
+// Wait for launched steps (if any) and check the device state: a device-side
+// rebuild that outgrew a list halted its step -- that step stopped right
+// after its list build and every later kernel did nothing.  Grow the
+// buffers, finish the step on the host-driven path and run the rest.
+int finish_steps(Ctx *c) {
+  int rc;
+  if (!c->pending) return CM3D_NB_OK;
+  CK(cudaEventSynchronize(c->step_ev));
+  c->pending = false;
   if (!c->h_istate[IS_HALT]) return CM3D_NB_OK;
-  // A device-side rebuild outgrew a list: that step stopped right after its
-  // list count and every later kernel did nothing.  Grow the buffers, finish
-  // the step on the host-driven path and run the remaining steps.
+  const int istep0 = c->pend_istep0, nsteps = c->pend_nsteps;
   c->overflows_host++;
   const int failed = c->h_istate[IS_ISTEP], intr = c->h_istate[IS_INTR];
   CK(cudaMemsetAsync(c->istate + IS_HALT, 0, sizeof(int), c->st));
@@ -695,6 +717,26 @@ int run_step(Ctx *c, int istep0, int nsteps) {
   int done = failed + 1 - istep0;
   if (done < nsteps) return run_step(c, failed + 1, nsteps - done);
   return CM3D_NB_OK;
+}
+
+// step() nsteps times: launch and finish
+int run_step(Ctx *c, int istep0, int nsteps) {
+  int rc;
+  if ((rc = launch_steps(c, istep0, nsteps))) return rc;
+  return finish_steps(c);
+}
+
+// non-blocking completion test of launched steps (finishes them when done)
+int query_steps(Ctx *c, int *done) {
+  *done = 1;
+  if (!c->pending) return CM3D_NB_OK;
+  cudaError_t e = cudaEventQuery(c->step_ev);
+  if (e == cudaErrorNotReady) {
+    *done = 0;
+    return CM3D_NB_OK;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
+  return finish_steps(c);
 }
 
 }  // namespace cm3d

@@ -85,6 +85,9 @@ def load_library() -> C.CDLL:
         "cm3d_nb_getvewald": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_step_init": (C.c_int, [vp]),
         "cm3d_nb_step": (C.c_int, [vp, C.c_int, C.c_int]),
+        "cm3d_nb_step_async": (C.c_int, [vp, C.c_int, C.c_int]),
+        "cm3d_nb_step_query": (C.c_int, [vp, ip]),
+        "cm3d_nb_step_wait": (C.c_int, [vp]),
         "cm3d_nb_get_energies": (C.c_int, [vp, C.POINTER(_abi.Energies)]),
         "cm3d_nb_list_count": (C.c_int, [vp, C.c_int, C.POINTER(ll)]),
         "cm3d_nb_get_list": (C.c_int, [vp, C.c_int, ip, ip, ll, C.POINTER(ll)]),
@@ -293,6 +296,19 @@ class Engine:
 
     def step(self, istep0: int, nsteps: int = 1) -> None:
         check(load_library().cm3d_nb_step(self._h, istep0, nsteps), "step")
+
+    def step_async(self, istep0: int, nsteps: int = 1) -> None:
+        """launch the steps and return (cm3d_nb_step_async)"""
+        check(load_library().cm3d_nb_step_async(self._h, istep0, nsteps), "step_async")
+
+    def step_done(self) -> bool:
+        """non-blocking: have the launched steps completed?"""
+        d = C.c_int(0)
+        check(load_library().cm3d_nb_step_query(self._h, C.byref(d)), "step_query")
+        return bool(d.value)
+
+    def step_wait(self) -> None:
+        check(load_library().cm3d_nb_step_wait(self._h), "step_wait")
 
     def energies(self) -> dict:
         e = _abi.Energies()

@@ -242,6 +242,15 @@ int cm3d_nb_step_init(cm3d_nb_ctx *ctx);
                      SIMPARMS.istep = istep0 (NVE; torsions, thermostats and
                      barostats are not part of the engine). */
 int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps);
+/* The same steps without waiting (no CM3D counterpart): cm3d_nb_step_async
+   launches them on the context's stream and returns, so that several
+   contexts' steps overlap on the device; cm3d_nb_step_query reports (*done)
+   whether they have completed, without blocking; cm3d_nb_step_wait blocks
+   until they have.  Every other call on the context first waits for them.
+   (Graph mode; with use_graph = 0 the steps run to completion at once.) */
+int cm3d_nb_step_async(cm3d_nb_ctx *ctx, int istep0, int nsteps);
+int cm3d_nb_step_query(cm3d_nb_ctx *ctx, int *done);
+int cm3d_nb_step_wait(cm3d_nb_ctx *ctx);
 /* getvireal(...,1)+geteng() md_fcntr.c:136,259 from the device accumulators */
 int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e);
 
