@@ -407,6 +407,9 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--partition", action="store_true",
+                    help="N > 1: split one ensemble over the ranks (LPT on the cost model, strong scaling) "
+                         "instead of one ensemble per rank (weak scaling)")
     ap.add_argument("--serving-sweep", action="store_true",
                     help="serving at 0.5, 1, 2, 4, 8 jobs/s over 120 s windows (long)")
     args = ap.parse_args()
@@ -448,10 +451,23 @@ def main() -> None:
     from cm3d_b200.engine import measure_peaks
     from cm3d_b200.setup import build_system
 
-    wls, desc, dsteps = workload(args.workload, seed=1 + rank)
+    partitioned = args.partition and world > 1
+    wls, desc, dsteps = workload(args.workload, seed=1 if partitioned else 1 + rank)
     steps = args.steps if args.steps is not None else dsteps
     warmup = args.warmup if args.warmup is not None else 20
     systems = [build_system(w) for w in wls]
+    natoms_job = sum(sm.natoms for sm in systems)
+    if partitioned:
+        # whole systems dealt to the ranks by LPT on the per-system cost model
+        from cm3d_b200.shard import imbalance, partition, system_cost
+        costs = [system_cost(sm) for sm in systems]
+        parts = partition(costs, world)
+        if any(len(p) == 0 for p in parts):
+            raise SystemExit("--partition: fewer systems than ranks")
+        shard_info = {"ranks": world, "imbalance": imbalance(costs, parts),
+                      "systems_per_rank": [len(p) for p in parts]}
+        systems = [systems[k] for k in parts[rank]]
+        wls = [wls[k] for k in parts[rank]]
     peaks = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     fp32, fp64 = measure_peaks(local)
@@ -460,15 +476,22 @@ def main() -> None:
     m = mixed_arm(systems, local, steps, warmup, flush, fp32, hbm, args.workload, min(steps, 100), dist)
     n = m["n"]
     ms = m["ms"]
-    value = world * n * steps / (ms / 1e3)
+    value = (natoms_job if partitioned else world * n) * steps / (ms / 1e3)
     dt_e2e, h2d, d2h, e2e_steps = m["e2e"]
-    e2e_value = world * n * e2e_steps / dt_e2e
+    atoms_all = natoms_job if partitioned else world * n
+    e2e_value = atoms_all * e2e_steps / dt_e2e
 
     plain = None
     if not args.no_plain:
         psteps = 10 if len(systems) > 1 else min(steps, 300)
         plain = plain_arm(systems, local, psteps, 3 if len(systems) > 1 else 10, flush)
-        plain["value"] *= world
+        pms = plain["ms_per_step"]
+        if dist:
+            t = torch.tensor([pms], dtype=torch.float64, device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        plain["ms_per_step"] = pms
+        plain["value"] = atoms_all / (pms / 1e3)
         plain["speedup_mixed_vs_plain"] = value / plain["value"]
 
     other = {}
@@ -504,12 +527,15 @@ def main() -> None:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": ms / steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "accumulate": "f64",
+            "scaling": "strong" if partitioned else "weak", "vs_baseline": None, "dtype": "f32",
+            "accumulate": "f64",
             "data": "synthetic (seeded; CM3D input decks from cm3d_b200.configs)",
             "config": {"workload": desc, "natoms": n, "systems": len(systems),
                        "mode": "mixed (FP32 compute, FP64 accumulation), one batch",
-                       "parallelism": f"{world} ranks, each its own ensemble (seed + rank)" if world > 1
-                       else "one GPU",
+                       "parallelism": (f"{world} ranks, the ensemble's systems split by LPT ({shard_info})"
+                                       if partitioned else
+                                       f"{world} ranks, each its own ensemble (seed + rank)" if world > 1
+                                       else "one GPU"),
                        "l2": "flushed between timed steps (256 MB write outside the step's events)",
                        "timing": "CUDA events around each step's graph replay on the engine stream; "
                                  "max over ranks"},
