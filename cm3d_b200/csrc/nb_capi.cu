@@ -842,7 +842,7 @@ static void energies_of(Ctx *c, int sy, cm3d_nb_energies *e) {
   e->vbond = a[ACC_VBOND];
   e->wbond = a[ACC_WBOND];
   e->vbend = a[ACC_VBEND];
-  e->wbend = 0.;
+  e->wbend = a[ACC_WBEND];
   double vol = deth(H.hmat), rvol = 1. / vol;
   e->US = e->vhinter + e->velec + e->vewald;
   e->U = e->vinter + e->velec + e->vewald;
@@ -854,12 +854,13 @@ static void energies_of(Ctx *c, int sy, cm3d_nb_energies *e) {
   e->Wtensor[8] -= H.wlrc * rvol;
   sym9(a, ACC_P2MT, e->p2m_tensor);
   double p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
-  double UI = e->vbond + e->vbend, WI = e->wbond;
+  double UI = e->vbond + e->vbend, WI = e->wbond + e->wbend;
   e->poth = e->US + H.vlrc / vol;
   e->poter = e->U + H.vlrc / vol;
   e->potra = UI;
   e->prsi = (p2m + e->W + WI) / (3 * vol);
-  for (int k = 0; k < 9; k++) e->prs_tensor[k] = (e->p2m_tensor[k] + e->Wtensor[k] + a[ACC_WBONDT + k]) / vol;
+  for (int k = 0; k < 9; k++)
+    e->prs_tensor[k] = (e->p2m_tensor[k] + e->Wtensor[k] + (a[ACC_WBONDT + k] + a[ACC_WBENDT + k])) / vol;
   e->zke = .5 * p2m;
   e->tiout = p2m / (double)H.ndof;
 }

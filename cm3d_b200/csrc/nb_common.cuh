@@ -40,10 +40,12 @@ enum {
   ACC_WBONDT = 48,        // 9
   ACC_VBEND = 57,         // getvbend energy
   ACC_P2MT = 58,          // 9: get_p2mt kinetic tensor
-  ACC_COUNT = 72,
+  ACC_WBEND = 67,         // getvbend virial (md_fbend.c compiles it with PRESSURE)
+  ACC_WBENDT = 68,        // 9
+  ACC_COUNT = 77,
   // each system owns ACC_STRIDE doubles of acc[]: its accumulators, then
   // device copies of its H^-1 (ACC_COUNT..+9) and H (+9..+18)
-  ACC_STRIDE = 96
+  ACC_STRIDE = 104
 };
 
 // Per-system parameters of a context that holds several independent systems

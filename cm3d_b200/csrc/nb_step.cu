@@ -211,7 +211,9 @@ __global__ void k_resetpos(int n, const SysP *__restrict__ sp, const int *__rest
 
 // start of force(1) (md_fcntr.c:64-73): zero fxl (and fxs), add the
 // excluded-pair correction of every group (ecorr, md_ewald.c:385-453), and
-// collect the group's bonded energies (getvbond / getvbend)
+// collect the group's bonded energies and virials (getvbond / getvbend; the
+// bend virial is the one md_fbend.c always compiles, its tensor formed from
+// absolute positions as there)
 __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
                              const double *__restrict__ pos, const double *__restrict__ q,
                              double *__restrict__ fxl, double *__restrict__ fxs, const int *__restrict__ gcoff,
@@ -224,10 +226,10 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
   if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = P.n;
-  // ecorr: pot, prs, t0 t1 t2 t4 t5 t8 | bond: v, w, t0..t8 | bend: v
-  double v[20];
+  // ecorr: pot, prs, t0 t1 t2 t4 t5 t8 | bond: v, w, t0..t8 | bend: v, w, t0..t8
+  double v[30];
 #pragma unroll
-  for (int k = 0; k < 20; k++) v[k] = 0.;
+  for (int k = 0; k < 30; k++) v[k] = 0.;
   int sy = -1;
   if (g < P.ngroups) {
     sy = sys_of[gatoms[gaoff[g]]];
@@ -281,14 +283,40 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
       double th = fabs(costh) >= 1. ? 1. : acos(costh);
       double dth = th - ep[b].x;
       v[19] += .5 * ep[b].y * dth * dth;
+      // bend virial (md_fbend.c:322-398), harmonic: dU/dth = 0 at |cos| = 1
+      const double dudth = fabs(costh) >= 1. ? 0. : ep[b].y * dth;
+      const double dthdcos = fabs(costh) >= 1. ? -1. : -1. / sqrt(1. - costh * costh);
+      const double dudcos = dudth * dthdcos;
+      const double c1x = costh * ax / al - bx * r11, c1y = costh * ay / al - by * r11,
+                   c1z = costh * az / al - bz * r11;
+      const double c2x = -costh * (ax / al + bx / bl) + (ax + bx) * r11;
+      const double c2y = -costh * (ay / al + by / bl) + (ay + by) * r11;
+      const double c2z = -costh * (az / al + bz / bl) + (az + bz) * r11;
+      const double c3x = costh * bx / bl - ax * r11, c3y = costh * by / bl - ay * r11,
+                   c3z = costh * bz / bl - az * r11;
+      const double xi = pos[i], xj = pos[j], xk = pos[k];
+      const double yi = pos[n + i], yj = pos[n + j], yk = pos[n + k];
+      const double zi = pos[2 * n + i], zj = pos[2 * n + j], zk = pos[2 * n + k];
+      v[20] += dudcos * (ax * c1x + ay * c1y + az * c1z - bx * c3x - by * c3y - bz * c3z);
+      v[21] += dudcos * (xi * c1x + xj * c2x + xk * c3x);
+      v[22] += dudcos * (yi * c1x + yj * c2x + yk * c3x);
+      v[23] += dudcos * (zi * c1x + zj * c2x + zk * c3x);
+      v[24] += dudcos * (xi * c1y + xj * c2y + xk * c3y);
+      v[25] += dudcos * (yi * c1y + yj * c2y + yk * c3y);
+      v[26] += dudcos * (zi * c1y + zj * c2y + zk * c3y);
+      v[27] += dudcos * (xi * c1z + xj * c2z + xk * c3z);
+      v[28] += dudcos * (yi * c1z + yj * c2z + yk * c3z);
+      v[29] += dudcos * (zi * c1z + zj * c2z + zk * c3z);
     }
   }
-  const int slots[20] = {ACC_POT_ECORR, ACC_PRS_ECORR, ACC_PRS_ECORRT + 0, ACC_PRS_ECORRT + 1,
+  const int slots[30] = {ACC_POT_ECORR, ACC_PRS_ECORR, ACC_PRS_ECORRT + 0, ACC_PRS_ECORRT + 1,
                          ACC_PRS_ECORRT + 2, ACC_PRS_ECORRT + 4, ACC_PRS_ECORRT + 5, ACC_PRS_ECORRT + 8,
                          ACC_VBOND, ACC_WBOND, ACC_WBONDT + 0, ACC_WBONDT + 1, ACC_WBONDT + 2,
                          ACC_WBONDT + 3, ACC_WBONDT + 4, ACC_WBONDT + 5, ACC_WBONDT + 6, ACC_WBONDT + 7,
-                         ACC_WBONDT + 8, ACC_VBEND};
-  sys_acc<20>(v, sy, acc, slots);
+                         ACC_WBONDT + 8, ACC_VBEND, ACC_WBEND, ACC_WBENDT + 0, ACC_WBENDT + 1,
+                         ACC_WBENDT + 2, ACC_WBENDT + 3, ACC_WBENDT + 4, ACC_WBENDT + 5, ACC_WBENDT + 6,
+                         ACC_WBENDT + 7, ACC_WBENDT + 8};
+  sys_acc<30>(v, sy, acc, slots);
 }
 
 // end of force(1) / force(0): rmass (utils/md_util.new.c:219) and, inside

@@ -57,7 +57,7 @@ struct orc {
   double spote, spothe, sprse, sprset[9];
   double vk_ewald, vp_ewald, vp_ewald_tensor[9];
   double pot_ecorr, prs_ecorr, prs_ecorr_tensor[9];
-  double vbond, wbond, wbondt[9], vbend;
+  double vbond, wbond, wbondt[9], vbend, wbend, wbendt[9];
 };
 
 static void *dup(const void *p, size_t bytes)
@@ -982,13 +982,16 @@ void orc_force(orc *o, int iflg)
   }
 }
 
-/* getvbond / getvbend energies  md_fbond.c:131-220, md_fbend.c:262-410
-   (the bend virial is compiled only with -DPRESSURE, off by default) */
+/* getvbond / getvbend energies and virials  md_fbond.c:131-220,
+   md_fbend.c:262-410.  md_fbend.c:38 defines PRESSURE for its own file, so the
+   bend virial is always on: a scalar that vanishes up to rounding (an angle
+   does not change under a uniform dilation) and a traceless tensor, formed
+   from the atoms' absolute positions */
 static void bonded_energies(orc *o)
 {
   int nb, i;
-  o->vbond = o->wbond = o->vbend = 0.;
-  for (i = 0; i < 9; i++) o->wbondt[i] = 0.;
+  o->vbond = o->wbond = o->vbend = o->wbend = 0.;
+  for (i = 0; i < 9; i++) o->wbondt[i] = o->wbendt[i] = 0.;
   for (nb = 0; nb < o->nbonds; nb++) {
     int a = o->ibond[nb], b = o->jbond[nb], idx = o->idxbond[nb];
     double dx = o->px[a] - o->px[b], dy = o->py[a] - o->py[b], dz = o->pz[a] - o->pz[b];
@@ -1013,6 +1016,30 @@ static void bonded_energies(orc *o)
     th = fabs(costh) >= 1. ? 1. : acos(costh);
     dth = th - o->eqbend[idx];
     o->vbend += .5 * o->fkbend[idx] * dth * dth;
+    {
+      /* harmonic: dU/dth = 0 at |cos| = 1 (md_fbend.c:322-327) */
+      double dudth = fabs(costh) >= 1. ? 0. : o->fkbend[idx] * dth;
+      double dthdcos = fabs(costh) >= 1. ? -1. : -1. / sqrt(1. - costh * costh);
+      double dudcos = dudth * dthdcos;
+      double c1x = costh * ax / al - bx * r11, c1y = costh * ay / al - by * r11, c1z = costh * az / al - bz * r11;
+      double c2x = -costh * (ax / al + bx / bl) + (ax + bx) * r11;
+      double c2y = -costh * (ay / al + by / bl) + (ay + by) * r11;
+      double c2z = -costh * (az / al + bz / bl) + (az + bz) * r11;
+      double c3x = costh * bx / bl - ax * r11, c3y = costh * by / bl - ay * r11, c3z = costh * bz / bl - az * r11;
+      double xi = o->px[a], xj = o->px[b], xk = o->px[c];
+      double yi = o->py[a], yj = o->py[b], yk = o->py[c];
+      double zi = o->pz[a], zj = o->pz[b], zk = o->pz[c];
+      o->wbend += dudcos * (ax * c1x + ay * c1y + az * c1z - bx * c3x - by * c3y - bz * c3z);
+      o->wbendt[0] += dudcos * (xi * c1x + xj * c2x + xk * c3x);
+      o->wbendt[1] += dudcos * (yi * c1x + yj * c2x + yk * c3x);
+      o->wbendt[2] += dudcos * (zi * c1x + zj * c2x + zk * c3x);
+      o->wbendt[3] += dudcos * (xi * c1y + xj * c2y + xk * c3y);
+      o->wbendt[4] += dudcos * (yi * c1y + yj * c2y + yk * c3y);
+      o->wbendt[5] += dudcos * (zi * c1y + zj * c2y + zk * c3y);
+      o->wbendt[6] += dudcos * (xi * c1z + xj * c2z + xk * c3z);
+      o->wbendt[7] += dudcos * (yi * c1z + yj * c2z + yk * c3z);
+      o->wbendt[8] += dudcos * (zi * c1z + zj * c2z + zk * c3z);
+    }
   }
 }
 
@@ -1038,7 +1065,7 @@ void orc_get_energies(orc *o, cm3d_nb_energies *e)
   e->vbond = o->vbond;
   e->wbond = o->wbond;
   e->vbend = o->vbend;
-  e->wbend = 0.;
+  e->wbend = o->wbend;
   e->US = e->vhinter + e->velec + e->vewald;
   e->U = e->vinter + e->velec + e->vewald;
   e->W = e->winter + e->welec + e->wewald;
@@ -1064,8 +1091,9 @@ void orc_get_energies(orc *o, cm3d_nb_energies *e)
   e->p2m_tensor[7] = e->p2m_tensor[5];
   p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
   {
-    double UI = e->vbond + e->vbend, WI = e->wbond, wit[9];
-    for (i = 0; i < 9; i++) wit[i] = o->wbondt[i];
+    /* UI, WI and WItensor as getvireal sums them (md_fcntr.c:205-215) */
+    double UI = e->vbond + e->vbend, WI = e->wbond + e->wbend, wit[9];
+    for (i = 0; i < 9; i++) wit[i] = o->wbondt[i] + o->wbendt[i];
     e->poth = e->US;
     e->poter = e->U;
     e->potra = UI;

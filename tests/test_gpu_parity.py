@@ -172,6 +172,10 @@ def test_trajectory(engine_lib, name, mode, graph):
         en = e.energies()
         for c, key in enumerate(("poter", "potra", "zke")):
             assert close(en[key], eng[k, c], ptol if c != 1 else 10 * ptol), (k, key)
+    # the pressure tensor after the last step, bend virial included (the
+    # traceless part that the scalar pressure does not see)
+    pt, want = np.array(en["prs_tensor"]), d["ef_prs_tensor"]
+    assert np.abs(pt - want).max() <= (ptol if mode == _abi.PLAIN_FP64 else 1e-3) * np.abs(want).max()
     pos = e.positions()
     ref = np.stack([d["final_px"], d["final_py"], d["final_pz"]])
     assert np.abs(pos - ref).max() <= (1e-9 if mode == _abi.PLAIN_FP64 else 1e-3)

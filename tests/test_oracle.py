@@ -77,8 +77,9 @@ def test_level1_forces_and_energies_exact(name):
         assert np.array_equal(np.array(e[k]), d[f"e0_{k}"]), k
     o.force(2)
     e = o.energies()
-    for k in ("prsi", "zke", "tiout", "poter", "potra"):
+    for k in ("prsi", "zke", "tiout", "poter", "potra", "wbend"):
         assert e[k] == float(d[f"e0_{k}"][0]), k
+    assert np.array_equal(np.array(e["prs_tensor"]), d["e0_prs_tensor"])
 
 
 @pytest.mark.parametrize("name", ["lj2", "lj256", "argon864", "water216", "binary256", "water4096"])
@@ -96,6 +97,13 @@ def test_trajectory_bit_exact(name):
     assert np.array_equal(o.positions(), np.stack([d["final_px"], d["final_py"], d["final_pz"]]))
     assert np.array_equal(o.velocities(), np.stack([d["final_vx"], d["final_vy"], d["final_vz"]]))
     assert o.rebuilds - 1 == int(eng[-1, 7])
+    # getvireal(..., 1) + geteng after the last step, the pressure tensor with
+    # the bend virial of md_fbend.c (always compiled with PRESSURE) included
+    e = o.energies()
+    for k in ("vbond", "vbend", "wbond", "wbend", "W", "U", "US", "prsi", "zke", "poter", "potra"):
+        assert e[k] == float(d[f"ef_{k}"][0]), k
+    for k in ("wintertensor", "welectensor", "wewaldtensor", "Wtensor", "prs_tensor"):
+        assert np.array_equal(np.array(e[k]), d[f"ef_{k}"]), k
 
 
 def test_lj_regression_known_answers():
