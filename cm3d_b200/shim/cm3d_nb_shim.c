@@ -1,0 +1,268 @@
+/*
+ * cm3d_nb_shim.c -- CM3D's step_init() and step() (integrate/md_step.c:32-159)
+ * on the B200 nonbonded engine, as a drop-in for CM3D's own md_step.o.
+ *
+ * Linked into CM3D in place of md_step.o (that object defines exactly these
+ * two functions), it lets CM3D's unmodified MD driver (md_mdcntr_new,
+ * main/md_mdcntr.new.c:174-178: step, geteng, gettngbr every step) run the
+ * whole RESPA step on the GPU:
+ *
+ *   step_init  builds the engine's system description from CM3D's own
+ *              SIMPARMS / COORDS / INTER structs once, uploads it
+ *              (cm3d_nb_create), runs CM3D's step_init sequence on the device
+ *              (cm3d_nb_step_init: get_ngbr, force(1), force(2)), and fills
+ *              CM3D's ENERGIES the way getvireal(..., 1) does
+ *              (energy/control/md_fcntr.c:136-257), then calls CM3D's own
+ *              geteng and gettngbr as md_step.c:53-55 does;
+ *   step       advances one outer step on the device (cm3d_nb_step with
+ *              SIMPARMS.istep), copies positions and velocities back into
+ *              COORDS (CM3D's writers and geteng read them) and refills
+ *              ENERGIES.
+ *
+ * What the engine does not compute -- thermostats and barostats, torsions,
+ * 1-4 and cross bonds, frozen atoms, external fields, dipoles, non-periodic
+ * boxes -- stops the run through md_error with the reason, as CM3D reports
+ * unsupported input; nothing falls back to a CPU path.
+ *
+ * Environment: CM3D_NB_MODE=plain selects the plain FP64 engine (default:
+ * mixed), CM3D_NB_DEVICE the CUDA device (default 0).
+ */
+#include "md.h"
+
+#include "cm3d_nb.h"
+
+static cm3d_nb_ctx *g_ctx = NULL;
+static int *g_map = NULL, *g_eoff = NULL, *g_eidx = NULL, *g_coff = NULL, *g_cidx = NULL;
+
+static void nb_fail(const char *what)
+{
+  char line[1400];
+  snprintf(line, sizeof line, "GPU nonbonded engine: %s: %s", what, cm3d_nb_last_error());
+  md_error(line);
+}
+
+static void nb_check(int rc, const char *what)
+{
+  if (rc != CM3D_NB_OK) nb_fail(what);
+}
+
+static void unsupported(const char *what)
+{
+  char line[400];
+  snprintf(line, sizeof line, "GPU nonbonded engine: %s is not supported", what);
+  md_error(line);
+}
+
+/* the features the engine computes (see the file header) */
+static void check_supported(SIMPARMS *simparms, COORDS *coords)
+{
+  if (simparms->iperd != 3) unsupported("a non-periodic or partially periodic box (iperd != 3)");
+  if (simparms->iensemble != 0) unsupported("an ensemble other than nve");
+  if (simparms->ivol) unsupported("a variable cell (ivol)");
+  if (simparms->nfreeze > 0) unsupported("frozen atoms");
+  if (simparms->iextern) unsupported("an external field");
+  if (simparms->ipolar) unsupported("polarizable dipoles");
+  if (coords->tors.ntorss > 0 || coords->onfo.n14s > 0 || coords->bondxs.nbondxs > 0)
+    unsupported("torsions, 1-4 interactions or cross bonds");
+}
+
+/* CSR copy of CM3D's per-atom exclusion lists (INTER.nexclude/exclude,
+   COUL.nexclude/exclude) */
+static void csr(int n, const int *cnt, int **lists, int **off, int **idx)
+{
+  int i, k, tot = 0;
+  for (i = 0; i < n; i++) tot += cnt ? cnt[i] : 0;
+  *off = (int *)malloc(sizeof(int) * (n + 1));
+  *idx = (int *)malloc(sizeof(int) * (tot > 0 ? tot : 1));
+  (*off)[0] = 0;
+  for (i = 0; i < n; i++) {
+    int c = cnt ? cnt[i] : 0;
+    for (k = 0; k < c; k++) (*idx)[(*off)[i] + k] = lists[i][k];
+    (*off)[i + 1] = (*off)[i] + c;
+  }
+}
+
+static void create_engine(SIMPARMS *simparms, COORDS *coords, INTER *inter)
+{
+  cm3d_nb_system s;
+  cm3d_nb_options opt;
+  const char *mode = getenv("CM3D_NB_MODE"), *dev = getenv("CM3D_NB_DEVICE");
+  int nt = simparms->ntypes, a, b;
+
+  memset(&s, 0, sizeof s);
+  s.natoms = simparms->natoms;
+  s.iperd = simparms->iperd;
+  s.nres_lrf = simparms->ninter;
+  s.nres_intra = simparms->ninnra;
+  s.nres_tors = simparms->ninrra;
+  s.ndof = simparms->ndof;
+  s.dt = simparms->dt;
+  s.vlrc = simparms->vlrc;
+  s.wlrc = simparms->wlrc;
+  memcpy(s.hmat, coords->hmat, sizeof s.hmat);
+  s.px = coords->px; s.py = coords->py; s.pz = coords->pz;
+  s.vx = coords->vx; s.vy = coords->vy; s.vz = coords->vz;
+  s.amass = coords->amass;
+  s.qch = coords->qch;
+  s.ntypes = nt;
+  s.itype = inter->itype;
+  g_map = (int *)malloc(sizeof(int) * (size_t)(nt * nt > 0 ? nt * nt : 1));
+  for (a = 0; a < nt; a++)
+    for (b = 0; b < nt; b++) g_map[a * nt + b] = inter->map[a][b];
+  s.map = g_map;
+  s.ninter = inter->ntype;
+  s.ntable = inter->ntable;
+  s.vtab = inter->ntype ? inter->vtab[0] : NULL;
+  s.dvtab = inter->ntype ? inter->dvtab[0] : NULL;
+  s.switchs = inter->ntype ? inter->switchs[0] : NULL;
+  s.rmaxs_cut2 = inter->rmaxs_cut2;
+  s.rmins_cut2 = inter->rmins_cut2;
+  s.rmaxl_cut2 = inter->rmaxl_cut2;
+  s.rminl_cut2 = inter->rminl_cut2;
+  s.rmaxs_skin2 = inter->rmaxs_skin2;
+  s.rmaxl_skin2 = inter->rmaxl_skin2;
+  s.dx2tab = inter->dx2tab;
+  s.skin_ter = inter->skin_ter;
+  s.rheal = inter->rheal;
+  if (coords->coul.ncharge > 0) {
+    s.coultab = inter->coultab;
+    s.dcoultab = inter->dcoultab;
+    s.switchse = inter->switchse;
+  }
+  s.dx2coul = inter->dx2coul;
+  s.rmins_coul2 = inter->rmins_coul2;
+  s.rmaxs_coul2 = inter->rmaxs_coul2;
+  s.rminl_coul2 = inter->rminl_coul2;
+  s.rmaxl_coul2 = inter->rmaxl_coul2;
+  s.rmaxs_skin2_e = inter->rmaxs_skin2_e;
+  s.rmaxl_skin2_e = inter->rmaxl_skin2_e;
+  csr(s.natoms, inter->nexclude, inter->exclude, &g_eoff, &g_eidx);
+  csr(s.natoms, coords->coul.nexclude, coords->coul.exclude, &g_coff, &g_cidx);
+  s.excl_off = g_eoff; s.excl_idx = g_eidx;
+  s.cexcl_off = g_coff; s.cexcl_idx = g_cidx;
+  s.ktot = coords->coul.ktot;
+  s.ka = coords->coul.ka; s.kb = coords->coul.kb; s.kc = coords->coul.kc;
+  s.kappa = coords->coul.kappa;
+  s.falp2 = coords->coul.falp2;
+  s.ewald_self = coords->coul.ewald_self;
+  s.ewald_bkg = coords->coul.ewald_bkg;
+  s.necorr = coords->coul.necorr;
+  s.iecorr = coords->coul.iecorr;
+  s.jecorr = coords->coul.jecorr;
+  s.nbonds = coords->bonds.nbonds;
+  s.nbond_types = coords->bonds.itypes;
+  s.ibond = coords->bonds.ibond; s.jbond = coords->bonds.jbond;
+  s.idxbond = coords->bonds.idxbond; s.itypbond = coords->bonds.itypbond;
+  s.eqbond = coords->bonds.eqbond; s.fkbond = coords->bonds.fkbond;
+  s.nbends = coords->bends.nbends;
+  s.nbend_types = coords->bends.itypes;
+  s.ibend = coords->bends.ibend; s.jbend = coords->bends.jbend; s.kbend = coords->bends.kbend;
+  s.idxbend = coords->bends.idxbend; s.itypbend = coords->bends.itypbend;
+  s.eqbend = coords->bends.eqbend; s.fkbend = coords->bends.fkbend;
+
+  cm3d_nb_default_options(&opt);
+  if (mode && strcmp(mode, "plain") == 0) opt.mode = CM3D_NB_PLAIN_FP64;
+  if (dev) opt.device = atoi(dev);
+  nb_check(cm3d_nb_create(&s, &opt, &g_ctx), "cm3d_nb_create");
+}
+
+/* ENERGIES as getvireal(..., 1) leaves them (md_fcntr.c:136-257): the engine
+   supplies every nonbonded, Ewald and bonded term; the terms it does not
+   compute are zero */
+static void fill_energies(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies)
+{
+  cm3d_nb_energies e;
+  double vol = get_deth(coords->hmat);
+  int i;
+  nb_check(cm3d_nb_get_energies(g_ctx, &e), "cm3d_nb_get_energies");
+  energies->vinter = e.vinter;
+  energies->vhinter = e.vhinter;
+  energies->velec = e.velec;
+  energies->vewald = e.vewald;
+  energies->vbond = e.vbond;
+  energies->vbend = e.vbend;
+  energies->vtors = energies->vbondx = energies->vonfo = energies->vonfo_e = 0.0;
+  energies->vextern = energies->vextern_e = 0.0;
+  energies->winter = e.winter;
+  energies->welec = e.welec;
+  energies->wewald = e.wewald;
+  energies->wbond = e.wbond;
+  energies->wbend = e.wbend;
+  energies->wtors = energies->wbondx = energies->wonfo = energies->wonfo_e = 0.0;
+  energies->wextern = energies->wextern_e = 0.0;
+  energies->US = e.US;
+  energies->U = e.U;
+  energies->W = e.W;
+  energies->UI = e.vbond + e.vbend;
+  energies->WI = e.wbond + e.wbend;
+  for (i = 0; i < 9; i++) {
+    energies->wintertensor[i] = e.wintertensor[i];
+    energies->welectensor[i] = e.welectensor[i];
+    energies->wewaldtensor[i] = e.wewaldtensor[i];
+    energies->Wtensor[i] = e.Wtensor[i];
+    /* bonded virial tensor: the engine's pressure tensor minus its kinetic
+       and nonbonded parts */
+    energies->WItensor[i] = e.prs_tensor[i] * vol - e.p2m_tensor[i] - e.Wtensor[i];
+    energies->wbondtensor[i] = energies->WItensor[i];
+    energies->wbendtensor[i] = energies->wtorstensor[i] = energies->wbondxtensor[i] = 0.0;
+    energies->wonfotensor[i] = energies->wonfo_etensor[i] = 0.0;
+  }
+  (void)simparms;
+}
+
+static void pull_state(COORDS *coords)
+{
+  nb_check(cm3d_nb_get_positions(g_ctx, coords->px, coords->py, coords->pz), "cm3d_nb_get_positions");
+  nb_check(cm3d_nb_get_velocities(g_ctx, coords->vx, coords->vy, coords->vz), "cm3d_nb_get_velocities");
+}
+
+static void pull_forces(COORDS *coords)
+{
+  nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXL, coords->fxl, coords->fyl, coords->fzl), "get_forces");
+  nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXS, coords->fxs, coords->fys, coords->fzs), "get_forces");
+  nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXA, coords->fxa, coords->fya, coords->fza), "get_forces");
+}
+
+/* NGBR as get_ngbr leaves it (energy/control/ngbr_list.c:308): the pair
+   counts of the current lists, and update = list builds so far - 1 (step_init
+   sets -1 and its first build makes it 0), which writescreen turns into
+   <ts/update> (output/md_writescreen.c:48-64) */
+static void list_counts(NGBR *ngbr)
+{
+  long long c;
+  cm3d_nb_status_t st;
+  nb_check(cm3d_nb_get_status(g_ctx, &st), "get_status");
+  ngbr->update = (int)(st.rebuilds - 1);
+  nb_check(cm3d_nb_list_count(g_ctx, CM3D_NB_LIST_T, &c), "list_count"); ngbr->nprt = (int)c;
+  nb_check(cm3d_nb_list_count(g_ctx, CM3D_NB_LIST_S, &c), "list_count"); ngbr->nprs = (int)c;
+  nb_check(cm3d_nb_list_count(g_ctx, CM3D_NB_LIST_TE, &c), "list_count"); ngbr->nprte = (int)c;
+  nb_check(cm3d_nb_list_count(g_ctx, CM3D_NB_LIST_SE, &c), "list_count"); ngbr->nprse = (int)c;
+}
+
+void step_init(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, NGBR *ngbr)
+{
+  check_supported(simparms, coords);
+  if (simparms->rank == 0) md_stdout("Calculating initial forces (B200 nonbonded engine)");
+  if (!g_ctx) {
+    create_engine(simparms, coords, inter);
+  } else {
+    nb_check(cm3d_nb_set_positions(g_ctx, coords->px, coords->py, coords->pz), "set_positions");
+    nb_check(cm3d_nb_set_velocities(g_ctx, coords->vx, coords->vy, coords->vz), "set_velocities");
+  }
+  nb_check(cm3d_nb_step_init(g_ctx), "step_init");
+  pull_forces(coords);
+  list_counts(ngbr);
+  fill_energies(simparms, coords, energies);
+  geteng(simparms, coords, energies);
+  gettngbr(ngbr);
+}
+
+void step(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, NGBR *ngbr)
+{
+  (void)inter;
+  nb_check(cm3d_nb_step(g_ctx, simparms->istep, 1), "step");
+  pull_state(coords);
+  list_counts(ngbr);
+  fill_energies(simparms, coords, energies);
+  gettngbr(ngbr);
+}
