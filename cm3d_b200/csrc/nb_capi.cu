@@ -86,7 +86,7 @@ static void destroy(Ctx *c) {
                   c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
                   c->cimg, c->nlen, c->acc,
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
-                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part};
+                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -164,6 +164,15 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
   c->dev = o.device;
   CK(cudaSetDevice(c->dev));
   CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->dev));
+  {
+    int optin = 0;
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
+    c->smem_optin = (size_t)optin;
+    // CM3D_NB_PAIR_KERNEL=list keeps single systems on the list-gather pair
+    // kernel (the one batches and small boxes use), for comparisons
+    const char *pk = getenv("CM3D_NB_PAIR_KERNEL");
+    if (pk && strcmp(pk, "list") == 0) c->win_ok = 0, c->win_env_off = 1;
+  }
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   c->mode = o.mode;
   c->need_short = o.need_short;
@@ -1028,6 +1037,13 @@ long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx) {
   return c ? c->launches : 0;
 }
 
+int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa) {
+  CTX;
+  if (kernel) *kernel = c->pair_used;
+  if (tpa) *tpa = c->tpa;
+  return CM3D_NB_OK;
+}
+
 int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]) {
   CTX;
   int rc;
@@ -1042,33 +1058,42 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   if (reps < 1) reps = 5;
   const int cand[4] = {4, 8, 16, 32};
   double best = 1e300;
-  int best_tpa = c->tpa;
+  int best_tpa = c->tpa, best_win = 0;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
   const bool timing = c->timing.on;
   c->timing.on = false;
-  for (int k = 0; k < 4; k++) {
-    c->tpa = cand[k];
-    if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
-    CK(cudaEventRecord(a, c->st));
-    for (int r = 0; r < reps; r++)
-      if ((rc = pair_forces(c, 1, 3))) return rc;
-    CK(cudaEventRecord(b, c->st));
-    CK(cudaEventSynchronize(b));
-    float ms = 0;
-    CK(cudaEventElapsedTime(&ms, a, b));
-    const double per = ms / reps;
-    if (ms_per_launch) ms_per_launch[k] = per;
-    if (per < best) {
-      best = per;
-      best_tpa = cand[k];
+  if (ms_per_launch)
+    for (int k = 0; k < 4; k++) ms_per_launch[k] = 1e300;
+  // the gather kernel, then (where the box allows it) the windowed kernel:
+  // a single system runs whichever is faster on its live lists
+  for (int win = 0; win <= (c->win_env_off ? 0 : 1); win++) {
+    c->win_ok = win;
+    for (int k = 0; k < 4; k++) {
+      c->tpa = cand[k];
+      if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
+      CK(cudaEventRecord(a, c->st));
+      for (int r = 0; r < reps; r++)
+        if ((rc = pair_forces(c, 1, 3))) return rc;
+      CK(cudaEventRecord(b, c->st));
+      CK(cudaEventSynchronize(b));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, a, b));
+      const double per = ms / reps;
+      if (ms_per_launch && per < ms_per_launch[k]) ms_per_launch[k] = per;
+      if (per < best) {
+        best = per;
+        best_tpa = cand[k];
+        best_win = win;
+      }
     }
   }
   c->timing.on = timing;
   cudaEventDestroy(a);
   cudaEventDestroy(b);
   c->tpa = best_tpa;
+  c->win_ok = best_win;
   if (tpa_chosen) *tpa_chosen = best_tpa;
   // a captured step holds the old launch configuration; the timing launches
   // added to the force blocks and accumulators: recompute force(1)

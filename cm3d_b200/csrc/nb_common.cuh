@@ -120,6 +120,9 @@ __device__ __forceinline__ void sys_acc(double (&v)[NV], int sys, double *acc, c
   if (__all_sync(full, sys == s0 || sys < 0)) {
 #pragma unroll
     for (int k = 0; k < NV; k++) {
+      // a quantity that is zero on every thread (e.g. no bonds in an LJ
+      // system) costs one vote, not a reduction
+      if (!__any_sync(full, sys >= 0 && v[k] != 0.0)) continue;
       double s = sys < 0 ? 0.0 : v[k];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(full, s, o);
@@ -188,6 +191,12 @@ struct Ctx {
   int ncoul = 0;                       // erfc tables (one per system with charges)
   int all_rebuild = 1;                 // list kernels: rebuild every system (host-driven builds)
   int num_sms = 148;
+  size_t smem_optin = 0;               // opt-in shared memory per block (bytes)
+  double *ered = nullptr;              // k_ereduce: per-block partial sums of one large system
+  unsigned *ered_done = nullptr;       // k_ereduce: blocks finished per quantity
+  int win_ok = 1;                      // single systems may use the windowed pair kernel
+  int win_env_off = 0;                 // CM3D_NB_PAIR_KERNEL=list: never
+  int pair_used = 0;                   // kernel of the last pair launch (CM3D_NB_PAIR_*)
   cudaStream_t st = nullptr;
   int mode = CM3D_NB_MIXED;
   int need_short = 0;
@@ -383,6 +392,7 @@ __device__ __forceinline__ void block_acc(double (&v)[NV], double *acc, const in
 int plain_pairs(Ctx *c, int iflg, int which);   // nb_plain.cu
 int plain_ecorr(Ctx *c, const int2 *ij);        // nb_plain.cu
 int mixed_pairs(Ctx *c, int iflg, int mask);    // nb_pair.cu
+bool win_applies(Ctx *c);                       // nb_pair.cu: windowed pair kernel possible
 int build_lists(Ctx *c, bool device_flag, bool all);   // nb_list.cu
 int list_setup(Ctx *c);                         // nb_list.cu
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused

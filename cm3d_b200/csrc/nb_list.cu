@@ -158,24 +158,32 @@ __global__ void k_cell_fill(int n, const int *__restrict__ sys_of, const int *__
   cell_atoms[cell_start[c] + slot] = i;
 }
 
-// order every cell's atoms by atom index (deterministic lists): one block
-// per cell ranks each atom among its cell's atoms (indices are distinct)
+// order every cell's atoms by (atom type, atom index): deterministic lists,
+// and the atoms of one type are neighbours in sorted order, so the lane
+// groups of a warp in the pair kernels mostly hold atoms of one type and
+// walk lists of the same make-up.  One block per cell ranks each atom among
+// its cell's atoms (keys are distinct).
+__device__ __forceinline__ long long sort_key(const int *__restrict__ itype, int i) {
+  return ((long long)itype[i] << 32) | (unsigned)i;
+}
+
 __global__ void k_cell_sort(int ncells, const int *__restrict__ cell_sys, const int *__restrict__ sreb, int all,
-                            const int *__restrict__ cell_start, int *__restrict__ cell_atoms,
-                            const int *__restrict__ gate) {
+                            const int *__restrict__ cell_start, const int *__restrict__ itype,
+                            int *__restrict__ cell_atoms, const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
-  __shared__ int s[1024];
+  __shared__ long long s[1024];
   const int c = blockIdx.x;
   if (sys_skip(cell_sys[c], sreb, all)) return;
   const int lo = cell_start[c], hi = cell_start[c + 1], m = hi - lo;
   if (m <= 1) return;
   if (m <= 1024) {
-    for (int k = threadIdx.x; k < m; k += blockDim.x) s[k] = cell_atoms[lo + k];
+    for (int k = threadIdx.x; k < m; k += blockDim.x) s[k] = sort_key(itype, cell_atoms[lo + k]);
     __syncthreads();
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
-      int v = s[k], r = 0;
+      const long long v = s[k];
+      int r = 0;
       for (int u = 0; u < m; u++) r += s[u] < v;
-      cell_atoms[lo + r] = v;
+      cell_atoms[lo + r] = (int)(v & 0xffffffffLL);
     }
     return;
   }
@@ -183,7 +191,7 @@ __global__ void k_cell_sort(int ncells, const int *__restrict__ cell_sys, const 
   for (int pass = 0; pass < m; pass++) {
     for (int k = lo + (pass & 1) + 2 * threadIdx.x; k + 1 < hi; k += 2 * blockDim.x) {
       int a0 = cell_atoms[k], a1 = cell_atoms[k + 1];
-      if (a0 > a1) {
+      if (sort_key(itype, a0) > sort_key(itype, a1)) {
         cell_atoms[k] = a1;
         cell_atoms[k + 1] = a0;
       }
@@ -397,10 +405,13 @@ __global__ void __launch_bounds__(256) k_list_half(
 
 // Mixed mode, one pass: the full list of sorted atom t (both directions,
 // every pair in CM3D's t or te list) written straight into its fixed slot
-// nbr[t * stride ...], in candidate order, its length into nlen[t].  An atom
-// with more than `stride` pairs writes the first `stride`, records the
-// length it needed (ST_NEED_STRIDE) and halts a captured step; the host then
-// widens the slots and builds again.
+// nbr[t * stride ...] in two segments, each in candidate order: the pairs in
+// an LJ list (t or s) from the front of the slot, their count in nlen[t], and
+// the electrostatics-only pairs from the back (the last one at the slot's
+// end), their count in nlen[n + t].  A pair kernel then runs the LJ arithmetic
+// only over the front segment.  An atom with more than `stride` pairs writes
+// none past its slot, records the length it needed (ST_NEED_STRIDE) and halts
+// a captured step; the host then widens the slots and builds again.
 __global__ void __launch_bounds__(256) k_list_full(
     int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
     int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
@@ -425,7 +436,7 @@ __global__ void __launch_bounds__(256) k_list_full(
   const int ti = itype[i];
   const bool qi = q[i] != 0.0;
   uint32_t *out = nbr + (size_t)t * stride;
-  int count = 0;
+  int na = 0, nb = 0;
   unsigned bad = 0;
   auto decide = [&](int first, int m) {
     int fl = 0, code = 13, u = 0;
@@ -435,23 +446,40 @@ __global__ void __launch_bounds__(256) k_list_full(
                        excl_idx, cexcl_off, cexcl_idx, cimg, code);
     }
     bad |= (fl >> 4) & 1;
-    const bool f = (fl & 5) != 0;
-    const unsigned bf = __ballot_sync(0xffffffffu, f);
-    if (f) {
-      const int slot = count + __popc(bf & lt_mask);
+    const bool fa = (fl & 3) != 0;                   // in an LJ list: front segment
+    const bool fb = !fa && (fl & 12) != 0;           // electrostatics only: back segment
+    const unsigned ba = __ballot_sync(0xffffffffu, fa), bb = __ballot_sync(0xffffffffu, fb);
+    if (fa || fb) {
       uint32_t e = (uint32_t)u | ((uint32_t)code << ENT_CODE_SHIFT);
       if (fl & 1) e |= ENT_LJ;
       if (fl & 2) e |= ENT_LJS;
       if (fl & 4) e |= ENT_EL;
       if (fl & 8) e |= ENT_ELS;
       if (fl & 32) e |= ENT_NEAR;
-      if (slot < stride) out[slot] = e;
+      // every write lands inside the slot; once the two segments meet (an
+      // overflow) the slot's contents no longer matter: the lengths are set
+      // to zero below and the list is built again with wider slots
+      if (fa) {
+        const int slot = na + __popc(ba & lt_mask);
+        if (slot < stride - nb) out[slot] = e;
+      } else {
+        const int slot = nb + __popc(bb & lt_mask);
+        if (slot < stride - na) out[stride - 1 - slot] = e;
+      }
     }
-    count += __popc(bf);
+    na += __popc(ba);
+    nb += __popc(bb);
   };
   walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide);
+  const int count = na + nb;
   if (lane == 0) {
-    nlen[t] = count < stride ? count : stride;
+    if (count <= stride) {
+      nlen[t] = na;
+      nlen[n + t] = nb;
+    } else {
+      nlen[t] = 0;
+      nlen[n + t] = 0;
+    }
     if (count > stride) {
       atomicMax((unsigned long long *)(stat + ST_NEED_STRIDE), (unsigned long long)count);
       if (halt) {
@@ -609,7 +637,8 @@ int list_setup(Ctx *c) {
   CK(cudaMemcpy(c->shift, c->h_sp[0].shift, sizeof(float4) * 27, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->shift + 27, c->h_sp[0].shift_lo, sizeof(float4) * 27, cudaMemcpyHostToDevice));
   if (c->mode == CM3D_NB_MIXED) {
-    CK(cudaMalloc(&c->nlen, sizeof(int) * (size_t)c->n));
+    CK(cudaMalloc(&c->nlen, sizeof(int) * 2 * (size_t)c->n));
+    CK(cudaMemset(c->nlen, 0, sizeof(int) * 2 * (size_t)c->n));
     long long s = ((long long)est_max + 31) / 32 * 32;
     if (s < 32) s = 32;
     c->nbr_stride = (int)s;
@@ -682,8 +711,8 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
   k_cell_scan<<<c->nsys, 256, 0, c->st>>>(c->sp, c->sreb, al, c->cell_cursor, c->cell_start, gate);
   k_cell_fill<<<grid_for(n, B), B, 0, c->st>>>(n, c->sys_of, c->sreb, al, c->cell_of, c->cell_start,
                                                 c->cell_cursor, c->cell_atoms, gate);
-  k_cell_sort<<<c->ncells, 256, 0, c->st>>>(c->ncells, c->cell_sys, c->sreb, al, c->cell_start, c->cell_atoms,
-                                            gate);
+  k_cell_sort<<<c->ncells, 256, 0, c->st>>>(c->ncells, c->cell_sys, c->sreb, al, c->cell_start, c->itype,
+                                            c->cell_atoms, gate);
   k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->sp, c->sys_of, c->sreb, al, c->cell_atoms, cimg, c->itype,
                                                   c->pos, c->q, c->rank, c->styp, c->corner, c->xq, gate);
   c->launches += 6;

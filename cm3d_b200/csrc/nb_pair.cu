@@ -69,6 +69,389 @@ __device__ __forceinline__ void min_image(const Box &B, float &dx, float &dy, fl
   }
 }
 
+// ------------------------------------------------------------------
+// Windowed pair kernel: one system whose cell grid has at least 3 cells per
+// axis (no on-the-fly minimum image).  A work item is one cell of i-atoms (or
+// a part of one); its block stages the 27 cells around it -- the only cells
+// its atoms' neighbours can be in -- into shared memory, each cell's atoms
+// already moved by that cell's periodic shift into the frame of the i-cell's
+// corner.  A list entry (j's sorted index u, shift code) then addresses the
+// staged copy as u + delta[code]: with 3 or more cells per axis the shift code
+// names the stencil cell, so no gather leaves the SM.  The list itself is
+// streamed in 16-byte vectors, one vector ahead of use.
+//
+// Window capacity is fixed at launch; an item whose 27 cells hold more atoms
+// reads its j-atoms from global memory instead (same arithmetic), so no
+// occupancy ever writes past the staged arrays.
+struct WinP {
+  int ncx, ncy, ncz;         // cells per axis (all >= 3)
+  int nitems, nsplit;        // items = cells x parts
+  int cap;                   // staged atoms per window
+};
+
+// Sums of one i-atom over its lanes' pairs (registers after inlining).
+struct WinAcc {
+  float fx, fy, fz, sx, sy, sz;   // FP32 chunk sums
+  double Fx, Fy, Fz, Sx, Sy, Sz, elj_hi;
+  float e[EP_COUNT];
+  int cnt;
+  unsigned under;
+};
+
+// Where an i-atom's j-atoms come from.
+//   SRC_WIN:    the staged window of its cell (periodic shift applied)
+//   SRC_GLOBAL: global memory (shift from the entry's code): a work item
+//               whose window did not fit
+enum { SRC_WIN = 0, SRC_GLOBAL = 1 };
+struct WinSrc {
+  const float4 *wx;              // staged positions (shift applied) + charge
+  const unsigned short *wt;      // staged types
+  const int *delta;              // window index = sorted index + delta[code]
+  unsigned wlast;                // staged atoms - 1
+  const float4 *xq;              // global: cell-relative positions + charge
+  const int *styp;
+  const float4 *shift;           // global: 27 hi shifts; shift_lo: 27 lo
+  const float4 *shift_lo;
+};
+// The tables of the atom's system.
+struct PairTab {
+  const float4 *tl, *te;         // LJ (3 float4 per knot) and erfc (2 per knot) coefficients
+  const float *fcut;             // 8 floats per interaction
+  const int *map;                // ntypes^2 interaction indices
+  int ntypes;
+  float rc2_el, dx2c, offc;
+};
+
+__device__ __forceinline__ void win_flush(WinAcc &A, bool need_s) {
+  A.Fx += A.fx; A.Fy += A.fy; A.Fz += A.fz;
+  A.fx = A.fy = A.fz = 0.f;
+  if (need_s) {
+    A.Sx += A.sx; A.Sy += A.sy; A.Sz += A.sz;
+    A.sx = A.sy = A.sz = 0.f;
+  }
+}
+
+// One segment [lo, hi) of atom i's slot.  LJ: the front segment (pairs in an
+// LJ list; their electrostatics too when HAS_EL); otherwise the back segment
+// (electrostatics only) or an electrostatics-only pass over the front.  The
+// arithmetic is branch-free: a pair that is not in range -- past the segment,
+// beyond the cut-off, or without the list flag -- contributes exact zeros
+// (its charge product and table weight are selected to 0), and every table
+// and window index is clamped in bounds.
+template <int TPA, bool NEED_S, bool HAS_EL, bool LJ, int SRC>
+__device__ __forceinline__ void win_segment(const MixedP &P, const WinSrc &S, const PairTab &T,
+                                            const uint32_t *__restrict__ nbr, long long lo, long long hi, int g,
+                                            float4 xi, int ti, WinAcc &A) {
+  const uint32_t fl_lj = P.iflg == 1 ? ENT_LJ : ENT_LJS;
+  const uint32_t fl_el = P.iflg == 1 ? ENT_EL : ENT_ELS;
+  const int ntm2 = P.ntable - 2;
+  auto pair = [&](uint32_t en, bool valid) {
+    en = valid ? en : (13u << ENT_CODE_SHIFT);      // sorted atom 0, zero shift, no list flag
+    const int code = (en >> ENT_CODE_SHIFT) & 31;
+    const int u = (int)(en & ENT_JMASK);
+    float4 xj;
+    int tj = 0;
+    float dx, dy, dz;
+    if (SRC == SRC_WIN) {
+      unsigned jl = (unsigned)(u + S.delta[code]);
+      jl = jl < S.wlast ? jl : S.wlast;
+      xj = S.wx[jl];
+      if (LJ) tj = S.wt[jl];
+      dx = xi.x - xj.x;
+      dy = xi.y - xj.y;
+      dz = xi.z - xj.z;
+    } else {
+      xj = S.xq[u];
+      if (LJ) tj = S.styp[u];
+      const float4 sh = S.shift[code], shl = S.shift_lo[code];
+      dx = ((xi.x - xj.x) + sh.x) + shl.x;
+      dy = ((xi.y - xj.y) + sh.y) + shl.y;
+      dz = ((xi.z - xj.z) + sh.z) + shl.z;
+    }
+    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    float ftot = 0.f, fsh = 0.f;
+    if (HAS_EL) {
+      const bool ok = (en & fl_el) != 0 && r2 < T.rc2_el;
+      const float p = fmaf(r2, T.dx2c, -T.offc);
+      int kk = (int)p;
+      A.under += (ok && kk < 1) ? 1u : 0u;
+      // below the table: CM3D's clamp (kk = 1, p = 1: the first knot)
+      const float fr = ok && kk >= 1 ? p - (float)kk : 0.f;
+      kk = kk < 1 ? 1 : (kk > ntm2 ? ntm2 : kk);
+      const float4 c0 = T.te[2 * kk];
+      const float qq = ok ? xi.w * xj.w : 0.f;
+      const float fe = qq * poly(fr, c0.x, c0.y, c0.z);
+      ftot = fe;
+      if (P.iflg == 1) {
+        const float4 c1 = T.te[2 * kk + 1];
+        A.e[EP_EEL] = fmaf(qq, poly(fr, c0.w, c1.x, c1.y), A.e[EP_EEL]);
+        A.e[EP_QQ] += qq;
+        const float fdx = fe * dx, fdy = fe * dy, fdz = fe * dz;
+        A.e[EP_VE0] = fmaf(fdx, dx, A.e[EP_VE0]);
+        A.e[EP_VE1] = fmaf(fdx, dy, A.e[EP_VE1]);
+        A.e[EP_VE2] = fmaf(fdx, dz, A.e[EP_VE2]);
+        A.e[EP_VE4] = fmaf(fdy, dy, A.e[EP_VE4]);
+        A.e[EP_VE5] = fmaf(fdy, dz, A.e[EP_VE5]);
+        A.e[EP_VE8] = fmaf(fdz, dz, A.e[EP_VE8]);
+        if (NEED_S) fsh = fe;                        // force_e's switch is never engaged
+      }
+    }
+    if (LJ) {
+      const bool isl = (en & fl_lj) != 0;
+      int in = T.map[ti * T.ntypes + tj];
+      in = in < 0 ? 0 : in;
+      // {rmaxl_cut2, rmins_cut2 dx2tab, dx2tab, vt} {rminl_cut2, rmaxs_cut2, -, -}
+      const float4 cA = reinterpret_cast<const float4 *>(T.fcut)[2 * in];
+      const bool needB = P.iflg == 0 || NEED_S;
+      const float4 cB = needB ? reinterpret_cast<const float4 *>(T.fcut)[2 * in + 1] : cA;
+      const bool ok = isl && r2 < (P.iflg == 1 ? cA.x : cB.y);
+      const float p = fmaf(r2, cA.z, -cA.y);
+      int kk = (int)p;
+      A.under += (ok && kk < 1) ? 1u : 0u;
+      const float fr = ok && kk >= 1 ? p - (float)kk : 0.f;
+      kk = kk < 1 ? 1 : (kk > ntm2 ? ntm2 : kk);
+      const float4 *Tk = T.tl + 3 * ((size_t)in * P.ntable + kk);
+      const float4 a0 = Tk[0], a1 = Tk[1], a2 = Tk[2];
+      const float okf = ok ? 1.f : 0.f;
+      const float f = okf * poly(fr, a0.x, a0.y, a0.z);
+      const float swv = (needB && r2 > cB.x) ? poly(fr, a1.z, a1.w, a2.x) : 1.f;
+      if (P.iflg == 1) {
+        ftot += f;
+        // V = v0 + p (vA + p vB) with v0 = hi (a0.w) + lo (a2.y): the hi
+        // parts are summed in FP64, so that an LJ energy whose pair terms
+        // cancel keeps FP64-like accuracy
+        A.elj_hi += ok ? (double)a0.w : 0.0;
+        const float vlo = okf * (a2.y + fr * fmaf(fr, a1.y, a1.x));
+        A.e[EP_ELJ] += vlo;
+        A.e[EP_ELJH] = fmaf(-okf, cA.w, A.e[EP_ELJH] + vlo);
+        const float fdx = f * dx, fdy = f * dy, fdz = f * dz;
+        A.e[EP_VL0] = fmaf(fdx, dx, A.e[EP_VL0]);
+        A.e[EP_VL1] = fmaf(fdx, dy, A.e[EP_VL1]);
+        A.e[EP_VL2] = fmaf(fdx, dz, A.e[EP_VL2]);
+        A.e[EP_VL4] = fmaf(fdy, dy, A.e[EP_VL4]);
+        A.e[EP_VL5] = fmaf(fdy, dz, A.e[EP_VL5]);
+        A.e[EP_VL8] = fmaf(fdz, dz, A.e[EP_VL8]);
+        if (NEED_S) fsh = fmaf(f, swv, fsh);
+      } else {
+        ftot = fmaf(f, swv, ftot);
+      }
+    }
+    // F_i = -f d  (md_fnopol.c:227-229)
+    A.fx = fmaf(-ftot, dx, A.fx);
+    A.fy = fmaf(-ftot, dy, A.fy);
+    A.fz = fmaf(-ftot, dz, A.fz);
+    if (NEED_S) {
+      A.sx = fmaf(-fsh, dx, A.sx);
+      A.sy = fmaf(-fsh, dy, A.sy);
+      A.sz = fmaf(-fsh, dz, A.sz);
+    }
+  };
+  // lane g owns the 16-byte vectors at la + 4 g + 4 TPA m (la: lo rounded
+  // down to a vector boundary; slots start on 128-byte boundaries since
+  // stride is a multiple of 32).  A vector that starts below hi ends inside
+  // the slot.  The next vector is loaded while the current one is used.
+  constexpr int STEP = 4 * TPA;
+  const long long la = lo & ~3LL;
+  long long kb = la + 4 * g;
+  uint4 nxt = make_uint4(0u, 0u, 0u, 0u);
+  if (kb < hi) nxt = __ldg(reinterpret_cast<const uint4 *>(nbr + kb));
+  for (; kb < hi; kb += STEP) {
+    const uint4 cur = nxt;
+    if (kb + STEP < hi) nxt = __ldg(reinterpret_cast<const uint4 *>(nbr + kb + STEP));
+    pair(cur.x, kb >= lo && kb < hi);
+    pair(cur.y, kb + 1 >= lo && kb + 1 < hi);
+    pair(cur.z, kb + 2 >= lo && kb + 2 < hi);
+    pair(cur.w, kb + 3 >= lo && kb + 3 < hi);
+    if (++A.cnt == 4) {                              // 16 pairs per FP32 chunk
+      win_flush(A, NEED_S);
+      A.cnt = 0;
+    }
+  }
+}
+
+template <int TPA, bool NEED_S, bool HAS_EL, int SRC>
+__device__ __forceinline__ void win_atom(const MixedP &P, const WinSrc &S, const PairTab &T,
+                                         const uint32_t *__restrict__ nbr, long long k0, int stride, int na, int nb,
+                                         int g, float4 xi, int ti, bool has_lj, bool has_el, WinAcc &A) {
+  // the front segment's pairs may carry charges too (an electrostatics-only
+  // call still walks it); a system without charges skips the electrostatic
+  // arithmetic altogether
+  const bool el = HAS_EL && has_el;
+  if (has_lj) {
+    if (el) win_segment<TPA, NEED_S, true, true, SRC>(P, S, T, nbr, k0, k0 + na, g, xi, ti, A);
+    else win_segment<TPA, NEED_S, false, true, SRC>(P, S, T, nbr, k0, k0 + na, g, xi, ti, A);
+  } else if (el) {
+    win_segment<TPA, NEED_S, true, false, SRC>(P, S, T, nbr, k0, k0 + na, g, xi, ti, A);
+  }
+  if (el) win_segment<TPA, NEED_S, true, false, SRC>(P, S, T, nbr, k0 + stride - nb, k0 + stride, g, xi, ti, A);
+  win_flush(A, NEED_S);
+}
+
+template <int TPA, bool NEED_S, bool HAS_EL>
+__global__ void __launch_bounds__(512, 1) k_pair_win(
+    MixedP P, WinP W, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
+    const int *__restrict__ cell_start, const int *__restrict__ nlen, int stride, const uint32_t *__restrict__ nbr,
+    const float4 *__restrict__ gshift, const int *__restrict__ gmap, const float *__restrict__ gfcut,
+    const float4 *__restrict__ gtl, const float4 *__restrict__ gte, double *__restrict__ fout,
+    double *__restrict__ fshort, float *__restrict__ epart, double *__restrict__ epart64,
+    long long *__restrict__ stat, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  extern __shared__ float4 sm[];
+  float4 *shift = sm;                                   // 27 hi + 27 lo
+  float *fcut = reinterpret_cast<float *>(sm + 54);     // 8 * ninter
+  const int nf4 = (8 * P.ninter + 3) / 4;
+  int *map = reinterpret_cast<int *>(sm + 54 + nf4);    // ntypes^2
+  const int nm4 = (P.ntypes * P.ntypes + 3) / 4;
+  float4 *tl = sm + 54 + nf4 + nm4;                     // LJ tables (3 * ninter * ntable)
+  const int nl = (P.mask & 1) ? 3 * P.ninter * P.ntable : 0;
+  float4 *te = tl + nl;                                 // erfc table (2 * ntable)
+  const int ne = HAS_EL ? 2 * P.ntable : 0;
+  float4 *wx = te + ne;                                 // staged window: cap float4
+  unsigned short *wt = reinterpret_cast<unsigned short *>(wx + W.cap);   // cap types
+  __shared__ int s_cs[27], s_cnt[27], s_off[27], s_delta[32], s_tot;
+
+  for (int k = threadIdx.x; k < 54; k += blockDim.x) shift[k] = gshift[k];
+  for (int k = threadIdx.x; k < 8 * P.ninter; k += blockDim.x) fcut[k] = gfcut[k];
+  for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) map[k] = gmap[k];
+  for (int k = threadIdx.x; k < nl; k += blockDim.x) tl[k] = gtl[k];
+  for (int k = threadIdx.x; k < ne; k += blockDim.x) te[k] = gte[k];
+
+  const int g = threadIdx.x % TPA;
+  const int groups = blockDim.x / TPA;
+  const bool has_lj = (P.mask & 1) != 0;
+  unsigned under = 0;
+
+  for (int item = blockIdx.x; item < W.nitems; item += gridDim.x) {
+    const int c = item / W.nsplit, part = item - c * W.nsplit;
+    const int cz = c % W.ncz, cy = (c / W.ncz) % W.ncy, cx = c / (W.ncz * W.ncy);
+    __syncthreads();                                     // the previous window is no longer read
+    if (threadIdx.x < 32) {
+      // window cell w = shift code: j-cell = i-cell - k, k = (w/9-1, w/3%3-1, w%3-1)
+      const int w = threadIdx.x;
+      int cnt = 0, cs = 0;
+      if (w < 27) {
+        int jx = cx - (w / 9 - 1), jy = cy - ((w / 3) % 3 - 1), jz = cz - (w % 3 - 1);
+        jx = jx < 0 ? jx + W.ncx : (jx >= W.ncx ? jx - W.ncx : jx);
+        jy = jy < 0 ? jy + W.ncy : (jy >= W.ncy ? jy - W.ncy : jy);
+        jz = jz < 0 ? jz + W.ncz : (jz >= W.ncz ? jz - W.ncz : jz);
+        const int jc = (jx * W.ncy + jy) * W.ncz + jz;
+        cs = cell_start[jc];
+        cnt = cell_start[jc + 1] - cs;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (w >= o) incl += v;
+      }
+      if (w < 27) {
+        s_cs[w] = cs;
+        s_cnt[w] = cnt;
+        s_off[w] = incl - cnt;
+      }
+      s_delta[w] = w < 27 ? incl - cnt - cs : 0;       // codes 27..31 never occur
+      if (w == 26) s_tot = incl;
+    }
+    __syncthreads();
+    const int wtot = s_tot;
+    const bool staged = wtot <= W.cap;
+    if (staged) {
+      for (int w = 0; w < 27; w++) {
+        const int cs = s_cs[w], cnt = s_cnt[w], off = s_off[w];
+        const float4 sh = shift[w], shl = shift[27 + w];
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+          const float4 x = xq[cs + k];
+          wx[off + k] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
+          if (has_lj) wt[off + k] = (unsigned short)styp[cs + k];
+        }
+      }
+    }
+    __syncthreads();
+    WinSrc S;
+    S.wx = wx;
+    S.wt = wt;
+    S.delta = s_delta;
+    S.wlast = (unsigned)(wtot > 0 ? wtot - 1 : 0);
+    S.xq = xq;
+    S.styp = styp;
+    S.shift = shift;
+    S.shift_lo = shift + 27;
+    PairTab T;
+    T.tl = tl;
+    T.te = te;
+    T.fcut = fcut;
+    T.map = map;
+    T.ntypes = P.ntypes;
+    T.rc2_el = P.rc2_el;
+    T.dx2c = P.dx2c;
+    T.offc = P.offc;
+    const int ci0 = s_cs[13], cin = s_cnt[13], ioff = s_off[13];
+    for (int r = part; r * groups < cin; r += W.nsplit) {
+      const int a = r * groups + threadIdx.x / TPA;
+      const bool active = a < cin;
+      const int t = ci0 + (active ? a : 0);
+      WinAcc A;
+      A.fx = A.fy = A.fz = A.sx = A.sy = A.sz = 0.f;
+      A.Fx = A.Fy = A.Fz = A.Sx = A.Sy = A.Sz = A.elj_hi = 0.0;
+#pragma unroll
+      for (int k = 0; k < EP_COUNT; k++) A.e[k] = 0.f;
+      A.cnt = 0;
+      A.under = 0;
+      if (active) {
+        // the centre cell's shift is zero: staged i and xq agree exactly
+        const float4 xi = staged ? wx[ioff + a] : xq[t];
+        const int ti = has_lj ? styp[t] : 0;
+        const int na = nlen[t], nb = nlen[P.n + t];
+        const long long k0 = (long long)t * stride;
+        if (staged)
+          win_atom<TPA, NEED_S, HAS_EL, SRC_WIN>(P, S, T, nbr, k0, stride, na, nb, g, xi, ti, has_lj, true, A);
+        else
+          win_atom<TPA, NEED_S, HAS_EL, SRC_GLOBAL>(P, S, T, nbr, k0, stride, na, nb, g, xi, ti, has_lj, true, A);
+      }
+      under += A.under;
+#pragma unroll
+      for (int o = TPA / 2; o > 0; o >>= 1) {
+        A.Fx += __shfl_xor_sync(0xffffffffu, A.Fx, o);
+        A.Fy += __shfl_xor_sync(0xffffffffu, A.Fy, o);
+        A.Fz += __shfl_xor_sync(0xffffffffu, A.Fz, o);
+        if (NEED_S) {
+          A.Sx += __shfl_xor_sync(0xffffffffu, A.Sx, o);
+          A.Sy += __shfl_xor_sync(0xffffffffu, A.Sy, o);
+          A.Sz += __shfl_xor_sync(0xffffffffu, A.Sz, o);
+        }
+        if (P.iflg == 1) {
+#pragma unroll
+          for (int k = 0; k < EP_COUNT; k++) A.e[k] += __shfl_xor_sync(0xffffffffu, A.e[k], o);
+          A.elj_hi += __shfl_xor_sync(0xffffffffu, A.elj_hi, o);
+        }
+      }
+      if (active && g == 0) {
+        const int i = sorig[t], n = P.n;
+        fout[i] += A.Fx;
+        fout[n + i] += A.Fy;
+        fout[2 * n + i] += A.Fz;
+        if (NEED_S && P.iflg == 1) {
+          fshort[i] += A.Sx;
+          fshort[n + i] += A.Sy;
+          fshort[2 * n + i] += A.Sz;
+        }
+        if (P.iflg == 1) {
+#pragma unroll
+          for (int k = 0; k < EP_COUNT; k++) epart[(size_t)k * n + t] = A.e[k];
+          epart64[t] = A.elj_hi;
+        }
+      }
+    }
+  }
+  if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), (unsigned long long)under);
+}
+
+// Gather kernel: batches, and single systems whose cell grid is too coarse
+// for the windowed kernel (or when that kernel is switched off).  Its lane
+// groups read j-atoms from global memory (L1/L2: a batch's systems are
+// small) and skip out-of-range pairs by branching, which suits short lists
+// where a good share of the listed pairs lies beyond the cut-off.
+//
 // BATCH = false: one system, its parameters in P and its shifts, cut-offs,
 // type map and (when they fit) tables staged in shared memory.  BATCH = true:
 // several systems; each atom group reads its system's parameters, shifts and
@@ -122,7 +505,10 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
     if (active) {
       const float4 xi = xq[t];
       const int ti = styp[t];
-      const long long k0 = (long long)t * stride, k1 = k0 + nlen[t];
+      // the slot's two segments: LJ-list pairs at the front, pairs in the
+      // electrostatic lists only at the back
+      const long long k0 = (long long)t * stride;
+      const long long seg[4] = {k0, k0 + nlen[t], k0 + stride - nlen[P.n + t], k0 + stride};
       float fx = 0, fy = 0, fz = 0, sx = 0, sy = 0, sz = 0;
       int cnt = 0;
       // this atom's system: shifts, type map, cut-offs and tables
@@ -238,7 +624,8 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
       // that PU independent loads are in flight; FP32 sums go to FP64 every
       // 16 pairs.  Entry 0 marks the end (a real entry has a list flag set).
       constexpr int PU = 4;
-      for (long long kb = k0 + g; kb < k1; kb += PU * TPA) {
+      for (int sg = 0; sg < 2; sg++)
+      for (long long kb = seg[2 * sg] + g, k1 = seg[2 * sg + 1]; kb < k1; kb += PU * TPA) {
         uint32_t en[PU];
         float4 xj[PU];
         int tj[PU];
@@ -312,14 +699,22 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
 // FP64 sums of the per-atom partials into CM3D's accumulators (one block per
 // quantity and system, fixed order: deterministic).  Every pair was seen from
 // both ends, hence the factor 1/2; CM3D's virials are -sum d_a d_b f.
+//
+// A system's atoms may be split over gridDim.z blocks (one large system): each
+// block stores its partial sum, and the last block of a quantity to finish
+// adds the partials in block order -- the result does not depend on which
+// block finished last -- and re-arms the counter for the next launch.
 __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const float *__restrict__ epart,
                           const double *__restrict__ epart64, double *__restrict__ accs,
-                          const int *__restrict__ gs) {
+                          double *__restrict__ part, unsigned *__restrict__ done, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   __shared__ double red[32];
-  const int q = blockIdx.x, sy = blockIdx.y;
+  __shared__ bool last;
+  const int q = blockIdx.x, sy = blockIdx.y, nz = gridDim.z;
   if (!((q < EP_EEL && (mask & 1)) || (q >= EP_EEL && (mask & 2)))) return;
-  const int a0 = sp[sy].a0, a1 = a0 + sp[sy].n;
+  const int sa0 = sp[sy].a0, sn = sp[sy].n;
+  const int chunk = (sn + nz - 1) / nz;
+  const int a0 = sa0 + blockIdx.z * chunk, a1 = min(sa0 + sn, a0 + chunk);
   const float tablast_e = sp[sy].tablast_e;
   double *acc = accs + (size_t)sy * ACC_STRIDE;
   // the LJ energies add the FP64 sums of the table's hi parts
@@ -330,9 +725,26 @@ __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const fl
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
-  if (threadIdx.x >= 32) return;
-  s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-  s = warp_sum(s);
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+  }
+  if (nz > 1) {
+    if (threadIdx.x == 0) {
+      part[(size_t)q * nz + blockIdx.z] = s;
+      __threadfence();
+      last = atomicAdd(done + q, 1u) == (unsigned)(nz - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const volatile double *pv = part + (size_t)q * nz;
+      s = 0;
+      for (int z = 0; z < nz; z++) s += pv[z];
+      done[q] = 0;
+    }
+  }
   if (threadIdx.x != 0) return;
   s *= 0.5;
   switch (q) {
@@ -356,6 +768,12 @@ __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const fl
 }
 
 // ------------------------------------------------------------------ host
+constexpr int EREDUCE_MAX_Z = 64;   // blocks per quantity for one large system
+
+// per-atom FP64 partials of the LJ energy's table hi parts, stored after the
+// EP_COUNT FP32 rows of epart
+static double *epart_hi(Ctx *c) { return reinterpret_cast<double *>(c->epart + (size_t)EP_COUNT * c->n); }
+
 static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
   size_t nf4 = (8 * (size_t)c->ninter + 3) / 4, nm4 = ((size_t)c->ntypes * c->ntypes + 3) / 4;
   size_t b = (54 + nf4 + nm4) * sizeof(float4);
@@ -365,10 +783,6 @@ static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
   }
   return b;
 }
-
-// per-atom FP64 partials of the LJ energy's table hi parts, stored after the
-// EP_COUNT FP32 rows of epart
-static double *epart_hi(Ctx *c) { return reinterpret_cast<double *>(c->epart + (size_t)EP_COUNT * c->n); }
 
 template <int TPA, bool SB, bool NS, bool BT>
 static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
@@ -407,7 +821,84 @@ static int launch_tpa(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   return CM3D_NB_OK;
 }
 
-bool g_smallbox_warned = false;
+// Windowed kernel for one system with >= 3 cells per axis: returns false
+// (nothing launched) when it does not apply and the list-gather kernel runs.
+// The window capacity is what shared memory leaves after the tables; an item
+// whose 27 cells hold more atoms falls back to global loads inside the kernel.
+constexpr size_t WIN_STATIC_SMEM = 1024;   // >= k_pair_win's static shared arrays (436 bytes)
+
+template <int TPA, bool NS, bool EL>
+static void launch_win_t(Ctx *c, const MixedP &P, const WinP &W, size_t smem, double *fout) {
+  auto kern = k_pair_win<TPA, NS, EL>;
+  // dynamic + static shared memory must fit the opt-in limit: the window
+  // budget keeps WIN_STATIC_SMEM bytes for the kernel's static arrays
+  static unsigned long long attr_devs = 0;
+  if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(c->smem_optin - WIN_STATIC_SMEM));
+    attr_devs |= 1ull << c->dev;
+  }
+  int grid = W.nitems < c->num_sms ? W.nitems : c->num_sms;
+  kern<<<grid, 512, smem, c->st>>>(P, W, c->xq, c->styp, c->cell_atoms, c->cell_start, c->nlen, c->nbr_stride,
+                                   c->nbr, c->shift, c->map, c->fcut, c->ftab_lj, c->ftab_el, fout, c->fxs, c->epart,
+                                   epart_hi(c), c->stat, c->gate);
+}
+
+template <int TPA>
+static void launch_win_tpa(Ctx *c, const MixedP &P, const WinP &W, size_t smem, double *fout, bool ns, bool el) {
+  if (ns) {
+    if (el) launch_win_t<TPA, true, true>(c, P, W, smem, fout);
+    else launch_win_t<TPA, true, false>(c, P, W, smem, fout);
+  } else {
+    if (el) launch_win_t<TPA, false, true>(c, P, W, smem, fout);
+    else launch_win_t<TPA, false, false>(c, P, W, smem, fout);
+  }
+}
+
+// whether the windowed kernel can run this context (shape only)
+bool win_applies(Ctx *c) {
+  return c->mode == CM3D_NB_MIXED && c->nsys == 1 && c->nc[0] >= 3 && c->nc[1] >= 3 && c->nc[2] >= 3 &&
+         c->ntypes <= 65535;
+}
+
+static bool launch_win(Ctx *c, const MixedP &P, bool ns, double *fout) {
+  if (!c->win_ok || !win_applies(c)) return false;
+  const int mask = P.mask;
+  size_t nf4 = (8 * (size_t)c->ninter + 3) / 4, nm4 = ((size_t)c->ntypes * c->ntypes + 3) / 4;
+  size_t fixed = (54 + nf4 + nm4) * sizeof(float4);
+  if (mask & 1) fixed += (size_t)3 * c->ninter * c->ntable * sizeof(float4);
+  if (mask & 2) fixed += (size_t)2 * c->ntable * sizeof(float4);
+  const size_t budget = c->smem_optin > WIN_STATIC_SMEM ? c->smem_optin - WIN_STATIC_SMEM : 0;
+  if (budget <= fixed) return false;
+  long long cap = (long long)((budget - fixed) / (sizeof(float4) + sizeof(unsigned short))) / 8 * 8;
+  const double mean_window = 27.0 * (double)c->n / (double)c->ncells;
+  if ((double)cap < 1.25 * mean_window) return false;
+  if (cap > 65536) cap = 65536;
+  WinP W;
+  W.ncx = c->nc[0];
+  W.ncy = c->nc[1];
+  W.ncz = c->nc[2];
+  W.cap = (int)cap;
+  const int groups = 512 / c->tpa;
+  const double per_cell = (double)c->n / (double)c->ncells;
+  int rounds = (int)ceil(per_cell / groups);
+  if (rounds < 1) rounds = 1;
+  // about four items per block where the cells allow it (parts of one cell
+  // restage its window, so no more than needed)
+  int want = (4 * c->num_sms + c->ncells - 1) / c->ncells;
+  W.nsplit = want < rounds ? want : rounds;
+  if (W.nsplit < 1) W.nsplit = 1;
+  W.nitems = c->ncells * W.nsplit;
+  const size_t smem = fixed + (size_t)cap * (sizeof(float4) + sizeof(unsigned short));
+  const bool el = (mask & 2) != 0;
+  switch (c->tpa) {
+    case 4: launch_win_tpa<4>(c, P, W, smem, fout, ns, el); break;
+    case 16: launch_win_tpa<16>(c, P, W, smem, fout, ns, el); break;
+    case 32: launch_win_tpa<32>(c, P, W, smem, fout, ns, el); break;
+    default: launch_win_tpa<8>(c, P, W, smem, fout, ns, el); break;
+  }
+  return true;
+}
 
 // mixed mode: which bit0 LJ, bit1 charges; iflg 1 -> fxl (+fxs), 0 -> fxs
 int mixed_pairs(Ctx *c, int iflg, int mask) {
@@ -446,7 +937,11 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
                                                   c->gate);
   cudaEvent_t e0;
   tbegin(c, 0, &e0);
-  if (c->nsys > 1) {
+  // one system with >= 3 cells per axis: staged 27-cell windows; anything
+  // else (batches, coarse cell grids): the gather kernel
+  c->pair_used = CM3D_NB_PAIR_WINDOW;
+  if (launch_win(c, P, ns, fout)) {
+  } else if ((c->pair_used = CM3D_NB_PAIR_GATHER), c->nsys > 1) {
     // several systems: per-system parameters and tables from global memory
     P.tab_smem = 0;
     if (ns) launch_tpa<false, true, true>(c, P, 0, fout);
@@ -461,8 +956,10 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   tend(c, 0, e0);
   c->launches += 2;
   if (iflg == 1) {
-    k_ereduce<<<dim3(EP_COUNT, c->nsys), c->nsys > 1 ? 256 : 1024, 0, c->st>>>(c->n, mask, c->sp, c->epart,
-                                                                                 epart_hi(c), c->acc, c->gate);
+    // one large system: its atoms over several blocks per quantity
+    const int nz = c->nsys > 1 ? 1 : std::max(1, std::min(EREDUCE_MAX_Z, c->n / 8192));
+    k_ereduce<<<dim3(EP_COUNT, c->nsys, nz), c->nsys > 1 ? 256 : 512, 0, c->st>>>(
+        c->n, mask, c->sp, c->epart, epart_hi(c), c->acc, c->ered, c->ered_done, c->gate);
     c->launches++;
   }
   CKL(c);
@@ -539,6 +1036,9 @@ int pair_setup(Ctx *c) {
   CK(cudaMemcpy(c->fcut, fc.data(), sizeof(float) * fc.size(), cudaMemcpyHostToDevice));
   // (the 27 cell shifts H k / nc are set up with the cell grid, list_setup)
   CK(cudaMalloc(&c->epart, (sizeof(float) * EP_COUNT + sizeof(double)) * (size_t)c->n));
+  CK(cudaMalloc(&c->ered, sizeof(double) * EP_COUNT * EREDUCE_MAX_Z));
+  CK(cudaMalloc(&c->ered_done, sizeof(unsigned) * EP_COUNT));
+  CK(cudaMemset(c->ered_done, 0, sizeof(unsigned) * EP_COUNT));
   if (c->tpa == 0) {
     // 8 lanes per atom: a group reads a full 32-byte sector of the list; more
     // lanes only for systems too small to fill the GPU

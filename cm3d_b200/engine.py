@@ -99,6 +99,7 @@ def load_library() -> C.CDLL:
         "cm3d_nb_launch_count": (ll, [vp]),
         "cm3d_nb_measure_peaks": (C.c_int, [C.c_int, dp, dp]),
         "cm3d_nb_autotune": (C.c_int, [vp, C.c_int, ip, dp]),
+        "cm3d_nb_pair_kernel": (C.c_int, [vp, ip, ip]),
         "cm3d_nb_lj_table": (C.c_int, [C.c_double] * 7 + [C.c_int, C.c_int, dp, dp, dp, dp]),
         "cm3d_nb_coul_table": (C.c_int, [C.c_double] * 6 + [C.c_int, C.c_int, C.c_int, dp, dp, dp, dp]),
         "cm3d_nb_ewald_kvectors": (C.c_int, [C.c_int, ip, ip, ip, ip, ip]),
@@ -259,12 +260,20 @@ class Engine:
         return {"velec": v.value, "welec": w.value, "welectensor": t}
 
     def autotune(self, reps: int = 5) -> dict:
-        """Pick the pair kernel's lanes per atom by timing 4/8/16/32 on the
-        current lists (cm3d_nb_autotune); returns the choice and the timings."""
+        """Pick the pair kernel (gather or window) and its lanes per atom by
+        timing 4/8/16/32 on the current lists (cm3d_nb_autotune); returns the
+        choice and, per lanes-per-atom choice, the faster kernel's time."""
         t = C.c_int(0)
         ms = np.zeros(4)
         check(load_library().cm3d_nb_autotune(self._h, reps, C.byref(t), _p(ms)), "autotune")
-        return {"tpa": int(t.value), "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
+        return {"tpa": int(t.value), "kernel": self.pair_kernel()[0],
+                "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
+
+    def pair_kernel(self) -> tuple[str, int]:
+        """(kernel of the last pair launch: "gather" or "window", lanes per atom)"""
+        k, t = C.c_int(0), C.c_int(0)
+        check(load_library().cm3d_nb_pair_kernel(self._h, C.byref(k), C.byref(t)), "pair_kernel")
+        return ("window" if k.value == 1 else "gather"), int(t.value)
 
     def system_energies(self, sys: int) -> dict:
         """getvireal + geteng of one system of a batch"""

@@ -280,12 +280,24 @@ long long cm3d_nb_launch_count(cm3d_nb_ctx *ctx);
    CUDA-core pair and k-space kernels.  No CM3D counterpart. */
 int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops);
 /* Autotuner of the mixed pair kernel (no CM3D counterpart): times the fused
-   LJ + real-space Ewald kernel with 4, 8, 16 and 32 lanes per atom on the
-   context's current lists (reps launches each, CUDA events), keeps the
-   fastest, and recomputes force(1) so the state is as before.  Call after
-   cm3d_nb_get_ngbr or cm3d_nb_step_init.  ms_per_launch[4] (may be NULL)
-   receives the four timings. */
+   LJ + real-space Ewald kernels (below) with 4, 8, 16 and 32 lanes per atom
+   on the context's current lists (reps launches each, CUDA events), keeps
+   the fastest, and recomputes force(1) so the state is as before.  Call
+   after cm3d_nb_get_ngbr or cm3d_nb_step_init.  ms_per_launch[4] (may be
+   NULL) receives, per lanes-per-atom choice, the time of the faster kernel. */
 int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]);
+/* The mixed pair kernels (no CM3D counterpart).  GATHER: lane groups read
+   j-atoms from global memory; batches and coarse cell grids always use it.
+   WINDOW: one system with >= 3 cells per axis; a block stages the 27 cells
+   around an i-cell in shared memory.  cm3d_nb_autotune times both (where the
+   box allows the window) at every lanes-per-atom choice, keeps the fastest,
+   and ms_per_launch[k] is the faster of the two at that choice.
+   CM3D_NB_PAIR_KERNEL=list in the environment at cm3d_nb_create keeps a
+   context on the gather kernel.  cm3d_nb_pair_kernel reports the kernel of
+   the last pair launch and the lanes per atom. */
+#define CM3D_NB_PAIR_GATHER 0
+#define CM3D_NB_PAIR_WINDOW 1
+int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
 
 /* ------------------------------------------- no-allocation variant */
 #define CM3D_NB_NOALLOC_MAX_CHARGES 32768   /* charged atoms per call */

@@ -1,7 +1,8 @@
 """The pair-kernel autotuner (cm3d_nb_autotune): it picks one of the
-candidate lane counts, leaves forces and energies as they were (the lane
-count only reorders FP32 partial sums: relative 1e-6), and a trajectory
-continues after it exactly as the mixed engine's bound requires."""
+candidate lane counts and, for a single system with 3 or more cells per axis,
+the gather or the windowed kernel; it leaves forces and energies as they were
+(lane count and kernel only reorder FP32 partial sums: relative 1e-6), and a
+trajectory continues after it exactly as the mixed engine's bound requires."""
 import numpy as np
 import pytest
 
@@ -13,7 +14,8 @@ from cm3d_b200.system import System
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("names", [["water216"], ["argon864", "binary256"]], ids=["single", "batch"])
+@pytest.mark.parametrize("names", [["water216"], ["water4096"], ["argon864", "binary256"]],
+                         ids=["single", "single-window", "batch"])
 def test_autotune_keeps_state(engine_lib, names):
     ds = [golden(n) for n in names]
     e = Engine([System.from_arrays(d) for d in ds], mode=_abi.MIXED)
@@ -22,6 +24,9 @@ def test_autotune_keeps_state(engine_lib, names):
     en0 = e.all_energies()
     res = e.autotune(reps=3)
     assert res["tpa"] in (4, 8, 16, 32)
+    assert res["kernel"] in ("gather", "window")
+    if len(names) > 1 or names[0] == "water216":
+        assert res["kernel"] == "gather"          # batches and coarse grids: gather only
     assert all(v > 0 for v in res["ms_per_launch"].values())
     f1 = e.forces(_abi.FXL)
     en1 = e.all_energies()

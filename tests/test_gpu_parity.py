@@ -199,6 +199,32 @@ def test_errors_are_reported(engine_lib):
         Engine(bad)
 
 
+@pytest.mark.parametrize("name", ["argon864", "water4096"])
+def test_window_kernel_matches_list_kernel(engine_lib, name, monkeypatch):
+    """Boxes with >= 3 cells per axis run the staged-window pair kernel; the
+    list-gather kernel (CM3D_NB_PAIR_KERNEL=list) evaluates the same pairs
+    in another order.  Both stay within the mixed tolerance of CM3D, and of
+    each other at FP32 summation-order level."""
+    d = golden(name)
+    out = {}
+    for kind in ("window", "list"):
+        if kind == "list":
+            monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", "list")
+        else:
+            monkeypatch.delenv("CM3D_NB_PAIR_KERNEL", raising=False)
+        e = Engine(System.from_arrays(d), mode=_abi.MIXED)
+        e.get_ngbr()
+        e.force(1)
+        out[kind] = (e.forces(_abi.FXL), e.energies())
+        e.close()
+    fs = force_scale(d) / float(np.sqrt((d["amass"] ** 2).mean()))
+    for kind in ("window", "list"):
+        assert rel_rms(out[kind][0], xyz(d, "acc_l"), fs) <= FTOL[_abi.MIXED], kind
+    assert rel_rms(out["window"][0], out["list"][0], fs) <= 1e-6
+    for k in ("vinter", "velec", "W"):
+        assert close(out["window"][1][k], out["list"][1][k], 1e-6), k
+
+
 def test_status_counts_resets(engine_lib):
     """water216 starts hot: CM3D's RESETPOS fires (reference log: 12 resets in
     20 steps); the engine counts the same events in plain FP64"""
