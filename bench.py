@@ -189,18 +189,19 @@ def e2e_run(eng, steps: int, istep0: int, n: int) -> tuple[float, int, int]:
     px, vx = [pinned(3 * n).reshape(3, n) for _ in range(2)]
     px[:] = eng.positions()
     vx[:] = eng.velocities()
+    etab = eng.energies_table()
     eng.synchronize()
     t0 = time.perf_counter()
     for s in range(steps):
         eng.set_positions(px)
         eng.set_velocities(vx)
         eng.step(istep0 + s, 1)
-        px[:] = eng.positions()
-        vx[:] = eng.velocities()
-        eng.all_energies()
+        eng.positions(out=px)
+        eng.velocities(out=vx)
+        eng.energies_table(out=etab)
     dt = time.perf_counter() - t0
     h2d = 2 * 3 * n * 8
-    d2h = 2 * 3 * n * 8 + 96 * 8 * eng.nsys
+    d2h = 2 * 3 * n * 8 + 104 * 8 * eng.nsys     # + every system's accumulator block (ACC_STRIDE doubles)
     return dt, h2d, d2h
 
 

@@ -67,6 +67,13 @@ class Energies(C.Structure):
         ("poter", C.c_double), ("poth", C.c_double), ("potra", C.c_double),
     ]
 
+    @classmethod
+    def numpy_dtype(cls):
+        """numpy structured dtype with the struct's layout (tensors as (9,))"""
+        import numpy as np
+        return np.dtype([(name, np.float64, (9,)) if issubclass(typ, C.Array) else (name, np.float64)
+                         for name, typ in cls._fields_])
+
     def as_dict(self) -> dict:
         out = {}
         for name, typ in self._fields_:

@@ -183,32 +183,38 @@ class Engine:
         self.close()
 
     # --------------------------------------------------------- transfers
-    def _get3(self, fn, *lead) -> np.ndarray:
-        x, y, z = (np.empty(self.n) for _ in range(3))
-        check(fn(self._h, *lead, _p(x), _p(y), _p(z)), fn.__name__)
-        return np.stack([x, y, z])
+    def _get3(self, fn, *lead, out=None) -> np.ndarray:
+        """x | y | z blocks into a new (3, n) array, or into `out` (a C-contiguous
+        float64 (3, n) array, e.g. in pinned host memory: the copies then go
+        straight into it)"""
+        if out is None:
+            out = np.empty((3, self.n))
+        elif out.shape != (3, self.n) or out.dtype != np.float64 or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of shape (3, {self.n})")
+        check(fn(self._h, *lead, _p(out[0]), _p(out[1]), _p(out[2])), fn.__name__)
+        return out
 
     def _set3(self, fn, a, *lead) -> None:
         a = np.asarray(a, dtype=np.float64)
         x, y, z = (np.ascontiguousarray(a[k]) for k in range(3))
         check(fn(self._h, *lead, _p(x), _p(y), _p(z)), fn.__name__)
 
-    def positions(self) -> np.ndarray:
-        return self._get3(load_library().cm3d_nb_get_positions)
+    def positions(self, out=None) -> np.ndarray:
+        return self._get3(load_library().cm3d_nb_get_positions, out=out)
 
     def set_positions(self, p) -> None:
         self._set3(load_library().cm3d_nb_set_positions, p)
 
-    def velocities(self) -> np.ndarray:
-        return self._get3(load_library().cm3d_nb_get_velocities)
+    def velocities(self, out=None) -> np.ndarray:
+        return self._get3(load_library().cm3d_nb_get_velocities, out=out)
 
     def set_velocities(self, v) -> None:
         self._set3(load_library().cm3d_nb_set_velocities, v)
 
-    def forces(self, which: int = _abi.FXL) -> np.ndarray:
+    def forces(self, which: int = _abi.FXL, out=None) -> np.ndarray:
         """The stored force block (accelerations after rmass, raw forces after
         force_ter/force_ter_e/fk_ewald/ecorr alone)."""
-        return self._get3(load_library().cm3d_nb_get_forces, which)
+        return self._get3(load_library().cm3d_nb_get_forces, which, out=out)
 
     def set_forces(self, f, which: int = _abi.FXL) -> None:
         L = load_library()
@@ -285,6 +291,21 @@ class Engine:
         arr = (_abi.Energies * self.nsys)()
         check(load_library().cm3d_nb_get_all_energies(self._h, arr), "get_all_energies")
         return [arr[k].as_dict() for k in range(self.nsys)]
+
+    def energies_table(self, out=None) -> np.ndarray:
+        """Every system's getvireal + geteng as one numpy structured array
+        (fields of cm3d_nb_energies, one row per system), written into `out`
+        when given: no per-system Python objects, for a host loop that reads
+        all systems every step."""
+        dt = _abi.Energies.numpy_dtype()
+        assert dt.itemsize == C.sizeof(_abi.Energies)
+        if out is None:
+            out = np.empty(self.nsys, dtype=dt)
+        elif out.dtype != dt or out.shape != (self.nsys,) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous energies_table array of this engine")
+        check(load_library().cm3d_nb_get_all_energies(self._h, out.ctypes.data_as(C.POINTER(_abi.Energies))),
+              "get_all_energies")
+        return out
 
     def system_counts(self) -> tuple[np.ndarray, np.ndarray]:
         """per-system (list rebuilds, RESETPOS events)"""

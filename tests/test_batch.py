@@ -135,6 +135,27 @@ def test_batch_trajectory(engine_lib, group, graph, monkeypatch):
         assert rb[s] == rb1[0] and rs[s] == rs1[0], (names[s], rb[s], rb1[0], rs[s], rs1[0])
 
 
+def test_host_buffers_and_energies_table(engine_lib):
+    """positions/velocities into caller arrays (e.g. pinned) and the
+    structured energies table give what the allocating calls give"""
+    ds, e = batch(GROUPS["water"])
+    e.step_init()
+    e.step(1, 2)
+    px = np.empty((3, e.n))
+    assert e.positions(out=px) is px
+    np.testing.assert_array_equal(px, e.positions())
+    vx = np.empty((3, e.n))
+    np.testing.assert_array_equal(e.velocities(out=vx), e.velocities())
+    with pytest.raises(ValueError):
+        e.positions(out=np.empty((e.n, 3)))
+    tab = e.energies_table()
+    for s, en in enumerate(e.all_energies()):
+        for k in ("poter", "vinter", "velec", "vewald", "prsi", "zke"):
+            assert tab[k][s] == en[k], k
+        np.testing.assert_array_equal(tab["prs_tensor"][s], en["prs_tensor"])
+    e.close()
+
+
 def test_batch_rejects_mismatched_steps(engine_lib):
     with pytest.raises(EngineError, match="dt"):
         batch(["argon864", "water216"])
