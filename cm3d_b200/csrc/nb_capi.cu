@@ -86,7 +86,7 @@ static void destroy(Ctx *c) {
                   c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
                   c->cimg, c->nlen, c->acc,
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
-                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done};
+                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -275,6 +275,8 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
     // interactions: global indices inter0 + local, type map per system
     P.ntypes = s->ntypes;
     P.map0 = (int)map.size();
+    P.inter0 = inter0;
+    P.ninter = s->ninter;
     for (int k = 0; k < s->ntypes * s->ntypes; k++) map.push_back(s->map[k] >= 0 ? inter0 + s->map[k] : -1);
     double r2 = 0;
     for (int in = 0; in < s->ninter; in++) {
@@ -1066,8 +1068,9 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   c->timing.on = false;
   if (ms_per_launch)
     for (int k = 0; k < 4; k++) ms_per_launch[k] = 1e300;
-  // the gather kernel, then (where the box allows it) the windowed kernel:
-  // a single system runs whichever is faster on its live lists
+  // the gather kernel, then (where it applies) the staged kernel -- a single
+  // system's 27-cell windows, or a batch's whole systems: the context runs
+  // whichever is faster on its live lists
   for (int win = 0; win <= (c->win_env_off ? 0 : 1); win++) {
     c->win_ok = win;
     for (int k = 0; k < 4; k++) {

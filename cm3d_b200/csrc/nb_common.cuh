@@ -58,6 +58,7 @@ struct SysP {
   int c0, ncells, nc[3];
   int nsx, nsy, nsz, sx[3], sy[3], sz[3];   // unique stencil offsets per axis
   int ntypes, map0;          // type map at map[map0 ...], ntypes^2 global interaction indices
+  int inter0, ninter;        // its interactions: global indices [inter0, inter0 + ninter)
   int coul;                  // Coulomb table index (tables at coul * ntable), -1: no charges
   int smallbox;              // box narrower than two list radii: minimum image per pair
   int q0, nq;
@@ -194,9 +195,15 @@ struct Ctx {
   size_t smem_optin = 0;               // opt-in shared memory per block (bytes)
   double *ered = nullptr;              // k_ereduce: per-block partial sums of one large system
   unsigned *ered_done = nullptr;       // k_ereduce: blocks finished per quantity
+  int lw_cap = 0;                      // staged list build: neighbourhood atoms per block (0: off)
+  size_t lw_smem_max = 0;              // its shared-memory limit (bytes)
   int win_ok = 1;                      // single systems may use the windowed pair kernel
   int win_env_off = 0;                 // CM3D_NB_PAIR_KERNEL=list: never
   int pair_used = 0;                   // kernel of the last pair launch (CM3D_NB_PAIR_*)
+  int4 *sys_items = nullptr;           // batch pair kernel work items {system, first, end, -}
+  int nsys_items = 0;
+  float4 *ftab_lj2 = nullptr;          // LJ force + energy coefficients, 2 float4 per knot
+  int stage_ntypes = 0, stage_ninter = 0;   // largest per-system type count / interaction count
   cudaStream_t st = nullptr;
   int mode = CM3D_NB_MIXED;
   int need_short = 0;

@@ -13,9 +13,9 @@
 // exclusion tests) or rmaxl_skin2_e / rmaxs_skin2_e (charged atoms, after the
 // charge-exclusion test).  The resulting pair sets are bit-identical to
 // CM3D's.  The cell grid itself is our own: cells at least one list radius
-// wide, atoms counting-sorted by cell (order inside a cell by atom index), and
-// a stencil of unique neighbour cells, so every pair within range is seen
-// exactly once per direction whatever CM3D's ncell_div is.
+// wide, atoms counting-sorted by cell (inside a cell by atom type, then atom
+// index), and a stencil of unique neighbour cells, so every pair within range
+// is seen exactly once per direction whatever CM3D's ncell_div is.
 //
 // A context may hold several independent systems (SysP, nb_common.cuh): each
 // has its own box, cell grid and parameters, its cells and atoms occupy
@@ -31,6 +31,10 @@
 //   xq, styp   cell-relative FP32 coordinates + charge and type, sorted order
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
 
 #include "nb_common.cuh"
 
@@ -403,8 +407,87 @@ __global__ void __launch_bounds__(256) k_list_half(
   }
 }
 
-// Mixed mode, one pass: the full list of sorted atom t (both directions,
-// every pair in CM3D's t or te list) written straight into its fixed slot
+// Candidates from a staged neighbourhood (k_list_win): `cnt` atoms with FP32
+// positions moved by their cell's shift into the frame of atom t's cell
+// (s_x) and their sorted indices (s_u, low ENT_JBITS bits), walked 32 at a
+// time with the same prefilter and in the same order as walk_candidates.  The
+// queue holds the staged index, and qr its FP32 squared distance.
+template <class Decide>
+__device__ __forceinline__ void walk_staged(int t, float4 xi4, float lim2, const float4 *s_x, const int *s_u,
+                                            int cnt, int *qbuf, float *qr, Decide &decide) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  int head = 0, tail = 0;
+  for (int k0 = 0; k0 < cnt; k0 += 32) {
+    const int k = k0 + lane;
+    bool keep = false;
+    float r2f = 0.f;
+    if (k < cnt) {
+      const float4 xs = s_x[k];
+      const int u = s_u[k] & (int)ENT_JMASK;
+      const float dx = xi4.x - xs.x, dy = xi4.y - xs.y, dz = xi4.z - xs.z;
+      r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      keep = u != t && r2f < lim2;
+    }
+    const unsigned bk = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int slot = (tail + __popc(bk & lt_mask)) & (LQ - 1);
+      qbuf[slot] = k;
+      qr[slot] = r2f;
+    }
+    tail += __popc(bk);
+    __syncwarp();
+    if (tail - head >= 32) {
+      decide(head, 32);
+      head += 32;
+      __syncwarp();
+    }
+  }
+  while (tail > head) {
+    const int m = tail - head < 32 ? tail - head : 32;
+    decide(head, m);
+    head += m;
+  }
+}
+
+// List flags from the FP32 squared distance of a staged pair (cell grid of 3
+// or more cells per axis, where the stencil image is the only image within
+// the list radius and its shift code the pair's).  Each comparison with a
+// list radius R^2 matches CM3D's FP64 one unless the FP32 value lies within
+// 4e-5 R^2 + 2e-3 A^2 of R^2 -- a margin ten times the FP32 error of a
+// squared distance formed from cell-relative coordinates (cells are narrower
+// than two list radii) -- and then *exact is set and the caller decides in
+// FP64 (exact_flags).  Same tests, same order as exact_flags.
+__device__ __forceinline__ int fast_flags(const SysP &P, int i, int j, int ti, int tj, bool qi, bool qj,
+                                          float r2f, const int *__restrict__ map, const double *__restrict__ icut,
+                                          const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
+                                          const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx,
+                                          bool *exact) {
+  const int intr = map[P.map0 + ti * P.ntypes + tj];
+  const bool lj_ok = intr >= 0;
+  const bool el_ok = qi && qj;
+  if (!lj_ok && !el_ok) return 0;
+  bool near = false;
+  auto below = [&](double R2d) {
+    const float R2 = (float)R2d;
+    near |= fabsf(r2f - R2) < fmaf(4e-5f, R2, 2e-3f);
+    return r2f < R2;
+  };
+  int flags = 0;
+  if (lj_ok && below(icut[8 * intr + 5]) && !excluded(i, j, excl_off, excl_idx)) {
+    flags |= 1;
+    if (below(icut[8 * intr + 4])) flags |= 2;
+  }
+  if (el_ok && below(P.rmaxl_skin2_e) && !excluded(i, j, cexcl_off, cexcl_idx)) {
+    flags |= 4;
+    if (below(P.rmaxs_skin2_e)) flags |= 8;
+  }
+  *exact = near;
+  return flags;
+}
+
+// The full list of sorted atom t (mixed mode; one warp): both directions,
+// every pair in CM3D's t or te list, written straight into its fixed slot
 // nbr[t * stride ...] in two segments, each in candidate order: the pairs in
 // an LJ list (t or s) from the front of the slot, their count in nlen[t], and
 // the electrostatics-only pairs from the back (the last one at the slot's
@@ -412,24 +495,20 @@ __global__ void __launch_bounds__(256) k_list_half(
 // only over the front segment.  An atom with more than `stride` pairs writes
 // none past its slot, records the length it needed (ST_NEED_STRIDE) and halts
 // a captured step; the host then widens the slots and builds again.
-__global__ void __launch_bounds__(256) k_list_full(
-    int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
-    int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
-    const float4 *__restrict__ xq, const double *__restrict__ pos, const int *__restrict__ itype,
-    const int *__restrict__ map, const double *__restrict__ icut, const double *__restrict__ q,
-    const int *__restrict__ excl_off, const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
-    const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, uint32_t *__restrict__ nbr,
-    int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
-  if (gated_off(gate, 1)) return;
-  __shared__ int qs[256 / 32][LQ];
-  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// STAGED: candidates from the block's staged neighbourhood (s_x, s_u, scnt),
+// otherwise from global memory through the stencil walk.
+template <bool STAGED>
+__device__ __forceinline__ void full_list_atom(
+    const SysP &P, int n, int t, int stride, const int *__restrict__ cell_atoms,
+    const int *__restrict__ cell_start, const float4 *__restrict__ xq, const double *__restrict__ pos,
+    const int *__restrict__ itype, const int *__restrict__ map, const double *__restrict__ icut,
+    const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
+    const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
+    uint32_t *__restrict__ nbr, int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt,
+    int *qbuf, float *qr, const float4 *s_x, const int *s_u, const int *s_j, const int *s_meta, int scnt,
+    bool fast) {
   const int lane = threadIdx.x & 31;
-  if (t >= n) return;                                     // whole warps
-  const int s = sys_of[t];
-  if (sys_skip(s, sreb, all)) return;                     // whole warps
-  const SysP &P = sp[s];
   const unsigned lt_mask = (1u << lane) - 1u;
-  int *qbuf = qs[threadIdx.x >> 5];
   const int i = cell_atoms[t];
   const int4 ci = cimg[i];
   const double xi = pos[i], yi = pos[n + i], zi = pos[2 * n + i];
@@ -441,9 +520,27 @@ __global__ void __launch_bounds__(256) k_list_full(
   auto decide = [&](int first, int m) {
     int fl = 0, code = 13, u = 0;
     if (lane < m) {
-      u = qbuf[(first + lane) & (LQ - 1)];
-      fl = exact_flags(P, n, i, cell_atoms[u], ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off,
-                       excl_idx, cexcl_off, cexcl_idx, cimg, code);
+      const int slot = (first + lane) & (LQ - 1);
+      if (STAGED) {
+        const int k = qbuf[slot];
+        const int uc = s_u[k];
+        u = uc & (int)ENT_JMASK;
+        const int j = s_j[k];
+        bool exact = !fast;
+        if (fast) {
+          const int meta = s_meta[k];
+          fl = fast_flags(P, i, j, ti, meta >> 1, qi, (meta & 1) != 0, qr[slot], map, icut, excl_off, excl_idx,
+                          cexcl_off, cexcl_idx, &exact);
+          code = (int)((unsigned)uc >> ENT_CODE_SHIFT);
+        }
+        if (exact)
+          fl = exact_flags(P, n, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
+                           cexcl_off, cexcl_idx, cimg, code);
+      } else {
+        u = qbuf[slot];
+        fl = exact_flags(P, n, i, cell_atoms[u], ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off,
+                         excl_idx, cexcl_off, cexcl_idx, cimg, code);
+      }
     }
     bad |= (fl >> 4) & 1;
     const bool fa = (fl & 3) != 0;                   // in an LJ list: front segment
@@ -470,7 +567,8 @@ __global__ void __launch_bounds__(256) k_list_full(
     na += __popc(ba);
     nb += __popc(bb);
   };
-  walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide);
+  if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide);
+  else walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide);
   const int count = na + nb;
   if (lane == 0) {
     if (count <= stride) {
@@ -488,6 +586,134 @@ __global__ void __launch_bounds__(256) k_list_full(
       }
     }
     if (bad) atomicAdd((unsigned long long *)(stat + ST_BADSHIFT), 1ull);
+  }
+}
+
+// Mixed mode, warp per atom over every atom (the candidates walked in global
+// memory): the fallback of k_list_win.
+__global__ void __launch_bounds__(256) k_list_full(
+    int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
+    int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    const float4 *__restrict__ xq, const double *__restrict__ pos, const int *__restrict__ itype,
+    const int *__restrict__ map, const double *__restrict__ icut, const double *__restrict__ q,
+    const int *__restrict__ excl_off, const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
+    const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, uint32_t *__restrict__ nbr,
+    int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  __shared__ int qs[256 / 32][LQ];
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= n) return;                                     // whole warps
+  const int s = sys_of[t];
+  if (sys_skip(s, sreb, all)) return;                     // whole warps
+  full_list_atom<false>(sp[s], n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
+                        excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[threadIdx.x >> 5],
+                        nullptr, nullptr, nullptr, nullptr, nullptr, 0, false);
+}
+
+// Mixed mode, block per cell: the block stages the cell's stencil
+// neighbourhood (every candidate of every atom of the cell: FP32 positions
+// moved by their cell's shift, sorted index + the cell's shift code, atom
+// index, type and charge flag) in shared memory once, then its warps build
+// the cell's atoms' lists from it: the prefilter reads shared memory, and in
+// a grid of 3 or more cells per axis the list flags come from the FP32
+// distance (fast_flags) except within a margin of a list radius, where the
+// FP64 test decides -- the same lists as the FP64 test of every candidate.
+// Blocks walk the cells of the systems being rebuilt; a cell whose
+// neighbourhood holds more than `cap` atoms is walked in global memory
+// instead (same decisions).
+constexpr int LW_THREADS = 256;
+constexpr size_t LW_BYTES_PER_ATOM = sizeof(float4) + 3 * sizeof(int);   // s_x, s_u, s_j, s_meta
+constexpr long long LW_MAX_CAP = 2048;     // largest staged neighbourhood (57 KB)
+
+__global__ void __launch_bounds__(LW_THREADS) k_list_win(
+    int ncells, const int *__restrict__ cell_sys, const SysP *__restrict__ sp, const int *__restrict__ sreb,
+    int all, int n, int stride, int cap, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    const float4 *__restrict__ xq, const double *__restrict__ pos, const int *__restrict__ itype,
+    const int *__restrict__ map, const double *__restrict__ icut, const double *__restrict__ q,
+    const int *__restrict__ excl_off, const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
+    const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg, uint32_t *__restrict__ nbr,
+    int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  extern __shared__ float4 s_x[];                        // cap
+  int *s_u = reinterpret_cast<int *>(s_x + cap);         // cap: sorted index | shift code << ENT_CODE_SHIFT
+  int *s_j = s_u + cap;                                  // cap: atom index
+  int *s_meta = s_j + cap;                               // cap: type * 2 + charged
+  __shared__ int qs[LW_THREADS / 32][LQ];
+  __shared__ float qrs[LW_THREADS / 32][LQ];
+  __shared__ int s_cs[27], s_cn[27], s_off[27], s_code[27], s_tot, s_nw;
+  __shared__ float4 s_sh[27];
+  const int warp = threadIdx.x >> 5;
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+    const int s = cell_sys[c];
+    if (sys_skip(s, sreb, all)) continue;                // whole blocks
+    const SysP &P = sp[s];
+    __syncthreads();                                     // the previous neighbourhood is no longer read
+    if (threadIdx.x < 32) {
+      // the system's stencil around cell c, one stencil cell per lane, in
+      // walk_candidates' order (x offsets outermost), and the prefix of
+      // their atom counts
+      const int w = threadIdx.x;
+      const int nw = P.nsx * P.nsy * P.nsz;
+      int cn = 0;
+      if (w < nw) {
+        const int lc = c - P.c0;
+        const int cz = lc % P.nc[2], cy = (lc / P.nc[2]) % P.nc[1], cx = lc / (P.nc[2] * P.nc[1]);
+        const int ox = P.sx[w / (P.nsy * P.nsz)], oy = P.sy[(w / P.nsz) % P.nsy], oz = P.sz[w % P.nsz];
+        int jx = cx + ox, jy = cy + oy, jz = cz + oz;
+        jx = jx < 0 ? jx + P.nc[0] : (jx >= P.nc[0] ? jx - P.nc[0] : jx);
+        jy = jy < 0 ? jy + P.nc[1] : (jy >= P.nc[1] ? jy - P.nc[1] : jy);
+        jz = jz < 0 ? jz + P.nc[2] : (jz >= P.nc[2] ? jz - P.nc[2] : jz);
+        const int cell = P.c0 + (jx * P.nc[1] + jy) * P.nc[2] + jz;
+        const int cs = cell_start[cell];
+        cn = cell_start[cell + 1] - cs;
+        s_cs[w] = cs;
+        s_cn[w] = cn;
+        s_code[w] = (1 - ox) * 9 + (1 - oy) * 3 + (1 - oz);
+        s_sh[w] = P.shift[s_code[w]];
+      }
+      int incl = cn;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (w >= o) incl += v;
+      }
+      if (w < nw) s_off[w] = incl - cn;
+      if (w == 31) {
+        s_nw = nw;
+        s_tot = incl;
+      }
+    }
+    __syncthreads();
+    const int tot = s_tot, nw = s_nw;
+    const bool staged = tot <= cap;
+    if (staged) {
+      for (int w = 0; w < nw; w++) {
+        const int cs = s_cs[w], cn = s_cn[w], off = s_off[w];
+        const int code = s_code[w] << ENT_CODE_SHIFT;
+        const float4 sh = s_sh[w];
+        for (int k = threadIdx.x; k < cn; k += blockDim.x) {
+          const float4 x = xq[cs + k];
+          const int j = cell_atoms[cs + k];
+          s_x[off + k] = make_float4(x.x - sh.x, x.y - sh.y, x.z - sh.z, 0.f);
+          s_u[off + k] = (cs + k) | code;
+          s_j[off + k] = j;
+          s_meta[off + k] = itype[j] * 2 + (q[j] != 0.0 ? 1 : 0);
+        }
+      }
+    }
+    __syncthreads();
+    const int lo = cell_start[c], hi = cell_start[c + 1];
+    const bool fast = P.nc[0] >= 3 && P.nc[1] >= 3 && P.nc[2] >= 3 && !P.smallbox;
+    for (int t = lo + warp; t < hi; t += LW_THREADS / 32) {
+      if (staged)
+        full_list_atom<true>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
+                             excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], qrs[warp], s_x,
+                             s_u, s_j, s_meta, tot, fast);
+      else
+        full_list_atom<false>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
+                              excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], nullptr,
+                              nullptr, nullptr, nullptr, nullptr, 0, false);
+    }
   }
 }
 
@@ -637,6 +863,23 @@ int list_setup(Ctx *c) {
   CK(cudaMemcpy(c->shift, c->h_sp[0].shift, sizeof(float4) * 27, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->shift + 27, c->h_sp[0].shift_lo, sizeof(float4) * 27, cudaMemcpyHostToDevice));
   if (c->mode == CM3D_NB_MIXED) {
+    // staged list build: room for 1.6x the largest mean stencil neighbourhood
+    // (+64), within the shared memory a block may opt into
+    double nb_max = 0;
+    for (int sy = 0; sy < c->nsys; sy++) {
+      const SysP &S = c->h_sp[sy];
+      const double per_cell = (double)S.n / (double)(S.ncells > 0 ? S.ncells : 1);
+      nb_max = std::max(nb_max, per_cell * S.nsx * S.nsy * S.nsz);
+    }
+    c->lw_smem_max = c->smem_optin > 8192 ? c->smem_optin - 8192 : 0;
+    long long cap = (long long)(1.6 * nb_max) + 64;
+    const long long cap_max = (long long)(c->lw_smem_max / LW_BYTES_PER_ATOM);
+    c->lw_cap = (int)std::min(cap, cap_max);
+    // a neighbourhood of thousands of atoms leaves one block per SM: the
+    // warp-per-atom walk through global memory keeps more warps in flight
+    if (c->lw_cap < 64 || cap > LW_MAX_CAP) c->lw_cap = 0;
+    const char *lk = getenv("CM3D_NB_LIST_KERNEL");
+    if (lk && strcmp(lk, "walk") == 0) c->lw_cap = 0;
     CK(cudaMalloc(&c->nlen, sizeof(int) * 2 * (size_t)c->n));
     CK(cudaMemset(c->nlen, 0, sizeof(int) * 2 * (size_t)c->n));
     long long s = ((long long)est_max + 31) / 32 * 32;
@@ -719,10 +962,29 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
   const long long warps_threads = 32LL * n;
   if (c->mode == CM3D_NB_MIXED) {
     for (;;) {
-      k_list_full<<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
-          n, c->sp, c->sys_of, c->sreb, al, c->nbr_stride, c->cell_atoms, c->cell_start, c->xq, c->pos, c->itype,
-          c->map, c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->nbr, c->nlen,
-          c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+      if (c->lw_cap > 0) {
+        // block per cell over the cells of the systems being rebuilt, the
+        // stencil neighbourhood staged in shared memory
+        const size_t smem = (size_t)c->lw_cap * LW_BYTES_PER_ATOM;
+        static unsigned long long attr_devs = 0;
+        if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
+          cudaFuncSetAttribute(k_list_win, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->lw_smem_max);
+          attr_devs |= 1ull << c->dev;
+        }
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list_win, LW_THREADS, smem);
+        long long grid = (long long)c->num_sms * (per_sm > 0 ? per_sm : 1);
+        if (grid > c->ncells) grid = c->ncells;
+        k_list_win<<<(int)grid, LW_THREADS, smem, c->st>>>(
+            c->ncells, c->cell_sys, c->sp, c->sreb, al, n, c->nbr_stride, c->lw_cap, c->cell_atoms, c->cell_start,
+            c->xq, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx,
+            cimg, c->nbr, c->nlen, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+      } else {
+        k_list_full<<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
+            n, c->sp, c->sys_of, c->sreb, al, c->nbr_stride, c->cell_atoms, c->cell_start, c->xq, c->pos,
+            c->itype, c->map, c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->nbr,
+            c->nlen, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+      }
       c->launches++;
       CKL(c);
       if (device_flag) break;

@@ -456,16 +456,37 @@ __global__ void __launch_bounds__(512, 1) k_pair_win(
 // type map and (when they fit) tables staged in shared memory.  BATCH = true:
 // several systems; each atom group reads its system's parameters, shifts and
 // tables (global interaction / Coulomb-table indices) from sp[sys_of[t]].
-template <int TPA, bool SMALLBOX, bool NEED_S, bool BATCH>
+//
+// STAGE (batches, full force without the RESPA switch): the blocks walk work
+// items -- a system, or a part of at most SYS_PART atoms of one -- instead of
+// striding over all atoms, and first copy the item's system parameters into
+// shared memory: its cell shifts, type map (local interaction indices),
+// cut-offs, LJ force/energy coefficients (2 float4 per knot) and erfc table.
+// Every per-pair parameter and table read is then a shared-memory load; the
+// j-atoms still come from global memory through L1.  Items come largest
+// system first (host-ordered), so the long ones start early.
+constexpr int SYS_PART = 1024;
+
+template <int TPA, bool SMALLBOX, bool NEED_S, bool BATCH, bool STAGE = false>
 __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
     MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ nlen, int stride, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
     const int *__restrict__ gmap, const float *__restrict__ gfcut, const float4 *__restrict__ gtl,
     const float4 *__restrict__ gte, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
     double *__restrict__ fout, double *__restrict__ fshort, float *__restrict__ epart,
-    double *__restrict__ epart64, long long *__restrict__ stat, const int *__restrict__ gs) {
+    double *__restrict__ epart64, long long *__restrict__ stat, const int *__restrict__ gs,
+    const int4 *__restrict__ items = nullptr, int nitems = 0, const float4 *__restrict__ gtl2 = nullptr,
+    int st_ntypes = 0, int st_ninter = 0) {
+  static_assert(!STAGE || BATCH, "staging is for batches");
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
+  // STAGE: one system's parameters (layout sized for the largest system)
+  float4 *st_shift = sm;                                                      // 54
+  int *st_map = reinterpret_cast<int *>(sm + 54);                             // st_ntypes^2
+  const int st_nm4 = (st_ntypes * st_ntypes + 3) / 4;
+  float *st_fcut = reinterpret_cast<float *>(sm + 54 + st_nm4);               // 8 * st_ninter
+  float4 *st_tl = sm + 54 + st_nm4 + 2 * st_ninter;                           // 2 * st_ninter * ntable
+  float4 *st_te = st_tl + 2 * st_ninter * P.ntable;                           // 2 * ntable
   float4 *shift = sm;                                   // 27 hi + 27 lo
   float *fcut = reinterpret_cast<float *>(sm + 54);     // 8 * ninter
   int nf4 = (8 * P.ninter + 3) / 4;
@@ -494,10 +515,9 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
   const uint32_t fl_lj = P.iflg == 1 ? ENT_LJ : ENT_LJS;
   const uint32_t fl_el = P.iflg == 1 ? ENT_EL : ENT_ELS;
   unsigned under = 0;
-  // persistent: every lane group walks atoms blockIdx-strided
-  for (int tb = blockIdx.x * groups; tb < P.n; tb += gridDim.x * groups) {
-    const int t = tb + threadIdx.x / TPA;
-    const bool active = t < P.n;
+  // one i-atom per lane group (every lane of the block calls it: it ends in
+  // warp shuffles)
+  auto do_atom = [&](const int t, const bool active) {
     double Fx = 0, Fy = 0, Fz = 0, Sx = 0, Sy = 0, Sz = 0, elj_hi = 0;
     float e[EP_COUNT];
 #pragma unroll
@@ -513,13 +533,13 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
       int cnt = 0;
       // this atom's system: shifts, type map, cut-offs and tables
       const SysP *Sp = BATCH ? sp + sys_of[t] : nullptr;
-      const float4 *shp = BATCH ? Sp->shift : shift;
-      const float4 *shlp = BATCH ? Sp->shift_lo : shift + 27;
-      const int *mapp = BATCH ? gmap + Sp->map0 : map;
-      const float *fcp = BATCH ? gfcut : fcut;
+      const float4 *shp = STAGE ? st_shift : BATCH ? Sp->shift : shift;
+      const float4 *shlp = STAGE ? st_shift + 27 : BATCH ? Sp->shift_lo : shift + 27;
+      const int *mapp = STAGE ? st_map : BATCH ? gmap + Sp->map0 : map;
+      const float *fcp = STAGE ? st_fcut : BATCH ? gfcut : fcut;
       const int ntyp = BATCH ? Sp->ntypes : P.ntypes;
       const bool has_el = (P.mask & 2) && (!BATCH || Sp->coul >= 0);
-      const float4 *tep = BATCH ? gte + (size_t)2 * P.ntable * (Sp->coul > 0 ? Sp->coul : 0) : te;
+      const float4 *tep = STAGE ? st_te : BATCH ? gte + (size_t)2 * P.ntable * (Sp->coul > 0 ? Sp->coul : 0) : te;
       const float rc2_el = BATCH ? Sp->rc2_el : P.rc2_el;
       const float dx2c = BATCH ? Sp->dx2c : P.dx2c;
       const float offc = BATCH ? Sp->offc : P.offc;
@@ -582,8 +602,20 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
               p = 1.f;
             }
             p -= (float)kk;
-            const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
-            const float4 a0 = T[0], a1 = T[1], a2 = T[2];
+            float4 a0, a1, a2;
+            if (STAGE) {
+              // {d0, dA, dB, v0 hi} {vA, vB, v0 lo, -}
+              const float4 *T = st_tl + 2 * (in * P.ntable + kk);
+              a0 = T[0];
+              const float4 b = T[1];
+              a1 = make_float4(b.x, b.y, 0.f, 0.f);
+              a2 = make_float4(0.f, b.z, 0.f, 0.f);
+            } else {
+              const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
+              a0 = T[0];
+              a1 = T[1];
+              a2 = T[2];
+            }
             const float f = poly(p, a0.x, a0.y, a0.z);
             float swv = 1.f;
             if (needB && r2 > cB.x) swv = poly(p, a1.z, a1.w, a2.x);
@@ -692,6 +724,39 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
         epart64[t] = elj_hi;
       }
     }
+  };
+  if (!STAGE) {
+    // persistent: every lane group walks atoms blockIdx-strided
+    for (int tb = blockIdx.x * groups; tb < P.n; tb += gridDim.x * groups) {
+      const int t = tb + threadIdx.x / TPA;
+      do_atom(t, t < P.n);
+    }
+  } else {
+    for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+      const int4 item = items[it];                       // {system, first atom, end atom, -}
+      const SysP &S = sp[item.x];
+      __syncthreads();                                   // the previous system is no longer read
+      for (int k = threadIdx.x; k < 27; k += blockDim.x) {
+        st_shift[k] = S.shift[k];
+        st_shift[27 + k] = S.shift_lo[k];
+      }
+      for (int k = threadIdx.x; k < S.ntypes * S.ntypes; k += blockDim.x) {
+        const int in = gmap[S.map0 + k];
+        st_map[k] = in >= 0 ? in - S.inter0 : -1;
+      }
+      for (int k = threadIdx.x; k < 8 * S.ninter; k += blockDim.x) st_fcut[k] = gfcut[8 * S.inter0 + k];
+      if (P.mask & 1)
+        for (int k = threadIdx.x; k < 2 * S.ninter * P.ntable; k += blockDim.x)
+          st_tl[k] = gtl2[(size_t)2 * S.inter0 * P.ntable + k];
+      if ((P.mask & 2) && S.coul >= 0)
+        for (int k = threadIdx.x; k < 2 * P.ntable; k += blockDim.x)
+          st_te[k] = gte[(size_t)2 * P.ntable * S.coul + k];
+      __syncthreads();
+      for (int tb = item.y; tb < item.z; tb += groups) {
+        const int t = tb + threadIdx.x / TPA;
+        do_atom(t, t < item.z);
+      }
+    }
   }
   if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), (unsigned long long)under);
 }
@@ -784,10 +849,10 @@ static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
   return b;
 }
 
-template <int TPA, bool SB, bool NS, bool BT>
+template <int TPA, bool SB, bool NS, bool BT, bool ST = false>
 static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   const int B = 256;
-  auto kern = k_pair_mixed<TPA, SB, NS, BT>;
+  auto kern = k_pair_mixed<TPA, SB, NS, BT, ST>;
   // the shared-memory limit is a per-device attribute: set it for every
   // device this process launches on
   static unsigned long long attr_devs = 0;
@@ -800,25 +865,40 @@ static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, B, smem);
   if (per_sm < 1) per_sm = 1;
-  long long need = ((long long)c->n * TPA + B - 1) / B;
+  long long need = ST ? (long long)c->nsys_items : ((long long)c->n * TPA + B - 1) / B;
   long long grid = (long long)c->num_sms * per_sm;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   kern<<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->nlen, c->nbr_stride, c->nbr, c->shift,
                                  c->map, c->fcut, c->ftab_lj, c->ftab_el, c->sp, c->sys_of, fout, c->fxs, c->epart,
-                                 epart_hi(c), c->stat, c->gate);
+                                 epart_hi(c), c->stat, c->gate, c->sys_items, c->nsys_items, c->ftab_lj2,
+                                 c->stage_ntypes, c->stage_ninter);
 }
 
-template <bool SB, bool NS, bool BT>
+template <bool SB, bool NS, bool BT, bool ST = false>
 static int launch_tpa(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   switch (c->tpa) {
-    case 4: launch_t<4, SB, NS, BT>(c, P, smem, fout); break;
-    case 8: launch_t<8, SB, NS, BT>(c, P, smem, fout); break;
-    case 16: launch_t<16, SB, NS, BT>(c, P, smem, fout); break;
-    case 32: launch_t<32, SB, NS, BT>(c, P, smem, fout); break;
-    default: launch_t<8, SB, NS, BT>(c, P, smem, fout); break;
+    case 4: launch_t<4, SB, NS, BT, ST>(c, P, smem, fout); break;
+    case 8: launch_t<8, SB, NS, BT, ST>(c, P, smem, fout); break;
+    case 16: launch_t<16, SB, NS, BT, ST>(c, P, smem, fout); break;
+    case 32: launch_t<32, SB, NS, BT, ST>(c, P, smem, fout); break;
+    default: launch_t<8, SB, NS, BT, ST>(c, P, smem, fout); break;
   }
   return CM3D_NB_OK;
+}
+
+// shared memory of the staged batch kernel: one system's parameters, sized
+// for the largest system
+static size_t stage_bytes(Ctx *c) {
+  const size_t nm4 = ((size_t)c->stage_ntypes * c->stage_ntypes + 3) / 4;
+  return (54 + nm4 + 2 * (size_t)c->stage_ninter + 2 * (size_t)c->stage_ninter * c->ntable + 2 * (size_t)c->ntable) *
+         sizeof(float4);
+}
+
+// whether a batch's pair launch can stage each system's parameters: the full
+// force level without the RESPA switch (the compact LJ knots hold no switch)
+static bool stage_applies(Ctx *c, int iflg, bool ns) {
+  return c->nsys > 1 && c->sys_items != nullptr && iflg == 1 && !ns;
 }
 
 // Windowed kernel for one system with >= 3 cells per axis: returns false
@@ -941,6 +1021,12 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   // else (batches, coarse cell grids): the gather kernel
   c->pair_used = CM3D_NB_PAIR_WINDOW;
   if (launch_win(c, P, ns, fout)) {
+  } else if (c->win_ok && stage_applies(c, iflg, ns)) {
+    // several systems: a block copies the parameters and tables of the
+    // system it works on into shared memory
+    c->pair_used = CM3D_NB_PAIR_SYSTEM;
+    P.tab_smem = 0;
+    launch_tpa<false, false, true, true>(c, P, stage_bytes(c), fout);
   } else if ((c->pair_used = CM3D_NB_PAIR_GATHER), c->nsys > 1) {
     // several systems: per-system parameters and tables from global memory
     P.tab_smem = 0;
@@ -1039,6 +1125,40 @@ int pair_setup(Ctx *c) {
   CK(cudaMalloc(&c->ered, sizeof(double) * EP_COUNT * EREDUCE_MAX_Z));
   CK(cudaMalloc(&c->ered_done, sizeof(unsigned) * EP_COUNT));
   CK(cudaMemset(c->ered_done, 0, sizeof(unsigned) * EP_COUNT));
+  if (c->nsys > 1) {
+    // work items of the staged batch kernel: every system in parts of at most
+    // SYS_PART atoms, largest system first; staging applies while the largest
+    // system fits in shared memory next to two more blocks on the SM
+    int mt = 0, mi = 0;
+    for (int sy = 0; sy < c->nsys; sy++) {
+      mt = std::max(mt, c->h_sp[sy].ntypes);
+      mi = std::max(mi, c->h_sp[sy].ninter);
+    }
+    c->stage_ntypes = mt;
+    c->stage_ninter = mi;
+    if (stage_bytes(c) <= c->smem_optin / 2 - 1024) {
+      std::vector<int> order(c->nsys);
+      for (int sy = 0; sy < c->nsys; sy++) order[sy] = sy;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return c->h_sp[a].n > c->h_sp[b].n; });
+      std::vector<int4> items;
+      for (int sy : order) {
+        const SysP &S = c->h_sp[sy];
+        for (int a = 0; a < S.n; a += SYS_PART)
+          items.push_back(make_int4(sy, S.a0 + a, S.a0 + std::min(S.n, a + SYS_PART), 0));
+      }
+      CK(cudaMalloc(&c->sys_items, sizeof(int4) * items.size()));
+      CK(cudaMemcpy(c->sys_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
+      c->nsys_items = (int)items.size();
+      // compact LJ coefficients: {d0, dA, dB, v0 hi} {vA, vB, v0 lo, 0}
+      std::vector<float4> tl2((size_t)2 * (ni > 0 ? ni : 1) * nt, make_float4(0.f, 0.f, 0.f, 0.f));
+      for (size_t k = 0; k < (size_t)ni * nt; k++) {
+        tl2[2 * k] = tl[3 * k];
+        tl2[2 * k + 1] = make_float4(tl[3 * k + 1].x, tl[3 * k + 1].y, tl[3 * k + 2].y, 0.f);
+      }
+      CK(cudaMalloc(&c->ftab_lj2, sizeof(float4) * tl2.size()));
+      CK(cudaMemcpy(c->ftab_lj2, tl2.data(), sizeof(float4) * tl2.size(), cudaMemcpyHostToDevice));
+    }
+  }
   if (c->tpa == 0) {
     // 8 lanes per atom: a group reads a full 32-byte sector of the list; more
     // lanes only for systems too small to fill the GPU

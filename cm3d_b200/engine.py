@@ -266,7 +266,7 @@ class Engine:
         return {"velec": v.value, "welec": w.value, "welectensor": t}
 
     def autotune(self, reps: int = 5) -> dict:
-        """Pick the pair kernel (gather or window) and its lanes per atom by
+        """Pick the pair kernel (gather, or the staged window/system kernel) and its lanes per atom by
         timing 4/8/16/32 on the current lists (cm3d_nb_autotune); returns the
         choice and, per lanes-per-atom choice, the faster kernel's time."""
         t = C.c_int(0)
@@ -276,10 +276,10 @@ class Engine:
                 "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
 
     def pair_kernel(self) -> tuple[str, int]:
-        """(kernel of the last pair launch: "gather" or "window", lanes per atom)"""
+        """(kernel of the last pair launch: "gather", "window" or "system", lanes per atom)"""
         k, t = C.c_int(0), C.c_int(0)
         check(load_library().cm3d_nb_pair_kernel(self._h, C.byref(k), C.byref(t)), "pair_kernel")
-        return ("window" if k.value == 1 else "gather"), int(t.value)
+        return {0: "gather", 1: "window", 2: "system"}[k.value], int(t.value)
 
     def system_energies(self, sys: int) -> dict:
         """getvireal + geteng of one system of a batch"""

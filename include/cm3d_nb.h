@@ -287,16 +287,18 @@ int cm3d_nb_measure_peaks(int device, double *fp32_tflops, double *fp64_tflops);
    NULL) receives, per lanes-per-atom choice, the time of the faster kernel. */
 int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]);
 /* The mixed pair kernels (no CM3D counterpart).  GATHER: lane groups read
-   j-atoms from global memory; batches and coarse cell grids always use it.
-   WINDOW: one system with >= 3 cells per axis; a block stages the 27 cells
-   around an i-cell in shared memory.  cm3d_nb_autotune times both (where the
-   box allows the window) at every lanes-per-atom choice, keeps the fastest,
-   and ms_per_launch[k] is the faster of the two at that choice.
-   CM3D_NB_PAIR_KERNEL=list in the environment at cm3d_nb_create keeps a
-   context on the gather kernel.  cm3d_nb_pair_kernel reports the kernel of
-   the last pair launch and the lanes per atom. */
+   j-atoms from global memory; any context can run it.  WINDOW: one system
+   with >= 3 cells per axis; a block stages the 27 cells around an i-cell in
+   shared memory.  SYSTEM: a batch whose largest system fits in shared memory;
+   a block stages the whole system it works on.  cm3d_nb_autotune times the
+   gather kernel and the staged one that applies at every lanes-per-atom
+   choice, keeps the fastest, and ms_per_launch[k] is the faster at that
+   choice.  CM3D_NB_PAIR_KERNEL=list in the environment at cm3d_nb_create
+   keeps a context on the gather kernel.  cm3d_nb_pair_kernel reports the
+   kernel of the last pair launch and the lanes per atom. */
 #define CM3D_NB_PAIR_GATHER 0
 #define CM3D_NB_PAIR_WINDOW 1
+#define CM3D_NB_PAIR_SYSTEM 2
 int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
 
 /* ------------------------------------------- no-allocation variant */
