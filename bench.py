@@ -332,14 +332,21 @@ def plain_arm(systems, device: int, steps: int, warmup: int, flush) -> dict:
 
 
 def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float, hbm: float, name: str,
-              e2e_steps: int, dist=None) -> dict:
+              e2e_steps: int, dist=None, pin=None) -> dict:
+    """pin = (lanes per atom, "gather" | "staged"): skip the autotuner and use
+    that choice (a profiler run reproduces the choice the autotuner makes
+    without the profiler, whose serialised timings would mislead it)."""
     import torch
     from cm3d_b200 import _abi
     from cm3d_b200.engine import Engine
-    eng = Engine(systems, mode=_abi.MIXED, device=device)
+    if pin and pin[1] == "gather":
+        os.environ["CM3D_NB_PAIR_KERNEL"] = "list"
+    eng = Engine(systems, mode=_abi.MIXED, device=device, tpa=pin[0] if pin else 0)
+    if pin:
+        os.environ.pop("CM3D_NB_PAIR_KERNEL", None)
     eng.workload_name = name
     eng.step_init()
-    tune = eng.autotune()
+    tune = {"tpa": pin[0], "kernel": pin[1], "pinned": True} if pin else eng.autotune()
     n = eng.n
     if dist:
         dist.barrier()
@@ -408,6 +415,10 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--tpa", type=int, default=0, choices=[0, 4, 8, 16, 32],
+                    help="pin the pair kernel's lanes per atom instead of autotuning (profiling runs)")
+    ap.add_argument("--pair-kernel", default="gather", choices=["gather", "staged"],
+                    help="with --tpa: the pair kernel to pin")
     ap.add_argument("--partition", action="store_true",
                     help="N > 1: split one ensemble over the ranks (LPT on the cost model, strong scaling) "
                          "instead of one ensemble per rank (weak scaling)")
@@ -474,7 +485,8 @@ def main() -> None:
     fp32, fp64 = measure_peaks(local)
     flush = l2_flusher(local)
 
-    m = mixed_arm(systems, local, steps, warmup, flush, fp32, hbm, args.workload, min(steps, 100), dist)
+    pin = (args.tpa, args.pair_kernel) if args.tpa else None
+    m = mixed_arm(systems, local, steps, warmup, flush, fp32, hbm, args.workload, min(steps, 100), dist, pin)
     n = m["n"]
     ms = m["ms"]
     value = (natoms_job if partitioned else world * n) * steps / (ms / 1e3)
