@@ -538,7 +538,9 @@ int kspace_setup(Ctx *c) {
   // split the rows over enough blocks to fill the machine in the force pass
   int split = 1;
   while ((long long)c->ftiles_tot * split < 148 * 4 && split < nrows_max) split *= 2;
-  // every split's A(k) must fit in shared memory
+  // every split's A(k) must fit in shared memory -- in 48 KB, so that four
+  // or more blocks share an SM and hide each other's latency (a single split
+  // of a large k set would leave one block per SM)
   for (;;) {
     size_t mx = 0;
     for (int sy = 0; sy < c->nsys; sy++) {
@@ -553,7 +555,7 @@ int kspace_setup(Ctx *c) {
       }
     }
     c->kf_smem = mx * sizeof(float2);
-    if (c->kf_smem <= 180 * 1024 || split >= nrows_max) break;
+    if (c->kf_smem <= 48 * 1024 || split >= nrows_max) break;
     split *= 2;
   }
   if (split > nrows_max) split = nrows_max;
