@@ -242,7 +242,9 @@ def roofline(eng, steps: int, istep0: int, fp32_tflops: float, hbm_gbs: float) -
     else:
         out = {"bound": "hbm", "achieved": nbytes / t / 1e9, "peak": hbm_gbs, "unit": "GB/s",
                "frac": (nbytes / t / 1e9) / hbm_gbs}
-    out.update({"traffic": traffic, "kernel": "k_pair_mixed (fused LJ + real-space Ewald)",
+    kind, tpa = eng.pair_kernel()
+    out.update({"traffic": traffic,
+                "kernel": f"{kind} pair kernel (fused LJ + real-space Ewald), {tpa} lanes per atom",
                 "ms_per_launch": t * 1e3, "launches": launches, "unique_pairs": pairs,
                 "pairs_te": int(pte_s.sum()), "pairs_t": int(pt_s.sum()),
                 "algorithmic_flops": flops, "algorithmic_bytes": nbytes,
