@@ -115,7 +115,8 @@ struct WinSrc {
 };
 // The tables of the atom's system.
 struct PairTab {
-  const float4 *tl, *te;         // LJ (3 float4 per knot) and erfc (2 per knot) coefficients
+  const float4 *tl, *te;         // LJ (3 float4 per knot) and erfc coefficients (ntable force
+                                 // float4, then ntable energy float4)
   const float *fcut;             // 8 floats per interaction
   const int *map;                // ntypes^2 interaction indices
   int ntypes;
@@ -178,12 +179,12 @@ __device__ __forceinline__ void win_segment(const MixedP &P, const WinSrc &S, co
       // below the table: CM3D's clamp (kk = 1, p = 1: the first knot)
       const float fr = ok && kk >= 1 ? p - (float)kk : 0.f;
       kk = kk < 1 ? 1 : (kk > ntm2 ? ntm2 : kk);
-      const float4 c0 = T.te[2 * kk];
+      const float4 c0 = T.te[kk];
       const float qq = ok ? xi.w * xj.w : 0.f;
       const float fe = qq * poly(fr, c0.x, c0.y, c0.z);
       ftot = fe;
       if (P.iflg == 1) {
-        const float4 c1 = T.te[2 * kk + 1];
+        const float4 c1 = T.te[P.ntable + kk];
         A.e[EP_EEL] = fmaf(qq, poly(fr, c0.w, c1.x, c1.y), A.e[EP_EEL]);
         A.e[EP_QQ] += qq;
         const float fdx = fe * dx, fdy = fe * dy, fdz = fe * dz;
@@ -304,7 +305,10 @@ __global__ void __launch_bounds__(512, 1) k_pair_win(
   const int nm4 = (P.ntypes * P.ntypes + 3) / 4;
   float4 *tl = sm + 54 + nf4 + nm4;                     // LJ tables (3 * ninter * ntable)
   const int nl = (P.mask & 1) ? 3 * P.ninter * P.ntable : 0;
-  float4 *te = tl + nl;                                 // erfc table (2 * ntable)
+  // erfc table (2 * ntable): the force coefficients of every knot, then the
+  // energy coefficients -- two arrays at a 16-byte stride, so that random
+  // knots spread over all bank groups (interleaved, each half would use half)
+  float4 *te = tl + nl;
   const int ne = HAS_EL ? 2 * P.ntable : 0;
   float4 *wx = te + ne;                                 // staged window: cap float4
   unsigned short *wt = reinterpret_cast<unsigned short *>(wx + W.cap);   // cap types
@@ -314,7 +318,7 @@ __global__ void __launch_bounds__(512, 1) k_pair_win(
   for (int k = threadIdx.x; k < 8 * P.ninter; k += blockDim.x) fcut[k] = gfcut[k];
   for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) map[k] = gmap[k];
   for (int k = threadIdx.x; k < nl; k += blockDim.x) tl[k] = gtl[k];
-  for (int k = threadIdx.x; k < ne; k += blockDim.x) te[k] = gte[k];
+  for (int k = threadIdx.x; k < ne; k += blockDim.x) te[(k & 1) * P.ntable + (k >> 1)] = gte[k];
 
   const int g = threadIdx.x % TPA;
   const int groups = blockDim.x / TPA;
