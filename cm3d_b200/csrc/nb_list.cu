@@ -171,36 +171,47 @@ __device__ __forceinline__ long long sort_key(const int *__restrict__ itype, int
   return ((long long)itype[i] << 32) | (unsigned)i;
 }
 
-__global__ void k_cell_sort(int ncells, const int *__restrict__ cell_sys, const int *__restrict__ sreb, int all,
-                            const int *__restrict__ cell_start, const int *__restrict__ itype,
-                            int *__restrict__ cell_atoms, const int *__restrict__ gate) {
+constexpr int SORT_CELLS = 8;      // cells per block of k_cell_sort
+constexpr int SORT_THREADS = 128;
+
+__global__ void __launch_bounds__(SORT_THREADS) k_cell_sort(int ncells, const int *__restrict__ cell_sys,
+                                                             const int *__restrict__ sreb, int all,
+                                                             const int *__restrict__ cell_start,
+                                                             const int *__restrict__ itype,
+                                                             int *__restrict__ cell_atoms,
+                                                             const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   __shared__ long long s[1024];
-  const int c = blockIdx.x;
-  if (sys_skip(cell_sys[c], sreb, all)) return;
-  const int lo = cell_start[c], hi = cell_start[c + 1], m = hi - lo;
-  if (m <= 1) return;
-  if (m <= 1024) {
-    for (int k = threadIdx.x; k < m; k += blockDim.x) s[k] = sort_key(itype, cell_atoms[lo + k]);
-    __syncthreads();
-    for (int k = threadIdx.x; k < m; k += blockDim.x) {
-      const long long v = s[k];
-      int r = 0;
-      for (int u = 0; u < m; u++) r += s[u] < v;
-      cell_atoms[lo + r] = (int)(v & 0xffffffffLL);
-    }
-    return;
-  }
-  // a cell with more than 1024 atoms: odd-even transposition sort in place
-  for (int pass = 0; pass < m; pass++) {
-    for (int k = lo + (pass & 1) + 2 * threadIdx.x; k + 1 < hi; k += 2 * blockDim.x) {
-      int a0 = cell_atoms[k], a1 = cell_atoms[k + 1];
-      if (sort_key(itype, a0) > sort_key(itype, a1)) {
-        cell_atoms[k] = a1;
-        cell_atoms[k + 1] = a0;
+  // SORT_CELLS consecutive cells per block: a batch has tens of thousands of
+  // cells of a few atoms each
+  const int c_end = min(ncells, (blockIdx.x + 1) * SORT_CELLS);
+  for (int c = blockIdx.x * SORT_CELLS; c < c_end; c++) {
+    if (sys_skip(cell_sys[c], sreb, all)) continue;     // whole blocks
+    const int lo = cell_start[c], hi = cell_start[c + 1], m = hi - lo;
+    if (m <= 1) continue;
+    __syncthreads();                                     // the previous cell's keys are no longer read
+    if (m <= 1024) {
+      for (int k = threadIdx.x; k < m; k += blockDim.x) s[k] = sort_key(itype, cell_atoms[lo + k]);
+      __syncthreads();
+      for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const long long v = s[k];
+        int r = 0;
+        for (int u = 0; u < m; u++) r += s[u] < v;
+        cell_atoms[lo + r] = (int)(v & 0xffffffffLL);
       }
+      continue;
     }
-    __syncthreads();
+    // a cell with more than 1024 atoms: odd-even transposition sort in place
+    for (int pass = 0; pass < m; pass++) {
+      for (int k = lo + (pass & 1) + 2 * threadIdx.x; k + 1 < hi; k += 2 * blockDim.x) {
+        int a0 = cell_atoms[k], a1 = cell_atoms[k + 1];
+        if (sort_key(itype, a0) > sort_key(itype, a1)) {
+          cell_atoms[k] = a1;
+          cell_atoms[k + 1] = a0;
+        }
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -954,8 +965,8 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
   k_cell_scan<<<c->nsys, 256, 0, c->st>>>(c->sp, c->sreb, al, c->cell_cursor, c->cell_start, gate);
   k_cell_fill<<<grid_for(n, B), B, 0, c->st>>>(n, c->sys_of, c->sreb, al, c->cell_of, c->cell_start,
                                                 c->cell_cursor, c->cell_atoms, gate);
-  k_cell_sort<<<c->ncells, 256, 0, c->st>>>(c->ncells, c->cell_sys, c->sreb, al, c->cell_start, c->itype,
-                                            c->cell_atoms, gate);
+  k_cell_sort<<<(c->ncells + SORT_CELLS - 1) / SORT_CELLS, SORT_THREADS, 0, c->st>>>(
+      c->ncells, c->cell_sys, c->sreb, al, c->cell_start, c->itype, c->cell_atoms, gate);
   k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->sp, c->sys_of, c->sreb, al, c->cell_atoms, cimg, c->itype,
                                                   c->pos, c->q, c->rank, c->styp, c->corner, c->xq, gate);
   c->launches += 6;

@@ -773,6 +773,8 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
 // block stores its partial sum, and the last block of a quantity to finish
 // adds the partials in block order -- the result does not depend on which
 // block finished last -- and re-arms the counter for the next launch.
+__device__ __forceinline__ void ep_to_acc(int q, double s, double *acc, float tablast_e);
+
 __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const float *__restrict__ epart,
                           const double *__restrict__ epart64, double *__restrict__ accs,
                           double *__restrict__ part, unsigned *__restrict__ done, const int *__restrict__ gs) {
@@ -815,7 +817,11 @@ __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const fl
     }
   }
   if (threadIdx.x != 0) return;
-  s *= 0.5;
+  ep_to_acc(q, 0.5 * s, acc, tablast_e);
+}
+
+// CM3D's accumulator update for one reduced quantity (sum already halved)
+__device__ __forceinline__ void ep_to_acc(int q, double s, double *acc, float tablast_e) {
   switch (q) {
     case EP_ELJ: atomicAdd(acc + ACC_SPOTL, s); break;
     case EP_ELJH: atomicAdd(acc + ACC_SPOTHL, s); break;
@@ -833,6 +839,46 @@ __global__ void k_ereduce(int n, int mask, const SysP *__restrict__ sp, const fl
     case EP_VE4: atomicAdd(acc + ACC_SPRSET + 4, -s); atomicAdd(acc + ACC_SPRSE, -s); break;
     case EP_VE5: atomicAdd(acc + ACC_SPRSET + 5, -s); break;
     case EP_VE8: atomicAdd(acc + ACC_SPRSET + 8, -s); atomicAdd(acc + ACC_SPRSE, -s); break;
+  }
+}
+
+// A batch's energy sums: one block per system adds up all its quantities in
+// one pass over its atoms (every quantity in a fixed order, as k_ereduce),
+// instead of a block per (quantity, system).
+constexpr int ERS_THREADS = 128;
+
+__global__ void __launch_bounds__(ERS_THREADS) k_ereduce_sys(int n, int mask, const SysP *__restrict__ sp,
+                                                              const float *__restrict__ epart,
+                                                              const double *__restrict__ epart64,
+                                                              double *__restrict__ accs, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  __shared__ double red[EP_COUNT][ERS_THREADS / 32];
+  const int sy = blockIdx.x;
+  const int a0 = sp[sy].a0, a1 = a0 + sp[sy].n;
+  const int q0 = (mask & 1) ? 0 : EP_EEL;
+  const int q1 = (mask & 2) && sp[sy].coul >= 0 ? EP_COUNT : EP_EEL;
+  double s[EP_COUNT];
+#pragma unroll
+  for (int q = 0; q < EP_COUNT; q++) s[q] = 0.0;
+  for (int t = a0 + threadIdx.x; t < a1; t += blockDim.x) {
+    const double h = (mask & 1) ? epart64[t] : 0.0;
+#pragma unroll
+    for (int q = 0; q < EP_COUNT; q++)
+      if (q >= q0 && q < q1) s[q] += (double)epart[(size_t)q * n + t] + ((q == EP_ELJ || q == EP_ELJH) ? h : 0.0);
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < EP_COUNT; q++) {
+    const double v = warp_sum(s[q]);
+    if (lane == 0) red[q][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < EP_COUNT) {
+    const int q = threadIdx.x;
+    if (q < q0 || q >= q1) return;
+    double v = 0.0;
+    for (int k = 0; k < ERS_THREADS / 32; k++) v += red[q][k];
+    ep_to_acc(q, 0.5 * v, accs + (size_t)sy * ACC_STRIDE, sp[sy].tablast_e);
   }
 }
 
@@ -1046,10 +1092,15 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   tend(c, 0, e0);
   c->launches += 2;
   if (iflg == 1) {
-    // one large system: its atoms over several blocks per quantity
-    const int nz = c->nsys > 1 ? 1 : std::max(1, std::min(EREDUCE_MAX_Z, c->n / 8192));
-    k_ereduce<<<dim3(EP_COUNT, c->nsys, nz), c->nsys > 1 ? 256 : 512, 0, c->st>>>(
-        c->n, mask, c->sp, c->epart, epart_hi(c), c->acc, c->ered, c->ered_done, c->gate);
+    if (c->nsys > 1) {
+      // a batch: one block per system, every quantity in one pass
+      k_ereduce_sys<<<c->nsys, ERS_THREADS, 0, c->st>>>(c->n, mask, c->sp, c->epart, epart_hi(c), c->acc, c->gate);
+    } else {
+      // one large system: its atoms over several blocks per quantity
+      const int nz = std::max(1, std::min(EREDUCE_MAX_Z, c->n / 8192));
+      k_ereduce<<<dim3(EP_COUNT, 1, nz), 512, 0, c->st>>>(c->n, mask, c->sp, c->epart, epart_hi(c), c->acc,
+                                                           c->ered, c->ered_done, c->gate);
+    }
     c->launches++;
   }
   CKL(c);
