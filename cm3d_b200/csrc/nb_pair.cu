@@ -471,7 +471,9 @@ __global__ void __launch_bounds__(512, 1) k_pair_win(
 // system first (host-ordered), so the long ones start early.
 constexpr int SYS_PART = 1024;
 
-template <int TPA, bool SMALLBOX, bool NEED_S, bool BATCH, bool STAGE = false>
+// TABLE2: the compact LJ table (2 float4 per knot), for the full force
+// without the RESPA switch (iflg 1, no short-force copy).
+template <int TPA, bool SMALLBOX, bool NEED_S, bool BATCH, bool STAGE = false, bool TABLE2 = false>
 __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
     MixedP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ nlen, int stride, const uint32_t *__restrict__ nbr, const float4 *__restrict__ gshift,
@@ -607,15 +609,16 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
             }
             p -= (float)kk;
             float4 a0, a1, a2;
-            if (STAGE) {
+            const int knot = in * P.ntable + kk;
+            if (STAGE || TABLE2) {
               // {d0, dA, dB, v0 hi} {vA, vB, v0 lo, -}
-              const float4 *T = st_tl + 2 * (in * P.ntable + kk);
+              const float4 *T = (STAGE ? st_tl : gtl2) + 2 * knot;
               a0 = T[0];
               const float4 b = T[1];
               a1 = make_float4(b.x, b.y, 0.f, 0.f);
               a2 = make_float4(0.f, b.z, 0.f, 0.f);
             } else {
-              const float4 *T = tl + 3 * ((size_t)in * P.ntable + kk);
+              const float4 *T = tl + 3 * knot;
               a0 = T[0];
               a1 = T[1];
               a2 = T[2];
@@ -899,10 +902,10 @@ static size_t smem_bytes(Ctx *c, bool with_tables, int mask) {
   return b;
 }
 
-template <int TPA, bool SB, bool NS, bool BT, bool ST = false>
+template <int TPA, bool SB, bool NS, bool BT, bool ST = false, bool T2 = false>
 static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   const int B = 256;
-  auto kern = k_pair_mixed<TPA, SB, NS, BT, ST>;
+  auto kern = k_pair_mixed<TPA, SB, NS, BT, ST, T2>;
   // the shared-memory limit is a per-device attribute: set it for every
   // device this process launches on
   static unsigned long long attr_devs = 0;
@@ -925,14 +928,14 @@ static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
                                  c->stage_ntypes, c->stage_ninter);
 }
 
-template <bool SB, bool NS, bool BT, bool ST = false>
+template <bool SB, bool NS, bool BT, bool ST = false, bool T2 = false>
 static int launch_tpa(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   switch (c->tpa) {
-    case 4: launch_t<4, SB, NS, BT, ST>(c, P, smem, fout); break;
-    case 8: launch_t<8, SB, NS, BT, ST>(c, P, smem, fout); break;
-    case 16: launch_t<16, SB, NS, BT, ST>(c, P, smem, fout); break;
-    case 32: launch_t<32, SB, NS, BT, ST>(c, P, smem, fout); break;
-    default: launch_t<8, SB, NS, BT, ST>(c, P, smem, fout); break;
+    case 4: launch_t<4, SB, NS, BT, ST, T2>(c, P, smem, fout); break;
+    case 8: launch_t<8, SB, NS, BT, ST, T2>(c, P, smem, fout); break;
+    case 16: launch_t<16, SB, NS, BT, ST, T2>(c, P, smem, fout); break;
+    case 32: launch_t<32, SB, NS, BT, ST, T2>(c, P, smem, fout); break;
+    default: launch_t<8, SB, NS, BT, ST, T2>(c, P, smem, fout); break;
   }
   return CM3D_NB_OK;
 }
@@ -1078,9 +1081,11 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
     P.tab_smem = 0;
     launch_tpa<false, false, true, true>(c, P, stage_bytes(c), fout);
   } else if ((c->pair_used = CM3D_NB_PAIR_GATHER), c->nsys > 1) {
-    // several systems: per-system parameters and tables from global memory
+    // several systems: per-system parameters and tables from global memory;
+    // the full force without the switch reads the compact LJ table
     P.tab_smem = 0;
     if (ns) launch_tpa<false, true, true>(c, P, 0, fout);
+    else if (iflg == 1) launch_tpa<false, false, true, false, true>(c, P, 0, fout);
     else launch_tpa<false, false, true>(c, P, 0, fout);
   } else if (sb) {
     if (ns) launch_tpa<true, true, false>(c, P, smem, fout);
@@ -1204,15 +1209,16 @@ int pair_setup(Ctx *c) {
       CK(cudaMalloc(&c->sys_items, sizeof(int4) * items.size()));
       CK(cudaMemcpy(c->sys_items, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice));
       c->nsys_items = (int)items.size();
-      // compact LJ coefficients: {d0, dA, dB, v0 hi} {vA, vB, v0 lo, 0}
-      std::vector<float4> tl2((size_t)2 * (ni > 0 ? ni : 1) * nt, make_float4(0.f, 0.f, 0.f, 0.f));
-      for (size_t k = 0; k < (size_t)ni * nt; k++) {
-        tl2[2 * k] = tl[3 * k];
-        tl2[2 * k + 1] = make_float4(tl[3 * k + 1].x, tl[3 * k + 1].y, tl[3 * k + 2].y, 0.f);
-      }
-      CK(cudaMalloc(&c->ftab_lj2, sizeof(float4) * tl2.size()));
-      CK(cudaMemcpy(c->ftab_lj2, tl2.data(), sizeof(float4) * tl2.size(), cudaMemcpyHostToDevice));
     }
+    // compact LJ coefficients for a batch's full force without the switch:
+    // {d0, dA, dB, v0 hi} {vA, vB, v0 lo, 0}
+    std::vector<float4> tl2((size_t)2 * (ni > 0 ? ni : 1) * nt, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (size_t k = 0; k < (size_t)ni * nt; k++) {
+      tl2[2 * k] = tl[3 * k];
+      tl2[2 * k + 1] = make_float4(tl[3 * k + 1].x, tl[3 * k + 1].y, tl[3 * k + 2].y, 0.f);
+    }
+    CK(cudaMalloc(&c->ftab_lj2, sizeof(float4) * tl2.size()));
+    CK(cudaMemcpy(c->ftab_lj2, tl2.data(), sizeof(float4) * tl2.size(), cudaMemcpyHostToDevice));
   }
   if (c->tpa == 0) {
     // 8 lanes per atom: a group reads a full 32-byte sector of the list; more
