@@ -958,7 +958,7 @@ static bool stage_applies(Ctx *c, int iflg, bool ns) {
 // (nothing launched) when it does not apply and the list-gather kernel runs.
 // The window capacity is what shared memory leaves after the tables; an item
 // whose 27 cells hold more atoms falls back to global loads inside the kernel.
-constexpr size_t WIN_STATIC_SMEM = 1024;   // >= k_pair_win's static shared arrays (436 bytes)
+constexpr size_t WIN_STATIC_SMEM = 1024;   // >= k_pair_win's static shared arrays (448 bytes)
 
 template <int TPA, bool NS, bool EL>
 static void launch_win_t(Ctx *c, const MixedP &P, const WinP &W, size_t smem, double *fout) {
