@@ -196,6 +196,7 @@ struct Ctx {
   double *ered = nullptr;              // k_ereduce: per-block partial sums of one large system
   unsigned *ered_done = nullptr;       // k_ereduce: blocks finished per quantity
   int lw_cap = 0;                      // staged list build: neighbourhood atoms per block (0: off)
+  int *rb_scan = nullptr;              // staged list build: cells rebuilt before each system (nsys + 1)
   size_t lw_smem_max = 0;              // its shared-memory limit (bytes)
   int win_ok = 1;                      // single systems may use the windowed pair kernel
   int win_env_off = 0;                 // CM3D_NB_PAIR_KERNEL=list: never

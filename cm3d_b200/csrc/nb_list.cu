@@ -621,6 +621,48 @@ __global__ void __launch_bounds__(256) k_list_full(
                         nullptr, nullptr, nullptr, nullptr, nullptr, 0, false);
 }
 
+// The cells of the systems being rebuilt, as one index range: rb_scan[s] is
+// the number of such cells in systems before s, rb_scan[nsys] their total.
+// A batch rebuilds a few of its systems on most steps; the list kernel then
+// walks those cells only instead of skipping every other system's.
+__global__ void k_rebuild_cells(int nsys, const SysP *__restrict__ sp, const int *__restrict__ sreb, int all,
+                                int *__restrict__ rb_scan, const int *__restrict__ gate) {
+  if (gated_off(gate, 1)) return;
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int base = 0; base < nsys; base += blockDim.x) {
+    const int sy = base + threadIdx.x;
+    const int v = sy < nsys && (all || sreb[sy] != 0) ? sp[sy].ncells : 0;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int t = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= o) t += u;
+      }
+      warp_tot[lane] = t;                              // inclusive over warps
+    }
+    __syncthreads();
+    const int before = carry + (w > 0 ? warp_tot[w - 1] : 0);
+    if (sy < nsys) rb_scan[sy] = before + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_tot[(blockDim.x >> 5) - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rb_scan[nsys] = carry;
+}
+
 // Mixed mode, block per cell: the block stages the cell's stencil
 // neighbourhood (every candidate of every atom of the cell: FP32 positions
 // moved by their cell's shift, sorted index + the cell's shift code, atom
@@ -637,8 +679,8 @@ constexpr size_t LW_BYTES_PER_ATOM = sizeof(float4) + 3 * sizeof(int);   // s_x,
 constexpr long long LW_MAX_CAP = 2048;     // largest staged neighbourhood (57 KB)
 
 __global__ void __launch_bounds__(LW_THREADS) k_list_win(
-    int ncells, const int *__restrict__ cell_sys, const SysP *__restrict__ sp, const int *__restrict__ sreb,
-    int all, int n, int stride, int cap, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
+    int nsys, const int *__restrict__ rb_scan, const SysP *__restrict__ sp, int n, int stride, int cap,
+    const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
     const float4 *__restrict__ xq, const double *__restrict__ pos, const int *__restrict__ itype,
     const int *__restrict__ map, const double *__restrict__ icut, const double *__restrict__ q,
     const int *__restrict__ excl_off, const int *__restrict__ excl_idx, const int *__restrict__ cexcl_off,
@@ -651,13 +693,22 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
   int *s_meta = s_j + cap;                               // cap: type * 2 + charged
   __shared__ int qs[LW_THREADS / 32][LQ];
   __shared__ float qrs[LW_THREADS / 32][LQ];
-  __shared__ int s_cs[27], s_cn[27], s_off[27], s_code[27], s_tot, s_nw;
+  __shared__ int s_cs[27], s_off[27], s_code[27], s_tot, s_nw;
   __shared__ float4 s_sh[27];
   const int warp = threadIdx.x >> 5;
-  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
-    const int s = cell_sys[c];
-    if (sys_skip(s, sreb, all)) continue;                // whole blocks
+  const int total = rb_scan[nsys];
+  for (int v = blockIdx.x; v < total; v += gridDim.x) {
+    // the system of rebuilt cell v: the last s with rb_scan[s] <= v (systems
+    // without rebuilt cells share their successor's value and are passed)
+    int sa = 0, sb = nsys;
+    while (sb - sa > 1) {
+      const int mid = (sa + sb) >> 1;
+      if (rb_scan[mid] <= v) sa = mid;
+      else sb = mid;
+    }
+    const int s = sa;
     const SysP &P = sp[s];
+    const int c = P.c0 + (v - rb_scan[s]);
     __syncthreads();                                     // the previous neighbourhood is no longer read
     if (threadIdx.x < 32) {
       // the system's stencil around cell c, one stencil cell per lane, in
@@ -678,7 +729,6 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
         const int cs = cell_start[cell];
         cn = cell_start[cell + 1] - cs;
         s_cs[w] = cs;
-        s_cn[w] = cn;
         s_code[w] = (1 - ox) * 9 + (1 - oy) * 3 + (1 - oz);
         s_sh[w] = P.shift[s_code[w]];
       }
@@ -698,18 +748,24 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
     const int tot = s_tot, nw = s_nw;
     const bool staged = tot <= cap;
     if (staged) {
-      for (int w = 0; w < nw; w++) {
-        const int cs = s_cs[w], cn = s_cn[w], off = s_off[w];
-        const int code = s_code[w] << ENT_CODE_SHIFT;
-        const float4 sh = s_sh[w];
-        for (int k = threadIdx.x; k < cn; k += blockDim.x) {
-          const float4 x = xq[cs + k];
-          const int j = cell_atoms[cs + k];
-          s_x[off + k] = make_float4(x.x - sh.x, x.y - sh.y, x.z - sh.z, 0.f);
-          s_u[off + k] = (cs + k) | code;
-          s_j[off + k] = j;
-          s_meta[off + k] = itype[j] * 2 + (q[j] != 0.0 ? 1 : 0);
+      // one pass over the whole neighbourhood, so that every thread's loads
+      // are in flight at once: staged atom g lies in the last stencil cell w
+      // with s_off[w] <= g (empty cells share their successor's offset)
+      for (int g = threadIdx.x; g < tot; g += blockDim.x) {
+        int wa = 0, wb = nw;
+        while (wb - wa > 1) {
+          const int mid = (wa + wb) >> 1;
+          if (s_off[mid] <= g) wa = mid;
+          else wb = mid;
         }
+        const int u = s_cs[wa] + (g - s_off[wa]);
+        const float4 x = xq[u];
+        const int j = cell_atoms[u];
+        const float4 sh = s_sh[wa];
+        s_x[g] = make_float4(x.x - sh.x, x.y - sh.y, x.z - sh.z, 0.f);
+        s_u[g] = u | (s_code[wa] << ENT_CODE_SHIFT);
+        s_j[g] = j;
+        s_meta[g] = itype[j] * 2 + (q[j] != 0.0 ? 1 : 0);
       }
     }
     __syncthreads();
@@ -891,6 +947,7 @@ int list_setup(Ctx *c) {
     if (c->lw_cap < 64 || cap > LW_MAX_CAP) c->lw_cap = 0;
     const char *lk = getenv("CM3D_NB_LIST_KERNEL");
     if (lk && strcmp(lk, "walk") == 0) c->lw_cap = 0;
+    CK(cudaMalloc(&c->rb_scan, sizeof(int) * ((size_t)c->nsys + 1)));
     CK(cudaMalloc(&c->nlen, sizeof(int) * 2 * (size_t)c->n));
     CK(cudaMemset(c->nlen, 0, sizeof(int) * 2 * (size_t)c->n));
     long long s = ((long long)est_max + 31) / 32 * 32;
@@ -986,10 +1043,12 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_list_win, LW_THREADS, smem);
         long long grid = (long long)c->num_sms * (per_sm > 0 ? per_sm : 1);
         if (grid > c->ncells) grid = c->ncells;
+        k_rebuild_cells<<<1, 1024, 0, c->st>>>(c->nsys, c->sp, c->sreb, al, c->rb_scan, gate);
         k_list_win<<<(int)grid, LW_THREADS, smem, c->st>>>(
-            c->ncells, c->cell_sys, c->sp, c->sreb, al, n, c->nbr_stride, c->lw_cap, c->cell_atoms, c->cell_start,
-            c->xq, c->pos, c->itype, c->map, c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx,
-            cimg, c->nbr, c->nlen, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+            c->nsys, c->rb_scan, c->sp, n, c->nbr_stride, c->lw_cap, c->cell_atoms, c->cell_start, c->xq, c->pos,
+            c->itype, c->map, c->icut, c->q, c->excl_off, c->excl_idx, c->cexcl_off, c->cexcl_idx, cimg, c->nbr,
+            c->nlen, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate);
+        c->launches++;
       } else {
         k_list_full<<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
             n, c->sp, c->sys_of, c->sreb, al, c->nbr_stride, c->cell_atoms, c->cell_start, c->xq, c->pos,
