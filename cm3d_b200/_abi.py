@@ -7,7 +7,8 @@ OK = 0
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_STATE, ERR_OVERFLOW, ERR_NODEV = -1, -2, -3, -4, -5, -6
 
 PLAIN_FP64, MIXED = 0, 1
-FXL, FXS, FXA = 0, 1, 2
+FXL, FXS, FXA, FXR = 0, 1, 2, 3
+MAXPOWER_TORS = 7
 LIST_T, LIST_S, LIST_TE, LIST_SE = 0, 1, 2, 3
 
 _dp = C.POINTER(C.c_double)
@@ -45,6 +46,20 @@ class SystemDesc(C.Structure):
         ("ibend", _ip), ("jbend", _ip), ("kbend", _ip), ("idxbend", _ip), ("itypbend", _ip),
         ("eqbend", _dp), ("fkbend", _dp),
         ("ntors", C.c_int), ("n14", C.c_int), ("nbondx", C.c_int),
+        ("ntors_types", C.c_int),
+        ("itors", _ip), ("jtors", _ip), ("ktors", _ip), ("ltors", _ip), ("idxtors", _ip),
+        ("tors_ind_pot", _ip), ("tors_ind_pot_num", _ip),
+        ("ntors_harm", C.c_int), ("eqtors", _dp), ("fktors", _dp),
+        ("ntors_series", C.c_int), ("vphi", _dp),
+        ("n14_types", C.c_int), ("n14table", C.c_int),
+        ("i14", _ip), ("j14", _ip), ("i14dx", _ip),
+        ("r14min2", _dp), ("r14max2", _dp), ("dx214tab", _dp),
+        ("v14tab", _dp), ("dv14tab", _dp),
+        ("scale_onefour", C.c_double), ("scale_onefour_e", C.c_double),
+        ("nbondx_types", C.c_int),
+        ("ibondx", _ip), ("jbondx", _ip), ("kbondx", _ip), ("idxbondx", _ip),
+        ("eq1bondx", _dp), ("eq2bondx", _dp), ("fkbondx", _dp),
+        ("nfreeze", C.c_int), ("ifreeze", _ip),
     ]
 
 
@@ -65,6 +80,9 @@ class Energies(C.Structure):
         ("zke", C.c_double), ("p2m_tensor", C.c_double * 9),
         ("prsi", C.c_double), ("prs_tensor", C.c_double * 9), ("tiout", C.c_double),
         ("poter", C.c_double), ("poth", C.c_double), ("potra", C.c_double),
+        ("vtors", C.c_double), ("wtors", C.c_double), ("vonfo", C.c_double),
+        ("vonfo_e", C.c_double), ("wonfo", C.c_double), ("wonfo_e", C.c_double),
+        ("UI", C.c_double), ("WI", C.c_double), ("WItensor", C.c_double * 9),
     ]
 
     @classmethod

@@ -280,6 +280,7 @@ def build_system(wl: Workload) -> System:
     sysm["ntors"] = 0
     sysm["n14"] = 0
     sysm["nbondx"] = 0
+    sysm["nfreeze"] = 0
     sysm["ncells"] = int(kw["ncell_div"])
     sysm["nocell_all"] = 1
     sysm["nlen"] = int(kw["nlen"])

@@ -1,8 +1,9 @@
 """Host-side description of one CM3D system for the engine.
 
 `System` holds, as numpy arrays, exactly the fields of CM3D's SIMPARMS /
-COORDS / INTER / COUL / BONDS / BENDS structs that the nonbonded path and the
-inner RESPA level read (include/md_typedef.h:59-268), under CM3D's names.
+COORDS / INTER / COUL / BONDS / BENDS / TORS / ONFO / BONDXS structs that the
+nonbonded path and the intramolecular RESPA levels read
+(include/md_typedef.h:59-268), under CM3D's names.
 `System.desc()` packs them into the C ABI struct `cm3d_nb_system`
 (include/cm3d_nb.h) without copying.
 
@@ -22,16 +23,21 @@ from . import _abi
 _F64 = ("hmat", "px", "py", "pz", "vx", "vy", "vz", "amass", "qch", "vtab", "dvtab",
         "switchs", "rmaxs_cut2", "rmins_cut2", "rmaxl_cut2", "rminl_cut2",
         "rmaxs_skin2", "rmaxl_skin2", "dx2tab", "coultab", "dcoultab", "switchse",
-        "eqbond", "fkbond", "eqbend", "fkbend")
+        "eqbond", "fkbond", "eqbend", "fkbend", "eqtors", "fktors", "vphi", "r14min2",
+        "r14max2", "dx214tab", "v14tab", "dv14tab", "eq1bondx", "eq2bondx", "fkbondx")
 _I32 = ("itype", "map", "excl_off", "excl_idx", "cexcl_off", "cexcl_idx", "ka", "kb",
         "kc", "iecorr", "jecorr", "ibond", "jbond", "idxbond", "itypbond", "ibend",
-        "jbend", "kbend", "idxbend", "itypbend")
+        "jbend", "kbend", "idxbend", "itypbend", "itors", "jtors", "ktors", "ltors",
+        "idxtors", "tors_ind_pot", "tors_ind_pot_num", "i14", "j14", "i14dx", "ibondx",
+        "jbondx", "kbondx", "idxbondx", "ifreeze")
 _SCALARS_F = ("dt", "vlrc", "wlrc", "skin", "rheal", "dx2coul", "rmins_coul2",
               "rmaxs_coul2", "rminl_coul2", "rmaxl_coul2", "rmaxs_skin2_e",
-              "rmaxl_skin2_e", "kappa", "falp2", "ewald_self", "ewald_bkg", "temp")
+              "rmaxl_skin2_e", "kappa", "falp2", "ewald_self", "ewald_bkg", "temp",
+              "scale_onefour", "scale_onefour_e")
 _SCALARS_I = ("natoms", "iperd", "nres_lrf", "nres_intra", "nres_tors", "ndof",
               "ntypes", "ninter", "ntable", "ktot", "necorr", "nbonds", "nbends",
-              "ntors", "n14", "nbondx", "ncells", "nocell_all", "nlen")
+              "ntors", "n14", "nbondx", "ncells", "nocell_all", "nlen", "n14table", "n14types",
+              "nfreeze")
 
 
 class System:
@@ -125,11 +131,15 @@ class System:
         for k in ("px", "py", "pz", "vx", "vy", "vz", "amass", "qch", "vtab", "dvtab",
                   "switchs", "rmaxs_cut2", "rmins_cut2", "rmaxl_cut2", "rminl_cut2",
                   "rmaxs_skin2", "rmaxl_skin2", "dx2tab", "coultab", "dcoultab",
-                  "switchse", "eqbond", "fkbond", "eqbend", "fkbend"):
+                  "switchse", "eqbond", "fkbond", "eqbend", "fkbend", "eqtors", "fktors",
+                  "vphi", "r14min2", "r14max2", "dx214tab", "v14tab", "dv14tab", "eq1bondx",
+                  "eq2bondx", "fkbondx"):
             setattr(d, k, self._ptr(k, C.c_double))
         for k in ("itype", "map", "excl_off", "excl_idx", "cexcl_off", "cexcl_idx",
                   "ka", "kb", "kc", "iecorr", "jecorr", "ibond", "jbond", "idxbond",
-                  "itypbond", "ibend", "jbend", "kbend", "idxbend", "itypbend"):
+                  "itypbond", "ibend", "jbend", "kbend", "idxbend", "itypbend", "itors",
+                  "jtors", "ktors", "ltors", "idxtors", "tors_ind_pot", "tors_ind_pot_num",
+                  "i14", "j14", "i14dx", "ibondx", "jbondx", "kbondx", "idxbondx", "ifreeze"):
             setattr(d, k, self._ptr(k, C.c_int))
         d.ntypes = s["ntypes"]
         d.ninter = s["ninter"]
@@ -149,5 +159,15 @@ class System:
         d.ntors = s.get("ntors", 0)
         d.n14 = s.get("n14", 0)
         d.nbondx = s.get("nbondx", 0)
+        # torsions, 1-4 pairs and cross bonds (TORS / ONFO / BONDXS)
+        d.ntors_types = int(a["tors_ind_pot"].size) if "tors_ind_pot" in a else 0
+        d.ntors_harm = int(a["eqtors"].size) if "eqtors" in a else 0
+        d.ntors_series = int(a["vphi"].size) // _abi.MAXPOWER_TORS if "vphi" in a else 0
+        d.n14_types = int(a["r14min2"].size) if "r14min2" in a else 0
+        d.n14table = s.get("n14table", 0)
+        d.scale_onefour = s.get("scale_onefour", 1.0)
+        d.scale_onefour_e = s.get("scale_onefour_e", 1.0)
+        d.nbondx_types = int(a["eq1bondx"].size) if "eq1bondx" in a else 0
+        d.nfreeze = s.get("nfreeze", 0)
         self._desc = d
         return d

@@ -51,7 +51,10 @@ extern "C" {
 /* which force block (COORDS fields) */
 #define CM3D_NB_FXL 0             /* fxl,fyl,fzl: long-range nonbonded */
 #define CM3D_NB_FXS 1             /* fxs,fys,fzs: short (switched) nonbonded */
-#define CM3D_NB_FXA 2             /* fxa,fya,fza: bonds + bends */
+#define CM3D_NB_FXA 2             /* fxa,fya,fza: bonds + bends + cross bonds */
+#define CM3D_NB_FXR 3             /* fxr,fyr,fzr: torsions + 1-4 pairs */
+
+#define CM3D_NB_MAXPOWER_TORS 7   /* MAXPOWER_TORS (include/md_defines.h:43) */
 
 /* which pair list (NGBR fields) */
 #define CM3D_NB_LIST_T 0          /* inpt/jnpt:   LJ, r^2 < rmaxl_skin2[intr] */
@@ -112,7 +115,36 @@ typedef struct cm3d_nb_system {
   int nbends, nbend_types;
   const int *ibend, *jbend, *kbend, *idxbend, *itypbend;
   const double *eqbend, *fkbend;
-  int ntors, n14, nbondx;    /* must be 0 for cm3d_nb_step() */
+  /* TORS / ONFO / BONDXS (md_typedef.h:81-100).  Torsions and 1-4 pairs
+     make the torsion RESPA level (force level 3 into fxr: ftors
+     md_ftors.c:117, fonfo md_fonefour.c:70); cross bonds join the bonds and
+     bends of level 2 (fbondx md_fbocross.c:40). */
+  int ntors, n14, nbondx;
+  int ntors_types;                            /* TORS.itypes */
+  const int *itors, *jtors, *ktors, *ltors;   /* [ntors] */
+  const int *idxtors;                         /* [ntors] torsion type */
+  const int *tors_ind_pot;                    /* [ntors_types] form: 0 harmonic in phi,
+                                                 1 cosine power series (2, cosine
+                                                 with phases, is refused) */
+  const int *tors_ind_pot_num;                /* [ntors_types] row of eqtors/fktors (form 0)
+                                                 or of vphi (form 1) */
+  int ntors_harm;                             /* rows of eqtors / fktors */
+  const double *eqtors, *fktors;
+  int ntors_series;                           /* rows of vphi */
+  const double *vphi;                         /* [ntors_series * CM3D_NB_MAXPOWER_TORS] */
+  int n14_types, n14table;
+  const int *i14, *j14, *i14dx;               /* [n14] atoms and 1-4 type */
+  const double *r14min2, *r14max2, *dx214tab; /* [n14_types] table ranges (squared) */
+  const double *v14tab, *dv14tab;             /* [n14_types * n14table] V and (dV/dr)/r */
+  double scale_onefour, scale_onefour_e;
+  int nbondx_types;
+  const int *ibondx, *jbondx, *kbondx, *idxbondx;   /* [nbondx] */
+  const double *eq1bondx, *eq2bondx, *fkbondx;      /* [nbondx_types] */
+  /* frozen atoms (SIMPARMS.nfreeze, COORDS.ifreeze): every force level ends
+     with their velocities and forces set to zero (freeze_atom
+     md_fcntr.c:311-329) */
+  int nfreeze;
+  const int *ifreeze;
 } cm3d_nb_system;
 
 typedef struct cm3d_nb_options {
@@ -134,6 +166,12 @@ typedef struct cm3d_nb_energies {
   double US, U, W, Wtensor[9];
   double zke, p2m_tensor[9];                         /* get_p2mt md_fcntr.c:332 */
   double prsi, prs_tensor[9], tiout, poter, poth, potra;
+  /* torsion level and cross bonds: getvtors md_ftors.c:296, getvonfo
+     md_fonefour.c:160, getvbondx md_fbocross.c:100 (which adds the cross
+     bonds' energy and virial to vbond / wbond); UI, WI and WItensor sum the
+     intramolecular terms as getvireal does (md_fcntr.c:206-215) */
+  double vtors, wtors, vonfo, vonfo_e, wonfo, wonfo_e;
+  double UI, WI, WItensor[9];
 } cm3d_nb_energies;
 
 typedef struct cm3d_nb_status_t {
@@ -205,8 +243,9 @@ int cm3d_nb_get_ngbr(cm3d_nb_ctx *ctx);
                      when the previous rebuild is fewer than 3 steps old. */
 int cm3d_nb_nrefsh(cm3d_nb_ctx *ctx, int istep, int *rebuilt);
 /* force()           energy/control/md_fcntr.c:44 for iflg 0 (short
-                     nonbonded), 1 (full nonbonded + Ewald) and 2 (bonds and
-                     bends); results stored as accelerations. */
+                     nonbonded), 1 (full nonbonded + Ewald), 2 (bonds, bends
+                     and cross bonds) and 3 (torsions and 1-4 pairs); results
+                     stored as accelerations. */
 int cm3d_nb_force(cm3d_nb_ctx *ctx, int iflg);
 /* force_ter()       energy/control/md_finter.c:110 -> force_npol()
                      energy/inter/md_fnopol.c:46: LJ over the t (iflg 1) or

@@ -38,7 +38,8 @@ def lib() -> C.CDLL:
         L.orc_create.restype = vp
         L.orc_create.argtypes = [C.POINTER(_abi.SystemDesc), C.c_int, C.c_int, C.c_int]
         for name in ("orc_destroy", "orc_get_ngbr", "orc_fk_ewald", "orc_ecorr",
-                     "orc_fbond", "orc_fbend", "orc_step_init"):
+                     "orc_fbond", "orc_fbend", "orc_fbondx", "orc_ftors", "orc_fonfo",
+                     "orc_step_init"):
             getattr(L, name).argtypes = [vp]
             getattr(L, name).restype = None
         for name in ("orc_force", "orc_force_ter", "orc_force_ter_e", "orc_rmass",
@@ -141,6 +142,15 @@ class Oracle:
 
     def fbond(self):
         lib().orc_fbond(self._h)
+
+    def fbondx(self):
+        lib().orc_fbondx(self._h)
+
+    def ftors(self):
+        lib().orc_ftors(self._h)
+
+    def fonfo(self):
+        lib().orc_fonfo(self._h)
 
     def fbend(self):
         lib().orc_fbend(self._h)

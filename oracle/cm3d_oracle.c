@@ -58,6 +58,16 @@ struct orc {
   double vk_ewald, vp_ewald, vp_ewald_tensor[9];
   double pot_ecorr, prs_ecorr, prs_ecorr_tensor[9];
   double vbond, wbond, wbondt[9], vbend, wbend, wbendt[9];
+  /* TORS / ONFO / BONDXS (md_typedef.h:81-100) and the torsion-level forces */
+  int ntors, *itors, *jtors, *ktors, *ltors, *idxtors, *tors_form, *tors_row;
+  double *eqtors, *fktors, *vphi;
+  int n14, n14table, *i14, *j14, *i14dx;
+  double *r14min2, *r14max2, *dx214tab, *v14tab, *dv14tab, scale14, scale14e;
+  int nbondx, *ibondx, *jbondx, *kbondx, *idxbondx;
+  double *eq1bondx, *eq2bondx, *fkbondx;
+  double *fxr;
+  int nfreeze, *ifreeze;
+  double vtors, wtors, wtorst[9], vonfo, vonfo_e, wonfo, wonfo_e, wonfot[9], wonfoet[9], wbondxt[9];
 };
 
 static void *dup(const void *p, size_t bytes)
@@ -217,6 +227,46 @@ orc *orc_create(const cm3d_nb_system *s, int ncells, int nocell_all, int nlen)
   o->itypbend = (int *)dup(s->itypbend, s->nbend_types * 4.);
   o->eqbend = (double *)dup(s->eqbend, s->nbend_types * 8.);
   o->fkbend = (double *)dup(s->fkbend, s->nbend_types * 8.);
+  o->ntors = s->ntors;
+  if (s->ntors > 0) {
+    o->itors = (int *)dup(s->itors, s->ntors * 4.);
+    o->jtors = (int *)dup(s->jtors, s->ntors * 4.);
+    o->ktors = (int *)dup(s->ktors, s->ntors * 4.);
+    o->ltors = (int *)dup(s->ltors, s->ntors * 4.);
+    o->idxtors = (int *)dup(s->idxtors, s->ntors * 4.);
+    o->tors_form = (int *)dup(s->tors_ind_pot, s->ntors_types * 4.);
+    o->tors_row = (int *)dup(s->tors_ind_pot_num, s->ntors_types * 4.);
+    o->eqtors = (double *)dup(s->eqtors, s->ntors_harm * 8.);
+    o->fktors = (double *)dup(s->fktors, s->ntors_harm * 8.);
+    o->vphi = (double *)dup(s->vphi, (double)s->ntors_series * CM3D_NB_MAXPOWER_TORS * 8.);
+  }
+  o->n14 = s->n14;
+  if (s->n14 > 0) {
+    o->n14table = s->n14table;
+    o->i14 = (int *)dup(s->i14, s->n14 * 4.);
+    o->j14 = (int *)dup(s->j14, s->n14 * 4.);
+    o->i14dx = (int *)dup(s->i14dx, s->n14 * 4.);
+    o->r14min2 = (double *)dup(s->r14min2, s->n14_types * 8.);
+    o->r14max2 = (double *)dup(s->r14max2, s->n14_types * 8.);
+    o->dx214tab = (double *)dup(s->dx214tab, s->n14_types * 8.);
+    o->v14tab = (double *)dup(s->v14tab, (double)s->n14_types * s->n14table * 8.);
+    o->dv14tab = (double *)dup(s->dv14tab, (double)s->n14_types * s->n14table * 8.);
+    o->scale14 = s->scale_onefour;
+    o->scale14e = s->scale_onefour_e;
+  }
+  o->nbondx = s->nbondx;
+  if (s->nbondx > 0) {
+    o->ibondx = (int *)dup(s->ibondx, s->nbondx * 4.);
+    o->jbondx = (int *)dup(s->jbondx, s->nbondx * 4.);
+    o->kbondx = (int *)dup(s->kbondx, s->nbondx * 4.);
+    o->idxbondx = (int *)dup(s->idxbondx, s->nbondx * 4.);
+    o->eq1bondx = (double *)dup(s->eq1bondx, s->nbondx_types * 8.);
+    o->eq2bondx = (double *)dup(s->eq2bondx, s->nbondx_types * 8.);
+    o->fkbondx = (double *)dup(s->fkbondx, s->nbondx_types * 8.);
+  }
+  o->fxr = (double *)calloc(3 * (size_t)n + 1, 8);
+  o->nfreeze = s->nfreeze;
+  o->ifreeze = (int *)dup(s->ifreeze, s->nfreeze * 4.);
   o->fxl = (double *)calloc(3 * (size_t)n + 1, 8);
   o->fxs = (double *)calloc(3 * (size_t)n + 1, 8);
   o->fxa = (double *)calloc(3 * (size_t)n + 1, 8);
@@ -240,7 +290,11 @@ void orc_destroy(orc *o)
                   o->jbend, o->kbend, o->idxbend, o->itypbend, o->eqbend, o->fkbend,
                   o->fxl, o->fxs, o->fxa, o->scr, o->rec, o->dxn, o->inpt, o->jnpt,
                   o->inps, o->jnps, o->inpte, o->jnpte, o->inpse, o->jnpse, o->icell,
-                  o->jcell, o->icelle, o->jcelle, o->hlist, o->lnk};
+                  o->jcell, o->icelle, o->jcelle, o->hlist, o->lnk, o->itors, o->jtors,
+                  o->ktors, o->ltors, o->idxtors, o->tors_form, o->tors_row, o->eqtors,
+                  o->fktors, o->vphi, o->i14, o->j14, o->i14dx, o->r14min2, o->r14max2,
+                  o->dx214tab, o->v14tab, o->dv14tab, o->ibondx, o->jbondx, o->kbondx,
+                  o->idxbondx, o->eq1bondx, o->eq2bondx, o->fkbondx, o->fxr, o->ifreeze};
   size_t i;
   for (i = 0; i < sizeof ptrs / sizeof ptrs[0]; i++) free(ptrs[i]);
   free(o);
@@ -272,7 +326,7 @@ void orc_get_velocities(orc *o, double *vx, double *vy, double *vz)
 }
 static double *block(orc *o, int which)
 {
-  return which == 0 ? o->fxl : which == 1 ? o->fxs : o->fxa;
+  return which == 0 ? o->fxl : which == 1 ? o->fxs : which == 2 ? o->fxa : o->fxr;
 }
 void orc_get_forces(orc *o, int which, double *fx, double *fy, double *fz)
 {
@@ -936,6 +990,230 @@ void orc_fbend(orc *o)
   free(f9);
 }
 
+/* fbondx  energy/intra/md_fbocross.c:40-97: the cross (bond-bond) term
+   fk (|ri - rj| - eq1)(|rj - rk| - eq2) */
+void orc_fbondx(orc *o)
+{
+  int nb, n = o->n;
+  double *fx = o->fxa, *fy = o->fxa + n, *fz = o->fxa + 2 * n;
+  for (nb = 0; nb < o->nbondx; nb++) {
+    int i = o->ibondx[nb], j = o->jbondx[nb], k = o->kbondx[nb], t = o->idxbondx[nb];
+    double ax = o->px[i] - o->px[j], ay = o->py[i] - o->py[j], az = o->pz[i] - o->pz[j];
+    double al = sqrt(ax * ax + ay * ay + az * az);
+    double bx = o->px[j] - o->px[k], by = o->py[j] - o->py[k], bz = o->pz[j] - o->pz[k];
+    double bl = sqrt(bx * bx + by * by + bz * bz);
+    double dr1 = al - o->eq1bondx[t], dr2 = bl - o->eq2bondx[t];
+    double fr1 = o->fkbondx[t] * dr2 / al, fr2 = o->fkbondx[t] * dr1 / bl;
+    fx[i] += -fr1 * ax; fy[i] += -fr1 * ay; fz[i] += -fr1 * az;
+    fx[j] += fr1 * ax - fr2 * bx; fy[j] += fr1 * ay - fr2 * by; fz[j] += fr1 * az - fr2 * bz;
+    fx[k] += fr2 * bx; fy[k] += fr2 * by; fz[k] += fr2 * bz;
+  }
+}
+
+/* One torsion i-j-k-l (md_ftors.c:161-289): with a = ri - rj, b = rj - rk,
+   c = rk - rl and the plane normals d = a x b, e = b x c, cos(phi) =
+   d.e / (|d| |e|).  dcos/dr of atom m is (dF_m - cos dG_m) / (|d| |e|), F = d.e
+   and G = |d| |e|; u1..u4 receive dU/dcos times that (the force is its
+   negative).  Returns cos(phi); *pot gets U, *dudcos_out dU/dcos / G. */
+typedef struct {
+  double a[3], b[3], c[3];
+  double dudcos;                         /* dU/dcos / G */
+  double u4[3];                          /* dF_4 - cos dG_4 */
+  double g1[3], g2[3], g3[3], g4[3];     /* dudcos (dF_m - cos dG_m) */
+} tors_terms;
+
+static double torsion(orc *o, int nt, double *pot, tors_terms *T)
+{
+  int i = o->itors[nt], j = o->jtors[nt], k = o->ktors[nt], l = o->ltors[nt];
+  int t = o->idxtors[nt], row = o->tors_row[t], m;
+  double ax = o->px[i] - o->px[j], ay = o->py[i] - o->py[j], az = o->pz[i] - o->pz[j];
+  double bx = o->px[j] - o->px[k], by = o->py[j] - o->py[k], bz = o->pz[j] - o->pz[k];
+  double cx = o->px[k] - o->px[l], cy = o->py[k] - o->py[l], cz = o->pz[k] - o->pz[l];
+  double dx = ay * bz - az * by, dy = az * bx - ax * bz, dz = ax * by - ay * bx;
+  double dl = sqrt(dx * dx + dy * dy + dz * dz);
+  double ex = by * cz - bz * cy, ey = bz * cx - bx * cz, ez = bx * cy - by * cx;
+  double el = sqrt(ex * ex + ey * ey + ez * ez);
+  double cphi = (dx * ex + dy * ey + dz * ez) / (dl * el);
+  double dudcos = 0., g, dre, erd;
+  if (o->tors_form[t] == 0) {
+    /* harmonic in phi (md_ftors.c:194-210, energy :362-381) */
+    double phi = 0., dphi;
+    if (cphi >= 1.0 || cphi <= -1.0) {
+      dphi = phi - o->eqtors[row];
+      dudcos = 0.;
+    } else {
+      phi = acos(cphi);
+      dphi = phi - o->eqtors[row];
+      dudcos = (o->fktors[row] * dphi) * (-1. / sqrt(1. - cphi * cphi));
+    }
+    *pot = .5 * o->fktors[row] * dphi * dphi;
+  } else {
+    /* power series in cos(phi) (md_ftors.c:211-220, energy :382-394) */
+    const double *v = o->vphi + (size_t)row * CM3D_NB_MAXPOWER_TORS;
+    double tpot = v[CM3D_NB_MAXPOWER_TORS - 1];
+    dudcos = ((double)CM3D_NB_MAXPOWER_TORS - 1.) * v[CM3D_NB_MAXPOWER_TORS - 1];
+    for (m = CM3D_NB_MAXPOWER_TORS - 2; m > 0; m--) dudcos = dudcos * cphi + v[m] * (double)m;
+    for (m = CM3D_NB_MAXPOWER_TORS - 2; m >= 0; m--) tpot = tpot * cphi + v[m];
+    *pot = tpot;
+  }
+  g = dl * el;
+  dre = dl / el;
+  erd = el / dl;
+  dudcos *= 1. / g;
+  T->a[0] = ax; T->a[1] = ay; T->a[2] = az;
+  T->b[0] = bx; T->b[1] = by; T->b[2] = bz;
+  T->c[0] = cx; T->c[1] = cy; T->c[2] = cz;
+  {
+    double f1x = by * ez - bz * ey, f1y = bz * ex - bx * ez, f1z = bx * ey - by * ex;
+    double f2x = (cy * dz - cz * dy + (az + bz) * ey - (ay + by) * ez);
+    double f2y = (cz * dx - cx * dz + (ax + bx) * ez - (az + bz) * ex);
+    double f2z = (cx * dy - cy * dx + (ay + by) * ex - (ax + bx) * ey);
+    double f3x = (ay * ez - az * ey + (bz + cz) * dy - (by + cy) * dz);
+    double f3y = (az * ex - ax * ez + (bx + cx) * dz - (bz + cz) * dx);
+    double f3z = (ax * ey - ay * ex + (by + cy) * dx - (bx + cx) * dy);
+    double f4x = by * dz - bz * dy, f4y = bz * dx - bx * dz, f4z = bx * dy - by * dx;
+    double h1x = (by * dz - bz * dy) * erd, h1y = (bz * dx - bx * dz) * erd, h1z = (bx * dy - by * dx) * erd;
+    double h2x = ((dy * (az + bz) - dz * (ay + by)) * erd + (cy * ez - cz * ey) * dre);
+    double h2y = ((dz * (ax + bx) - dx * (az + bz)) * erd + (cz * ex - cx * ez) * dre);
+    double h2z = ((dx * (ay + by) - dy * (ax + bx)) * erd + (cx * ey - cy * ex) * dre);
+    double h3x = ((ay * dz - az * dy) * erd + (ey * (bz + cz) - ez * (by + cy)) * dre);
+    double h3y = ((az * dx - ax * dz) * erd + (ez * (bx + cx) - ex * (bz + cz)) * dre);
+    double h3z = ((ax * dy - ay * dx) * erd + (ex * (by + cy) - ey * (bx + cx)) * dre);
+    double h4x = (by * ez - bz * ey) * dre, h4y = (bz * ex - bx * ez) * dre, h4z = (bx * ey - by * ex) * dre;
+    T->g1[0] = dudcos * (f1x - cphi * h1x); T->g1[1] = dudcos * (f1y - cphi * h1y); T->g1[2] = dudcos * (f1z - cphi * h1z);
+    T->g2[0] = dudcos * (f2x - cphi * h2x); T->g2[1] = dudcos * (f2y - cphi * h2y); T->g2[2] = dudcos * (f2z - cphi * h2z);
+    T->g3[0] = dudcos * (f3x - cphi * h3x); T->g3[1] = dudcos * (f3y - cphi * h3y); T->g3[2] = dudcos * (f3z - cphi * h3z);
+    T->u4[0] = f4x - cphi * h4x; T->u4[1] = f4y - cphi * h4y; T->u4[2] = f4z - cphi * h4z;
+    T->g4[0] = dudcos * T->u4[0]; T->g4[1] = dudcos * T->u4[1]; T->g4[2] = dudcos * T->u4[2];
+    T->dudcos = dudcos;
+  }
+  return cphi;
+}
+
+/* ftors  energy/intra/md_ftors.c:117-293: fxr -= dU/dcos dcos/dr */
+void orc_ftors(orc *o)
+{
+  int nt, c, n = o->n;
+  for (nt = 0; nt < o->ntors; nt++) {
+    int at[4] = {o->itors[nt], o->jtors[nt], o->ktors[nt], o->ltors[nt]};
+    double pot;
+    tors_terms T;
+    torsion(o, nt, &pot, &T);
+    for (c = 0; c < 3; c++) o->fxr[c * n + at[0]] -= T.g1[c];
+    for (c = 0; c < 3; c++) o->fxr[c * n + at[1]] -= T.g2[c];
+    for (c = 0; c < 3; c++) o->fxr[c * n + at[2]] -= T.g3[c];
+    for (c = 0; c < 3; c++) o->fxr[c * n + at[3]] -= T.g4[c];
+  }
+}
+
+/* quadratic interpolation of a 1-4 table at squared distance dis2
+   (md_fonefour.c:124-140); *under is set (and the first knot used) below
+   the table's start */
+static double onfo_interp(orc *o, const double *tab, int t, double dis2, int *under)
+{
+  double p = (dis2 - o->r14min2[t]) * o->dx214tab[t];
+  int k = (int)p;
+  const double *v = tab + (size_t)t * o->n14table;
+  double fm1, f0, f1;
+  if (k < 1) {
+    *under = 1;
+    k = 1;
+    p = 1.;
+  }
+  p = p - (double)k;
+  fm1 = v[k - 1];
+  f0 = v[k];
+  f1 = v[k + 1];
+  return f0 + .5 * p * (f1 - fm1 + p * (fm1 - 2. * f0 + f1));
+}
+
+/* fonfo  energy/intra/md_fonefour.c:70-157: tabulated 1-4 force (scaled by
+   scale_onefour) plus the bare 1-4 Coulomb force (scaled by
+   scale_onefour_e), within r14max */
+void orc_fonfo(orc *o)
+{
+  int k14, n = o->n;
+  double *fx = o->fxr, *fy = o->fxr + n, *fz = o->fxr + 2 * n;
+  for (k14 = 0; k14 < o->n14; k14++) {
+    int i = o->i14[k14], j = o->j14[k14], t = o->i14dx[k14], under = 0;
+    double xd = o->px[i] - o->px[j], yd = o->py[i] - o->py[j], zd = o->pz[i] - o->pz[j];
+    double dis2 = xd * xd + yd * yd + zd * zd, fcc, qij;
+    if (!(dis2 < o->r14max2[t])) continue;
+    fcc = onfo_interp(o, o->dv14tab, t, dis2, &under) * o->scale14;
+    if (under) o->underflows++;
+    if ((qij = o->qch[i] * o->qch[j]) != 0) fcc -= qij * o->scale14e / (sqrt(dis2) * dis2);
+    xd *= fcc; yd *= fcc; zd *= fcc;
+    fx[i] -= xd; fy[i] -= yd; fz[i] -= zd;
+    fx[j] += xd; fy[j] += yd; fz[j] += zd;
+  }
+}
+
+/* getvtors / getvonfo / getvbondx  md_ftors.c:296-542 (PRESSURE on, as that
+   file defines it), md_fonefour.c:160-314, md_fbocross.c:100-168 */
+static void tors_energies(orc *o)
+{
+  int nt, k14, nb, r, c;
+  double st[9] = {0}, spot = 0., sprs = 0., spelec = 0., swelec = 0., sw[9] = {0}, se[9] = {0};
+  o->vtors = 0.;
+  for (nt = 0; nt < o->ntors; nt++) {
+    double pot;
+    tors_terms T;
+    torsion(o, nt, &pot, &T);
+    o->vtors += pot;
+    /* the i-j, j-k and j-l separations times the forces on i, k and l
+       (md_ftors.c:483-519) */
+    for (r = 0; r < 3; r++)
+      for (c = 0; c < 3; c++) st[3 * r + c] -= T.a[r] * T.g1[c];
+    for (r = 0; r < 3; r++)
+      for (c = 0; c < 3; c++) st[3 * r + c] += T.b[r] * T.g3[c];
+    for (r = 0; r < 3; r++)
+      for (c = 0; c < 3; c++) st[3 * r + c] += (T.b[r] + T.c[r]) * T.dudcos * T.u4[c];
+  }
+  for (c = 0; c < 9; c++) o->wtorst[c] = st[c];
+  o->wtors = st[0] + st[4] + st[8];
+  for (k14 = 0; k14 < o->n14; k14++) {
+    int i = o->i14[k14], j = o->j14[k14], t = o->i14dx[k14], under = 0;
+    double d[3] = {o->px[i] - o->px[j], o->py[i] - o->py[j], o->pz[i] - o->pz[j]};
+    double dis2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], f, qij;
+    if (!(dis2 < o->r14max2[t])) continue;
+    spot += onfo_interp(o, o->v14tab, t, dis2, &under);
+    f = onfo_interp(o, o->dv14tab, t, dis2, &under);
+    sprs -= dis2 * f;
+    for (r = 0; r < 3; r++)
+      for (c = 0; c < 3; c++) sw[3 * r + c] -= d[c] * d[r] * f;
+    if ((qij = o->qch[i] * o->qch[j]) != 0) {
+      f = qij / sqrt(dis2);
+      spelec += f;
+      swelec += f;
+      for (r = 0; r < 3; r++)
+        for (c = 0; c < 3; c++) se[3 * r + c] += f * d[c] * d[r] / dis2;
+    }
+  }
+  o->vonfo = spot * o->scale14;
+  o->wonfo = sprs * o->scale14;
+  o->vonfo_e = spelec * o->scale14e;
+  o->wonfo_e = swelec * o->scale14e;
+  for (c = 0; c < 9; c++) {
+    o->wonfot[c] = sw[c] * o->scale14;
+    o->wonfoet[c] = se[c] * o->scale14e;
+  }
+  for (c = 0; c < 9; c++) o->wbondxt[c] = 0.;
+  spot = sprs = 0.;
+  for (nb = 0; nb < o->nbondx; nb++) {
+    int i = o->ibondx[nb], j = o->jbondx[nb], k = o->kbondx[nb], t = o->idxbondx[nb];
+    double a[3] = {o->px[i] - o->px[j], o->py[i] - o->py[j], o->pz[i] - o->pz[j]};
+    double b[3] = {o->px[j] - o->px[k], o->py[j] - o->py[k], o->pz[j] - o->pz[k]};
+    double al = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]), bl = sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]);
+    double dr1 = al - o->eq1bondx[t], dr2 = bl - o->eq2bondx[t], fk = o->fkbondx[t];
+    spot += fk * dr1 * dr2;
+    sprs -= fk * (bl * dr1 + al * dr2);
+    for (r = 0; r < 3; r++)
+      for (c = 0; c < 3; c++) o->wbondxt[3 * r + c] -= fk * (dr1 * b[c] * b[r] / bl + dr2 * a[c] * a[r] / al);
+  }
+  o->vbond += spot;
+  o->wbond += sprs;
+}
+
 /* rmass  utils/md_util.new.c:219 */
 void orc_rmass(orc *o, int which)
 {
@@ -949,7 +1227,19 @@ void orc_rmass(orc *o, int which)
   }
 }
 
-/* force  energy/control/md_fcntr.c:44-134 (levels 0, 1, 2) */
+/* freeze_atom  md_fcntr.c:311-329: frozen atoms lose their velocity and
+   every force block */
+static void freeze_atoms(orc *o)
+{
+  int f, c, n = o->n;
+  for (f = 0; f < o->nfreeze; f++) {
+    int j = o->ifreeze[f];
+    o->vx[j] = o->vy[j] = o->vz[j] = 0.;
+    for (c = 0; c < 3; c++) o->fxs[c * n + j] = o->fxl[c * n + j] = o->fxa[c * n + j] = o->fxr[c * n + j] = 0.;
+  }
+}
+
+/* force  energy/control/md_fcntr.c:44-134 (levels 0-3) */
 void orc_force(orc *o, int iflg)
 {
   switch (iflg) {
@@ -975,11 +1265,19 @@ void orc_force(orc *o, int iflg)
       orc_zero_forces(o, 2);
       orc_fbond(o);
       orc_fbend(o);
+      orc_fbondx(o);
       orc_rmass(o, 2);
       break;
-    default:
+    case 3:
+      orc_zero_forces(o, 3);
+      orc_ftors(o);
+      orc_fonfo(o);
+      orc_rmass(o, 3);
       break;
+    default:
+      return;
   }
+  freeze_atoms(o);
 }
 
 /* getvbond / getvbend energies and virials  md_fbond.c:131-220,
@@ -1062,6 +1360,7 @@ void orc_get_energies(orc *o, cm3d_nb_energies *e)
     for (i = 0; i < 9; i++) e->wewaldtensor[i] = o->vp_ewald_tensor[i] + o->prs_ecorr_tensor[i];
   }
   bonded_energies(o);
+  tors_energies(o);
   e->vbond = o->vbond;
   e->wbond = o->wbond;
   e->vbend = o->vbend;
@@ -1092,8 +1391,19 @@ void orc_get_energies(orc *o, cm3d_nb_energies *e)
   p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
   {
     /* UI, WI and WItensor as getvireal sums them (md_fcntr.c:205-215) */
-    double UI = e->vbond + e->vbend, WI = e->wbond + e->wbend, wit[9];
-    for (i = 0; i < 9; i++) wit[i] = o->wbondt[i] + o->wbendt[i];
+    double UI, WI, *wit = e->WItensor;
+    e->vtors = o->vtors;
+    e->wtors = o->wtors;
+    e->vonfo = o->vonfo;
+    e->vonfo_e = o->vonfo_e;
+    e->wonfo = o->wonfo;
+    e->wonfo_e = o->wonfo_e;
+    UI = e->vbond + e->vbend + e->vtors + e->vonfo + e->vonfo_e;
+    WI = e->wbond + e->wbend + e->wtors + e->wonfo + e->wonfo_e;
+    for (i = 0; i < 9; i++)
+      wit[i] = o->wbondt[i] + o->wbendt[i] + o->wtorst[i] + o->wonfot[i] + o->wonfoet[i] + o->wbondxt[i];
+    e->UI = UI;
+    e->WI = WI;
     e->poth = e->US;
     e->poter = e->U;
     e->potra = UI;
@@ -1145,9 +1455,10 @@ void orc_step_init(orc *o)
   orc_get_ngbr(o);
   orc_force(o, 1);
   orc_force(o, 2);
+  orc_force(o, 3);
 }
 
-/* step  integrate/md_step.c:62-159 (NVE, no torsion level) */
+/* step  integrate/md_step.c:62-159 (NVE) */
 void orc_step(orc *o, int istep0, int nsteps)
 {
   int s, n3 = 3 * o->n, i;
@@ -1172,7 +1483,8 @@ void orc_step(orc *o, int istep0, int nsteps)
         }
       }
       for (inrra = 0; inrra < ninrra; inrra++) {
-        /* the torsion level contributes fxr = 0 (no torsions in the engine) */
+        for (c = 0; c < 3; c++)
+          for (i = 0; i < n; i++) V[c][i] += dtr2 * o->fxr[c * n + i];
         for (intra = 0; intra < ninnra; intra++) {
           for (c = 0; c < 3; c++)
             for (i = 0; i < n; i++) V[c][i] += dta2 * o->fxa[c * n + i];
@@ -1184,8 +1496,9 @@ void orc_step(orc *o, int istep0, int nsteps)
           for (c = 0; c < 3; c++)
             for (i = 0; i < n; i++) V[c][i] += dta2 * o->fxa[c * n + i];
         }
+        orc_force(o, 3);
         for (c = 0; c < 3; c++)
-          for (i = 0; i < n; i++) V[c][i] += dtr2 * 0.0;
+          for (i = 0; i < n; i++) V[c][i] += dtr2 * o->fxr[c * n + i];
       }
       nrefsh(o, istep);
       if (intr == ninter - 1) {

@@ -44,6 +44,9 @@ void orc_fk_ewald(orc *o);
 void orc_ecorr(orc *o);
 void orc_fbond(orc *o);
 void orc_fbend(orc *o);
+void orc_fbondx(orc *o);
+void orc_ftors(orc *o);
+void orc_fonfo(orc *o);
 void orc_rmass(orc *o, int which);
 
 /* out[0..]: see orc_get_energies in cm3d_oracle.c (same layout as

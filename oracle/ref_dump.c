@@ -72,6 +72,8 @@ static void dump_energies(const char *pfx, ENERGIES *e)
   E1(US); E1(U); E1(W); E1(UI); E1(WI);
   E9(wintertensor); E9(welectensor); E9(wewaldtensor); E9(Wtensor);
   E1(prsi); E9(prs_tensor); E1(zke); E1(tiout); E1(poth); E1(poter); E1(potra);
+  E1(vtors); E1(vonfo); E1(vonfo_e); E1(vbondx); E1(wtors); E1(wonfo); E1(wonfo_e); E1(wbondx);
+  E9(wtorstensor); E9(wonfotensor); E9(wonfo_etensor); E9(wbondxtensor); E9(WItensor);
 #undef E1
 #undef E9
 }
@@ -261,9 +263,70 @@ int main(int argc, char *argv[])
     recd("eqbend", coords.bends.itypes, coords.bends.eqbend);
     recd("fkbend", coords.bends.itypes, coords.bends.fkbend);
   }
+  /* frozen atoms (freeze_atom md_fcntr.c:311, applied at the end of every force level) */
+  rec1i("nfreeze", simparms.nfreeze);
+  if (simparms.nfreeze > 0) reci("ifreeze", simparms.nfreeze, coords.ifreeze);
   rec1i("ntors", coords.tors.ntorss);
   rec1i("n14", coords.onfo.n14s);
   rec1i("nbondx", coords.bondxs.nbondxs);
+  /* torsions (the torsion RESPA level, md_ftors.c:117): per torsion its four
+     atoms and type; per type the potential form (0 harmonic, 1 cosine power
+     series) and the index into eqtors/fktors or vphi */
+  if (coords.tors.ntorss > 0) {
+    int t, nh = 0, nv = 0;
+    reci("itors", coords.tors.ntorss, coords.tors.itors);
+    reci("jtors", coords.tors.ntorss, coords.tors.jtors);
+    reci("ktors", coords.tors.ntorss, coords.tors.ktors);
+    reci("ltors", coords.tors.ntorss, coords.tors.ltors);
+    reci("idxtors", coords.tors.ntorss, coords.tors.idxtors);
+    reci("tors_ind_pot", coords.tors.itypes, coords.tors.ind_pot);
+    reci("tors_ind_pot_num", coords.tors.itypes, coords.tors.ind_pot_num);
+    for (t = 0; t < coords.tors.itypes; t++) {
+      int k = coords.tors.ind_pot_num[t] + 1;
+      if (coords.tors.ind_pot[t] == 0 && k > nh) nh = k;
+      if (coords.tors.ind_pot[t] == 1 && k > nv) nv = k;
+    }
+    if (nh > 0) {
+      recd("eqtors", nh, coords.tors.eqtors);
+      recd("fktors", nh, coords.tors.fktors);
+    }
+    if (nv > 0) recd("vphi", (long long)nv * MAXPOWER_TORS, &coords.tors.vphi[0][0]);
+  }
+  /* 1-4 pairs (md_fonefour.c:70): tabulated potential and force per type */
+  if (coords.onfo.n14s > 0) {
+    int t;
+    reci("i14", coords.onfo.n14s, coords.onfo.i14);
+    reci("j14", coords.onfo.n14s, coords.onfo.j14);
+    reci("i14dx", coords.onfo.n14s, coords.onfo.i14dx);
+    rec1i("n14table", coords.onfo.n14table);
+    rec1i("n14types", coords.onfo.itypes);
+    recd("r14min2", coords.onfo.itypes, coords.onfo.r14min2);
+    recd("r14max2", coords.onfo.itypes, coords.onfo.r14max2);
+    recd("dx214tab", coords.onfo.itypes, coords.onfo.dx214tab);
+    rec1d("scale_onefour", coords.onfo.scale_onefour);
+    rec1d("scale_onefour_e", coords.onfo.scale_onefour_e);
+    {
+      double *v = (double *)malloc(sizeof(double) * 2 * (size_t)coords.onfo.itypes * coords.onfo.n14table);
+      double *dv = v + (size_t)coords.onfo.itypes * coords.onfo.n14table;
+      for (t = 0; t < coords.onfo.itypes; t++) {
+        memcpy(v + (size_t)t * coords.onfo.n14table, coords.onfo.v14tab[t], sizeof(double) * coords.onfo.n14table);
+        memcpy(dv + (size_t)t * coords.onfo.n14table, coords.onfo.dv14tab[t], sizeof(double) * coords.onfo.n14table);
+      }
+      recd("v14tab", (long long)coords.onfo.itypes * coords.onfo.n14table, v);
+      recd("dv14tab", (long long)coords.onfo.itypes * coords.onfo.n14table, dv);
+      free(v);
+    }
+  }
+  /* cross bonds (md_fbocross.c:40) */
+  if (coords.bondxs.nbondxs > 0) {
+    reci("ibondx", coords.bondxs.nbondxs, coords.bondxs.ibondx);
+    reci("jbondx", coords.bondxs.nbondxs, coords.bondxs.jbondx);
+    reci("kbondx", coords.bondxs.nbondxs, coords.bondxs.kbondx);
+    reci("idxbondx", coords.bondxs.nbondxs, coords.bondxs.idxbox);
+    recd("eq1bondx", coords.bondxs.itypes, coords.bondxs.eq1bondx);
+    recd("eq2bondx", coords.bondxs.itypes, coords.bondxs.eq2bondx);
+    recd("fkbondx", coords.bondxs.itypes, coords.bondxs.fkbondx);
+  }
 
   /* ---- neighbour lists after step_init (get_ngbr ngbr_list.c:297) ---- */
   rec1i("nprt", ngbr.nprt); rec1i("nprs", ngbr.nprs);
@@ -349,6 +412,23 @@ int main(int argc, char *argv[])
     zero3(coords.fxa, coords.fya, coords.fza, n);
     fbend(&simparms, &coords);
     rec_force("f_bend", n, coords.fxa, coords.fya, coords.fza, coords.amass, 0);
+    /* cross bonds (inner level) and the torsion level: fbondx md_fbocross.c:40,
+       ftors md_ftors.c:117, fonfo md_fonefour.c:70 */
+    if (coords.bondxs.nbondxs > 0) {
+      zero3(coords.fxa, coords.fya, coords.fza, n);
+      fbondx(&simparms, &coords);
+      rec_force("f_bondx", n, coords.fxa, coords.fya, coords.fza, coords.amass, 0);
+    }
+    if (coords.tors.ntorss > 0) {
+      zero3(coords.fxr, coords.fyr, coords.fzr, n);
+      ftors(&simparms, &coords);
+      rec_force("f_tors", n, coords.fxr, coords.fyr, coords.fzr, coords.amass, 0);
+    }
+    if (coords.onfo.n14s > 0) {
+      zero3(coords.fxr, coords.fyr, coords.fzr, n);
+      fonfo(&simparms, &coords);
+      rec_force("f_onfo", n, coords.fxr, coords.fyr, coords.fzr, coords.amass, 0);
+    }
   }
   /* restore the state step_init left behind (forces are re-made by step()) */
   force(&simparms, &coords, &inter, &ngbr, 2);

@@ -103,7 +103,7 @@ def main() -> None:
         run_case("lj2", d, "lj.input_ljnve.2", 10, True, True)
         d = os.path.join(tmp, "abutane")
         copy_ref_test("abutane", d)
-        run_case("abutane", d, "abutane.input", 0, True, True)
+        run_case("abutane", d, "abutane.input", 20, True, True)
         # synthetic workloads in CM3D's formats
         cases = [
             ("argon864", configs.argon_fcc(ntime=20), 20, True, True),

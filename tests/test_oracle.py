@@ -61,11 +61,20 @@ def test_force_terms_bit_exact(name):
         o.zero_forces(2)
         fn()
         assert np.array_equal(o.forces(2), xyz(d, key)), key
+    # cross bonds (level 2), torsions and 1-4 pairs (level 3)
+    for key, fn, blk in (("f_bondx", o.fbondx, 2), ("f_tors", o.ftors, 3), ("f_onfo", o.fonfo, 3)):
+        if key in d:
+            o.zero_forces(blk)
+            fn()
+            assert np.array_equal(o.forces(blk), xyz(d, key)), key
 
 
-@pytest.mark.parametrize("name", [c for c in CASES if c != "abutane"])
+
+TORS_KEYS = ("vtors", "wtors", "vonfo", "vonfo_e", "wonfo", "wonfo_e", "UI", "WI")
+
+
+@pytest.mark.parametrize("name", CASES)
 def test_level1_forces_and_energies_exact(name):
-    # abutane freezes two atoms (~mol_freeze), which is outside this path
     d, o = make(name)
     o.get_ngbr()
     o.force(1)
@@ -77,12 +86,17 @@ def test_level1_forces_and_energies_exact(name):
         assert np.array_equal(np.array(e[k]), d[f"e0_{k}"]), k
     o.force(2)
     e = o.energies()
-    for k in ("prsi", "zke", "tiout", "poter", "potra", "wbend"):
+    for k in ("prsi", "zke", "tiout", "poter", "potra", "wbend", "vbond", "wbond") + TORS_KEYS:
         assert e[k] == float(d[f"e0_{k}"][0]), k
     assert np.array_equal(np.array(e["prs_tensor"]), d["e0_prs_tensor"])
+    assert np.array_equal(np.array(e["WItensor"]), d["e0_WItensor"])
+    # the torsion level (torsions + 1-4 pairs), with abutane's frozen atoms
+    if "acc_r" in d:                   # not stored for the large fixtures
+        o.force(3)
+        assert np.array_equal(o.forces(3), xyz(d, "acc_r"))
 
 
-@pytest.mark.parametrize("name", ["lj2", "lj256", "argon864", "water216", "binary256", "water4096"])
+@pytest.mark.parametrize("name", ["lj2", "lj256", "abutane", "argon864", "water216", "binary256", "water4096"])
 def test_trajectory_bit_exact(name):
     """CM3D's step() (RESPA, nrefsh with RESETPOS) for the dumped number of
     steps: per-step energies and final state identical"""
@@ -100,7 +114,7 @@ def test_trajectory_bit_exact(name):
     # getvireal(..., 1) + geteng after the last step, the pressure tensor with
     # the bend virial of md_fbend.c (always compiled with PRESSURE) included
     e = o.energies()
-    for k in ("vbond", "vbend", "wbond", "wbend", "W", "U", "US", "prsi", "zke", "poter", "potra"):
+    for k in ("vbond", "vbend", "wbond", "wbend", "W", "U", "US", "prsi", "zke", "poter", "potra") + TORS_KEYS:
         assert e[k] == float(d[f"ef_{k}"][0]), k
     for k in ("wintertensor", "welectensor", "wewaldtensor", "Wtensor", "prs_tensor"):
         assert np.array_equal(np.array(e[k]), d[f"ef_{k}"]), k
