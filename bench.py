@@ -201,7 +201,7 @@ def e2e_run(eng, steps: int, istep0: int, n: int) -> tuple[float, int, int]:
         eng.energies_table(out=etab)
     dt = time.perf_counter() - t0
     h2d = 2 * 3 * n * 8
-    d2h = 2 * 3 * n * 8 + 104 * 8 * eng.nsys     # + every system's accumulator block (ACC_STRIDE doubles)
+    d2h = 2 * 3 * n * 8 + 144 * 8 * eng.nsys     # + every system's accumulator block (ACC_STRIDE doubles)
     return dt, h2d, d2h
 
 

@@ -86,7 +86,8 @@ static void destroy(Ctx *c) {
                   c->lst[1], c->lst[2], c->lst[3], c->nbr, c->xq, c->epart, c->styp, c->shift, c->corner,
                   c->cimg, c->nlen, c->acc,
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
-                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan};
+                  c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan,
+                  c->fxr, c->intra_buf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -210,6 +211,8 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
     H.ninter = s->ninter;
     H.vlrc = s->vlrc;
     H.wlrc = s->wlrc;
+    H.scale14 = s->n14 > 0 ? s->scale_onefour : 1.0;
+    H.scale14e = s->n14 > 0 ? s->scale_onefour_e : 1.0;
     H.iperd = s->iperd;
     memcpy(H.hmat, s->hmat, sizeof H.hmat);
     {
@@ -373,6 +376,7 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
   if ((rc = upload<double>(&c->fxl, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->fxs, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->fxa, nullptr, n3))) return rc;
+  if ((rc = upload<double>(&c->fxr, nullptr, n3))) return rc;
   if ((rc = upload<double>(&c->dxn, pos.data(), n3))) return rc;
   if ((rc = upload(&c->mass, mass.data(), n))) return rc;
   if ((rc = upload(&c->q, q.data(), n))) return rc;
@@ -414,10 +418,6 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
   if ((rc = kspace_setup(c))) return rc;
   if ((rc = step_setup(c, systems, nsys))) return rc;
   if ((rc = upload(&c->sp, c->h_sp.data(), c->h_sp.size()))) return rc;
-  for (int sy = 0; sy < nsys; sy++) {
-    const cm3d_nb_system *s = systems + sy;
-    if (s->ntors > 0 || s->n14 > 0 || s->nbondx > 0) c->name = "has-torsions";
-  }
   CK(cudaDeviceSynchronize());
   return CM3D_NB_OK;
 }
@@ -476,7 +476,11 @@ __global__ void k_scale_rmass(int n, double *__restrict__ f, const double *__res
 }
 
 static double *block_of(Ctx *c, int which) {
-  return which == CM3D_NB_FXL ? c->fxl : which == CM3D_NB_FXS ? c->fxs : which == CM3D_NB_FXA ? c->fxa : nullptr;
+  return which == CM3D_NB_FXL   ? c->fxl
+         : which == CM3D_NB_FXS ? c->fxs
+         : which == CM3D_NB_FXA ? c->fxa
+         : which == CM3D_NB_FXR ? c->fxr
+                                : nullptr;
 }
 
 static int pull_acc(Ctx *c) {
@@ -789,35 +793,24 @@ int cm3d_nb_getvewald(cm3d_nb_ctx *ctx, double *pot_ewald, double *prs_ewald, do
 int cm3d_nb_step_init(cm3d_nb_ctx *ctx) {
   CTX;
   int rc;
-  if (c->name == "has-torsions") {
-    set_error("step_init(): torsions, 1-4 terms and cross bonds are not part of the engine");
-    return CM3D_NB_ERR_ARG;
-  }
   c->h_istate[IS_ISTEP] = 0;
   c->h_istate[IS_ISTEPLAST] = 0;
   CK(cudaMemcpyAsync(c->istate, c->h_istate, sizeof(int) * 2, cudaMemcpyHostToDevice, c->st));
   if ((rc = build_lists(c, false, true))) return rc;
   if ((rc = run_force(c, 1))) return rc;
   if ((rc = run_force(c, 2))) return rc;
+  if ((rc = run_force(c, 3))) return rc;
   c->forces_valid = true;
   return CM3D_NB_OK;
 }
 
 int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
   CTX;
-  if (c->name == "has-torsions") {
-    set_error("step(): torsions, 1-4 terms and cross bonds are not part of the engine");
-    return CM3D_NB_ERR_ARG;
-  }
   return run_step(c, istep0, nsteps);
 }
 
 int cm3d_nb_step_async(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
   CTX;
-  if (c->name == "has-torsions") {
-    set_error("step(): torsions, 1-4 terms and cross bonds are not part of the engine");
-    return CM3D_NB_ERR_ARG;
-  }
   return launch_steps(c, istep0, nsteps);
 }
 
@@ -865,13 +858,25 @@ static void energies_of(Ctx *c, int sy, cm3d_nb_energies *e) {
   e->Wtensor[8] -= H.wlrc * rvol;
   sym9(a, ACC_P2MT, e->p2m_tensor);
   double p2m = e->p2m_tensor[0] + e->p2m_tensor[4] + e->p2m_tensor[8];
-  double UI = e->vbond + e->vbend, WI = e->wbond + e->wbend;
+  // torsions (virial = the tensor's trace, md_ftors.c:532), 1-4 pairs scaled
+  // as getvonfo scales its sums (md_fonefour.c:303-312); the 1-4 Coulomb
+  // virial equals its energy term by term
+  e->vtors = a[ACC_VTORS];
+  e->wtors = a[ACC_WTORST + 0] + a[ACC_WTORST + 4] + a[ACC_WTORST + 8];
+  e->vonfo = a[ACC_VONFO] * H.scale14;
+  e->wonfo = a[ACC_WONFO] * H.scale14;
+  e->vonfo_e = a[ACC_VONFO_E] * H.scale14e;
+  e->wonfo_e = a[ACC_VONFO_E] * H.scale14e;
+  e->UI = e->vbond + e->vbend + e->vtors + e->vonfo + e->vonfo_e;
+  e->WI = e->wbond + e->wbend + e->wtors + e->wonfo + e->wonfo_e;
+  for (int k = 0; k < 9; k++)
+    e->WItensor[k] = a[ACC_WBONDT + k] + a[ACC_WBENDT + k] + a[ACC_WTORST + k] + a[ACC_WONFOT + k] * H.scale14 +
+                     a[ACC_WONFOET + k] * H.scale14e + a[ACC_WBONDXT + k];
   e->poth = e->US + H.vlrc / vol;
   e->poter = e->U + H.vlrc / vol;
-  e->potra = UI;
-  e->prsi = (p2m + e->W + WI) / (3 * vol);
-  for (int k = 0; k < 9; k++)
-    e->prs_tensor[k] = (e->p2m_tensor[k] + e->Wtensor[k] + (a[ACC_WBONDT + k] + a[ACC_WBENDT + k])) / vol;
+  e->potra = e->UI;
+  e->prsi = (p2m + e->W + e->WI) / (3 * vol);
+  for (int k = 0; k < 9; k++) e->prs_tensor[k] = (e->p2m_tensor[k] + e->Wtensor[k] + e->WItensor[k]) / vol;
   e->zke = .5 * p2m;
   e->tiout = p2m / (double)H.ndof;
 }

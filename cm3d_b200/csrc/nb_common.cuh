@@ -42,10 +42,18 @@ enum {
   ACC_P2MT = 58,          // 9: get_p2mt kinetic tensor
   ACC_WBEND = 67,         // getvbend virial (md_fbend.c compiles it with PRESSURE)
   ACC_WBENDT = 68,        // 9
-  ACC_COUNT = 77,
+  ACC_VTORS = 77,         // getvtors energy (its virial is the tensor's trace)
+  ACC_WTORST = 78,        // 9: torsion virial tensor (md_ftors.c PRESSURE)
+  ACC_VONFO = 87,         // getvonfo: tabulated 1-4 energy (unscaled)
+  ACC_VONFO_E = 88,       //           1-4 Coulomb energy (unscaled)
+  ACC_WONFO = 89,         //           tabulated 1-4 virial (unscaled)
+  ACC_WONFOT = 90,        // 9
+  ACC_WONFOET = 99,       // 9: 1-4 Coulomb virial tensor (unscaled)
+  ACC_WBONDXT = 108,      // 9: getvbondx tensor (its energy and virial go to ACC_VBOND/WBOND)
+  ACC_COUNT = 117,
   // each system owns ACC_STRIDE doubles of acc[]: its accumulators, then
   // device copies of its H^-1 (ACC_COUNT..+9) and H (+9..+18)
-  ACC_STRIDE = 104
+  ACC_STRIDE = 144
 };
 
 // Per-system parameters of a context that holds several independent systems
@@ -167,10 +175,34 @@ struct SysH {
   int n = 0, ncharge = 0, ndof = 1, ntypes = 0, ninter = 0, ktot = 0, iperd = 3;
   double hmat[9], hmati[9];
   double vlrc = 0, wlrc = 0, ewald_self = 0, ewald_bkg = 0;
+  double scale14 = 1, scale14e = 1;   // ONFO.scale_onefour / scale_onefour_e
   double rlist = 0;          // largest list radius (LJ or charges, with skin)
   std::vector<int4> krows;   // k rows {ka, kb, kc0, len} of the system's k set
   std::vector<int> krow_k0;  // first k of each row (system-local)
   std::vector<int> ka, kb, kc;
+};
+
+// Intramolecular terms beyond bonds and bends, in groups (CM3D's order
+// inside a group): cross bonds join level 2 (fbondx md_fbocross.c:40),
+// torsions and 1-4 pairs make the torsion level (ftors md_ftors.c:117, fonfo
+// md_fonefour.c:70).  1-4 types are numbered across the systems of a batch,
+// each with its own table of o14_ntab[t] knots from o14_tab0[t].
+struct IntraDev {
+  const int *bx_off = nullptr;          // ngroups + 1
+  const int4 *bx_ijk = nullptr;         // {i, j, k, -}
+  const double4 *bx_par = nullptr;      // {eq1, eq2, fk, -}
+  const int *tor_off = nullptr;         // ngroups + 1
+  const int4 *tor_ijkl = nullptr;
+  const int2 *tor_par = nullptr;        // {form (0 harmonic, 1 cosine series), row}
+  const double2 *tor_h = nullptr;       // harmonic rows {eq, fk}
+  const double *tor_v = nullptr;        // series rows of CM3D_NB_MAXPOWER_TORS coefficients
+  const int *o14_off = nullptr;         // ngroups + 1
+  const int4 *o14_ij = nullptr;         // {i, j, type, -}
+  const double4 *o14_rng = nullptr;     // per type {rmin2, rmax2, dx2tab, scale}
+  const double *o14_se = nullptr;       // per type scale_onefour_e
+  const int2 *o14_tab = nullptr;        // per type {first knot, knots}
+  const double *o14_v = nullptr, *o14_dv = nullptr;
+  const unsigned char *frz = nullptr;   // per atom: frozen (nullptr: none)
 };
 
 struct Ctx {
@@ -224,6 +256,7 @@ struct Ctx {
   double tablast_e = 0;        // coultab[ntable-4] (finter_e.c:67)
   // ---- per-atom device arrays (original order)
   double *pos = nullptr, *vel = nullptr, *fxl = nullptr, *fxs = nullptr, *fxa = nullptr;
+  double *fxr = nullptr;                // torsion level (torsions + 1-4 pairs)
   double *mass = nullptr, *q = nullptr, *dxn = nullptr, *snap = nullptr;
   int *itype = nullptr;
   // ---- parameters on device
@@ -264,6 +297,10 @@ struct Ctx {
   int4 *bend_ijk = nullptr;
   double2 *bend_p = nullptr;
   int2 *ecorr_ij = nullptr;             // grouped order
+  IntraDev intra;                       // cross bonds, torsions, 1-4 pairs, frozen atoms
+  bool has_tors_level = false;          // any torsion or 1-4 pair
+  bool has_intra_x = false;             // any cross bond, torsion or 1-4 pair
+  double *intra_buf = nullptr;          // one allocation behind the IntraDev arrays
   // ---- cell grid and lists
   int nc[3] = {1, 1, 1}, ncells = 1;
   int *cell_of = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *cell_atoms = nullptr;

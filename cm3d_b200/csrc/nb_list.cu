@@ -516,7 +516,7 @@ __device__ __forceinline__ void full_list_atom(
     const double *__restrict__ q, const int *__restrict__ excl_off, const int *__restrict__ excl_idx,
     const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
     uint32_t *__restrict__ nbr, int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt,
-    int *qbuf, float *qr, const float4 *s_x, const int *s_u, const int *s_j, const int *s_meta, int scnt,
+    int *qbuf, float *qr, const float4 *s_x, const int *s_u, const int *s_j, int scnt,
     bool fast) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -539,7 +539,7 @@ __device__ __forceinline__ void full_list_atom(
         const int j = s_j[k];
         bool exact = !fast;
         if (fast) {
-          const int meta = s_meta[k];
+          const int meta = __float_as_int(s_x[k].w);
           fl = fast_flags(P, i, j, ti, meta >> 1, qi, (meta & 1) != 0, qr[slot], map, icut, excl_off, excl_idx,
                           cexcl_off, cexcl_idx, &exact);
           code = (int)((unsigned)uc >> ENT_CODE_SHIFT);
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(256) k_list_full(
   if (sys_skip(s, sreb, all)) return;                     // whole warps
   full_list_atom<false>(sp[s], n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                         excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[threadIdx.x >> 5],
-                        nullptr, nullptr, nullptr, nullptr, nullptr, 0, false);
+                        nullptr, nullptr, nullptr, nullptr, 0, false);
 }
 
 // The cells of the systems being rebuilt, as one index range: rb_scan[s] is
@@ -675,8 +675,8 @@ __global__ void k_rebuild_cells(int nsys, const SysP *__restrict__ sp, const int
 // neighbourhood holds more than `cap` atoms is walked in global memory
 // instead (same decisions).
 constexpr int LW_THREADS = 256;
-constexpr size_t LW_BYTES_PER_ATOM = sizeof(float4) + 3 * sizeof(int);   // s_x, s_u, s_j, s_meta
-constexpr long long LW_MAX_CAP = 2048;     // largest staged neighbourhood (57 KB)
+constexpr size_t LW_BYTES_PER_ATOM = sizeof(float4) + 2 * sizeof(int);   // s_x (w: type, charge), s_u, s_j
+constexpr long long LW_MAX_CAP = 2048;     // largest staged neighbourhood (48 KB)
 
 __global__ void __launch_bounds__(LW_THREADS) k_list_win(
     int nsys, const int *__restrict__ rb_scan, const SysP *__restrict__ sp, int n, int stride, int cap,
@@ -690,7 +690,6 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
   extern __shared__ float4 s_x[];                        // cap
   int *s_u = reinterpret_cast<int *>(s_x + cap);         // cap: sorted index | shift code << ENT_CODE_SHIFT
   int *s_j = s_u + cap;                                  // cap: atom index
-  int *s_meta = s_j + cap;                               // cap: type * 2 + charged
   __shared__ int qs[LW_THREADS / 32][LQ];
   __shared__ float qrs[LW_THREADS / 32][LQ];
   __shared__ int s_cs[27], s_off[27], s_code[27], s_tot, s_nw;
@@ -762,10 +761,9 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
         const float4 x = xq[u];
         const int j = cell_atoms[u];
         const float4 sh = s_sh[wa];
-        s_x[g] = make_float4(x.x - sh.x, x.y - sh.y, x.z - sh.z, 0.f);
+        s_x[g] = make_float4(x.x - sh.x, x.y - sh.y, x.z - sh.z, __int_as_float(itype[j] * 2 + (q[j] != 0.0 ? 1 : 0)));
         s_u[g] = u | (s_code[wa] << ENT_CODE_SHIFT);
         s_j[g] = j;
-        s_meta[g] = itype[j] * 2 + (q[j] != 0.0 ? 1 : 0);
       }
     }
     __syncthreads();
@@ -775,11 +773,11 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
       if (staged)
         full_list_atom<true>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                              excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], qrs[warp], s_x,
-                             s_u, s_j, s_meta, tot, fast);
+                             s_u, s_j, tot, fast);
       else
         full_list_atom<false>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                               excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], nullptr,
-                              nullptr, nullptr, nullptr, nullptr, 0, false);
+                              nullptr, nullptr, nullptr, 0, false);
     }
   }
 }

@@ -7,9 +7,16 @@
 // harmonic fbond/fbend of the inner level (energy/intra/md_fbond.c:76-125,
 // md_fbend.c:126-260).
 //
-// Bonds, bends and excluded-pair corrections only couple atoms of one
-// molecule, so the atoms are partitioned into groups (connected components
-// of those terms) and one thread owns a group: the whole inner loop -- every
+// The intramolecular terms beyond them -- cross bonds in the inner level
+// (fbondx, energy/intra/md_fbocross.c:40-97), torsions and 1-4 pairs in the
+// torsion level (ftors md_ftors.c:117-293, fonfo md_fonefour.c:70-157) -- and
+// the frozen atoms of freeze_atom (energy/control/md_fcntr.c:311-329) follow
+// the same scheme.
+//
+// Bonds, bends, cross bonds, torsions, 1-4 pairs and excluded-pair
+// corrections only couple atoms of one molecule, so the atoms are
+// partitioned into groups (connected components of those terms) and one
+// thread owns a group: the whole inner loop -- every
 // ninnra substep with its bonded forces -- runs in one kernel with no grid
 // synchronisation, followed by the displacement test of nrefsh.  The
 // excluded-pair correction (ecorr) and the bonded energies of getvireal are
@@ -75,11 +82,191 @@ __device__ __forceinline__ void group_bonded(int g, int n, const double *__restr
   }
 }
 
-// force(2) alone: bonds + bends of every group into fxa, then rmass
+// cross bonds of group g into fxa: fk (|ri - rj| - eq1)(|rj - rk| - eq2)
+__device__ __forceinline__ void group_bondx(int g, int n, const double *__restrict__ pos, double *__restrict__ fxa,
+                                            const IntraDev &X) {
+  for (int b = X.bx_off[g]; b < X.bx_off[g + 1]; b++) {
+    const int4 t = X.bx_ijk[b];
+    const double4 p = X.bx_par[b];
+    const int i = t.x, j = t.y, k = t.z;
+    const double ax = pos[i] - pos[j], ay = pos[n + i] - pos[n + j], az = pos[2 * n + i] - pos[2 * n + j];
+    const double al = sqrt(ax * ax + ay * ay + az * az);
+    const double bx = pos[j] - pos[k], by = pos[n + j] - pos[n + k], bz = pos[2 * n + j] - pos[2 * n + k];
+    const double bl = sqrt(bx * bx + by * by + bz * bz);
+    const double dr1 = al - p.x, dr2 = bl - p.y;
+    const double fr1 = p.z * dr2 / al, fr2 = p.z * dr1 / bl;
+    fxa[i] += -fr1 * ax; fxa[n + i] += -fr1 * ay; fxa[2 * n + i] += -fr1 * az;
+    fxa[j] += fr1 * ax - fr2 * bx; fxa[n + j] += fr1 * ay - fr2 * by; fxa[2 * n + j] += fr1 * az - fr2 * bz;
+    fxa[k] += fr2 * bx; fxa[n + k] += fr2 * by; fxa[2 * n + k] += fr2 * bz;
+  }
+}
+
+// One torsion i-j-k-l.  With a = ri - rj, b = rj - rk, c = rk - rl and the
+// plane normals d = a x b, e = b x c: cos(phi) = d.e / (|d| |e|).  For atom m,
+// dcos/dr_m = (dF_m - cos dG_m) / G with F = d.e and G = |d| |e|; g[m] holds
+// dU/dcos times that, the negative of the force.  u4 and dudcos (dU/dcos / G)
+// are kept for the virial's j-l term.
+struct TorsTerm {
+  double a[3], b[3], c[3], g[4][3], u4[3], dudcos, pot;
+};
+
+__device__ __forceinline__ void torsion_term(int n, const double *__restrict__ pos, int4 at, int2 par,
+                                             const IntraDev &X, TorsTerm &T) {
+  const int i = at.x, j = at.y, k = at.z, l = at.w;
+  const double ax = pos[i] - pos[j], ay = pos[n + i] - pos[n + j], az = pos[2 * n + i] - pos[2 * n + j];
+  const double bx = pos[j] - pos[k], by = pos[n + j] - pos[n + k], bz = pos[2 * n + j] - pos[2 * n + k];
+  const double cx = pos[k] - pos[l], cy = pos[n + k] - pos[n + l], cz = pos[2 * n + k] - pos[2 * n + l];
+  const double dx = ay * bz - az * by, dy = az * bx - ax * bz, dz = ax * by - ay * bx;
+  const double dl = sqrt(dx * dx + dy * dy + dz * dz);
+  const double ex = by * cz - bz * cy, ey = bz * cx - bx * cz, ez = bx * cy - by * cx;
+  const double el = sqrt(ex * ex + ey * ey + ez * ez);
+  const double cphi = (dx * ex + dy * ey + dz * ez) / (dl * el);
+  double dudcos;
+  if (par.x == 0) {
+    // harmonic in phi; dU/dphi dphi/dcos, zero at |cos| = 1
+    const double2 h = X.tor_h[par.y];
+    double phi = 0., dphi;
+    if (cphi >= 1.0 || cphi <= -1.0) {
+      dphi = phi - h.x;
+      dudcos = 0.;
+    } else {
+      phi = acos(cphi);
+      dphi = phi - h.x;
+      dudcos = (h.y * dphi) * (-1. / sqrt(1. - cphi * cphi));
+    }
+    T.pot = .5 * h.y * dphi * dphi;
+  } else {
+    // power series sum_m v_m cos^m (Horner's scheme for U and dU/dcos)
+    const double *v = X.tor_v + (size_t)par.y * CM3D_NB_MAXPOWER_TORS;
+    double tpot = v[CM3D_NB_MAXPOWER_TORS - 1];
+    dudcos = ((double)CM3D_NB_MAXPOWER_TORS - 1.) * v[CM3D_NB_MAXPOWER_TORS - 1];
+    for (int m = CM3D_NB_MAXPOWER_TORS - 2; m > 0; m--) dudcos = dudcos * cphi + v[m] * (double)m;
+    for (int m = CM3D_NB_MAXPOWER_TORS - 2; m >= 0; m--) tpot = tpot * cphi + v[m];
+    T.pot = tpot;
+  }
+  const double G = dl * el, dre = dl / el, erd = el / dl;
+  dudcos *= 1. / G;
+  T.dudcos = dudcos;
+  T.a[0] = ax; T.a[1] = ay; T.a[2] = az;
+  T.b[0] = bx; T.b[1] = by; T.b[2] = bz;
+  T.c[0] = cx; T.c[1] = cy; T.c[2] = cz;
+  // dF_m and dG_m of the four atoms (F and G differentiated by hand)
+  const double f1x = by * ez - bz * ey, f1y = bz * ex - bx * ez, f1z = bx * ey - by * ex;
+  const double f2x = (cy * dz - cz * dy + (az + bz) * ey - (ay + by) * ez);
+  const double f2y = (cz * dx - cx * dz + (ax + bx) * ez - (az + bz) * ex);
+  const double f2z = (cx * dy - cy * dx + (ay + by) * ex - (ax + bx) * ey);
+  const double f3x = (ay * ez - az * ey + (bz + cz) * dy - (by + cy) * dz);
+  const double f3y = (az * ex - ax * ez + (bx + cx) * dz - (bz + cz) * dx);
+  const double f3z = (ax * ey - ay * ex + (by + cy) * dx - (bx + cx) * dy);
+  const double f4x = by * dz - bz * dy, f4y = bz * dx - bx * dz, f4z = bx * dy - by * dx;
+  const double h1x = (by * dz - bz * dy) * erd, h1y = (bz * dx - bx * dz) * erd, h1z = (bx * dy - by * dx) * erd;
+  const double h2x = ((dy * (az + bz) - dz * (ay + by)) * erd + (cy * ez - cz * ey) * dre);
+  const double h2y = ((dz * (ax + bx) - dx * (az + bz)) * erd + (cz * ex - cx * ez) * dre);
+  const double h2z = ((dx * (ay + by) - dy * (ax + bx)) * erd + (cx * ey - cy * ex) * dre);
+  const double h3x = ((ay * dz - az * dy) * erd + (ey * (bz + cz) - ez * (by + cy)) * dre);
+  const double h3y = ((az * dx - ax * dz) * erd + (ez * (bx + cx) - ex * (bz + cz)) * dre);
+  const double h3z = ((ax * dy - ay * dx) * erd + (ex * (by + cy) - ey * (bx + cx)) * dre);
+  const double h4x = (by * ez - bz * ey) * dre, h4y = (bz * ex - bx * ez) * dre, h4z = (bx * ey - by * ex) * dre;
+  T.g[0][0] = dudcos * (f1x - cphi * h1x); T.g[0][1] = dudcos * (f1y - cphi * h1y); T.g[0][2] = dudcos * (f1z - cphi * h1z);
+  T.g[1][0] = dudcos * (f2x - cphi * h2x); T.g[1][1] = dudcos * (f2y - cphi * h2y); T.g[1][2] = dudcos * (f2z - cphi * h2z);
+  T.g[2][0] = dudcos * (f3x - cphi * h3x); T.g[2][1] = dudcos * (f3y - cphi * h3y); T.g[2][2] = dudcos * (f3z - cphi * h3z);
+  T.u4[0] = f4x - cphi * h4x; T.u4[1] = f4y - cphi * h4y; T.u4[2] = f4z - cphi * h4z;
+  T.g[3][0] = dudcos * T.u4[0]; T.g[3][1] = dudcos * T.u4[1]; T.g[3][2] = dudcos * T.u4[2];
+}
+
+// quadratic interpolation of a 1-4 table at squared distance dis2; below the
+// table's start the first knot is used and *under set (md_fonefour.c:125-128)
+__device__ __forceinline__ double o14_interp(const double *__restrict__ tab, int2 tb, double4 rng, double dis2,
+                                             bool *under) {
+  double p = (dis2 - rng.x) * rng.z;
+  int k = (int)p;
+  if (k < 1) {
+    *under = true;
+    k = 1;
+    p = 1.;
+  }
+  // CM3D's tables end three knots past rmax14 (dx2tab = (ntab - 3)/(rmax^2 -
+  // rmin^2)), so k + 1 < ntab for every dis2 < rmax14^2; the clamp only
+  // keeps other input in bounds
+  k = k < tb.y - 2 ? k : tb.y - 2;
+  p = p - (double)k;
+  const double *v = tab + tb.x;
+  const double fm1 = v[k - 1], f0 = v[k], f1 = v[k + 1];
+  return f0 + .5 * p * (f1 - fm1 + p * (fm1 - 2. * f0 + f1));
+}
+
+// the torsion level of group g into fxr (raw forces): its torsions, then its
+// 1-4 pairs (tabulated force times scale_onefour, bare Coulomb times
+// scale_onefour_e, within rmax14)
+__device__ __forceinline__ void group_tors_level(int g, int n, const double *__restrict__ pos,
+                                                 const double *__restrict__ q, double *__restrict__ fxr,
+                                                 const IntraDev &X, long long *__restrict__ stat) {
+  if (!X.tor_off) return;
+  for (int t = X.tor_off[g]; t < X.tor_off[g + 1]; t++) {
+    const int4 at = X.tor_ijkl[t];
+    TorsTerm T;
+    torsion_term(n, pos, at, X.tor_par[t], X, T);
+    const int ids[4] = {at.x, at.y, at.z, at.w};
+#pragma unroll
+    for (int m = 0; m < 4; m++) {
+      fxr[ids[m]] -= T.g[m][0];
+      fxr[n + ids[m]] -= T.g[m][1];
+      fxr[2 * n + ids[m]] -= T.g[m][2];
+    }
+  }
+  bool under = false;
+  for (int o = X.o14_off[g]; o < X.o14_off[g + 1]; o++) {
+    const int4 pr = X.o14_ij[o];
+    const int i = pr.x, j = pr.y;
+    double xd = pos[i] - pos[j], yd = pos[n + i] - pos[n + j], zd = pos[2 * n + i] - pos[2 * n + j];
+    const double dis2 = xd * xd + yd * yd + zd * zd;
+    const double4 rng = X.o14_rng[pr.z];
+    if (!(dis2 < rng.y)) continue;
+    double fcc = o14_interp(X.o14_dv, X.o14_tab[pr.z], rng, dis2, &under) * rng.w;
+    const double qij = q[i] * q[j];
+    if (qij != 0) fcc -= qij * X.o14_se[pr.z] / (sqrt(dis2) * dis2);
+    xd *= fcc; yd *= fcc; zd *= fcc;
+    fxr[i] -= xd; fxr[n + i] -= yd; fxr[2 * n + i] -= zd;
+    fxr[j] += xd; fxr[n + j] += yd; fxr[2 * n + j] += zd;
+  }
+  if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), 1ull);
+}
+
+// freeze_atom for one atom after a force level: no velocity, and the level's
+// force block zeroed (the other blocks already are: every level zeroes them)
+__device__ __forceinline__ void freeze_one(int i, int n, double *__restrict__ vel, double *__restrict__ f) {
+  vel[i] = vel[n + i] = vel[2 * n + i] = 0.;
+  f[i] = f[n + i] = f[2 * n + i] = 0.;
+}
+
+// force(3) alone: torsions + 1-4 pairs of every group into fxr, rmass, freeze
+__global__ void k_tors_level(StepP P, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
+                             const double *__restrict__ pos, const double *__restrict__ q,
+                             const double *__restrict__ mass, double *__restrict__ vel, double *__restrict__ fxr,
+                             IntraDev X, long long *__restrict__ stat) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.ngroups) return;
+  const int n = P.n;
+  for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
+    int i = gatoms[a];
+    fxr[i] = fxr[n + i] = fxr[2 * n + i] = 0.;
+  }
+  group_tors_level(g, n, pos, q, fxr, X, stat);
+  for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
+    int i = gatoms[a];
+    double r = 1. / mass[i];
+    fxr[i] *= r; fxr[n + i] *= r; fxr[2 * n + i] *= r;
+    if (X.frz && X.frz[i]) freeze_one(i, n, vel, fxr);
+  }
+}
+
+// force(2) alone: bonds + bends + cross bonds of every group into fxa, then
+// rmass and freeze
 __global__ void k_bonded(StepP P, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
-                         const double *__restrict__ pos, const double *__restrict__ mass, double *__restrict__ fxa,
-                         const int *__restrict__ gboff, const int4 *__restrict__ bij, const double2 *__restrict__ bp,
-                         const int *__restrict__ geoff, const int4 *__restrict__ eijk, const double2 *__restrict__ ep) {
+                         const double *__restrict__ pos, const double *__restrict__ mass, double *__restrict__ vel,
+                         double *__restrict__ fxa, const int *__restrict__ gboff, const int4 *__restrict__ bij,
+                         const double2 *__restrict__ bp, const int *__restrict__ geoff,
+                         const int4 *__restrict__ eijk, const double2 *__restrict__ ep, IntraDev X) {
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= P.ngroups) return;
   const int n = P.n;
@@ -88,16 +275,19 @@ __global__ void k_bonded(StepP P, const int *__restrict__ gaoff, const int *__re
     fxa[i] = fxa[n + i] = fxa[2 * n + i] = 0.;
   }
   group_bonded(g, n, pos, fxa, gboff, bij, bp, geoff, eijk, ep);
+  if (X.bx_off) group_bondx(g, n, pos, fxa, X);
   for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
     int i = gatoms[a];
     double r = 1. / mass[i];
     fxa[i] *= r; fxa[n + i] *= r; fxa[2 * n + i] *= r;
+    if (X.frz && X.frz[i]) freeze_one(i, n, vel, fxa);
   }
 }
 
 // One pass of md_step.c:95-136 for level `intr`: the kick with the
 // nonbonded accelerations, the ninrra x ninnra inner loop with force(2) on
 // this group, then nrefsh's displacement test.
+template <bool INTRA>
 __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
                         double *__restrict__ pos, double *__restrict__ vel, const double *__restrict__ mass,
                         const double *__restrict__ fxl, const double *__restrict__ fxs, double *__restrict__ fxa,
@@ -106,7 +296,8 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
                         const int *__restrict__ geoff, const int4 *__restrict__ eijk,
                         const double2 *__restrict__ ep, const SysP *__restrict__ sp,
                         const int *__restrict__ sys_of, int *__restrict__ sreb, int *__restrict__ istate,
-                        const int *__restrict__ gs) {
+                        const int *__restrict__ gs, IntraDev X, const double *__restrict__ q,
+                        double *__restrict__ fxr, long long *__restrict__ stat) {
   if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g == 0) istate[IS_INTR] = intr;
@@ -122,9 +313,18 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
       else vel[x] += P.dts2 * fxs[x];
     }
   }
-  const bool bonded = gboff[g + 1] > gboff[g] || geoff[g + 1] > geoff[g];
+  const bool has_bx = INTRA && X.bx_off && X.bx_off[g + 1] > X.bx_off[g];
+  const bool bonded = gboff[g + 1] > gboff[g] || geoff[g + 1] > geoff[g] || has_bx;
+  // a group without torsions or 1-4 pairs has fxr = 0: its torsion-level
+  // kicks change nothing and are skipped
+  const bool tors = INTRA && X.tor_off && (X.tor_off[g + 1] > X.tor_off[g] || X.o14_off[g + 1] > X.o14_off[g]);
   for (int inrra = 0; inrra < P.ninrra; inrra++) {
-    // the torsion level (fxr) is empty in this engine
+    if (tors) {
+      for (int a = a0; a < a1; a++) {
+        int i = gatoms[a];
+        for (int d = 0; d < 3; d++) vel[d * n + i] += P.dtr2 * fxr[d * n + i];
+      }
+    }
     for (int intra = 0; intra < P.ninnra; intra++) {
       for (int a = a0; a < a1; a++) {
         int i = gatoms[a];
@@ -141,15 +341,32 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
           fxa[i] = fxa[n + i] = fxa[2 * n + i] = 0.;
         }
         group_bonded(g, n, pos, fxa, gboff, bij, bp, geoff, eijk, ep);
+        if (has_bx) group_bondx(g, n, pos, fxa, X);
         for (int a = a0; a < a1; a++) {
           int i = gatoms[a];
           double r = 1. / mass[i];
           fxa[i] *= r; fxa[n + i] *= r; fxa[2 * n + i] *= r;
+          if (INTRA && X.frz && X.frz[i]) freeze_one(i, n, vel, fxa);
         }
       }
       for (int a = a0; a < a1; a++) {
         int i = gatoms[a];
         for (int d = 0; d < 3; d++) vel[d * n + i] += P.dta2 * fxa[d * n + i];
+      }
+    }
+    // force(3) on this group, then the closing torsion-level kick
+    if (tors) {
+      for (int a = a0; a < a1; a++) {
+        int i = gatoms[a];
+        fxr[i] = fxr[n + i] = fxr[2 * n + i] = 0.;
+      }
+      group_tors_level(g, n, pos, q, fxr, X, stat);
+      for (int a = a0; a < a1; a++) {
+        int i = gatoms[a];
+        double r = 1. / mass[i];
+        fxr[i] *= r; fxr[n + i] *= r; fxr[2 * n + i] *= r;
+        if (X.frz && X.frz[i]) freeze_one(i, n, vel, fxr);
+        for (int d = 0; d < 3; d++) vel[d * n + i] += P.dtr2 * fxr[d * n + i];
       }
     }
   }
@@ -319,6 +536,99 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
   sys_acc<30>(v, sy, acc, slots);
 }
 
+// energies and virials of the cross bonds, torsions and 1-4 pairs, per group
+// (getvbondx md_fbocross.c:100-168, getvtors md_ftors.c:296-542 with its
+// PRESSURE tensor, getvonfo md_fonefour.c:160-314).  The 1-4 sums are kept
+// unscaled; the host applies scale_onefour / scale_onefour_e per system.
+__global__ void k_intra_energy(StepP P, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
+                               const double *__restrict__ pos, const double *__restrict__ q, IntraDev X,
+                               double *__restrict__ acc, const int *__restrict__ sys_of,
+                               const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = P.n;
+  // bondx: v, w, t[9] | tors: v, t[9] | onfo: v, w, t[9], v_e, t_e[9]
+  double v[42];
+#pragma unroll
+  for (int k = 0; k < 42; k++) v[k] = 0.;
+  int sy = -1;
+  if (g < P.ngroups) {
+    sy = sys_of[gatoms[gaoff[g]]];
+    for (int b = X.bx_off[g]; b < X.bx_off[g + 1]; b++) {
+      const int4 t = X.bx_ijk[b];
+      const double4 p = X.bx_par[b];
+      const double a3[3] = {pos[t.x] - pos[t.y], pos[n + t.x] - pos[n + t.y], pos[2 * n + t.x] - pos[2 * n + t.y]};
+      const double b3[3] = {pos[t.y] - pos[t.z], pos[n + t.y] - pos[n + t.z], pos[2 * n + t.y] - pos[2 * n + t.z]};
+      const double al = sqrt(a3[0] * a3[0] + a3[1] * a3[1] + a3[2] * a3[2]);
+      const double bl = sqrt(b3[0] * b3[0] + b3[1] * b3[1] + b3[2] * b3[2]);
+      const double dr1 = al - p.x, dr2 = bl - p.y, fk = p.z;
+      v[0] += fk * dr1 * dr2;
+      v[1] -= fk * (bl * dr1 + al * dr2);
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[2 + 3 * r + c] -= fk * (dr1 * b3[c] * b3[r] / bl + dr2 * a3[c] * a3[r] / al);
+    }
+    for (int t = X.tor_off[g]; t < X.tor_off[g + 1]; t++) {
+      TorsTerm T;
+      torsion_term(n, pos, X.tor_ijkl[t], X.tor_par[t], X, T);
+      v[11] += T.pot;
+      // the i-j, j-k and j-l separations times the forces on i, k and l
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          double w = v[12 + 3 * r + c];
+          w -= T.a[r] * T.g[0][c];
+          w += T.b[r] * T.g[2][c];
+          w += (T.b[r] + T.c[r]) * T.dudcos * T.u4[c];
+          v[12 + 3 * r + c] = w;
+        }
+    }
+    bool under = false;
+    for (int o = X.o14_off[g]; o < X.o14_off[g + 1]; o++) {
+      const int4 pr = X.o14_ij[o];
+      const int i = pr.x, j = pr.y;
+      const double d[3] = {pos[i] - pos[j], pos[n + i] - pos[n + j], pos[2 * n + i] - pos[2 * n + j]};
+      const double dis2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      const double4 rng = X.o14_rng[pr.z];
+      if (!(dis2 < rng.y)) continue;
+      const int2 tb = X.o14_tab[pr.z];
+      v[21] += o14_interp(X.o14_v, tb, rng, dis2, &under);
+      const double f = o14_interp(X.o14_dv, tb, rng, dis2, &under);
+      v[22] -= dis2 * f;
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) v[23 + 3 * r + c] -= d[c] * d[r] * f;
+      const double qij = q[i] * q[j];
+      if (qij != 0) {
+        const double fe = qij / sqrt(dis2);
+        v[32] += fe;
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) v[33 + 3 * r + c] += fe * d[c] * d[r] / dis2;
+      }
+    }
+  }
+  int slots[42];
+  slots[0] = ACC_VBOND;
+  slots[1] = ACC_WBOND;
+  slots[11] = ACC_VTORS;
+  slots[21] = ACC_VONFO;
+  slots[22] = ACC_WONFO;
+  slots[32] = ACC_VONFO_E;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    slots[2 + k] = ACC_WBONDXT + k;
+    slots[12 + k] = ACC_WTORST + k;
+    slots[23 + k] = ACC_WONFOT + k;
+    slots[33 + k] = ACC_WONFOET + k;
+  }
+  sys_acc<42>(v, sy, acc, slots);
+}
+
 // end of force(1) / force(0): rmass (utils/md_util.new.c:219) and, inside
 // step(), the closing kick of md_step.c:139-145; then the kinetic tensor of
 // get_p2mt (md_fcntr.c:332-354) for geteng
@@ -326,7 +636,7 @@ __global__ void k_finish(int n, int level, int kick, int rm_l, int rm_s, double 
                          const double *__restrict__ mass, double *__restrict__ fxl, double *__restrict__ fxs,
                          double *__restrict__ vel, double *__restrict__ acc, int *__restrict__ istate,
                          int advance_step, const int *__restrict__ sys_of, int batch,
-                         const int *__restrict__ gs) {
+                         const int *__restrict__ gs, const unsigned char *__restrict__ frz) {
   if (gated_off(gs, 0)) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[6] = {0, 0, 0, 0, 0, 0};
@@ -334,10 +644,18 @@ __global__ void k_finish(int n, int level, int kick, int rm_l, int rm_s, double 
   if (i < n) {
     sy = sys_of[i];
     double r = 1. / mass[i];
+    // freeze_atom closes the force level: the atom keeps no velocity and
+    // no force, so the kick below leaves it at rest
+    const bool frozen = frz && frz[i];
     for (int d = 0; d < 3; d++) {
       int x = d * n + i;
       if (rm_l) fxl[x] *= r;
       if (rm_s) fxs[x] *= r;
+      if (frozen) {
+        if (level == 1) fxl[x] = 0.;
+        fxs[x] = 0.;
+        vel[x] = 0.;
+      }
       if (kick) {
         if (level == 1) vel[x] += dk_l * fxl[x] + (rm_s ? dk_s * fxs[x] : 0.0);
         else vel[x] += dk_s * fxs[x];
@@ -394,6 +712,188 @@ struct UF {
   }
 };
 
+// cross bonds, torsions, 1-4 pairs (global atom indices, CM3D's order within
+// each system, systems in batch order) and their parameters, and the frozen
+// atoms, as read from the system descriptions
+struct IntraHost {
+  std::vector<int4> bx, tor, o14;        // {i, j, k, -} / {i, j, k, l} / {i, j, type, -}
+  std::vector<double4> bx_par;
+  std::vector<int2> tor_par;             // {form, row}
+  std::vector<double2> tor_h;
+  std::vector<double> tor_v;
+  std::vector<double4> o14_rng;
+  std::vector<double> o14_se, o14_v, o14_dv;
+  std::vector<int2> o14_tab;
+  std::vector<unsigned char> frz;
+  bool any_frz = false;
+};
+
+static int collect_intra(Ctx *c, const cm3d_nb_system *systems, int nsys, IntraHost &ih) {
+  ih.frz.assign((size_t)c->n, 0);
+  for (int sy = 0; sy < nsys; sy++) {
+    const cm3d_nb_system *s = systems + sy;
+    const int a0 = c->h_sp[sy].a0, ns = s->natoms;
+    auto atom_ok = [&](int i) { return i >= 0 && i < ns; };
+    for (int b = 0; b < s->nbondx; b++) {
+      const int t = s->idxbondx[b];
+      if (t < 0 || t >= s->nbondx_types || !atom_ok(s->ibondx[b]) || !atom_ok(s->jbondx[b]) ||
+          !atom_ok(s->kbondx[b])) {
+        set_error("system %d cross bond %d: type or atom index out of range", sy, b);
+        return CM3D_NB_ERR_ARG;
+      }
+      ih.bx.push_back(make_int4(a0 + s->ibondx[b], a0 + s->jbondx[b], a0 + s->kbondx[b], 0));
+      ih.bx_par.push_back(make_double4(s->eq1bondx[t], s->eq2bondx[t], s->fkbondx[t], 0.));
+    }
+    const int h0 = (int)ih.tor_h.size(), v0 = (int)(ih.tor_v.size() / CM3D_NB_MAXPOWER_TORS);
+    if (s->ntors > 0) {
+      for (int k = 0; k < s->ntors_harm; k++) ih.tor_h.push_back(make_double2(s->eqtors[k], s->fktors[k]));
+      for (int k = 0; k < s->ntors_series * CM3D_NB_MAXPOWER_TORS; k++) ih.tor_v.push_back(s->vphi[k]);
+    }
+    for (int t = 0; t < s->ntors; t++) {
+      const int ty = s->idxtors[t];
+      if (ty < 0 || ty >= s->ntors_types || !atom_ok(s->itors[t]) || !atom_ok(s->jtors[t]) ||
+          !atom_ok(s->ktors[t]) || !atom_ok(s->ltors[t])) {
+        set_error("system %d torsion %d: type or atom index out of range", sy, t);
+        return CM3D_NB_ERR_ARG;
+      }
+      const int form = s->tors_ind_pot[ty], row = s->tors_ind_pot_num[ty];
+      int2 par;
+      if (form == 0 && row >= 0 && row < s->ntors_harm) {
+        par = make_int2(0, h0 + row);
+      } else if (form == 1 && row >= 0 && row < s->ntors_series) {
+        par = make_int2(1, v0 + row);
+      } else if (form == 2) {
+        // CM3D's getvtors has no break after this case and stops in its
+        // default branch (md_ftors.c:398-423), so no run uses it
+        set_error("system %d torsion type %d: the cosine series with phases (ind_pot 2) is not supported", sy, ty);
+        return CM3D_NB_ERR_ARG;
+      } else {
+        set_error("system %d torsion type %d: form %d / row %d out of range", sy, ty, form, row);
+        return CM3D_NB_ERR_ARG;
+      }
+      ih.tor.push_back(make_int4(a0 + s->itors[t], a0 + s->jtors[t], a0 + s->ktors[t], a0 + s->ltors[t]));
+      ih.tor_par.push_back(par);
+    }
+    const int o0 = (int)ih.o14_rng.size();
+    if (s->n14 > 0) {
+      if (s->n14table < 4) {
+        set_error("system %d: 1-4 tables of %d knots", sy, s->n14table);
+        return CM3D_NB_ERR_ARG;
+      }
+      for (int t = 0; t < s->n14_types; t++) {
+        ih.o14_rng.push_back(make_double4(s->r14min2[t], s->r14max2[t], s->dx214tab[t], s->scale_onefour));
+        ih.o14_se.push_back(s->scale_onefour_e);
+        ih.o14_tab.push_back(make_int2((int)ih.o14_v.size(), s->n14table));
+        const size_t k0 = (size_t)t * s->n14table;
+        ih.o14_v.insert(ih.o14_v.end(), s->v14tab + k0, s->v14tab + k0 + s->n14table);
+        ih.o14_dv.insert(ih.o14_dv.end(), s->dv14tab + k0, s->dv14tab + k0 + s->n14table);
+      }
+    }
+    for (int k = 0; k < s->n14; k++) {
+      const int ty = s->i14dx[k];
+      if (ty < 0 || ty >= s->n14_types || !atom_ok(s->i14[k]) || !atom_ok(s->j14[k])) {
+        set_error("system %d 1-4 pair %d: type or atom index out of range", sy, k);
+        return CM3D_NB_ERR_ARG;
+      }
+      ih.o14.push_back(make_int4(a0 + s->i14[k], a0 + s->j14[k], o0 + ty, 0));
+    }
+    for (int f = 0; f < s->nfreeze; f++) {
+      if (!atom_ok(s->ifreeze[f])) {
+        set_error("system %d frozen atom %d out of range", sy, s->ifreeze[f]);
+        return CM3D_NB_ERR_ARG;
+      }
+      ih.frz[(size_t)(a0 + s->ifreeze[f])] = 1;
+      ih.any_frz = true;
+    }
+  }
+  return CM3D_NB_OK;
+}
+
+// group the intramolecular terms (CM3D's order kept inside a group) and copy
+// them, with their parameters and the frozen-atom flags, to one device buffer
+static int upload_intra(Ctx *c, const IntraHost &ih, const std::vector<int> &gid, int ng) {
+  c->has_tors_level = !ih.tor.empty() || !ih.o14.empty();
+  c->has_intra_x = c->has_tors_level || !ih.bx.empty();
+  if (!c->has_intra_x && !ih.any_frz) return CM3D_NB_OK;
+  std::vector<char> h;
+  auto add = [&](const void *p, size_t bytes) {
+    size_t off = (h.size() + 15) & ~(size_t)15;
+    h.resize(off + (bytes > 0 ? bytes : 16));
+    if (bytes) memcpy(&h[off], p, bytes);
+    return off;
+  };
+  // a term goes to the group of its first atom; the offsets are per group
+  auto group_terms = [&](const std::vector<int4> &terms, std::vector<int> &off, std::vector<int> &order) {
+    off.assign((size_t)ng + 1, 0);
+    for (const int4 &t : terms) off[gid[t.x] + 1]++;
+    for (int g = 0; g < ng; g++) off[g + 1] += off[g];
+    std::vector<int> cur(off.begin(), off.end() - 1);
+    order.assign(terms.size(), 0);
+    for (size_t k = 0; k < terms.size(); k++) order[cur[gid[terms[k].x]]++] = (int)k;
+  };
+  size_t o_bx_off = 0, o_bx = 0, o_bxp = 0, o_tor_off = 0, o_tor = 0, o_torp = 0, o_th = 0, o_tv = 0;
+  size_t o_o14_off = 0, o_o14 = 0, o_rng = 0, o_se = 0, o_tab = 0, o_v = 0, o_dv = 0, o_frz = 0;
+  if (c->has_intra_x) {
+    std::vector<int> off, order;
+    group_terms(ih.bx, off, order);
+    std::vector<int4> bx(order.size());
+    std::vector<double4> bxp(order.size());
+    for (size_t k = 0; k < order.size(); k++) {
+      bx[k] = ih.bx[order[k]];
+      bxp[k] = ih.bx_par[order[k]];
+    }
+    o_bx_off = add(off.data(), sizeof(int) * off.size());
+    o_bx = add(bx.data(), sizeof(int4) * bx.size());
+    o_bxp = add(bxp.data(), sizeof(double4) * bxp.size());
+    group_terms(ih.tor, off, order);
+    std::vector<int4> tor(order.size());
+    std::vector<int2> torp(order.size());
+    for (size_t k = 0; k < order.size(); k++) {
+      tor[k] = ih.tor[order[k]];
+      torp[k] = ih.tor_par[order[k]];
+    }
+    o_tor_off = add(off.data(), sizeof(int) * off.size());
+    o_tor = add(tor.data(), sizeof(int4) * tor.size());
+    o_torp = add(torp.data(), sizeof(int2) * torp.size());
+    o_th = add(ih.tor_h.data(), sizeof(double2) * ih.tor_h.size());
+    o_tv = add(ih.tor_v.data(), sizeof(double) * ih.tor_v.size());
+    group_terms(ih.o14, off, order);
+    std::vector<int4> o14(order.size());
+    for (size_t k = 0; k < order.size(); k++) o14[k] = ih.o14[order[k]];
+    o_o14_off = add(off.data(), sizeof(int) * off.size());
+    o_o14 = add(o14.data(), sizeof(int4) * o14.size());
+    o_rng = add(ih.o14_rng.data(), sizeof(double4) * ih.o14_rng.size());
+    o_se = add(ih.o14_se.data(), sizeof(double) * ih.o14_se.size());
+    o_tab = add(ih.o14_tab.data(), sizeof(int2) * ih.o14_tab.size());
+    o_v = add(ih.o14_v.data(), sizeof(double) * ih.o14_v.size());
+    o_dv = add(ih.o14_dv.data(), sizeof(double) * ih.o14_dv.size());
+  }
+  if (ih.any_frz) o_frz = add(ih.frz.data(), ih.frz.size());
+  CK(cudaMalloc(&c->intra_buf, h.size()));
+  CK(cudaMemcpy(c->intra_buf, h.data(), h.size(), cudaMemcpyHostToDevice));
+  const char *b = reinterpret_cast<const char *>(c->intra_buf);
+  IntraDev &X = c->intra;
+  if (c->has_intra_x) {
+    X.bx_off = reinterpret_cast<const int *>(b + o_bx_off);
+    X.bx_ijk = reinterpret_cast<const int4 *>(b + o_bx);
+    X.bx_par = reinterpret_cast<const double4 *>(b + o_bxp);
+    X.tor_off = reinterpret_cast<const int *>(b + o_tor_off);
+    X.tor_ijkl = reinterpret_cast<const int4 *>(b + o_tor);
+    X.tor_par = reinterpret_cast<const int2 *>(b + o_torp);
+    X.tor_h = reinterpret_cast<const double2 *>(b + o_th);
+    X.tor_v = reinterpret_cast<const double *>(b + o_tv);
+    X.o14_off = reinterpret_cast<const int *>(b + o_o14_off);
+    X.o14_ij = reinterpret_cast<const int4 *>(b + o_o14);
+    X.o14_rng = reinterpret_cast<const double4 *>(b + o_rng);
+    X.o14_se = reinterpret_cast<const double *>(b + o_se);
+    X.o14_tab = reinterpret_cast<const int2 *>(b + o_tab);
+    X.o14_v = reinterpret_cast<const double *>(b + o_v);
+    X.o14_dv = reinterpret_cast<const double *>(b + o_dv);
+  }
+  if (ih.any_frz) X.frz = reinterpret_cast<const unsigned char *>(b + o_frz);
+  return CM3D_NB_OK;
+}
+
 int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   const int n = c->n;
   // every system's bonds, bends and excluded Ewald pairs with global atom
@@ -424,6 +924,9 @@ int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
     }
     for (int b = 0; b < s->necorr; b++) mc.push_back(make_int2(a0 + s->iecorr[b], a0 + s->jecorr[b]));
   }
+  IntraHost ih;
+  int rc;
+  if ((rc = collect_intra(c, systems, nsys, ih))) return rc;
   const int nb = (int)mb.size(), ne = (int)me.size(), nc = (int)mc.size();
   UF uf(n);
   for (int b = 0; b < nb; b++) uf.u(mb[b].x, mb[b].y);
@@ -432,6 +935,16 @@ int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
     uf.u(me[b].y, me[b].z);
   }
   for (int b = 0; b < nc; b++) uf.u(mc[b].x, mc[b].y);
+  for (const int4 &t : ih.bx) {
+    uf.u(t.x, t.y);
+    uf.u(t.y, t.z);
+  }
+  for (const int4 &t : ih.tor) {
+    uf.u(t.x, t.y);
+    uf.u(t.y, t.z);
+    uf.u(t.z, t.w);
+  }
+  for (const int4 &t : ih.o14) uf.u(t.x, t.y);
   // groups numbered by their lowest atom
   std::vector<int> gid(n, -1), root_gid(n, -1);
   int ng = 0;
@@ -502,15 +1015,32 @@ int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   CK(cudaMemcpy(c->bend_p, ep.data(), sizeof(double2) * ep.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ecorr_ij, cij.data(), sizeof(int2) * cij.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ecorr_pairs, cpair.data(), sizeof(int2) * cpair.size(), cudaMemcpyHostToDevice));
-  return CM3D_NB_OK;
+  return upload_intra(c, ih, gid, ng);
 }
 
 int run_bonded(Ctx *c) {
   StepP P = step_params(c);
   const int B = 128;
-  k_bonded<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, c->grp_atom_off, c->grp_atoms, c->pos, c->mass, c->fxa,
-                                                     c->grp_bond_off, c->bond_ij, c->bond_p, c->grp_bend_off,
-                                                     c->bend_ijk, c->bend_p);
+  k_bonded<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, c->grp_atom_off, c->grp_atoms, c->pos, c->mass, c->vel,
+                                                     c->fxa, c->grp_bond_off, c->bond_ij, c->bond_p,
+                                                     c->grp_bend_off, c->bend_ijk, c->bend_p, c->intra);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+// force(3): the torsion level (torsions + 1-4 pairs) into fxr; with neither
+// in the context fxr is zero and only frozen atoms need their velocity cleared
+int run_tors_level(Ctx *c) {
+  if (!c->has_tors_level && !c->intra.frz) {
+    CK(cudaMemsetAsync(c->fxr, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+    return CM3D_NB_OK;
+  }
+  StepP P = step_params(c);
+  const int B = 128;
+  if (!c->has_tors_level) CK(cudaMemsetAsync(c->fxr, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+  k_tors_level<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, c->grp_atom_off, c->grp_atoms, c->pos, c->q, c->mass,
+                                                         c->vel, c->fxr, c->intra, c->stat);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
@@ -526,8 +1056,13 @@ int group_init(Ctx *c, bool zero_fxs) {
                                                          c->ecorr_ij, c->grp_bond_off, c->bond_ij, c->bond_p,
                                                          c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc, c->sp,
                                                          c->sys_of, c->gate);
-  tend(c, 3, e0);
   c->launches++;
+  if (c->has_intra_x) {
+    k_intra_energy<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, c->grp_atom_off, c->grp_atoms, c->pos, c->q,
+                                                             c->intra, c->acc, c->sys_of, c->gate);
+    c->launches++;
+  }
+  tend(c, 3, e0);
   CKL(c);
   return CM3D_NB_OK;
 }
@@ -537,7 +1072,7 @@ int finish_level1(Ctx *c, double dter, double dter1, bool kick) {
   bool rs = c->need_short || c->nres_lrf > 1;
   k_finish<<<grid_for(c->n, B), B, 0, c->st>>>(c->n, 1, kick ? 1 : 0, 1, rs ? 1 : 0, dter, dter1, c->mass, c->fxl,
                                                c->fxs, c->vel, c->acc, c->istate, kick ? 1 : 0, c->sys_of,
-                                               c->nsys > 1, c->gate);
+                                               c->nsys > 1, c->gate, c->intra.frz);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
@@ -545,7 +1080,8 @@ int finish_level1(Ctx *c, double dter, double dter1, bool kick) {
 
 static int finish_level0(Ctx *c, double dts2, bool kick) {
   k_finish<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, 0, kick ? 1 : 0, 0, 1, 0, dts2, c->mass, c->fxl, c->fxs,
-                                                   c->vel, c->acc, c->istate, 0, c->sys_of, c->nsys > 1, c->gate);
+                                                   c->vel, c->acc, c->istate, 0, c->sys_of, c->nsys > 1, c->gate,
+                                                   c->intra.frz);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
@@ -581,10 +1117,11 @@ static int zero_acc(Ctx *c) {
   return CM3D_NB_OK;
 }
 
-// force(iflg) of md_fcntr.c:44-134 (levels 0, 1, 2)
+// force(iflg) of md_fcntr.c:44-134 (levels 0-3)
 int run_force(Ctx *c, int iflg) {
   int rc;
   if (iflg == 2) return run_bonded(c);
+  if (iflg == 3) return run_tors_level(c);
   if (!c->lists_built) {
     set_error("force(%d) before get_ngbr(): the pair lists do not exist yet", iflg);
     return CM3D_NB_ERR_STATE;
@@ -632,10 +1169,12 @@ static int one_level(Ctx *c, int intr, bool gated) {
   if ((rc = clear_rebuild(c))) return rc;
   cudaEvent_t e0;
   tbegin(c, 3, &e0);
-  k_inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
+  auto inner = c->has_intra_x || c->intra.frz ? k_inner<true> : k_inner<false>;
+  inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
                                                     c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
                                                     c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
-                                                    c->bend_p, c->sp, c->sys_of, c->sreb, c->istate, c->gate);
+                                                    c->bend_p, c->sp, c->sys_of, c->sreb, c->istate, c->gate,
+                                                    c->intra, c->q, c->fxr, c->stat);
   tend(c, 3, e0);
   c->launches++;
   CKL(c);

@@ -10,7 +10,8 @@
  *   step_init  builds the engine's system description from CM3D's own
  *              SIMPARMS / COORDS / INTER structs once, uploads it
  *              (cm3d_nb_create), runs CM3D's step_init sequence on the device
- *              (cm3d_nb_step_init: get_ngbr, force(1), force(2)), and fills
+ *              (cm3d_nb_step_init: get_ngbr, force(1), force(2),
+ *              force(3)), and fills
  *              CM3D's ENERGIES the way getvireal(..., 1) does
  *              (energy/control/md_fcntr.c:136-257), then calls CM3D's own
  *              geteng and gettngbr as md_step.c:53-55 does;
@@ -19,9 +20,9 @@
  *              COORDS (CM3D's writers and geteng read them) and refills
  *              ENERGIES.
  *
- * What the engine does not compute -- thermostats and barostats, torsions,
- * 1-4 and cross bonds, frozen atoms, external fields, dipoles, non-periodic
- * boxes -- stops the run through md_error with the reason, as CM3D reports
+ * What the engine does not compute -- thermostats and barostats, external
+ * fields, dipoles, non-periodic boxes, the phased cosine torsion form --
+ * stops the run through md_error with the reason, as CM3D reports
  * unsupported input; nothing falls back to a CPU path.
  *
  * Environment: CM3D_NB_MODE=plain selects the plain FP64 engine (default:
@@ -33,6 +34,7 @@
 
 static cm3d_nb_ctx *g_ctx = NULL;
 static int *g_map = NULL, *g_eoff = NULL, *g_eidx = NULL, *g_coff = NULL, *g_cidx = NULL;
+static double *g_v14 = NULL, *g_dv14 = NULL;
 
 static void nb_fail(const char *what)
 {
@@ -59,11 +61,9 @@ static void check_supported(SIMPARMS *simparms, COORDS *coords)
   if (simparms->iperd != 3) unsupported("a non-periodic or partially periodic box (iperd != 3)");
   if (simparms->iensemble != 0) unsupported("an ensemble other than nve");
   if (simparms->ivol) unsupported("a variable cell (ivol)");
-  if (simparms->nfreeze > 0) unsupported("frozen atoms");
   if (simparms->iextern) unsupported("an external field");
   if (simparms->ipolar) unsupported("polarizable dipoles");
-  if (coords->tors.ntorss > 0 || coords->onfo.n14s > 0 || coords->bondxs.nbondxs > 0)
-    unsupported("torsions, 1-4 interactions or cross bonds");
+  (void)coords;
 }
 
 /* CSR copy of CM3D's per-atom exclusion lists (INTER.nexclude/exclude,
@@ -159,6 +159,55 @@ static void create_engine(SIMPARMS *simparms, COORDS *coords, INTER *inter)
   s.ibend = coords->bends.ibend; s.jbend = coords->bends.jbend; s.kbend = coords->bends.kbend;
   s.idxbend = coords->bends.idxbend; s.itypbend = coords->bends.itypbend;
   s.eqbend = coords->bends.eqbend; s.fkbend = coords->bends.fkbend;
+  /* torsions, 1-4 pairs, cross bonds (TORS / ONFO / BONDXS) */
+  s.ntors = coords->tors.ntorss;
+  if (s.ntors > 0) {
+    int t, nh = 0, nv = 0;
+    s.ntors_types = coords->tors.itypes;
+    s.itors = coords->tors.itors; s.jtors = coords->tors.jtors;
+    s.ktors = coords->tors.ktors; s.ltors = coords->tors.ltors;
+    s.idxtors = coords->tors.idxtors;
+    s.tors_ind_pot = coords->tors.ind_pot;
+    s.tors_ind_pot_num = coords->tors.ind_pot_num;
+    for (t = 0; t < coords->tors.itypes; t++) {
+      int k = coords->tors.ind_pot_num[t] + 1;
+      if (coords->tors.ind_pot[t] == 0 && k > nh) nh = k;
+      if (coords->tors.ind_pot[t] == 1 && k > nv) nv = k;
+    }
+    s.ntors_harm = nh;
+    s.eqtors = coords->tors.eqtors; s.fktors = coords->tors.fktors;
+    s.ntors_series = nv;
+    s.vphi = nv > 0 ? &coords->tors.vphi[0][0] : NULL;
+  }
+  s.n14 = coords->onfo.n14s;
+  if (s.n14 > 0) {
+    /* ONFO's tables are rows of a dmatrix: copy them into one block */
+    int t, nt14 = coords->onfo.itypes, nk = coords->onfo.n14table;
+    g_v14 = (double *)malloc(sizeof(double) * (size_t)nt14 * nk);
+    g_dv14 = (double *)malloc(sizeof(double) * (size_t)nt14 * nk);
+    for (t = 0; t < nt14; t++) {
+      memcpy(g_v14 + (size_t)t * nk, coords->onfo.v14tab[t], sizeof(double) * nk);
+      memcpy(g_dv14 + (size_t)t * nk, coords->onfo.dv14tab[t], sizeof(double) * nk);
+    }
+    s.n14_types = nt14;
+    s.n14table = nk;
+    s.i14 = coords->onfo.i14; s.j14 = coords->onfo.j14; s.i14dx = coords->onfo.i14dx;
+    s.r14min2 = coords->onfo.r14min2; s.r14max2 = coords->onfo.r14max2;
+    s.dx214tab = coords->onfo.dx214tab;
+    s.v14tab = g_v14; s.dv14tab = g_dv14;
+    s.scale_onefour = coords->onfo.scale_onefour;
+    s.scale_onefour_e = coords->onfo.scale_onefour_e;
+  }
+  s.nbondx = coords->bondxs.nbondxs;
+  if (s.nbondx > 0) {
+    s.nbondx_types = coords->bondxs.itypes;
+    s.ibondx = coords->bondxs.ibondx; s.jbondx = coords->bondxs.jbondx;
+    s.kbondx = coords->bondxs.kbondx; s.idxbondx = coords->bondxs.idxbox;
+    s.eq1bondx = coords->bondxs.eq1bondx; s.eq2bondx = coords->bondxs.eq2bondx;
+    s.fkbondx = coords->bondxs.fkbondx;
+  }
+  s.nfreeze = simparms->nfreeze;
+  s.ifreeze = coords->ifreeze;
 
   cm3d_nb_default_options(&opt);
   if (mode && strcmp(mode, "plain") == 0) opt.mode = CM3D_NB_PLAIN_FP64;
@@ -172,7 +221,6 @@ static void create_engine(SIMPARMS *simparms, COORDS *coords, INTER *inter)
 static void fill_energies(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies)
 {
   cm3d_nb_energies e;
-  double vol = get_deth(coords->hmat);
   int i;
   nb_check(cm3d_nb_get_energies(g_ctx, &e), "cm3d_nb_get_energies");
   energies->vinter = e.vinter;
@@ -181,33 +229,39 @@ static void fill_energies(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies
   energies->vewald = e.vewald;
   energies->vbond = e.vbond;
   energies->vbend = e.vbend;
-  energies->vtors = energies->vbondx = energies->vonfo = energies->vonfo_e = 0.0;
+  energies->vtors = e.vtors;
+  energies->vonfo = e.vonfo;
+  energies->vonfo_e = e.vonfo_e;
+  energies->vbondx = 0.0;             /* getvbondx adds into vbond (md_fcntr.c:182) */
   energies->vextern = energies->vextern_e = 0.0;
   energies->winter = e.winter;
   energies->welec = e.welec;
   energies->wewald = e.wewald;
   energies->wbond = e.wbond;
   energies->wbend = e.wbend;
-  energies->wtors = energies->wbondx = energies->wonfo = energies->wonfo_e = 0.0;
+  energies->wtors = e.wtors;
+  energies->wonfo = e.wonfo;
+  energies->wonfo_e = e.wonfo_e;
+  energies->wbondx = 0.0;
   energies->wextern = energies->wextern_e = 0.0;
   energies->US = e.US;
   energies->U = e.U;
   energies->W = e.W;
-  energies->UI = e.vbond + e.vbend;
-  energies->WI = e.wbond + e.wbend;
+  energies->UI = e.UI;
+  energies->WI = e.WI;
   for (i = 0; i < 9; i++) {
     energies->wintertensor[i] = e.wintertensor[i];
     energies->welectensor[i] = e.welectensor[i];
     energies->wewaldtensor[i] = e.wewaldtensor[i];
     energies->Wtensor[i] = e.Wtensor[i];
-    /* bonded virial tensor: the engine's pressure tensor minus its kinetic
-       and nonbonded parts */
-    energies->WItensor[i] = e.prs_tensor[i] * vol - e.p2m_tensor[i] - e.Wtensor[i];
+    /* the intramolecular virial tensor as one sum (CM3D reads only the sum) */
+    energies->WItensor[i] = e.WItensor[i];
     energies->wbondtensor[i] = energies->WItensor[i];
     energies->wbendtensor[i] = energies->wtorstensor[i] = energies->wbondxtensor[i] = 0.0;
     energies->wonfotensor[i] = energies->wonfo_etensor[i] = 0.0;
   }
   (void)simparms;
+  (void)coords;
 }
 
 static void pull_state(COORDS *coords)
@@ -221,6 +275,7 @@ static void pull_forces(COORDS *coords)
   nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXL, coords->fxl, coords->fyl, coords->fzl), "get_forces");
   nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXS, coords->fxs, coords->fys, coords->fzs), "get_forces");
   nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXA, coords->fxa, coords->fya, coords->fza), "get_forces");
+  nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXR, coords->fxr, coords->fyr, coords->fzr), "get_forces");
 }
 
 /* NGBR as get_ngbr leaves it (energy/control/ngbr_list.c:308): the pair

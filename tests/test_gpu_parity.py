@@ -32,7 +32,7 @@ ETOL = {_abi.PLAIN_FP64: 1e-10, _abi.MIXED: 1e-5}
 VTOL = {_abi.PLAIN_FP64: 1e-10, _abi.MIXED: 5e-5}
 VIRIAL_KEYS = {"winter", "welec", "W", "prsi"}
 ALL = ["lj2", "lj256", "abutane", "argon864", "water216", "binary256", "water4096"]
-DYN = ["lj2", "lj256", "argon864", "water216", "binary256", "water4096"]   # no frozen atoms / torsions
+DYN = ALL
 
 
 def engine(name, mode, **kw):
@@ -141,12 +141,24 @@ def test_level1_forces_and_energies(engine_lib, name, mode):
     e.close()
 
 
+def frozen_zeroed(d, f):
+    """f with the frozen atoms' rows zeroed, as freeze_atom leaves a level"""
+    f = f.copy()
+    if int(d.get("nfreeze", [0])[0]) > 0:
+        f[:, d["ifreeze"]] = 0.0
+    return f
+
+
 @pytest.mark.parametrize("name", DYN)
 def test_bonded_level(engine_lib, name):
+    """force(2): bonds + bends + cross bonds, then rmass and freeze"""
     d, e = engine(name, _abi.MIXED)
     e.force(2)
     m = d["amass"]
-    want = (xyz(d, "f_bond") + xyz(d, "f_bend")) / m
+    want = xyz(d, "f_bond") + xyz(d, "f_bend")
+    if "f_bondx" in d:
+        want = want + xyz(d, "f_bondx")
+    want = frozen_zeroed(d, want / m)
     # the generated molecules start at exactly r0 / theta0, where the bonded
     # forces are round-off: floor the denominator with the system's force scale
     fs = force_scale(d) / float(np.sqrt((m ** 2).mean()))
@@ -235,3 +247,38 @@ def test_status_counts_resets(engine_lib):
     assert st["resets"] == 12
     assert st["rebuilds"] == 14      # step_init's build + 13 during the run
     e.close()
+
+
+TORS_ENERGIES = ("vtors", "wtors", "vonfo", "vonfo_e", "wonfo", "wonfo_e", "UI", "WI", "vbond", "wbond", "potra")
+
+
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+def test_torsion_level(engine_lib, mode):
+    """force(3) (ftors + fonfo, rmass, freeze) against CM3D's fxr after
+    step_init, and the torsion, 1-4 and cross-bond energies and virials of
+    getvireal; these terms are FP64 in both engines"""
+    d, e = engine("abutane", mode)
+    e.get_ngbr()
+    e.force(1)
+    e.force(2)
+    e.force(3)
+    fs = force_scale(d) / float(np.sqrt((d["amass"] ** 2).mean()))
+    assert rel_rms(e.forces(_abi.FXR), xyz(d, "acc_r"), fs) <= 1e-12
+    en = e.energies()
+    for k in TORS_ENERGIES:
+        assert close(en[k], float(d[f"e0_{k}"][0]), 1e-12 if k != "wtors" else 1e-9), k
+    wit, want = np.array(en["WItensor"]), d["e0_WItensor"]
+    assert np.abs(wit - want).max() <= 1e-12 * np.abs(want).max()
+    e.close()
+
+
+def test_torsion_terms_refused_form(engine_lib):
+    """the phased cosine form (ind_pot 2), on which CM3D's getvtors stops, is
+    refused at create with the reason"""
+    d = golden("abutane")
+    s = System.from_arrays(d)
+    ind = s["tors_ind_pot"].copy()
+    ind[0] = 2
+    s["tors_ind_pot"] = ind
+    with pytest.raises(EngineError, match="ind_pot 2"):
+        Engine(s, mode=_abi.MIXED)
