@@ -19,7 +19,8 @@ Printed: one JSON line (rank 0) with the contract's keys plus
   cpu_baseline    CM3D itself (oracle/_ref/ref_bench) on this host's cores
   e2e             the same metric through the public API with host buffers
   latency         per-step device time p50 / p99
-  other_workloads the water-12288 box, mixed and plain, in the same run
+  other_workloads the water-12288 box, mixed and plain, and 1024 boxes of
+                  CM3D's abutane molecule (the torsion level), in the same run
   serving         the serving loop on a Poisson stream of water-box jobs
                   (4 jobs/s over 5 s): job latency p50/p95/p99 and aggregate
                   atom-steps/s, mixed against plain FP64 on the same jobs
@@ -379,6 +380,27 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
             "clocks": clk.summary(), "autotune": tune}
 
 
+def intra_arm(device: int, copies: int, steps: int, warmup: int, flush) -> dict:
+    """The torsion path: CM3D's test/abutane molecule (14 atoms: torsions,
+    1-4 pairs, cross bonds, two frozen atoms, Ewald; RESPA nres_tors 2,
+    nres_intra 2), `copies` independent boxes in one batch, from the
+    state CM3D itself dumped (tests/golden/abutane.npz)."""
+    from cm3d_b200 import _abi
+    from cm3d_b200.engine import Engine
+    from cm3d_b200.system import System
+    d = dict(np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "abutane.npz")))
+    base = System.from_arrays(d)
+    eng = Engine([base.copy() for _ in range(copies)], mode=_abi.MIXED, device=device)
+    eng.step_init()
+    ms, launches, _ = timed_run(eng, steps, warmup, 1, flush)
+    n = eng.n
+    eng.close()
+    return {"workload": f"abutane-{copies}: CM3D's test/abutane molecule (14 atoms, 27 torsions, 27 1-4 "
+                        f"pairs, 3 cross bonds, 2 frozen atoms, Ewald), {copies} boxes in one batch",
+            "value": n * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+            "gpu_launches_per_step": launches / steps}
+
+
 def serving_arm(rate: float, window: float, device: int, plain: bool) -> dict:
     """The serving loop (cm3d_b200.serving) on a Poisson stream of water-box
     jobs (configs.serving_plan: molecules log-uniform in [256, 16384], steps
@@ -523,6 +545,9 @@ def main() -> None:
             "speedup_mixed_vs_plain": (wval / wplain["value"]) if wplain else None,
             "roofline": wm["roofline"], "autotune": wm["autotune"],
             "status": {k: wm["status"][k] for k in ("rebuilds", "resets")}}
+
+    if not args.no_extra and world == 1:
+        other["abutane1024"] = intra_arm(local, 1024, 200, 10, flush)
 
     serving = None
     if not args.no_extra and world == 1:
