@@ -285,6 +285,7 @@ struct Ctx {
   int *icharge = nullptr;
   int *ka_d = nullptr, *kb_d = nullptr, *kc_d = nullptr;
   int ks_tiles = 0, ks_tile_atoms = 0, kf_split = 1;
+  bool ks_small = false;                // batch of systems with <= 32 charges: one-warp k-space tiles
   size_t kf_smem = 0;
   double *kf_part = nullptr;            // per row split partial reciprocal forces (mixed, split > 1)
   int2 *ecorr_pairs = nullptr;          // CM3D's iecorr/jecorr order

@@ -35,6 +35,13 @@ constexpr int KS_THREADS = 256;
 constexpr int KS_A = 8;            // atoms per thread, structure factors
 constexpr int KF_A = 2;            // atoms per thread, forces
 constexpr int MAX_ROWLEN = 128;    // 2 kmax + 1 <= 128
+// A batch whose every system has at most KS_SMALL charges (small molecules
+// with a large k set) runs the structure factors and forces with one warp
+// per block and one atom per thread: the 256 x 8 atom tiles would leave all
+// but a few lanes idle.  For such systems both tilings hold each atom in the
+// same lane of warp 0 and add only exact zeros besides, so the results are
+// bit for bit the same.
+constexpr int KS_SMALL = 32;
 
 // ------------------------------------------------------------ mixed mode
 // BATCH = true (every kernel below): the context holds several systems and
@@ -69,7 +76,7 @@ __device__ __forceinline__ float phase_rad(unsigned phi) {
   return (float)(int)phi * 1.4629180792671596e-09f;   // 2 pi / 2^32
 }
 
-template <bool BATCH>
+template <bool BATCH, int A = KS_A>
 __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *__restrict__ kfrac, int nrows,
                                                            const int4 *__restrict__ rows,
                                                            const int *__restrict__ row_k0, int rows_per_block,
@@ -80,12 +87,12 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
   if (gated_off(gs, 0)) return;
   __shared__ float2 red[KS_THREADS / 32][MAX_ROWLEN];
   // this block's atoms [abase, aend), rows [rbeg, rend) and partial-S(k) base
-  int abase = blockIdx.x * (KS_THREADS * KS_A), aend = nq, rbeg = 0, rend = nrows;
+  int abase = blockIdx.x * (blockDim.x * A), aend = nq, rbeg = 0, rend = nrows;
   long long sbase = (long long)blockIdx.x * ktot;
   if (BATCH) {
     const SysP &S = sp[tile_sys[blockIdx.x]];
     const int lt = blockIdx.x - S.ktile0;
-    abase = S.q0 + lt * (KS_THREADS * KS_A);
+    abase = S.q0 + lt * (blockDim.x * A);
     aend = S.q0 + S.nq;
     rbeg = S.krow0;
     rend = S.krow0 + S.nrows;
@@ -94,11 +101,11 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
   const int r0 = rbeg + blockIdx.y * rows_per_block;
   const int r1 = min(rend, r0 + rows_per_block);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  unsigned u0[KS_A], u1[KS_A], u2[KS_A];
-  float tq[KS_A], cs[KS_A], sn[KS_A];
+  unsigned u0[A], u1[A], u2[A];
+  float tq[A], cs[A], sn[A];
 #pragma unroll
-  for (int m = 0; m < KS_A; m++) {
-    int a = abase + m * KS_THREADS + threadIdx.x;
+  for (int m = 0; m < A; m++) {
+    int a = abase + m * blockDim.x + threadIdx.x;
     if (a < aend) {
       uint4 v = kfrac[a];
       u0[m] = v.x; u1[m] = v.y; u2[m] = v.z;
@@ -113,20 +120,23 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
   for (int r = r0; r < r1; r++) {
     const int4 row = rows[r];
     const int len = row.w;
-    float c[KS_A], s[KS_A];
+    float c[A], s[A];
 #pragma unroll
-    for (int m = 0; m < KS_A; m++) {
+    for (int m = 0; m < A; m++) {
       unsigned phi = (unsigned)row.x * u0[m] + (unsigned)row.y * u1[m] + (unsigned)row.z * u2[m];
       __sincosf(phase_rad(phi), &s[m], &c[m]);
     }
     for (int kk = 0; kk < len; kk++) {
       float sr = 0.f, si = 0.f;
 #pragma unroll
-      for (int m = 0; m < KS_A; m++) {
+      for (int m = 0; m < A; m++) {
         sr = fmaf(tq[m], c[m], sr);
         si = fmaf(tq[m], s[m], si);
-        float cn = c[m] * cs[m] - s[m] * sn[m];
-        float snn = s[m] * cs[m] + c[m] * sn[m];
+        // explicit roundings: every instantiation (tile shape) rotates
+        // the phase with the same operations, so a system's sums do not
+        // depend on the tiling the compiler saw
+        float cn = fmaf(c[m], cs[m], -__fmul_rn(s[m], sn[m]));
+        float snn = fmaf(s[m], cs[m], __fmul_rn(c[m], sn[m]));
         c[m] = cn;
         s[m] = snn;
       }
@@ -139,7 +149,7 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
     for (int kk = threadIdx.x; kk < len; kk += blockDim.x) {
       double ar = 0, ai = 0;
 #pragma unroll
-      for (int q2 = 0; q2 < KS_THREADS / 32; q2++) {
+      for (int q2 = 0; q2 < (int)(blockDim.x >> 5); q2++) {
         ar += red[q2][kk].x;
         ai += red[q2][kk].y;
       }
@@ -207,7 +217,7 @@ __global__ void k_sred(int ktot, int ntiles, const double2 *__restrict__ spart, 
   else block_acc<11>(v, acc, slots);
 }
 
-template <bool BATCH>
+template <bool BATCH, int A = KF_A>
 __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4 *__restrict__ kfrac,
                                                              const int *__restrict__ icharge, int n, int nrows,
                                                              const int4 *__restrict__ rows,
@@ -230,20 +240,20 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
     r0 = S.krow0 + blockIdx.y * rps;
     r1 = min(rend, r0 + rps);
     kend = r1 < rend ? (r1 > r0 ? row_k0[r1] : 0) : S.kk0 + S.ktot;
-    abase = S.q0 + (blockIdx.x - S.ftile0) * (blockDim.x * KF_A);
+    abase = S.q0 + (blockIdx.x - S.ftile0) * (blockDim.x * A);
     aend = S.q0 + S.nq;
     hmati = S.hi;
   } else {
     r0 = blockIdx.y * rows_per_split;
     r1 = min(nrows, r0 + rows_per_split);
     kend = (r1 < nrows) ? row_k0[r1] : ktot;
-    abase = blockIdx.x * (blockDim.x * KF_A);
+    abase = blockIdx.x * (blockDim.x * A);
     aend = nq;
   }
   if (r0 >= r1) {
     // no rows for this split: its share of the partial forces is zero
     if (part)
-      for (int m = 0; m < KF_A; m++) {
+      for (int m = 0; m < A; m++) {
         const int jq = abase + m * blockDim.x + threadIdx.x;
         if (jq < aend) {
           const size_t o = ((size_t)blockIdx.y * nq + jq) * 3;
@@ -255,12 +265,12 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
   const int kbase = row_k0[r0];
   for (int k = threadIdx.x; k < kend - kbase; k += blockDim.x) ak_s[k] = akf[kbase + k];
   __syncthreads();
-  unsigned u0[KF_A], u1[KF_A], u2[KF_A];
-  float cs[KF_A], sn[KF_A], tq[KF_A];
-  double U0[KF_A], U1[KF_A], U2[KF_A];
-  int jq[KF_A];
+  unsigned u0[A], u1[A], u2[A];
+  float cs[A], sn[A], tq[A];
+  double U0[A], U1[A], U2[A];
+  int jq[A];
 #pragma unroll
-  for (int m = 0; m < KF_A; m++) {
+  for (int m = 0; m < A; m++) {
     jq[m] = abase + m * blockDim.x + threadIdx.x;
     U0[m] = U1[m] = U2[m] = 0.0;
     if (jq[m] < aend) {
@@ -277,9 +287,9 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
     const int4 row = rows[r];
     const int len = row.w;
     const int kb0 = row_k0[r] - kbase;
-    float c[KF_A], s[KF_A], W0[KF_A], W1[KF_A];
+    float c[A], s[A], W0[A], W1[A];
 #pragma unroll
-    for (int m = 0; m < KF_A; m++) {
+    for (int m = 0; m < A; m++) {
       unsigned phi = (unsigned)row.x * u0[m] + (unsigned)row.y * u1[m] + (unsigned)row.z * u2[m];
       __sincosf(phase_rad(phi), &s[m], &c[m]);
       W0[m] = W1[m] = 0.f;
@@ -288,34 +298,37 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
     for (int kk = 0; kk < len; kk++) {
       const float2 a = ak_s[kb0 + kk];
 #pragma unroll
-      for (int m = 0; m < KF_A; m++) {
-        float wv = a.x * s[m] - a.y * c[m];
-        W0[m] += wv;
+      for (int m = 0; m < A; m++) {
+        float wv = fmaf(a.x, s[m], -__fmul_rn(a.y, c[m]));
+        W0[m] = __fadd_rn(W0[m], wv);
         W1[m] = fmaf(kcf, wv, W1[m]);
-        float cn = c[m] * cs[m] - s[m] * sn[m];
-        float snn = s[m] * cs[m] + c[m] * sn[m];
+        // explicit roundings: every instantiation (tile shape) rotates
+        // the phase with the same operations, so a system's sums do not
+        // depend on the tiling the compiler saw
+        float cn = fmaf(c[m], cs[m], -__fmul_rn(s[m], sn[m]));
+        float snn = fmaf(s[m], cs[m], __fmul_rn(c[m], sn[m]));
         c[m] = cn;
         s[m] = snn;
       }
       kcf += 1.f;
     }
 #pragma unroll
-    for (int m = 0; m < KF_A; m++) {
-      U0[m] += (double)row.x * (double)W0[m];
-      U1[m] += (double)row.y * (double)W0[m];
-      U2[m] += (double)W1[m];
+    for (int m = 0; m < A; m++) {
+      U0[m] = fma((double)row.x, (double)W0[m], U0[m]);
+      U1[m] = fma((double)row.y, (double)W0[m], U1[m]);
+      U2[m] = __dadd_rn(U2[m], (double)W1[m]);
     }
   }
   const double TPI = 2.0 * M_PI;
 #pragma unroll
-  for (int m = 0; m < KF_A; m++) {
+  for (int m = 0; m < A; m++) {
     if (jq[m] >= aend) continue;
     int i = icharge[jq[m]];
     double t = TPI * (double)tq[m];
     // F = tq 2 pi H^-T U  (k = 2 pi H^-T n, md_ewald.c:248-251)
-    double fx = t * (hmati[0] * U0[m] + hmati[3] * U1[m] + hmati[6] * U2[m]);
-    double fy = t * (hmati[1] * U0[m] + hmati[4] * U1[m] + hmati[7] * U2[m]);
-    double fz = t * (hmati[2] * U0[m] + hmati[5] * U1[m] + hmati[8] * U2[m]);
+    double fx = __dmul_rn(t, fma(hmati[6], U2[m], fma(hmati[3], U1[m], __dmul_rn(hmati[0], U0[m]))));
+    double fy = __dmul_rn(t, fma(hmati[7], U2[m], fma(hmati[4], U1[m], __dmul_rn(hmati[1], U0[m]))));
+    double fz = __dmul_rn(t, fma(hmati[8], U2[m], fma(hmati[5], U1[m], __dmul_rn(hmati[2], U0[m]))));
     if (part) {
       // one partial per row split, summed in a fixed order by k_kforce_sum
       const size_t o = ((size_t)blockIdx.y * nq + jq[m]) * 3;
@@ -466,8 +479,11 @@ int kspace_setup(Ctx *c) {
   std::vector<int4> rows;
   std::vector<int> k0, ka, kb, kc, k_sys, ktile_sys, ftile_sys;
   const bool mixed = c->mode == CM3D_NB_MIXED;
-  const int per_tile = mixed ? KS_THREADS * KS_A : KS_THREADS;
-  const int per_ftile = mixed ? KS_THREADS * KF_A : KS_THREADS;
+  bool small = mixed && c->nsys > 1;
+  for (int sy = 0; sy < c->nsys && small; sy++) small = c->hs[sy].ncharge <= KS_SMALL;
+  c->ks_small = small;
+  const int per_tile = small ? KS_SMALL : mixed ? KS_THREADS * KS_A : KS_THREADS;
+  const int per_ftile = small ? KS_SMALL : mixed ? KS_THREADS * KF_A : KS_THREADS;
   int qoff = 0, nrows_max = 0;
   long long spart_tot = 0;
   for (int sy = 0; sy < c->nsys; sy++) {
@@ -574,6 +590,7 @@ static void kforce_attr(int dev) {
   if (dev < 64 && (done & (1ull << dev))) return;
   cudaFuncSetAttribute(k_kforce_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_kforce_mixed<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_kforce_mixed<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (dev < 64) done |= 1ull << dev;
 }
 
@@ -584,21 +601,33 @@ static int kspace_forces_batch(Ctx *c) {
   tbegin(c, 1, &e0);
   k_kprep<true><<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, nullptr,
                                                                c->sp, c->sys_of, c->kfrac, nullptr, c->gate);
+  // enough row chunks per tile to fill the machine (one-warp blocks: 32
+  // blocks per SM)
+  const long long target = c->ks_small ? 148LL * 32 : 148LL * 4;
   int ych = 1;
-  while ((long long)c->ktiles_tot * ych < 148 * 4 && ych < c->nrows_max) ych *= 2;
+  while ((long long)c->ktiles_tot * ych < target && ych < c->nrows_max) ych *= 2;
   const int rpb = (c->nrows_max + ych - 1) / ych;
   dim3 gsf(c->ktiles_tot, (c->nrows_max + rpb - 1) / rpb);
-  k_sfac_mixed<true><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0, c->spart,
-                                                    c->sp, c->ktile_sys, c->gate);
+  if (c->ks_small)
+    k_sfac_mixed<true, 1><<<gsf, KS_SMALL, 0, c->st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0,
+                                                       c->spart, c->sp, c->ktile_sys, c->gate);
+  else
+    k_sfac_mixed<true><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0,
+                                                      c->spart, c->sp, c->ktile_sys, c->gate);
   k_sred<true><<<grid_for(c->ktot, 256), 256, 0, c->st>>>(c->ktot, 0, c->spart, c->ka_d, c->kb_d, c->kc_d, nullptr,
                                                            0.0, 0.0, c->sk, c->akf, nullptr, c->acc, c->sp,
                                                            c->k_sys, c->gate);
   kforce_attr(c->dev);
   dim3 gf(c->ftiles_tot, c->kf_split);
   double *part = c->kf_split > 1 ? c->kf_part : nullptr;
-  k_kforce_mixed<true><<<gf, KS_THREADS, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0, c->rows,
-                                                               c->row_k0, 0, c->akf, 0, nullptr, 0, c->fxl, part,
-                                                               c->sp, c->ftile_sys, c->gate);
+  if (c->ks_small)
+    k_kforce_mixed<true, 1><<<gf, KS_SMALL, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0,
+                                                                 c->rows, c->row_k0, 0, c->akf, 0, nullptr, 0,
+                                                                 c->fxl, part, c->sp, c->ftile_sys, c->gate);
+  else
+    k_kforce_mixed<true><<<gf, KS_THREADS, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0,
+                                                                 c->rows, c->row_k0, 0, c->akf, 0, nullptr, 0,
+                                                                 c->fxl, part, c->sp, c->ftile_sys, c->gate);
   c->launches += 4;
   if (part) {
     k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->kf_split, part, c->icharge, c->n,

@@ -32,6 +32,9 @@ GROUPS = {
     "dt5fs": ["argon864", "binary256"],
     "dt1fs": ["lj256", "lj2"],
     "water": ["water216", "water4096"],
+    # two copies of CM3D's abutane molecule: torsions, 1-4 pairs, cross bonds,
+    # frozen atoms, and a batch whose systems all take the one-warp k-space tiles
+    "tors": ["abutane", "abutane"],
 }
 ETOL, VTOL, FTOL = 1e-5, 5e-5, 1e-5
 VIRIAL_KEYS = {"winter", "welec", "W", "prsi"}
