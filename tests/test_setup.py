@@ -134,3 +134,31 @@ def test_workloads_are_seeded_and_sized():
     assert np.allclose((m[:, None] * a.vel).sum(0), 0, atol=1e-9)
     t = float((m[:, None] * a.vel ** 2).sum()) / (3 * a.natoms - 3)
     assert abs(t - 120.0) < 1e-9
+
+
+def test_system_description_carries_the_torsion_level():
+    """CM3D's abutane state (dumped by the reference) packed into the C ABI's
+    cm3d_nb_system: torsions, 1-4 pairs, cross bonds and frozen atoms with
+    the counts and table sizes CM3D reports, every array present"""
+    from cm3d_b200 import _abi
+    d = golden("abutane")
+    s = System.from_arrays(d)
+    desc = s.desc()
+    assert (desc.ntors, desc.n14, desc.nbondx, desc.nfreeze) == (27, 27, 3, 2)
+    assert desc.ntors_types == int(d["tors_ind_pot"].size)
+    # every torsion type of the deck is a cosine power series (form 1)
+    assert desc.ntors_harm == 0 and desc.ntors_series == int(d["vphi"].size) // _abi.MAXPOWER_TORS
+    assert desc.n14_types == int(d["n14types"][0]) and desc.n14table == int(d["n14table"][0])
+    assert desc.nbondx_types == int(d["eq1bondx"].size)
+    assert (desc.scale_onefour, desc.scale_onefour_e) == (float(d["scale_onefour"][0]),
+                                                         float(d["scale_onefour_e"][0]))
+    for name in ("itors", "jtors", "ktors", "ltors", "idxtors", "tors_ind_pot", "tors_ind_pot_num", "vphi",
+                 "i14", "j14", "i14dx", "r14min2", "r14max2", "dx214tab", "v14tab", "dv14tab", "ibondx",
+                 "jbondx", "kbondx", "idxbondx", "eq1bondx", "eq2bondx", "fkbondx", "ifreeze"):
+        assert bool(getattr(desc, name)), name
+    assert list(desc.ifreeze[:2]) == list(d["ifreeze"])
+    # a system without them (generated argon) leaves the fields empty
+    from cm3d_b200.setup import build_system
+    a = build_system(configs.argon_fcc(ncell=3, ntime=2)).desc()
+    assert (a.ntors, a.n14, a.nbondx, a.nfreeze) == (0, 0, 0, 0)
+    assert not bool(a.itors) and not bool(a.ifreeze)

@@ -162,3 +162,27 @@ def test_relinked_cm3d_without_a_device_fails_loudly(tmp_path):
     assert rc != 0
     assert "GPU nonbonded engine: cm3d_nb_create" in out
     assert "Begining Molecular Dynamics" not in out
+
+
+@needs_bins
+def test_relinked_cm3d_accepts_a_torsion_deck(tmp_path):
+    """CM3D's own test/abutane deck (torsions, 1-4 pairs, cross bonds, frozen
+    atoms) passes the shim's feature check and reaches the engine; without a
+    device it then stops at cm3d_nb_create, not with an "is not supported".
+    The deck is read from the reference tree, so this host-only test is
+    skipped where that tree is absent."""
+    import shutil
+    src = os.path.join(os.environ.get("CM3D_REF", "/root/reference"), "test", "abutane")
+    if not os.path.isdir(src):
+        pytest.skip("the reference tree's test/abutane deck is not on this machine")
+    work = tmp_path / "abutane"
+    shutil.copytree(src, work)
+    for root, _dirs, files in os.walk(work):
+        for f in files:
+            os.chmod(os.path.join(root, f), 0o644)
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    p = subprocess.run([GPU_CM3D, "abutane.input"], cwd=str(work), env=env, stdout=subprocess.PIPE,
+                       stderr=subprocess.STDOUT, text=True, timeout=300)
+    assert p.returncode != 0
+    assert "is not supported" not in p.stdout, p.stdout[-2000:]
+    assert "GPU nonbonded engine: cm3d_nb_create" in p.stdout, p.stdout[-2000:]
