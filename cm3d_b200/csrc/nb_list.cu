@@ -423,17 +423,48 @@ __global__ void __launch_bounds__(256) k_list_half(
 // (s_x) and their sorted indices (s_u, low ENT_JBITS bits), walked 32 at a
 // time with the same prefilter and in the same order as walk_candidates.  The
 // queue holds the staged index, and qr its FP32 squared distance.
+//
+// With `prune` (an orthorhombic cell grid of three or more cells per axis,
+// cells cw wide), the lanes first bound atom t's distance from each stencil
+// cell (the gaps to the cell's faces, each shortened by 1e-3 A) and the walk
+// skips the cells that lie wholly beyond lim2: none of their atoms would pass
+// the prefilter, and the others keep their order, so the lists are the same.
+// s_off holds the stencil cells' first staged index, s_code their shift code.
 template <class Decide>
 __device__ __forceinline__ void walk_staged(int t, float4 xi4, float lim2, const float4 *s_x, const int *s_u,
-                                            int cnt, int *qbuf, float *qr, Decide &decide) {
+                                            int cnt, int *qbuf, float *qr, Decide &decide, const int *s_off,
+                                            const int *s_code, int nw, bool prune, float3 cw) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
+  unsigned vis = nw >= 32 ? 0xffffffffu : (1u << nw) - 1u;
+  if (prune) {
+    bool v = false;
+    if (lane < nw) {
+      const int code = s_code[lane];
+      const int ox = 1 - code / 9, oy = 1 - (code / 3) % 3, oz = 1 - code % 3;
+      const float gx = fmaxf((ox > 0 ? cw.x - xi4.x : ox < 0 ? xi4.x : 0.f) - 1e-3f, 0.f);
+      const float gy = fmaxf((oy > 0 ? cw.y - xi4.y : oy < 0 ? xi4.y : 0.f) - 1e-3f, 0.f);
+      const float gz = fmaxf((oz > 0 ? cw.z - xi4.z : oz < 0 ? xi4.z : 0.f) - 1e-3f, 0.f);
+      v = gx * gx + gy * gy + gz * gz < lim2;
+    }
+    vis = __ballot_sync(0xffffffffu, v);
+  }
   int head = 0, tail = 0;
-  for (int k0 = 0; k0 < cnt; k0 += 32) {
+  for (int w = 0; w < nw;) {
+    if (!((vis >> w) & 1u)) {
+      w++;
+      continue;
+    }
+    // a run of visited stencil cells is one contiguous span of staged atoms
+    int e = w;
+    while (e + 1 < nw && ((vis >> (e + 1)) & 1u)) e++;
+    const int a = s_off[w], b = e + 1 < nw ? s_off[e + 1] : cnt;
+    w = e + 1;
+  for (int k0 = a; k0 < b; k0 += 32) {
     const int k = k0 + lane;
     bool keep = false;
     float r2f = 0.f;
-    if (k < cnt) {
+    if (k < b) {
       const float4 xs = s_x[k];
       const int u = s_u[k] & (int)ENT_JMASK;
       const float dx = xi4.x - xs.x, dy = xi4.y - xs.y, dz = xi4.z - xs.z;
@@ -453,6 +484,7 @@ __device__ __forceinline__ void walk_staged(int t, float4 xi4, float lim2, const
       head += 32;
       __syncwarp();
     }
+  }
   }
   while (tail > head) {
     const int m = tail - head < 32 ? tail - head : 32;
@@ -517,7 +549,8 @@ __device__ __forceinline__ void full_list_atom(
     const int *__restrict__ cexcl_off, const int *__restrict__ cexcl_idx, const int4 *__restrict__ cimg,
     uint32_t *__restrict__ nbr, int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt,
     int *qbuf, float *qr, const float4 *s_x, const int *s_u, const int *s_j, int scnt,
-    bool fast) {
+    bool fast, const int *s_off = nullptr, const int *s_code = nullptr, int nw = 0, bool prune = false,
+    float3 cw = make_float3(0.f, 0.f, 0.f)) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int i = cell_atoms[t];
@@ -578,7 +611,7 @@ __device__ __forceinline__ void full_list_atom(
     na += __popc(ba);
     nb += __popc(bb);
   };
-  if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide);
+  if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide, s_off, s_code, nw, prune, cw);
   else walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide);
   const int count = na + nb;
   if (lane == 0) {
@@ -769,11 +802,13 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
     __syncthreads();
     const int lo = cell_start[c], hi = cell_start[c + 1];
     const bool fast = P.nc[0] >= 3 && P.nc[1] >= 3 && P.nc[2] >= 3 && !P.smallbox;
+    const bool ortho = P.h[1] == 0. && P.h[2] == 0. && P.h[3] == 0. && P.h[5] == 0. && P.h[6] == 0. && P.h[7] == 0.;
+    const float3 cw = make_float3(P.hF[0] / (float)P.nc[0], P.hF[4] / (float)P.nc[1], P.hF[8] / (float)P.nc[2]);
     for (int t = lo + warp; t < hi; t += LW_THREADS / 32) {
       if (staged)
         full_list_atom<true>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                              excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], qrs[warp], s_x,
-                             s_u, s_j, tot, fast);
+                             s_u, s_j, tot, fast, s_off, s_code, nw, fast && ortho && nw == 27, cw);
       else
         full_list_atom<false>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                               excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], nullptr,
