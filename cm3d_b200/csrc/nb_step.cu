@@ -734,6 +734,20 @@ static int collect_intra(Ctx *c, const cm3d_nb_system *systems, int nsys, IntraH
     const cm3d_nb_system *s = systems + sy;
     const int a0 = c->h_sp[sy].a0, ns = s->natoms;
     auto atom_ok = [&](int i) { return i >= 0 && i < ns; };
+    // every array a nonzero count refers to must be there
+    const bool missing =
+        (s->nbondx > 0 && (!s->ibondx || !s->jbondx || !s->kbondx || !s->idxbondx || !s->eq1bondx ||
+                           !s->eq2bondx || !s->fkbondx)) ||
+        (s->ntors > 0 && (!s->itors || !s->jtors || !s->ktors || !s->ltors || !s->idxtors || !s->tors_ind_pot ||
+                          !s->tors_ind_pot_num || (s->ntors_harm > 0 && (!s->eqtors || !s->fktors)) ||
+                          (s->ntors_series > 0 && !s->vphi))) ||
+        (s->n14 > 0 && (!s->i14 || !s->j14 || !s->i14dx || !s->r14min2 || !s->r14max2 || !s->dx214tab ||
+                        !s->v14tab || !s->dv14tab)) ||
+        (s->nfreeze > 0 && !s->ifreeze);
+    if (missing) {
+      set_error("system %d: a cross-bond, torsion, 1-4 or frozen-atom array is NULL while its count is not 0", sy);
+      return CM3D_NB_ERR_ARG;
+    }
     for (int b = 0; b < s->nbondx; b++) {
       const int t = s->idxbondx[b];
       if (t < 0 || t >= s->nbondx_types || !atom_ok(s->ibondx[b]) || !atom_ok(s->jbondx[b]) ||
