@@ -60,6 +60,8 @@ class SystemDesc(C.Structure):
         ("ibondx", _ip), ("jbondx", _ip), ("kbondx", _ip), ("idxbondx", _ip),
         ("eq1bondx", _dp), ("eq2bondx", _dp), ("fkbondx", _dp),
         ("nfreeze", C.c_int), ("ifreeze", _ip),
+        ("iensemble", C.c_int), ("ntherm", C.c_int), ("nchain", C.c_int), ("ithm", _ip),
+        ("mnh", _dp), ("gkt", _dp), ("nhc_eta", _dp), ("nhc_veta", _dp),
     ]
 
 

@@ -140,6 +140,12 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
       set_error("cm3d_nb_create: system %d: ntable = %d is too small", sy, s->ntable);
       return CM3D_NB_ERR_ARG;
     }
+    if (s->iensemble != 0 || s->ntherm > 0) {
+      set_error("cm3d_nb_create: system %d: thermostats and barostats (iensemble %d, %d thermostats) are not "
+                "supported: the engine integrates NVE",
+                sy, s->iensemble, s->ntherm);
+      return CM3D_NB_ERR_ARG;
+    }
     const cm3d_nb_system *s0 = systems;
     if (s->ntable != s0->ntable || s->dt != s0->dt || s->nres_lrf != s0->nres_lrf ||
         s->nres_intra != s0->nres_intra || s->nres_tors != s0->nres_tors) {

@@ -281,6 +281,9 @@ def build_system(wl: Workload) -> System:
     sysm["n14"] = 0
     sysm["nbondx"] = 0
     sysm["nfreeze"] = 0
+    sysm["iensemble"] = 0            # NVE: no thermostat chains
+    sysm["ntherm"] = 0
+    sysm["nchain"] = 0
     sysm["ncells"] = int(kw["ncell_div"])
     sysm["nocell_all"] = 1
     sysm["nlen"] = int(kw["nlen"])

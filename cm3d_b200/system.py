@@ -24,12 +24,12 @@ _F64 = ("hmat", "px", "py", "pz", "vx", "vy", "vz", "amass", "qch", "vtab", "dvt
         "switchs", "rmaxs_cut2", "rmins_cut2", "rmaxl_cut2", "rminl_cut2",
         "rmaxs_skin2", "rmaxl_skin2", "dx2tab", "coultab", "dcoultab", "switchse",
         "eqbond", "fkbond", "eqbend", "fkbend", "eqtors", "fktors", "vphi", "r14min2",
-        "r14max2", "dx214tab", "v14tab", "dv14tab", "eq1bondx", "eq2bondx", "fkbondx")
+        "r14max2", "dx214tab", "v14tab", "dv14tab", "eq1bondx", "eq2bondx", "fkbondx", "mnh", "gkt", "nhc_eta", "nhc_veta")
 _I32 = ("itype", "map", "excl_off", "excl_idx", "cexcl_off", "cexcl_idx", "ka", "kb",
         "kc", "iecorr", "jecorr", "ibond", "jbond", "idxbond", "itypbond", "ibend",
         "jbend", "kbend", "idxbend", "itypbend", "itors", "jtors", "ktors", "ltors",
         "idxtors", "tors_ind_pot", "tors_ind_pot_num", "i14", "j14", "i14dx", "ibondx",
-        "jbondx", "kbondx", "idxbondx", "ifreeze")
+        "jbondx", "kbondx", "idxbondx", "ifreeze", "ithm")
 _SCALARS_F = ("dt", "vlrc", "wlrc", "skin", "rheal", "dx2coul", "rmins_coul2",
               "rmaxs_coul2", "rminl_coul2", "rmaxl_coul2", "rmaxs_skin2_e",
               "rmaxl_skin2_e", "kappa", "falp2", "ewald_self", "ewald_bkg", "temp",
@@ -37,7 +37,7 @@ _SCALARS_F = ("dt", "vlrc", "wlrc", "skin", "rheal", "dx2coul", "rmins_coul2",
 _SCALARS_I = ("natoms", "iperd", "nres_lrf", "nres_intra", "nres_tors", "ndof",
               "ntypes", "ninter", "ntable", "ktot", "necorr", "nbonds", "nbends",
               "ntors", "n14", "nbondx", "ncells", "nocell_all", "nlen", "n14table", "n14types",
-              "nfreeze")
+              "nfreeze", "iensemble", "ntherm", "nchain")
 
 
 class System:
@@ -133,13 +133,14 @@ class System:
                   "rmaxs_skin2", "rmaxl_skin2", "dx2tab", "coultab", "dcoultab",
                   "switchse", "eqbond", "fkbond", "eqbend", "fkbend", "eqtors", "fktors",
                   "vphi", "r14min2", "r14max2", "dx214tab", "v14tab", "dv14tab", "eq1bondx",
-                  "eq2bondx", "fkbondx"):
+                  "eq2bondx", "fkbondx", "mnh", "gkt", "nhc_eta", "nhc_veta"):
             setattr(d, k, self._ptr(k, C.c_double))
         for k in ("itype", "map", "excl_off", "excl_idx", "cexcl_off", "cexcl_idx",
                   "ka", "kb", "kc", "iecorr", "jecorr", "ibond", "jbond", "idxbond",
                   "itypbond", "ibend", "jbend", "kbend", "idxbend", "itypbend", "itors",
                   "jtors", "ktors", "ltors", "idxtors", "tors_ind_pot", "tors_ind_pot_num",
-                  "i14", "j14", "i14dx", "ibondx", "jbondx", "kbondx", "idxbondx", "ifreeze"):
+                  "i14", "j14", "i14dx", "ibondx", "jbondx", "kbondx", "idxbondx", "ifreeze",
+                  "ithm"):
             setattr(d, k, self._ptr(k, C.c_int))
         d.ntypes = s["ntypes"]
         d.ninter = s["ninter"]
@@ -169,5 +170,8 @@ class System:
         d.scale_onefour_e = s.get("scale_onefour_e", 1.0)
         d.nbondx_types = int(a["eq1bondx"].size) if "eq1bondx" in a else 0
         d.nfreeze = s.get("nfreeze", 0)
+        d.iensemble = s.get("iensemble", 0)
+        d.ntherm = s.get("ntherm", 0)
+        d.nchain = s.get("nchain", 0)
         self._desc = d
         return d

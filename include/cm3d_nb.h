@@ -145,6 +145,13 @@ typedef struct cm3d_nb_system {
      md_fcntr.c:311-329) */
   int nfreeze;
   const int *ifreeze;
+  /* SIMPARMS.iensemble / ntherm / nchain and COORDS' Nose-Hoover chain state
+     (md_typedef.h:122-125, 203-224; set_therm_new md_therm.new.c:32).  The
+     engine integrates NVE: cm3d_nb_create refuses iensemble != 0 or
+     ntherm > 0.  The fields describe a thermostatted run to the CPU checker. */
+  int iensemble, ntherm, nchain;
+  const int *ithm;                            /* [natoms] thermostat of each atom (-1: none) */
+  const double *mnh, *gkt, *nhc_eta, *nhc_veta;   /* [ntherm * nchain] */
 } cm3d_nb_system;
 
 typedef struct cm3d_nb_options {

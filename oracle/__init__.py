@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
         L.orc_get_energies.restype = None
         L.orc_step.argtypes = [vp, C.c_int, C.c_int]
         L.orc_step.restype = None
+        L.orc_get_nhc.argtypes = [vp, dp, dp]
+        L.orc_get_nhc.restype = None
         for name in ("orc_rebuilds", "orc_resets", "orc_underflows"):
             getattr(L, name).argtypes = [vp]
             getattr(L, name).restype = C.c_longlong
@@ -142,6 +144,13 @@ class Oracle:
 
     def fbond(self):
         lib().orc_fbond(self._h)
+
+    def nhc_state(self):
+        """the Nose-Hoover chains' (eta, veta), each ntherm x nchain"""
+        nt, nc = int(self.sys.get("ntherm", 0)), int(self.sys.get("nchain", 0))
+        eta, veta = np.zeros(max(nt * nc, 1)), np.zeros(max(nt * nc, 1))
+        lib().orc_get_nhc(self._h, _p(eta), _p(veta))
+        return eta[:nt * nc].reshape(nt, nc), veta[:nt * nc].reshape(nt, nc)
 
     def fbondx(self):
         lib().orc_fbondx(self._h)

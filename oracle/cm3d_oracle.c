@@ -67,6 +67,10 @@ struct orc {
   double *eq1bondx, *eq2bondx, *fkbondx;
   double *fxr;
   int nfreeze, *ifreeze;
+  /* Nose-Hoover chains (SIMPARMS.ntherm / nchain, COORDS.ithm, mnh, gkt,
+     eta, veta, feta, p2mt) */
+  int ntherm, nchain, *ithm;
+  double *mnh, *gkt, *eta, *veta, *feta, *p2mt;
   double vtors, wtors, wtorst[9], vonfo, vonfo_e, wonfo, wonfo_e, wonfot[9], wonfoet[9], wbondxt[9];
 };
 
@@ -267,6 +271,18 @@ orc *orc_create(const cm3d_nb_system *s, int ncells, int nocell_all, int nlen)
   o->fxr = (double *)calloc(3 * (size_t)n + 1, 8);
   o->nfreeze = s->nfreeze;
   o->ifreeze = (int *)dup(s->ifreeze, s->nfreeze * 4.);
+  o->ntherm = s->ntherm;
+  o->nchain = s->nchain;
+  if (s->ntherm > 0) {
+    size_t tc = (size_t)s->ntherm * s->nchain;
+    o->ithm = (int *)dup(s->ithm, n * 4.);
+    o->mnh = (double *)dup(s->mnh, tc * 8.);
+    o->gkt = (double *)dup(s->gkt, tc * 8.);
+    o->eta = (double *)dup(s->nhc_eta, tc * 8.);
+    o->veta = (double *)dup(s->nhc_veta, tc * 8.);
+    o->feta = (double *)calloc(tc, 8);
+    o->p2mt = (double *)calloc((size_t)s->ntherm, 8);
+  }
   o->fxl = (double *)calloc(3 * (size_t)n + 1, 8);
   o->fxs = (double *)calloc(3 * (size_t)n + 1, 8);
   o->fxa = (double *)calloc(3 * (size_t)n + 1, 8);
@@ -294,7 +310,8 @@ void orc_destroy(orc *o)
                   o->ktors, o->ltors, o->idxtors, o->tors_form, o->tors_row, o->eqtors,
                   o->fktors, o->vphi, o->i14, o->j14, o->i14dx, o->r14min2, o->r14max2,
                   o->dx214tab, o->v14tab, o->dv14tab, o->ibondx, o->jbondx, o->kbondx,
-                  o->idxbondx, o->eq1bondx, o->eq2bondx, o->fkbondx, o->fxr, o->ifreeze};
+                  o->idxbondx, o->eq1bondx, o->eq2bondx, o->fkbondx, o->fxr, o->ifreeze,
+                  o->ithm, o->mnh, o->gkt, o->eta, o->veta, o->feta, o->p2mt};
   size_t i;
   for (i = 0; i < sizeof ptrs / sizeof ptrs[0]; i++) free(ptrs[i]);
   free(o);
@@ -1418,6 +1435,72 @@ void orc_get_energies(orc *o, cm3d_nb_energies *e)
   e->tiout = p2m / (double)o->ndof;
 }
 
+/* Nose-Hoover chains.  forcen_new (integrate/md_therm.new.c:175-198): the
+   thermostats' kinetic sums and the chain forces.  An atom without a
+   thermostat (ithm -1) adds to no sum here; CM3D would write p2mt[-1]. */
+static void nhc_forces(orc *o)
+{
+  int i, j, n = o->n, nc = o->nchain;
+  for (j = 0; j < o->ntherm; j++) o->p2mt[j] = 0.;
+  for (i = 0; i < n; i++)
+    if (o->ithm[i] >= 0)
+      o->p2mt[o->ithm[i]] += o->amass[i] * (o->vx[i] * o->vx[i] + o->vy[i] * o->vy[i] + o->vz[i] * o->vz[i]);
+  for (j = 0; j < o->ntherm; j++) {
+    double *f = o->feta + (size_t)j * nc, *m = o->mnh + (size_t)j * nc, *g = o->gkt + (size_t)j * nc,
+           *v = o->veta + (size_t)j * nc;
+    f[0] = (o->p2mt[j] - g[0]) / m[0];
+    for (i = 1; i < nc; i++) f[i] = (m[i - 1] * v[i - 1] * v[i - 1] - g[i]) / m[i];
+  }
+}
+
+/* the atoms' velocity scaling by exp(-dt/2 veta_0) of their thermostat */
+static void nhc_scale(orc *o, double dta2)
+{
+  int i, n = o->n;
+  for (i = 0; i < n; i++) {
+    double e = o->ithm[i] >= 0 ? exp(-dta2 * o->veta[(size_t)o->ithm[i] * o->nchain]) : exp(-dta2 * 0.);
+    o->vx[i] *= e;
+    o->vy[i] *= e;
+    o->vz[i] *= e;
+  }
+}
+
+/* intnhc_new  integrate/md_therm.new.c:278-333: one thermostat half step of
+   dta2 in CM3D's order (scale, chain links from the top, forces, chain
+   velocities and positions, links from the bottom, scale) */
+static void intnhc(orc *o, double dta2)
+{
+  int i, j, nc = o->nchain, nt = o->ntherm;
+  double dta = 2. * dta2;
+  double *v = o->veta, *f = o->feta, *m = o->mnh, *g = o->gkt;
+  nhc_scale(o, dta2);
+  for (i = 0; i < nc - 1; i++)
+    for (j = 0; j < nt; j++) v[(size_t)j * nc + i] *= exp(-dta2 * v[(size_t)j * nc + i + 1]);
+  nhc_forces(o);
+  for (i = 0; i < nc; i++)
+    for (j = 0; j < nt; j++) v[(size_t)j * nc + i] += dta2 * f[(size_t)j * nc + i];
+  for (i = 0; i < nc; i++)
+    for (j = 0; j < nt; j++) o->eta[(size_t)j * nc + i] += dta * v[(size_t)j * nc + i];
+  for (j = 0; j < nt; j++) v[(size_t)j * nc] += dta2 * f[(size_t)j * nc];
+  for (i = 1; i < nc; i++)
+    for (j = 0; j < nt; j++) {
+      size_t k = (size_t)j * nc + i;
+      v[k] += dta2 * (m[k - 1] * v[k - 1] * v[k - 1] - g[k]) / m[k];
+    }
+  for (i = nc - 2; i >= 0; i--)
+    for (j = 0; j < nt; j++) v[(size_t)j * nc + i] *= exp(-dta2 * v[(size_t)j * nc + i + 1]);
+  nhc_scale(o, dta2);
+}
+
+void orc_get_nhc(orc *o, double *eta, double *veta)
+{
+  size_t tc = (size_t)o->ntherm * o->nchain;
+  if (tc) {
+    memcpy(eta, o->eta, tc * 8);
+    memcpy(veta, o->veta, tc * 8);
+  }
+}
+
 /* nrefsh  energy/control/md_finter.c:43-108 (verlist branch) */
 static void nrefsh(orc *o, int istep)
 {
@@ -1458,7 +1541,7 @@ void orc_step_init(orc *o)
   orc_force(o, 3);
 }
 
-/* step  integrate/md_step.c:62-159 (NVE) */
+/* step  integrate/md_step.c:62-159 (NVE, or NVT with Nose-Hoover chains) */
 void orc_step(orc *o, int istep0, int nsteps)
 {
   int s, n3 = 3 * o->n, i;
@@ -1490,6 +1573,7 @@ void orc_step(orc *o, int istep0, int nsteps)
             for (i = 0; i < n; i++) V[c][i] += dta2 * o->fxa[c * n + i];
           for (c = 0; c < 3; c++)
             for (i = 0; i < n; i++) P[c][i] += dta2 * V[c][i];
+          if (o->ntherm) intnhc(o, dta2);    /* md_step.c:117 (no barostat) */
           for (c = 0; c < 3; c++)
             for (i = 0; i < n; i++) P[c][i] += dta2 * V[c][i];
           orc_force(o, 2);

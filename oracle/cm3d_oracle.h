@@ -54,6 +54,8 @@ void orc_rmass(orc *o, int which);
 void orc_get_energies(orc *o, cm3d_nb_energies *e);
 void orc_step_init(orc *o);
 void orc_step(orc *o, int istep0, int nsteps);
+/* the Nose-Hoover chain state (ntherm x nchain each) */
+void orc_get_nhc(orc *o, double *eta, double *veta);
 long long orc_rebuilds(orc *o);
 long long orc_resets(orc *o);
 long long orc_underflows(orc *o);

@@ -263,6 +263,29 @@ int main(int argc, char *argv[])
     recd("eqbend", coords.bends.itypes, coords.bends.eqbend);
     recd("fkbend", coords.bends.itypes, coords.bends.fkbend);
   }
+  /* Nose-Hoover chain thermostats (set_therm_new md_therm.new.c:32, state
+     after samveta): per thermostat and chain link the masses mnh, targets
+     gkt, positions eta and velocities veta; ithm maps atoms to thermostats */
+  rec1i("iensemble", simparms.iensemble);
+  rec1i("ntherm", simparms.ntherm);
+  rec1i("nchain", simparms.nchain);
+  if (simparms.ntherm > 0) {
+    int t;
+    double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)simparms.ntherm * simparms.nchain);
+    reci("ithm", n, coords.ithm);
+    for (t = 0; t < simparms.ntherm; t++) {
+      size_t o = (size_t)t * simparms.nchain, tot = (size_t)simparms.ntherm * simparms.nchain;
+      memcpy(buf + o, coords.mnh[t], sizeof(double) * simparms.nchain);
+      memcpy(buf + tot + o, coords.gkt[t], sizeof(double) * simparms.nchain);
+      memcpy(buf + 2 * tot + o, coords.eta[t], sizeof(double) * simparms.nchain);
+      memcpy(buf + 3 * tot + o, coords.veta[t], sizeof(double) * simparms.nchain);
+    }
+    recd("mnh", (long long)simparms.ntherm * simparms.nchain, buf);
+    recd("gkt", (long long)simparms.ntherm * simparms.nchain, buf + (size_t)simparms.ntherm * simparms.nchain);
+    recd("nhc_eta", (long long)simparms.ntherm * simparms.nchain, buf + 2 * (size_t)simparms.ntherm * simparms.nchain);
+    recd("nhc_veta", (long long)simparms.ntherm * simparms.nchain, buf + 3 * (size_t)simparms.ntherm * simparms.nchain);
+    free(buf);
+  }
   /* frozen atoms (freeze_atom md_fcntr.c:311, applied at the end of every force level) */
   rec1i("nfreeze", simparms.nfreeze);
   if (simparms.nfreeze > 0) reci("ifreeze", simparms.nfreeze, coords.ifreeze);
@@ -467,6 +490,17 @@ int main(int argc, char *argv[])
     recd("final_vx", n, coords.vx); recd("final_vy", n, coords.vy);
     recd("final_vz", n, coords.vz);
     rec_force("final_acc_l", n, coords.fxl, coords.fyl, coords.fzl, coords.amass, 0);
+    if (simparms.ntherm > 0) {
+      int t;
+      double *buf = (double *)malloc(sizeof(double) * 2 * (size_t)simparms.ntherm * simparms.nchain);
+      for (t = 0; t < simparms.ntherm; t++) {
+        memcpy(buf + (size_t)t * simparms.nchain, coords.eta[t], sizeof(double) * simparms.nchain);
+        memcpy(buf + (size_t)(simparms.ntherm + t) * simparms.nchain, coords.veta[t], sizeof(double) * simparms.nchain);
+      }
+      recd("final_nhc_eta", (long long)simparms.ntherm * simparms.nchain, buf);
+      recd("final_nhc_veta", (long long)simparms.ntherm * simparms.nchain, buf + (size_t)simparms.ntherm * simparms.nchain);
+      free(buf);
+    }
     dump_energies("ef_", &energies);
   }
   fwrite("ENDDUMP!", 1, 8, g_out);

@@ -6,7 +6,7 @@ Run here (the reference tree must be present; the GPU box never runs this):
     python tests/golden/make_golden.py
 
 For every case it writes a CM3D input deck (the reference's own test decks for
-test/lj and test/abutane, copied from the reference tree into a scratch
+test/lj -- NVE and NVT -- and test/abutane, copied from the reference tree into a scratch
 directory; generated decks for the synthetic workloads), runs
 oracle/_ref/ref_dump (CM3D's startup + step_init + step, dumped at full
 precision) and stores the result as <case>.npz.  Pair lists of the larger
@@ -101,6 +101,7 @@ def main() -> None:
         copy_ref_test("lj", d)
         run_case("lj256", d, "lj.input_ljnve", 20, True, True)
         run_case("lj2", d, "lj.input_ljnve.2", 10, True, True)
+        run_case("lj256nvt", d, "lj.input_ljnvt", 20, True, True)
         d = os.path.join(tmp, "abutane")
         copy_ref_test("abutane", d)
         run_case("abutane", d, "abutane.input", 20, True, True)

@@ -128,3 +128,24 @@ def test_lj_regression_known_answers():
     assert len(o.pair_list(0)[0]) == 7851
     assert len(o.pair_list(1)[0]) == 2334
     assert round(o.energies()["vinter"], 6) == -1232.123279
+
+
+def test_nvt_trajectory_bit_exact():
+    """CM3D's test/lj NVT deck (lj.input_ljnvt: one global Nose-Hoover chain
+    of length 3, md_therm.new.c:278): the oracle's step with intnhc in the
+    inner loop follows CM3D's per-step energies, final positions and
+    velocities and the final chain state bit for bit"""
+    d, o = make("lj256nvt")
+    assert int(d["ntherm"][0]) == 1 and int(d["nchain"][0]) == 3
+    o.step_init()
+    eng = d["traj_eng"].reshape(-1, 8)
+    for k in range(int(d["nsteps"][0])):
+        o.step(1 + k, 1)
+        e = o.energies()
+        got = [e["poter"], e["potra"], e["zke"], e["vinter"], e["velec"], e["vewald"], e["prsi"]]
+        assert got == list(eng[k, :7]), f"step {k + 1}"
+    assert np.array_equal(o.positions(), np.stack([d["final_px"], d["final_py"], d["final_pz"]]))
+    assert np.array_equal(o.velocities(), np.stack([d["final_vx"], d["final_vy"], d["final_vz"]]))
+    eta, veta = o.nhc_state()
+    assert np.array_equal(eta.ravel(), d["final_nhc_eta"])
+    assert np.array_equal(veta.ravel(), d["final_nhc_veta"])

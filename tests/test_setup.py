@@ -162,3 +162,14 @@ def test_system_description_carries_the_torsion_level():
     a = build_system(configs.argon_fcc(ncell=3, ntime=2)).desc()
     assert (a.ntors, a.n14, a.nbondx, a.nfreeze) == (0, 0, 0, 0)
     assert not bool(a.itors) and not bool(a.ifreeze)
+
+
+def test_engine_refuses_thermostats_on_the_host(engine_lib):
+    """the engine integrates NVE: a thermostatted system (CM3D's NVT deck) is
+    refused by cm3d_nb_create before any device work, with the reason"""
+    from cm3d_b200 import _abi
+    from cm3d_b200.engine import Engine, EngineError
+    s = System.from_arrays(golden("lj256nvt"))
+    assert s.desc().ntherm == 1 and s.desc().iensemble == 1
+    with pytest.raises(EngineError, match="thermostats and barostats"):
+        Engine(s, mode=_abi.MIXED)
