@@ -87,7 +87,7 @@ static void destroy(Ctx *c) {
                   c->cimg, c->nlen, c->acc,
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
                   c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan,
-                  c->fxr, c->intra_buf};
+                  c->fxr, c->intra_buf, c->ithm, c->nhc};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -140,10 +140,19 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
       set_error("cm3d_nb_create: system %d: ntable = %d is too small", sy, s->ntable);
       return CM3D_NB_ERR_ARG;
     }
-    if (s->iensemble != 0 || s->ntherm > 0) {
-      set_error("cm3d_nb_create: system %d: thermostats and barostats (iensemble %d, %d thermostats) are not "
-                "supported: the engine integrates NVE",
+    // NVE, or NVT with Nose-Hoover chains (the same chain length in every
+    // system of a batch); barostats (NPT) are not supported
+    const bool nvt = s->iensemble == 1 && s->ntherm > 0 && s->nchain > 0 && s->ithm && s->mnh && s->gkt &&
+                     s->nhc_eta && s->nhc_veta;
+    if (!(s->iensemble == 0 && s->ntherm == 0) && !nvt) {
+      set_error("cm3d_nb_create: system %d: ensemble %d with %d thermostats is not supported: the engine "
+                "integrates NVE or NVT with Nose-Hoover chains, without barostats",
                 sy, s->iensemble, s->ntherm);
+      return CM3D_NB_ERR_ARG;
+    }
+    if (s->iensemble != systems[0].iensemble || (nvt && s->nchain != systems[0].nchain)) {
+      set_error("cm3d_nb_create_batch: system %d: every system of a batch needs the same ensemble and chain length",
+                sy);
       return CM3D_NB_ERR_ARG;
     }
     const cm3d_nb_system *s0 = systems;

@@ -302,6 +302,10 @@ struct Ctx {
   bool has_tors_level = false;          // any torsion or 1-4 pair
   bool has_intra_x = false;             // any cross bond, torsion or 1-4 pair
   double *intra_buf = nullptr;          // one allocation behind the IntraDev arrays
+  // Nose-Hoover chains (NVT): thermostats numbered across the batch's systems
+  int ntherm = 0, nchain = 0;
+  int *ithm = nullptr;                  // per atom: its thermostat, -1 none
+  double *nhc = nullptr;                // mnh | gkt | eta | veta | feta, ntherm * nchain each, then p2m (ntherm)
   // ---- cell grid and lists
   int nc[3] = {1, 1, 1}, ncells = 1;
   int *cell_of = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *cell_atoms = nullptr;

@@ -36,6 +36,7 @@ struct StepP {
   double skin2q;      // (skin/2)^2 = .25 skin^2  (md_finter.c:63)
   double kappa, kappa2;
   int use_fxs;
+  int nchain;         // Nose-Hoover chain length (NVT), 0 for NVE
 };
 
 // bonded forces of one group into fxa (raw forces), fbond/fbend in CM3D's order
@@ -385,6 +386,151 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
   }
 }
 
+// ---- NVT: the inner level with Nose-Hoover chains (intnhc_new,
+// integrate/md_therm.new.c:278-333, called between the two half drifts of
+// every inner substep, md_step.c:117).  The chain update needs every
+// thermostat's kinetic sum, a reduction over all groups, so each inner
+// substep runs as three launches: k_nvt_a (kicks, first half drift, the
+// first velocity scaling, kinetic partial sums), k_nvt_chain (one thread per
+// thermostat) and k_nvt_c (second scaling, second half drift, bonded
+// forces, kicks and, at the level's end, the displacement test).
+
+__device__ __forceinline__ double nhc_factor(int thm, int nchain, double dta2, const double *__restrict__ veta) {
+  return exp(-dta2 * (thm >= 0 ? veta[(size_t)thm * nchain] : 0.));
+}
+
+__global__ void k_nvt_a(StepP P, int intr, int level_start, int tors_start, const int *__restrict__ gaoff,
+                        const int *__restrict__ gatoms, double *__restrict__ pos, double *__restrict__ vel,
+                        const double *__restrict__ mass, const double *__restrict__ fxl,
+                        const double *__restrict__ fxs, const double *__restrict__ fxa,
+                        const double *__restrict__ fxr, const int *__restrict__ ithm,
+                        const double *__restrict__ veta, double *__restrict__ p2m, IntraDev X,
+                        int *__restrict__ istate, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g == 0 && level_start) istate[IS_INTR] = intr;
+  if (g >= P.ngroups) return;
+  const int n = P.n;
+  const bool tors = X.tor_off && (X.tor_off[g + 1] > X.tor_off[g] || X.o14_off[g + 1] > X.o14_off[g]);
+  for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
+    const int i = gatoms[a];
+    for (int d = 0; d < 3; d++) {
+      const int x = d * n + i;
+      if (level_start) {
+        if (intr == 0) vel[x] += P.dter * fxl[x] + (P.use_fxs ? P.dter1 * fxs[x] : 0.0);
+        else vel[x] += P.dts2 * fxs[x];
+      }
+      if (tors_start && tors) vel[x] += P.dtr2 * fxr[x];
+      vel[x] += P.dta2 * fxa[x];
+      pos[x] += P.dta2 * vel[x];
+    }
+    const int thm = ithm[i];
+    const double e = nhc_factor(thm, P.nchain, P.dta2, veta);
+    vel[i] *= e;
+    vel[n + i] *= e;
+    vel[2 * n + i] *= e;
+    if (thm >= 0)
+      atomicAdd(p2m + thm, mass[i] * (vel[i] * vel[i] + vel[n + i] * vel[n + i] + vel[2 * n + i] * vel[2 * n + i]));
+  }
+}
+
+// the chain half step of one thermostat, in intnhc_new's order: links from
+// the top, forces (forcen_new, md_therm.new.c:175-198), velocities and
+// positions, the recurrence, links from the bottom
+__global__ void k_nvt_chain(int ntherm, int nchain, double dta2, double *__restrict__ nhc,
+                            const double *__restrict__ p2m, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntherm) return;
+  const size_t tc = (size_t)ntherm * nchain, o = (size_t)j * nchain;
+  const double *m = nhc + o, *gk = nhc + tc + o;
+  double *eta = nhc + 2 * tc + o, *v = nhc + 3 * tc + o, *f = nhc + 4 * tc + o;
+  const double dta = 2. * dta2;
+  for (int i = 0; i < nchain - 1; i++) v[i] *= exp(-dta2 * v[i + 1]);
+  f[0] = (p2m[j] - gk[0]) / m[0];
+  for (int i = 1; i < nchain; i++) f[i] = (m[i - 1] * v[i - 1] * v[i - 1] - gk[i]) / m[i];
+  for (int i = 0; i < nchain; i++) v[i] += dta2 * f[i];
+  for (int i = 0; i < nchain; i++) eta[i] += dta * v[i];
+  v[0] += dta2 * f[0];
+  for (int i = 1; i < nchain; i++) v[i] += dta2 * (m[i - 1] * v[i - 1] * v[i - 1] - gk[i]) / m[i];
+  for (int i = nchain - 2; i >= 0; i--) v[i] *= exp(-dta2 * v[i + 1]);
+}
+
+__global__ void k_nvt_c(StepP P, int tors_end, int level_end, const int *__restrict__ gaoff,
+                        const int *__restrict__ gatoms, double *__restrict__ pos, double *__restrict__ vel,
+                        const double *__restrict__ mass, const double *__restrict__ q, double *__restrict__ fxa,
+                        double *__restrict__ fxr, const double *__restrict__ dxn, const int *__restrict__ gboff,
+                        const int4 *__restrict__ bij, const double2 *__restrict__ bp,
+                        const int *__restrict__ geoff, const int4 *__restrict__ eijk,
+                        const double2 *__restrict__ ep, const int *__restrict__ ithm,
+                        const double *__restrict__ veta, const SysP *__restrict__ sp,
+                        const int *__restrict__ sys_of, int *__restrict__ sreb, int *__restrict__ istate,
+                        IntraDev X, long long *__restrict__ stat, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.ngroups) return;
+  const int n = P.n;
+  const int a0 = gaoff[g], a1 = gaoff[g + 1];
+  const bool has_bx = X.bx_off && X.bx_off[g + 1] > X.bx_off[g];
+  const bool bonded = gboff[g + 1] > gboff[g] || geoff[g + 1] > geoff[g] || has_bx;
+  const bool tors = X.tor_off && (X.tor_off[g + 1] > X.tor_off[g] || X.o14_off[g + 1] > X.o14_off[g]);
+  for (int a = a0; a < a1; a++) {
+    const int i = gatoms[a];
+    const double e = nhc_factor(ithm[i], P.nchain, P.dta2, veta);
+    for (int d = 0; d < 3; d++) {
+      const int x = d * n + i;
+      vel[x] *= e;
+      pos[x] += P.dta2 * vel[x];
+    }
+  }
+  if (bonded) {
+    for (int a = a0; a < a1; a++) {
+      const int i = gatoms[a];
+      fxa[i] = fxa[n + i] = fxa[2 * n + i] = 0.;
+    }
+    group_bonded(g, n, pos, fxa, gboff, bij, bp, geoff, eijk, ep);
+    if (has_bx) group_bondx(g, n, pos, fxa, X);
+    for (int a = a0; a < a1; a++) {
+      const int i = gatoms[a];
+      const double r = 1. / mass[i];
+      fxa[i] *= r; fxa[n + i] *= r; fxa[2 * n + i] *= r;
+      if (X.frz && X.frz[i]) freeze_one(i, n, vel, fxa);
+    }
+  }
+  for (int a = a0; a < a1; a++) {
+    const int i = gatoms[a];
+    for (int d = 0; d < 3; d++) vel[d * n + i] += P.dta2 * fxa[d * n + i];
+  }
+  if (tors_end && tors) {
+    for (int a = a0; a < a1; a++) {
+      const int i = gatoms[a];
+      fxr[i] = fxr[n + i] = fxr[2 * n + i] = 0.;
+    }
+    group_tors_level(g, n, pos, q, fxr, X, stat);
+    for (int a = a0; a < a1; a++) {
+      const int i = gatoms[a];
+      const double r = 1. / mass[i];
+      fxr[i] *= r; fxr[n + i] *= r; fxr[2 * n + i] *= r;
+      if (X.frz && X.frz[i]) freeze_one(i, n, vel, fxr);
+      for (int d = 0; d < 3; d++) vel[d * n + i] += P.dtr2 * fxr[d * n + i];
+    }
+  }
+  if (level_end) {
+    const int sy = sys_of[gatoms[a0]];
+    const double skin2q = sp[sy].skin2q;
+    bool far = false;
+    for (int a = a0; a < a1; a++) {
+      const int i = gatoms[a];
+      const double xc = dxn[i] - pos[i], yc = dxn[n + i] - pos[n + i], zc = dxn[2 * n + i] - pos[2 * n + i];
+      if (xc * xc + yc * yc + zc * zc > skin2q) far = true;
+    }
+    if (far) {
+      sreb[sy] = 1;
+      istate[IS_REBUILD] = 1;
+    }
+  }
+}
+
 // standalone displacement test (cm3d_nb_nrefsh)
 __global__ void k_disp(int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
                        const double *__restrict__ pos, const double *__restrict__ dxn, int *__restrict__ sreb,
@@ -695,6 +841,7 @@ static StepP step_params(Ctx *c) {
   P.kappa = c->kappa;
   P.kappa2 = c->kappa2;
   P.use_fxs = c->nres_lrf > 1 || c->need_short;
+  P.nchain = c->nchain;
   return P;
 }
 
@@ -908,6 +1055,43 @@ static int upload_intra(Ctx *c, const IntraHost &ih, const std::vector<int> &gid
   return CM3D_NB_OK;
 }
 
+// Nose-Hoover chains of every system, thermostats numbered across the batch
+// (system order), with their state as CM3D holds it after samveta
+static int nvt_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
+  if (systems[0].iensemble != 1) return CM3D_NB_OK;
+  const int nch = systems[0].nchain;
+  int nt = 0;
+  for (int sy = 0; sy < nsys; sy++) nt += systems[sy].ntherm;
+  const size_t tc = (size_t)nt * nch;
+  std::vector<double> h(5 * tc + (size_t)nt, 0.0);
+  std::vector<int> thm((size_t)c->n, -1);
+  int t0 = 0;
+  for (int sy = 0; sy < nsys; sy++) {
+    const cm3d_nb_system *s = systems + sy;
+    const size_t o = (size_t)t0 * nch, k = (size_t)s->ntherm * nch;
+    std::copy(s->mnh, s->mnh + k, h.begin() + o);
+    std::copy(s->gkt, s->gkt + k, h.begin() + tc + o);
+    std::copy(s->nhc_eta, s->nhc_eta + k, h.begin() + 2 * tc + o);
+    std::copy(s->nhc_veta, s->nhc_veta + k, h.begin() + 3 * tc + o);
+    for (int i = 0; i < s->natoms; i++) {
+      const int j = s->ithm[i];
+      if (j >= s->ntherm) {
+        set_error("system %d atom %d: thermostat %d of %d", sy, i, j, s->ntherm);
+        return CM3D_NB_ERR_ARG;
+      }
+      thm[(size_t)(c->h_sp[sy].a0 + i)] = j >= 0 ? t0 + j : -1;
+    }
+    t0 += s->ntherm;
+  }
+  c->ntherm = nt;
+  c->nchain = nch;
+  CK(cudaMalloc(&c->nhc, sizeof(double) * h.size()));
+  CK(cudaMemcpy(c->nhc, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c->ithm, sizeof(int) * thm.size()));
+  CK(cudaMemcpy(c->ithm, thm.data(), sizeof(int) * thm.size(), cudaMemcpyHostToDevice));
+  return CM3D_NB_OK;
+}
+
 int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   const int n = c->n;
   // every system's bonds, bends and excluded Ewald pairs with global atom
@@ -1029,7 +1213,8 @@ int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   CK(cudaMemcpy(c->bend_p, ep.data(), sizeof(double2) * ep.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ecorr_ij, cij.data(), sizeof(int2) * cij.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ecorr_pairs, cpair.data(), sizeof(int2) * cpair.size(), cudaMemcpyHostToDevice));
-  return upload_intra(c, ih, gid, ng);
+  if ((rc = upload_intra(c, ih, gid, ng))) return rc;
+  return nvt_setup(c, systems, nsys);
 }
 
 int run_bonded(Ctx *c) {
@@ -1183,14 +1368,36 @@ static int one_level(Ctx *c, int intr, bool gated) {
   if ((rc = clear_rebuild(c))) return rc;
   cudaEvent_t e0;
   tbegin(c, 3, &e0);
-  auto inner = c->has_intra_x || c->intra.frz ? k_inner<true> : k_inner<false>;
-  inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
-                                                    c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
-                                                    c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
-                                                    c->bend_p, c->sp, c->sys_of, c->sreb, c->istate, c->gate,
-                                                    c->intra, c->q, c->fxr, c->stat);
+  if (c->ntherm > 0) {
+    // NVT: three launches per inner substep (k_nvt_a, k_nvt_chain, k_nvt_c)
+    const size_t tc = (size_t)c->ntherm * c->nchain;
+    double *veta = c->nhc + 3 * tc, *p2m = c->nhc + 5 * tc;
+    for (int inrra = 0; inrra < c->nres_tors; inrra++)
+      for (int intra = 0; intra < c->nres_intra; intra++) {
+        CK(cudaMemsetAsync(p2m, 0, sizeof(double) * (size_t)c->ntherm, c->st));
+        k_nvt_a<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, inrra == 0 && intra == 0, intra == 0,
+                                                          c->grp_atom_off, c->grp_atoms, c->pos, c->vel, c->mass,
+                                                          c->fxl, c->fxs, c->fxa, c->fxr, c->ithm, veta, p2m,
+                                                          c->intra, c->istate, c->gate);
+        k_nvt_chain<<<grid_for(c->ntherm, 64), 64, 0, c->st>>>(c->ntherm, c->nchain, P.dta2, c->nhc, p2m,
+                                                               c->gate);
+        k_nvt_c<<<grid_for(c->ngroups, B), B, 0, c->st>>>(
+            P, intra == c->nres_intra - 1, inrra == c->nres_tors - 1 && intra == c->nres_intra - 1,
+            c->grp_atom_off, c->grp_atoms, c->pos, c->vel, c->mass, c->q, c->fxa, c->fxr, c->dxn,
+            c->grp_bond_off, c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk, c->bend_p, c->ithm, veta,
+            c->sp, c->sys_of, c->sreb, c->istate, c->intra, c->stat, c->gate);
+        c->launches += 3;
+      }
+  } else {
+    auto inner = c->has_intra_x || c->intra.frz ? k_inner<true> : k_inner<false>;
+    inner<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, c->grp_atom_off, c->grp_atoms, c->pos, c->vel,
+                                                      c->mass, c->fxl, c->fxs, c->fxa, c->dxn, c->grp_bond_off,
+                                                      c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk,
+                                                      c->bend_p, c->sp, c->sys_of, c->sreb, c->istate, c->gate,
+                                                      c->intra, c->q, c->fxr, c->stat);
+    c->launches++;
+  }
   tend(c, 3, e0);
-  c->launches++;
   CKL(c);
   if ((rc = reset_positions(c))) return rc;
   if (gated) {

@@ -146,9 +146,11 @@ typedef struct cm3d_nb_system {
   int nfreeze;
   const int *ifreeze;
   /* SIMPARMS.iensemble / ntherm / nchain and COORDS' Nose-Hoover chain state
-     (md_typedef.h:122-125, 203-224; set_therm_new md_therm.new.c:32).  The
-     engine integrates NVE: cm3d_nb_create refuses iensemble != 0 or
-     ntherm > 0.  The fields describe a thermostatted run to the CPU checker. */
+     (md_typedef.h:122-125, 203-224; set_therm_new md_therm.new.c:32), as
+     samveta leaves it.  iensemble 0 (NVE, no thermostats) or 1 (NVT: the
+     chains integrated by intnhc_new, md_therm.new.c:278, inside the inner
+     level of step()); cm3d_nb_create refuses anything else (barostats).
+     Every system of a batch has the same ensemble and chain length. */
   int iensemble, ntherm, nchain;
   const int *ithm;                            /* [natoms] thermostat of each atom (-1: none) */
   const double *mnh, *gkt, *nhc_eta, *nhc_veta;   /* [ntherm * nchain] */

@@ -35,6 +35,8 @@ GROUPS = {
     # two copies of CM3D's abutane molecule: torsions, 1-4 pairs, cross bonds,
     # frozen atoms, and a batch whose systems all take the one-warp k-space tiles
     "tors": ["abutane", "abutane"],
+    # two copies of CM3D's NVT deck: one Nose-Hoover chain per system
+    "nvt": ["lj256nvt", "lj256nvt"],
 }
 ETOL, VTOL, FTOL = 1e-5, 5e-5, 1e-5
 VIRIAL_KEYS = {"winter", "welec", "W", "prsi"}

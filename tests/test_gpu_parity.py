@@ -282,3 +282,26 @@ def test_torsion_terms_refused_form(engine_lib):
     s["tors_ind_pot"] = ind
     with pytest.raises(EngineError, match="ind_pot 2"):
         Engine(s, mode=_abi.MIXED)
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+@pytest.mark.parametrize("mode", MODES, ids=lambda m: MODE_ID[m])
+def test_nvt_trajectory(engine_lib, mode, graph):
+    """CM3D's test/lj NVT deck (one global Nose-Hoover chain of length 3):
+    the engine's step with the chain update between the inner half drifts
+    (k_nvt_a / k_nvt_chain / k_nvt_c) against CM3D's per-step energies and
+    final positions.  The thermostat's kinetic sum is accumulated with
+    atomics, so even the plain engine differs from CM3D in summation order."""
+    d, e = engine("lj256nvt", mode, use_graph=graph)
+    e.step_init()
+    eng = d["traj_eng"].reshape(-1, 8)
+    ptol = 1e-9 if mode == _abi.PLAIN_FP64 else 2e-4
+    for k in range(int(d["nsteps"][0])):
+        e.step(1 + k, 1)
+        en = e.energies()
+        for c, key in enumerate(("poter", "potra", "zke")):
+            assert close(en[key], eng[k, c], ptol), (k, key)
+    pos = e.positions()
+    ref = np.stack([d["final_px"], d["final_py"], d["final_pz"]])
+    assert np.abs(pos - ref).max() <= (1e-9 if mode == _abi.PLAIN_FP64 else 1e-3)
+    e.close()

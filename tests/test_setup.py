@@ -164,12 +164,19 @@ def test_system_description_carries_the_torsion_level():
     assert not bool(a.itors) and not bool(a.ifreeze)
 
 
-def test_engine_refuses_thermostats_on_the_host(engine_lib):
-    """the engine integrates NVE: a thermostatted system (CM3D's NVT deck) is
-    refused by cm3d_nb_create before any device work, with the reason"""
+def test_engine_refuses_barostats_on_the_host(engine_lib):
+    """the engine integrates NVE or NVT: an NPT system (iensemble 2), or NVT
+    without its chain state, is refused by cm3d_nb_create before any device
+    work, with the reason"""
     from cm3d_b200 import _abi
     from cm3d_b200.engine import Engine, EngineError
     s = System.from_arrays(golden("lj256nvt"))
     assert s.desc().ntherm == 1 and s.desc().iensemble == 1
-    with pytest.raises(EngineError, match="thermostats and barostats"):
+    s["iensemble"] = 2
+    with pytest.raises(EngineError, match="without barostats"):
+        Engine(s, mode=_abi.MIXED)
+    s = System.from_arrays(golden("lj256nvt"))
+    del s.a["nhc_veta"]
+    s._desc = None
+    with pytest.raises(EngineError, match="without barostats"):
         Engine(s, mode=_abi.MIXED)
