@@ -949,6 +949,24 @@ int cm3d_nb_system_counts(cm3d_nb_ctx *ctx, long long *rebuilds, long long *rese
   return CM3D_NB_OK;
 }
 
+int cm3d_nb_get_nhc(cm3d_nb_ctx *ctx, int sys, double *eta, double *veta, int *ntherm, int *nchain) {
+  CTX;
+  if (sys < 0 || sys >= c->nsys) {
+    set_error("get_nhc: system %d of %d", sys, c->nsys);
+    return CM3D_NB_ERR_ARG;
+  }
+  const int nt = c->ntherm > 0 ? c->therm0[(size_t)sys + 1] - c->therm0[(size_t)sys] : 0;
+  if (ntherm) *ntherm = nt;
+  if (nchain) *nchain = c->ntherm > 0 ? c->nchain : 0;
+  if (nt == 0) return CM3D_NB_OK;
+  const size_t tc = (size_t)c->ntherm * c->nchain, o = (size_t)c->therm0[(size_t)sys] * c->nchain,
+               k = (size_t)nt * c->nchain;
+  CK(cudaStreamSynchronize(c->st));
+  if (eta) CK(cudaMemcpy(eta, c->nhc + 2 * tc + o, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  if (veta) CK(cudaMemcpy(veta, c->nhc + 3 * tc + o, sizeof(double) * k, cudaMemcpyDeviceToHost));
+  return CM3D_NB_OK;
+}
+
 // The mixed engine's rebuilds write only its full list.  CM3D's half lists
 // are produced on request by rebuilding from the positions of the last
 // rebuild (dxn): the same cells and the same pairs, without touching the

@@ -306,6 +306,7 @@ struct Ctx {
   int ntherm = 0, nchain = 0;
   int *ithm = nullptr;                  // per atom: its thermostat, -1 none
   double *nhc = nullptr;                // mnh | gkt | eta | veta | feta, ntherm * nchain each, then p2m (ntherm)
+  std::vector<int> therm0;              // per system: its first thermostat (nsys + 1 entries)
   // ---- cell grid and lists
   int nc[3] = {1, 1, 1}, ncells = 1;
   int *cell_of = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *cell_atoms = nullptr;

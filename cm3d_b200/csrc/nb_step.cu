@@ -1066,9 +1066,11 @@ static int nvt_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   std::vector<double> h(5 * tc + (size_t)nt, 0.0);
   std::vector<int> thm((size_t)c->n, -1);
   int t0 = 0;
+  c->therm0.assign((size_t)nsys + 1, 0);
   for (int sy = 0; sy < nsys; sy++) {
     const cm3d_nb_system *s = systems + sy;
     const size_t o = (size_t)t0 * nch, k = (size_t)s->ntherm * nch;
+    c->therm0[(size_t)sy] = t0;
     std::copy(s->mnh, s->mnh + k, h.begin() + o);
     std::copy(s->gkt, s->gkt + k, h.begin() + tc + o);
     std::copy(s->nhc_eta, s->nhc_eta + k, h.begin() + 2 * tc + o);
@@ -1083,6 +1085,7 @@ static int nvt_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
     }
     t0 += s->ntherm;
   }
+  c->therm0[(size_t)nsys] = t0;
   c->ntherm = nt;
   c->nchain = nch;
   CK(cudaMalloc(&c->nhc, sizeof(double) * h.size()));

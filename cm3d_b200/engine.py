@@ -65,6 +65,7 @@ def load_library() -> C.CDLL:
         "cm3d_nb_get_system_energies": (C.c_int, [vp, C.c_int, C.POINTER(_abi.Energies)]),
         "cm3d_nb_get_all_energies": (C.c_int, [vp, C.POINTER(_abi.Energies)]),
         "cm3d_nb_system_counts": (C.c_int, [vp, C.POINTER(ll), C.POINTER(ll)]),
+        "cm3d_nb_get_nhc": (C.c_int, [vp, C.c_int, dp, dp, ip, ip]),
         "cm3d_nb_set_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_get_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_velocities": (C.c_int, [vp, dp, dp, dp]),
@@ -306,6 +307,17 @@ class Engine:
         check(load_library().cm3d_nb_get_all_energies(self._h, out.ctypes.data_as(C.POINTER(_abi.Energies))),
               "get_all_energies")
         return out
+
+    def nhc_state(self, sys: int = 0) -> tuple[np.ndarray, np.ndarray]:
+        """NVT: system `sys`'s Nose-Hoover chain (eta, veta), ntherm x nchain
+        each (empty for NVE)"""
+        L = load_library()
+        nt, nc = C.c_int(0), C.c_int(0)
+        check(L.cm3d_nb_get_nhc(self._h, sys, None, None, C.byref(nt), C.byref(nc)), "get_nhc")
+        eta, veta = np.zeros(max(nt.value * nc.value, 1)), np.zeros(max(nt.value * nc.value, 1))
+        check(L.cm3d_nb_get_nhc(self._h, sys, _p(eta), _p(veta), None, None), "get_nhc")
+        k = nt.value * nc.value
+        return eta[:k].reshape(nt.value, nc.value), veta[:k].reshape(nt.value, nc.value)
 
     def system_counts(self) -> tuple[np.ndarray, np.ndarray]:
         """per-system (list rebuilds, RESETPOS events)"""

@@ -229,6 +229,10 @@ int cm3d_nb_get_system_energies(cm3d_nb_ctx *ctx, int sys, cm3d_nb_energies *e);
 int cm3d_nb_get_all_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e);
 /* per-system list rebuilds and RESETPOS events since creation (arrays of nsys) */
 int cm3d_nb_system_counts(cm3d_nb_ctx *ctx, long long *rebuilds, long long *resets);
+/* NVT: system sys's Nose-Hoover chain positions and velocities (COORDS.eta,
+   veta, md_typedef.h:224), ntherm x nchain each, as the steps left them;
+   *ntherm and *nchain receive the sizes (0 for an NVE context) */
+int cm3d_nb_get_nhc(cm3d_nb_ctx *ctx, int sys, double *eta, double *veta, int *ntherm, int *nchain);
 
 /* host <-> device state (COORDS.px..pz, vx..vz, hmat) */
 int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py,

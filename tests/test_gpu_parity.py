@@ -304,4 +304,10 @@ def test_nvt_trajectory(engine_lib, mode, graph):
     pos = e.positions()
     ref = np.stack([d["final_px"], d["final_py"], d["final_pz"]])
     assert np.abs(pos - ref).max() <= (1e-9 if mode == _abi.PLAIN_FP64 else 1e-3)
+    # the chain state read back through cm3d_nb_get_nhc
+    eta, veta = e.nhc_state()
+    assert eta.shape == veta.shape == (1, 3)
+    for got, key in ((eta, "final_nhc_eta"), (veta, "final_nhc_veta")):
+        want = d[key]
+        assert np.abs(got.ravel() - want).max() <= (1e-8 if mode == _abi.PLAIN_FP64 else 1e-3) * np.abs(want).max()
     e.close()
