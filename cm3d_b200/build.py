@@ -28,6 +28,7 @@ SOURCES = [
     ("nb_list.cu", ["-fmad=false"]),
     ("nb_plain.cu", ["-fmad=false"]),
     ("nb_pair.cu", []),
+    ("nb_cwin.cu", []),
     ("nb_kspace.cu", []),
     ("nb_step.cu", []),
     ("nb_capi.cu", []),

@@ -87,7 +87,8 @@ static void destroy(Ctx *c) {
                   c->cimg, c->nlen, c->acc,
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
                   c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan,
-                  c->fxr, c->intra_buf, c->ithm, c->nhc};
+                  c->fxr, c->intra_buf, c->ithm, c->nhc, c->cwl, c->cwn, c->cw_tf, c->cw_tg, c->cw_tl,
+                  c->cw_part};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -430,6 +431,7 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
   memset(c->h_istate, 0, sizeof(int) * IS_COUNT);
   if ((rc = list_setup(c))) return rc;
   if ((rc = pair_setup(c))) return rc;
+  if ((rc = cw_setup(c))) return rc;
   if ((rc = kspace_setup(c))) return rc;
   if ((rc = step_setup(c, systems, nsys))) return rc;
   if ((rc = upload(&c->sp, c->h_sp.data(), c->h_sp.size()))) return rc;
@@ -1098,7 +1100,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   if (reps < 1) reps = 5;
   const int cand[4] = {4, 8, 16, 32};
   double best = 1e300;
-  int best_tpa = c->tpa, best_win = 0;
+  int best_tpa = c->tpa, best_win = 0, best_cw = 0;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -1106,12 +1108,17 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   c->timing.on = false;
   if (ms_per_launch)
     for (int k = 0; k < 4; k++) ms_per_launch[k] = 1e300;
-  // the gather kernel, then (where it applies) the staged kernel -- a single
-  // system's 27-cell windows, or a batch's whole systems: the context runs
-  // whichever is faster on its live lists
-  for (int win = 0; win <= (c->win_env_off ? 0 : 1); win++) {
-    c->win_ok = win;
+  // kind 0: the gather kernel; 1: the staged kernel that applies (a single
+  // system's 27-cell windows, or a batch's whole systems); 2: the compact
+  // window list (one system, nb_cwin.cu) -- the context runs whichever is
+  // fastest on its live lists
+  for (int kind = 0; kind <= 2; kind++) {
+    if (kind == 1 && c->win_env_off) continue;
+    if (kind == 2 && !c->cw_ok) continue;
+    c->win_ok = kind == 1;
+    c->cw_use = kind == 2;
     for (int k = 0; k < 4; k++) {
+      if (kind == 2 && cand[k] < 8) continue;        // the compact kernel runs 8, 16 or 32 lanes per atom
       c->tpa = cand[k];
       if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
       CK(cudaEventRecord(a, c->st));
@@ -1126,7 +1133,8 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
       if (per < best) {
         best = per;
         best_tpa = cand[k];
-        best_win = win;
+        best_win = kind == 1;
+        best_cw = kind == 2;
       }
     }
   }
@@ -1135,6 +1143,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   cudaEventDestroy(b);
   c->tpa = best_tpa;
   c->win_ok = best_win;
+  c->cw_use = best_cw;
   if (tpa_chosen) *tpa_chosen = best_tpa;
   // a captured step holds the old launch configuration; the timing launches
   // added to the force blocks and accumulators: recompute force(1)

@@ -95,6 +95,7 @@ enum {
   ST_REBUILDS = 4,
   ST_BADSHIFT = 5,        // a pair's cell shift fell outside the 27-entry table
   ST_NEED_STRIDE = 6,     // longest full list that did not fit its slot
+  ST_CWIN = 7,            // a cell window too large for the compact list (nb_cwin.cu)
   ST_COUNT = 8
 };
 // device integer state
@@ -236,6 +237,21 @@ struct Ctx {
   int4 *sys_items = nullptr;           // batch pair kernel work items {system, first, end, -}
   int nsys_items = 0;
   float4 *ftab_lj2 = nullptr;          // LJ force + energy coefficients, 2 float4 per knot
+  // compact-window pair path (nb_cwin.cu): one system, >= 3 cells per axis
+  int cw_ok = 0;                       // set up and valid for this context
+  int cw_use = 0;                      // preferred over the window/gather kernels (autotuner)
+  int cw_rf = 1, cw_rg = 1;            // table copies in shared memory
+  int cw_cap = 0;                      // window slots
+  size_t cw_smem = 0;                  // dynamic shared memory of k_pair_cw
+  int cw_words = 0;                    // 8-byte words per atom slot of the compact list
+  uint2 *cwl = nullptr;                // compact list (16-bit window indices, lane-interleaved blocks)
+  int2 *cwn = nullptr;                 // per sorted atom: LJ-segment and electrostatics-only lengths
+  float4 *cw_tf = nullptr;             // erfc force coefficients + base energy
+  float2 *cw_tg = nullptr;             // erfc energy slope and curvature
+  float4 *cw_tl = nullptr;             // LJ, 2 float4 per knot
+  float cw_lj1[4] = {0, 0, 0, 0};      // the one LJ interaction: rc^2, dx2tab, offset, vt
+  int cw_nsplit = 1, cw_nitems = 0;    // work items: cells x parts
+  double *cw_part = nullptr;           // per-item FP64 energy/virial sums
   int stage_ntypes = 0, stage_ninter = 0;   // largest per-system type count / interaction count
   cudaStream_t st = nullptr;
   int mode = CM3D_NB_MIXED;
@@ -448,6 +464,11 @@ int build_lists(Ctx *c, bool device_flag, bool all);   // nb_list.cu
 int list_setup(Ctx *c);                         // nb_list.cu
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused
 int pair_setup(Ctx *c);                         // nb_pair.cu
+int cw_setup(Ctx *c);                           // nb_cwin.cu: compact-window path (after pair_setup)
+int cw_convert(Ctx *c, bool device_flag);       // nb_cwin.cu: master list -> compact list
+bool cw_applies(Ctx *c, int iflg, bool ns);     // nb_cwin.cu
+int cw_pairs(Ctx *c, int mask, double *fout);   // nb_cwin.cu: pair kernel launch
+int cw_ereduce(Ctx *c, int mask);               // nb_cwin.cu: its energy/virial sums
 int kspace_forces(Ctx *c);                      // nb_kspace.cu
 int kspace_setup(Ctx *c);                       // nb_kspace.cu
 int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys);   // nb_step.cu

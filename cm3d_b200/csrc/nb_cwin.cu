@@ -1,0 +1,759 @@
+// nb_cwin.cu -- compact-window pair kernel for one large system.
+//
+// The physics is that of force_npol (energy/inter/md_fnopol.c:46-255) and
+// force_e (energy/inter/finter_e.c:42-233): CM3D's tables on the r^2 grid,
+// its 3-point interpolation f = f0 + p (A + p B) (finter_e.c:122-136), the
+// cut-off test `dis2 < rmax2` (finter_e.c:119) and its energy shifts -- the
+// same sums as nb_pair.cu, laid out so that the kernel's shared-memory
+// traffic per pair is close to the minimum.
+//
+// The master full list (nb_list.cu: per cell-sorted atom, 32-bit entries of
+// sorted index + cell-shift code + list flags) is rewritten after every
+// rebuild into a compact list (k_cw_convert):
+//
+//   * a 16-bit entry holds the index of j in the 27-cell window of i's cell
+//     (the window a pair-kernel block stages in shared memory, each cell
+//     already moved by its periodic shift), so an entry names j's staged
+//     position directly: no shift code, no index translation per pair; and
+//     the list is half the bytes;
+//   * every segment (LJ-list pairs first, then electrostatics-only pairs) is
+//     stored in blocks of 128 entries interleaved by lane: the 8-byte word
+//     `w` of a block holds entries w, w + 32, w + 64, w + 96, so that in each
+//     of the four passes over a block the 32 lanes of a warp read 32
+//     consecutive entries -- mostly consecutive window slots of one cell,
+//     which spreads a warp's window loads over the shared-memory banks.
+//
+// The pair kernel (k_pair_cw) keeps the tables in shared memory replicated
+// RF (RG) times, lane l reading copy l % RF: with RF = 8 the 16-byte force
+// coefficients a lane reads always lie in bank group l % 8, so a warp's 32
+// random table reads take 4 shared-memory wavefronts -- the minimum for 512
+// bytes -- instead of the ~7 that random 16-byte reads cost.
+//
+// Precision and order: distances, interpolation and the per-pair products
+// are FP32 (cell-relative coordinates, as in nb_pair.cu); each lane sums its
+// pairs of one atom in FP32 (about 20 pairs for 32 lanes per atom) and then
+// adds that chunk in FP64: forces across the atom's lanes (fixed shuffle
+// tree), energies and virials into per-lane FP64 sums that the block adds up
+// per work item and k_cw_ereduce adds over items, all in a fixed order.  The
+// results do not depend on timing: a run repeats bit for bit.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "nb_common.cuh"
+
+namespace cm3d {
+
+constexpr int CW_THREADS = 512;
+constexpr int CW_ROW = 32;                  // interleave width (entries per pass of a block)
+constexpr int CW_BLOCK = 4 * CW_ROW;        // entries per block: one 8-byte word per lane
+constexpr uint32_t CW_IDX = 0x3FFFu;        // window index bits of an entry
+constexpr uint32_t CW_EL = 0x4000u;         // LJ-segment entry: the pair is also in CM3D's te list
+constexpr int CW_MAX_CAP = 16382;           // window slots (the dummy slot `cap` must fit 14 bits)
+constexpr float CW_MAGIC = 12582912.0f;     // 1.5 * 2^23: p + MAGIC rounded toward zero holds floor(p)
+constexpr unsigned CW_MAGIC_BITS = 0x4B400000u;
+constexpr int CW_STATIC_SMEM = 6144;        // >= the kernel's static shared arrays (5.2 KB)
+
+// per-item FP64 sums (each pair is seen from both ends: k_cw_ereduce halves)
+enum { CQ_EEL = 0, CQ_QQ, CQ_VE0, CQ_VE1, CQ_VE2, CQ_VE4, CQ_VE5, CQ_VE8,
+       CQ_ELJ, CQ_VSH, CQ_VL0, CQ_VL1, CQ_VL2, CQ_VL4, CQ_VL5, CQ_VL8, CQ_COUNT };
+
+struct CwP {
+  int n, ncx, ncy, ncz, nitems, nsplit, cap, words;   // words: 8-byte words per atom slot
+  int ntable, ntypes, ninter, rf, rg;
+  float rc2_el, dx2c, offc, pmax;
+  // one LJ interaction (LJM 1): cut-off^2, dx2tab, rmins_cut2 * dx2tab, vtab[ntable-4]
+  float rc2_l, dx2l, offl, vtl;
+};
+
+// ------------------------------------------------------------------
+// Master list -> compact list.  Block per cell: the cell's 27-cell window
+// layout (stencil cell w = shift code, j-cell = i-cell - k_w, cells in code
+// order) gives delta[w] = window offset - first sorted index, so entry
+// (u, w) becomes window index u + delta[w].  A window larger than `cap`
+// cannot be indexed: the cell's atoms get empty lists, ST_CWIN counts it and
+// a captured step halts (the host then turns the compact path off).
+__global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words,
+                                                    const int *__restrict__ cell_start,
+                                                    const int *__restrict__ nlen, int stride,
+                                                    const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
+                                                    int2 *__restrict__ cwn, long long *__restrict__ stat,
+                                                    int *__restrict__ halt, const int *__restrict__ gs) {
+  if (gated_off(gs, 1)) return;
+  __shared__ int s_delta[32], s_tot;
+  const int ncells = ncx * ncy * ncz;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t dummy = (uint32_t)cap;
+  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
+    __syncthreads();                                   // the previous cell's deltas are no longer read
+    if (warp == 0) {
+      const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
+      int cnt = 0, cs = 0;
+      if (lane < 27) {
+        int jx = cx - (lane / 9 - 1), jy = cy - ((lane / 3) % 3 - 1), jz = cz - (lane % 3 - 1);
+        jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
+        jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
+        jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
+        const int jc = (jx * ncy + jy) * ncz + jz;
+        cs = cell_start[jc];
+        cnt = cell_start[jc + 1] - cs;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      s_delta[lane] = lane < 27 ? incl - cnt - cs : 0;
+      if (lane == 26) s_tot = incl;
+    }
+    __syncthreads();
+    const int tot = s_tot;
+    const bool fits = tot <= cap;
+    if (!fits && threadIdx.x == 0) {
+      atomicAdd((unsigned long long *)(stat + ST_CWIN), 1ull);
+      if (halt) *halt = 1;
+    }
+    const int lo = cell_start[c], hi = cell_start[c + 1];
+    for (int t = lo + warp; t < hi; t += nwarps) {
+      const int na = fits ? nlen[t] : 0, nb = fits ? nlen[n + t] : 0;
+      const uint32_t *src = nbr + (size_t)t * stride;
+      uint2 *dst = cwl + (size_t)t * words;
+      const int nba = (na + CW_BLOCK - 1) / CW_BLOCK, nbb = (nb + CW_BLOCK - 1) / CW_BLOCK;
+      for (int b = 0; b < nba + nbb; b++) {
+        const bool front = b < nba;
+        const int e0 = (front ? b : b - nba) * CW_BLOCK, cnt = front ? na : nb;
+        uint32_t v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const int e = e0 + k * CW_ROW + lane;
+          uint32_t o = dummy;
+          if (e < cnt) {
+            // the back segment runs from the slot's end towards its front
+            const uint32_t en = front ? src[e] : src[stride - nb + e];
+            const int code = (en >> ENT_CODE_SHIFT) & 31;
+            const int wi = (int)(en & ENT_JMASK) + s_delta[code];
+            // inside the window by construction (a pair's shift code names
+            // j's stencil cell); anything else would index past the staged
+            // atoms, so it becomes the dummy
+            o = wi >= 0 && wi < tot ? (uint32_t)wi : dummy;
+            if (front && (en & ENT_EL) && o != dummy) o |= CW_EL;
+          }
+          v[k] = o;
+        }
+        dst[b * CW_ROW + lane] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
+      }
+      if (lane == 0) cwn[t] = make_int2(na, nb);
+    }
+  }
+}
+
+// ------------------------------------------------------------------
+// Pair kernel.  Block per work item (a cell, or one of `nsplit` parts of
+// its atoms); the block stages the cell's window and then walks the item's
+// atoms with TPA lanes per atom.
+//   HAS_EL: the system has charges; LJM: 0 no LJ, 1 one LJ interaction (its
+//   parameters in CwP), 2 several (type map, cut-offs and tables per pair).
+struct CwAcc {
+  float fx, fy, fz;              // sum qj f d over the electrostatic pairs (x qi at the end)
+  float gx, gy, gz;              // sum f d over the LJ pairs
+  float eel, qs, ve[6];          // sum qj V, sum qj, sum qj f d d
+  float elo, vsh, vl[6];         // LJ: energy lo parts, sum vt, sum f d d
+  double elj_hi;                 // LJ: energy hi parts (FP64)
+  float pmin;                    // smallest table coordinate of an in-range pair (underflow test)
+};
+
+__device__ __forceinline__ void cw_zero(CwAcc &A) {
+  A.fx = A.fy = A.fz = A.gx = A.gy = A.gz = 0.f;
+  A.eel = A.qs = A.elo = A.vsh = 0.f;
+#pragma unroll
+  for (int k = 0; k < 6; k++) A.ve[k] = A.vl[k] = 0.f;
+  A.elj_hi = 0.0;
+  A.pmin = 3.0e38f;
+}
+
+// floor of p in [1, 2^22) by the rounding of one FP32 add (RZ mode); returns
+// the fraction and leaves the float bits MAGIC + floor(p) in kb
+__device__ __forceinline__ float cw_split(float p, unsigned &kb) {
+  const float t = __fadd_rz(p, CW_MAGIC);
+  kb = __float_as_uint(t);
+  return p - (t - CW_MAGIC);
+}
+
+// One electrostatic pair, j staged at xj (charge in w).  `el`: the pair is in
+// the te list (back-segment pairs always are).
+template <bool TRACK>
+__device__ __forceinline__ void cw_elec(const CwP &P, const float4 xj, float dx, float dy, float dz, float r2,
+                                        bool el, const float4 *__restrict__ tf, const float2 *__restrict__ tg,
+                                        CwAcc &A) {
+  const bool ok = el && r2 < P.rc2_el;
+  float p = fmaf(r2, P.dx2c, -P.offc);
+  if (TRACK) A.pmin = fminf(A.pmin, ok ? p : 3.0e38f);
+  else A.pmin = fminf(A.pmin, p);
+  // CM3D's clamp below the table (k = 1, fraction 0); out-of-range pairs
+  // read the last knot and contribute zero (their charge is selected to 0)
+  p = fminf(fmaxf(p, 1.f), P.pmax);
+  unsigned kb;
+  const float fr = cw_split(p, kb);
+  const unsigned k = kb - CW_MAGIC_BITS;
+  const float4 c = tf[k * (unsigned)P.rf];
+  const float2 d = tg[k * (unsigned)P.rg];
+  const float qj = ok ? xj.w : 0.f;
+  const float fe = qj * fmaf(fr, fmaf(fr, c.z, c.y), c.x);
+  A.eel = fmaf(qj, fmaf(fr, fmaf(fr, d.y, d.x), c.w), A.eel);
+  A.qs += qj;
+  const float ux = fe * dx, uy = fe * dy, uz = fe * dz;
+  A.fx += ux;
+  A.fy += uy;
+  A.fz += uz;
+  A.ve[0] = fmaf(ux, dx, A.ve[0]);
+  A.ve[1] = fmaf(ux, dy, A.ve[1]);
+  A.ve[2] = fmaf(ux, dz, A.ve[2]);
+  A.ve[3] = fmaf(uy, dy, A.ve[3]);
+  A.ve[4] = fmaf(uy, dz, A.ve[4]);
+  A.ve[5] = fmaf(uz, dz, A.ve[5]);
+}
+
+// One LJ pair of interaction parameters {rc2, dx2, off, vt}; tl holds 2
+// float4 per knot {d0, dA, dB, v0 hi} {vA, vB, v0 lo, -}.
+__device__ __forceinline__ void cw_lj(const CwP &P, float dx, float dy, float dz, float r2, float rc2, float dx2,
+                                      float off, float vt, const float4 *__restrict__ tl, float &pminl,
+                                      CwAcc &A) {
+  const bool ok = r2 < rc2;
+  float p = fmaf(r2, dx2, -off);
+  pminl = fminf(pminl, ok ? p : 3.0e38f);
+  p = fminf(fmaxf(p, 1.f), P.pmax);
+  unsigned kb;
+  const float fr = cw_split(p, kb);
+  const unsigned k = kb - CW_MAGIC_BITS;
+  const float4 a = tl[2 * k], b = tl[2 * k + 1];
+  const float okf = ok ? 1.f : 0.f;
+  const float f = okf * fmaf(fr, fmaf(fr, a.z, a.y), a.x);
+  A.elj_hi += ok ? (double)a.w : 0.0;
+  A.elo = fmaf(okf, fmaf(fr, fmaf(fr, b.y, b.x), b.z), A.elo);
+  A.vsh = fmaf(okf, vt, A.vsh);
+  const float ux = f * dx, uy = f * dy, uz = f * dz;
+  A.gx += ux;
+  A.gy += uy;
+  A.gz += uz;
+  A.vl[0] = fmaf(ux, dx, A.vl[0]);
+  A.vl[1] = fmaf(ux, dy, A.vl[1]);
+  A.vl[2] = fmaf(ux, dz, A.vl[2]);
+  A.vl[3] = fmaf(uy, dy, A.vl[3]);
+  A.vl[4] = fmaf(uy, dz, A.vl[4]);
+  A.vl[5] = fmaf(uz, dz, A.vl[5]);
+}
+
+template <int TPA, bool HAS_EL, int LJM>
+__global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
+    CwP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
+    const int *__restrict__ cell_start, const int2 *__restrict__ cwn, const uint2 *__restrict__ cwl,
+    const float4 *__restrict__ gshift, const int *__restrict__ gmap, const float *__restrict__ gfcut,
+    const float4 *__restrict__ gtf, const float2 *__restrict__ gtg, const float4 *__restrict__ gtl,
+    double *__restrict__ fout, double *__restrict__ ipart, long long *__restrict__ stat,
+    const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  extern __shared__ float4 sm[];
+  // tables first (16-byte aligned), then the window
+  float4 *tf = sm;                                                    // ntable * rf
+  float2 *tg = reinterpret_cast<float2 *>(tf + (HAS_EL ? P.ntable * P.rf : 0));   // ntable * rg
+  // (an even number of float2, so that the next array starts on 16 bytes)
+  float4 *tl = reinterpret_cast<float4 *>(tg + (HAS_EL ? (P.ntable * P.rg + 1) / 2 * 2 : 0));   // 2 ninter ntable
+  const int nl = LJM ? 2 * P.ninter * P.ntable : 0;
+  float4 *wx = tl + nl;                                               // cap + 1 staged atoms
+  unsigned char *wt = reinterpret_cast<unsigned char *>(wx + P.cap + 1);   // LJM 2: their types
+  __shared__ int s_cs[27], s_cnt[27], s_off[27], s_tot;
+  __shared__ float4 s_shift[54];
+  __shared__ int s_map[256];
+  __shared__ float4 s_cut[64];                                        // LJM 2: {rc2, dx2, off, vt}
+  __shared__ double s_red[CW_THREADS / 32][CQ_COUNT];
+
+  for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = gshift[k];
+  if (HAS_EL)
+    for (int k = threadIdx.x; k < P.ntable * P.rf; k += blockDim.x) tf[k] = gtf[k / P.rf];
+  if (HAS_EL)
+    for (int k = threadIdx.x; k < P.ntable * P.rg; k += blockDim.x) tg[k] = gtg[k / P.rg];
+  for (int k = threadIdx.x; k < nl; k += blockDim.x) tl[k] = gtl[k];
+  if (LJM == 2) {
+    for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) s_map[k] = gmap[k];
+    for (int k = threadIdx.x; k < P.ninter; k += blockDim.x)
+      s_cut[k] = make_float4(gfcut[8 * k], gfcut[8 * k + 2], gfcut[8 * k + 1], gfcut[8 * k + 3]);
+  }
+  if (threadIdx.x == 0) {
+    wx[P.cap] = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);   // the dummy entry's partner: out of range
+    if (LJM == 2) wt[P.cap] = 0;
+  }
+  const int lane = threadIdx.x & 31;
+  const int g = threadIdx.x % TPA;
+  const int groups = CW_THREADS / TPA;
+  const float4 *tfl = tf + lane % P.rf;                 // this lane's table copies
+  const float2 *tgl = tg + lane % P.rg;
+  unsigned long long under = 0;
+
+  for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
+    const int c = item / P.nsplit, part = item - c * P.nsplit;
+    const int cz = c % P.ncz, cy = (c / P.ncz) % P.ncy, cx = c / (P.ncz * P.ncy);
+    __syncthreads();                                       // the previous window is no longer read
+    if (threadIdx.x < 32) {
+      const int w = threadIdx.x;
+      int cnt = 0, cs = 0;
+      if (w < 27) {
+        int jx = cx - (w / 9 - 1), jy = cy - ((w / 3) % 3 - 1), jz = cz - (w % 3 - 1);
+        jx = jx < 0 ? jx + P.ncx : (jx >= P.ncx ? jx - P.ncx : jx);
+        jy = jy < 0 ? jy + P.ncy : (jy >= P.ncy ? jy - P.ncy : jy);
+        jz = jz < 0 ? jz + P.ncz : (jz >= P.ncz ? jz - P.ncz : jz);
+        const int jc = (jx * P.ncy + jy) * P.ncz + jz;
+        cs = cell_start[jc];
+        cnt = cell_start[jc + 1] - cs;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (w >= o) incl += v;
+      }
+      if (w < 27) {
+        s_cs[w] = cs;
+        s_cnt[w] = cnt;
+        s_off[w] = incl - cnt;
+      }
+      if (w == 26) s_tot = incl;
+    }
+    __syncthreads();
+    // a window that does not fit was given empty lists by k_cw_convert
+    const bool staged = s_tot <= P.cap;
+    if (staged) {
+      for (int w = 0; w < 27; w++) {
+        const int cs = s_cs[w], cnt = s_cnt[w], off = s_off[w];
+        const float4 sh = s_shift[w], shl = s_shift[27 + w];
+        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
+          const float4 x = xq[cs + k];
+          wx[off + k] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
+          if (LJM == 2) wt[off + k] = (unsigned char)styp[cs + k];
+        }
+      }
+    }
+    __syncthreads();
+    double E[CQ_COUNT];
+#pragma unroll
+    for (int q = 0; q < CQ_COUNT; q++) E[q] = 0.0;
+    const int ci0 = s_cs[13], cin = s_cnt[13], ioff = s_off[13];
+    for (int r = part; r * groups < cin; r += P.nsplit) {
+      const int a = r * groups + threadIdx.x / TPA;
+      const bool active = staged && a < cin;
+      const int t = ci0 + (active ? a : 0);
+      CwAcc A;
+      cw_zero(A);
+      float pminl = 3.0e38f;
+      // an inactive lane group reads the dummy slot (its window may not exist)
+      const int ia = active ? ioff + a : P.cap;
+      const float4 xi = wx[ia];
+      const int ti = LJM == 2 ? wt[ia] : 0;
+      const int2 nn = active ? cwn[t] : make_int2(0, 0);
+      const int nba = (nn.x + CW_BLOCK - 1) / CW_BLOCK, nbb = (nn.y + CW_BLOCK - 1) / CW_BLOCK;
+      const uint2 *words = cwl + (size_t)t * P.words;
+      // blocks [0, nba) hold the LJ segment, [nba, nba + nbb) the electrostatics-only one
+      auto walk = [&](auto &&front_pair, auto &&back_pair) {
+        for (int b = 0; b < nba + nbb; b++) {
+          const bool front = b < nba;
+          const int m = front ? min(CW_BLOCK, nn.x - b * CW_BLOCK) : min(CW_BLOCK, nn.y - (b - nba) * CW_BLOCK);
+          const int rows = (m + CW_ROW - 1) / CW_ROW;
+#pragma unroll
+          for (int w0 = 0; w0 < CW_ROW; w0 += TPA) {
+            const uint2 v = __ldg(words + b * CW_ROW + w0 + g);
+            const uint32_t e[4] = {v.x & 0xFFFFu, v.x >> 16, v.y & 0xFFFFu, v.y >> 16};
+            if (front) {
+#pragma unroll
+              for (int k = 0; k < 4; k++)
+                if (k < rows) front_pair(e[k]);
+            } else {
+#pragma unroll
+              for (int k = 0; k < 4; k++)
+                if (k < rows) back_pair(e[k]);
+            }
+          }
+        }
+      };
+      auto geom = [&](uint32_t e, float4 &xj, float &dx, float &dy, float &dz) {
+        xj = wx[e & CW_IDX];
+        dx = xi.x - xj.x;
+        dy = xi.y - xj.y;
+        dz = xi.z - xj.z;
+        return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      };
+      auto lj_pair = [&](uint32_t e, float dx, float dy, float dz, float r2, float &pm, CwAcc &Acc) {
+        if (LJM == 1) {
+          cw_lj(P, dx, dy, dz, r2, P.rc2_l, P.dx2l, P.offl, P.vtl, tl, pm, Acc);
+        } else if (LJM == 2) {
+          const int tj = wt[e & CW_IDX];
+          const int in = s_map[ti * P.ntypes + tj];
+          const float4 cut = s_cut[in < 0 ? 0 : in];
+          // a pair without an LJ interaction (map -1) never reaches the LJ
+          // segment; a dummy may, with an out-of-range distance
+          cw_lj(P, dx, dy, dz, in < 0 ? 3.0e38f : r2, cut.x, cut.y, cut.z, cut.w,
+                tl + (size_t)2 * (in < 0 ? 0 : in) * P.ntable, pm, Acc);
+        }
+      };
+      walk(
+          [&](uint32_t e) {
+            float4 xj;
+            float dx, dy, dz;
+            const float r2 = geom(e, xj, dx, dy, dz);
+            if (HAS_EL) cw_elec<true>(P, xj, dx, dy, dz, r2, (e & CW_EL) != 0, tfl, tgl, A);
+            lj_pair(e, dx, dy, dz, r2, pminl, A);
+          },
+          [&](uint32_t e) {
+            if (HAS_EL) {
+              float4 xj;
+              float dx, dy, dz;
+              const float r2 = geom(e, xj, dx, dy, dz);
+              cw_elec<false>(P, xj, dx, dy, dz, r2, true, tfl, tgl, A);
+            }
+          });
+      // CM3D's table underflow (k < 1) is counted per pair; the walk only
+      // tracks the smallest table coordinate, and an atom with an underflow
+      // (none in a sane system) is walked again to count them
+      if (active && (A.pmin < 1.f || pminl < 1.f)) {
+        CwAcc B;
+        cw_zero(B);
+        unsigned cnt = 0;
+        walk(
+            [&](uint32_t e) {
+              float4 xj;
+              float dx, dy, dz;
+              const float r2 = geom(e, xj, dx, dy, dz);
+              if (HAS_EL) {
+                const bool ok = (e & CW_EL) && r2 < P.rc2_el;
+                cnt += (ok && fmaf(r2, P.dx2c, -P.offc) < 1.f) ? 1u : 0u;
+              }
+              float pm2 = 3.0e38f;
+              lj_pair(e, dx, dy, dz, r2, pm2, B);
+              cnt += pm2 < 1.f ? 1u : 0u;
+            },
+            [&](uint32_t e) {
+              if (HAS_EL) {
+                float4 xj;
+                float dx, dy, dz;
+                const float r2 = geom(e, xj, dx, dy, dz);
+                cnt += (r2 < P.rc2_el && fmaf(r2, P.dx2c, -P.offc) < 1.f) ? 1u : 0u;
+              }
+            });
+        under += cnt;
+      }
+      // forces: F_i = -(qi sum qj f d + sum f_lj d), the chunk in FP64 and
+      // summed over the atom's lanes
+      const double qi = (double)xi.w;
+      double Fx = -(qi * (double)A.fx + (double)A.gx);
+      double Fy = -(qi * (double)A.fy + (double)A.gy);
+      double Fz = -(qi * (double)A.fz + (double)A.gz);
+#pragma unroll
+      for (int o = TPA / 2; o > 0; o >>= 1) {
+        Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+        Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+        Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+      }
+      if (active && g == 0) {
+        const int i = sorig[t], n = P.n;
+        fout[i] += Fx;
+        fout[n + i] += Fy;
+        fout[2 * n + i] += Fz;
+      }
+      if (active) {
+        E[CQ_EEL] += qi * (double)A.eel;
+        E[CQ_QQ] += qi * (double)A.qs;
+#pragma unroll
+        for (int k = 0; k < 6; k++) E[CQ_VE0 + k] += qi * (double)A.ve[k];
+        E[CQ_ELJ] += A.elj_hi + (double)A.elo;
+        E[CQ_VSH] += (double)A.vsh;
+#pragma unroll
+        for (int k = 0; k < 6; k++) E[CQ_VL0 + k] += (double)A.vl[k];
+      }
+    }
+    // the item's sums: warps, then the block, in a fixed order
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < CQ_COUNT; q++) {
+      const double v = warp_sum(E[q]);
+      if (lane == 0) s_red[warp][q] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < CQ_COUNT) {
+      double s = 0.0;
+      for (int w = 0; w < CW_THREADS / 32; w++) s += s_red[w][threadIdx.x];
+      ipart[(size_t)item * CQ_COUNT + threadIdx.x] = s;
+    }
+  }
+  if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), under);
+}
+
+// Sum of the items' partials into CM3D's accumulators: one block, warp q
+// sums quantity q over the items (fixed order), then one thread applies the
+// sums in a fixed order (several quantities feed one accumulator); each pair
+// was counted from both ends, hence 1/2.
+__global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce(int nitems, int mask, double tablast_e,
+                                                               const double *__restrict__ ipart,
+                                                               double *__restrict__ acc, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  __shared__ double s_q[CQ_COUNT];
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int it = lane; it < nitems; it += 32) s += ipart[(size_t)it * CQ_COUNT + q];
+  s = warp_sum(s);
+  if (lane == 0) s_q[q] = 0.5 * s;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  const double *v = s_q;
+  if (mask & 2) {
+    acc[ACC_SPOTE] += v[CQ_EEL];
+    acc[ACC_SPOTHE] += v[CQ_EEL] - tablast_e * v[CQ_QQ];
+    acc[ACC_SPRSE] -= v[CQ_VE0] + v[CQ_VE4] + v[CQ_VE8];
+    acc[ACC_SPRSET + 0] -= v[CQ_VE0];
+    acc[ACC_SPRSET + 1] -= v[CQ_VE1];
+    acc[ACC_SPRSET + 2] -= v[CQ_VE2];
+    acc[ACC_SPRSET + 4] -= v[CQ_VE4];
+    acc[ACC_SPRSET + 5] -= v[CQ_VE5];
+    acc[ACC_SPRSET + 8] -= v[CQ_VE8];
+  }
+  if (mask & 1) {
+    acc[ACC_SPOTL] += v[CQ_ELJ];
+    acc[ACC_SPOTHL] += v[CQ_ELJ] - v[CQ_VSH];
+    acc[ACC_SPRSL] -= v[CQ_VL0] + v[CQ_VL4] + v[CQ_VL8];
+    acc[ACC_SPRSLT + 0] -= v[CQ_VL0];
+    acc[ACC_SPRSLT + 1] -= v[CQ_VL1];
+    acc[ACC_SPRSLT + 2] -= v[CQ_VL2];
+    acc[ACC_SPRSLT + 4] -= v[CQ_VL4];
+    acc[ACC_SPRSLT + 5] -= v[CQ_VL5];
+    acc[ACC_SPRSLT + 8] -= v[CQ_VL8];
+  }
+}
+
+// ------------------------------------------------------------------ host
+static size_t cw_table_bytes(const Ctx *c, int rf, int rg, int ljm) {
+  size_t b = 0;
+  if (c->ncharge > 0)
+    b += (size_t)c->ntable * rf * sizeof(float4) + ((size_t)c->ntable * rg + 1) / 2 * 2 * sizeof(float2);
+  if (ljm) b += (size_t)2 * c->ninter * c->ntable * sizeof(float4);
+  return b;
+}
+
+static int cw_ljm(const Ctx *c) {
+  if (c->ninter == 0) return 0;
+  return c->ninter == 1 ? 1 : 2;
+}
+
+// Whether the compact path can run this context, and its tables and window
+// size: one system, at least 3 cells per axis, the full force level without
+// the RESPA switch copy, a window of the mean size (x 1.25, + 64) next to the
+// tables in the shared memory a block may use.  Table copies are reduced
+// (8, 4, 2, 1) until it fits.
+int cw_setup(Ctx *c) {
+  c->cw_ok = 0;
+  if (c->mode != CM3D_NB_MIXED || c->nsys != 1) return CM3D_NB_OK;
+  if (c->nc[0] < 3 || c->nc[1] < 3 || c->nc[2] < 3) return CM3D_NB_OK;
+  if (c->need_short || c->nres_lrf > 1) return CM3D_NB_OK;
+  if (c->ntypes > 16 || c->ninter > 64) return CM3D_NB_OK;       // static map / cut-off arrays
+  const char *pk = getenv("CM3D_NB_PAIR_KERNEL");
+  if (pk && (strcmp(pk, "list") == 0 || strcmp(pk, "window") == 0)) return CM3D_NB_OK;
+  const int ljm = cw_ljm(c);
+  const double mean_window = 27.0 * (double)c->n / (double)c->ncells;
+  const size_t want_cap = (size_t)(1.25 * mean_window) + 64;
+  const size_t budget = c->smem_optin > CW_STATIC_SMEM ? c->smem_optin - CW_STATIC_SMEM : 0;
+  const size_t per_slot = sizeof(float4) + (ljm == 2 ? 1 : 0);
+  int rf = 8, rg = 8;
+  for (;;) {
+    const size_t tb = cw_table_bytes(c, rf, rg, ljm);
+    if (tb + (want_cap + 1) * per_slot + 16 <= budget) break;
+    if (rf == 1 && rg == 1) return CM3D_NB_OK;
+    if (rg > 1) rg /= 2;
+    else rf /= 2;
+  }
+  const size_t tb = cw_table_bytes(c, rf, rg, ljm);
+  long long cap = (long long)((budget - tb - 16) / per_slot) - 1;
+  cap = std::min<long long>(cap, CW_MAX_CAP);
+  // CM3D_NB_CW_CAP lowers the window capacity (tests of the fall-back)
+  const char *ce = getenv("CM3D_NB_CW_CAP");
+  if (ce && atoi(ce) > 0) cap = std::min<long long>(cap, atoi(ce));
+  c->cw_rf = rf;
+  c->cw_rg = rg;
+  c->cw_cap = (int)cap;
+  c->cw_smem = tb + ((size_t)cap + 1) * sizeof(float4) + (ljm == 2 ? (size_t)cap + 1 : 0);
+  c->cw_smem = (c->cw_smem + 15) / 16 * 16;
+  // slot: each segment rounded up to whole blocks
+  const long long blocks = (c->nbr_stride + CW_BLOCK - 1) / CW_BLOCK + 1;
+  c->cw_words = (int)(blocks * CW_ROW);
+  CK(cudaMalloc(&c->cwl, sizeof(uint2) * (size_t)c->n * (size_t)c->cw_words));
+  CK(cudaMalloc(&c->cwn, sizeof(int2) * (size_t)c->n));
+  CK(cudaMemset(c->cwn, 0, sizeof(int2) * (size_t)c->n));
+  // tables: erfc force coefficients + base energy, energy slope/curvature;
+  // LJ 2 float4 per knot (the compact layout of nb_pair.cu's batch tables)
+  const int nt = c->ntable;
+  if (c->ncharge > 0) {
+    std::vector<double> ct(nt), dct(nt);
+    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    std::vector<float4> tf(nt, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<float2> tg(nt, make_float2(0.f, 0.f));
+    for (int k = 1; k <= nt - 2; k++) {
+      const double d0 = dct[k], da = 0.5 * (dct[k + 1] - dct[k - 1]),
+                   db = 0.5 * (dct[k - 1] - 2.0 * dct[k] + dct[k + 1]);
+      const double v0 = ct[k], va = 0.5 * (ct[k + 1] - ct[k - 1]), vb = 0.5 * (ct[k - 1] - 2.0 * ct[k] + ct[k + 1]);
+      tf[k] = make_float4((float)d0, (float)da, (float)db, (float)v0);
+      tg[k] = make_float2((float)va, (float)vb);
+    }
+    CK(cudaMalloc(&c->cw_tf, sizeof(float4) * nt));
+    CK(cudaMalloc(&c->cw_tg, sizeof(float2) * nt));
+    CK(cudaMemcpy(c->cw_tf, tf.data(), sizeof(float4) * nt, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->cw_tg, tg.data(), sizeof(float2) * nt, cudaMemcpyHostToDevice));
+  }
+  if (ljm) {
+    const int ni = c->ninter;
+    std::vector<double> vt((size_t)ni * nt), dv((size_t)ni * nt), cut(8 * (size_t)ni);
+    CK(cudaMemcpy(vt.data(), c->vtab, sizeof(double) * vt.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dv.data(), c->dvtab, sizeof(double) * dv.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cut.data(), c->icut, sizeof(double) * cut.size(), cudaMemcpyDeviceToHost));
+    std::vector<float4> tl((size_t)2 * ni * nt, make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int in = 0; in < ni; in++)
+      for (int k = 1; k <= nt - 2; k++) {
+        const double *d = &dv[(size_t)in * nt], *v = &vt[(size_t)in * nt];
+        const double d0 = d[k], da = 0.5 * (d[k + 1] - d[k - 1]), db = 0.5 * (d[k - 1] - 2.0 * d[k] + d[k + 1]);
+        const double v0 = v[k], va = 0.5 * (v[k + 1] - v[k - 1]), vb = 0.5 * (v[k - 1] - 2.0 * v[k] + v[k + 1]);
+        // v0 as hi + lo: the kernel sums the hi parts in FP64
+        const float hi = (float)v0;
+        tl[2 * ((size_t)in * nt + k)] = make_float4((float)d0, (float)da, (float)db, hi);
+        tl[2 * ((size_t)in * nt + k) + 1] = make_float4((float)va, (float)vb, (float)(v0 - (double)hi), 0.f);
+      }
+    CK(cudaMalloc(&c->cw_tl, sizeof(float4) * tl.size()));
+    CK(cudaMemcpy(c->cw_tl, tl.data(), sizeof(float4) * tl.size(), cudaMemcpyHostToDevice));
+    if (ljm == 1) {
+      const double *q = &cut[0];
+      c->cw_lj1[0] = (float)q[2];           // rmaxl_cut2
+      c->cw_lj1[1] = (float)q[6];           // dx2tab
+      c->cw_lj1[2] = (float)(q[1] * q[6]);  // rmins_cut2 * dx2tab
+      c->cw_lj1[3] = (float)q[7];           // vtab[ntable - 4]
+    }
+  }
+  // work items: cells, split into parts where the cells are fewer than four
+  // per SM (each part stages its cell's window again)
+  const int want = (4 * c->num_sms + c->ncells - 1) / c->ncells;
+  c->cw_nsplit = std::max(1, std::min(want, 8));
+  c->cw_nitems = c->ncells * c->cw_nsplit;
+  CK(cudaMalloc(&c->cw_part, sizeof(double) * CQ_COUNT * (size_t)c->cw_nitems));
+  c->cw_ok = 1;
+  c->cw_use = 1;
+  return CM3D_NB_OK;
+}
+
+// after a (gated) rebuild of the master list: the compact list
+int cw_convert(Ctx *c, bool device_flag) {
+  if (!c->cw_ok) return CM3D_NB_OK;
+  // the master slots widen on overflow (host-driven builds only): so do ours
+  const int words = (int)(((c->nbr_stride + CW_BLOCK - 1) / CW_BLOCK + 1) * CW_ROW);
+  if (words > c->cw_words) {
+    CK(cudaStreamSynchronize(c->st));
+    cudaFree(c->cwl);
+    c->cwl = nullptr;
+    CK(cudaMalloc(&c->cwl, sizeof(uint2) * (size_t)c->n * (size_t)words));
+    c->cw_words = words;
+    if (c->graph) {
+      cudaGraphExecDestroy(c->graph);
+      c->graph = nullptr;
+    }
+  }
+  const int *gate = device_flag ? c->istate : nullptr;
+  const int grid = std::min(c->ncells, c->num_sms * 8);
+  k_cw_convert<<<grid, 256, 0, c->st>>>(c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n, c->cw_words, c->cell_start,
+                                        c->nlen, c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat,
+                                        device_flag ? c->istate + IS_HALT : nullptr, gate);
+  c->launches++;
+  CKL(c);
+  if (!device_flag) {
+    // a host-driven build: a window that did not fit turns the compact path
+    // off for this context (the gather/window kernels read the master list)
+    CK(cudaMemcpyAsync(c->h_stat, c->stat, sizeof(long long) * ST_COUNT, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_stat[ST_CWIN] > 0) {
+      c->cw_ok = 0;
+      c->cw_use = 0;
+      long long zero = 0;
+      CK(cudaMemcpy(c->stat + ST_CWIN, &zero, sizeof(long long), cudaMemcpyHostToDevice));
+    }
+  }
+  return CM3D_NB_OK;
+}
+
+template <int TPA, bool EL, int LJM>
+static void cw_launch_t(Ctx *c, const CwP &P, double *fout) {
+  auto kern = k_pair_cw<TPA, EL, LJM>;
+  static unsigned long long attr_devs = 0;
+  if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(c->smem_optin - CW_STATIC_SMEM));
+    attr_devs |= 1ull << c->dev;
+  }
+  const int grid = std::min(P.nitems, c->num_sms);
+  kern<<<grid, CW_THREADS, c->cw_smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl,
+                                                 c->shift, c->map, c->fcut, c->cw_tf, c->cw_tg, c->cw_tl, fout,
+                                                 c->cw_part, c->stat, c->gate);
+}
+
+template <bool EL, int LJM>
+static void cw_launch_tpa(Ctx *c, const CwP &P, double *fout) {
+  switch (c->tpa) {
+    case 8: cw_launch_t<8, EL, LJM>(c, P, fout); break;
+    case 16: cw_launch_t<16, EL, LJM>(c, P, fout); break;
+    default: cw_launch_t<32, EL, LJM>(c, P, fout); break;
+  }
+}
+
+bool cw_applies(Ctx *c, int iflg, bool ns) { return c->cw_ok && c->cw_use && iflg == 1 && !ns; }
+
+// full force level of one system through the compact path (the caller
+// checked cw_applies); mask bit0 LJ, bit1 charges
+int cw_pairs(Ctx *c, int mask, double *fout) {
+  CwP P;
+  P.n = c->n;
+  P.ncx = c->nc[0];
+  P.ncy = c->nc[1];
+  P.ncz = c->nc[2];
+  P.nsplit = c->cw_nsplit;
+  P.nitems = c->cw_nitems;
+  P.cap = c->cw_cap;
+  P.words = c->cw_words;
+  P.ntable = c->ntable;
+  P.ntypes = c->ntypes;
+  P.ninter = c->ninter;
+  P.rf = c->cw_rf;
+  P.rg = c->cw_rg;
+  P.rc2_el = (float)c->rmaxl_coul2;
+  P.dx2c = (float)c->dx2coul;
+  P.offc = (float)(c->rmins_coul2 * c->dx2coul);
+  P.pmax = (float)(c->ntable - 3);
+  P.rc2_l = c->cw_lj1[0];
+  P.dx2l = c->cw_lj1[1];
+  P.offl = c->cw_lj1[2];
+  P.vtl = c->cw_lj1[3];
+  const bool el = (mask & 2) != 0;
+  const int ljm = (mask & 1) ? cw_ljm(c) : 0;
+  if (el) {
+    if (ljm == 0) cw_launch_tpa<true, 0>(c, P, fout);
+    else if (ljm == 1) cw_launch_tpa<true, 1>(c, P, fout);
+    else cw_launch_tpa<true, 2>(c, P, fout);
+  } else {
+    if (ljm == 1) cw_launch_tpa<false, 1>(c, P, fout);
+    else if (ljm == 2) cw_launch_tpa<false, 2>(c, P, fout);
+  }
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int cw_ereduce(Ctx *c, int mask) {
+  k_cw_ereduce<<<1, CQ_COUNT * 32, 0, c->st>>>(c->cw_nitems, mask, c->tablast_e, c->cw_part, c->acc, c->gate);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+}  // namespace cm3d

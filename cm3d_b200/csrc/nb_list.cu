@@ -1099,6 +1099,10 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
       if (rc) return rc;
     }
   }
+  if (c->mode == CM3D_NB_MIXED) {
+    int rc = cw_convert(c, device_flag);
+    if (rc) return rc;
+  }
   if (want_half) {
     k_list_half<false><<<grid_for(warps_threads, 256), 256, 0, c->st>>>(
         n, c->sp, c->sys_of, caps(c), c->cell_atoms, c->cell_start, c->xq, c->pos, c->itype, c->map, c->icut,

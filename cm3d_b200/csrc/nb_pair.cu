@@ -1070,6 +1070,16 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
                                                   c->gate);
   cudaEvent_t e0;
   tbegin(c, 0, &e0);
+  if (cw_applies(c, iflg, ns)) {
+    // one system with >= 3 cells per axis, full force level: the compact
+    // window list (nb_cwin.cu) and its own energy sums
+    c->pair_used = CM3D_NB_PAIR_COMPACT;
+    int rc = cw_pairs(c, mask, fout);
+    tend(c, 0, e0);
+    c->launches++;
+    if (rc) return rc;
+    return cw_ereduce(c, mask);
+  }
   // one system with >= 3 cells per axis: staged 27-cell windows; anything
   // else (batches, coarse cell grids): the gather kernel
   c->pair_used = CM3D_NB_PAIR_WINDOW;

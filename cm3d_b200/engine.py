@@ -277,10 +277,10 @@ class Engine:
                 "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
 
     def pair_kernel(self) -> tuple[str, int]:
-        """(kernel of the last pair launch: "gather", "window" or "system", lanes per atom)"""
+        """(kernel of the last pair launch: "gather", "window", "system" or "compact", lanes per atom)"""
         k, t = C.c_int(0), C.c_int(0)
         check(load_library().cm3d_nb_pair_kernel(self._h, C.byref(k), C.byref(t)), "pair_kernel")
-        return {0: "gather", 1: "window", 2: "system"}[k.value], int(t.value)
+        return {0: "gather", 1: "window", 2: "system", 3: "compact"}[k.value], int(t.value)
 
     def system_energies(self, sys: int) -> dict:
         """getvireal + geteng of one system of a batch"""

@@ -342,7 +342,11 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
    j-atoms from global memory; any context can run it.  WINDOW: one system
    with >= 3 cells per axis; a block stages the 27 cells around an i-cell in
    shared memory.  SYSTEM: a batch whose largest system fits in shared memory;
-   a block stages the whole system it works on.  cm3d_nb_autotune times the
+   a block stages the whole system it works on.  COMPACT: one system with >= 3
+   cells per axis at the full force level (no RESPA switch copy); its list is
+   rewritten after each rebuild as 16-bit indices into the i-cell's staged
+   27-cell window, and its tables are replicated across the shared-memory
+   banks.  CM3D_NB_PAIR_KERNEL=window keeps a context off the compact kernel.  cm3d_nb_autotune times the
    gather kernel and the staged one that applies at every lanes-per-atom
    choice, keeps the fastest, and ms_per_launch[k] is the faster at that
    choice.  CM3D_NB_PAIR_KERNEL=list in the environment at cm3d_nb_create
@@ -351,6 +355,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
 #define CM3D_NB_PAIR_GATHER 0
 #define CM3D_NB_PAIR_WINDOW 1
 #define CM3D_NB_PAIR_SYSTEM 2
+#define CM3D_NB_PAIR_COMPACT 3
 int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
 
 /* ------------------------------------------- no-allocation variant */

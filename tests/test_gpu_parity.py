@@ -220,13 +220,14 @@ def test_window_kernel_matches_list_kernel(engine_lib, name, monkeypatch):
     d = golden(name)
     out = {}
     for kind in ("window", "list"):
-        if kind == "list":
-            monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", "list")
-        else:
-            monkeypatch.delenv("CM3D_NB_PAIR_KERNEL", raising=False)
+        # (a lone system with >= 3 cells per axis would otherwise take the
+        # compact-window kernel, tests/test_compact.py)
+        monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", kind)
         e = Engine(System.from_arrays(d), mode=_abi.MIXED)
+        monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
         e.get_ngbr()
         e.force(1)
+        assert e.pair_kernel()[0] == {"window": "window", "list": "gather"}[kind]
         out[kind] = (e.forces(_abi.FXL), e.energies())
         e.close()
     fs = force_scale(d) / float(np.sqrt((d["amass"] ** 2).mean()))
