@@ -262,44 +262,65 @@ def ref_bench_bin() -> str | None:
     return p if os.path.exists(p) else None
 
 
-def cpu_steps(natoms: int, charged: bool) -> int:
-    # ~10-20 s of CM3D on one core: LJ runs near 4e5 atom-steps/s, Ewald
-    # systems near 3.5e4
-    rate = 3.0e4 if charged else 3.0e5
-    return max(2, min(2000, int(12.0 * rate / max(natoms, 1))))
+def cpu_cost(wl) -> float:
+    """estimated seconds of one CM3D step of a workload's system on one core
+    (fit to ref_bench timings of 96 ensemble boxes: t = n (0.63 + 41 rho) us
+    for LJ boxes, n (443 rho) us for charged Ewald boxes, rho = n / V in
+    atoms per A^3; the water boxes fall near the charged line)"""
+    rho = wl.natoms / float(wl.box) ** 3
+    charged = "kmax" in wl.keywords
+    return wl.natoms * ((443.0 * rho) if charged else (0.63 + 41.4 * rho)) * 1e-6
 
 
-def cpu_reference(wls, procs: int) -> dict:
-    """CM3D itself on the host: `procs` processes, each running one system of
-    the workload (a sample spread over the ensemble) for a bounded number of
-    steps of CM3D's step() after its own start-up; aggregate atom-steps/s over
-    the longest process time."""
+def cpu_bounded_steps(wls, cores: int, steps: int, budget_s: float = 30.0) -> int:
+    """the timed steps of a CPU run: `steps`, fewer where the workload's
+    estimated step time on `cores` cores (one system per core, cpu_cost)
+    would make them take longer than budget_s"""
+    per_core = sorted((cpu_cost(w) for w in wls), reverse=True)
+    est = max(sum(per_core) / max(1, min(cores, len(wls))), per_core[0])
+    return max(1, min(steps, int(budget_s / max(est, 1e-9))))
+
+
+def run_deck(exe: str, inp: str, steps: int, warmup: int) -> dict:
+    """CM3D's start-up, `warmup` untimed and `steps` timed iterations of its
+    MD loop body in one process (ref_bench); its JSON line"""
+    out = subprocess.run([exe, os.path.basename(inp), str(steps), str(warmup)], cwd=os.path.dirname(inp),
+                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, check=True).stdout
+    return json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
+
+
+def cpu_reference(wls, cores: int, steps: int, warmup: int) -> dict:
+    """CM3D itself (oracle/_ref/ref_bench, built from its sources with gcc
+    -O2) on the host cores over the whole workload: every system runs
+    `warmup` untimed and then `steps` timed iterations of CM3D's MD loop
+    body (main/md_mdcntr.new.c:176-178), one process per system (CM3D is
+    single-threaded), `cores` processes at any moment from a queue ordered
+    by estimated cost, so every core stays busy until the queue runs dry.
+    Each process times its own steps.  value = all atom-steps / (the timed
+    seconds of all processes / cores): the rate of `cores` cores that do
+    nothing but CM3D steps (start-up and the queue's tail excluded, which
+    favours the CPU)."""
+    import concurrent.futures as cf
     exe = ref_bench_bin()
-    pick = np.linspace(0, len(wls) - 1, num=min(procs, len(wls))).round().astype(int)
-    if len(wls) == 1:
-        pick = np.zeros(procs, int)
+    order = sorted(range(len(wls)), key=lambda k: -cpu_cost(wls[k]))
+    cores = max(1, min(cores, len(wls)))
+    t0 = time.perf_counter()
     with tempfile.TemporaryDirectory() as tmp:
-        jobs = []
-        for p, k in enumerate(pick):
-            wl = wls[int(k)]
-            d = os.path.join(tmp, f"r{p}")
-            inp = wl.write(d)
-            steps = cpu_steps(wl.natoms, "kmax" in wl.keywords)
-            jobs.append(subprocess.Popen([exe, os.path.basename(inp), str(steps)], cwd=d,
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True))
-        res = []
-        for j in jobs:
-            out, _ = j.communicate()
-            line = [ln for ln in out.splitlines() if ln.startswith("{")][-1]
-            res.append(json.loads(line))
-    tmax = max(r["seconds"] for r in res)
+        decks = {k: wls[k].write(os.path.join(tmp, f"s{k}")) for k in order}
+        with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+            res = list(ex.map(lambda k: run_deck(exe, decks[k], steps, warmup), order))
+    elapsed = time.perf_counter() - t0
+    busy = sum(r["seconds"] for r in res)
     total = sum(r["natoms"] * r["steps"] for r in res)
     natoms = sum(r["natoms"] for r in res)
-    return {"value": total / tmax, "unit": UNIT, "cores": len(res), "kind": "reference",
-            "sample": f"{len(res)} host processes, each CM3D step() (oracle/_ref/ref_bench, gcc -O2) on one "
-                      f"system of the workload ({natoms} atoms in all) for a bounded number of steps after "
-                      f"its start-up; value = their atom-steps / the longest process time",
-            "single_process_mean": float(np.mean([r["atom_steps_per_s"] for r in res]))}
+    return {"value": total / (busy / cores), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"the whole workload ({len(wls)} systems, {natoms} atoms), {warmup} untimed + {steps} timed "
+                      f"steps each of CM3D's MD loop body (oracle/_ref/ref_bench, gcc -O2), one process per "
+                      f"system, {cores} at a time from a queue; value = atom-steps / (summed timed seconds / "
+                      f"{cores} cores)",
+            "steps": steps, "warmup": warmup, "timed_core_s": busy,
+            "elapsed_s_with_startup": elapsed, "atom_steps": total,
+            "single_core_rate": total / busy}
 
 
 def cpu_port(systems, steps: int) -> dict:
@@ -342,8 +363,8 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
     import torch
     from cm3d_b200 import _abi
     from cm3d_b200.engine import Engine
-    if pin and pin[1] == "gather":
-        os.environ["CM3D_NB_PAIR_KERNEL"] = "list"
+    if pin and pin[1] in ("gather", "staged"):
+        os.environ["CM3D_NB_PAIR_KERNEL"] = "list" if pin[1] == "gather" else "window"
     eng = Engine(systems, mode=_abi.MIXED, device=device, tpa=pin[0] if pin else 0)
     if pin:
         os.environ.pop("CM3D_NB_PAIR_KERNEL", None)
@@ -441,7 +462,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--tpa", type=int, default=0, choices=[0, 4, 8, 16, 32],
                     help="pin the pair kernel's lanes per atom instead of autotuning (profiling runs)")
-    ap.add_argument("--pair-kernel", default="gather", choices=["gather", "staged"],
+    ap.add_argument("--pair-kernel", default="gather", choices=["gather", "staged", "compact"],
                     help="with --tpa: the pair kernel to pin")
     ap.add_argument("--partition", action="store_true",
                     help="N > 1: split one ensemble over the ranks (LPT on the cost model, strong scaling) "
@@ -460,14 +481,15 @@ def main() -> None:
         steps = args.steps if args.steps is not None else dsteps
         warmup = args.warmup if args.warmup is not None else 20
         procs = max(1, min(os.cpu_count() or 1, 64))
+        rsteps = cpu_bounded_steps(wls, procs, steps)
         if ref_bench_bin():
-            base = cpu_reference(wls, procs)
+            base = cpu_reference(wls, procs, rsteps, min(warmup, rsteps))
         else:
             from cm3d_b200.setup import build_system
-            base = cpu_port([build_system(wls[0])], 20)
+            base = cpu_port([build_system(wls[0])], rsteps)
         natoms = sum(w.natoms for w in wls)
         line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
-                "n_gpus": args.gpus, "steps": steps, "warmup": warmup,
+                "n_gpus": args.gpus, "steps": rsteps, "warmup": min(warmup, rsteps),
                 "ms_per_step": 1e3 * natoms / base["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": {"workload": desc, "natoms": natoms,
@@ -558,8 +580,10 @@ def main() -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = (cpu_reference(wls, max(1, min(os.cpu_count() or 1, 64))) if ref_bench_bin()
-               else cpu_port(systems, 20))
+        cores = max(1, min(os.cpu_count() or 1, 64))
+        csteps = cpu_bounded_steps(wls, cores, 10)
+        cpu = (cpu_reference(wls, cores, csteps, min(2, csteps)) if ref_bench_bin()
+               else cpu_port(systems, csteps))
 
     if rank == 0:
         dt_ps = float(systems[0]["dt"])

@@ -11,7 +11,9 @@
  *   {"natoms": N, "steps": S, "seconds": T, "atom_steps_per_s": N*S/T,
  *    "poter": U}
  *
- * usage:  ref_bench <cm3d input file> <nsteps>   (run from the deck's directory)
+ * usage:  ref_bench <cm3d input file> <nsteps> [warmup]
+ *         (run from the deck's directory; warmup: untimed loop iterations
+ *         before the timed ones, default 0)
  */
 #include <time.h>
 
@@ -27,7 +29,7 @@ int main(int argc, char *argv[])
   NGBR ngbr;
   INTER inter;
   ENERGIES energies;
-  int s, nsteps;
+  int s, nsteps, warmup;
   struct timespec t0, t1;
   double sec;
 
@@ -36,6 +38,7 @@ int main(int argc, char *argv[])
     return 2;
   }
   nsteps = atoi(argv[2]);
+  warmup = argc > 3 ? atoi(argv[3]) : 0;
   memset(&simparms, 0, sizeof simparms);
   memset(&filenames, 0, sizeof filenames);
   memset(&coords, 0, sizeof coords);
@@ -58,6 +61,11 @@ int main(int argc, char *argv[])
   gethinv9(coords.hmat, coords.hmati);
   step_init(&simparms, &coords, &energies, &inter, &ngbr);
   simparms.istep = 1;
+  for (s = 0; s < warmup; s++, simparms.istep++) {
+    step(&simparms, &coords, &energies, &inter, &ngbr);
+    geteng(&simparms, &coords, &energies);
+    gettngbr(&ngbr);
+  }
   clock_gettime(CLOCK_MONOTONIC, &t0);
   for (s = 0; s < nsteps; s++, simparms.istep++) {
     step(&simparms, &coords, &energies, &inter, &ngbr);
