@@ -1118,7 +1118,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
     c->win_ok = kind == 1;
     c->cw_use = kind == 2;
     for (int k = 0; k < 4; k++) {
-      if (kind == 2 && cand[k] < 8) continue;        // the compact kernel runs 8, 16 or 32 lanes per atom
+      if (kind == 2 && cand[k] != 32) continue;      // the compact kernel runs a warp per atom
       c->tpa = cand[k];
       if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
       CK(cudaEventRecord(a, c->st));

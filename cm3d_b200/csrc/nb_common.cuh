@@ -240,7 +240,6 @@ struct Ctx {
   // compact-window pair path (nb_cwin.cu): one system, >= 3 cells per axis
   int cw_ok = 0;                       // set up and valid for this context
   int cw_use = 0;                      // preferred over the window/gather kernels (autotuner)
-  int cw_rf = 1, cw_rg = 1;            // table copies in shared memory
   int cw_cap = 0;                      // window slots
   size_t cw_smem = 0;                  // dynamic shared memory of k_pair_cw
   int cw_words = 0;                    // 8-byte words per atom slot of the compact list

@@ -56,15 +56,19 @@ constexpr int CW_MAX_CAP = 16382;           // window slots (the dummy slot `cap
 constexpr float CW_MAGIC = 12582912.0f;     // 1.5 * 2^23: p + MAGIC rounded toward zero holds floor(p)
 constexpr unsigned CW_MAGIC_BITS = 0x4B400000u;
 constexpr int CW_STATIC_SMEM = 6144;        // >= the kernel's static shared arrays (5.2 KB)
+constexpr int CW_RF = 8;                    // copies of the erfc force table (lane l reads copy l % 8)
+constexpr int CW_RG = 8;                    // copies of the erfc energy table
 
 // per-item FP64 sums (each pair is seen from both ends: k_cw_ereduce halves)
-enum { CQ_EEL = 0, CQ_QQ, CQ_VE0, CQ_VE1, CQ_VE2, CQ_VE4, CQ_VE5, CQ_VE8,
+enum { CQ_EEL = 0, CQ_QQ_UNUSED, CQ_VE0, CQ_VE1, CQ_VE2, CQ_VE4, CQ_VE5, CQ_VE8,
        CQ_ELJ, CQ_VSH, CQ_VL0, CQ_VL1, CQ_VL2, CQ_VL4, CQ_VL5, CQ_VL8, CQ_COUNT };
 
 struct CwP {
   int n, ncx, ncy, ncz, nitems, nsplit, cap, words;   // words: 8-byte words per atom slot
-  int ntable, ntypes, ninter, rf, rg;
+  int ntable, ntypes, ninter;
   float rc2_el, dx2c, offc, pmax;
+  float sat_a, sat_b;        // dx2 / pmax, -rmin^2 dx2 / pmax: the saturated table coordinate
+  float r2under;             // r^2 below which the erfc table underflows (p < 1)
   // one LJ interaction (LJM 1): cut-off^2, dx2tab, rmins_cut2 * dx2tab, vtab[ntable-4]
   float rc2_l, dx2l, offl, vtl;
 };
@@ -153,26 +157,36 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
 
 // ------------------------------------------------------------------
 // Pair kernel.  Block per work item (a cell, or one of `nsplit` parts of
-// its atoms); the block stages the cell's window and then walks the item's
-// atoms with TPA lanes per atom.
+// its atoms); the block stages the cell's window, then each warp takes one
+// i-atom at a time and its 32 lanes walk the atom's list blocks (every
+// branch is warp-uniform).  The next two blocks' list words are loaded
+// while a block is being evaluated.
 //   HAS_EL: the system has charges; LJM: 0 no LJ, 1 one LJ interaction (its
 //   parameters in CwP), 2 several (type map, cut-offs and tables per pair).
+//
+// Electrostatic table lookup without a range test: the table coordinate
+// p = (r^2 - rmin^2) dx2 is formed as pmax * sat((r^2 - rmin^2) dx2 / pmax),
+// saturated to [0, pmax] by the FMA itself; knot 0 holds CM3D's clamp below
+// the table (k = 1, fraction 0: the value at knot 1), knot pmax = ntable - 3
+// holds zeros.  A pair at or beyond the cut-off (CM3D's `dis2 < rmax2`
+// test: p < ntable - 3 exactly when r^2 < rc^2) and the padding entries
+// therefore read zero coefficients and contribute nothing.
 struct CwAcc {
   float fx, fy, fz;              // sum qj f d over the electrostatic pairs (x qi at the end)
   float gx, gy, gz;              // sum f d over the LJ pairs
-  float eel, qs, ve[6];          // sum qj V, sum qj, sum qj f d d
+  float eel, ve[6];              // sum qj V, sum qj f d d
   float elo, vsh, vl[6];         // LJ: energy lo parts, sum vt, sum f d d
   double elj_hi;                 // LJ: energy hi parts (FP64)
-  float pmin;                    // smallest table coordinate of an in-range pair (underflow test)
+  float r2min, pminl;            // underflow tests: smallest r^2 (electrostatics), LJ table coordinate
 };
 
 __device__ __forceinline__ void cw_zero(CwAcc &A) {
   A.fx = A.fy = A.fz = A.gx = A.gy = A.gz = 0.f;
-  A.eel = A.qs = A.elo = A.vsh = 0.f;
+  A.eel = A.elo = A.vsh = 0.f;
 #pragma unroll
   for (int k = 0; k < 6; k++) A.ve[k] = A.vl[k] = 0.f;
   A.elj_hi = 0.0;
-  A.pmin = 3.0e38f;
+  A.r2min = A.pminl = 3.0e38f;
 }
 
 // floor of p in [1, 2^22) by the rounding of one FP32 add (RZ mode); returns
@@ -183,28 +197,20 @@ __device__ __forceinline__ float cw_split(float p, unsigned &kb) {
   return p - (t - CW_MAGIC);
 }
 
-// One electrostatic pair, j staged at xj (charge in w).  `el`: the pair is in
-// the te list (back-segment pairs always are).
-template <bool TRACK>
-__device__ __forceinline__ void cw_elec(const CwP &P, const float4 xj, float dx, float dy, float dz, float r2,
-                                        bool el, const float4 *__restrict__ tf, const float2 *__restrict__ tg,
-                                        CwAcc &A) {
-  const bool ok = el && r2 < P.rc2_el;
-  float p = fmaf(r2, P.dx2c, -P.offc);
-  if (TRACK) A.pmin = fminf(A.pmin, ok ? p : 3.0e38f);
-  else A.pmin = fminf(A.pmin, p);
-  // CM3D's clamp below the table (k = 1, fraction 0); out-of-range pairs
-  // read the last knot and contribute zero (their charge is selected to 0)
-  p = fminf(fmaxf(p, 1.f), P.pmax);
-  unsigned kb;
-  const float fr = cw_split(p, kb);
-  const unsigned k = kb - CW_MAGIC_BITS;
-  const float4 c = tf[k * (unsigned)P.rf];
-  const float2 d = tg[k * (unsigned)P.rg];
-  const float qj = ok ? xj.w : 0.f;
+// One electrostatic pair: j staged at xj (charge in w), qj = xj.w or 0 (an
+// LJ-segment pair outside the te list).  tf / tg: this lane's table copies.
+__device__ __forceinline__ void cw_elec(const CwP &P, float qj, float dx, float dy, float dz, float r2,
+                                        const float4 *__restrict__ tf, const float2 *__restrict__ tg, CwAcc &A) {
+  A.r2min = fminf(A.r2min, r2);
+  const float ps = __saturatef(fmaf(r2, P.sat_a, P.sat_b));
+  const float t = __fmaf_rz(ps, P.pmax, CW_MAGIC);
+  const float kf = t - CW_MAGIC;
+  const float fr = fmaf(ps, P.pmax, -kf);
+  const unsigned k = __float_as_uint(t) - CW_MAGIC_BITS;
+  const float4 c = tf[k * CW_RF];
+  const float2 d = tg[k * CW_RG];
   const float fe = qj * fmaf(fr, fmaf(fr, c.z, c.y), c.x);
   A.eel = fmaf(qj, fmaf(fr, fmaf(fr, d.y, d.x), c.w), A.eel);
-  A.qs += qj;
   const float ux = fe * dx, uy = fe * dy, uz = fe * dz;
   A.fx += ux;
   A.fy += uy;
@@ -220,11 +226,10 @@ __device__ __forceinline__ void cw_elec(const CwP &P, const float4 xj, float dx,
 // One LJ pair of interaction parameters {rc2, dx2, off, vt}; tl holds 2
 // float4 per knot {d0, dA, dB, v0 hi} {vA, vB, v0 lo, -}.
 __device__ __forceinline__ void cw_lj(const CwP &P, float dx, float dy, float dz, float r2, float rc2, float dx2,
-                                      float off, float vt, const float4 *__restrict__ tl, float &pminl,
-                                      CwAcc &A) {
+                                      float off, float vt, const float4 *__restrict__ tl, CwAcc &A) {
   const bool ok = r2 < rc2;
   float p = fmaf(r2, dx2, -off);
-  pminl = fminf(pminl, ok ? p : 3.0e38f);
+  A.pminl = fminf(A.pminl, ok ? p : 3.0e38f);
   p = fminf(fmaxf(p, 1.f), P.pmax);
   unsigned kb;
   const float fr = cw_split(p, kb);
@@ -247,7 +252,7 @@ __device__ __forceinline__ void cw_lj(const CwP &P, float dx, float dy, float dz
   A.vl[5] = fmaf(uz, dz, A.vl[5]);
 }
 
-template <int TPA, bool HAS_EL, int LJM>
+template <bool HAS_EL, int LJM>
 __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     CwP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ cell_start, const int2 *__restrict__ cwn, const uint2 *__restrict__ cwl,
@@ -258,24 +263,23 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
   // tables first (16-byte aligned), then the window
-  float4 *tf = sm;                                                    // ntable * rf
-  float2 *tg = reinterpret_cast<float2 *>(tf + (HAS_EL ? P.ntable * P.rf : 0));   // ntable * rg
-  // (an even number of float2, so that the next array starts on 16 bytes)
-  float4 *tl = reinterpret_cast<float4 *>(tg + (HAS_EL ? (P.ntable * P.rg + 1) / 2 * 2 : 0));   // 2 ninter ntable
+  float4 *tf = sm;                                                    // ntable * CW_RF
+  float2 *tg = reinterpret_cast<float2 *>(tf + (HAS_EL ? P.ntable * CW_RF : 0));   // ntable * CW_RG
+  float4 *tl = reinterpret_cast<float4 *>(tg + (HAS_EL ? P.ntable * CW_RG : 0));   // 2 ninter ntable
   const int nl = LJM ? 2 * P.ninter * P.ntable : 0;
   float4 *wx = tl + nl;                                               // cap + 1 staged atoms
   unsigned char *wt = reinterpret_cast<unsigned char *>(wx + P.cap + 1);   // LJM 2: their types
-  __shared__ int s_cs[27], s_cnt[27], s_off[27], s_tot;
+  __shared__ int s_cs[27], s_off[28];
   __shared__ float4 s_shift[54];
   __shared__ int s_map[256];
   __shared__ float4 s_cut[64];                                        // LJM 2: {rc2, dx2, off, vt}
   __shared__ double s_red[CW_THREADS / 32][CQ_COUNT];
 
   for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = gshift[k];
-  if (HAS_EL)
-    for (int k = threadIdx.x; k < P.ntable * P.rf; k += blockDim.x) tf[k] = gtf[k / P.rf];
-  if (HAS_EL)
-    for (int k = threadIdx.x; k < P.ntable * P.rg; k += blockDim.x) tg[k] = gtg[k / P.rg];
+  if (HAS_EL) {
+    for (int k = threadIdx.x; k < P.ntable * CW_RF; k += blockDim.x) tf[k] = gtf[k / CW_RF];
+    for (int k = threadIdx.x; k < P.ntable * CW_RG; k += blockDim.x) tg[k] = gtg[k / CW_RG];
+  }
   for (int k = threadIdx.x; k < nl; k += blockDim.x) tl[k] = gtl[k];
   if (LJM == 2) {
     for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) s_map[k] = gmap[k];
@@ -286,22 +290,20 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     wx[P.cap] = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);   // the dummy entry's partner: out of range
     if (LJM == 2) wt[P.cap] = 0;
   }
-  const int lane = threadIdx.x & 31;
-  const int g = threadIdx.x % TPA;
-  const int groups = CW_THREADS / TPA;
-  const float4 *tfl = tf + lane % P.rf;                 // this lane's table copies
-  const float2 *tgl = tg + lane % P.rg;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int NWARP = CW_THREADS / 32;
+  const float4 *tfl = tf + (lane & (CW_RF - 1));          // this lane's table copies
+  const float2 *tgl = tg + (lane & (CW_RG - 1));
   unsigned long long under = 0;
 
   for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
     const int c = item / P.nsplit, part = item - c * P.nsplit;
     const int cz = c % P.ncz, cy = (c / P.ncz) % P.ncy, cx = c / (P.ncz * P.ncy);
     __syncthreads();                                       // the previous window is no longer read
-    if (threadIdx.x < 32) {
-      const int w = threadIdx.x;
+    if (warp == 0) {
       int cnt = 0, cs = 0;
-      if (w < 27) {
-        int jx = cx - (w / 9 - 1), jy = cy - ((w / 3) % 3 - 1), jz = cz - (w % 3 - 1);
+      if (lane < 27) {
+        int jx = cx - (lane / 9 - 1), jy = cy - ((lane / 3) % 3 - 1), jz = cz - (lane % 3 - 1);
         jx = jx < 0 ? jx + P.ncx : (jx >= P.ncx ? jx - P.ncx : jx);
         jy = jy < 0 ? jy + P.ncy : (jy >= P.ncy ? jy - P.ncy : jy);
         jz = jz < 0 ? jz + P.ncz : (jz >= P.ncz ? jz - P.ncz : jz);
@@ -313,26 +315,46 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (w >= o) incl += v;
+        if (lane >= o) incl += v;
       }
-      if (w < 27) {
-        s_cs[w] = cs;
-        s_cnt[w] = cnt;
-        s_off[w] = incl - cnt;
+      if (lane < 27) {
+        s_cs[lane] = cs;
+        s_off[lane] = incl - cnt;
       }
-      if (w == 26) s_tot = incl;
+      if (lane == 26) s_off[27] = incl;
     }
     __syncthreads();
+    const int tot = s_off[27];
     // a window that does not fit was given empty lists by k_cw_convert
-    const bool staged = s_tot <= P.cap;
+    const bool staged = tot <= P.cap;
     if (staged) {
-      for (int w = 0; w < 27; w++) {
-        const int cs = s_cs[w], cnt = s_cnt[w], off = s_off[w];
-        const float4 sh = s_shift[w], shl = s_shift[27 + w];
-        for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-          const float4 x = xq[cs + k];
-          wx[off + k] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
-          if (LJM == 2) wt[off + k] = (unsigned char)styp[cs + k];
+      // one pass over the whole window, two slots per thread in flight:
+      // staged slot g lies in the last stencil cell w with s_off[w] <= g
+      for (int g0 = threadIdx.x; g0 < tot; g0 += 2 * CW_THREADS) {
+        int gg[2], uu[2], ww[2];
+        float4 xx[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int g = g0 + h * CW_THREADS;
+          int wa = 0, wb = 27;
+          while (wb - wa > 1) {
+            const int mid = (wa + wb) >> 1;
+            if (s_off[mid] <= g) wa = mid;
+            else wb = mid;
+          }
+          gg[h] = g;
+          ww[h] = wa;
+          uu[h] = s_cs[wa] + (g - s_off[wa]);
+          xx[h] = g < tot ? xq[uu[h]] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          if (gg[h] < tot) {
+            const float4 sh = s_shift[ww[h]], shl = s_shift[27 + ww[h]];
+            const float4 x = xx[h];
+            wx[gg[h]] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
+            if (LJM == 2) wt[gg[h]] = (unsigned char)styp[uu[h]];
+          }
         }
       }
     }
@@ -340,43 +362,35 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     double E[CQ_COUNT];
 #pragma unroll
     for (int q = 0; q < CQ_COUNT; q++) E[q] = 0.0;
-    const int ci0 = s_cs[13], cin = s_cnt[13], ioff = s_off[13];
-    for (int r = part; r * groups < cin; r += P.nsplit) {
-      const int a = r * groups + threadIdx.x / TPA;
-      const bool active = staged && a < cin;
-      const int t = ci0 + (active ? a : 0);
+    const int ci0 = s_cs[13], cin = s_off[14] - s_off[13], ioff = s_off[13];
+    // the item's atoms r * NWARP + warp, r = part, part + nsplit, ...; the
+    // next atom's lengths and first two list words are loaded while this
+    // one is evaluated (every slot holds at least two blocks)
+    const int astep = P.nsplit * NWARP;
+    int2 nn_nx = make_int2(0, 0);
+    uint2 p0 = make_uint2(0u, 0u), p1 = make_uint2(0u, 0u);
+    if (staged && part * NWARP + warp < cin) {
+      const int tn = ci0 + part * NWARP + warp;
+      nn_nx = cwn[tn];
+      p0 = __ldg(cwl + (size_t)tn * P.words + lane);
+      p1 = __ldg(cwl + (size_t)tn * P.words + CW_ROW + lane);
+    }
+    for (int a = part * NWARP + warp; staged && a < cin; a += astep) {
+      const int t = ci0 + a;
+      const int2 nn = nn_nx;
+      uint2 w0 = p0, w1 = p1;
+      if (a + astep < cin) {
+        const int tn = t + astep;
+        nn_nx = cwn[tn];
+        p0 = __ldg(cwl + (size_t)tn * P.words + lane);
+        p1 = __ldg(cwl + (size_t)tn * P.words + CW_ROW + lane);
+      }
       CwAcc A;
       cw_zero(A);
-      float pminl = 3.0e38f;
-      // an inactive lane group reads the dummy slot (its window may not exist)
-      const int ia = active ? ioff + a : P.cap;
-      const float4 xi = wx[ia];
-      const int ti = LJM == 2 ? wt[ia] : 0;
-      const int2 nn = active ? cwn[t] : make_int2(0, 0);
-      const int nba = (nn.x + CW_BLOCK - 1) / CW_BLOCK, nbb = (nn.y + CW_BLOCK - 1) / CW_BLOCK;
-      const uint2 *words = cwl + (size_t)t * P.words;
-      // blocks [0, nba) hold the LJ segment, [nba, nba + nbb) the electrostatics-only one
-      auto walk = [&](auto &&front_pair, auto &&back_pair) {
-        for (int b = 0; b < nba + nbb; b++) {
-          const bool front = b < nba;
-          const int m = front ? min(CW_BLOCK, nn.x - b * CW_BLOCK) : min(CW_BLOCK, nn.y - (b - nba) * CW_BLOCK);
-          const int rows = (m + CW_ROW - 1) / CW_ROW;
-#pragma unroll
-          for (int w0 = 0; w0 < CW_ROW; w0 += TPA) {
-            const uint2 v = __ldg(words + b * CW_ROW + w0 + g);
-            const uint32_t e[4] = {v.x & 0xFFFFu, v.x >> 16, v.y & 0xFFFFu, v.y >> 16};
-            if (front) {
-#pragma unroll
-              for (int k = 0; k < 4; k++)
-                if (k < rows) front_pair(e[k]);
-            } else {
-#pragma unroll
-              for (int k = 0; k < 4; k++)
-                if (k < rows) back_pair(e[k]);
-            }
-          }
-        }
-      };
+      const float4 xi = wx[ioff + a];
+      const int ti = LJM == 2 ? wt[ioff + a] : 0;
+      const int nba = (nn.x + CW_BLOCK - 1) / CW_BLOCK, nbt = nba + (nn.y + CW_BLOCK - 1) / CW_BLOCK;
+      const uint2 *words = cwl + (size_t)t * P.words + lane;
       auto geom = [&](uint32_t e, float4 &xj, float &dx, float &dy, float &dz) {
         xj = wx[e & CW_IDX];
         dx = xi.x - xj.x;
@@ -384,88 +398,111 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
         dz = xi.z - xj.z;
         return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
       };
-      auto lj_pair = [&](uint32_t e, float dx, float dy, float dz, float r2, float &pm, CwAcc &Acc) {
+      auto lj_pair = [&](uint32_t e, float dx, float dy, float dz, float r2, CwAcc &Acc) {
         if (LJM == 1) {
-          cw_lj(P, dx, dy, dz, r2, P.rc2_l, P.dx2l, P.offl, P.vtl, tl, pm, Acc);
+          cw_lj(P, dx, dy, dz, r2, P.rc2_l, P.dx2l, P.offl, P.vtl, tl, Acc);
         } else if (LJM == 2) {
           const int tj = wt[e & CW_IDX];
           const int in = s_map[ti * P.ntypes + tj];
           const float4 cut = s_cut[in < 0 ? 0 : in];
           // a pair without an LJ interaction (map -1) never reaches the LJ
-          // segment; a dummy may, with an out-of-range distance
+          // segment; a padding entry may, with an out-of-range distance
           cw_lj(P, dx, dy, dz, in < 0 ? 3.0e38f : r2, cut.x, cut.y, cut.z, cut.w,
-                tl + (size_t)2 * (in < 0 ? 0 : in) * P.ntable, pm, Acc);
+                tl + (size_t)2 * (in < 0 ? 0 : in) * P.ntable, Acc);
         }
       };
-      walk(
-          [&](uint32_t e) {
+      auto front_pair = [&](uint32_t e, CwAcc &Acc) {
+        float4 xj;
+        float dx, dy, dz;
+        const float r2 = geom(e, xj, dx, dy, dz);
+        if (HAS_EL) cw_elec(P, (e & CW_EL) ? xj.w : 0.f, dx, dy, dz, (e & CW_EL) ? r2 : 3.0e38f, tfl, tgl, Acc);
+        lj_pair(e, dx, dy, dz, r2, Acc);
+      };
+      auto back_pair = [&](uint32_t e, CwAcc &Acc) {
+        if (HAS_EL) {
+          float4 xj;
+          float dx, dy, dz;
+          const float r2 = geom(e, xj, dx, dy, dz);
+          cw_elec(P, xj.w, dx, dy, dz, r2, tfl, tgl, Acc);
+        }
+      };
+      // block b's word of this lane; the next two are in flight
+      const uint2 pad = make_uint2((uint32_t)P.cap | ((uint32_t)P.cap << 16), (uint32_t)P.cap | ((uint32_t)P.cap << 16));
+      if (nbt < 2) w1 = pad;
+      for (int b = 0; b < nbt; b++) {
+        const uint2 w2 = b + 2 < nbt ? __ldg(words + (b + 2) * CW_ROW) : pad;
+        const bool front = b < nba;
+        const int m = front ? min(CW_BLOCK, nn.x - b * CW_BLOCK) : min(CW_BLOCK, nn.y - (b - nba) * CW_BLOCK);
+        const uint32_t e[4] = {w0.x & 0xFFFFu, w0.x >> 16, w0.y & 0xFFFFu, w0.y >> 16};
+        if (front && m == CW_BLOCK) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) front_pair(e[k], A);
+        } else if (front) {
+          front_pair(e[0], A);
+#pragma unroll
+          for (int k = 1; k < 4; k++)
+            if (k * CW_ROW < m) front_pair(e[k], A);
+        } else if (m == CW_BLOCK) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) back_pair(e[k], A);
+        } else {
+          back_pair(e[0], A);
+#pragma unroll
+          for (int k = 1; k < 4; k++)
+            if (k * CW_ROW < m) back_pair(e[k], A);
+        }
+        w0 = w1;
+        w1 = w2;
+      }
+      // CM3D's table underflow (k < 1) is counted per pair; the walk only
+      // tracks the smallest distance and LJ table coordinate, and an atom
+      // with an underflow (none in a sane system) is walked again to count
+      // them
+      if (__any_sync(0xffffffffu, A.r2min < P.r2under || A.pminl < 1.f)) {
+        unsigned cnt = 0;
+        for (int b = 0; b < nbt; b++) {
+          const uint2 w = __ldg(words + b * CW_ROW);
+          const uint32_t e[4] = {w.x & 0xFFFFu, w.x >> 16, w.y & 0xFFFFu, w.y >> 16};
+          const bool front = b < nba;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
             float4 xj;
             float dx, dy, dz;
-            const float r2 = geom(e, xj, dx, dy, dz);
-            if (HAS_EL) cw_elec<true>(P, xj, dx, dy, dz, r2, (e & CW_EL) != 0, tfl, tgl, A);
-            lj_pair(e, dx, dy, dz, r2, pminl, A);
-          },
-          [&](uint32_t e) {
-            if (HAS_EL) {
-              float4 xj;
-              float dx, dy, dz;
-              const float r2 = geom(e, xj, dx, dy, dz);
-              cw_elec<false>(P, xj, dx, dy, dz, r2, true, tfl, tgl, A);
+            const float r2 = geom(e[k], xj, dx, dy, dz);
+            const bool el = HAS_EL && (!front || (e[k] & CW_EL));
+            cnt += (el && r2 < P.rc2_el && fmaf(r2, P.dx2c, -P.offc) < 1.f) ? 1u : 0u;
+            if (front && LJM) {
+              CwAcc B;
+              cw_zero(B);
+              lj_pair(e[k], dx, dy, dz, r2, B);
+              cnt += B.pminl < 1.f ? 1u : 0u;
             }
-          });
-      // CM3D's table underflow (k < 1) is counted per pair; the walk only
-      // tracks the smallest table coordinate, and an atom with an underflow
-      // (none in a sane system) is walked again to count them
-      if (active && (A.pmin < 1.f || pminl < 1.f)) {
-        CwAcc B;
-        cw_zero(B);
-        unsigned cnt = 0;
-        walk(
-            [&](uint32_t e) {
-              float4 xj;
-              float dx, dy, dz;
-              const float r2 = geom(e, xj, dx, dy, dz);
-              if (HAS_EL) {
-                const bool ok = (e & CW_EL) && r2 < P.rc2_el;
-                cnt += (ok && fmaf(r2, P.dx2c, -P.offc) < 1.f) ? 1u : 0u;
-              }
-              float pm2 = 3.0e38f;
-              lj_pair(e, dx, dy, dz, r2, pm2, B);
-              cnt += pm2 < 1.f ? 1u : 0u;
-            },
-            [&](uint32_t e) {
-              if (HAS_EL) {
-                float4 xj;
-                float dx, dy, dz;
-                const float r2 = geom(e, xj, dx, dy, dz);
-                cnt += (r2 < P.rc2_el && fmaf(r2, P.dx2c, -P.offc) < 1.f) ? 1u : 0u;
-              }
-            });
+          }
+        }
         under += cnt;
       }
       // forces: F_i = -(qi sum qj f d + sum f_lj d), the chunk in FP64 and
       // summed over the atom's lanes
+      // (a transposing reduction: after the first two levels each lane
+      // carries one component, lanes 0-7 x, 8-15 y, 16-23 z)
       const double qi = (double)xi.w;
-      double Fx = -(qi * (double)A.fx + (double)A.gx);
-      double Fy = -(qi * (double)A.fy + (double)A.gy);
-      double Fz = -(qi * (double)A.fz + (double)A.gz);
+      const double Fx = -(qi * (double)A.fx + (double)A.gx);
+      const double Fy = -(qi * (double)A.fy + (double)A.gy);
+      const double Fz = -(qi * (double)A.fz + (double)A.gz);
+      const bool up = (lane & 16) != 0, odd = (lane & 8) != 0;
+      const double k0 = (up ? Fz : Fx) + __shfl_xor_sync(0xffffffffu, up ? Fx : Fz, 16);
+      const double k1 = (up ? 0.0 : Fy) + __shfl_xor_sync(0xffffffffu, up ? Fy : 0.0, 16);
+      double Fc = (odd ? k1 : k0) + __shfl_xor_sync(0xffffffffu, odd ? k0 : k1, 8);
 #pragma unroll
-      for (int o = TPA / 2; o > 0; o >>= 1) {
-        Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
-        Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
-        Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+      for (int o = 4; o > 0; o >>= 1) Fc += __shfl_xor_sync(0xffffffffu, Fc, o);
+      if ((lane & 7) == 0 && lane < 24) {
+        const int comp = lane >> 3;                   // 0 x, 1 y, 2 z
+        fout[(size_t)comp * P.n + sorig[t]] += Fc;
       }
-      if (active && g == 0) {
-        const int i = sorig[t], n = P.n;
-        fout[i] += Fx;
-        fout[n + i] += Fy;
-        fout[2 * n + i] += Fz;
-      }
-      if (active) {
-        E[CQ_EEL] += qi * (double)A.eel;
-        E[CQ_QQ] += qi * (double)A.qs;
+      E[CQ_EEL] += qi * (double)A.eel;
 #pragma unroll
-        for (int k = 0; k < 6; k++) E[CQ_VE0 + k] += qi * (double)A.ve[k];
+      for (int k = 0; k < 6; k++) E[CQ_VE0 + k] += qi * (double)A.ve[k];
+      if (LJM) {
         E[CQ_ELJ] += A.elj_hi + (double)A.elo;
         E[CQ_VSH] += (double)A.vsh;
 #pragma unroll
@@ -473,7 +510,6 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
       }
     }
     // the item's sums: warps, then the block, in a fixed order
-    const int warp = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < CQ_COUNT; q++) {
       const double v = warp_sum(E[q]);
@@ -482,11 +518,11 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     __syncthreads();
     if (threadIdx.x < CQ_COUNT) {
       double s = 0.0;
-      for (int w = 0; w < CW_THREADS / 32; w++) s += s_red[w][threadIdx.x];
+      for (int w = 0; w < NWARP; w++) s += s_red[w][threadIdx.x];
       ipart[(size_t)item * CQ_COUNT + threadIdx.x] = s;
     }
   }
-  if (under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), under);
+  if (lane == 0 && under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), under);
 }
 
 // Sum of the items' partials into CM3D's accumulators: one block, warp q
@@ -507,8 +543,9 @@ __global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce(int nitems, int ma
   if (threadIdx.x != 0) return;
   const double *v = s_q;
   if (mask & 2) {
+    // (CM3D's shifted sum spothe, finter_e.c:197, is read by nothing --
+    // getsvirter_e reports spote -- and this path does not form it)
     acc[ACC_SPOTE] += v[CQ_EEL];
-    acc[ACC_SPOTHE] += v[CQ_EEL] - tablast_e * v[CQ_QQ];
     acc[ACC_SPRSE] -= v[CQ_VE0] + v[CQ_VE4] + v[CQ_VE8];
     acc[ACC_SPRSET + 0] -= v[CQ_VE0];
     acc[ACC_SPRSET + 1] -= v[CQ_VE1];
@@ -531,10 +568,9 @@ __global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce(int nitems, int ma
 }
 
 // ------------------------------------------------------------------ host
-static size_t cw_table_bytes(const Ctx *c, int rf, int rg, int ljm) {
+static size_t cw_table_bytes(const Ctx *c, int ljm) {
   size_t b = 0;
-  if (c->ncharge > 0)
-    b += (size_t)c->ntable * rf * sizeof(float4) + ((size_t)c->ntable * rg + 1) / 2 * 2 * sizeof(float2);
+  if (c->ncharge > 0) b += (size_t)c->ntable * (CW_RF * sizeof(float4) + CW_RG * sizeof(float2));
   if (ljm) b += (size_t)2 * c->ninter * c->ntable * sizeof(float4);
   return b;
 }
@@ -547,8 +583,7 @@ static int cw_ljm(const Ctx *c) {
 // Whether the compact path can run this context, and its tables and window
 // size: one system, at least 3 cells per axis, the full force level without
 // the RESPA switch copy, a window of the mean size (x 1.25, + 64) next to the
-// tables in the shared memory a block may use.  Table copies are reduced
-// (8, 4, 2, 1) until it fits.
+// tables in the shared memory a block may use.
 int cw_setup(Ctx *c) {
   c->cw_ok = 0;
   if (c->mode != CM3D_NB_MIXED || c->nsys != 1) return CM3D_NB_OK;
@@ -562,22 +597,13 @@ int cw_setup(Ctx *c) {
   const size_t want_cap = (size_t)(1.25 * mean_window) + 64;
   const size_t budget = c->smem_optin > CW_STATIC_SMEM ? c->smem_optin - CW_STATIC_SMEM : 0;
   const size_t per_slot = sizeof(float4) + (ljm == 2 ? 1 : 0);
-  int rf = 8, rg = 8;
-  for (;;) {
-    const size_t tb = cw_table_bytes(c, rf, rg, ljm);
-    if (tb + (want_cap + 1) * per_slot + 16 <= budget) break;
-    if (rf == 1 && rg == 1) return CM3D_NB_OK;
-    if (rg > 1) rg /= 2;
-    else rf /= 2;
-  }
-  const size_t tb = cw_table_bytes(c, rf, rg, ljm);
+  const size_t tb = cw_table_bytes(c, ljm);
+  if (tb + (want_cap + 1) * per_slot + 16 > budget) return CM3D_NB_OK;
   long long cap = (long long)((budget - tb - 16) / per_slot) - 1;
   cap = std::min<long long>(cap, CW_MAX_CAP);
   // CM3D_NB_CW_CAP lowers the window capacity (tests of the fall-back)
   const char *ce = getenv("CM3D_NB_CW_CAP");
   if (ce && atoi(ce) > 0) cap = std::min<long long>(cap, atoi(ce));
-  c->cw_rf = rf;
-  c->cw_rg = rg;
   c->cw_cap = (int)cap;
   c->cw_smem = tb + ((size_t)cap + 1) * sizeof(float4) + (ljm == 2 ? (size_t)cap + 1 : 0);
   c->cw_smem = (c->cw_smem + 15) / 16 * 16;
@@ -594,9 +620,13 @@ int cw_setup(Ctx *c) {
     std::vector<double> ct(nt), dct(nt);
     CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    // knot 0: CM3D's clamp below the table (the value at knot 1, no slope);
+    // knots ntable - 3 and up: zeros (the saturated coordinate of a pair at
+    // or beyond the cut-off reads knot ntable - 3)
     std::vector<float4> tf(nt, make_float4(0.f, 0.f, 0.f, 0.f));
     std::vector<float2> tg(nt, make_float2(0.f, 0.f));
-    for (int k = 1; k <= nt - 2; k++) {
+    tf[0] = make_float4((float)dct[1], 0.f, 0.f, (float)ct[1]);
+    for (int k = 1; k <= nt - 4; k++) {
       const double d0 = dct[k], da = 0.5 * (dct[k + 1] - dct[k - 1]),
                    db = 0.5 * (dct[k - 1] - 2.0 * dct[k] + dct[k + 1]);
       const double v0 = ct[k], va = 0.5 * (ct[k + 1] - ct[k - 1]), vb = 0.5 * (ct[k - 1] - 2.0 * ct[k] + ct[k + 1]);
@@ -684,9 +714,9 @@ int cw_convert(Ctx *c, bool device_flag) {
   return CM3D_NB_OK;
 }
 
-template <int TPA, bool EL, int LJM>
+template <bool EL, int LJM>
 static void cw_launch_t(Ctx *c, const CwP &P, double *fout) {
-  auto kern = k_pair_cw<TPA, EL, LJM>;
+  auto kern = k_pair_cw<EL, LJM>;
   static unsigned long long attr_devs = 0;
   if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(c->smem_optin - CW_STATIC_SMEM));
@@ -696,15 +726,6 @@ static void cw_launch_t(Ctx *c, const CwP &P, double *fout) {
   kern<<<grid, CW_THREADS, c->cw_smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl,
                                                  c->shift, c->map, c->fcut, c->cw_tf, c->cw_tg, c->cw_tl, fout,
                                                  c->cw_part, c->stat, c->gate);
-}
-
-template <bool EL, int LJM>
-static void cw_launch_tpa(Ctx *c, const CwP &P, double *fout) {
-  switch (c->tpa) {
-    case 8: cw_launch_t<8, EL, LJM>(c, P, fout); break;
-    case 16: cw_launch_t<16, EL, LJM>(c, P, fout); break;
-    default: cw_launch_t<32, EL, LJM>(c, P, fout); break;
-  }
 }
 
 bool cw_applies(Ctx *c, int iflg, bool ns) { return c->cw_ok && c->cw_use && iflg == 1 && !ns; }
@@ -724,12 +745,13 @@ int cw_pairs(Ctx *c, int mask, double *fout) {
   P.ntable = c->ntable;
   P.ntypes = c->ntypes;
   P.ninter = c->ninter;
-  P.rf = c->cw_rf;
-  P.rg = c->cw_rg;
   P.rc2_el = (float)c->rmaxl_coul2;
   P.dx2c = (float)c->dx2coul;
   P.offc = (float)(c->rmins_coul2 * c->dx2coul);
   P.pmax = (float)(c->ntable - 3);
+  P.sat_a = (float)(c->dx2coul / (c->ntable - 3));
+  P.sat_b = (float)(-c->rmins_coul2 * c->dx2coul / (c->ntable - 3));
+  P.r2under = (float)(c->rmins_coul2 + 1.0 / c->dx2coul);
   P.rc2_l = c->cw_lj1[0];
   P.dx2l = c->cw_lj1[1];
   P.offl = c->cw_lj1[2];
@@ -737,12 +759,12 @@ int cw_pairs(Ctx *c, int mask, double *fout) {
   const bool el = (mask & 2) != 0;
   const int ljm = (mask & 1) ? cw_ljm(c) : 0;
   if (el) {
-    if (ljm == 0) cw_launch_tpa<true, 0>(c, P, fout);
-    else if (ljm == 1) cw_launch_tpa<true, 1>(c, P, fout);
-    else cw_launch_tpa<true, 2>(c, P, fout);
+    if (ljm == 0) cw_launch_t<true, 0>(c, P, fout);
+    else if (ljm == 1) cw_launch_t<true, 1>(c, P, fout);
+    else cw_launch_t<true, 2>(c, P, fout);
   } else {
-    if (ljm == 1) cw_launch_tpa<false, 1>(c, P, fout);
-    else if (ljm == 2) cw_launch_tpa<false, 2>(c, P, fout);
+    if (ljm == 1) cw_launch_t<false, 1>(c, P, fout);
+    else if (ljm == 2) cw_launch_t<false, 2>(c, P, fout);
   }
   c->launches++;
   CKL(c);

@@ -1,8 +1,10 @@
 """The pair-kernel autotuner (cm3d_nb_autotune): it picks one of the
 candidate lane counts and, for a single system with 3 or more cells per axis,
-the gather or the windowed kernel; it leaves forces and energies as they were
-(lane count and kernel only reorder FP32 partial sums: relative 1e-6), and a
-trajectory continues after it exactly as the mixed engine's bound requires."""
+the gather, windowed or compact-window kernel; it leaves forces as they were
+(lane count and kernel only reorder FP32 partial sums: relative 1e-6) and
+energies within the mixed engine's bound (1e-5: the kernels sum energies in
+FP32 chunks of different lengths before FP64), and a trajectory continues
+after it as the mixed engine's bound requires."""
 import numpy as np
 import pytest
 
@@ -24,7 +26,7 @@ def test_autotune_keeps_state(engine_lib, names):
     en0 = e.all_energies()
     res = e.autotune(reps=3)
     assert res["tpa"] in (4, 8, 16, 32)
-    assert res["kernel"] in ("gather", "window", "system")
+    assert res["kernel"] in ("gather", "window", "system", "compact")
     if len(names) > 1:
         assert res["kernel"] in ("gather", "system")   # a batch: gather or whole systems staged
     elif names[0] == "water216":
@@ -36,7 +38,7 @@ def test_autotune_keeps_state(engine_lib, names):
     assert rel_rms(f1, f0, fs) <= 1e-6
     for a, b in zip(en0, en1):
         for k in ("vinter", "velec", "vewald", "U", "W", "zke"):
-            assert abs(a[k] - b[k]) <= 1e-6 * max(abs(b[k]), 1.0), k
+            assert abs(a[k] - b[k]) <= 1e-5 * max(abs(b[k]), 1.0), k
     e.step(1, 5)                      # the step graph is recaptured with the new lane count
     assert np.isfinite(e.positions()).all()
     e.close()

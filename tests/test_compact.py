@@ -4,10 +4,11 @@ rewritten after each rebuild as 16-bit window indices; its kernel reads j
 from the staged 27-cell window and the tables from bank-replicated copies.
 
 Checked here:
-  - it is the kernel a lone system with >= 3 cells per axis runs, at 8, 16
-    and 32 lanes per atom, within the mixed bounds of CM3D's dumped forces,
-    energies and virials, and within FP32 summation order of the window and
-    list-gather kernels on the same lists;
+  - it is the kernel a lone system with >= 3 cells per axis runs (one
+    LJ interaction, several LJ interactions with the per-pair type map, no
+    charges, charges), within the mixed bounds of CM3D's dumped forces,
+    energies and virials or of the plain FP64 engine, and within FP32
+    summation order of the window and list-gather kernels on the same lists;
   - a force evaluation repeats bit for bit (every sum in a fixed order);
   - a cell window larger than the kernel's capacity turns the path off on
     the host and the context falls back to the window kernel, with the same
@@ -102,21 +103,46 @@ def test_compact_is_default_and_matches(engine_lib, name, monkeypatch):
             assert close(out["compact"][1][k], out[kind][1][k], 2e-6), (kind, k)
 
 
-@pytest.mark.parametrize("tpa", [8, 16, 32])
-def test_compact_lanes_per_atom(engine_lib, tpa):
-    d = golden("water4096")
-    f, en, used = level1(System.from_arrays(d), _abi.MIXED, tpa=tpa)
-    assert used == "compact"
-    fs = force_scale(d) / float(np.sqrt((d["amass"] ** 2).mean()))
-    assert rel_rms(f, xyz(d, "acc_l"), fs) <= FTOL
-    for k in ("vinter", "velec", "W", "prsi"):
-        tol = VTOL if k in VIRIAL_KEYS else ETOL
-        assert close(en[k], float(d[f"e0_{k}"][0]), tol), k
+def test_compact_binary_mixture_several_lj_types(engine_lib, monkeypatch):
+    """4000-atom charged LJ binary (three LJ interactions: the per-pair type
+    map path), positions shaken off the FCC start: the compact kernel against
+    the plain FP64 engine and the gather kernel on the same positions"""
+    from cm3d_b200 import configs, setup
+    sm = setup.build_system(configs.charged_binary(natoms=4000, seed=3))
+    rng = np.random.default_rng(5)
+    pos = None
+    out = {}
+    for key, mode, env in (("plain", _abi.PLAIN_FP64, None), ("compact", _abi.MIXED, None),
+                           ("gather", _abi.MIXED, "list")):
+        if env:
+            monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", env)
+        e = Engine(sm, mode=mode)
+        if env:
+            monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
+        if pos is None:
+            pos = e.positions() + rng.normal(scale=0.15, size=(3, e.n))
+        e.set_positions(pos)
+        e.get_ngbr()
+        e.force(1)
+        if mode == _abi.MIXED:
+            assert e.pair_kernel()[0] == key
+        f = e.forces(_abi.FXL)
+        e.force(2)
+        out[key] = (f, e.energies())
+        e.close()
+    st = error_stats(out["compact"][0], out["plain"][0])
+    record("binary4000", {"level1": st})
+    assert st["rel_rms"] <= FTOL
+    assert rel_rms(out["compact"][0], out["gather"][0]) <= 1e-6
+    for k in ENERGY_KEYS:
+        assert close(out["compact"][1][k], out["plain"][1][k], ETOL), k
+    for k in VIRIAL_KEYS:
+        assert close(out["compact"][1][k], out["plain"][1][k], VTOL), k
 
 
 def test_compact_repeats_bit_for_bit(engine_lib):
     d = golden("water4096")
-    e = Engine(System.from_arrays(d), mode=_abi.MIXED, tpa=32)
+    e = Engine(System.from_arrays(d), mode=_abi.MIXED)
     e.get_ngbr()
     runs = []
     for _ in range(3):
@@ -142,7 +168,8 @@ def test_compact_window_overflow_falls_back(engine_lib, monkeypatch):
     assert used == "window"
     fw, enw, _ = level1(System.from_arrays(d), _abi.MIXED, "window", monkeypatch=monkeypatch)
     np.testing.assert_array_equal(f, fw)
-    assert en["W"] == enw["W"] and en["U"] == enw["U"]
+    # (the window kernel's energy sums end in FP64 atomics: last-bit order)
+    assert close(en["W"], enw["W"], 1e-13) and close(en["U"], enw["U"], 1e-13)
 
 
 @pytest.fixture(scope="module")
