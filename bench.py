@@ -63,7 +63,7 @@ def workload(name: str, seed: int):
             "rho* U(0.6,0.9), T* U(0.7,1.5), 75% argon LJ / 25% charged +/-0.5 e binary (Ewald alpha 3.2/rc, " \
             "kmax 5), rc min(2.5 sigma, 0.45 L), skin 0.3 sigma, FCC start, dt 5 fs, one batch", 300
     if name == "water12288":
-        return [configs.water_box(ngrid=16, seed=seed, ntime=1000, placement="octant")], \
+        return [configs.water_box(ngrid=16, seed=seed, ntime=1000)], \
             "water-12288: 4096 flexible 3-site waters on a 16^3 grid (seeded orientations, no intermolecular " \
             "contact under 1.9 A), L 49.66 A, alpha 0.31, kmax 7, rc 10 A, skin 0.5 A, RESPA 0.5/2 fs " \
             "(nres_intra 4), 300 K", 1000

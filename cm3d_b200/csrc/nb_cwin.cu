@@ -122,33 +122,84 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
       if (halt) *halt = 1;
     }
     const int lo = cell_start[c], hi = cell_start[c + 1];
+    const unsigned lt = (1u << lane) - 1u;
     for (int t = lo + warp; t < hi; t += nwarps) {
       const int na = fits ? nlen[t] : 0, nb = fits ? nlen[n + t] : 0;
       const uint32_t *src = nbr + (size_t)t * stride;
       uint2 *dst = cwl + (size_t)t * words;
       const int nba = (na + CW_BLOCK - 1) / CW_BLOCK, nbb = (nb + CW_BLOCK - 1) / CW_BLOCK;
-      for (int b = 0; b < nba + nbb; b++) {
-        const bool front = b < nba;
-        const int e0 = (front ? b : b - nba) * CW_BLOCK, cnt = front ? na : nb;
-        uint32_t v[4];
+      // padding first: every slot of the atom's blocks holds the dummy
+      for (int b = 0; b < nba + nbb; b++) dst[b * CW_ROW + lane] = make_uint2(dummy | (dummy << 16), dummy | (dummy << 16));
+      __syncwarp();
+      for (int sg = 0; sg < 2; sg++) {
+        const bool front = sg == 0;
+        const int m = front ? na : nb;
+        const uint32_t *in = front ? src : src + (stride - nb);   // the back segment ends at the slot's end
+        unsigned short *out = reinterpret_cast<unsigned short *>(dst + (front ? 0 : nba * CW_ROW));
+        auto window_index = [&](int e, uint32_t &o) -> int {
+          const uint32_t en = in[e];
+          const int code = (en >> ENT_CODE_SHIFT) & 31;
+          const int wi = (int)(en & ENT_JMASK) + s_delta[code];
+          // inside the window by construction (a pair's shift code names
+          // j's stencil cell); anything else would index past the staged
+          // atoms, so it becomes the dummy
+          o = wi >= 0 && wi < tot ? (uint32_t)wi : dummy;
+          if (front && (en & ENT_EL) && o != dummy) o |= CW_EL;
+          return (int)(o & 7u);
+        };
+        // bank classes: the window slot mod 8 (the 16-byte bank group of
+        // the staged position).  Position j of the segment is read by lane
+        // j % 32, so putting a class-(j % 8) entry at j gives the 8 lanes of
+        // each quarter-warp 8 different bank groups; the entries that do
+        // not fit their own class's positions fill the rest in order.
+        int cnt[8];
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          const int e = e0 + k * CW_ROW + lane;
-          uint32_t o = dummy;
-          if (e < cnt) {
-            // the back segment runs from the slot's end towards its front
-            const uint32_t en = front ? src[e] : src[stride - nb + e];
-            const int code = (en >> ENT_CODE_SHIFT) & 31;
-            const int wi = (int)(en & ENT_JMASK) + s_delta[code];
-            // inside the window by construction (a pair's shift code names
-            // j's stencil cell); anything else would index past the staged
-            // atoms, so it becomes the dummy
-            o = wi >= 0 && wi < tot ? (uint32_t)wi : dummy;
-            if (front && (en & ENT_EL) && o != dummy) o |= CW_EL;
-          }
-          v[k] = o;
+        for (int q = 0; q < 8; q++) cnt[q] = 0;
+        for (int e0 = 0; e0 < m; e0 += 32) {
+          uint32_t o;
+          const int cl = e0 + lane < m ? window_index(e0 + lane, o) : -1;
+#pragma unroll
+          for (int q = 0; q < 8; q++) cnt[q] += __popc(__ballot_sync(0xffffffffu, cl == q));
         }
-        dst[b * CW_ROW + lane] = make_uint2(v[0] | (v[1] << 16), v[2] | (v[3] << 16));
+        const int Q = m >> 3;
+        int run[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) run[q] = 0;
+        for (int e0 = 0; e0 < m; e0 += 32) {
+          uint32_t o = dummy;
+          const int cl = e0 + lane < m ? window_index(e0 + lane, o) : -1;
+          int rank = 0, lbase = 0;
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const unsigned bq = __ballot_sync(0xffffffffu, cl == q);
+            if (cl == q) rank = run[q] + __popc(bq & lt);
+            if (q < cl) lbase += max(0, cnt[q] - Q);
+            run[q] += __popc(bq);
+          }
+          if (cl >= 0) {
+            int pos;
+            if (rank < Q) {
+              pos = cl + 8 * rank;
+            } else {
+              // the L-th free position: the unused class positions of the
+              // classes short of Q entries, in class order, then the tail
+              int L = lbase + rank - Q;
+              pos = -1;
+#pragma unroll
+              for (int q = 0; q < 8; q++) {
+                const int d = max(0, Q - cnt[q]);
+                if (pos < 0) {
+                  if (L < d) pos = q + 8 * (cnt[q] + L);
+                  else L -= d;
+                }
+              }
+              if (pos < 0) pos = 8 * Q + L;
+            }
+            // position -> (block, row, lane): 16-bit entry k of word w
+            const int bb = pos / CW_BLOCK, r = pos - bb * CW_BLOCK;
+            out[(bb * CW_ROW + (r & (CW_ROW - 1))) * 4 + (r >> 5)] = (unsigned short)o;
+          }
+        }
       }
       if (lane == 0) cwn[t] = make_int2(na, nb);
     }
@@ -197,18 +248,34 @@ __device__ __forceinline__ float cw_split(float p, unsigned &kb) {
   return p - (t - CW_MAGIC);
 }
 
-// One electrostatic pair: j staged at xj (charge in w), qj = xj.w or 0 (an
-// LJ-segment pair outside the te list).  tf / tg: this lane's table copies.
+// Shared-memory loads from 32-bit shared-window addresses (the hot loop's
+// address arithmetic stays in 32 bits: one shift-and-add per address).
+__device__ __forceinline__ float4 lds_f4(unsigned a) {
+  float4 v;
+  asm("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+  return v;
+}
+__device__ __forceinline__ float2 lds_f2(unsigned a) {
+  float2 v;
+  asm("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+  return v;
+}
+
+// One electrostatic pair: qj = j's charge, or 0 for an LJ-segment pair
+// outside the te list.  tfb / tgb: this lane's table copies as 32-bit shared
+// addresses less MAGIC_BITS knots, so that the float bits of the split
+// coordinate address the knot directly (k * stride = bits * stride - MAGIC_BITS
+// * stride, mod 2^32).
 __device__ __forceinline__ void cw_elec(const CwP &P, float qj, float dx, float dy, float dz, float r2,
-                                        const float4 *__restrict__ tf, const float2 *__restrict__ tg, CwAcc &A) {
+                                        unsigned tfb, unsigned tgb, CwAcc &A) {
   A.r2min = fminf(A.r2min, r2);
   const float ps = __saturatef(fmaf(r2, P.sat_a, P.sat_b));
   const float t = __fmaf_rz(ps, P.pmax, CW_MAGIC);
   const float kf = t - CW_MAGIC;
   const float fr = fmaf(ps, P.pmax, -kf);
-  const unsigned k = __float_as_uint(t) - CW_MAGIC_BITS;
-  const float4 c = tf[k * CW_RF];
-  const float2 d = tg[k * CW_RG];
+  const unsigned kb = __float_as_uint(t);
+  const float4 c = lds_f4(tfb + kb * (unsigned)(CW_RF * sizeof(float4)));
+  const float2 d = lds_f2(tgb + kb * (unsigned)(CW_RG * sizeof(float2)));
   const float fe = qj * fmaf(fr, fmaf(fr, c.z, c.y), c.x);
   A.eel = fmaf(qj, fmaf(fr, fmaf(fr, d.y, d.x), c.w), A.eel);
   const float ux = fe * dx, uy = fe * dy, uz = fe * dz;
@@ -274,6 +341,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   __shared__ int s_map[256];
   __shared__ float4 s_cut[64];                                        // LJM 2: {rc2, dx2, off, vt}
   __shared__ double s_red[CW_THREADS / 32][CQ_COUNT];
+  static_assert(CQ_COUNT == 16, "the transposing reduction gives lane pair q quantity q of 16");
 
   for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = gshift[k];
   if (HAS_EL) {
@@ -292,8 +360,12 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = CW_THREADS / 32;
-  const float4 *tfl = tf + (lane & (CW_RF - 1));          // this lane's table copies
-  const float2 *tgl = tg + (lane & (CW_RG - 1));
+  // this lane's table copies and the window as 32-bit shared addresses
+  const unsigned tfb = (unsigned)__cvta_generic_to_shared(tf + (lane & (CW_RF - 1))) -
+                       CW_MAGIC_BITS * (unsigned)(CW_RF * sizeof(float4));
+  const unsigned tgb = (unsigned)__cvta_generic_to_shared(tg + (lane & (CW_RG - 1))) -
+                       CW_MAGIC_BITS * (unsigned)(CW_RG * sizeof(float2));
+  const unsigned wxb = (unsigned)__cvta_generic_to_shared(wx);
   unsigned long long under = 0;
 
   for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
@@ -359,9 +431,9 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
       }
     }
     __syncthreads();
-    double E[CQ_COUNT];
-#pragma unroll
-    for (int q = 0; q < CQ_COUNT; q++) E[q] = 0.0;
+    // energy and virial sums: lane l keeps quantity (l >> 1) of CQ_* in
+    // FP64 (both lanes of a pair hold it), plus its own FP64 LJ hi parts
+    double Eq = 0.0, Ehi = 0.0;
     const int ci0 = s_cs[13], cin = s_off[14] - s_off[13], ioff = s_off[13];
     // the item's atoms r * NWARP + warp, r = part, part + nsplit, ...; the
     // next atom's lengths and first two list words are loaded while this
@@ -392,7 +464,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
       const int nba = (nn.x + CW_BLOCK - 1) / CW_BLOCK, nbt = nba + (nn.y + CW_BLOCK - 1) / CW_BLOCK;
       const uint2 *words = cwl + (size_t)t * P.words + lane;
       auto geom = [&](uint32_t e, float4 &xj, float &dx, float &dy, float &dz) {
-        xj = wx[e & CW_IDX];
+        xj = lds_f4(wxb + ((e & CW_IDX) << 4));
         dx = xi.x - xj.x;
         dy = xi.y - xj.y;
         dz = xi.z - xj.z;
@@ -415,7 +487,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
         float4 xj;
         float dx, dy, dz;
         const float r2 = geom(e, xj, dx, dy, dz);
-        if (HAS_EL) cw_elec(P, (e & CW_EL) ? xj.w : 0.f, dx, dy, dz, (e & CW_EL) ? r2 : 3.0e38f, tfl, tgl, Acc);
+        if (HAS_EL) cw_elec(P, (e & CW_EL) ? xj.w : 0.f, dx, dy, dz, (e & CW_EL) ? r2 : 3.0e38f, tfb, tgb, Acc);
         lj_pair(e, dx, dy, dz, r2, Acc);
       };
       auto back_pair = [&](uint32_t e, CwAcc &Acc) {
@@ -423,7 +495,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
           float4 xj;
           float dx, dy, dz;
           const float r2 = geom(e, xj, dx, dy, dz);
-          cw_elec(P, xj.w, dx, dy, dz, r2, tfl, tgl, Acc);
+          cw_elec(P, xj.w, dx, dy, dz, r2, tfb, tgb, Acc);
         }
       };
       // block b's word of this lane; the next two are in flight
@@ -499,21 +571,36 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
         const int comp = lane >> 3;                   // 0 x, 1 y, 2 z
         fout[(size_t)comp * P.n + sorig[t]] += Fc;
       }
-      E[CQ_EEL] += qi * (double)A.eel;
+      // the atom's 16 quantities (CQ_* order) over the warp: three
+      // transposing FP32 levels (8 lanes' chunks, about 160 pairs, then each
+      // lane carries two quantities), FP64 for the last two levels, so lane
+      // pair (2q, 2q + 1) ends with quantity q's atom total
+      {
+        const float qf = xi.w;
+        float v[16] = {qf * A.eel, 0.f, qf * A.ve[0], qf * A.ve[1], qf * A.ve[2], qf * A.ve[3], qf * A.ve[4],
+                       qf * A.ve[5], A.elo, A.vsh, A.vl[0], A.vl[1], A.vl[2], A.vl[3], A.vl[4], A.vl[5]};
 #pragma unroll
-      for (int k = 0; k < 6; k++) E[CQ_VE0 + k] += qi * (double)A.ve[k];
-      if (LJM) {
-        E[CQ_ELJ] += A.elj_hi + (double)A.elo;
-        E[CQ_VSH] += (double)A.vsh;
+        for (int h = 8, o = 16; h >= 2; h >>= 1, o >>= 1) {
+          const bool hi = (lane & o) != 0;
 #pragma unroll
-        for (int k = 0; k < 6; k++) E[CQ_VL0 + k] += (double)A.vl[k];
+          for (int i = 0; i < h; i++) {
+            const float snd = hi ? v[i] : v[i + h];
+            const float kp = hi ? v[i + h] : v[i];
+            v[i] = kp + __shfl_xor_sync(0xffffffffu, snd, o);
+          }
+        }
+        const bool b1 = (lane & 2) != 0;
+        const double d0 = (double)v[0], d1 = (double)v[1];
+        double dq = (b1 ? d1 : d0) + __shfl_xor_sync(0xffffffffu, b1 ? d0 : d1, 2);
+        dq += __shfl_xor_sync(0xffffffffu, dq, 1);
+        Eq += dq;
+        Ehi += A.elj_hi;
       }
     }
     // the item's sums: warps, then the block, in a fixed order
-#pragma unroll
-    for (int q = 0; q < CQ_COUNT; q++) {
-      const double v = warp_sum(E[q]);
-      if (lane == 0) s_red[warp][q] = v;
+    {
+      const double hi = warp_sum(Ehi);
+      if ((lane & 1) == 0) s_red[warp][lane >> 1] = Eq + ((lane >> 1) == CQ_ELJ ? hi : 0.0);
     }
     __syncthreads();
     if (threadIdx.x < CQ_COUNT) {

@@ -11,9 +11,11 @@
  *   {"natoms": N, "steps": S, "seconds": T, "atom_steps_per_s": N*S/T,
  *    "poter": U}
  *
- * usage:  ref_bench <cm3d input file> <nsteps> [warmup]
+ * usage:  ref_bench <cm3d input file> <nsteps> [warmup [trace]]
  *         (run from the deck's directory; warmup: untimed loop iterations
- *         before the timed ones, default 0)
+ *         before the timed ones, default 0; trace: after every timed step
+ *         print "T istep poth potra zke" at %.17g -- the terms of CM3D's
+ *         conserved energy ham of an NVE run, integrate/md_averages.new.c:100)
  */
 #include <time.h>
 
@@ -29,7 +31,7 @@ int main(int argc, char *argv[])
   NGBR ngbr;
   INTER inter;
   ENERGIES energies;
-  int s, nsteps, warmup;
+  int s, nsteps, warmup, trace;
   struct timespec t0, t1;
   double sec;
 
@@ -39,6 +41,7 @@ int main(int argc, char *argv[])
   }
   nsteps = atoi(argv[2]);
   warmup = argc > 3 ? atoi(argv[3]) : 0;
+  trace = argc > 4 && strcmp(argv[4], "trace") == 0;
   memset(&simparms, 0, sizeof simparms);
   memset(&filenames, 0, sizeof filenames);
   memset(&coords, 0, sizeof coords);
@@ -71,6 +74,8 @@ int main(int argc, char *argv[])
     step(&simparms, &coords, &energies, &inter, &ngbr);
     geteng(&simparms, &coords, &energies);
     gettngbr(&ngbr);
+    if (trace)
+      printf("T %d %.17g %.17g %.17g\n", simparms.istep, energies.poth, energies.potra, energies.zke);
   }
   clock_gettime(CLOCK_MONOTONIC, &t1);
   sec = (double)(t1.tv_sec - t0.tv_sec) + 1e-9 * (double)(t1.tv_nsec - t0.tv_nsec);
