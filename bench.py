@@ -230,11 +230,23 @@ def roofline(eng, steps: int, istep0: int, fp32_tflops: float, hbm_gbs: float) -
     t = ms / 1e3 / max(launches, 1)
     t_bw = nbytes / (hbm_gbs * 1e9)
     t_fl = flops / (fp32_tflops * 1e12)
-    traffic = None
+    # DRAM bytes per launch from an ncu capture (profiles/pair_kernel_traffic.json),
+    # used only while the kernel's source is the one that was captured
+    kind, tpa = eng.pair_kernel()
+    traffic, traffic_src = None, "no capture of this kernel"
     try:
+        import hashlib
         with open(os.path.join(ROOT, "profiles", "pair_kernel_traffic.json")) as fh:
-            tr = json.load(fh)
-        traffic = tr.get(eng.workload_name, {}).get("dram_bytes_per_launch")
+            tr = json.load(fh).get(eng.workload_name, {})
+        src = os.path.join(ROOT, "cm3d_b200", "csrc", "nb_cwin.cu" if kind == "compact" else "nb_pair.cu")
+        with open(src, "rb") as fh:
+            sha = hashlib.sha256(fh.read()).hexdigest()[:16]
+        if tr.get("pair_kernel") == kind and tr.get("source_sha16") == sha:
+            traffic = tr.get("dram_bytes_per_launch")
+            traffic_src = f"{tr.get('source')} (captured {tr.get('date')}, kernel source sha {sha})"
+        elif tr:
+            traffic_src = f"capture of {tr.get('pair_kernel')} at source sha {tr.get('source_sha16')} is stale " \
+                          f"(now {kind}, sha {sha}): not used"
     except Exception:
         pass
     if t_fl >= t_bw:
@@ -243,8 +255,7 @@ def roofline(eng, steps: int, istep0: int, fp32_tflops: float, hbm_gbs: float) -
     else:
         out = {"bound": "hbm", "achieved": nbytes / t / 1e9, "peak": hbm_gbs, "unit": "GB/s",
                "frac": (nbytes / t / 1e9) / hbm_gbs}
-    kind, tpa = eng.pair_kernel()
-    out.update({"traffic": traffic,
+    out.update({"traffic": traffic, "traffic_source": traffic_src,
                 "kernel": f"{kind} pair kernel (fused LJ + real-space Ewald), {tpa} lanes per atom",
                 "ms_per_launch": t * 1e3, "launches": launches, "unique_pairs": pairs,
                 "pairs_te": int(pte_s.sum()), "pairs_t": int(pt_s.sum()),
@@ -422,6 +433,45 @@ def intra_arm(device: int, copies: int, steps: int, warmup: int, flush) -> dict:
             "gpu_launches_per_step": launches / steps}
 
 
+def nve_arm(device: int) -> dict:
+    """Energy conservation (cm3d_b200.drift): the least-squares drift of
+    CM3D's conserved energy ham per atom per ns over 1000 NVE steps, for the
+    mixed and plain FP64 engines and for CM3D itself from the same initial
+    state.  argon864 starts on its FCC lattice, and CM3D runs here on the host
+    (oracle/_ref/ref_bench in its trace mode).  water12288 starts from the
+    state CM3D equilibrated at 300 K (tests/golden/water12288_eq.npz); CM3D's
+    1000 steps of it (about 7 minutes on one core) are the committed
+    trajectory of tests/golden/make_nve.py."""
+    from cm3d_b200 import _abi, configs
+    from cm3d_b200.drift import drift_stats, engine_series
+    from cm3d_b200.setup import build_system
+    golden = os.path.join(ROOT, "tests", "golden")
+    with open(os.path.join(golden, "nve_cm3d.json")) as fh:
+        ref = json.load(fh)
+    eq = np.load(os.path.join(golden, "water12288_eq.npz"))
+    wls = {"argon864": configs.argon_fcc(seed=1, ntime=1000),
+           "water12288": configs.water_box(ngrid=16, seed=1, ntime=1000).with_state(eq["pos"], eq["vel"])}
+    out = {}
+    for name, wl in wls.items():
+        r = ref[name]
+        n, dt, nsteps = r["natoms"], r["dt_ps"], r["nsteps"]
+        sm = build_system(wl)
+        row = {"steps": nsteps, "dt_fs": dt * 1e3, "start": r["start"]}
+        for key, mode in (("mixed", _abi.MIXED), ("plain_fp64", _abi.PLAIN_FP64)):
+            row[key] = drift_stats(engine_series(sm, mode, nsteps, device), dt, n)
+        cm3d_ham, src = r["ham"], "tests/golden/nve_cm3d.json (CM3D run by tests/golden/make_nve.py)"
+        if name == "argon864" and ref_bench_bin():
+            with tempfile.TemporaryDirectory() as tmp:
+                inp = wl.write(tmp)
+                txt = subprocess.run([ref_bench_bin(), os.path.basename(inp), str(nsteps), "0", "trace"], cwd=tmp,
+                                     stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, check=True).stdout
+            cm3d_ham = [sum(float(v) for v in ln.split()[2:5]) for ln in txt.splitlines() if ln.startswith("T ")]
+            src = "oracle/_ref/ref_bench on this host, this run"
+        row["cm3d"] = {**drift_stats(cm3d_ham, dt, n), "source": src}
+        out[name] = row
+    return out
+
+
 def serving_arm(rate: float, window: float, device: int, plain: bool) -> dict:
     """The serving loop (cm3d_b200.serving) on a Poisson stream of water-box
     jobs (configs.serving_plan: molecules log-uniform in [256, 16384], steps
@@ -569,7 +619,27 @@ def main() -> None:
             "status": {k: wm["status"][k] for k in ("rebuilds", "resets")}}
 
     if not args.no_extra and world == 1:
+        # the single large box (C3) and the small argon box (C1), mixed and
+        # plain FP64, with the pair kernel's roofline
+        for wname, wsteps, wwarm, psteps in (("water331776", 50, 5, 10), ("argon864", 500, 20, 300)):
+            if args.workload == wname:
+                continue
+            wwl, wdesc, _ = workload(wname, seed=1)
+            wsys = [build_system(w) for w in wwl]
+            wm = mixed_arm(wsys, local, wsteps, wwarm, flush, fp32, hbm, wname, 10)
+            wval = wm["n"] * wsteps / (wm["ms"] / 1e3)
+            wplain = None if args.no_plain else plain_arm(wsys, local, psteps, 3, flush)
+            other[wname] = {
+                "workload": wdesc, "value": wval, "unit": UNIT, "ms_per_step": wm["ms"] / wsteps,
+                "steps": wsteps, "ns_per_day": (wsteps / (wm["ms"] / 1e3)) * float(wsys[0]["dt"]) * 86400.0 / 1e3,
+                "plain_fp64": wplain, "speedup_mixed_vs_plain": (wval / wplain["value"]) if wplain else None,
+                "roofline": wm["roofline"], "autotune": wm["autotune"],
+                "status": {k: wm["status"][k] for k in ("rebuilds", "resets", "table_underflow")}}
         other["abutane1024"] = intra_arm(local, 1024, 200, 10, flush)
+
+    nve = None
+    if not args.no_extra and world == 1:
+        nve = nve_arm(local)
 
     serving = None
     if not args.no_extra and world == 1:
@@ -615,6 +685,7 @@ def main() -> None:
             "plain_fp64": plain,
             "other_workloads": other,
             "serving": serving,
+            "nve_drift": nve,
             "peaks": {"fp32_tflops": fp32, "fp64_tflops": fp64, "hbm_gbs": hbm},
             "clocks": m["clocks"],
             "status": {k: m["status"][k] for k in ("rebuilds", "resets", "overflows", "table_underflow")},

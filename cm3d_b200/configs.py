@@ -97,6 +97,11 @@ class Workload:
         rows += ["0 0 0"] * 3
         return "\n".join(rows) + "\n"
 
+    def with_state(self, pos: np.ndarray, vel: np.ndarray) -> "Workload":
+        """the same workload started from other positions and velocities"""
+        import dataclasses
+        return dataclasses.replace(self, pos=np.array(pos, dtype=float), vel=np.array(vel, dtype=float))
+
     def write(self, directory: str) -> str:
         """Write the full input deck; returns the keyword-file path."""
         os.makedirs(directory, exist_ok=True)
@@ -521,3 +526,14 @@ def serving_workload(req: ServingRequest) -> Workload:
     return water_box(ngrid=req.ngrid, seed=req.seed, rc=rc, alpha=3.1 / rc,
                      kmax=int(math.ceil(7.0 * L / 49.66)), ntime=req.nsteps, placement="octant",
                      name=f"job{req.index:04d}")
+
+
+def read_restart(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """positions and velocities (N, 3) from a CM3D restart file
+    (output/md_writestart.c:31-80: five header lines, then x y z vx vy vz
+    per atom)"""
+    with open(path) as fh:
+        lines = fh.read().splitlines()
+    n = int(lines[0].split()[1])
+    rows = np.array([[float(v) for v in ln.split()[:6]] for ln in lines[5:5 + n]])
+    return rows[:, :3].copy(), rows[:, 3:].copy()

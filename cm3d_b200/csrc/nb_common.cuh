@@ -322,6 +322,14 @@ struct Ctx {
   int *ithm = nullptr;                  // per atom: its thermostat, -1 none
   double *nhc = nullptr;                // mnh | gkt | eta | veta | feta, ntherm * nchain each, then p2m (ntherm)
   std::vector<int> therm0;              // per system: its first thermostat (nsys + 1 entries)
+  // kinetic sums of the thermostats in a fixed order: per-atom terms m v^2
+  // (nvt_kin), summed by one warp per chunk of at most NVT_CHUNK atoms of one
+  // thermostat (th_atoms in thermostat order, th_chunk {first, end}), the
+  // chunks of thermostat j (th_choff[j] .. th_choff[j + 1]) added in order
+  double *nvt_kin = nullptr, *nvt_chsum = nullptr;
+  int *th_atoms = nullptr, *th_choff = nullptr;
+  int2 *th_chunk = nullptr;
+  int nth_chunks = 0;
   // ---- cell grid and lists
   int nc[3] = {1, 1, 1}, ncells = 1;
   int *cell_of = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *cell_atoms = nullptr;

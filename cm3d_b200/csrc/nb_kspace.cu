@@ -553,7 +553,7 @@ int kspace_setup(Ctx *c) {
   CK(cudaMalloc(&c->kposd, sizeof(double4) * (size_t)c->ncharge));
   // split the rows over enough blocks to fill the machine in the force pass
   int split = 1;
-  while ((long long)c->ftiles_tot * split < 148 * 4 && split < nrows_max) split *= 2;
+  while ((long long)c->ftiles_tot * split < (long long)c->num_sms * 4 && split < nrows_max) split *= 2;
   // every split's A(k) must fit in shared memory -- in 48 KB, so that four
   // or more blocks share an SM and hide each other's latency (a single split
   // of a large k set would leave one block per SM)
@@ -603,7 +603,7 @@ static int kspace_forces_batch(Ctx *c) {
                                                                c->sp, c->sys_of, c->kfrac, nullptr, c->gate);
   // enough row chunks per tile to fill the machine (one-warp blocks: 32
   // blocks per SM)
-  const long long target = c->ks_small ? 148LL * 32 : 148LL * 4;
+  const long long target = (long long)c->num_sms * (c->ks_small ? 32 : 4);
   int ych = 1;
   while ((long long)c->ktiles_tot * ych < target && ych < c->nrows_max) ych *= 2;
   const int rpb = (c->nrows_max + ych - 1) / ych;
@@ -654,7 +654,8 @@ int kspace_forces(Ctx *c) {
                                                                 c->kposd, c->gate);
   // structure factors: enough row chunks per tile to fill the machine
   int rpb = c->nrows;
-  while (rpb > 1 && (long long)c->ks_tiles * ((c->nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
+  while (rpb > 1 && (long long)c->ks_tiles * ((c->nrows + rpb - 1) / rpb) < (long long)c->num_sms * 4)
+    rpb = (rpb + 1) / 2;
   dim3 gsf(c->ks_tiles, (c->nrows + rpb - 1) / rpb);
   if (mixed)
     k_sfac_mixed<false><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb,
@@ -663,7 +664,7 @@ int kspace_forces(Ctx *c) {
     k_sfac_plain<<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
                                                 dhmati, c->spart, c->gate);
   int ib = 256, gb = grid_for(c->ktot, ib);
-  if (gb > 148 * 4) gb = 148 * 4;
+  if (gb > c->num_sms * 4) gb = c->num_sms * 4;
   k_sred<false><<<gb, ib, 0, c->st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
                                       c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc,
                                       nullptr, nullptr, c->gate);
@@ -825,22 +826,31 @@ __global__ void k_na_finish(const double *__restrict__ acc, double six, double s
 
 // per-device set-up, once: the scratch area's address (cudaGetSymbolAddress
 // with the device current) and the force kernel's shared-memory limit
-static std::once_flag g_na_once[NA_MAX_DEVICES];
-static cudaError_t g_na_err[NA_MAX_DEVICES];
-static const char *g_na_what[NA_MAX_DEVICES];
+// per-device set-up, done by the first call on a device that succeeds: a
+// failed set-up (say, a first call made during a stream capture) is not
+// remembered, the next call tries again
+static std::mutex g_na_mu;
+static bool g_na_ready[NA_MAX_DEVICES];
 static unsigned char *g_na_ptr[NA_MAX_DEVICES];
+static int g_na_sms[NA_MAX_DEVICES];
 
-static void na_device_setup(int dev) {
+static cudaError_t na_device_setup(int dev, const char **what) {
   void *p = nullptr;
+  *what = "cudaGetSymbolAddress(scratch)";
   cudaError_t e = cudaGetSymbolAddress(&p, g_na_scratch);
-  g_na_what[dev] = "cudaGetSymbolAddress(scratch)";
-  if (e == cudaSuccess) {
-    // the same limit kspace_forces sets, so that neither caller lowers it
-    e = cudaFuncSetAttribute(k_kforce_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    g_na_what[dev] = "cudaFuncSetAttribute(k_kforce_mixed)";
-  }
-  g_na_err[dev] = e;
-  g_na_ptr[dev] = e == cudaSuccess ? (unsigned char *)p : nullptr;
+  if (e != cudaSuccess) return e;
+  // the same limit kspace_forces sets, so that neither caller lowers it
+  *what = "cudaFuncSetAttribute(k_kforce_mixed)";
+  e = cudaFuncSetAttribute(k_kforce_mixed<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e != cudaSuccess) return e;
+  int sms = 0;
+  *what = "cudaDeviceGetAttribute(multiProcessorCount)";
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  g_na_ptr[dev] = (unsigned char *)p;
+  g_na_sms[dev] = sms > 0 ? sms : 1;
+  g_na_ready[dev] = true;
+  return cudaSuccess;
 }
 
 struct NaDeviceGuard {
@@ -893,9 +903,16 @@ static int fk_ewald_noalloc(int device, cudaStream_t st, int natoms, const doubl
     CK(cudaSetDevice(device));
     guard.switched = true;
   }
-  std::call_once(g_na_once[device], na_device_setup, device);
-  if (g_na_err[device] != cudaSuccess) return cuda_fail(g_na_err[device], g_na_what[device]);
+  {
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (!g_na_ready[device]) {
+      const char *what = "";
+      const cudaError_t e = na_device_setup(device, &what);
+      if (e != cudaSuccess) return cuda_fail(e, what);
+    }
+  }
   unsigned char *base = g_na_ptr[device];
+  const int nsm = g_na_sms[device];
   uint4 *kfrac = (uint4 *)(base + NA_OFF_KFRAC);
   double2 *spart = (double2 *)(base + NA_OFF_SPART);
   double2 *sk = (double2 *)(base + NA_OFF_SK);
@@ -942,18 +959,18 @@ static int fk_ewald_noalloc(int device, cudaStream_t st, int natoms, const doubl
     // grids chosen as kspace_setup/kspace_forces choose them
     const int ks_tiles = (ncharge + KS_THREADS * KS_A - 1) / (KS_THREADS * KS_A);
     int rpb = nrows;
-    while (rpb > 1 && (long long)ks_tiles * ((nrows + rpb - 1) / rpb) < 148 * 4) rpb = (rpb + 1) / 2;
+    while (rpb > 1 && (long long)ks_tiles * ((nrows + rpb - 1) / rpb) < nsm * 4) rpb = (rpb + 1) / 2;
     dim3 gsf(ks_tiles, (nrows + rpb - 1) / rpb);
     k_sfac_mixed<false><<<gsf, KS_THREADS, 0, st>>>(ncharge, kfrac, nrows, rows, row_k0, rpb, ktot, spart, nullptr,
                                                     nullptr, nullptr);
     int gb = grid_for(ktot, 256);
-    if (gb > 148 * 4) gb = 148 * 4;
+    if (gb > nsm * 4) gb = nsm * 4;
     k_sred<false><<<gb, 256, 0, st>>>(ktot, ks_tiles, spart, ka, kb, kc, dhmati, rvol, falp2, sk, akf, nullptr, acc,
                                       nullptr, nullptr, nullptr);
     const int per_block = KS_THREADS * KF_A;
     const int tiles = (ncharge + per_block - 1) / per_block;
     int split = 1;
-    while (tiles * split < 148 * 4 && split < nrows) split *= 2;
+    while (tiles * split < nsm * 4 && split < nrows) split *= 2;
     if (split > nrows) split = nrows;
     const int rps = (nrows + split - 1) / split;
     size_t smem = 0;

@@ -212,8 +212,8 @@ int plain_pairs(Ctx *c, int iflg, int which) {
   // rebuild inside a CUDA graph may have changed
   long long np = c->hcount[list] > 0 ? c->hcount[list] : 1;
   int grid = grid_for(np, B);
-  if (grid < 148 * 8) grid = 148 * 8;
-  if (grid > 148 * 16) grid = 148 * 16;
+  if (grid < c->num_sms * 8) grid = c->num_sms * 8;
+  if (grid > c->num_sms * 16) grid = c->num_sms * 16;
   const long long *npd = c->ltot + list;
   cudaEvent_t e0;
   tbegin(c, 0, &e0);

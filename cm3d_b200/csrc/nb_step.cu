@@ -390,8 +390,9 @@ __global__ void k_inner(StepP P, int intr, const int *__restrict__ gaoff, const 
 // integrate/md_therm.new.c:278-333, called between the two half drifts of
 // every inner substep, md_step.c:117).  The chain update needs every
 // thermostat's kinetic sum, a reduction over all groups, so each inner
-// substep runs as three launches: k_nvt_a (kicks, first half drift, the
-// first velocity scaling, kinetic partial sums), k_nvt_chain (one thread per
+// substep runs as four launches: k_nvt_a (kicks, first half drift, the
+// first velocity scaling, each atom's kinetic term), k_nvt_ksum (the
+// thermostats' kinetic sums in a fixed order), k_nvt_chain (one thread per
 // thermostat) and k_nvt_c (second scaling, second half drift, bonded
 // forces, kicks and, at the level's end, the displacement test).
 
@@ -404,7 +405,7 @@ __global__ void k_nvt_a(StepP P, int intr, int level_start, int tors_start, cons
                         const double *__restrict__ mass, const double *__restrict__ fxl,
                         const double *__restrict__ fxs, const double *__restrict__ fxa,
                         const double *__restrict__ fxr, const int *__restrict__ ithm,
-                        const double *__restrict__ veta, double *__restrict__ p2m, IntraDev X,
+                        const double *__restrict__ veta, double *__restrict__ kin, IntraDev X,
                         int *__restrict__ istate, const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -429,16 +430,33 @@ __global__ void k_nvt_a(StepP P, int intr, int level_start, int tors_start, cons
     vel[i] *= e;
     vel[n + i] *= e;
     vel[2 * n + i] *= e;
-    if (thm >= 0)
-      atomicAdd(p2m + thm, mass[i] * (vel[i] * vel[i] + vel[n + i] * vel[n + i] + vel[2 * n + i] * vel[2 * n + i]));
+    // this atom's kinetic term; k_nvt_ksum adds them per thermostat in a
+    // fixed order (atoms without a thermostat are in no chunk)
+    kin[i] = mass[i] * (vel[i] * vel[i] + vel[n + i] * vel[n + i] + vel[2 * n + i] * vel[2 * n + i]);
   }
+}
+
+// the kinetic sums of the thermostats' chunks: one warp per chunk, a lane-
+// strided sum and the warp's fixed shuffle tree (the same order every step,
+// alone or in a batch)
+__global__ void k_nvt_ksum(int nchunks, const int2 *__restrict__ chunk, const int *__restrict__ atoms,
+                           const double *__restrict__ kin, double *__restrict__ chsum, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  const int ch = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (ch >= nchunks) return;
+  const int2 r = chunk[ch];
+  double s = 0.0;
+  for (int k = r.x + lane; k < r.y; k += 32) s += kin[atoms[k]];
+  s = warp_sum(s);
+  if (lane == 0) chsum[ch] = s;
 }
 
 // the chain half step of one thermostat, in intnhc_new's order: links from
 // the top, forces (forcen_new, md_therm.new.c:175-198), velocities and
 // positions, the recurrence, links from the bottom
 __global__ void k_nvt_chain(int ntherm, int nchain, double dta2, double *__restrict__ nhc,
-                            const double *__restrict__ p2m, const int *__restrict__ gs) {
+                            const double *__restrict__ chsum, const int *__restrict__ choff,
+                            const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ntherm) return;
@@ -447,7 +465,9 @@ __global__ void k_nvt_chain(int ntherm, int nchain, double dta2, double *__restr
   double *eta = nhc + 2 * tc + o, *v = nhc + 3 * tc + o, *f = nhc + 4 * tc + o;
   const double dta = 2. * dta2;
   for (int i = 0; i < nchain - 1; i++) v[i] *= exp(-dta2 * v[i + 1]);
-  f[0] = (p2m[j] - gk[0]) / m[0];
+  double p2m = 0.0;
+  for (int k = choff[j]; k < choff[j + 1]; k++) p2m += chsum[k];
+  f[0] = (p2m - gk[0]) / m[0];
   for (int i = 1; i < nchain; i++) f[i] = (m[i - 1] * v[i - 1] * v[i - 1] - gk[i]) / m[i];
   for (int i = 0; i < nchain; i++) v[i] += dta2 * f[i];
   for (int i = 0; i < nchain; i++) eta[i] += dta * v[i];
@@ -1092,6 +1112,32 @@ static int nvt_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   CK(cudaMemcpy(c->nhc, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
   CK(cudaMalloc(&c->ithm, sizeof(int) * thm.size()));
   CK(cudaMemcpy(c->ithm, thm.data(), sizeof(int) * thm.size(), cudaMemcpyHostToDevice));
+  // the thermostats' atoms in thermostat order (atom order inside one) and
+  // their chunks of at most NVT_CHUNK atoms
+  constexpr int NVT_CHUNK = 1024;
+  std::vector<std::vector<int>> by(nt);
+  for (int i = 0; i < c->n; i++)
+    if (thm[(size_t)i] >= 0) by[(size_t)thm[(size_t)i]].push_back(i);
+  std::vector<int> atoms, choff(1, 0);
+  std::vector<int2> chunks;
+  for (int j = 0; j < nt; j++) {
+    const int a0 = (int)atoms.size();
+    atoms.insert(atoms.end(), by[(size_t)j].begin(), by[(size_t)j].end());
+    for (int k = a0; k < (int)atoms.size(); k += NVT_CHUNK)
+      chunks.push_back(make_int2(k, std::min((int)atoms.size(), k + NVT_CHUNK)));
+    choff.push_back((int)chunks.size());
+  }
+  c->nth_chunks = (int)chunks.size();
+  CK(cudaMalloc(&c->nvt_kin, sizeof(double) * (size_t)c->n));
+  CK(cudaMemset(c->nvt_kin, 0, sizeof(double) * (size_t)c->n));
+  CK(cudaMalloc(&c->th_atoms, sizeof(int) * std::max<size_t>(atoms.size(), 1)));
+  if (!atoms.empty()) CK(cudaMemcpy(c->th_atoms, atoms.data(), sizeof(int) * atoms.size(), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c->th_chunk, sizeof(int2) * std::max<size_t>(chunks.size(), 1)));
+  if (!chunks.empty())
+    CK(cudaMemcpy(c->th_chunk, chunks.data(), sizeof(int2) * chunks.size(), cudaMemcpyHostToDevice));
+  CK(cudaMalloc(&c->nvt_chsum, sizeof(double) * std::max<size_t>(chunks.size(), 1)));
+  CK(cudaMalloc(&c->th_choff, sizeof(int) * choff.size()));
+  CK(cudaMemcpy(c->th_choff, choff.data(), sizeof(int) * choff.size(), cudaMemcpyHostToDevice));
   return CM3D_NB_OK;
 }
 
@@ -1372,24 +1418,26 @@ static int one_level(Ctx *c, int intr, bool gated) {
   cudaEvent_t e0;
   tbegin(c, 3, &e0);
   if (c->ntherm > 0) {
-    // NVT: three launches per inner substep (k_nvt_a, k_nvt_chain, k_nvt_c)
+    // NVT: four launches per inner substep (k_nvt_a, k_nvt_ksum, k_nvt_chain, k_nvt_c)
     const size_t tc = (size_t)c->ntherm * c->nchain;
-    double *veta = c->nhc + 3 * tc, *p2m = c->nhc + 5 * tc;
+    double *veta = c->nhc + 3 * tc;
     for (int inrra = 0; inrra < c->nres_tors; inrra++)
       for (int intra = 0; intra < c->nres_intra; intra++) {
-        CK(cudaMemsetAsync(p2m, 0, sizeof(double) * (size_t)c->ntherm, c->st));
         k_nvt_a<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, intr, inrra == 0 && intra == 0, intra == 0,
                                                           c->grp_atom_off, c->grp_atoms, c->pos, c->vel, c->mass,
-                                                          c->fxl, c->fxs, c->fxa, c->fxr, c->ithm, veta, p2m,
+                                                          c->fxl, c->fxs, c->fxa, c->fxr, c->ithm, veta, c->nvt_kin,
                                                           c->intra, c->istate, c->gate);
-        k_nvt_chain<<<grid_for(c->ntherm, 64), 64, 0, c->st>>>(c->ntherm, c->nchain, P.dta2, c->nhc, p2m,
+        k_nvt_ksum<<<grid_for(32LL * c->nth_chunks, 256), 256, 0, c->st>>>(c->nth_chunks, c->th_chunk, c->th_atoms,
+                                                                          c->nvt_kin, c->nvt_chsum, c->gate);
+        k_nvt_chain<<<grid_for(c->ntherm, 64), 64, 0, c->st>>>(c->ntherm, c->nchain, P.dta2, c->nhc, c->nvt_chsum,
+                                                               c->th_choff,
                                                                c->gate);
         k_nvt_c<<<grid_for(c->ngroups, B), B, 0, c->st>>>(
             P, intra == c->nres_intra - 1, inrra == c->nres_tors - 1 && intra == c->nres_intra - 1,
             c->grp_atom_off, c->grp_atoms, c->pos, c->vel, c->mass, c->q, c->fxa, c->fxr, c->dxn,
             c->grp_bond_off, c->bond_ij, c->bond_p, c->grp_bend_off, c->bend_ijk, c->bend_p, c->ithm, veta,
             c->sp, c->sys_of, c->sreb, c->istate, c->intra, c->stat, c->gate);
-        c->launches += 3;
+        c->launches += 4;
       }
   } else {
     auto inner = c->has_intra_x || c->intra.frz ? k_inner<true> : k_inner<false>;

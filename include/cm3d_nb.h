@@ -382,8 +382,15 @@ int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
    area up (the CUDA runtime may load the library's device code at that
    moment, which is when the static area itself is reserved) and raises the
    force kernel's shared-memory limit.  Make that first call before any stream
-   capture and where a one-time cost is acceptable.  Every call launches six
-   kernels on `stream` and returns without waiting for them.
+   capture and where a one-time cost is acceptable.  A set-up that fails is
+   not remembered: the next call on that device tries it again.  Every call
+   launches six kernels on `stream` and returns without waiting for them.
+
+   Where the k-vectors are split over several blocks per atom, the forces
+   are summed with FP64 atomic adds whose order varies: two calls on the
+   same inputs agree to summation-order rounding (far inside the mixed
+   engine's 1e-5 relative bound, as tests/test_zz_no_alloc.py checks), not
+   bit for bit.  The energies and virials are summed in a fixed order.
 
    The call clears the scratch accumulators itself; nothing has to start at
    zero except what the caller wants in fxl, to which the forces are added.

@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 from cm3d_b200 import configs  # noqa: E402
 from oracle.dumpio import read_dump  # noqa: E402
 
-REF = os.environ.get("CM3D_REF", "/root/reference")
+REF = os.environ.get("CM3D_REF", "")   # the CM3D source tree (its test/ decks); main() requires it
 DUMP = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
 
 LISTS = (("t", "inpt", "jnpt"), ("s", "inps", "jnps"),
@@ -93,6 +93,8 @@ def copy_ref_test(sub: str, dst: str) -> None:
 
 
 def main() -> None:
+    if not REF or not os.path.isdir(REF):
+        sys.exit("set CM3D_REF to the CM3D source tree")
     if not os.path.exists(DUMP):
         sys.exit("build the dump harness first: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:

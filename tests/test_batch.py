@@ -167,3 +167,71 @@ def test_batch_rejects_mismatched_steps(engine_lib):
     d = golden("lj256")
     with pytest.raises(EngineError, match="mixed"):
         Engine([System.from_arrays(d), System.from_arrays(d)], mode=_abi.PLAIN_FP64)
+
+
+def _thermostat_variants():
+    """two NVT systems from CM3D's lj256nvt deck with other thermostat
+    layouts: A splits the atoms over two thermostats (even / odd index), B
+    leaves the first 16 atoms without a thermostat (ithm -1, as
+    \\mol_therm_opt{none} beside a thermostatted species does)"""
+    d = golden("lj256nvt")
+    nc = int(d["nchain"][0])
+    a = System.from_arrays(d)
+    a["ntherm"] = np.array([2], dtype=np.int32)
+    a["ithm"] = (np.arange(256) % 2).astype(np.int32)
+    half = d["gkt"].copy()
+    half[0] *= 0.5
+    a["gkt"] = np.concatenate([half, half])
+    a["mnh"] = np.concatenate([d["mnh"], d["mnh"]])
+    a["nhc_eta"] = np.zeros(2 * nc)
+    a["nhc_veta"] = np.zeros(2 * nc)
+    b = System.from_arrays(d)
+    ithm = np.zeros(256, dtype=np.int32)
+    ithm[:16] = -1
+    b["ithm"] = ithm
+    return [a, b]
+
+
+@pytest.mark.parametrize("mode", [_abi.PLAIN_FP64, _abi.MIXED], ids=["plain", "mixed"])
+def test_nvt_thermostat_layouts_alone_and_in_batch(engine_lib, mode):
+    """several thermostats in one system, atoms without a thermostat, and
+    systems with different numbers of thermostats in one batch: each system's
+    chain state (cm3d_nb_get_nhc, also for system 1) and positions after 10
+    steps are the same alone and in the batch (the thermostats' kinetic sums
+    run in a fixed order), and, in plain FP64, CM3D's algorithm's (the
+    oracle's) to 1e-9"""
+    from oracle import Oracle
+    systems = _thermostat_variants()
+    nsteps = 10
+    e = Engine([s.copy() for s in systems], mode=mode, tpa=TPA)
+    e.step_init()
+    e.step(1, nsteps)
+    pos = e.positions()
+    states = [e.nhc_state(k) for k in range(2)]
+    e.close()
+    for k, s in enumerate(systems):
+        a0, n = e.ranges[k]
+        one = Engine(s.copy(), mode=mode, tpa=TPA)
+        one.step_init()
+        one.step(1, nsteps)
+        eta1, veta1 = one.nhc_state()
+        p1 = one.positions()
+        one.close()
+        shape = (int(np.asarray(s["ntherm"]).ravel()[0]), int(np.asarray(s["nchain"]).ravel()[0]))
+        assert eta1.shape == states[k][0].shape == shape
+        if mode == _abi.PLAIN_FP64:
+            np.testing.assert_array_equal(states[k][0], eta1)
+            np.testing.assert_array_equal(states[k][1], veta1)
+            np.testing.assert_array_equal(pos[:, a0:a0 + n], p1)
+            o = Oracle(s.copy())
+            o.step_init()
+            o.step(1, nsteps)
+            eo, vo = o.nhc_state()
+            np.testing.assert_allclose(eta1, np.asarray(eo).reshape(eta1.shape), rtol=1e-9, atol=1e-12)
+            np.testing.assert_allclose(veta1, np.asarray(vo).reshape(veta1.shape), rtol=1e-9, atol=1e-12)
+            np.testing.assert_allclose(p1, o.positions(), rtol=0, atol=1e-9)
+        else:
+            # the batch's pair kernel (gather) and a lone system's may differ
+            # in FP32 summation order: the same trajectory to the mixed bound
+            np.testing.assert_allclose(states[k][1], veta1, rtol=1e-4, atol=1e-9)
+            assert np.abs(pos[:, a0:a0 + n] - p1).max() <= 1e-6

@@ -100,3 +100,60 @@ def test_ensemble_steps_like_oracle(engine_lib, boxes):
         for k in ("poter", "zke"):
             assert close(en[s][k], eo[k], 2e-4, floor=1e-6 * max(1.0, abs(eo["poter"]))), (s, k)
         assert rb[s] == o.rebuilds and rs[s] == o.resets, (s, rb[s], o.rebuilds, rs[s], o.resets)
+
+
+@pytest.fixture(scope="module")
+def large_boxes():
+    """a slice of the headline ensemble itself (configs.ensemble(1024, seed
+    2024)): its two largest LJ boxes and two largest charged boxes (3,900-4,100
+    atoms) and the two smallest of each kind"""
+    from cm3d_b200 import configs, setup
+    wls = configs.ensemble(1024, seed=2024)
+    nat = np.array([w.natoms for w in wls])
+    ch = np.array(["kmax" in w.keywords for w in wls])
+    pick = []
+    for kind in (False, True):
+        idx = np.flatnonzero(ch == kind)
+        order = idx[np.argsort(nat[idx])]
+        pick += list(order[-2:]) + list(order[:2])
+    return [setup.build_system(wls[k]) for k in sorted(pick)]
+
+
+def test_headline_kernel_on_large_boxes(engine_lib, large_boxes, monkeypatch):
+    """the kernel the headline runs -- the batch gather kernel with 4 lanes
+    per atom and the compact LJ table (the autotuner's choice on the
+    ensemble) -- on boxes up to 4,096 atoms against each box's oracle, at
+    positions the oracle reached after 10 steps"""
+    from oracle import Oracle
+    pos = []
+    for sm in large_boxes:
+        o = Oracle(sm, nocell_all=1)
+        o.step_init()
+        o.step(1, 10)
+        pos.append(o.positions())
+    monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", "list")
+    e = Engine(large_boxes, mode=_abi.MIXED, tpa=4)
+    monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
+    e.set_positions(np.concatenate(pos, axis=1))
+    e.get_ngbr()
+    e.force(1)
+    assert e.pair_kernel() == ("gather", 4)
+    e.force(2)
+    f = e.forces(_abi.FXL)
+    en = e.all_energies()
+    e.close()
+    assert max(sm.natoms for sm in large_boxes) >= 3900
+    for s, sm in enumerate(large_boxes):
+        a0, n = e.ranges[s]
+        o = Oracle(sm, nocell_all=1)
+        o.set_positions(pos[s])
+        o.get_ngbr()
+        o.force(1)
+        o.force(2)
+        fo = o.forces(_abi.FXL)
+        scale = float(np.sqrt((fo * fo).mean()))
+        assert rel_rms(f[:, a0:a0 + n], fo, scale) <= FTOL, s
+        eo = o.energies()
+        for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke"):
+            tol = VTOL if k in VIRIAL_KEYS else ETOL
+            assert close(en[s][k], eo[k], tol, floor=1e-6 * max(1.0, abs(eo["U"]))), (s, k, en[s][k], eo[k])

@@ -1,0 +1,68 @@
+"""NVE energy conservation against CM3D's own runs.
+
+CM3D's conserved energy ham (integrate/md_averages.new.c:100) over 1000 NVE
+steps, from tests/golden/nve_cm3d.json (made by tests/golden/make_nve.py
+with CM3D built from its sources), against the engine's, mixed and plain
+FP64, from the same initial state:
+
+  argon864    the LJ argon FCC start, dt 5 fs (5 ps)
+  water12288  4096 flexible waters equilibrated by CM3D at 300 K
+              (tests/golden/water12288_eq.npz), RESPA 0.5/2 fs (2 ps)
+
+The drift is the least-squares slope of ham per atom per ns
+(cm3d_b200.drift).  The bound: the engine's |drift| is at most CM3D's
+|drift| plus three standard errors of the two fits (the trajectories are
+chaotic: the engine and CM3D part ways within a few hundred steps, so their
+drifts are two samples of the same integrator's behaviour, not one number).
+The plain engine also follows CM3D's ham step by step at the start.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+from cm3d_b200 import _abi
+from cm3d_b200.drift import drift_stats, engine_series
+
+pytestmark = pytest.mark.gpu
+
+
+def cases():
+    from cm3d_b200 import configs
+    eq = np.load(os.path.join(GOLDEN, "water12288_eq.npz"))
+    return {"argon864": configs.argon_fcc(seed=1, ntime=1000),
+            "water12288": configs.water_box(ngrid=16, seed=1, ntime=1000).with_state(eq["pos"], eq["vel"])}
+
+
+@pytest.fixture(scope="module")
+def cm3d_runs():
+    with open(os.path.join(GOLDEN, "nve_cm3d.json")) as fh:
+        return json.load(fh)
+
+
+@pytest.mark.parametrize("name", ["argon864", "water12288"])
+def test_nve_drift_no_worse_than_cm3d(engine_lib, cm3d_runs, name):
+    from cm3d_b200.setup import build_system
+    ref = cm3d_runs[name]
+    wl = cases()[name]
+    sm = build_system(wl)
+    n, dt, nsteps = ref["natoms"], ref["dt_ps"], ref["nsteps"]
+    want = drift_stats(ref["ham"], dt, n)
+    out = {"cm3d": want}
+    for key, mode in (("plain_fp64", _abi.PLAIN_FP64), ("mixed", _abi.MIXED)):
+        ham = engine_series(sm, mode, nsteps)
+        got = drift_stats(ham, dt, n)
+        out[key] = got
+        if mode == _abi.PLAIN_FP64:
+            # the same trajectory as CM3D's at the start (10 steps)
+            np.testing.assert_allclose(ham[:10], ref["ham"][:10], rtol=1e-9)
+        bound = abs(want["drift_per_atom_per_ns"]) + 3.0 * (want["drift_se_per_atom_per_ns"] +
+                                                             got["drift_se_per_atom_per_ns"])
+        assert abs(got["drift_per_atom_per_ns"]) <= bound, (key, got, want)
+    print("NVE", name, json.dumps(out))
+    path = os.environ.get("CM3D_NB_ERRLOG")
+    if path:
+        with open(path, "a") as fh:
+            fh.write(json.dumps({"config": f"nve_{name}", **out}) + "\n")
