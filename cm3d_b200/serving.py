@@ -8,7 +8,9 @@ time.  The server
     fits the HBM budget next to the jobs already resident (first come, first
     served: a job that does not fit holds the queue until memory frees up);
   * keeps every admitted job's state resident in its own engine context,
-    with its own CUDA stream and step graph;
+    with its own CUDA stream and step graph; a job's context is created and
+    its start-up (lists, first forces) run on a worker thread, so that an
+    admission does not hold up the polling of the jobs already running;
   * advances every active job in chunks of steps launched asynchronously
     (cm3d_nb_step_async), so that the chunks of all active jobs are in
     flight together and their kernels overlap on the device, and polls them
@@ -25,6 +27,7 @@ plain FP64 engine, one job per context and per launch.
 """
 from __future__ import annotations
 
+import concurrent.futures as cf
 import math
 import time
 from dataclasses import dataclass, field
@@ -79,9 +82,11 @@ class Server:
     """Continuous-batching MD server on one device (see the module text)."""
 
     def __init__(self, device: int = 0, hbm_budget: float = 150e9, mode: int = _abi.MIXED,
-                 chunk: int = 50, use_graph: bool = True, tpa: int = 0, idle_sleep: float = 2e-4):
+                 chunk: int = 50, use_graph: bool = True, tpa: int = 0, idle_sleep: float = 2e-4,
+                 setup_workers: int = 2):
         self.device, self.budget, self.mode = device, float(hbm_budget), mode
         self.chunk, self.use_graph, self.tpa, self.idle_sleep = chunk, use_graph, tpa, idle_sleep
+        self.setup_workers = setup_workers
         self.queue: list[Job] = []
         self.finished: list[Job] = []
         self.max_active = 0
@@ -90,6 +95,17 @@ class Server:
     def submit(self, job: Job) -> None:
         self.queue.append(job)
         self.queue.sort(key=lambda j: (j.arrival, j.id))
+
+    def _prepare(self, job: Job) -> Engine:
+        """a job's context and start-up (runs on a worker thread)"""
+        eng = Engine(job.system, mode=self.mode, device=self.device, tpa=self.tpa, use_graph=self.use_graph)
+        try:
+            eng.step_init()
+            eng.synchronize()
+        except Exception:
+            eng.close()
+            raise
+        return eng
 
     def _finish(self, job: Job, eng: Engine, now: float) -> None:
         en = eng.energies()
@@ -104,27 +120,42 @@ class Server:
         admitted before its arrival time)."""
         t0 = clock()
         active: list[list] = []            # [job, engine, bytes, steps in flight]
+        starting: list[tuple] = []         # (job, bytes, future of its engine)
         used = 0
         pending = list(self.queue)
         self.queue = []
-        while pending or active:
-            # admission: first come, first served, against the budget
+        pool = cf.ThreadPoolExecutor(max_workers=self.setup_workers)
+        try:
+            return self._loop(clock, realtime, t0, active, starting, used, pending, pool)
+        finally:
+            pool.shutdown(wait=True)
+
+    def _loop(self, clock, realtime, t0, active, starting, used, pending, pool):
+        while pending or active or starting:
+            # admission: first come, first served, against the budget; the
+            # context is set up on a worker thread
             while pending and (not realtime or pending[0].arrival <= clock() - t0):
                 job = pending[0]
                 need = device_bytes(job.system)
-                if active and used + need > self.budget:
+                if (active or starting) and used + need > self.budget:
                     break
                 pending.pop(0)
-                eng = Engine(job.system, mode=self.mode, device=self.device, tpa=self.tpa,
-                             use_graph=self.use_graph)
-                eng.step_init()
-                job.admitted = clock() - t0
                 used += need
+                starting.append((job, need, pool.submit(self._prepare, job)))
+            # jobs whose start-up has finished join the running set
+            still_starting = []
+            for job, need, fut in starting:
+                if not fut.done():
+                    still_starting.append((job, need, fut))
+                    continue
+                eng = fut.result()
+                job.admitted = clock() - t0
                 k = min(self.chunk, job.nsteps)
                 eng.step_async(1, k)
                 active.append([job, eng, need, k])
                 self.max_active = max(self.max_active, len(active))
                 self.max_bytes = max(self.max_bytes, used)
+            starting[:] = still_starting
             # completions: non-blocking polls, then the next chunk or retirement
             progressed = False
             still = []
@@ -145,7 +176,7 @@ class Server:
                 eng.step_async(1 + job.done_steps, k)
                 slot[3] = k
                 still.append(slot)
-            active = still
+            active[:] = still
             if not progressed and (not pending or (realtime and pending[0].arrival > clock() - t0)):
                 time.sleep(self.idle_sleep)
         return self.finished

@@ -209,3 +209,56 @@ def test_water331776_mixed_against_plain_fp64(engine_lib, water331776):
         assert close(em[k], ep[k], 1e-5), (k, em[k], ep[k])
     vm, vp = pair[_abi.MIXED][2]["welectensor"], pair[_abi.PLAIN_FP64][2]["welectensor"]
     assert np.abs(vm - vp).max() <= 1e-5 * np.abs(vp).max()
+
+
+# ------------------------------------------------------------------ error table
+def _mixed_vs_plain(sysm, positions=None):
+    """level-1 forces, energies and virials of the mixed engine (default
+    kernels) against the plain FP64 engine on the same positions"""
+    out = {}
+    for key, mode in (("plain", _abi.PLAIN_FP64), ("mixed", _abi.MIXED)):
+        e = Engine(sysm, mode=mode)
+        if positions is not None:
+            e.set_positions(positions)
+        e.get_ngbr()
+        e.force(1)
+        f = e.forces(_abi.FXL)
+        e.force(2)
+        out[key] = (f, e.energies(), e.pair_kernel()[0] if mode == _abi.MIXED else "plain")
+        e.close()
+    st = error_stats(out["mixed"][0], out["plain"][0])
+    rel = {k: abs(out["mixed"][1][k] - out["plain"][1][k]) / abs(out["plain"][1][k])
+           for k in ENERGY_KEYS + VIRIAL_KEYS if out["plain"][1][k] != 0}
+    return st, rel, out["mixed"][2]
+
+
+@pytest.mark.parametrize("name", ["argon864", "water12288"])
+def test_error_table_small_configs(engine_lib, name):
+    """C1 (argon, its FCC start shaken by 0.1 A so that forces are not pure
+    round-off) and C2 (water, the bench's start): mixed against plain FP64"""
+    from cm3d_b200 import configs, setup
+    wl = configs.argon_fcc(seed=1) if name == "argon864" else configs.water_box(ngrid=16, seed=1)
+    sm = setup.build_system(wl)
+    pos = None
+    if name == "argon864":
+        pos = np.asarray(wl.pos, float).T + np.random.default_rng(2).normal(scale=0.1, size=(3, wl.natoms))
+    st, rel, kind = _mixed_vs_plain(sm, pos)
+    record(name, {"kernel": kind, "level1": st, "energies_rel": rel})
+    assert st["rel_rms"] <= FTOL
+    for k, v in rel.items():
+        assert v <= (VTOL if k in VIRIAL_KEYS else ETOL), (k, v)
+
+
+@pytest.mark.parametrize("ngrid", [6, 25])
+def test_error_table_serving_jobs(engine_lib, ngrid):
+    """C5: water jobs at the two ends of the serving workload's sizes (216
+    and 15,625 molecules; rc = min(10 A, 0.45 L), alpha = 3.1 / rc, kmax =
+    ceil(7 L / 49.66))"""
+    from cm3d_b200 import configs, setup
+    req = configs.ServingRequest(index=0, arrival=0.0, ngrid=ngrid, nsteps=500, seed=5)
+    sm = setup.build_system(configs.serving_workload(req))
+    st, rel, kind = _mixed_vs_plain(sm)
+    record(f"serving_water{3 * ngrid ** 3}", {"kernel": kind, "level1": st, "energies_rel": rel})
+    assert st["rel_rms"] <= FTOL
+    for k, v in rel.items():
+        assert v <= (VTOL if k in VIRIAL_KEYS else ETOL), (k, v)
