@@ -10,10 +10,12 @@ FP64, from the same initial state:
               (tests/golden/water12288_eq.npz), RESPA 0.5/2 fs (2 ps)
 
 The drift is the least-squares slope of ham per atom per ns
-(cm3d_b200.drift).  The bound: the engine's |drift| is at most CM3D's
-|drift| plus three standard errors of the two fits (the trajectories are
-chaotic: the engine and CM3D part ways within a few hundred steps, so their
-drifts are two samples of the same integrator's behaviour, not one number).
+(cm3d_b200.drift).  The bound: the engine's |drift| is at most 1.1 times
+CM3D's |drift| plus three standard errors of the two fits.  The
+trajectories are chaotic -- the engine and CM3D part ways within a few
+hundred steps -- so their drifts are two samples of the same integrator's
+behaviour, not one number; the water box drifts by a systematic amount
+(CM3D's RESPA with flexible bonds at a 2 fs outer step), which both share.
 The plain engine also follows CM3D's ham step by step at the start.
 """
 import json
@@ -58,8 +60,8 @@ def test_nve_drift_no_worse_than_cm3d(engine_lib, cm3d_runs, name):
         if mode == _abi.PLAIN_FP64:
             # the same trajectory as CM3D's at the start (10 steps)
             np.testing.assert_allclose(ham[:10], ref["ham"][:10], rtol=1e-9)
-        bound = abs(want["drift_per_atom_per_ns"]) + 3.0 * (want["drift_se_per_atom_per_ns"] +
-                                                             got["drift_se_per_atom_per_ns"])
+        bound = 1.1 * abs(want["drift_per_atom_per_ns"]) + 3.0 * (want["drift_se_per_atom_per_ns"] +
+                                                                   got["drift_se_per_atom_per_ns"])
         assert abs(got["drift_per_atom_per_ns"]) <= bound, (key, got, want)
     print("NVE", name, json.dumps(out))
     path = os.environ.get("CM3D_NB_ERRLOG")
