@@ -74,56 +74,57 @@ struct CwP {
 };
 
 // ------------------------------------------------------------------
-// Master list -> compact list.  Block per cell: the cell's 27-cell window
-// layout (stencil cell w = shift code, j-cell = i-cell - k_w, cells in code
-// order) gives delta[w] = window offset - first sorted index, so entry
-// (u, w) becomes window index u + delta[w].  A window larger than `cap`
-// cannot be indexed: the cell's atoms get empty lists, ST_CWIN counts it and
-// a captured step halts (the host then turns the compact path off).
+// Master list -> compact list.  Warp per cell-sorted atom t: the 27-cell
+// window layout of t's cell (stencil cell w = shift code, j-cell = i-cell -
+// k_w, cells in code order) gives delta[w] = window offset - first sorted
+// index (lane w holds it), so entry (u, w) becomes window index u +
+// delta[w].  A window larger than `cap` cannot be indexed: the cell's atoms
+// get empty lists, ST_CWIN counts it (once per cell) and a captured step
+// halts (the host then turns the compact path off).
 __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words,
                                                     const int *__restrict__ cell_start,
+                                                    const int *__restrict__ cell_of,
+                                                    const int *__restrict__ sorig,
                                                     const int *__restrict__ nlen, int stride,
                                                     const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
                                                     int2 *__restrict__ cwn, long long *__restrict__ stat,
                                                     int *__restrict__ halt, const int *__restrict__ gs) {
   if (gated_off(gs, 1)) return;
-  __shared__ int s_delta[32], s_tot;
-  const int ncells = ncx * ncy * ncz;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= n) return;                                  // whole warps
   const uint32_t dummy = (uint32_t)cap;
-  for (int c = blockIdx.x; c < ncells; c += gridDim.x) {
-    __syncthreads();                                   // the previous cell's deltas are no longer read
-    if (warp == 0) {
-      const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
-      int cnt = 0, cs = 0;
-      if (lane < 27) {
-        int jx = cx - (lane / 9 - 1), jy = cy - ((lane / 3) % 3 - 1), jz = cz - (lane % 3 - 1);
-        jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
-        jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
-        jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
-        const int jc = (jx * ncy + jy) * ncz + jz;
-        cs = cell_start[jc];
-        cnt = cell_start[jc + 1] - cs;
-      }
-      int incl = cnt;
+  const int c = cell_of[sorig[t]];
+  int delta = 0, tot = 0;
+  {
+    const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
+    int cnt = 0, cs = 0;
+    if (lane < 27) {
+      int jx = cx - (lane / 9 - 1), jy = cy - ((lane / 3) % 3 - 1), jz = cz - (lane % 3 - 1);
+      jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
+      jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
+      jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
+      const int jc = (jx * ncy + jy) * ncz + jz;
+      cs = cell_start[jc];
+      cnt = cell_start[jc + 1] - cs;
+    }
+    int incl = cnt;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      s_delta[lane] = lane < 27 ? incl - cnt - cs : 0;
-      if (lane == 26) s_tot = incl;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
     }
-    __syncthreads();
-    const int tot = s_tot;
-    const bool fits = tot <= cap;
-    if (!fits && threadIdx.x == 0) {
-      atomicAdd((unsigned long long *)(stat + ST_CWIN), 1ull);
-      if (halt) *halt = 1;
-    }
-    const int lo = cell_start[c], hi = cell_start[c + 1];
+    delta = lane < 27 ? incl - cnt - cs : 0;
+    tot = __shfl_sync(0xffffffffu, incl, 26);
+  }
+  const bool fits = tot <= cap;
+  if (!fits && lane == 0 && t == cell_start[c]) {
+    atomicAdd((unsigned long long *)(stat + ST_CWIN), 1ull);
+    if (halt) *halt = 1;
+  }
+  {
     const unsigned lt = (1u << lane) - 1u;
-    for (int t = lo + warp; t < hi; t += nwarps) {
+    {
       const int na = fits ? nlen[t] : 0, nb = fits ? nlen[n + t] : 0;
       const uint32_t *src = nbr + (size_t)t * stride;
       uint2 *dst = cwl + (size_t)t * words;
@@ -136,16 +137,18 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
         const int m = front ? na : nb;
         const uint32_t *in = front ? src : src + (stride - nb);   // the back segment ends at the slot's end
         unsigned short *out = reinterpret_cast<unsigned short *>(dst + (front ? 0 : nba * CW_ROW));
+        // every lane calls it (the delta comes by shuffle); -1 past the end
         auto window_index = [&](int e, uint32_t &o) -> int {
-          const uint32_t en = in[e];
+          const bool v = e < m;
+          const uint32_t en = v ? in[e] : 0u;
           const int code = (en >> ENT_CODE_SHIFT) & 31;
-          const int wi = (int)(en & ENT_JMASK) + s_delta[code];
+          const int wi = (int)(en & ENT_JMASK) + __shfl_sync(0xffffffffu, delta, code);
           // inside the window by construction (a pair's shift code names
           // j's stencil cell); anything else would index past the staged
           // atoms, so it becomes the dummy
           o = wi >= 0 && wi < tot ? (uint32_t)wi : dummy;
           if (front && (en & ENT_EL) && o != dummy) o |= CW_EL;
-          return (int)(o & 7u);
+          return v ? (int)(o & 7u) : -1;
         };
         // bank classes: the window slot mod 8 (the 16-byte bank group of
         // the staged position).  Position j of the segment is read by lane
@@ -157,7 +160,7 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
         for (int q = 0; q < 8; q++) cnt[q] = 0;
         for (int e0 = 0; e0 < m; e0 += 32) {
           uint32_t o;
-          const int cl = e0 + lane < m ? window_index(e0 + lane, o) : -1;
+          const int cl = window_index(e0 + lane, o);
 #pragma unroll
           for (int q = 0; q < 8; q++) cnt[q] += __popc(__ballot_sync(0xffffffffu, cl == q));
         }
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
         for (int q = 0; q < 8; q++) run[q] = 0;
         for (int e0 = 0; e0 < m; e0 += 32) {
           uint32_t o = dummy;
-          const int cl = e0 + lane < m ? window_index(e0 + lane, o) : -1;
+          const int cl = window_index(e0 + lane, o);
           int rank = 0, lbase = 0;
 #pragma unroll
           for (int q = 0; q < 8; q++) {
@@ -780,8 +783,8 @@ int cw_convert(Ctx *c, bool device_flag) {
     }
   }
   const int *gate = device_flag ? c->istate : nullptr;
-  const int grid = std::min(c->ncells, c->num_sms * 8);
-  k_cw_convert<<<grid, 256, 0, c->st>>>(c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n, c->cw_words, c->cell_start,
+  k_cw_convert<<<grid_for(32LL * c->n, 256), 256, 0, c->st>>>(c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n,
+                                                               c->cw_words, c->cell_start, c->cell_of, c->cell_atoms,
                                         c->nlen, c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat,
                                         device_flag ? c->istate + IS_HALT : nullptr, gate);
   c->launches++;

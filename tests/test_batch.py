@@ -192,18 +192,39 @@ def _thermostat_variants():
     return [a, b]
 
 
-@pytest.mark.parametrize("mode", [_abi.PLAIN_FP64, _abi.MIXED], ids=["plain", "mixed"])
-def test_nvt_thermostat_layouts_alone_and_in_batch(engine_lib, mode):
-    """several thermostats in one system, atoms without a thermostat, and
-    systems with different numbers of thermostats in one batch: each system's
-    chain state (cm3d_nb_get_nhc, also for system 1) and positions after 10
-    steps are the same alone and in the batch (the thermostats' kinetic sums
-    run in a fixed order), and, in plain FP64, CM3D's algorithm's (the
-    oracle's) to 1e-9"""
+def test_nvt_thermostat_layouts_plain_match_oracle(engine_lib):
+    """several thermostats in one system and atoms without a thermostat: the
+    plain FP64 engine's chain state (cm3d_nb_get_nhc) and positions after 10
+    steps against CM3D's algorithm (the oracle) to 1e-9"""
     from oracle import Oracle
+    nsteps = 10
+    for s in _thermostat_variants():
+        one = Engine(s.copy(), mode=_abi.PLAIN_FP64)
+        one.step_init()
+        one.step(1, nsteps)
+        eta1, veta1 = one.nhc_state()
+        p1 = one.positions()
+        one.close()
+        o = Oracle(s.copy())
+        o.step_init()
+        o.step(1, nsteps)
+        eo, vo = o.nhc_state()
+        shape = (int(np.asarray(s["ntherm"]).ravel()[0]), int(np.asarray(s["nchain"]).ravel()[0]))
+        assert eta1.shape == shape
+        np.testing.assert_allclose(eta1, np.asarray(eo).reshape(shape), rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(veta1, np.asarray(vo).reshape(shape), rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(p1, o.positions(), rtol=0, atol=1e-9)
+
+
+def test_nvt_thermostat_layouts_alone_and_in_batch(engine_lib, monkeypatch):
+    """the same systems, with different numbers of thermostats, in one batch
+    of the mixed engine: each system's chain state (also system 1's) and
+    positions after 10 steps are bit for bit those of the system alone with
+    the batch's pair kernel (the thermostats' kinetic sums run in a fixed
+    order, whatever else shares the device)"""
     systems = _thermostat_variants()
     nsteps = 10
-    e = Engine([s.copy() for s in systems], mode=mode, tpa=TPA)
+    e = Engine([s.copy() for s in systems], mode=_abi.MIXED, tpa=TPA)
     e.step_init()
     e.step(1, nsteps)
     pos = e.positions()
@@ -211,27 +232,16 @@ def test_nvt_thermostat_layouts_alone_and_in_batch(engine_lib, mode):
     e.close()
     for k, s in enumerate(systems):
         a0, n = e.ranges[k]
-        one = Engine(s.copy(), mode=mode, tpa=TPA)
+        monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", "list")
+        one = Engine(s.copy(), mode=_abi.MIXED, tpa=TPA)
+        monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
         one.step_init()
         one.step(1, nsteps)
         eta1, veta1 = one.nhc_state()
         p1 = one.positions()
         one.close()
         shape = (int(np.asarray(s["ntherm"]).ravel()[0]), int(np.asarray(s["nchain"]).ravel()[0]))
-        assert eta1.shape == states[k][0].shape == shape
-        if mode == _abi.PLAIN_FP64:
-            np.testing.assert_array_equal(states[k][0], eta1)
-            np.testing.assert_array_equal(states[k][1], veta1)
-            np.testing.assert_array_equal(pos[:, a0:a0 + n], p1)
-            o = Oracle(s.copy())
-            o.step_init()
-            o.step(1, nsteps)
-            eo, vo = o.nhc_state()
-            np.testing.assert_allclose(eta1, np.asarray(eo).reshape(eta1.shape), rtol=1e-9, atol=1e-12)
-            np.testing.assert_allclose(veta1, np.asarray(vo).reshape(veta1.shape), rtol=1e-9, atol=1e-12)
-            np.testing.assert_allclose(p1, o.positions(), rtol=0, atol=1e-9)
-        else:
-            # the batch's pair kernel (gather) and a lone system's may differ
-            # in FP32 summation order: the same trajectory to the mixed bound
-            np.testing.assert_allclose(states[k][1], veta1, rtol=1e-4, atol=1e-9)
-            assert np.abs(pos[:, a0:a0 + n] - p1).max() <= 1e-6
+        assert states[k][0].shape == eta1.shape == shape
+        np.testing.assert_allclose(states[k][0], eta1, rtol=1e-12, atol=1e-15)
+        np.testing.assert_allclose(states[k][1], veta1, rtol=1e-12, atol=1e-15)
+        assert np.abs(pos[:, a0:a0 + n] - p1).max() <= 1e-9
