@@ -61,6 +61,7 @@ class Workload:
     box: float = 0.0                     # cubic edge, Angstrom
     temp: float = 0.0
     dt_fs: float = 1.0
+    therm_opt: str = "none"              # each species' \mol_therm_opt (nvt: "global")
 
     @property
     def natoms(self) -> int:
@@ -75,7 +76,7 @@ class Workload:
         out = []
         for idx, (mol, nmol, _top) in enumerate(self.species, start=1):
             out.append(f"~mol_def[\\mol_parm_file{{{mol}.top}} "
-                       f"\\mol_therm_opt{{none}} \\nmol{{{nmol}}} "
+                       f"\\mol_therm_opt{{{self.therm_opt}}} \\nmol{{{nmol}}} "
                        f"\\mol_index{{{idx}}}]")
         return "\n".join(out) + "\n"
 
@@ -162,9 +163,13 @@ def _null_parm(a: str, b: str) -> str:
 # ----------------------------------------------------------------- argon
 def argon_fcc(ncell: int = 6, density: float = 0.8442, temp: float = 120.0,
               seed: int = 1, rc_sigma: float = 2.5, skin_sigma: float = 0.3,
-              dt_fs: float = 5.0, ntime: int = 1000, name: str = "argon") -> Workload:
+              dt_fs: float = 5.0, ntime: int = 1000, name: str = "argon",
+              nvt_chain: int = 0) -> Workload:
     """LJ argon on an FCC lattice, reduced density `density`; cut and shifted
-    LJ at `rc_sigma` sigma; Verlet list with a `skin_sigma` sigma skin."""
+    LJ at `rc_sigma` sigma; Verlet list with a `skin_sigma` sigma skin.
+    nvt_chain > 0: CM3D's NVT with one global Nose-Hoover chain of that
+    length at `temp` (keywords ensemble nvt and len_nhc, each species'
+    mol_therm_opt global)."""
     sig, eps, mass = ARGON["sig"], ARGON["eps"], ARGON["mass"]
     n = 4 * ncell ** 3
     L = (n / density) ** (1.0 / 3.0) * sig
@@ -180,9 +185,12 @@ def argon_fcc(ncell: int = 6, density: float = 0.8442, temp: float = 120.0,
     kw = _base_keywords(name, dt_fs, temp, ntime)
     kw.update({"skin": skin_sigma * sig, "shift": 1, "nres_lrf": 1,
                "nres_intra": 1, "nres_tors": 1, "neighbor_list": "verlist"})
+    if nvt_chain > 0:
+        kw.update({"ensemble": "nvt", "len_nhc": nvt_chain})
     top = (f"~mol_name_def[\\mol_name{{argon}}\\natom{{1}}\\nbond{{0}}]\n"
            f"~atom_def[\\atom_typ{{ar}}\\atom_ind{{1}}\\mass{{{mass!r}}}\\charge{{0}}]\n")
     return Workload(name=name, keywords=kw, species=[("argon", n, top)],
+                    therm_opt="global" if nvt_chain > 0 else "none",
                     inter_parms=[_lj_parm("ar", "ar", eps, sig, 0.55 * sig, rc, rc)],
                     pos=pos, vel=vel, mass_amu=m, box=L, temp=temp, dt_fs=dt_fs)
 

@@ -20,10 +20,16 @@
  *              COORDS (CM3D's writers and geteng read them) and refills
  *              ENERGIES.
  *
- * What the engine does not compute -- thermostats and barostats, external
- * fields, dipoles, non-periodic boxes, the phased cosine torsion form --
- * stops the run through md_error with the reason, as CM3D reports
- * unsupported input; nothing falls back to a CPU path.
+ * NVT (Nose-Hoover chains, intnhc_new in md_step.c:117): CM3D's chain state
+ * (COORDS.eta / veta / mnh / gkt, SIMPARMS.ntherm / nchain, ithm) goes to
+ * the engine at step_init, and after every step the chains' eta and veta
+ * come back into COORDS, where CM3D's thermostat energy (getengn) and its
+ * restart writer read them.
+ *
+ * What the engine does not compute -- barostats (npt_*), external fields,
+ * dipoles, non-periodic boxes, the phased cosine torsion form -- stops the
+ * run through md_error with the reason, as CM3D reports unsupported input;
+ * nothing falls back to a CPU path.
  *
  * Environment: CM3D_NB_MODE=plain selects the plain FP64 engine (default:
  * mixed), CM3D_NB_DEVICE the CUDA device (default 0).
@@ -35,6 +41,7 @@
 static cm3d_nb_ctx *g_ctx = NULL;
 static int *g_map = NULL, *g_eoff = NULL, *g_eidx = NULL, *g_coff = NULL, *g_cidx = NULL;
 static double *g_v14 = NULL, *g_dv14 = NULL;
+static double *g_nhc = NULL;   /* NVT: mnh | gkt | eta | veta, ntherm * nchain each (row-major) */
 
 static void nb_fail(const char *what)
 {
@@ -59,7 +66,8 @@ static void unsupported(const char *what)
 static void check_supported(SIMPARMS *simparms, COORDS *coords)
 {
   if (simparms->iperd != 3) unsupported("a non-periodic or partially periodic box (iperd != 3)");
-  if (simparms->iensemble != 0) unsupported("an ensemble other than nve");
+  if (simparms->iensemble != 0 && simparms->iensemble != 1)
+    unsupported("a barostat (an ensemble other than nve or nvt)");
   if (simparms->ivol) unsupported("a variable cell (ivol)");
   if (simparms->iextern) unsupported("an external field");
   if (simparms->ipolar) unsupported("polarizable dipoles");
@@ -208,6 +216,27 @@ static void create_engine(SIMPARMS *simparms, COORDS *coords, INTER *inter)
   }
   s.nfreeze = simparms->nfreeze;
   s.ifreeze = coords->ifreeze;
+  if (simparms->iensemble == 1) {
+    /* CM3D's chains are dmatrix rows [ntherm][nchain]: flat copies */
+    int j, k, nt = simparms->ntherm, nc = simparms->nchain;
+    size_t tc = (size_t)nt * nc;
+    g_nhc = (double *)malloc(sizeof(double) * 4 * (tc > 0 ? tc : 1));
+    for (j = 0; j < nt; j++)
+      for (k = 0; k < nc; k++) {
+        g_nhc[(size_t)j * nc + k] = coords->mnh[j][k];
+        g_nhc[tc + (size_t)j * nc + k] = coords->gkt[j][k];
+        g_nhc[2 * tc + (size_t)j * nc + k] = coords->eta[j][k];
+        g_nhc[3 * tc + (size_t)j * nc + k] = coords->veta[j][k];
+      }
+    s.iensemble = 1;
+    s.ntherm = nt;
+    s.nchain = nc;
+    s.ithm = coords->ithm;
+    s.mnh = g_nhc;
+    s.gkt = g_nhc + tc;
+    s.nhc_eta = g_nhc + 2 * tc;
+    s.nhc_veta = g_nhc + 3 * tc;
+  }
 
   cm3d_nb_default_options(&opt);
   if (mode && strcmp(mode, "plain") == 0) opt.mode = CM3D_NB_PLAIN_FP64;
@@ -264,10 +293,21 @@ static void fill_energies(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies
   (void)coords;
 }
 
-static void pull_state(COORDS *coords)
+static void pull_state(SIMPARMS *simparms, COORDS *coords)
 {
   nb_check(cm3d_nb_get_positions(g_ctx, coords->px, coords->py, coords->pz), "cm3d_nb_get_positions");
   nb_check(cm3d_nb_get_velocities(g_ctx, coords->vx, coords->vy, coords->vz), "cm3d_nb_get_velocities");
+  if (g_nhc) {
+    /* the chains as the step left them (cm3d_nb_get_nhc) into COORDS */
+    int j, k, nt = simparms->ntherm, nc = simparms->nchain;
+    size_t tc = (size_t)nt * nc;
+    nb_check(cm3d_nb_get_nhc(g_ctx, 0, g_nhc + 2 * tc, g_nhc + 3 * tc, NULL, NULL), "cm3d_nb_get_nhc");
+    for (j = 0; j < nt; j++)
+      for (k = 0; k < nc; k++) {
+        coords->eta[j][k] = g_nhc[2 * tc + (size_t)j * nc + k];
+        coords->veta[j][k] = g_nhc[3 * tc + (size_t)j * nc + k];
+      }
+  }
 }
 
 static void pull_forces(COORDS *coords)
@@ -316,7 +356,7 @@ void step(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, 
 {
   (void)inter;
   nb_check(cm3d_nb_step(g_ctx, simparms->istep, 1), "step");
-  pull_state(coords);
+  pull_state(simparms, coords);
   list_counts(ngbr);
   fill_energies(simparms, coords, energies);
   gettngbr(ngbr);

@@ -45,6 +45,10 @@ NUM = re.compile(r"[-+]?\d+(?:\.\d*)?(?:[eE][-+]?\d+)?")
 def deck(kind: str):
     if kind == "argon":
         wl = configs.argon_fcc(ncell=4, ntime=20)
+    elif kind == "argon_nvt":
+        # CM3D's NVT: one global Nose-Hoover chain of length 3 (the chain
+        # state goes to the engine and comes back into COORDS every step)
+        wl = configs.argon_fcc(ncell=4, ntime=20, nvt_chain=3)
     else:
         wl = configs.water_box(ngrid=6, ntime=20, seed=7, placement="octant")
     wl.keywords["iwr_screen"] = 10
@@ -123,7 +127,7 @@ def compare(cpu_out: str, gpu_out: str, rtol: float, atol: float, exact_counts: 
 @needs_bins
 @pytest.mark.gpu
 @pytest.mark.timeout(900)
-@pytest.mark.parametrize("kind", ["argon", "water"])
+@pytest.mark.parametrize("kind", ["argon", "water", "argon_nvt"])
 @pytest.mark.parametrize("mode", ["plain", "mixed"])
 def test_relinked_cm3d_matches_cm3d(tmp_path, kind, mode):
     wl = deck(kind)
