@@ -105,4 +105,4 @@ class Energies(C.Structure):
 class Status(C.Structure):
     _fields_ = [("table_underflow", C.c_longlong), ("rebuilds", C.c_longlong),
                 ("resets", C.c_longlong), ("overflows", C.c_longlong),
-                ("nonfinite", C.c_int), ("last_istep", C.c_int)]
+                ("nonfinite", C.c_int), ("last_istep", C.c_int), ("stage_timeouts", C.c_int)]

@@ -1036,6 +1036,7 @@ int cm3d_nb_get_status(cm3d_nb_ctx *ctx, cm3d_nb_status_t *st) {
   st->overflows = c->overflows_host;
   st->nonfinite = (int)c->h_stat[ST_NONFINITE];
   st->last_istep = c->h_istate[IS_ISTEP];
+  st->stage_timeouts = (int)c->h_stat[ST_STAGE_TIMEOUT];
   return CM3D_NB_OK;
 }
 

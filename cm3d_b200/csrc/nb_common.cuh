@@ -96,7 +96,8 @@ enum {
   ST_BADSHIFT = 5,        // a pair's cell shift fell outside the 27-entry table
   ST_NEED_STRIDE = 6,     // longest full list that did not fit its slot
   ST_CWIN = 7,            // a cell window too large for the compact list (nb_cwin.cu)
-  ST_COUNT = 8
+  ST_STAGE_TIMEOUT = 8,   // a window's bulk copies not complete within the wait limit (nb_cwin.cu)
+  ST_COUNT = 9
 };
 // device integer state
 enum {

@@ -264,6 +264,39 @@ __device__ __forceinline__ float2 lds_f2(unsigned a) {
   return v;
 }
 
+// Window staging by bulk copies (TMA, cp.async.bulk, no multicast: the
+// source is this GPU's own memory) completing on a block mbarrier.
+__device__ __forceinline__ void mbar_init(unsigned bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Generic-proxy accesses of the window (the previous item's reads) before
+// the async-proxy writes of the next copies.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// Waits for the phase of the given parity to complete; false after `limit`
+// polls (each try_wait may suspend the thread for a while first).
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int limit) {
+  for (int it = 0; it < limit; it++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+constexpr int CW_WAIT_LIMIT = 1 << 22;
+
 // One electrostatic pair: qj = j's charge, or 0 for an LJ-segment pair
 // outside the te list.  tfb / tgb: this lane's table copies as 32-bit shared
 // addresses less MAGIC_BITS knots, so that the float bits of the split
@@ -344,6 +377,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   __shared__ int s_map[256];
   __shared__ float4 s_cut[64];                                        // LJM 2: {rc2, dx2, off, vt}
   __shared__ double s_red[CW_THREADS / 32][CQ_COUNT];
+  __shared__ __align__(8) unsigned long long s_mbar;
   static_assert(CQ_COUNT == 16, "the transposing reduction gives lane pair q quantity q of 16");
 
   for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = gshift[k];
@@ -357,9 +391,12 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     for (int k = threadIdx.x; k < P.ninter; k += blockDim.x)
       s_cut[k] = make_float4(gfcut[8 * k], gfcut[8 * k + 2], gfcut[8 * k + 1], gfcut[8 * k + 3]);
   }
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_mbar);
+  unsigned phase = 0;
   if (threadIdx.x == 0) {
     wx[P.cap] = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);   // the dummy entry's partner: out of range
     if (LJM == 2) wt[P.cap] = 0;
+    mbar_init(bar);
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr int NWARP = CW_THREADS / 32;
@@ -403,33 +440,40 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     // a window that does not fit was given empty lists by k_cw_convert
     const bool staged = tot <= P.cap;
     if (staged) {
-      // one pass over the whole window, two slots per thread in flight:
-      // staged slot g lies in the last stencil cell w with s_off[w] <= g
-      for (int g0 = threadIdx.x; g0 < tot; g0 += 2 * CW_THREADS) {
-        int gg[2], uu[2], ww[2];
-        float4 xx[2];
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          const int g = g0 + h * CW_THREADS;
-          int wa = 0, wb = 27;
-          while (wb - wa > 1) {
-            const int mid = (wa + wb) >> 1;
-            if (s_off[mid] <= g) wa = mid;
-            else wb = mid;
-          }
-          gg[h] = g;
-          ww[h] = wa;
-          uu[h] = s_cs[wa] + (g - s_off[wa]);
-          xx[h] = g < tot ? xq[uu[h]] : make_float4(0.f, 0.f, 0.f, 0.f);
+      // each stencil cell's atoms are a contiguous run of the cell-sorted
+      // positions: one bulk copy per cell into its window range (16-byte
+      // rows, so every address and size is a multiple of 16), all
+      // completing on the block's mbarrier
+      if (warp == 0) {
+        fence_async_smem();
+        if (lane == 0) mbar_expect(bar, (unsigned)tot * (unsigned)sizeof(float4));
+        __syncwarp();
+        if (lane < 27) {
+          const int cnt = s_off[lane + 1] - s_off[lane];
+          if (cnt > 0)
+            bulk_g2s(wxb + (unsigned)s_off[lane] * (unsigned)sizeof(float4), xq + s_cs[lane],
+                     (unsigned)cnt * (unsigned)sizeof(float4), bar);
         }
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-          if (gg[h] < tot) {
-            const float4 sh = s_shift[ww[h]], shl = s_shift[27 + ww[h]];
-            const float4 x = xx[h];
-            wx[gg[h]] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
-            if (LJM == 2) wt[gg[h]] = (unsigned char)styp[uu[h]];
-          }
+      }
+      const bool arrived = mbar_wait(bar, phase, CW_WAIT_LIMIT);
+      phase ^= 1u;
+      if (!__syncthreads_and(arrived)) {
+        // the copies did not complete (never seen): count it, wait once
+        // more for copies still in flight, and leave the block's remaining
+        // items undone; the host reads the count in the status
+        if (threadIdx.x == 0) atomicAdd((unsigned long long *)(stat + ST_STAGE_TIMEOUT), 1ull);
+        mbar_wait(bar, phase ^ 1u, CW_WAIT_LIMIT);
+        return;
+      }
+      // the cell's periodic shift and the cell-relative origin, in place
+      // (and the types of a multi-type system)
+      for (int w = warp; w < 27; w += NWARP) {
+        const float4 sh = s_shift[w], shl = s_shift[27 + w];
+        const int g0 = s_off[w], g1 = s_off[w + 1], u0 = s_cs[w] - g0;
+        for (int g = g0 + lane; g < g1; g += 32) {
+          const float4 x = wx[g];
+          wx[g] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
+          if (LJM == 2) wt[g] = (unsigned char)styp[u0 + g];
         }
       }
     }

@@ -190,6 +190,10 @@ typedef struct cm3d_nb_status_t {
   long long overflows;        /* list-capacity overflows handled by regrowth */
   int nonfinite;              /* a NaN/Inf reached the forces or energies */
   int last_istep;
+  int stage_timeouts;         /* pair-kernel blocks whose window copies did not
+                                 complete within the wait limit (their work was
+                                 not done: the step's results are invalid);
+                                 0 in every run so far */
 } cm3d_nb_status_t;
 
 typedef struct cm3d_nb_ctx cm3d_nb_ctx;

@@ -149,6 +149,8 @@ def test_compact_repeats_bit_for_bit(engine_lib):
         e.force(1)
         runs.append((e.forces(_abi.FXL), e.getsvirter_e(), e.getsvirter()))
     assert e.pair_kernel()[0] == "compact"
+    # every block's window copies (bulk copies on an mbarrier) completed
+    assert e.status()["stage_timeouts"] == 0
     e.close()
     for f, ve, vl in runs[1:]:
         np.testing.assert_array_equal(f, runs[0][0])
