@@ -33,6 +33,24 @@
  *
  * Environment: CM3D_NB_MODE=plain selects the plain FP64 engine (default:
  * mixed), CM3D_NB_DEVICE the CUDA device (default 0).
+ *
+ * Compiled with -DCM3D_NB_ROUTE_B the same file is the routine-level
+ * binding instead: CM3D keeps its own step() and host integrator
+ * (md_step.c, thermostat included), and only the nonbonded routines go to
+ * the engine --
+ *
+ *   get_ngbr   (energy/control/ngbr_list.c:297, with get_ngbr_e) the
+ *              engine's four lists from the current positions;
+ *   nrefsh     (energy/control/md_finter.c:43) the engine's skin test and
+ *              RESETPOS pull-back (cm3d_nb_nrefsh), positions read back;
+ *   force      (energy/control/md_fcntr.c:44) every level on the engine,
+ *              positions in and the level's force block out per call;
+ *   getvireal  (energy/control/md_fcntr.c:136) ENERGIES from the engine's
+ *              accumulators, as for route A.
+ *
+ * CM3D's objects that define these four (md_fcntr.o, md_finter.o,
+ * ngbr_list.o) are linked as copies in which the four symbols are weak, so
+ * that the definitions here take their place (cm3d_b200/shim/Makefile).
  */
 #include "md.h"
 
@@ -66,8 +84,11 @@ static void unsupported(const char *what)
 static void check_supported(SIMPARMS *simparms, COORDS *coords)
 {
   if (simparms->iperd != 3) unsupported("a non-periodic or partially periodic box (iperd != 3)");
+#ifndef CM3D_NB_ROUTE_B
+  /* route B: CM3D's own step integrates the chains on the host */
   if (simparms->iensemble != 0 && simparms->iensemble != 1)
     unsupported("a barostat (an ensemble other than nve or nvt)");
+#endif
   if (simparms->ivol) unsupported("a variable cell (ivol)");
   if (simparms->iextern) unsupported("an external field");
   if (simparms->ipolar) unsupported("polarizable dipoles");
@@ -216,6 +237,7 @@ static void create_engine(SIMPARMS *simparms, COORDS *coords, INTER *inter)
   }
   s.nfreeze = simparms->nfreeze;
   s.ifreeze = coords->ifreeze;
+#ifndef CM3D_NB_ROUTE_B
   if (simparms->iensemble == 1) {
     /* CM3D's chains are dmatrix rows [ntherm][nchain]: flat copies */
     int j, k, nt = simparms->ntherm, nc = simparms->nchain;
@@ -237,6 +259,7 @@ static void create_engine(SIMPARMS *simparms, COORDS *coords, INTER *inter)
     s.nhc_eta = g_nhc + 2 * tc;
     s.nhc_veta = g_nhc + 3 * tc;
   }
+#endif
 
   cm3d_nb_default_options(&opt);
   if (mode && strcmp(mode, "plain") == 0) opt.mode = CM3D_NB_PLAIN_FP64;
@@ -334,6 +357,7 @@ static void list_counts(NGBR *ngbr)
   nb_check(cm3d_nb_list_count(g_ctx, CM3D_NB_LIST_SE, &c), "list_count"); ngbr->nprse = (int)c;
 }
 
+#ifndef CM3D_NB_ROUTE_B
 void step_init(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, NGBR *ngbr)
 {
   check_supported(simparms, coords);
@@ -361,3 +385,83 @@ void step(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, 
   fill_energies(simparms, coords, energies);
   gettngbr(ngbr);
 }
+#else /* CM3D_NB_ROUTE_B */
+
+static void push_positions(COORDS *coords)
+{
+  nb_check(cm3d_nb_set_positions(g_ctx, coords->px, coords->py, coords->pz), "set_positions");
+}
+
+/* get_ngbr (energy/control/ngbr_list.c:297): the first call -- from CM3D's
+   step_init -- creates the engine from SIMPARMS / COORDS / INTER; every call
+   builds the engine's lists from COORDS' positions and sets NGBR's pair
+   counts and update (CM3D's own host lists are not built) */
+void get_ngbr(SIMPARMS *simparms, COORDS *coords, INTER *inter, NGBR *ngbr)
+{
+  if (!g_ctx) {
+    check_supported(simparms, coords);
+    create_engine(simparms, coords, inter);
+  } else {
+    push_positions(coords);
+  }
+  nb_check(cm3d_nb_get_ngbr(g_ctx), "get_ngbr");
+  list_counts(ngbr);
+}
+
+/* nrefsh (energy/control/md_finter.c:43): the skin test against the last
+   build's positions, RESETPOS, and the rebuild, on the engine; a rebuild
+   may have pulled positions back, so COORDS gets them again */
+void nrefsh(SIMPARMS *simparms, COORDS *coords, INTER *inter, NGBR *ngbr)
+{
+  int rebuilt = 0;
+  (void)inter;
+  push_positions(coords);
+  nb_check(cm3d_nb_nrefsh(g_ctx, simparms->istep, &rebuilt), "nrefsh");
+  if (rebuilt) {
+    nb_check(cm3d_nb_get_positions(g_ctx, coords->px, coords->py, coords->pz), "get_positions");
+    list_counts(ngbr);
+  }
+}
+
+/* force (energy/control/md_fcntr.c:44): the level on the engine, its force
+   block(s) back as accelerations; frozen atoms' velocities go through the
+   engine's freeze_atom too */
+void force(SIMPARMS *simparms, COORDS *coords, INTER *inter, NGBR *ngbr, int iflg)
+{
+  (void)inter;
+  (void)ngbr;
+  push_positions(coords);
+  if (simparms->nfreeze > 0)
+    nb_check(cm3d_nb_set_velocities(g_ctx, coords->vx, coords->vy, coords->vz), "set_velocities");
+  nb_check(cm3d_nb_force(g_ctx, iflg), "force");
+  switch (iflg) {
+    case 1:
+      nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXL, coords->fxl, coords->fyl, coords->fzl), "get_forces");
+      /* fall through: level 1 also refills fxs */
+    case 0:
+      nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXS, coords->fxs, coords->fys, coords->fzs), "get_forces");
+      break;
+    case 2:
+      nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXA, coords->fxa, coords->fya, coords->fza), "get_forces");
+      break;
+    case 3:
+      nb_check(cm3d_nb_get_forces(g_ctx, CM3D_NB_FXR, coords->fxr, coords->fyr, coords->fzr), "get_forces");
+      break;
+    default:
+      md_error("force: level out of range");
+  }
+  if (simparms->nfreeze > 0)
+    nb_check(cm3d_nb_get_velocities(g_ctx, coords->vx, coords->vy, coords->vz), "get_velocities");
+}
+
+/* getvireal (energy/control/md_fcntr.c:136) for iflg 1, the only form
+   CM3D's step and step_init use: the engine's accumulators of the last
+   force(1) and its bonded terms */
+void getvireal(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, NGBR *ngbr, int iflg)
+{
+  (void)inter;
+  (void)ngbr;
+  if (iflg != 1) md_error("GPU nonbonded engine: getvireal is bound for iflg 1 only");
+  fill_energies(simparms, coords, energies);
+}
+#endif /* CM3D_NB_ROUTE_B */

@@ -32,10 +32,18 @@ from cm3d_b200 import configs
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CPU_CM3D = os.path.join(ROOT, "oracle", "_ref", "cm3d")
 GPU_CM3D = os.path.join(ROOT, "cm3d_b200", "shim", "_build", "cm3d_gpu")
+# route B: CM3D's own step() and host integrator; get_ngbr, nrefsh, force and
+# getvireal bound to the engine
+GPU_CM3D_B = os.path.join(ROOT, "cm3d_b200", "shim", "_build", "cm3d_gpu_b")
 
 needs_bins = pytest.mark.skipif(
     not (os.path.exists(CPU_CM3D) and os.path.exists(GPU_CM3D)),
     reason="CM3D and its relinked build are made from the CM3D source tree (make -C oracle ref; "
+           "make -C cm3d_b200/shim)")
+
+needs_bins_b = pytest.mark.skipif(
+    not (os.path.exists(CPU_CM3D) and os.path.exists(GPU_CM3D_B)),
+    reason="CM3D and its route-B build are made from the CM3D source tree (make -C oracle ref; "
            "make -C cm3d_b200/shim)")
 
 VAL = re.compile(r"^<([^>]+)>\s*=\s*(\S+)\s*~\s*(\S+)")
@@ -147,6 +155,45 @@ def test_relinked_cm3d_matches_cm3d(tmp_path, kind, mode):
     assert pc.shape == pg.shape == (wl.natoms, 3)
     np.testing.assert_array_equal(hc, hg)
     assert float(np.abs(pg - pc).max()) <= pos_tol
+
+
+@needs_bins_b
+@pytest.mark.gpu
+@pytest.mark.timeout(900)
+@pytest.mark.parametrize("kind", ["argon", "water", "argon_nvt"])
+@pytest.mark.parametrize("mode", ["plain", "mixed"])
+def test_route_b_binding_matches_cm3d(tmp_path, kind, mode):
+    """Route B: CM3D's own step() (its RESPA loop and, for NVT, its
+    Nose-Hoover chains on the host) with the neighbour lists, the skin test
+    and every force level on the engine -- positions in and forces out at
+    each call.  Same reports and tolerances as the relinked step."""
+    wl = deck(kind)
+    rc, cpu_out = run(CPU_CM3D, wl, tmp_path / "cpu")
+    assert rc == 0, cpu_out[-2000:]
+    rc, gpu_out = run(GPU_CM3D_B, wl, tmp_path / "gpu", {"CM3D_NB_MODE": mode, "CM3D_NB_DEVICE": "0"})
+    assert rc == 0, gpu_out[-2000:]
+    if mode == "plain":
+        compare(cpu_out, gpu_out, rtol=1e-7, atol=3e-6, exact_counts=True)
+        pos_tol = 3e-4
+    else:
+        compare(cpu_out, gpu_out, rtol=2e-4, atol=3e-6, exact_counts=False)
+        pos_tol = 2e-3
+    pc, hc = read_restart(str(tmp_path / "cpu" / f"{wl.name}.rest_N"))
+    pg, hg = read_restart(str(tmp_path / "gpu" / f"{wl.name}.rest_N"))
+    np.testing.assert_array_equal(hc, hg)
+    assert float(np.abs(pg - pc).max()) <= pos_tol
+
+
+@needs_bins_b
+def test_route_b_binding_without_a_device_fails_loudly(tmp_path):
+    """the bound get_ngbr (called by CM3D's own step_init) reaches the engine
+    and stops there without a device: CM3D's host list and force routines
+    are not what runs"""
+    wl = configs.argon_fcc(ncell=3, ntime=2)
+    rc, out = run(GPU_CM3D_B, wl, tmp_path, {"CUDA_VISIBLE_DEVICES": ""})
+    assert rc != 0
+    assert "GPU nonbonded engine: cm3d_nb_create" in out
+    assert "Begining Molecular Dynamics" not in out
 
 
 @needs_bins
