@@ -164,12 +164,14 @@ def _null_parm(a: str, b: str) -> str:
 def argon_fcc(ncell: int = 6, density: float = 0.8442, temp: float = 120.0,
               seed: int = 1, rc_sigma: float = 2.5, skin_sigma: float = 0.3,
               dt_fs: float = 5.0, ntime: int = 1000, name: str = "argon",
-              nvt_chain: int = 0) -> Workload:
+              nvt_chain: int = 0, npt: str = "", p_ext: float = 1.0) -> Workload:
     """LJ argon on an FCC lattice, reduced density `density`; cut and shifted
     LJ at `rc_sigma` sigma; Verlet list with a `skin_sigma` sigma skin.
     nvt_chain > 0: CM3D's NVT with one global Nose-Hoover chain of that
     length at `temp` (keywords ensemble nvt and len_nhc, each species'
-    mol_therm_opt global)."""
+    mol_therm_opt global).  npt "npt_i" or "npt_f": CM3D's barostat at
+    `p_ext` (keyword p_ext) with a chain of 3 on the volume (nbar) next to
+    the thermostat chain (length nvt_chain, 3 if not given)."""
     sig, eps, mass = ARGON["sig"], ARGON["eps"], ARGON["mass"]
     n = 4 * ncell ** 3
     L = (n / density) ** (1.0 / 3.0) * sig
@@ -185,7 +187,10 @@ def argon_fcc(ncell: int = 6, density: float = 0.8442, temp: float = 120.0,
     kw = _base_keywords(name, dt_fs, temp, ntime)
     kw.update({"skin": skin_sigma * sig, "shift": 1, "nres_lrf": 1,
                "nres_intra": 1, "nres_tors": 1, "neighbor_list": "verlist"})
-    if nvt_chain > 0:
+    if npt:
+        nvt_chain = nvt_chain or 3
+        kw.update({"ensemble": npt, "len_nhc": nvt_chain, "nbar": 3, "p_ext": p_ext})
+    elif nvt_chain > 0:
         kw.update({"ensemble": "nvt", "len_nhc": nvt_chain})
     top = (f"~mol_name_def[\\mol_name{{argon}}\\natom{{1}}\\nbond{{0}}]\n"
            f"~atom_def[\\atom_typ{{ar}}\\atom_ind{{1}}\\mass{{{mass!r}}}\\charge{{0}}]\n")

@@ -112,6 +112,47 @@ static void destroy(Ctx *c) {
 // The systems' atoms are concatenated in order; every per-system parameter
 // goes to SysP / SysH.  Batches need the mixed engine and the same ntable,
 // time step and RESPA levels in every system.
+// H^-1 and 1/det H of a system's box into its host and kernel parameters
+static void box_params(SysP &P, SysH &H) {
+  const double *h = H.hmat;
+  double *hi = H.hmati;
+  double rvol = 1. / (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
+                      h[2] * (h[3] * h[7] - h[4] * h[6]));
+  hi[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
+  hi[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
+  hi[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
+  hi[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
+  hi[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
+  hi[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
+  hi[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
+  hi[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
+  hi[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
+  P.rvol = rvol;
+  for (int k = 0; k < 9; k++) {
+    P.h[k] = H.hmat[k];
+    P.hi[k] = H.hmati[k];
+    P.hF[k] = (float)H.hmat[k];
+    P.hiF[k] = (float)H.hmati[k];
+  }
+}
+
+// width of the box along each direction (1 / |row d of H^-1|)
+static double box_width(const SysH &H, int d) {
+  return 1.0 / sqrt(H.hmati[3 * d] * H.hmati[3 * d] + H.hmati[3 * d + 1] * H.hmati[3 * d + 1] +
+                    H.hmati[3 * d + 2] * H.hmati[3 * d + 2]);
+}
+
+// boxes narrower than two list radii need the on-the-fly minimum image (for
+// the pairs near the image boundary, see near_s)
+static void box_widths(SysP &P, const SysH &H) {
+  P.smallbox = 0;
+  for (int d = 0; d < 3; d++) {
+    const double w = box_width(H, d);
+    if (w < 2.0 * H.rlist) P.smallbox = 1;
+    P.near_s[d] = 0.5 - 1.01 * H.skin / w - 1e-6;
+  }
+}
+
 static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options *opt, Ctx **out) {
   if (!systems || !out || nsys < 1) {
     set_error("cm3d_nb_create: null argument or no systems");
@@ -231,28 +272,7 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
     H.scale14e = s->n14 > 0 ? s->scale_onefour_e : 1.0;
     H.iperd = s->iperd;
     memcpy(H.hmat, s->hmat, sizeof H.hmat);
-    {
-      const double *h = H.hmat;
-      double *hi = H.hmati;
-      double rvol = 1. / (h[0] * (h[4] * h[8] - h[5] * h[7]) + h[1] * (h[5] * h[6] - h[3] * h[8]) +
-                          h[2] * (h[3] * h[7] - h[4] * h[6]));
-      hi[0] = (h[4] * h[8] - h[5] * h[7]) * rvol;
-      hi[1] = (h[2] * h[7] - h[1] * h[8]) * rvol;
-      hi[2] = (h[1] * h[5] - h[2] * h[4]) * rvol;
-      hi[3] = (h[5] * h[6] - h[3] * h[8]) * rvol;
-      hi[4] = (h[0] * h[8] - h[2] * h[6]) * rvol;
-      hi[5] = (h[2] * h[3] - h[0] * h[5]) * rvol;
-      hi[6] = (h[3] * h[7] - h[4] * h[6]) * rvol;
-      hi[7] = (h[1] * h[6] - h[0] * h[7]) * rvol;
-      hi[8] = (h[0] * h[4] - h[1] * h[3]) * rvol;
-      P.rvol = rvol;
-    }
-    for (int k = 0; k < 9; k++) {
-      P.h[k] = H.hmat[k];
-      P.hi[k] = H.hmati[k];
-      P.hF[k] = (float)H.hmat[k];
-      P.hiF[k] = (float)H.hmati[k];
-    }
+    box_params(P, H);
     P.kappa = s->kappa;
     P.kappa2 = s->kappa * s->kappa;
     P.falp2 = s->falp2;
@@ -339,15 +359,8 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
       P.rmaxl_skin2_e = P.rmaxs_skin2_e = -1.0;
     }
     H.rlist = sqrt(r2);
-    // boxes narrower than two list radii need the on-the-fly minimum image
-    // (for the pairs near the image boundary, see near_s)
-    P.smallbox = 0;
-    for (int d = 0; d < 3; d++) {
-      double w = 1.0 / sqrt(H.hmati[3 * d] * H.hmati[3 * d] + H.hmati[3 * d + 1] * H.hmati[3 * d + 1] +
-                            H.hmati[3 * d + 2] * H.hmati[3 * d + 2]);
-      if (w < 2.0 * H.rlist) P.smallbox = 1;
-      P.near_s[d] = 0.5 - 1.01 * s->skin_ter / w - 1e-6;
-    }
+    H.skin = s->skin_ter;
+    box_widths(P, H);
     a0 += ns;
   }
   c->ncoul = ncoul;
@@ -610,6 +623,55 @@ int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py, 
   CTX;
   return put3(c, c->pos, px, py, pz);
 }
+// A new box for a one-system context (a barostat's step): every parameter
+// derived from H -- H^-1, the volume, the small-box test, the cell grid's
+// neighbour shifts and the device copies the kernels read -- follows it; the
+// grid keeps its cell counts, which stays valid while every cell is at least
+// a list radius wide.
+int cm3d_nb_set_box(cm3d_nb_ctx *ctx, const double hmat[9]) {
+  CTX;
+  if (c->nsys != 1) {
+    set_error("set_box: a batch of %d systems (one system only)", c->nsys);
+    return CM3D_NB_ERR_ARG;
+  }
+  SysH H = c->hs[0];
+  SysP P = c->h_sp[0];
+  memcpy(H.hmat, hmat, sizeof H.hmat);
+  box_params(P, H);
+  if (!(P.rvol > 0.0) || !isfinite(P.rvol)) {
+    set_error("set_box: a singular or left-handed box matrix");
+    return CM3D_NB_ERR_ARG;
+  }
+  if (H.iperd == 3)
+    for (int d = 0; d < 3; d++)
+      if (box_width(H, d) / P.nc[d] < H.rlist) {
+        set_error("set_box: the box shrank below the cell grid (%d cells of width %g < list radius %g along "
+                  "direction %d); create a new context for this box",
+                  P.nc[d], box_width(H, d) / P.nc[d], H.rlist, d);
+        return CM3D_NB_ERR_STATE;
+      }
+  box_widths(P, H);
+  cell_shifts(P, H);
+  c->hs[0] = H;
+  c->h_sp[0] = P;
+  memcpy(c->hmat, H.hmat, sizeof c->hmat);
+  memcpy(c->hmati, H.hmati, sizeof c->hmati);
+  CK(cudaStreamSynchronize(c->st));
+  CK(cudaMemcpy(c->sp, c->h_sp.data(), sizeof(SysP), cudaMemcpyHostToDevice));
+  if (c->shift) {
+    CK(cudaMemcpy(c->shift, P.shift, sizeof(float4) * 27, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->shift + 27, P.shift_lo, sizeof(float4) * 27, cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(c->acc + ACC_COUNT, H.hmati, sizeof(double) * 9, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->acc + ACC_COUNT + 9, H.hmat, sizeof(double) * 9, cudaMemcpyHostToDevice));
+  // a captured step holds the old box in its launch parameters
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return CM3D_NB_OK;
+}
+
 int cm3d_nb_get_positions(cm3d_nb_ctx *ctx, double *px, double *py, double *pz) {
   CTX;
   return get3(c, c->pos, px, py, pz);

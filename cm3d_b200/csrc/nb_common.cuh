@@ -179,6 +179,7 @@ struct SysH {
   double vlrc = 0, wlrc = 0, ewald_self = 0, ewald_bkg = 0;
   double scale14 = 1, scale14e = 1;   // ONFO.scale_onefour / scale_onefour_e
   double rlist = 0;          // largest list radius (LJ or charges, with skin)
+  double skin = 0;           // INTER.skin_ter
   std::vector<int4> krows;   // k rows {ka, kb, kc0, len} of the system's k set
   std::vector<int> krow_k0;  // first k of each row (system-local)
   std::vector<int> ka, kb, kc;
@@ -470,6 +471,7 @@ int mixed_pairs(Ctx *c, int iflg, int mask);    // nb_pair.cu
 bool win_applies(Ctx *c);                       // nb_pair.cu: windowed pair kernel possible
 int build_lists(Ctx *c, bool device_flag, bool all);   // nb_list.cu
 int list_setup(Ctx *c);                         // nb_list.cu
+void cell_shifts(SysP &P, const SysH &H);       // nb_list.cu
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused
 int pair_setup(Ctx *c);                         // nb_pair.cu
 int cw_setup(Ctx *c);                           // nb_cwin.cu: compact-window path (after pair_setup)

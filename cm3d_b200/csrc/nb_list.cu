@@ -885,6 +885,23 @@ static void stencil(int nc, int *s, int *ns) {
 // fractional direction: plane spacing 1 / |row d of hmati|), their stencils,
 // the 27 cell-corner shifts and the FP32 prefilter radius; fills the cell
 // fields of c->h_sp and allocates the binning and list arrays.
+// the 27 neighbour-cell displacements of a system's grid (one cell step
+// along each box vector), as FP32 hi + lo parts
+void cell_shifts(SysP &P, const SysH &H) {
+  for (int a = -1; a <= 1; a++)
+    for (int b = -1; b <= 1; b++)
+      for (int d = -1; d <= 1; d++) {
+        double f0 = (double)a / P.nc[0], f1 = (double)b / P.nc[1], f2 = (double)d / P.nc[2];
+        const double *h = H.hmat;
+        const double v0 = h[0] * f0 + h[1] * f1 + h[2] * f2, v1 = h[3] * f0 + h[4] * f1 + h[5] * f2,
+                     v2 = h[6] * f0 + h[7] * f1 + h[8] * f2;
+        const int k = (a + 1) * 9 + (b + 1) * 3 + (d + 1);
+        P.shift[k] = make_float4((float)v0, (float)v1, (float)v2, 0.f);
+        P.shift_lo[k] = make_float4((float)(v0 - (double)(float)v0), (float)(v1 - (double)(float)v1),
+                                    (float)(v2 - (double)(float)v2), 0.f);
+      }
+}
+
 int list_setup(Ctx *c) {
   int c0 = 0;
   double est_max = 32.0;
@@ -913,18 +930,7 @@ int list_setup(Ctx *c) {
     const bool pre = P.nc[0] >= 3 && P.nc[1] >= 3 && P.nc[2] >= 3;
     const double rl = H.rlist + 1e-3;
     P.lim2 = pre ? (float)(rl * rl) : INFINITY;
-    for (int a = -1; a <= 1; a++)
-      for (int b = -1; b <= 1; b++)
-        for (int d = -1; d <= 1; d++) {
-          double f0 = (double)a / P.nc[0], f1 = (double)b / P.nc[1], f2 = (double)d / P.nc[2];
-          const double *h = H.hmat;
-          const double v0 = h[0] * f0 + h[1] * f1 + h[2] * f2, v1 = h[3] * f0 + h[4] * f1 + h[5] * f2,
-                       v2 = h[6] * f0 + h[7] * f1 + h[8] * f2;
-          const int k = (a + 1) * 9 + (b + 1) * 3 + (d + 1);
-          P.shift[k] = make_float4((float)v0, (float)v1, (float)v2, 0.f);
-          P.shift_lo[k] = make_float4((float)(v0 - (double)(float)v0), (float)(v1 - (double)(float)v1),
-                                      (float)(v2 - (double)(float)v2), 0.f);
-        }
+    cell_shifts(P, H);
     // first guess of the full-list slot: 1.3 x the mean number of atoms in
     // a list sphere, plus 64
     double vol = fabs(H.hmat[0] * (H.hmat[4] * H.hmat[8] - H.hmat[5] * H.hmat[7]) +

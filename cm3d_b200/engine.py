@@ -67,6 +67,7 @@ def load_library() -> C.CDLL:
         "cm3d_nb_system_counts": (C.c_int, [vp, C.POINTER(ll), C.POINTER(ll)]),
         "cm3d_nb_get_nhc": (C.c_int, [vp, C.c_int, dp, dp, ip, ip]),
         "cm3d_nb_set_positions": (C.c_int, [vp, dp, dp, dp]),
+        "cm3d_nb_set_box": (C.c_int, [vp, dp]),
         "cm3d_nb_get_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_velocities": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_get_velocities": (C.c_int, [vp, dp, dp, dp]),
@@ -205,6 +206,11 @@ class Engine:
 
     def set_positions(self, p) -> None:
         self._set3(load_library().cm3d_nb_set_positions, p)
+
+    def set_box(self, hmat) -> None:
+        """a new box matrix (row-major 3x3) for a one-system context"""
+        h = np.ascontiguousarray(np.asarray(hmat, dtype=np.float64).reshape(9))
+        check(load_library().cm3d_nb_set_box(self._h, h.ctypes.data_as(C.POINTER(C.c_double))), "set_box")
 
     def velocities(self, out=None) -> np.ndarray:
         return self._get3(load_library().cm3d_nb_get_velocities, out=out)

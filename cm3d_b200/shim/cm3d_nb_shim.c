@@ -48,6 +48,9 @@
  *   getvireal  (energy/control/md_fcntr.c:136) ENERGIES from the engine's
  *              accumulators, as for route A.
  *
+ * With a barostat (npt_i, npt_f: intbar in md_step.c moves COORDS.hmat) each
+ * call hands the engine the current box first (cm3d_nb_set_box).
+ *
  * CM3D's objects that define these four (md_fcntr.o, md_finter.o,
  * ngbr_list.o) are linked as copies in which the four symbols are weak, so
  * that the definitions here take their place (cm3d_b200/shim/Makefile).
@@ -85,11 +88,12 @@ static void check_supported(SIMPARMS *simparms, COORDS *coords)
 {
   if (simparms->iperd != 3) unsupported("a non-periodic or partially periodic box (iperd != 3)");
 #ifndef CM3D_NB_ROUTE_B
-  /* route B: CM3D's own step integrates the chains on the host */
+  /* route B: CM3D's own step integrates the chains and the barostat on the
+     host, and the engine follows the box (cm3d_nb_set_box) */
   if (simparms->iensemble != 0 && simparms->iensemble != 1)
     unsupported("a barostat (an ensemble other than nve or nvt)");
-#endif
   if (simparms->ivol) unsupported("a variable cell (ivol)");
+#endif
   if (simparms->iextern) unsupported("an external field");
   if (simparms->ipolar) unsupported("polarizable dipoles");
   (void)coords;
@@ -387,8 +391,15 @@ void step(SIMPARMS *simparms, COORDS *coords, ENERGIES *energies, INTER *inter, 
 }
 #else /* CM3D_NB_ROUTE_B */
 
+static double g_box[9];
+
+/* the current box (when a barostat moved it) and positions to the engine */
 static void push_positions(COORDS *coords)
 {
+  if (memcmp(g_box, coords->hmat, sizeof g_box) != 0) {
+    nb_check(cm3d_nb_set_box(g_ctx, coords->hmat), "set_box");
+    memcpy(g_box, coords->hmat, sizeof g_box);
+  }
   nb_check(cm3d_nb_set_positions(g_ctx, coords->px, coords->py, coords->pz), "set_positions");
 }
 
@@ -401,6 +412,7 @@ void get_ngbr(SIMPARMS *simparms, COORDS *coords, INTER *inter, NGBR *ngbr)
   if (!g_ctx) {
     check_supported(simparms, coords);
     create_engine(simparms, coords, inter);
+    memcpy(g_box, coords->hmat, sizeof g_box);
   } else {
     push_positions(coords);
   }

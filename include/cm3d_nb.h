@@ -242,6 +242,12 @@ int cm3d_nb_get_nhc(cm3d_nb_ctx *ctx, int sys, double *eta, double *veta, int *n
 int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py,
                           const double *pz);
 int cm3d_nb_get_positions(cm3d_nb_ctx *ctx, double *px, double *py, double *pz);
+/* a new box matrix (COORDS.hmat, row-major) for a one-system context, as
+   CM3D's barostats (intbar, integrate/md_baro.c:72) change it between force
+   calls: H^-1, the volume and every box-derived parameter follow.  The cell
+   grid keeps its counts: a box that shrinks below it (a cell narrower than
+   the list radius) returns CM3D_NB_ERR_STATE, and a new context is needed. */
+int cm3d_nb_set_box(cm3d_nb_ctx *ctx, const double hmat[9]);
 int cm3d_nb_set_velocities(cm3d_nb_ctx *ctx, const double *vx, const double *vy,
                            const double *vz);
 int cm3d_nb_get_velocities(cm3d_nb_ctx *ctx, double *vx, double *vy, double *vz);
