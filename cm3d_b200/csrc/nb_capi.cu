@@ -105,6 +105,9 @@ static void destroy(Ctx *c) {
   }
   if (c->step_ev) cudaEventDestroy(c->step_ev);
   if (c->st) cudaStreamDestroy(c->st);
+  if (c->st2) cudaStreamDestroy(c->st2);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   delete c;
 }
 
@@ -232,6 +235,9 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
     if (pk && strcmp(pk, "list") == 0) c->win_ok = 0, c->win_env_off = 1;
   }
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
   c->mode = o.mode;
   c->need_short = o.need_short;
   c->tpa = o.tpa;

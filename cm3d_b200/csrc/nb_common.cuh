@@ -255,6 +255,8 @@ struct Ctx {
   double *cw_part = nullptr;           // per-item FP64 energy/virial sums
   int stage_ntypes = 0, stage_ninter = 0;   // largest per-system type count / interaction count
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;                // side stream: force(1)'s k-space beside the list build
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int mode = CM3D_NB_MIXED;
   int need_short = 0;
   int tpa = 0;
@@ -480,6 +482,9 @@ bool cw_applies(Ctx *c, int iflg, bool ns);     // nb_cwin.cu
 int cw_pairs(Ctx *c, int mask, double *fout);   // nb_cwin.cu: pair kernel launch
 int cw_ereduce(Ctx *c, int mask);               // nb_cwin.cu: its energy/virial sums
 int kspace_forces(Ctx *c);                      // nb_kspace.cu
+bool kspace_async_ok(const Ctx *c);             // nb_kspace.cu: force(1)'s k-space beside the lists/pairs
+int kspace_fork(Ctx *c);                        // nb_kspace.cu
+int kspace_join(Ctx *c);                        // nb_kspace.cu
 int kspace_setup(Ctx *c);                       // nb_kspace.cu
 int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys);   // nb_step.cu
 int run_step(Ctx *c, int istep0, int nsteps);   // nb_step.cu

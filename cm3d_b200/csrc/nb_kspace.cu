@@ -576,7 +576,8 @@ int kspace_setup(Ctx *c) {
   }
   if (split > nrows_max) split = nrows_max;
   c->kf_split = split;
-  if (mixed && split > 1) {
+  if (mixed) {
+    // (also with one split: the forked k-space of a step writes partials)
     // zeroed once: the charged atoms of systems without k-vectors keep zero partials
     CK(cudaMalloc(&c->kf_part, sizeof(double) * 3 * (size_t)split * c->ncharge));
     CK(cudaMemset(c->kf_part, 0, sizeof(double) * 3 * (size_t)split * c->ncharge));
@@ -596,10 +597,10 @@ static void kforce_attr(int dev) {
 
 // several systems (mixed mode): every system's structure factors, totals
 // and forces in one launch per stage
-static int kspace_forces_batch(Ctx *c) {
+static int kspace_forces_batch(Ctx *c, cudaStream_t st, bool defer) {
   cudaEvent_t e0;
   tbegin(c, 1, &e0);
-  k_kprep<true><<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, nullptr,
+  k_kprep<true><<<grid_for(c->ncharge, 256), 256, 0, st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, nullptr,
                                                                c->sp, c->sys_of, c->kfrac, nullptr, c->gate);
   // enough row chunks per tile to fill the machine (one-warp blocks: 32
   // blocks per SM)
@@ -609,28 +610,28 @@ static int kspace_forces_batch(Ctx *c) {
   const int rpb = (c->nrows_max + ych - 1) / ych;
   dim3 gsf(c->ktiles_tot, (c->nrows_max + rpb - 1) / rpb);
   if (c->ks_small)
-    k_sfac_mixed<true, 1><<<gsf, KS_SMALL, 0, c->st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0,
+    k_sfac_mixed<true, 1><<<gsf, KS_SMALL, 0, st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0,
                                                        c->spart, c->sp, c->ktile_sys, c->gate);
   else
-    k_sfac_mixed<true><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0,
+    k_sfac_mixed<true><<<gsf, KS_THREADS, 0, st>>>(c->ncharge, c->kfrac, 0, c->rows, c->row_k0, rpb, 0,
                                                       c->spart, c->sp, c->ktile_sys, c->gate);
-  k_sred<true><<<grid_for(c->ktot, 256), 256, 0, c->st>>>(c->ktot, 0, c->spart, c->ka_d, c->kb_d, c->kc_d, nullptr,
+  k_sred<true><<<grid_for(c->ktot, 256), 256, 0, st>>>(c->ktot, 0, c->spart, c->ka_d, c->kb_d, c->kc_d, nullptr,
                                                            0.0, 0.0, c->sk, c->akf, nullptr, c->acc, c->sp,
                                                            c->k_sys, c->gate);
   kforce_attr(c->dev);
   dim3 gf(c->ftiles_tot, c->kf_split);
-  double *part = c->kf_split > 1 ? c->kf_part : nullptr;
+  double *part = c->kf_split > 1 || defer ? c->kf_part : nullptr;
   if (c->ks_small)
-    k_kforce_mixed<true, 1><<<gf, KS_SMALL, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0,
+    k_kforce_mixed<true, 1><<<gf, KS_SMALL, c->kf_smem, st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0,
                                                                  c->rows, c->row_k0, 0, c->akf, 0, nullptr, 0,
                                                                  c->fxl, part, c->sp, c->ftile_sys, c->gate);
   else
-    k_kforce_mixed<true><<<gf, KS_THREADS, c->kf_smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0,
+    k_kforce_mixed<true><<<gf, KS_THREADS, c->kf_smem, st>>>(c->ncharge, c->kfrac, c->icharge, c->n, 0,
                                                                  c->rows, c->row_k0, 0, c->akf, 0, nullptr, 0,
                                                                  c->fxl, part, c->sp, c->ftile_sys, c->gate);
   c->launches += 4;
-  if (part) {
-    k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->kf_split, part, c->icharge, c->n,
+  if (part && !defer) {
+    k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, st>>>(c->ncharge, c->kf_split, part, c->icharge, c->n,
                                                                 c->fxl, c->gate);
     c->launches++;
   }
@@ -639,9 +640,11 @@ static int kspace_forces_batch(Ctx *c) {
   return CM3D_NB_OK;
 }
 
-int kspace_forces(Ctx *c) {
+// k-space of force(1) on stream `st`; with `defer` (mixed mode) the forces
+// stay in the per-split partials and kspace_sum adds them to fxl later
+static int kspace_run(Ctx *c, cudaStream_t st, bool defer) {
   if (c->ncharge == 0 || c->ktot == 0) return CM3D_NB_OK;
-  if (c->nsys > 1) return kspace_forces_batch(c);
+  if (c->nsys > 1) return kspace_forces_batch(c, st, defer);
   const double *dhmati = c->acc + ACC_COUNT;
   double vol = c->hmat[0] * (c->hmat[4] * c->hmat[8] - c->hmat[5] * c->hmat[7]) +
                c->hmat[1] * (c->hmat[5] * c->hmat[6] - c->hmat[3] * c->hmat[8]) +
@@ -649,7 +652,7 @@ int kspace_forces(Ctx *c) {
   cudaEvent_t e0;
   tbegin(c, 1, &e0);
   const bool mixed = c->mode == CM3D_NB_MIXED;
-  k_kprep<false><<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, dhmati,
+  k_kprep<false><<<grid_for(c->ncharge, 256), 256, 0, st>>>(c->ncharge, c->icharge, c->n, c->pos, c->q, dhmati,
                                                                 nullptr, nullptr, mixed ? c->kfrac : nullptr,
                                                                 c->kposd, c->gate);
   // structure factors: enough row chunks per tile to fill the machine
@@ -658,14 +661,14 @@ int kspace_forces(Ctx *c) {
     rpb = (rpb + 1) / 2;
   dim3 gsf(c->ks_tiles, (c->nrows + rpb - 1) / rpb);
   if (mixed)
-    k_sfac_mixed<false><<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb,
+    k_sfac_mixed<false><<<gsf, KS_THREADS, 0, st>>>(c->ncharge, c->kfrac, c->nrows, c->rows, c->row_k0, rpb,
                                                        c->ktot, c->spart, nullptr, nullptr, c->gate);
   else
-    k_sfac_plain<<<gsf, KS_THREADS, 0, c->st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
+    k_sfac_plain<<<gsf, KS_THREADS, 0, st>>>(c->ncharge, c->kposd, c->nrows, c->rows, c->row_k0, rpb, c->ktot,
                                                 dhmati, c->spart, c->gate);
   int ib = 256, gb = grid_for(c->ktot, ib);
   if (gb > c->num_sms * 4) gb = c->num_sms * 4;
-  k_sred<false><<<gb, ib, 0, c->st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
+  k_sred<false><<<gb, ib, 0, st>>>(c->ktot, c->ks_tiles, c->spart, c->ka_d, c->kb_d, c->kc_d, dhmati, 1.0 / vol,
                                       c->falp2, c->sk, mixed ? c->akf : nullptr, mixed ? nullptr : c->akd, c->acc,
                                       nullptr, nullptr, c->gate);
   int split = c->kf_split;
@@ -676,22 +679,57 @@ int kspace_forces(Ctx *c) {
     // shared memory: the A(k) of one split's rows
     size_t smem = c->kf_smem;
     kforce_attr(c->dev);
-    k_kforce_mixed<false><<<gf, KS_THREADS, smem, c->st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows,
+    k_kforce_mixed<false><<<gf, KS_THREADS, smem, st>>>(c->ncharge, c->kfrac, c->icharge, c->n, c->nrows,
                                                             c->rows, c->row_k0, rps, c->akf, c->ktot, dhmati,
-                                                            0, c->fxl, split > 1 ? c->kf_part : nullptr, nullptr,
-                                                            nullptr, c->gate);
-    if (split > 1) {
-      k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, split, c->kf_part, c->icharge,
+                                                            0, c->fxl, split > 1 || defer ? c->kf_part : nullptr,
+                                                            nullptr, nullptr, c->gate);
+    if (split > 1 && !defer) {
+      k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, st>>>(c->ncharge, split, c->kf_part, c->icharge,
                                                                   c->n, c->fxl, c->gate);
       c->launches++;
     }
   } else {
     dim3 gf((c->ncharge + 255) / 256, split);
-    k_kforce_plain<<<gf, 256, 0, c->st>>>(c->ncharge, c->kposd, c->icharge, c->n, c->nrows, c->rows, c->row_k0,
+    k_kforce_plain<<<gf, 256, 0, st>>>(c->ncharge, c->kposd, c->icharge, c->n, c->nrows, c->rows, c->row_k0,
                                           rps, c->akd, c->ktot, dhmati, split > 1, c->fxl, c->gate);
   }
   c->launches += 4;
   tend(c, 1, e0);
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
+int kspace_forces(Ctx *c) { return kspace_run(c, c->st, false); }
+
+// Whether force(1)'s k-space can run beside the list build and the pair
+// kernels: mixed mode (its forces go through the per-split partials, which
+// nothing else writes), charges with k-vectors, no per-class kernel timing
+// (whose events live on the main stream).
+bool kspace_async_ok(const Ctx *c) {
+  return c->mode == CM3D_NB_MIXED && c->ncharge > 0 && c->ktot > 0 && c->kf_part && c->st2 && !c->timing.on;
+}
+
+// Fork: the k-space kernels of force(1) on the side stream, after what the
+// main stream has enqueued so far (positions final, accumulators zeroed).
+// They read positions and charges and write the k-space accumulators and
+// the partial forces only -- none of which the list build, group_init or
+// the pair kernels touch.
+int kspace_fork(Ctx *c) {
+  CK(cudaEventRecord(c->ev_fork, c->st));
+  CK(cudaStreamWaitEvent(c->st2, c->ev_fork, 0));
+  int rc = kspace_run(c, c->st2, true);
+  if (rc) return rc;
+  CK(cudaEventRecord(c->ev_join, c->st2));
+  return CM3D_NB_OK;
+}
+
+// Join: the main stream waits for the forked k-space and adds its partial
+// forces to fxl in split order (after the pair forces, as without the fork)
+int kspace_join(Ctx *c) {
+  CK(cudaStreamWaitEvent(c->st, c->ev_join, 0));
+  k_kforce_sum<<<grid_for(c->ncharge, 256), 256, 0, c->st>>>(c->ncharge, c->kf_split, c->kf_part, c->icharge, c->n,
+                                                              c->fxl, c->gate);
+  c->launches++;
   CKL(c);
   return CM3D_NB_OK;
 }

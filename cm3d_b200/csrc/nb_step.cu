@@ -1391,15 +1391,17 @@ int run_force(Ctx *c, int iflg) {
 }
 
 // the nonbonded level that closes RESPA level `intr` (md_step.c:138-146):
-// force(1) + kick on the last level, force(0) + kick otherwise
-static int close_level(Ctx *c, int intr) {
+// force(1) + kick on the last level, force(0) + kick otherwise.  ks_forked:
+// the accumulators were zeroed and the k-space runs on the side stream
+// already (kspace_fork), joined here after the pair forces.
+static int close_level(Ctx *c, int intr, bool ks_forked = false) {
   int rc;
   StepP P = step_params(c);
   if (intr == c->nres_lrf - 1) {
-    if ((rc = zero_acc(c))) return rc;
+    if (!ks_forked && (rc = zero_acc(c))) return rc;
     if ((rc = group_init(c, P.use_fxs))) return rc;
     if ((rc = pair_forces(c, 1, 3))) return rc;
-    if ((rc = kspace_forces(c))) return rc;
+    if ((rc = ks_forked ? kspace_join(c) : kspace_forces(c))) return rc;
     return finish_level1(c, P.dter, P.dter1, true);
   }
   CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
@@ -1451,6 +1453,13 @@ static int one_level(Ctx *c, int intr, bool gated) {
   tend(c, 3, e0);
   CKL(c);
   if ((rc = reset_positions(c))) return rc;
+  // the positions are final for this level: force(1)'s k-space can start on
+  // the side stream while the lists are rebuilt and the pair forces run
+  const bool fork = intr == c->nres_lrf - 1 && kspace_async_ok(c);
+  if (fork) {
+    if ((rc = zero_acc(c))) return rc;
+    if ((rc = kspace_fork(c))) return rc;
+  }
   if (gated) {
     if ((rc = build_lists(c, true, false))) return rc;
   } else {
@@ -1460,7 +1469,7 @@ static int one_level(Ctx *c, int intr, bool gated) {
       if ((rc = build_lists(c, false, false))) return rc;
     }
   }
-  return close_level(c, intr);
+  return close_level(c, intr, fork);
 }
 
 static int one_step(Ctx *c, bool gated) {
