@@ -518,7 +518,11 @@ def main() -> None:
                     help="N > 1: split one ensemble over the ranks (LPT on the cost model, strong scaling) "
                          "instead of one ensemble per rank (weak scaling)")
     ap.add_argument("--serving-sweep", action="store_true",
-                    help="serving at 0.5, 1, 2, 4, 8 jobs/s over 120 s windows (long)")
+                    help="serving at 0.5, 1, 2, 4, 8 jobs/s over --serving-window s windows (long)")
+    ap.add_argument("--serving-window", type=float, default=120.0,
+                    help="arrival window of each --serving-sweep rate, seconds")
+    ap.add_argument("--serving-only", action="store_true",
+                    help="with --serving-sweep: run the sweep alone and print its list (one GPU)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -547,6 +551,17 @@ def main() -> None:
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return
+
+    if args.serving_sweep and args.serving_only:
+        sweep = []
+        for r in (0.5, 1.0, 2.0, 4.0, 8.0):
+            t0 = time.perf_counter()
+            res = serving_arm(r, args.serving_window, local, not args.no_plain)
+            res["wall_total_s"] = time.perf_counter() - t0
+            print(json.dumps(res), flush=True)
+            sweep.append(res)
+        print(json.dumps({"serving_sweep": sweep}))
         return
 
     import torch
@@ -644,7 +659,7 @@ def main() -> None:
     serving = None
     if not args.no_extra and world == 1:
         if args.serving_sweep:
-            serving = [serving_arm(r, 120.0, local, not args.no_plain) for r in (0.5, 1.0, 2.0, 4.0, 8.0)]
+            serving = [serving_arm(r, args.serving_window, local, not args.no_plain) for r in (0.5, 1.0, 2.0, 4.0, 8.0)]
         else:
             serving = serving_arm(4.0, 5.0, local, not args.no_plain)
 

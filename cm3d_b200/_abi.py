@@ -67,7 +67,7 @@ class SystemDesc(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int), ("mode", C.c_int), ("need_short", C.c_int),
-                ("tpa", C.c_int), ("use_graph", C.c_int)]
+                ("tpa", C.c_int), ("use_graph", C.c_int), ("cell_scale", C.c_double)]
 
 
 class Energies(C.Structure):

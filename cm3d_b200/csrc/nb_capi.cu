@@ -242,6 +242,7 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
   c->need_short = o.need_short;
   c->tpa = o.tpa;
   c->use_graph = o.use_graph;
+  c->cell_scale = o.cell_scale >= 1.0 ? o.cell_scale : 1.0;
   c->nsys = nsys;
   c->h_sp.assign(nsys, SysP());
   c->hs.assign(nsys, SysH());
@@ -571,6 +572,7 @@ void cm3d_nb_default_options(cm3d_nb_options *opt) {
   opt->need_short = 0;
   opt->tpa = 0;
   opt->use_graph = 1;
+  opt->cell_scale = 1.0;
 }
 
 int cm3d_nb_create(const cm3d_nb_system *sys, const cm3d_nb_options *opt, cm3d_nb_ctx **out) {
@@ -1155,6 +1157,18 @@ int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa) {
   return CM3D_NB_OK;
 }
 
+int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit) {
+  CTX;
+  if (sys < 0 || sys >= c->nsys) {
+    set_error("grid: system %d of %d", sys, c->nsys);
+    return CM3D_NB_ERR_ARG;
+  }
+  if (nc)
+    for (int d = 0; d < 3; d++) nc[d] = c->h_sp[sys].nc[d];
+  if (nsplit) *nsplit = c->cw_ok ? c->cw_nsplit : 1;
+  return CM3D_NB_OK;
+}
+
 int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]) {
   CTX;
   int rc;
@@ -1169,7 +1183,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   if (reps < 1) reps = 5;
   const int cand[4] = {4, 8, 16, 32};
   double best = 1e300;
-  int best_tpa = c->tpa, best_win = 0, best_cw = 0;
+  int best_tpa = c->tpa, best_win = 0, best_cw = 0, best_split = c->cw_nsplit;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -1186,26 +1200,32 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
     if (kind == 2 && !c->cw_ok) continue;
     c->win_ok = kind == 1;
     c->cw_use = kind == 2;
-    for (int k = 0; k < 4; k++) {
-      if (kind == 2 && cand[k] != 32) continue;      // the compact kernel runs a warp per atom
-      c->tpa = cand[k];
-      if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
-      CK(cudaEventRecord(a, c->st));
-      for (int r = 0; r < reps; r++)
-        if ((rc = pair_forces(c, 1, 3))) return rc;
-      CK(cudaEventRecord(b, c->st));
-      CK(cudaEventSynchronize(b));
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, a, b));
-      const double per = ms / reps;
-      if (ms_per_launch && per < ms_per_launch[k]) ms_per_launch[k] = per;
-      if (per < best) {
-        best = per;
-        best_tpa = cand[k];
-        best_win = kind == 1;
-        best_cw = kind == 2;
+    // the compact kernel runs a warp per atom; its tile is the number of
+    // parts each cell's atoms are split into (work items per cell, each
+    // staging the cell's window): 1, 2, 4, 8
+    for (int k = 0; k < 4; k++)
+      for (int sp = 1; sp <= (kind == 2 ? CW_MAX_SPLIT : 1); sp *= 2) {
+        if (kind == 2 && cand[k] != 32) continue;
+        c->tpa = cand[k];
+        if (kind == 2) cw_set_split(c, sp);
+        if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
+        CK(cudaEventRecord(a, c->st));
+        for (int r = 0; r < reps; r++)
+          if ((rc = pair_forces(c, 1, 3))) return rc;
+        CK(cudaEventRecord(b, c->st));
+        CK(cudaEventSynchronize(b));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, a, b));
+        const double per = ms / reps;
+        if (ms_per_launch && per < ms_per_launch[k]) ms_per_launch[k] = per;
+        if (per < best) {
+          best = per;
+          best_tpa = cand[k];
+          best_win = kind == 1;
+          best_cw = kind == 2;
+          if (kind == 2) best_split = sp;
+        }
       }
-    }
   }
   c->timing.on = timing;
   cudaEventDestroy(a);
@@ -1213,6 +1233,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   c->tpa = best_tpa;
   c->win_ok = best_win;
   c->cw_use = best_cw;
+  if (c->cw_ok) cw_set_split(c, best_split);
   if (tpa_chosen) *tpa_chosen = best_tpa;
   // a captured step holds the old launch configuration; the timing launches
   // added to the force blocks and accumulators: recompute force(1)

@@ -260,6 +260,7 @@ struct Ctx {
   int mode = CM3D_NB_MIXED;
   int need_short = 0;
   int tpa = 0;
+  double cell_scale = 1.0;   // list cells at least this many list radii wide
   int use_graph = 1;
   // ---- sizes and scalars
   int n = 0, ntypes = 0, ninter = 0, ntable = 0, ncharge = 0, ktot = 0, necorr = 0;
@@ -477,6 +478,8 @@ void cell_shifts(SysP &P, const SysH &H);       // nb_list.cu
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused
 int pair_setup(Ctx *c);                         // nb_pair.cu
 int cw_setup(Ctx *c);                           // nb_cwin.cu: compact-window path (after pair_setup)
+constexpr int CW_MAX_SPLIT = 8;                 // most parts a cell's atoms are split into
+void cw_set_split(Ctx *c, int nsplit);          // nb_cwin.cu
 int cw_convert(Ctx *c, bool device_flag);       // nb_cwin.cu: master list -> compact list
 bool cw_applies(Ctx *c, int iflg, bool ns);     // nb_cwin.cu
 int cw_pairs(Ctx *c, int mask, double *fout);   // nb_cwin.cu: pair kernel launch

@@ -800,14 +800,20 @@ int cw_setup(Ctx *c) {
     }
   }
   // work items: cells, split into parts where the cells are fewer than four
-  // per SM (each part stages its cell's window again)
+  // per SM (each part stages its cell's window again); the autotuner may
+  // choose another split (room for the largest)
   const int want = (4 * c->num_sms + c->ncells - 1) / c->ncells;
-  c->cw_nsplit = std::max(1, std::min(want, 8));
-  c->cw_nitems = c->ncells * c->cw_nsplit;
-  CK(cudaMalloc(&c->cw_part, sizeof(double) * CQ_COUNT * (size_t)c->cw_nitems));
+  CK(cudaMalloc(&c->cw_part, sizeof(double) * CQ_COUNT * (size_t)c->ncells * CW_MAX_SPLIT));
+  cw_set_split(c, std::max(1, std::min(want, CW_MAX_SPLIT)));
   c->cw_ok = 1;
   c->cw_use = 1;
   return CM3D_NB_OK;
+}
+
+// work items of the compact kernel: each cell's atoms in `nsplit` parts
+void cw_set_split(Ctx *c, int nsplit) {
+  c->cw_nsplit = std::max(1, std::min(nsplit, CW_MAX_SPLIT));
+  c->cw_nitems = c->ncells * c->cw_nsplit;
 }
 
 // after a (gated) rebuild of the master list: the compact list

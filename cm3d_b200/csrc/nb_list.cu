@@ -912,7 +912,7 @@ int list_setup(Ctx *c) {
     for (int d = 0; d < 3; d++) {
       double w = 1.0 / sqrt(H.hmati[3 * d] * H.hmati[3 * d] + H.hmati[3 * d + 1] * H.hmati[3 * d + 1] +
                             H.hmati[3 * d + 2] * H.hmati[3 * d + 2]);
-      int m = H.rlist > 0 ? (int)floor(w / H.rlist) : 1;
+      int m = H.rlist > 0 ? (int)floor(w / (H.rlist * c->cell_scale)) : 1;
       m = m < 1 ? 1 : (m > 1000 ? 1000 : m);
       P.nc[d] = m;
       tot *= m;

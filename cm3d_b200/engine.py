@@ -68,6 +68,7 @@ def load_library() -> C.CDLL:
         "cm3d_nb_get_nhc": (C.c_int, [vp, C.c_int, dp, dp, ip, ip]),
         "cm3d_nb_set_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_box": (C.c_int, [vp, dp]),
+        "cm3d_nb_grid": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), ip]),
         "cm3d_nb_get_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_velocities": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_get_velocities": (C.c_int, [vp, dp, dp, dp]),
@@ -147,7 +148,7 @@ class Engine:
     atoms back to back; `ranges[s]` is system s's (first, natoms)."""
 
     def __init__(self, system, mode: int = _abi.MIXED, device: int = 0,
-                 need_short: bool = False, tpa: int = 0, use_graph: bool = True):
+                 need_short: bool = False, tpa: int = 0, use_graph: bool = True, cell_scale: float = 1.0):
         L = load_library()
         systems = list(system) if isinstance(system, (list, tuple)) else [system]
         self.systems = systems
@@ -156,7 +157,7 @@ class Engine:
         self.n = sum(s.natoms for s in systems)
         self.mode = mode
         opt = _abi.Options(device=device, mode=mode, need_short=int(need_short), tpa=tpa,
-                           use_graph=int(use_graph))
+                           use_graph=int(use_graph), cell_scale=float(cell_scale))
         h = C.c_void_p()
         descs = (_abi.SystemDesc * self.nsys)(*[s.desc() for s in systems])
         check(L.cm3d_nb_create_batch(descs, self.nsys, C.byref(opt), C.byref(h)), "cm3d_nb_create_batch")
@@ -279,8 +280,16 @@ class Engine:
         t = C.c_int(0)
         ms = np.zeros(4)
         check(load_library().cm3d_nb_autotune(self._h, reps, C.byref(t), _p(ms)), "autotune")
-        return {"tpa": int(t.value), "kernel": self.pair_kernel()[0],
+        nc, split = self.grid(0)
+        return {"tpa": int(t.value), "kernel": self.pair_kernel()[0], "cells": nc, "compact_split": split,
                 "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
+
+    def grid(self, sys: int = 0) -> tuple[list, int]:
+        """(cells per box direction of system `sys`, parts per cell of the compact kernel's work items)"""
+        nc = (C.c_int * 3)()
+        sp = C.c_int(0)
+        check(load_library().cm3d_nb_grid(self._h, sys, nc, C.byref(sp)), "grid")
+        return [int(x) for x in nc], int(sp.value)
 
     def pair_kernel(self) -> tuple[str, int]:
         """(kernel of the last pair launch: "gather", "window", "system" or "compact", lanes per atom)"""
@@ -398,6 +407,36 @@ class Engine:
 
 
 # ----------------------------------------------------- host set-up helpers
+def tune_cell_scale(systems, device: int = 0, scales=(1.0, 1.25), steps: int = 20, warmup: int = 5,
+                    reps: int = 5) -> dict:
+    """Cell size by measurement: for each candidate cell width (in list
+    radii; cm3d_nb_options.cell_scale) a fresh mixed context of the same
+    systems runs step_init, the kernel autotuner (pair kernel, lanes per
+    atom, compact tile) and `warmup` + `steps` graph steps; the step time is
+    measured with CUDA events around the timed steps.  Returns the fastest
+    scale with every candidate's step time and kernel choice; the systems
+    themselves are not changed."""
+    import torch
+    out = {}
+    for s in scales:
+        with Engine(systems, mode=_abi.MIXED, device=device, cell_scale=s) as e:
+            e.step_init()
+            tune = e.autotune(reps)
+            e.step(1, warmup)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st = torch.cuda.ExternalStream(e.stream(), device=device)
+            e.synchronize()
+            a.record(st)
+            e.step_async(1 + warmup, steps)
+            b.record(st)
+            e.step_wait()
+            b.synchronize()
+            out[s] = {"ms_per_step": a.elapsed_time(b) / steps, "kernel": tune["kernel"], "tpa": tune["tpa"],
+                      "cells": tune["cells"], "compact_split": tune["compact_split"]}
+    best = min(out, key=lambda k: out[k]["ms_per_step"])
+    return {"cell_scale": best, "candidates": out}
+
+
 def lj_table(eps, sig, rmin, rmax, rres, rheal, skin, ntable, shift):
     """get_ter_parm's LJ table (input/md_getparm.c:236-366) via the C ABI."""
     L = load_library()

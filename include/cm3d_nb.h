@@ -164,6 +164,10 @@ typedef struct cm3d_nb_options {
                                 dter1 = 0 otherwise, md_step.c:78,99) */
   int tpa;                   /* mixed pair kernel: lanes per atom (0 = auto) */
   int use_graph;             /* capture cm3d_nb_step() in a CUDA graph */
+  double cell_scale;         /* list-build cells at least cell_scale list radii
+                                wide (>= 1; 0 or below 1 means 1): fewer, larger
+                                cells -- larger windows per pair-kernel block,
+                                more candidates per atom in the list build */
 } cm3d_nb_options;
 
 /* energies/virials collected as getvireal()+geteng() do (md_fcntr.c:136-308) */
@@ -367,6 +371,10 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
 #define CM3D_NB_PAIR_SYSTEM 2
 #define CM3D_NB_PAIR_COMPACT 3
 int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
+/* the cell grid of system `sys` (cells per box direction) and, for the
+   compact path, the parts each cell's atoms are split into (work items per
+   cell; 1 elsewhere) */
+int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit);
 
 /* ------------------------------------------- no-allocation variant */
 #define CM3D_NB_NOALLOC_MAX_CHARGES 32768   /* charged atoms per call */
