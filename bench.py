@@ -373,15 +373,22 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
     without the profiler, whose serialised timings would mislead it)."""
     import torch
     from cm3d_b200 import _abi
-    from cm3d_b200.engine import Engine
+    from cm3d_b200.engine import Engine, tune_cell_scale
     if pin and pin[1] in ("gather", "staged"):
         os.environ["CM3D_NB_PAIR_KERNEL"] = "list" if pin[1] == "gather" else "window"
-    eng = Engine(systems, mode=_abi.MIXED, device=device, tpa=pin[0] if pin else 0)
+    # the cell size by measurement (fresh contexts per candidate, before the
+    # measured one; every rank the same way)
+    cells = None if pin else tune_cell_scale(systems, device=device)
+    eng = Engine(systems, mode=_abi.MIXED, device=device, tpa=pin[0] if pin else 0,
+                 cell_scale=cells["cell_scale"] if cells else 1.0)
     if pin:
         os.environ.pop("CM3D_NB_PAIR_KERNEL", None)
     eng.workload_name = name
     eng.step_init()
     tune = {"tpa": pin[0], "kernel": pin[1], "pinned": True} if pin else eng.autotune()
+    if cells:
+        tune["cell_scale"] = cells["cell_scale"]
+        tune["cell_scale_candidates"] = {str(k): v for k, v in cells["candidates"].items()}
     n = eng.n
     if dist:
         dist.barrier()
