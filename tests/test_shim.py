@@ -180,7 +180,12 @@ def test_route_b_binding_matches_cm3d(tmp_path, kind, mode):
         compare(cpu_out, gpu_out, rtol=1e-7, atol=3e-6, exact_counts=True)
         pos_tol = 3e-4
     else:
-        compare(cpu_out, gpu_out, rtol=2e-4, atol=3e-6, exact_counts=False)
+        # under a barostat the chain and volume variables integrate the
+        # pressure, whose mixed-engine error (a small difference of large
+        # virials) is the largest of any printed quantity: the thermostat
+        # energy per chain (about 0.1 K against atom energies of hundreds of
+        # K) then differs by a few 1e-4 K after 20 steps
+        compare(cpu_out, gpu_out, rtol=2e-4, atol=1e-3 if "npt" in kind else 3e-6, exact_counts=False)
         pos_tol = 2e-3
     pc, hc = read_restart(str(tmp_path / "cpu" / f"{wl.name}.rest_N"))
     pg, hg = read_restart(str(tmp_path / "gpu" / f"{wl.name}.rest_N"))
