@@ -88,7 +88,9 @@ static void destroy(Ctx *c) {
                   c->stat, c->istate, c->sp, c->sys_of, c->cell_sys, c->sreb, c->slast, c->sstat,
                   c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan,
                   c->fxr, c->intra_buf, c->ithm, c->nhc, c->cwl, c->cwn, c->cw_tf, c->cw_tg, c->cw_tl,
-                  c->cw_part, c->nvt_kin, c->nvt_chsum, c->th_atoms, c->th_choff, c->th_chunk};
+                  c->cw_part, c->nvt_kin, c->nvt_chsum, c->th_atoms, c->th_choff, c->th_chunk,
+                  c->cw_sys, c->cw_sitems, c->cw_items, c->cw_gidx};
+  cw_destroy(c);
   for (void *p : ptrs)
     if (p) cudaFree(p);
   void *hp[] = {c->h_acc, c->h_stat, c->h_istate, c->h_ltot, c->h_sstat};
@@ -352,6 +354,9 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
       }
       P.rmaxl_skin2_e = s->rmaxl_skin2_e;
       P.rmaxs_skin2_e = s->rmaxs_skin2_e;
+      H.rmaxl_coul2 = s->rmaxl_coul2;
+      H.dx2coul = s->dx2coul;
+      H.rmins_coul2 = s->rmins_coul2;
       P.rc2_el = (float)s->rmaxl_coul2;
       P.dx2c = (float)s->dx2coul;
       P.offc = (float)(s->rmins_coul2 * s->dx2coul);
@@ -1202,10 +1207,12 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
     c->cw_use = kind == 2;
     // the compact kernel runs a warp per atom; its tile is the number of
     // parts each cell's atoms are split into (work items per cell, each
-    // staging the cell's window): 1, 2, 4, 8
+    // staging the cell's window): 1, 2, 4, 8.  In a batch the lanes per
+    // atom are those of the gather kernel that runs the other systems, and
+    // the items are whole cells.
     for (int k = 0; k < 4; k++)
-      for (int sp = 1; sp <= (kind == 2 ? CW_MAX_SPLIT : 1); sp *= 2) {
-        if (kind == 2 && cand[k] != 32) continue;
+      for (int sp = 1; sp <= (kind == 2 && !c->cw_batch ? CW_MAX_SPLIT : 1); sp *= 2) {
+        if (kind == 2 && cand[k] != 32 && !c->cw_batch) continue;
         c->tpa = cand[k];
         if (kind == 2) cw_set_split(c, sp);
         if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)

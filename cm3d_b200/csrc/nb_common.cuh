@@ -180,6 +180,7 @@ struct SysH {
   double scale14 = 1, scale14e = 1;   // ONFO.scale_onefour / scale_onefour_e
   double rlist = 0;          // largest list radius (LJ or charges, with skin)
   double skin = 0;           // INTER.skin_ter
+  double rmaxl_coul2 = 0, dx2coul = 0, rmins_coul2 = 0;   // charges: cut-off^2, table spacing, table start^2
   std::vector<int4> krows;   // k rows {ka, kb, kc0, len} of the system's k set
   std::vector<int> krow_k0;  // first k of each row (system-local)
   std::vector<int> ka, kb, kc;
@@ -253,6 +254,17 @@ struct Ctx {
   float cw_lj1[4] = {0, 0, 0, 0};      // the one LJ interaction: rc^2, dx2tab, offset, vt
   int cw_nsplit = 1, cw_nitems = 0;    // work items: cells x parts
   double *cw_part = nullptr;           // per-item FP64 energy/virial sums
+  // a batch: the systems with >= 3 cells per axis in the compact kernel (in
+  // groups of systems with the same tables), the others in the gather kernel
+  int cw_batch = 0;
+  int *cw_sys = nullptr;               // per system: 1 = compact (device)
+  int2 *cw_sitems = nullptr;           // per system: its items {first, count} (device)
+  int4 *cw_items = nullptr;            // {system, cell of the system, part, parts}, by group (device)
+  int *cw_gidx = nullptr;              // sorted atoms of the gather-kernel systems (device)
+  int cw_ng = 0;
+  void *cw_grp = nullptr;              // the groups (host, nb_cwin.cu)
+  const int *pair_gidx = nullptr;      // a gather launch over these sorted atoms only
+  int pair_ng = 0;
   int stage_ntypes = 0, stage_ninter = 0;   // largest per-system type count / interaction count
   cudaStream_t st = nullptr;
   cudaStream_t st2 = nullptr;                // side stream: force(1)'s k-space beside the list build
@@ -480,7 +492,8 @@ int pair_setup(Ctx *c);                         // nb_pair.cu
 int cw_setup(Ctx *c);                           // nb_cwin.cu: compact-window path (after pair_setup)
 constexpr int CW_MAX_SPLIT = 8;                 // most parts a cell's atoms are split into
 void cw_set_split(Ctx *c, int nsplit);          // nb_cwin.cu
-int cw_convert(Ctx *c, bool device_flag);       // nb_cwin.cu: master list -> compact list
+int cw_convert(Ctx *c, bool device_flag, bool all);   // nb_cwin.cu: master list -> compact list
+void cw_destroy(Ctx *c);                        // nb_cwin.cu: host-side group data
 bool cw_applies(Ctx *c, int iflg, bool ns);     // nb_cwin.cu
 int cw_pairs(Ctx *c, int mask, double *fout);   // nb_cwin.cu: pair kernel launch
 int cw_ereduce(Ctx *c, int mask);               // nb_cwin.cu: its energy/virial sums

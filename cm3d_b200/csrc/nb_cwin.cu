@@ -41,6 +41,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <string>
+#include <type_traits>
 #include <vector>
 
 #include "nb_common.cuh"
@@ -71,6 +73,7 @@ struct CwP {
   float r2under;             // r^2 below which the erfc table underflows (p < 1)
   // one LJ interaction (LJM 1): cut-off^2, dx2tab, rmins_cut2 * dx2tab, vtab[ntable-4]
   float rc2_l, dx2l, offl, vtl;
+  int map0, inter0;          // a batch group: the type map and cut-offs of its first system
 };
 
 // ------------------------------------------------------------------
@@ -88,13 +91,29 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
                                                     const int *__restrict__ nlen, int stride,
                                                     const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
                                                     int2 *__restrict__ cwn, long long *__restrict__ stat,
-                                                    int *__restrict__ halt, const int *__restrict__ gs) {
+                                                    int *__restrict__ halt, const int *__restrict__ gs,
+                                                    const SysP *__restrict__ sp = nullptr,
+                                                    const int *__restrict__ sys_of = nullptr,
+                                                    const int *__restrict__ cwsys = nullptr,
+                                                    const int *__restrict__ sreb = nullptr, int all = 1) {
   if (gated_off(gs, 1)) return;
   const int lane = threadIdx.x & 31;
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (t >= n) return;                                  // whole warps
+  // a batch (cwsys set): only the atoms of compact systems that were just
+  // rebuilt, each on its own system's grid (a system's sorted indices span
+  // its own atom range, so sys_of[t] is t's system)
+  int c0 = 0;
+  if (cwsys) {
+    const int s = sys_of[t];
+    if (!cwsys[s] || (!all && sreb[s] == 0)) return;
+    ncx = sp[s].nc[0];
+    ncy = sp[s].nc[1];
+    ncz = sp[s].nc[2];
+    c0 = sp[s].c0;
+  }
   const uint32_t dummy = (uint32_t)cap;
-  const int c = cell_of[sorig[t]];
+  const int c = cell_of[sorig[t]] - c0;
   int delta = 0, tot = 0;
   {
     const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
@@ -104,7 +123,7 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
       jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
       jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
       jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
-      const int jc = (jx * ncy + jy) * ncz + jz;
+      const int jc = c0 + (jx * ncy + jy) * ncz + jz;
       cs = cell_start[jc];
       cnt = cell_start[jc + 1] - cs;
     }
@@ -118,7 +137,7 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
     tot = __shfl_sync(0xffffffffu, incl, 26);
   }
   const bool fits = tot <= cap;
-  if (!fits && lane == 0 && t == cell_start[c]) {
+  if (!fits && lane == 0 && t == cell_start[c0 + c]) {
     atomicAdd((unsigned long long *)(stat + ST_CWIN), 1ull);
     if (halt) *halt = 1;
   }
@@ -355,14 +374,20 @@ __device__ __forceinline__ void cw_lj(const CwP &P, float dx, float dy, float dz
   A.vl[5] = fmaf(uz, dz, A.vl[5]);
 }
 
-template <bool HAS_EL, int LJM>
+// BATCH: the work items of one group of a batch's systems -- systems whose
+// tables and pair parameters are the same, so that P and the staged tables
+// serve them all -- given as {system, cell of the system, part, parts};
+// each item's cell grid and shifts come from its system's SysP, and its
+// partial sums go to item0 + item.
+template <bool HAS_EL, int LJM, bool BATCH = false>
 __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     CwP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ cell_start, const int2 *__restrict__ cwn, const uint2 *__restrict__ cwl,
     const float4 *__restrict__ gshift, const int *__restrict__ gmap, const float *__restrict__ gfcut,
     const float4 *__restrict__ gtf, const float2 *__restrict__ gtg, const float4 *__restrict__ gtl,
     double *__restrict__ fout, double *__restrict__ ipart, long long *__restrict__ stat,
-    const int *__restrict__ gs) {
+    const int *__restrict__ gs, const int4 *__restrict__ items = nullptr, const SysP *__restrict__ sp = nullptr,
+    int item0 = 0) {
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
   // tables first (16-byte aligned), then the window
@@ -380,16 +405,24 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   __shared__ __align__(8) unsigned long long s_mbar;
   static_assert(CQ_COUNT == 16, "the transposing reduction gives lane pair q quantity q of 16");
 
-  for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = gshift[k];
+  if (!BATCH)
+    for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = gshift[k];
   if (HAS_EL) {
     for (int k = threadIdx.x; k < P.ntable * CW_RF; k += blockDim.x) tf[k] = gtf[k / CW_RF];
     for (int k = threadIdx.x; k < P.ntable * CW_RG; k += blockDim.x) tg[k] = gtg[k / CW_RG];
   }
   for (int k = threadIdx.x; k < nl; k += blockDim.x) tl[k] = gtl[k];
   if (LJM == 2) {
-    for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) s_map[k] = gmap[k];
-    for (int k = threadIdx.x; k < P.ninter; k += blockDim.x)
-      s_cut[k] = make_float4(gfcut[8 * k], gfcut[8 * k + 2], gfcut[8 * k + 1], gfcut[8 * k + 3]);
+    // the type map as local interaction indices (a batch's global map holds
+    // inter0 + local); the cut-offs of those interactions
+    for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) {
+      const int in = gmap[P.map0 + k];
+      s_map[k] = in >= 0 ? in - P.inter0 : -1;
+    }
+    for (int k = threadIdx.x; k < P.ninter; k += blockDim.x) {
+      const float *f = gfcut + 8 * (P.inter0 + k);
+      s_cut[k] = make_float4(f[0], f[2], f[1], f[3]);
+    }
   }
   const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_mbar);
   unsigned phase = 0;
@@ -409,17 +442,34 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   unsigned long long under = 0;
 
   for (int item = blockIdx.x; item < P.nitems; item += gridDim.x) {
-    const int c = item / P.nsplit, part = item - c * P.nsplit;
-    const int cz = c % P.ncz, cy = (c / P.ncz) % P.ncy, cx = c / (P.ncz * P.ncy);
+    int c, part, nsplit, ncx = P.ncx, ncy = P.ncy, ncz = P.ncz, c0 = 0, sys = 0;
+    if (BATCH) {
+      const int4 it = items[item];
+      sys = it.x;
+      c = it.y;
+      part = it.z;
+      nsplit = it.w;
+      ncx = sp[sys].nc[0];
+      ncy = sp[sys].nc[1];
+      ncz = sp[sys].nc[2];
+      c0 = sp[sys].c0;
+    } else {
+      c = item / P.nsplit;
+      part = item - c * P.nsplit;
+      nsplit = P.nsplit;
+    }
+    const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
     __syncthreads();                                       // the previous window is no longer read
+    if (BATCH)
+      for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[k] = k < 27 ? sp[sys].shift[k] : sp[sys].shift_lo[k - 27];
     if (warp == 0) {
       int cnt = 0, cs = 0;
       if (lane < 27) {
         int jx = cx - (lane / 9 - 1), jy = cy - ((lane / 3) % 3 - 1), jz = cz - (lane % 3 - 1);
-        jx = jx < 0 ? jx + P.ncx : (jx >= P.ncx ? jx - P.ncx : jx);
-        jy = jy < 0 ? jy + P.ncy : (jy >= P.ncy ? jy - P.ncy : jy);
-        jz = jz < 0 ? jz + P.ncz : (jz >= P.ncz ? jz - P.ncz : jz);
-        const int jc = (jx * P.ncy + jy) * P.ncz + jz;
+        jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
+        jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
+        jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
+        const int jc = c0 + (jx * ncy + jy) * ncz + jz;
         cs = cell_start[jc];
         cnt = cell_start[jc + 1] - cs;
       }
@@ -485,7 +535,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     // the item's atoms r * NWARP + warp, r = part, part + nsplit, ...; the
     // next atom's lengths and first two list words are loaded while this
     // one is evaluated (every slot holds at least two blocks)
-    const int astep = P.nsplit * NWARP;
+    const int astep = nsplit * NWARP;
     int2 nn_nx = make_int2(0, 0);
     uint2 p0 = make_uint2(0u, 0u), p1 = make_uint2(0u, 0u);
     if (staged && part * NWARP + warp < cin) {
@@ -577,7 +627,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
       // tracks the smallest distance and LJ table coordinate, and an atom
       // with an underflow (none in a sane system) is walked again to count
       // them
-      if (__any_sync(0xffffffffu, A.r2min < P.r2under || A.pminl < 1.f)) {
+      if (__any_sync(0xffffffffu, (HAS_EL && A.r2min < P.r2under) || (LJM && A.pminl < 1.f))) {
         unsigned cnt = 0;
         for (int b = 0; b < nbt; b++) {
           const uint2 w = __ldg(words + b * CW_ROW);
@@ -653,7 +703,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     if (threadIdx.x < CQ_COUNT) {
       double s = 0.0;
       for (int w = 0; w < NWARP; w++) s += s_red[w][threadIdx.x];
-      ipart[(size_t)item * CQ_COUNT + threadIdx.x] = s;
+      ipart[(size_t)(item0 + item) * CQ_COUNT + threadIdx.x] = s;
     }
   }
   if (lane == 0 && under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), under);
@@ -663,19 +713,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
 // sums quantity q over the items (fixed order), then one thread applies the
 // sums in a fixed order (several quantities feed one accumulator); each pair
 // was counted from both ends, hence 1/2.
-__global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce(int nitems, int mask, double tablast_e,
-                                                               const double *__restrict__ ipart,
-                                                               double *__restrict__ acc, const int *__restrict__ gs) {
-  if (gated_off(gs, 0)) return;
-  __shared__ double s_q[CQ_COUNT];
-  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double s = 0.0;
-  for (int it = lane; it < nitems; it += 32) s += ipart[(size_t)it * CQ_COUNT + q];
-  s = warp_sum(s);
-  if (lane == 0) s_q[q] = 0.5 * s;
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  const double *v = s_q;
+__device__ void cw_apply(int mask, const double *v, double *acc) {
   if (mask & 2) {
     // (CM3D's shifted sum spothe, finter_e.c:197, is read by nothing --
     // getsvirter_e reports spote -- and this path does not form it)
@@ -701,64 +739,69 @@ __global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce(int nitems, int ma
   }
 }
 
+__global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce(int nitems, int mask, double tablast_e,
+                                                               const double *__restrict__ ipart,
+                                                               double *__restrict__ acc, const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  __shared__ double s_q[CQ_COUNT];
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int it = lane; it < nitems; it += 32) s += ipart[(size_t)it * CQ_COUNT + q];
+  s = warp_sum(s);
+  if (lane == 0) s_q[q] = 0.5 * s;
+  __syncthreads();
+  if (threadIdx.x == 0) cw_apply(mask, s_q, acc);
+}
+
+// The same for a batch's compact systems: block per system, its items
+// {first, count} (none: a gather-kernel system, nothing to do), its own
+// accumulators; LJ sums where it has LJ interactions, electrostatic ones
+// where it has charges.
+__global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce_sys(int mask, const int2 *__restrict__ sitems,
+                                                                   const SysP *__restrict__ sp,
+                                                                   const double *__restrict__ ipart,
+                                                                   double *__restrict__ acc,
+                                                                   const int *__restrict__ gs) {
+  if (gated_off(gs, 0)) return;
+  const int sy = blockIdx.x;
+  const int2 r = sitems[sy];
+  if (r.y == 0) return;
+  __shared__ double s_q[CQ_COUNT];
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int it = lane; it < r.y; it += 32) s += ipart[(size_t)(r.x + it) * CQ_COUNT + q];
+  s = warp_sum(s);
+  if (lane == 0) s_q[q] = 0.5 * s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int m = mask & ((sp[sy].ninter > 0 ? 1 : 0) | (sp[sy].coul >= 0 ? 2 : 0));
+    cw_apply(m, s_q, acc + (size_t)sy * ACC_STRIDE);
+  }
+}
+
 // ------------------------------------------------------------------ host
-static size_t cw_table_bytes(const Ctx *c, int ljm) {
+static int cw_ljm_of(int ninter) { return ninter == 0 ? 0 : (ninter == 1 ? 1 : 2); }
+
+static size_t cw_table_bytes(bool el, int ljm, int ninter, int ntable) {
   size_t b = 0;
-  if (c->ncharge > 0) b += (size_t)c->ntable * (CW_RF * sizeof(float4) + CW_RG * sizeof(float2));
-  if (ljm) b += (size_t)2 * c->ninter * c->ntable * sizeof(float4);
+  if (el) b += (size_t)ntable * (CW_RF * sizeof(float4) + CW_RG * sizeof(float2));
+  if (ljm) b += (size_t)2 * ninter * ntable * sizeof(float4);
   return b;
 }
 
-static int cw_ljm(const Ctx *c) {
-  if (c->ninter == 0) return 0;
-  return c->ninter == 1 ? 1 : 2;
-}
-
-// Whether the compact path can run this context, and its tables and window
-// size: one system, at least 3 cells per axis, the full force level without
-// the RESPA switch copy, a window of the mean size (x 1.25, + 64) next to the
-// tables in the shared memory a block may use.
-int cw_setup(Ctx *c) {
-  c->cw_ok = 0;
-  if (c->mode != CM3D_NB_MIXED || c->nsys != 1) return CM3D_NB_OK;
-  if (c->nc[0] < 3 || c->nc[1] < 3 || c->nc[2] < 3) return CM3D_NB_OK;
-  if (c->need_short || c->nres_lrf > 1) return CM3D_NB_OK;
-  if (c->ntypes > 16 || c->ninter > 64) return CM3D_NB_OK;       // static map / cut-off arrays
-  const char *pk = getenv("CM3D_NB_PAIR_KERNEL");
-  if (pk && (strcmp(pk, "list") == 0 || strcmp(pk, "window") == 0)) return CM3D_NB_OK;
-  const int ljm = cw_ljm(c);
-  const double mean_window = 27.0 * (double)c->n / (double)c->ncells;
-  const size_t want_cap = (size_t)(1.25 * mean_window) + 64;
-  const size_t budget = c->smem_optin > CW_STATIC_SMEM ? c->smem_optin - CW_STATIC_SMEM : 0;
-  const size_t per_slot = sizeof(float4) + (ljm == 2 ? 1 : 0);
-  const size_t tb = cw_table_bytes(c, ljm);
-  if (tb + (want_cap + 1) * per_slot + 16 > budget) return CM3D_NB_OK;
-  long long cap = (long long)((budget - tb - 16) / per_slot) - 1;
-  cap = std::min<long long>(cap, CW_MAX_CAP);
-  // CM3D_NB_CW_CAP lowers the window capacity (tests of the fall-back)
-  const char *ce = getenv("CM3D_NB_CW_CAP");
-  if (ce && atoi(ce) > 0) cap = std::min<long long>(cap, atoi(ce));
-  c->cw_cap = (int)cap;
-  c->cw_smem = tb + ((size_t)cap + 1) * sizeof(float4) + (ljm == 2 ? (size_t)cap + 1 : 0);
-  c->cw_smem = (c->cw_smem + 15) / 16 * 16;
-  // slot: each segment rounded up to whole blocks
-  const long long blocks = (c->nbr_stride + CW_BLOCK - 1) / CW_BLOCK + 1;
-  c->cw_words = (int)(blocks * CW_ROW);
-  CK(cudaMalloc(&c->cwl, sizeof(uint2) * (size_t)c->n * (size_t)c->cw_words));
-  CK(cudaMalloc(&c->cwn, sizeof(int2) * (size_t)c->n));
-  CK(cudaMemset(c->cwn, 0, sizeof(int2) * (size_t)c->n));
-  // tables: erfc force coefficients + base energy, energy slope/curvature;
-  // LJ 2 float4 per knot (the compact layout of nb_pair.cu's batch tables)
-  const int nt = c->ntable;
-  if (c->ncharge > 0) {
-    std::vector<double> ct(nt), dct(nt);
-    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
-    // knot 0: CM3D's clamp below the table (the value at knot 1, no slope);
-    // knots ntable - 3 and up: zeros (the saturated coordinate of a pair at
-    // or beyond the cut-off reads knot ntable - 3)
-    std::vector<float4> tf(nt, make_float4(0.f, 0.f, 0.f, 0.f));
-    std::vector<float2> tg(nt, make_float2(0.f, 0.f));
+// The compact tables of one system: erfc force coefficients + base energy
+// and energy slope/curvature (knot 0: CM3D's clamp below the table, the
+// value at knot 1 with no slope; knots ntable - 3 and up: zeros, which the
+// saturated coordinate of a pair at or beyond the cut-off reads); LJ 2 float4
+// per knot {d0, dA, dB, v0 hi} {vA, vB, v0 lo, -} for its interactions.
+static void cw_build_tables(int nt, const double *ct, const double *dct, const double *vt, const double *dv,
+                            int ninter, std::vector<float4> &tf, std::vector<float2> &tg, std::vector<float4> &tl) {
+  tf.clear();
+  tg.clear();
+  tl.clear();
+  if (ct) {
+    tf.assign(nt, make_float4(0.f, 0.f, 0.f, 0.f));
+    tg.assign(nt, make_float2(0.f, 0.f));
     tf[0] = make_float4((float)dct[1], 0.f, 0.f, (float)ct[1]);
     for (int k = 1; k <= nt - 4; k++) {
       const double d0 = dct[k], da = 0.5 * (dct[k + 1] - dct[k - 1]),
@@ -767,36 +810,140 @@ int cw_setup(Ctx *c) {
       tf[k] = make_float4((float)d0, (float)da, (float)db, (float)v0);
       tg[k] = make_float2((float)va, (float)vb);
     }
+  }
+  tl.assign((size_t)2 * ninter * nt, make_float4(0.f, 0.f, 0.f, 0.f));
+  for (int in = 0; in < ninter; in++)
+    for (int k = 1; k <= nt - 2; k++) {
+      const double *d = dv + (size_t)in * nt, *v = vt + (size_t)in * nt;
+      const double d0 = d[k], da = 0.5 * (d[k + 1] - d[k - 1]), db = 0.5 * (d[k - 1] - 2.0 * d[k] + d[k + 1]);
+      const double v0 = v[k], va = 0.5 * (v[k + 1] - v[k - 1]), vb = 0.5 * (v[k - 1] - 2.0 * v[k] + v[k + 1]);
+      // v0 as hi + lo: the kernel sums the hi parts in FP64
+      const float hi = (float)v0;
+      tl[2 * ((size_t)in * nt + k)] = make_float4((float)d0, (float)da, (float)db, hi);
+      tl[2 * ((size_t)in * nt + k) + 1] = make_float4((float)va, (float)vb, (float)(v0 - (double)hi), 0.f);
+    }
+}
+
+// the erfc part of the pair parameters of a system with charges
+static void cw_coul_params(CwP &P, int nt, double rmaxl_coul2, double dx2coul, double rmins_coul2) {
+  P.rc2_el = (float)rmaxl_coul2;
+  P.dx2c = (float)dx2coul;
+  P.offc = (float)(rmins_coul2 * dx2coul);
+  P.pmax = (float)(nt - 3);
+  P.sat_a = (float)(dx2coul / (nt - 3));
+  P.sat_b = (float)(-rmins_coul2 * dx2coul / (nt - 3));
+  P.r2under = (float)(rmins_coul2 + 1.0 / dx2coul);
+}
+
+// the one-interaction LJ parameters from its 8 cut-off doubles (icut)
+static void cw_lj1_params(CwP &P, const double *q) {
+  P.rc2_l = (float)q[2];          // rmaxl_cut2
+  P.dx2l = (float)q[6];           // dx2tab
+  P.offl = (float)(q[1] * q[6]);  // rmins_cut2 * dx2tab
+  P.vtl = (float)q[7];            // vtab[ntable - 4]
+}
+
+// A group of a batch's compact systems: the same tables and parameters.
+struct CwGroup {
+  bool el = false;
+  int ljm = 0;
+  CwP P;                   // parameters; nitems = the group's items
+  int item0 = 0;           // first item (global item index)
+  size_t smem = 0;
+  size_t tf0 = 0, tl0 = 0; // offsets of its tables in cw_tf / cw_tg (knots) and cw_tl (float4)
+  std::string key;         // tables + parameters, byte for byte
+};
+
+static std::vector<CwGroup> &cw_groups(Ctx *c) { return *reinterpret_cast<std::vector<CwGroup> *>(c->cw_grp); }
+
+void cw_destroy(Ctx *c) {
+  delete reinterpret_cast<std::vector<CwGroup> *>(c->cw_grp);
+  c->cw_grp = nullptr;
+}
+
+static bool cw_env_off() {
+  const char *pk = getenv("CM3D_NB_PAIR_KERNEL");
+  return pk && (strcmp(pk, "list") == 0 || strcmp(pk, "window") == 0);
+}
+
+// CM3D_NB_CW_CAP lowers the window capacity (tests of the fall-back)
+static long long cw_env_cap(long long cap) {
+  const char *ce = getenv("CM3D_NB_CW_CAP");
+  if (ce && atoi(ce) > 0) cap = std::min<long long>(cap, atoi(ce));
+  return cap;
+}
+
+// the compact list's 8-byte words per atom slot: each segment rounded up to
+// whole blocks
+static int cw_words_for(long long stride) { return (int)(((stride + CW_BLOCK - 1) / CW_BLOCK + 1) * CW_ROW); }
+
+static int cw_setup_batch(Ctx *c);
+
+// Whether the compact path can run this context, and its tables and window
+// size: one system with at least 3 cells per axis (a batch: cw_setup_batch),
+// the full force level without the RESPA switch copy, a window of the mean
+// size (x 1.25, + 64) next to the tables in the shared memory a block may use.
+int cw_setup(Ctx *c) {
+  c->cw_ok = 0;
+  if (c->mode != CM3D_NB_MIXED) return CM3D_NB_OK;
+  if (c->need_short || c->nres_lrf > 1) return CM3D_NB_OK;
+  if (cw_env_off()) return CM3D_NB_OK;
+  if (c->nsys > 1) return cw_setup_batch(c);
+  if (c->nc[0] < 3 || c->nc[1] < 3 || c->nc[2] < 3) return CM3D_NB_OK;
+  if (c->ntypes > 16 || c->ninter > 64) return CM3D_NB_OK;       // static map / cut-off arrays
+  const int ljm = cw_ljm_of(c->ninter);
+  const bool el = c->ncharge > 0;
+  const double mean_window = 27.0 * (double)c->n / (double)c->ncells;
+  const size_t want_cap = (size_t)(1.25 * mean_window) + 64;
+  const size_t budget = c->smem_optin > CW_STATIC_SMEM ? c->smem_optin - CW_STATIC_SMEM : 0;
+  const size_t per_slot = sizeof(float4) + (ljm == 2 ? 1 : 0);
+  const size_t tb = cw_table_bytes(el, ljm, c->ninter, c->ntable);
+  if (tb + (want_cap + 1) * per_slot + 16 > budget) return CM3D_NB_OK;
+  long long cap = (long long)((budget - tb - 16) / per_slot) - 1;
+  cap = cw_env_cap(std::min<long long>(cap, CW_MAX_CAP));
+  c->cw_cap = (int)cap;
+  c->cw_smem = tb + ((size_t)cap + 1) * sizeof(float4) + (ljm == 2 ? (size_t)cap + 1 : 0);
+  c->cw_smem = (c->cw_smem + 15) / 16 * 16;
+  c->cw_words = cw_words_for(c->nbr_stride);
+  CK(cudaMalloc(&c->cwl, sizeof(uint2) * (size_t)c->n * (size_t)c->cw_words));
+  CK(cudaMalloc(&c->cwn, sizeof(int2) * (size_t)c->n));
+  CK(cudaMemset(c->cwn, 0, sizeof(int2) * (size_t)c->n));
+  const int nt = c->ntable;
+  std::vector<double> ct, dct, vt, dv, cut;
+  if (el) {
+    ct.resize(nt);
+    dct.resize(nt);
+    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * nt, cudaMemcpyDeviceToHost));
+  }
+  if (ljm) {
+    vt.resize((size_t)c->ninter * nt);
+    dv.resize(vt.size());
+    cut.resize(8 * (size_t)c->ninter);
+    CK(cudaMemcpy(vt.data(), c->vtab, sizeof(double) * vt.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dv.data(), c->dvtab, sizeof(double) * dv.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cut.data(), c->icut, sizeof(double) * cut.size(), cudaMemcpyDeviceToHost));
+  }
+  std::vector<float4> tf, tl;
+  std::vector<float2> tg;
+  cw_build_tables(nt, el ? ct.data() : nullptr, el ? dct.data() : nullptr, vt.data(), dv.data(), ljm ? c->ninter : 0,
+                  tf, tg, tl);
+  if (el) {
     CK(cudaMalloc(&c->cw_tf, sizeof(float4) * nt));
     CK(cudaMalloc(&c->cw_tg, sizeof(float2) * nt));
     CK(cudaMemcpy(c->cw_tf, tf.data(), sizeof(float4) * nt, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(c->cw_tg, tg.data(), sizeof(float2) * nt, cudaMemcpyHostToDevice));
   }
   if (ljm) {
-    const int ni = c->ninter;
-    std::vector<double> vt((size_t)ni * nt), dv((size_t)ni * nt), cut(8 * (size_t)ni);
-    CK(cudaMemcpy(vt.data(), c->vtab, sizeof(double) * vt.size(), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(dv.data(), c->dvtab, sizeof(double) * dv.size(), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(cut.data(), c->icut, sizeof(double) * cut.size(), cudaMemcpyDeviceToHost));
-    std::vector<float4> tl((size_t)2 * ni * nt, make_float4(0.f, 0.f, 0.f, 0.f));
-    for (int in = 0; in < ni; in++)
-      for (int k = 1; k <= nt - 2; k++) {
-        const double *d = &dv[(size_t)in * nt], *v = &vt[(size_t)in * nt];
-        const double d0 = d[k], da = 0.5 * (d[k + 1] - d[k - 1]), db = 0.5 * (d[k - 1] - 2.0 * d[k] + d[k + 1]);
-        const double v0 = v[k], va = 0.5 * (v[k + 1] - v[k - 1]), vb = 0.5 * (v[k - 1] - 2.0 * v[k] + v[k + 1]);
-        // v0 as hi + lo: the kernel sums the hi parts in FP64
-        const float hi = (float)v0;
-        tl[2 * ((size_t)in * nt + k)] = make_float4((float)d0, (float)da, (float)db, hi);
-        tl[2 * ((size_t)in * nt + k) + 1] = make_float4((float)va, (float)vb, (float)(v0 - (double)hi), 0.f);
-      }
     CK(cudaMalloc(&c->cw_tl, sizeof(float4) * tl.size()));
     CK(cudaMemcpy(c->cw_tl, tl.data(), sizeof(float4) * tl.size(), cudaMemcpyHostToDevice));
     if (ljm == 1) {
-      const double *q = &cut[0];
-      c->cw_lj1[0] = (float)q[2];           // rmaxl_cut2
-      c->cw_lj1[1] = (float)q[6];           // dx2tab
-      c->cw_lj1[2] = (float)(q[1] * q[6]);  // rmins_cut2 * dx2tab
-      c->cw_lj1[3] = (float)q[7];           // vtab[ntable - 4]
+      CwP q;
+      cw_lj1_params(q, &cut[0]);
+      c->cw_lj1[0] = q.rc2_l;
+      c->cw_lj1[1] = q.dx2l;
+      c->cw_lj1[2] = q.offl;
+      c->cw_lj1[3] = q.vtl;
     }
   }
   // work items: cells, split into parts where the cells are fewer than four
@@ -810,33 +957,202 @@ int cw_setup(Ctx *c) {
   return CM3D_NB_OK;
 }
 
-// work items of the compact kernel: each cell's atoms in `nsplit` parts
+// A batch: every system with at least 3 cells per axis (and at most 16 atom
+// types and 64 interactions) runs in the compact kernel; the systems whose
+// tables and pair parameters agree byte for byte form a group, one launch
+// each with the group's tables staged once per block; the other systems run
+// in the gather kernel.  Items: one per cell, in system order within a group.
+static int cw_setup_batch(Ctx *c) {
+  const int nt = c->ntable, nsys = c->nsys;
+  std::vector<double> ct, dct, vt((size_t)c->ninter * nt), dv(vt.size()), cut(8 * (size_t)c->ninter);
+  if (c->ninter > 0) {
+    CK(cudaMemcpy(vt.data(), c->vtab, sizeof(double) * vt.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dv.data(), c->dvtab, sizeof(double) * dv.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cut.data(), c->icut, sizeof(double) * cut.size(), cudaMemcpyDeviceToHost));
+  }
+  if (c->ncoul > 0) {
+    ct.resize((size_t)c->ncoul * nt);
+    dct.resize(ct.size());
+    CK(cudaMemcpy(ct.data(), c->coultab, sizeof(double) * ct.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(dct.data(), c->dcoultab, sizeof(double) * dct.size(), cudaMemcpyDeviceToHost));
+  }
+  size_t nmap = 0;
+  for (int s = 0; s < nsys; s++) nmap = std::max(nmap, (size_t)(c->h_sp[s].map0 + c->h_sp[s].ntypes * c->h_sp[s].ntypes));
+  std::vector<int> gmap(nmap > 0 ? nmap : 1);
+  if (nmap) CK(cudaMemcpy(gmap.data(), c->map, sizeof(int) * nmap, cudaMemcpyDeviceToHost));
+
+  auto *groups = new std::vector<CwGroup>();
+  c->cw_grp = groups;
+  std::vector<int> gid(nsys, -1), cwsys(nsys, 0);
+  std::vector<std::vector<float4>> gtf, gtl;
+  std::vector<std::vector<float2>> gtg;
+  double want_window = 0.0;
+  for (int s = 0; s < nsys; s++) {
+    const SysP &S = c->h_sp[s];
+    const SysH &H = c->hs[s];
+    if (S.nc[0] < 3 || S.nc[1] < 3 || S.nc[2] < 3) continue;
+    if (S.ntypes > 16 || S.ninter > 64) continue;
+    const bool el = S.coul >= 0;
+    const int ljm = cw_ljm_of(S.ninter);
+    if (!el && !ljm) continue;
+    std::vector<float4> tf, tl;
+    std::vector<float2> tg;
+    cw_build_tables(nt, el ? &ct[(size_t)S.coul * nt] : nullptr, el ? &dct[(size_t)S.coul * nt] : nullptr,
+                    S.ninter ? &vt[(size_t)S.inter0 * nt] : nullptr, S.ninter ? &dv[(size_t)S.inter0 * nt] : nullptr,
+                    S.ninter, tf, tg, tl);
+    CwP P;
+    memset(&P, 0, sizeof P);
+    P.ntable = nt;
+    P.ntypes = S.ntypes;
+    P.ninter = S.ninter;
+    P.pmax = (float)(nt - 3);
+    if (el) cw_coul_params(P, nt, H.rmaxl_coul2, H.dx2coul, H.rmins_coul2);
+    if (ljm == 1) cw_lj1_params(P, &cut[8 * (size_t)S.inter0]);
+    // the group key: everything the kernel reads besides the geometry
+    std::string key;
+    auto put = [&](const void *p, size_t b) { key.append(reinterpret_cast<const char *>(p), b); };
+    const int hdr[4] = {el ? 1 : 0, ljm, S.ntypes, S.ninter};
+    put(hdr, sizeof hdr);
+    const float prm[11] = {P.rc2_el, P.dx2c, P.offc, P.pmax, P.sat_a, P.sat_b, P.r2under, P.rc2_l, P.dx2l, P.offl, P.vtl};
+    put(prm, sizeof prm);
+    put(tf.data(), sizeof(float4) * tf.size());
+    put(tg.data(), sizeof(float2) * tg.size());
+    put(tl.data(), sizeof(float4) * tl.size());
+    for (int k = 0; k < S.ntypes * S.ntypes; k++) {
+      const int in = gmap[S.map0 + k];
+      const int loc = in >= 0 ? in - S.inter0 : -1;
+      put(&loc, sizeof loc);
+    }
+    for (int k = 0; k < S.ninter; k++) {
+      const double *q = &cut[8 * ((size_t)S.inter0 + k)];
+      const float f4[4] = {(float)q[0], (float)q[2], (float)q[1], (float)q[3]};
+      put(f4, sizeof f4);
+    }
+    int g = -1;
+    for (size_t k = 0; k < groups->size(); k++)
+      if ((*groups)[k].key == key) g = (int)k;
+    if (g < 0) {
+      CwGroup G;
+      G.el = el;
+      G.ljm = ljm;
+      P.map0 = S.map0;
+      P.inter0 = S.inter0;
+      G.P = P;
+      G.key = key;
+      groups->push_back(G);
+      gtf.push_back(tf);
+      gtg.push_back(tg);
+      gtl.push_back(tl);
+      g = (int)groups->size() - 1;
+    }
+    gid[s] = g;
+    cwsys[s] = 1;
+    want_window = std::max(want_window, 27.0 * (double)S.n / (double)S.ncells);
+  }
+  if (groups->empty()) return CM3D_NB_OK;
+  // one window capacity for all groups: what shared memory leaves next to
+  // the largest tables, and at least the largest mean window x 1.25 + 64
+  const size_t budget = c->smem_optin > CW_STATIC_SMEM ? c->smem_optin - CW_STATIC_SMEM : 0;
+  long long cap = CW_MAX_CAP;
+  for (const CwGroup &G : *groups) {
+    const size_t tb = cw_table_bytes(G.el, G.ljm, G.P.ninter, nt);
+    const size_t per_slot = sizeof(float4) + (G.ljm == 2 ? 1 : 0);
+    const long long room = budget > tb + 16 ? (long long)((budget - tb - 16) / per_slot) - 1 : 0;
+    cap = std::min(cap, room);
+  }
+  cap = cw_env_cap(cap);
+  if ((double)cap < 1.25 * want_window + 64.0) {
+    groups->clear();
+    return CM3D_NB_OK;
+  }
+  c->cw_cap = (int)cap;
+  // items by group, systems in order; tables back to back
+  std::vector<int4> items;
+  std::vector<int2> sitems(nsys, make_int2(0, 0));
+  std::vector<float4> atf, atl;
+  std::vector<float2> atg;
+  for (size_t g = 0; g < groups->size(); g++) {
+    CwGroup &G = (*groups)[g];
+    G.item0 = (int)items.size();
+    for (int s = 0; s < nsys; s++) {
+      if (gid[s] != (int)g) continue;
+      const SysP &S = c->h_sp[s];
+      sitems[s] = make_int2((int)items.size(), S.ncells);
+      for (int k = 0; k < S.ncells; k++) items.push_back(make_int4(s, k, 0, 1));
+    }
+    G.P.nitems = (int)items.size() - G.item0;
+    G.P.nsplit = 1;
+    G.P.cap = c->cw_cap;
+    G.tf0 = atf.size();
+    G.tl0 = atl.size();
+    atf.insert(atf.end(), gtf[g].begin(), gtf[g].end());
+    atg.insert(atg.end(), gtg[g].begin(), gtg[g].end());
+    atl.insert(atl.end(), gtl[g].begin(), gtl[g].end());
+    const size_t tb = cw_table_bytes(G.el, G.ljm, G.P.ninter, nt);
+    G.smem = (tb + ((size_t)c->cw_cap + 1) * sizeof(float4) + (G.ljm == 2 ? (size_t)c->cw_cap + 1 : 0) + 15) / 16 * 16;
+  }
+  // the gather kernel's atoms: the other systems' (a system's sorted
+  // indices span its own atom range)
+  std::vector<int> gidx;
+  for (int s = 0; s < nsys; s++)
+    if (!cwsys[s])
+      for (int a = c->h_sp[s].a0; a < c->h_sp[s].a0 + c->h_sp[s].n; a++) gidx.push_back(a);
+  c->cw_ng = (int)gidx.size();
+  auto upload_v = [&](auto **dst, const auto &v) -> int {
+    using T = typename std::remove_reference<decltype(v)>::type::value_type;
+    CK(cudaMalloc((void **)dst, sizeof(T) * (v.empty() ? 1 : v.size())));
+    if (!v.empty()) CK(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return CM3D_NB_OK;
+  };
+  int rc;
+  if ((rc = upload_v(&c->cw_items, items)) || (rc = upload_v(&c->cw_sitems, sitems)) ||
+      (rc = upload_v(&c->cw_sys, cwsys)) || (rc = upload_v(&c->cw_gidx, gidx)) || (rc = upload_v(&c->cw_tf, atf)) ||
+      (rc = upload_v(&c->cw_tg, atg)) || (rc = upload_v(&c->cw_tl, atl)))
+    return rc;
+  c->cw_words = cw_words_for(c->nbr_stride);
+  CK(cudaMalloc(&c->cwl, sizeof(uint2) * (size_t)c->n * (size_t)c->cw_words));
+  CK(cudaMalloc(&c->cwn, sizeof(int2) * (size_t)c->n));
+  CK(cudaMemset(c->cwn, 0, sizeof(int2) * (size_t)c->n));
+  c->cw_nitems = (int)items.size();
+  c->cw_nsplit = 1;
+  CK(cudaMalloc(&c->cw_part, sizeof(double) * CQ_COUNT * (size_t)c->cw_nitems));
+  c->cw_batch = 1;
+  c->cw_ok = 1;
+  c->cw_use = 1;
+  return CM3D_NB_OK;
+}
+
+// work items of the compact kernel (one system): each cell's atoms in
+// `nsplit` parts
 void cw_set_split(Ctx *c, int nsplit) {
+  if (c->cw_batch) return;
   c->cw_nsplit = std::max(1, std::min(nsplit, CW_MAX_SPLIT));
   c->cw_nitems = c->ncells * c->cw_nsplit;
 }
 
-// after a (gated) rebuild of the master list: the compact list
-int cw_convert(Ctx *c, bool device_flag) {
+// after a (gated) rebuild of the master list: the compact list (a batch:
+// of the compact systems being rebuilt, or of all after the slots widened)
+int cw_convert(Ctx *c, bool device_flag, bool all) {
   if (!c->cw_ok) return CM3D_NB_OK;
   // the master slots widen on overflow (host-driven builds only): so do ours
-  const int words = (int)(((c->nbr_stride + CW_BLOCK - 1) / CW_BLOCK + 1) * CW_ROW);
+  const int words = cw_words_for(c->nbr_stride);
   if (words > c->cw_words) {
     CK(cudaStreamSynchronize(c->st));
     cudaFree(c->cwl);
     c->cwl = nullptr;
     CK(cudaMalloc(&c->cwl, sizeof(uint2) * (size_t)c->n * (size_t)words));
     c->cw_words = words;
+    all = true;
     if (c->graph) {
       cudaGraphExecDestroy(c->graph);
       c->graph = nullptr;
     }
   }
   const int *gate = device_flag ? c->istate : nullptr;
-  k_cw_convert<<<grid_for(32LL * c->n, 256), 256, 0, c->st>>>(c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n,
-                                                               c->cw_words, c->cell_start, c->cell_of, c->cell_atoms,
-                                        c->nlen, c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat,
-                                        device_flag ? c->istate + IS_HALT : nullptr, gate);
+  k_cw_convert<<<grid_for(32LL * c->n, 256), 256, 0, c->st>>>(
+      c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n, c->cw_words, c->cell_start, c->cell_of, c->cell_atoms, c->nlen,
+      c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate, c->sp,
+      c->sys_of, c->cw_batch ? c->cw_sys : nullptr, c->sreb, all ? 1 : 0);
   c->launches++;
   CKL(c);
   if (!device_flag) {
@@ -854,26 +1170,57 @@ int cw_convert(Ctx *c, bool device_flag) {
   return CM3D_NB_OK;
 }
 
-template <bool EL, int LJM>
-static void cw_launch_t(Ctx *c, const CwP &P, double *fout) {
-  auto kern = k_pair_cw<EL, LJM>;
+template <bool EL, int LJM, bool BATCH>
+static void cw_launch_t(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
+                        const float4 *tl, const int4 *items, int item0) {
+  auto kern = k_pair_cw<EL, LJM, BATCH>;
   static unsigned long long attr_devs = 0;
   if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(c->smem_optin - CW_STATIC_SMEM));
     attr_devs |= 1ull << c->dev;
   }
   const int grid = std::min(P.nitems, c->num_sms);
-  kern<<<grid, CW_THREADS, c->cw_smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl,
-                                                 c->shift, c->map, c->fcut, c->cw_tf, c->cw_tg, c->cw_tl, fout,
-                                                 c->cw_part, c->stat, c->gate);
+  kern<<<grid, CW_THREADS, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl, c->shift,
+                                          c->map, c->fcut, tf, tg, tl, fout, c->cw_part, c->stat, c->gate, items,
+                                          c->sp, item0);
+}
+
+template <bool BATCH>
+static void cw_launch(Ctx *c, bool el, int ljm, const CwP &P, size_t smem, double *fout, const float4 *tf,
+                      const float2 *tg, const float4 *tl, const int4 *items, int item0) {
+  if (el) {
+    if (ljm == 0) cw_launch_t<true, 0, BATCH>(c, P, smem, fout, tf, tg, tl, items, item0);
+    else if (ljm == 1) cw_launch_t<true, 1, BATCH>(c, P, smem, fout, tf, tg, tl, items, item0);
+    else cw_launch_t<true, 2, BATCH>(c, P, smem, fout, tf, tg, tl, items, item0);
+  } else {
+    if (ljm == 1) cw_launch_t<false, 1, BATCH>(c, P, smem, fout, tf, tg, tl, items, item0);
+    else if (ljm == 2) cw_launch_t<false, 2, BATCH>(c, P, smem, fout, tf, tg, tl, items, item0);
+  }
 }
 
 bool cw_applies(Ctx *c, int iflg, bool ns) { return c->cw_ok && c->cw_use && iflg == 1 && !ns; }
 
-// full force level of one system through the compact path (the caller
-// checked cw_applies); mask bit0 LJ, bit1 charges
+// full force level through the compact path (the caller checked cw_applies):
+// one system, or a batch's compact groups (the caller runs the gather kernel
+// over the other systems' atoms); mask bit0 LJ, bit1 charges
 int cw_pairs(Ctx *c, int mask, double *fout) {
+  if (c->cw_batch) {
+    for (const CwGroup &G : cw_groups(c)) {
+      CwP P = G.P;
+      P.n = c->n;
+      P.words = c->cw_words;
+      const bool el = G.el && (mask & 2);
+      const int ljm = (mask & 1) ? G.ljm : 0;
+      if (!el && !ljm) continue;
+      cw_launch<true>(c, el, ljm, P, G.smem, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,
+                      c->cw_items + G.item0, G.item0);
+      c->launches++;
+    }
+    CKL(c);
+    return CM3D_NB_OK;
+  }
   CwP P;
+  memset(&P, 0, sizeof P);
   P.n = c->n;
   P.ncx = c->nc[0];
   P.ncy = c->nc[1];
@@ -885,34 +1232,24 @@ int cw_pairs(Ctx *c, int mask, double *fout) {
   P.ntable = c->ntable;
   P.ntypes = c->ntypes;
   P.ninter = c->ninter;
-  P.rc2_el = (float)c->rmaxl_coul2;
-  P.dx2c = (float)c->dx2coul;
-  P.offc = (float)(c->rmins_coul2 * c->dx2coul);
-  P.pmax = (float)(c->ntable - 3);
-  P.sat_a = (float)(c->dx2coul / (c->ntable - 3));
-  P.sat_b = (float)(-c->rmins_coul2 * c->dx2coul / (c->ntable - 3));
-  P.r2under = (float)(c->rmins_coul2 + 1.0 / c->dx2coul);
+  cw_coul_params(P, c->ntable, c->rmaxl_coul2, c->dx2coul, c->rmins_coul2);
   P.rc2_l = c->cw_lj1[0];
   P.dx2l = c->cw_lj1[1];
   P.offl = c->cw_lj1[2];
   P.vtl = c->cw_lj1[3];
   const bool el = (mask & 2) != 0;
-  const int ljm = (mask & 1) ? cw_ljm(c) : 0;
-  if (el) {
-    if (ljm == 0) cw_launch_t<true, 0>(c, P, fout);
-    else if (ljm == 1) cw_launch_t<true, 1>(c, P, fout);
-    else cw_launch_t<true, 2>(c, P, fout);
-  } else {
-    if (ljm == 1) cw_launch_t<false, 1>(c, P, fout);
-    else if (ljm == 2) cw_launch_t<false, 2>(c, P, fout);
-  }
+  const int ljm = (mask & 1) ? cw_ljm_of(c->ninter) : 0;
+  cw_launch<false>(c, el, ljm, P, c->cw_smem, fout, c->cw_tf, c->cw_tg, c->cw_tl, nullptr, 0);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;
 }
 
 int cw_ereduce(Ctx *c, int mask) {
-  k_cw_ereduce<<<1, CQ_COUNT * 32, 0, c->st>>>(c->cw_nitems, mask, c->tablast_e, c->cw_part, c->acc, c->gate);
+  if (c->cw_batch)
+    k_cw_ereduce_sys<<<c->nsys, CQ_COUNT * 32, 0, c->st>>>(mask, c->cw_sitems, c->sp, c->cw_part, c->acc, c->gate);
+  else
+    k_cw_ereduce<<<1, CQ_COUNT * 32, 0, c->st>>>(c->cw_nitems, mask, c->tablast_e, c->cw_part, c->acc, c->gate);
   c->launches++;
   CKL(c);
   return CM3D_NB_OK;

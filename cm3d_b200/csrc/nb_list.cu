@@ -998,6 +998,19 @@ int list_setup(Ctx *c) {
   return CM3D_NB_OK;
 }
 
+// one warp per atom: its front segment (nlen[t] entries) and back segment
+// (nlen[n + t]) from a slot of `old_s` entries into one of `new_s`
+__global__ void k_regrow_copy(int n, int old_s, int new_s, const int *__restrict__ nlen,
+                              const uint32_t *__restrict__ src, uint32_t *__restrict__ dst) {
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (t >= n) return;
+  const int na = min(nlen[t], old_s), nb = min(nlen[n + t], old_s - na);
+  const uint32_t *a = src + (size_t)t * old_s;
+  uint32_t *b = dst + (size_t)t * new_s;
+  for (int k = lane; k < na; k += 32) b[k] = a[k];
+  for (int k = lane; k < nb; k += 32) b[new_s - nb + k] = a[old_s - nb + k];
+}
+
 // grow list buffers to hold at least `need` entries (with 50% headroom)
 static int grow(Ctx *c, int which, long long need) {
   if (need <= c->lcap[which]) return CM3D_NB_OK;
@@ -1024,10 +1037,17 @@ static int grow_full(Ctx *c, long long need) {
     c->graph = nullptr;
   }
   CK(cudaStreamSynchronize(c->st));
-  if (c->nbr) cudaFree(c->nbr);
-  c->nbr = nullptr;
-  cudaError_t e = cudaMalloc(&c->nbr, sizeof(uint32_t) * (size_t)c->n * (size_t)s);
+  uint32_t *wider = nullptr;
+  cudaError_t e = cudaMalloc(&wider, sizeof(uint32_t) * (size_t)c->n * (size_t)s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(full list)");
+  // the lists of the systems not being rebuilt stay valid: both segments of
+  // every slot move into the wider slots (a rebuilt system's are rewritten)
+  if (c->nbr)
+    k_regrow_copy<<<grid_for((long long)c->n * 32, 256), 256, 0, c->st>>>(c->n, c->nbr_stride, (int)s, c->nlen,
+                                                                           c->nbr, wider);
+  CK(cudaStreamSynchronize(c->st));
+  if (c->nbr) cudaFree(c->nbr);
+  c->nbr = wider;
   c->nbr_stride = (int)s;
   c->lcap[LT_FULL] = (long long)c->n * s;
   return CM3D_NB_OK;
@@ -1106,7 +1126,7 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
     }
   }
   if (c->mode == CM3D_NB_MIXED) {
-    int rc = cw_convert(c, device_flag);
+    int rc = cw_convert(c, device_flag, all);
     if (rc) return rc;
   }
   if (want_half) {

@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
     double *__restrict__ fout, double *__restrict__ fshort, float *__restrict__ epart,
     double *__restrict__ epart64, long long *__restrict__ stat, const int *__restrict__ gs,
     const int4 *__restrict__ items = nullptr, int nitems = 0, const float4 *__restrict__ gtl2 = nullptr,
-    int st_ntypes = 0, int st_ninter = 0) {
+    int st_ntypes = 0, int st_ninter = 0, const int *__restrict__ gidx = nullptr, int ng = 0) {
   static_assert(!STAGE || BATCH, "staging is for batches");
   if (gated_off(gs, 0)) return;
   extern __shared__ float4 sm[];
@@ -733,10 +733,14 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
     }
   };
   if (!STAGE) {
-    // persistent: every lane group walks atoms blockIdx-strided
-    for (int tb = blockIdx.x * groups; tb < P.n; tb += gridDim.x * groups) {
-      const int t = tb + threadIdx.x / TPA;
-      do_atom(t, t < P.n);
+    // persistent: every lane group walks atoms blockIdx-strided (with gidx:
+    // only the listed sorted atoms, the rest of a batch being in the
+    // compact kernel)
+    const int nloop = gidx ? ng : P.n;
+    for (int tb = blockIdx.x * groups; tb < nloop; tb += gridDim.x * groups) {
+      const int tt = tb + threadIdx.x / TPA;
+      const int t = gidx ? (tt < ng ? gidx[tt] : 0) : tt;
+      do_atom(t, tt < nloop);
     }
   } else {
     for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -853,8 +857,10 @@ constexpr int ERS_THREADS = 128;
 __global__ void __launch_bounds__(ERS_THREADS) k_ereduce_sys(int n, int mask, const SysP *__restrict__ sp,
                                                               const float *__restrict__ epart,
                                                               const double *__restrict__ epart64,
-                                                              double *__restrict__ accs, const int *__restrict__ gs) {
+                                                              double *__restrict__ accs, const int *__restrict__ gs,
+                                                              const int *__restrict__ skip = nullptr) {
   if (gated_off(gs, 0)) return;
+  if (skip && skip[blockIdx.x]) return;                  // a compact system: its own reduction
   __shared__ double red[EP_COUNT][ERS_THREADS / 32];
   const int sy = blockIdx.x;
   const int a0 = sp[sy].a0, a1 = a0 + sp[sy].n;
@@ -918,14 +924,15 @@ static void launch_t(Ctx *c, const MixedP &P, size_t smem, double *fout) {
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, B, smem);
   if (per_sm < 1) per_sm = 1;
-  long long need = ST ? (long long)c->nsys_items : ((long long)c->n * TPA + B - 1) / B;
+  const long long nat = c->pair_gidx ? c->pair_ng : c->n;
+  long long need = ST ? (long long)c->nsys_items : (nat * TPA + B - 1) / B;
   long long grid = (long long)c->num_sms * per_sm;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   kern<<<grid, B, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->nlen, c->nbr_stride, c->nbr, c->shift,
                                  c->map, c->fcut, c->ftab_lj, c->ftab_el, c->sp, c->sys_of, fout, c->fxs, c->epart,
                                  epart_hi(c), c->stat, c->gate, c->sys_items, c->nsys_items, c->ftab_lj2,
-                                 c->stage_ntypes, c->stage_ninter);
+                                 c->stage_ntypes, c->stage_ninter, c->pair_gidx, c->pair_ng);
 }
 
 template <bool SB, bool NS, bool BT, bool ST = false, bool T2 = false>
@@ -1074,10 +1081,24 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
     // one system with >= 3 cells per axis, full force level: the compact
     // window list (nb_cwin.cu) and its own energy sums
     c->pair_used = CM3D_NB_PAIR_COMPACT;
+    c->launches++;                                   // k_xq_update
     int rc = cw_pairs(c, mask, fout);
-    tend(c, 0, e0);
-    c->launches++;
     if (rc) return rc;
+    if (c->cw_batch && c->cw_ng > 0) {
+      // a batch: the other systems' atoms in the gather kernel
+      P.tab_smem = 0;
+      c->pair_gidx = c->cw_gidx;
+      c->pair_ng = c->cw_ng;
+      launch_tpa<false, false, true, false, true>(c, P, 0, fout);
+      c->pair_gidx = nullptr;
+      c->pair_ng = 0;
+      c->launches++;
+      k_ereduce_sys<<<c->nsys, ERS_THREADS, 0, c->st>>>(c->n, mask, c->sp, c->epart, epart_hi(c), c->acc, c->gate,
+                                                         c->cw_sys);
+      c->launches++;
+    }
+    tend(c, 0, e0);
+    CKL(c);
     return cw_ereduce(c, mask);
   }
   // one system with >= 3 cells per axis: staged 27-cell windows; anything

@@ -3,12 +3,14 @@
 Every system of a batch must come out as it does alone.  The checks:
   - its pair lists, cut out of the batch's lists, are bit-exact with CM3D's;
   - its forces and energies match the same system in its own context
-    with the same pair kernel (relative 1e-12 / 1e-10; a lone system with
-    3 or more cells per axis otherwise takes the staged-window pair kernel,
-    CM3D_NB_PAIR_KERNEL=list keeps it on the list-gather kernel that
-    batches use) and, with the window kernel, to FP32 summation order
-    (1e-6); and CM3D's within the mixed engine's stated bounds (forces
-    1e-5, energies 1e-5, virials 5e-5);
+    with the same pair kernel (relative 1e-12 / 1e-10).  A system with 3 or
+    more cells per axis at the full force level runs in the compact kernel
+    in a batch as alone; the others run in the list-gather kernel in a
+    batch, and alone CM3D_NB_PAIR_KERNEL=list keeps them on it (a lone
+    system would otherwise take the staged-window kernel); against the
+    lone default kernel the forces agree to FP32 summation order (1e-6);
+    and CM3D's within the mixed engine's stated bounds (forces 1e-5,
+    energies 1e-5, virials 5e-5);
   - its trajectory tracks CM3D's per-step energies (2e-4, as for a single
     system) and its own single-context run (positions within 1e-9 A), with
     the same number of list rebuilds and RESETPOS events.
@@ -54,6 +56,18 @@ def close(a, b, tol):
     return abs(a - b) <= tol * max(abs(b), 1e-300) or abs(a - b) <= 1e-9
 
 
+def lone_env(d):
+    """CM3D_NB_PAIR_KERNEL for the lone run that uses the kernel the system
+    gets in a batch: none where alone it takes the compact kernel, "list"
+    (the gather kernel) otherwise"""
+    one = Engine(System.from_arrays(d), mode=_abi.MIXED, tpa=TPA)
+    one.get_ngbr()
+    one.force(1)
+    kind = one.pair_kernel()[0]
+    one.close()
+    return None if kind == "compact" else "list"
+
+
 @pytest.mark.parametrize("group", list(GROUPS))
 def test_batch_lists_bit_exact(engine_lib, group):
     ds, e = batch(GROUPS[group])
@@ -88,9 +102,12 @@ def test_batch_forces_and_energies(engine_lib, group, monkeypatch):
         one.force(1)
         fw = one.forces(_abi.FXL)
         one.close()
-        monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", "list")
+        env = lone_env(d)
+        if env:
+            monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", env)
         one = Engine(System.from_arrays(d), mode=_abi.MIXED, tpa=TPA)
-        monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
+        if env:
+            monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
         one.get_ngbr()
         one.force(1)
         one.force(2)
@@ -128,9 +145,12 @@ def test_batch_trajectory(engine_lib, group, graph, monkeypatch):
     e.close()
     for s, d in enumerate(ds):
         a0, n = e.ranges[s]
-        monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", "list")
+        env = lone_env(d)
+        if env:
+            monkeypatch.setenv("CM3D_NB_PAIR_KERNEL", env)
         one = Engine(System.from_arrays(d), mode=_abi.MIXED, tpa=TPA, use_graph=graph)
-        monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
+        if env:
+            monkeypatch.delenv("CM3D_NB_PAIR_KERNEL")
         one.step_init()
         one.step(1, nsteps)
         p1 = one.positions()

@@ -163,7 +163,76 @@ def test_headline_kernel_on_large_boxes(engine_lib, large_boxes, monkeypatch):
             assert close(en[s][k], eo[k], tol, floor=1e-6 * max(1.0, abs(eo["U"]))), (s, k, en[s][k], eo[k])
     import json
     import os
-    line = json.dumps({"config": "ensemble_large_boxes", "kernel": "gather, 4 lanes per atom", "boxes": stats})
+    line = json.dumps({"config": "ensemble_large_boxes_gather", "kernel": "gather, 4 lanes per atom", "boxes": stats})
+    print("ERRSTAT", line)
+    if os.environ.get("CM3D_NB_ERRLOG"):
+        with open(os.environ["CM3D_NB_ERRLOG"], "a") as fh:
+            fh.write(line + "\n")
+
+
+def test_compact_batch_on_large_boxes(engine_lib, large_boxes):
+    """the headline's default pair path: the batch's boxes with 3 or more
+    cells per axis in the compact kernel (grouped by their tables), the
+    others in the gather kernel in the same force call -- on the headline
+    ensemble's largest and smallest boxes against each box's oracle, at
+    positions the oracle reached after 10 steps; the compact boxes' forces
+    are bit-identical to the same box alone (one system, compact kernel),
+    and a repeat of the force call gives the same bits"""
+    from oracle import Oracle
+    pos = []
+    for sm in large_boxes:
+        o = Oracle(sm, nocell_all=1)
+        o.step_init()
+        o.step(1, 10)
+        pos.append(o.positions())
+    e = Engine(large_boxes, mode=_abi.MIXED, tpa=4)
+    e.set_positions(np.concatenate(pos, axis=1))
+    e.get_ngbr()
+    e.force(1)
+    assert e.pair_kernel()[0] == "compact"
+    f = e.forces(_abi.FXL)
+    e.force(1)
+    np.testing.assert_array_equal(e.forces(_abi.FXL), f)
+    e.force(2)
+    en = e.all_energies()
+    grids = [e.grid(s)[0] for s in range(len(large_boxes))]
+    assert e.status()["stage_timeouts"] == 0
+    e.close()
+    ncompact = 0
+    stats = []
+    for s, sm in enumerate(large_boxes):
+        a0, n = e.ranges[s]
+        if min(grids[s]) >= 3:
+            ncompact += 1
+            one = Engine(sm, mode=_abi.MIXED)
+            one.set_positions(pos[s])
+            one.get_ngbr()
+            one.force(1)
+            assert one.pair_kernel()[0] == "compact"
+            np.testing.assert_array_equal(f[:, a0:a0 + n], one.forces(_abi.FXL))
+            one.close()
+        o = Oracle(sm, nocell_all=1)
+        o.set_positions(pos[s])
+        o.get_ngbr()
+        o.force(1)
+        o.force(2)
+        fo = o.forces(_abi.FXL)
+        scale = float(np.sqrt((fo * fo).mean()))
+        assert rel_rms(f[:, a0:a0 + n], fo, scale) <= FTOL, s
+        d = np.sqrt(((f[:, a0:a0 + n] - fo) ** 2).sum(axis=0))
+        stats.append({"natoms": n, "charged": bool(sm.get("ncharge", 0)), "cells": grids[s],
+                      "kernel": "compact" if min(grids[s]) >= 3 else "gather",
+                      "rel_rms": rel_rms(f[:, a0:a0 + n], fo),
+                      "max_atom_over_rms": float(d.max() / np.sqrt((fo * fo).sum(axis=0).mean()))})
+        eo = o.energies()
+        for k in ("vinter", "velec", "vewald", "U", "W", "prsi", "zke"):
+            tol = VTOL if k in VIRIAL_KEYS else ETOL
+            assert close(en[s][k], eo[k], tol, floor=1e-6 * max(1.0, abs(eo["U"]))), (s, k, en[s][k], eo[k])
+    assert 0 < ncompact < len(large_boxes), "the slice should hold compact and gather boxes"
+    import json
+    import os
+    line = json.dumps({"config": "ensemble_large_boxes_compact", "kernel": "compact batch + gather, 4 lanes",
+                       "boxes": stats})
     print("ERRSTAT", line)
     if os.environ.get("CM3D_NB_ERRLOG"):
         with open(os.environ["CM3D_NB_ERRLOG"], "a") as fh:
