@@ -517,6 +517,7 @@ def main() -> None:
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the secondary workloads")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--tpa", type=int, default=0, choices=[0, 4, 8, 16, 32],
                     help="pin the pair kernel's lanes per atom instead of autotuning (profiling runs)")
     ap.add_argument("--pair-kernel", default="gather", choices=["gather", "staged", "compact"],
@@ -664,7 +665,7 @@ def main() -> None:
         nve = nve_arm(local)
 
     serving = None
-    if not args.no_extra and world == 1:
+    if not args.no_extra and not args.no_serving and world == 1:
         if args.serving_sweep:
             serving = [serving_arm(r, args.serving_window, local, not args.no_plain) for r in (0.5, 1.0, 2.0, 4.0, 8.0)]
         else:

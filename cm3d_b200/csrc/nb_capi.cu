@@ -1162,7 +1162,7 @@ int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa) {
   return CM3D_NB_OK;
 }
 
-int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit) {
+int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit, int *block_threads) {
   CTX;
   if (sys < 0 || sys >= c->nsys) {
     set_error("grid: system %d of %d", sys, c->nsys);
@@ -1171,6 +1171,7 @@ int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit) {
   if (nc)
     for (int d = 0; d < 3; d++) nc[d] = c->h_sp[sys].nc[d];
   if (nsplit) *nsplit = c->cw_ok ? c->cw_nsplit : 1;
+  if (block_threads) *block_threads = c->cw_ok ? c->cw_nt : 0;
   return CM3D_NB_OK;
 }
 
@@ -1188,7 +1189,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   if (reps < 1) reps = 5;
   const int cand[4] = {4, 8, 16, 32};
   double best = 1e300;
-  int best_tpa = c->tpa, best_win = 0, best_cw = 0, best_split = c->cw_nsplit;
+  int best_tpa = c->tpa, best_win = 0, best_cw = 0, best_split = c->cw_nsplit, best_nt = c->cw_nt;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -1211,10 +1212,14 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
     // atom are those of the gather kernel that runs the other systems, and
     // the items are whole cells.
     for (int k = 0; k < 4; k++)
-      for (int sp = 1; sp <= (kind == 2 && !c->cw_batch ? CW_MAX_SPLIT : 1); sp *= 2) {
+      for (int sp = 1; sp <= (kind == 2 && !c->cw_batch ? CW_MAX_SPLIT : 1); sp *= 2)
+      for (int nt = 512; nt <= (kind == 2 ? 640 : 512); nt += 128) {
         if (kind == 2 && cand[k] != 32 && !c->cw_batch) continue;
         c->tpa = cand[k];
-        if (kind == 2) cw_set_split(c, sp);
+        if (kind == 2) {
+          cw_set_split(c, sp);
+          c->cw_nt = nt;
+        }
         if ((rc = pair_forces(c, 1, 3))) return rc;   // warm-up (first launch sets attributes)
         CK(cudaEventRecord(a, c->st));
         for (int r = 0; r < reps; r++)
@@ -1230,7 +1235,10 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
           best_tpa = cand[k];
           best_win = kind == 1;
           best_cw = kind == 2;
-          if (kind == 2) best_split = sp;
+          if (kind == 2) {
+            best_split = sp;
+            best_nt = nt;
+          }
         }
       }
   }
@@ -1240,7 +1248,10 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   c->tpa = best_tpa;
   c->win_ok = best_win;
   c->cw_use = best_cw;
-  if (c->cw_ok) cw_set_split(c, best_split);
+  if (c->cw_ok) {
+    cw_set_split(c, best_split);
+    c->cw_nt = best_nt;
+  }
   if (tpa_chosen) *tpa_chosen = best_tpa;
   // a captured step holds the old launch configuration; the timing launches
   // added to the force blocks and accumulators: recompute force(1)

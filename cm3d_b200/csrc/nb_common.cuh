@@ -253,6 +253,7 @@ struct Ctx {
   float4 *cw_tl = nullptr;             // LJ, 2 float4 per knot
   float cw_lj1[4] = {0, 0, 0, 0};      // the one LJ interaction: rc^2, dx2tab, offset, vt
   int cw_nsplit = 1, cw_nitems = 0;    // work items: cells x parts
+  int cw_nt = 512;                     // threads per pair-kernel block (512 or 640; autotuner)
   double *cw_part = nullptr;           // per-item FP64 energy/virial sums
   // a batch: the systems with >= 3 cells per axis in the compact kernel (in
   // groups of systems with the same tables), the others in the gather kernel

@@ -49,7 +49,8 @@
 
 namespace cm3d {
 
-constexpr int CW_THREADS = 512;
+constexpr int CW_THREADS = 512;            // threads of a pair-kernel block (or CW_THREADS_WIDE)
+constexpr int CW_THREADS_WIDE = 640;       // 20 warps at 96 registers: the autotuner picks either
 constexpr int CW_ROW = 32;                  // interleave width (entries per pass of a block)
 constexpr int CW_BLOCK = 4 * CW_ROW;        // entries per block: one 8-byte word per lane
 constexpr uint32_t CW_IDX = 0x3FFFu;        // window index bits of an entry
@@ -379,8 +380,8 @@ __device__ __forceinline__ void cw_lj(const CwP &P, float dx, float dy, float dz
 // serve them all -- given as {system, cell of the system, part, parts};
 // each item's cell grid and shifts come from its system's SysP, and its
 // partial sums go to item0 + item.
-template <bool HAS_EL, int LJM, bool BATCH = false>
-__global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
+template <bool HAS_EL, int LJM, bool BATCH = false, int NT = CW_THREADS>
+__global__ void __launch_bounds__(NT, 1) k_pair_cw(
     CwP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ cell_start, const int2 *__restrict__ cwn, const uint2 *__restrict__ cwl,
     const float4 *__restrict__ gshift, const int *__restrict__ gmap, const float *__restrict__ gfcut,
@@ -401,7 +402,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
   __shared__ float4 s_shift[54];
   __shared__ int s_map[256];
   __shared__ float4 s_cut[64];                                        // LJM 2: {rc2, dx2, off, vt}
-  __shared__ double s_red[CW_THREADS / 32][CQ_COUNT];
+  __shared__ double s_red[NT / 32][CQ_COUNT];
   __shared__ __align__(8) unsigned long long s_mbar;
   static_assert(CQ_COUNT == 16, "the transposing reduction gives lane pair q quantity q of 16");
 
@@ -432,7 +433,7 @@ __global__ void __launch_bounds__(CW_THREADS, 1) k_pair_cw(
     mbar_init(bar);
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  constexpr int NWARP = CW_THREADS / 32;
+  constexpr int NWARP = NT / 32;
   // this lane's table copies and the window as 32-bit shared addresses
   const unsigned tfb = (unsigned)__cvta_generic_to_shared(tf + (lane & (CW_RF - 1))) -
                        CW_MAGIC_BITS * (unsigned)(CW_RF * sizeof(float4));
@@ -1170,19 +1171,26 @@ int cw_convert(Ctx *c, bool device_flag, bool all) {
   return CM3D_NB_OK;
 }
 
-template <bool EL, int LJM, bool BATCH>
-static void cw_launch_t(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
-                        const float4 *tl, const int4 *items, int item0) {
-  auto kern = k_pair_cw<EL, LJM, BATCH>;
+template <bool EL, int LJM, bool BATCH, int NT>
+static void cw_launch_nt(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
+                         const float4 *tl, const int4 *items, int item0) {
+  auto kern = k_pair_cw<EL, LJM, BATCH, NT>;
   static unsigned long long attr_devs = 0;
   if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(c->smem_optin - CW_STATIC_SMEM));
     attr_devs |= 1ull << c->dev;
   }
   const int grid = std::min(P.nitems, c->num_sms);
-  kern<<<grid, CW_THREADS, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl, c->shift,
+  kern<<<grid, NT, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl, c->shift,
                                           c->map, c->fcut, tf, tg, tl, fout, c->cw_part, c->stat, c->gate, items,
                                           c->sp, item0);
+}
+
+template <bool EL, int LJM, bool BATCH>
+static void cw_launch_t(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
+                        const float4 *tl, const int4 *items, int item0) {
+  if (c->cw_nt == CW_THREADS_WIDE) cw_launch_nt<EL, LJM, BATCH, CW_THREADS_WIDE>(c, P, smem, fout, tf, tg, tl, items, item0);
+  else cw_launch_nt<EL, LJM, BATCH, CW_THREADS>(c, P, smem, fout, tf, tg, tl, items, item0);
 }
 
 template <bool BATCH>

@@ -68,7 +68,7 @@ def load_library() -> C.CDLL:
         "cm3d_nb_get_nhc": (C.c_int, [vp, C.c_int, dp, dp, ip, ip]),
         "cm3d_nb_set_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_box": (C.c_int, [vp, dp]),
-        "cm3d_nb_grid": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), ip]),
+        "cm3d_nb_grid": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), ip, ip]),
         "cm3d_nb_get_positions": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_set_velocities": (C.c_int, [vp, dp, dp, dp]),
         "cm3d_nb_get_velocities": (C.c_int, [vp, dp, dp, dp]),
@@ -280,16 +280,17 @@ class Engine:
         t = C.c_int(0)
         ms = np.zeros(4)
         check(load_library().cm3d_nb_autotune(self._h, reps, C.byref(t), _p(ms)), "autotune")
-        nc, split = self.grid(0)
+        nc, split, nt = self.grid(0)
         return {"tpa": int(t.value), "kernel": self.pair_kernel()[0], "cells": nc, "compact_split": split,
-                "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
+                "compact_block_threads": nt, "ms_per_launch": {4: ms[0], 8: ms[1], 16: ms[2], 32: ms[3]}}
 
-    def grid(self, sys: int = 0) -> tuple[list, int]:
-        """(cells per box direction of system `sys`, parts per cell of the compact kernel's work items)"""
+    def grid(self, sys: int = 0) -> tuple[list, int, int]:
+        """(cells per box direction of system `sys`, parts per cell of the compact kernel's work items,
+        threads of its blocks (0 without the compact path))"""
         nc = (C.c_int * 3)()
-        sp = C.c_int(0)
-        check(load_library().cm3d_nb_grid(self._h, sys, nc, C.byref(sp)), "grid")
-        return [int(x) for x in nc], int(sp.value)
+        sp, nt = C.c_int(0), C.c_int(0)
+        check(load_library().cm3d_nb_grid(self._h, sys, nc, C.byref(sp), C.byref(nt)), "grid")
+        return [int(x) for x in nc], int(sp.value), int(nt.value)
 
     def pair_kernel(self) -> tuple[str, int]:
         """(kernel of the last pair launch: "gather", "window", "system" or "compact", lanes per atom)"""
@@ -432,7 +433,8 @@ def tune_cell_scale(systems, device: int = 0, scales=(1.0, 1.25), steps: int = 2
             e.step_wait()
             b.synchronize()
             out[s] = {"ms_per_step": a.elapsed_time(b) / steps, "kernel": tune["kernel"], "tpa": tune["tpa"],
-                      "cells": tune["cells"], "compact_split": tune["compact_split"]}
+                      "cells": tune["cells"], "compact_split": tune["compact_split"],
+                      "compact_block_threads": tune["compact_block_threads"]}
     best = min(out, key=lambda k: out[k]["ms_per_step"])
     return {"cell_scale": best, "candidates": out}
 

@@ -373,8 +373,8 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
 int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
 /* the cell grid of system `sys` (cells per box direction) and, for the
    compact path, the parts each cell's atoms are split into (work items per
-   cell; 1 elsewhere) */
-int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit);
+   cell; 1 elsewhere) and the threads of its blocks (0 without it) */
+int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit, int *block_threads);
 
 /* ------------------------------------------- no-allocation variant */
 #define CM3D_NB_NOALLOC_MAX_CHARGES 32768   /* charged atoms per call */
