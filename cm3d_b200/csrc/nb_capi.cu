@@ -13,6 +13,11 @@ namespace cm3d {
 
 static thread_local char g_err[1024] = "";
 
+std::recursive_mutex &device_mutex() {
+  static std::recursive_mutex mu;
+  return mu;
+}
+
 void set_error(const char *fmt, ...) {
   va_list ap;
   va_start(ap, fmt);
@@ -585,6 +590,7 @@ int cm3d_nb_create(const cm3d_nb_system *sys, const cm3d_nb_options *opt, cm3d_n
 }
 
 int cm3d_nb_create_batch(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options *opt, cm3d_nb_ctx **out) {
+  DevLock lock(device_mutex());
   Ctx *c = nullptr;
   int rc = create(systems, nsys, opt, &c);
   if (rc) {
@@ -596,7 +602,10 @@ int cm3d_nb_create_batch(const cm3d_nb_system *systems, int nsys, const cm3d_nb_
   return CM3D_NB_OK;
 }
 
-void cm3d_nb_destroy(cm3d_nb_ctx *ctx) { destroy(reinterpret_cast<Ctx *>(ctx)); }
+void cm3d_nb_destroy(cm3d_nb_ctx *ctx) {
+  DevLock lock(device_mutex());
+  destroy(reinterpret_cast<Ctx *>(ctx));
+}
 
 // every entry point first finishes asynchronously launched steps
 #define CTX                                         \
@@ -643,6 +652,7 @@ int cm3d_nb_set_positions(cm3d_nb_ctx *ctx, const double *px, const double *py, 
 // a list radius wide.
 int cm3d_nb_set_box(cm3d_nb_ctx *ctx, const double hmat[9]) {
   CTX;
+  DevLock lock(device_mutex());
   if (c->nsys != 1) {
     set_error("set_box: a batch of %d systems (one system only)", c->nsys);
     return CM3D_NB_ERR_ARG;
@@ -1177,6 +1187,7 @@ int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit, int *block_t
 
 int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_launch[4]) {
   CTX;
+  DevLock lock(device_mutex());
   int rc;
   if (c->mode != CM3D_NB_MIXED) {
     set_error("autotune: the plain FP64 engine has nothing to tune");
@@ -1205,6 +1216,13 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
     if (kind == 1 && c->win_env_off) continue;
     if (kind == 2 && !c->cw_ok) continue;
     c->win_ok = kind == 1;
+    if (kind == 2 && !c->cw_use) {
+      // the compact lists are kept only while the compact path is in use:
+      // convert every system's master list first
+      c->cw_use = 1;
+      if ((rc = cw_convert(c, false, true))) return rc;
+      if (!c->cw_ok) continue;                       // a window did not fit
+    }
     c->cw_use = kind == 2;
     // the compact kernel runs a warp per atom; its tile is the number of
     // parts each cell's atoms are split into (work items per cell, each

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -486,6 +487,12 @@ int plain_ecorr(Ctx *c, const int2 *ij);        // nb_plain.cu
 int mixed_pairs(Ctx *c, int iflg, int mask);    // nb_pair.cu
 bool win_applies(Ctx *c);                       // nb_pair.cu: windowed pair kernel possible
 int build_lists(Ctx *c, bool device_flag, bool all);   // nb_list.cu
+// Held across every CUDA call that can synchronize the whole device (context
+// creation and destruction, allocation and freeing at run time) and across
+// every graph capture: a device-wide synchronization from one host thread
+// while another captures a step graph would invalidate that capture.
+std::recursive_mutex &device_mutex();           // nb_capi.cu
+using DevLock = std::lock_guard<std::recursive_mutex>;
 int list_setup(Ctx *c);                         // nb_list.cu
 void cell_shifts(SysP &P, const SysH &H);       // nb_list.cu
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused

@@ -1134,10 +1134,13 @@ void cw_set_split(Ctx *c, int nsplit) {
 // after a (gated) rebuild of the master list: the compact list (a batch:
 // of the compact systems being rebuilt, or of all after the slots widened)
 int cw_convert(Ctx *c, bool device_flag, bool all) {
-  if (!c->cw_ok) return CM3D_NB_OK;
+  // (a context whose autotuner chose another kernel keeps no compact lists;
+  // the autotuner converts them all before it times the compact path)
+  if (!c->cw_ok || !c->cw_use) return CM3D_NB_OK;
   // the master slots widen on overflow (host-driven builds only): so do ours
   const int words = cw_words_for(c->nbr_stride);
   if (words > c->cw_words) {
+    DevLock lock(device_mutex());
     CK(cudaStreamSynchronize(c->st));
     cudaFree(c->cwl);
     c->cwl = nullptr;

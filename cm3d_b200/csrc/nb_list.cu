@@ -1014,6 +1014,7 @@ __global__ void k_regrow_copy(int n, int old_s, int new_s, const int *__restrict
 // grow list buffers to hold at least `need` entries (with 50% headroom)
 static int grow(Ctx *c, int which, long long need) {
   if (need <= c->lcap[which]) return CM3D_NB_OK;
+  DevLock lock(device_mutex());
   long long cap = need + need / 2 + 4096;
   if (c->graph) {
     // a captured step holds the old buffer addresses
@@ -1030,6 +1031,7 @@ static int grow(Ctx *c, int which, long long need) {
 
 // widen the full-list slots to hold `need` entries (+1/8 and 32 spare)
 static int grow_full(Ctx *c, long long need) {
+  DevLock lock(device_mutex());
   long long s = (need + need / 8 + 32 + 31) / 32 * 32;
   if (s <= c->nbr_stride) s = c->nbr_stride + 32;
   if (c->graph) {

@@ -1513,6 +1513,7 @@ int launch_steps(Ctx *c, int istep0, int nsteps) {
   // graph replay: one captured step, every kernel gated on the device state
   // (rebuild flag; halt after a list overflow)
   if (!c->graph) {
+    DevLock lock(device_mutex());
     cudaGraph_t g;
     long long l0 = c->launches;
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
