@@ -71,6 +71,17 @@ __global__ void k_kprep(int nq, const int *__restrict__ icharge, int n, const do
   if (kposd) kposd[jq] = make_double4(x, y, z, tq);
 }
 
+// One step of the phase recursion along kc for two atoms at once, in packed
+// FP32 (sm_100's two-wide FMA and multiply): per element the same roundings
+// as the scalar c' = fma(c, cs, -(s sn)), s' = fma(s, cs, c sn), so a
+// system's phases do not depend on which form ran (nsn = -sn, exact).
+__device__ __forceinline__ void rot2(float2 &c, float2 &s, float2 cs, float2 sn, float2 nsn) {
+  const float2 cn = __ffma2_rn(c, cs, __fmul2_rn(s, nsn));
+  const float2 snn = __ffma2_rn(s, cs, __fmul2_rn(c, sn));
+  c = cn;
+  s = snn;
+}
+
 __device__ __forceinline__ float phase_rad(unsigned phi) {
   // (int)phi / 2^32 of a turn, in [-pi, pi)
   return (float)(int)phi * 1.4629180792671596e-09f;   // 2 pi / 2^32
@@ -117,6 +128,17 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
       tq[m] = 0.f; cs[m] = 1.f; sn[m] = 0.f;
     }
   }
+  // atoms in pairs for the packed phase recursion (A even)
+  constexpr int H = A / 2 > 0 ? A / 2 : 1;
+  float2 cs2[H], sn2[H], nsn2[H];
+  if constexpr (A % 2 == 0) {
+#pragma unroll
+    for (int j = 0; j < A / 2; j++) {
+      cs2[j] = make_float2(cs[2 * j], cs[2 * j + 1]);
+      sn2[j] = make_float2(sn[2 * j], sn[2 * j + 1]);
+      nsn2[j] = make_float2(-sn[2 * j], -sn[2 * j + 1]);
+    }
+  }
   for (int r = r0; r < r1; r++) {
     const int4 row = rows[r];
     const int len = row.w;
@@ -126,19 +148,39 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
       unsigned phi = (unsigned)row.x * u0[m] + (unsigned)row.y * u1[m] + (unsigned)row.z * u2[m];
       __sincosf(phase_rad(phi), &s[m], &c[m]);
     }
+    float2 c2[H], s2[H];
+    if constexpr (A % 2 == 0) {
+#pragma unroll
+      for (int j = 0; j < A / 2; j++) {
+        c2[j] = make_float2(c[2 * j], c[2 * j + 1]);
+        s2[j] = make_float2(s[2 * j], s[2 * j + 1]);
+      }
+    }
     for (int kk = 0; kk < len; kk++) {
       float sr = 0.f, si = 0.f;
+      if constexpr (A % 2 == 0) {
+        // the sums in atom order as below; the recursion two atoms at a time
 #pragma unroll
-      for (int m = 0; m < A; m++) {
-        sr = fmaf(tq[m], c[m], sr);
-        si = fmaf(tq[m], s[m], si);
-        // explicit roundings: every instantiation (tile shape) rotates
-        // the phase with the same operations, so a system's sums do not
-        // depend on the tiling the compiler saw
-        float cn = fmaf(c[m], cs[m], -__fmul_rn(s[m], sn[m]));
-        float snn = fmaf(s[m], cs[m], __fmul_rn(c[m], sn[m]));
-        c[m] = cn;
-        s[m] = snn;
+        for (int j = 0; j < A / 2; j++) {
+          sr = fmaf(tq[2 * j], c2[j].x, sr);
+          si = fmaf(tq[2 * j], s2[j].x, si);
+          sr = fmaf(tq[2 * j + 1], c2[j].y, sr);
+          si = fmaf(tq[2 * j + 1], s2[j].y, si);
+          rot2(c2[j], s2[j], cs2[j], sn2[j], nsn2[j]);
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < A; m++) {
+          sr = fmaf(tq[m], c[m], sr);
+          si = fmaf(tq[m], s[m], si);
+          // explicit roundings: every instantiation (tile shape) rotates
+          // the phase with the same operations, so a system's sums do not
+          // depend on the tiling the compiler saw
+          float cn = fmaf(c[m], cs[m], -__fmul_rn(s[m], sn[m]));
+          float snn = fmaf(s[m], cs[m], __fmul_rn(c[m], sn[m]));
+          c[m] = cn;
+          s[m] = snn;
+        }
       }
       sr = warp_sum(sr);
       si = warp_sum(si);
@@ -283,6 +325,16 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
       tq[m] = 0.f; cs[m] = 1.f; sn[m] = 0.f;
     }
   }
+  constexpr int H = A / 2 > 0 ? A / 2 : 1;
+  float2 cs2[H], sn2[H], nsn2[H];
+  if constexpr (A % 2 == 0) {
+#pragma unroll
+    for (int j = 0; j < A / 2; j++) {
+      cs2[j] = make_float2(cs[2 * j], cs[2 * j + 1]);
+      sn2[j] = make_float2(sn[2 * j], sn[2 * j + 1]);
+      nsn2[j] = make_float2(-sn[2 * j], -sn[2 * j + 1]);
+    }
+  }
   for (int r = r0; r < r1; r++) {
     const int4 row = rows[r];
     const int len = row.w;
@@ -295,22 +347,56 @@ __global__ void __launch_bounds__(KS_THREADS) k_kforce_mixed(int nq, const uint4
       W0[m] = W1[m] = 0.f;
     }
     float kcf = (float)row.z;
-    for (int kk = 0; kk < len; kk++) {
-      const float2 a = ak_s[kb0 + kk];
+    if constexpr (A % 2 == 0) {
+      // two atoms per packed operation; per element the roundings of the
+      // scalar form below (wv = fma(a.x, s, -(a.y c)), W0 += wv, W1 += kc wv)
+      float2 c2[A / 2], s2[A / 2], w02[A / 2], w12[A / 2];
 #pragma unroll
-      for (int m = 0; m < A; m++) {
-        float wv = fmaf(a.x, s[m], -__fmul_rn(a.y, c[m]));
-        W0[m] = __fadd_rn(W0[m], wv);
-        W1[m] = fmaf(kcf, wv, W1[m]);
-        // explicit roundings: every instantiation (tile shape) rotates
-        // the phase with the same operations, so a system's sums do not
-        // depend on the tiling the compiler saw
-        float cn = fmaf(c[m], cs[m], -__fmul_rn(s[m], sn[m]));
-        float snn = fmaf(s[m], cs[m], __fmul_rn(c[m], sn[m]));
-        c[m] = cn;
-        s[m] = snn;
+      for (int j = 0; j < A / 2; j++) {
+        c2[j] = make_float2(c[2 * j], c[2 * j + 1]);
+        s2[j] = make_float2(s[2 * j], s[2 * j + 1]);
+        w02[j] = make_float2(0.f, 0.f);
+        w12[j] = make_float2(0.f, 0.f);
       }
-      kcf += 1.f;
+      float2 kc2 = make_float2(kcf, kcf);
+      const float2 one2 = make_float2(1.f, 1.f);
+      for (int kk = 0; kk < len; kk++) {
+        const float2 a = ak_s[kb0 + kk];
+        const float2 ax2 = make_float2(a.x, a.x), nay2 = make_float2(-a.y, -a.y);
+#pragma unroll
+        for (int j = 0; j < A / 2; j++) {
+          const float2 wv = __ffma2_rn(ax2, s2[j], __fmul2_rn(nay2, c2[j]));
+          w02[j] = __fadd2_rn(w02[j], wv);
+          w12[j] = __ffma2_rn(kc2, wv, w12[j]);
+          rot2(c2[j], s2[j], cs2[j], sn2[j], nsn2[j]);
+        }
+        kc2 = __fadd2_rn(kc2, one2);
+      }
+#pragma unroll
+      for (int j = 0; j < A / 2; j++) {
+        W0[2 * j] = w02[j].x;
+        W0[2 * j + 1] = w02[j].y;
+        W1[2 * j] = w12[j].x;
+        W1[2 * j + 1] = w12[j].y;
+      }
+    } else {
+      for (int kk = 0; kk < len; kk++) {
+        const float2 a = ak_s[kb0 + kk];
+#pragma unroll
+        for (int m = 0; m < A; m++) {
+          float wv = fmaf(a.x, s[m], -__fmul_rn(a.y, c[m]));
+          W0[m] = __fadd_rn(W0[m], wv);
+          W1[m] = fmaf(kcf, wv, W1[m]);
+          // explicit roundings: every instantiation (tile shape) rotates
+          // the phase with the same operations, so a system's sums do not
+          // depend on the tiling the compiler saw
+          float cn = fmaf(c[m], cs[m], -__fmul_rn(s[m], sn[m]));
+          float snn = fmaf(s[m], cs[m], __fmul_rn(c[m], sn[m]));
+          c[m] = cn;
+          s[m] = snn;
+        }
+        kcf += 1.f;
+      }
     }
 #pragma unroll
     for (int m = 0; m < A; m++) {
