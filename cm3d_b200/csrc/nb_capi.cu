@@ -692,7 +692,7 @@ int cm3d_nb_set_box(cm3d_nb_ctx *ctx, const double hmat[9]) {
     cudaGraphExecDestroy(c->graph);
     c->graph = nullptr;
   }
-  return CM3D_NB_OK;
+  return refresh_corners(c);
 }
 
 int cm3d_nb_get_positions(cm3d_nb_ctx *ctx, double *px, double *py, double *pz) {

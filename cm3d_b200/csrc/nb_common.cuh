@@ -495,6 +495,7 @@ std::recursive_mutex &device_mutex();           // nb_capi.cu
 using DevLock = std::lock_guard<std::recursive_mutex>;
 int list_setup(Ctx *c);                         // nb_list.cu
 void cell_shifts(SysP &P, const SysH &H);       // nb_list.cu
+int refresh_corners(Ctx *c);                    // nb_list.cu: cell corners under a new box
 int pair_forces(Ctx *c, int iflg, int which);   // nb_pair.cu: which 0 LJ, 1 elec, 2 fused
 int pair_setup(Ctx *c);                         // nb_pair.cu
 int cw_setup(Ctx *c);                           // nb_cwin.cu: compact-window path (after pair_setup)

@@ -848,6 +848,19 @@ __global__ void k_sorted_init(int n, const SysP *__restrict__ sp, const int *__r
   styp[t] = itype[i];
 }
 
+// The cell corners (and FP32 cell-relative positions) under a new box: every
+// atom keeps its cell and image, its corner moves with H (mixed mode; the
+// pair kernels' shifts, also H-derived, are updated beside this).
+int refresh_corners(Ctx *c) {
+  if (c->mode != CM3D_NB_MIXED || !c->lists_built) return CM3D_NB_OK;
+  k_sorted_init<<<grid_for(c->n, 256), 256, 0, c->st>>>(c->n, c->sp, c->sys_of, c->sreb, 1, c->cell_atoms,
+                                                        c->cimg, c->itype, c->pos, c->q, c->rank, c->styp,
+                                                        c->corner, c->xq, nullptr);
+  c->launches++;
+  CKL(c);
+  return CM3D_NB_OK;
+}
+
 // dxn = pos of the rebuilt systems (ngbr_list.c:577-580) and, per rebuilt
 // system, isteplast = istep (md_finter.c:98)
 __global__ void k_snapshot(int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of,
