@@ -368,7 +368,7 @@ def plain_arm(systems, device: int, steps: int, warmup: int, flush) -> dict:
 
 def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float, hbm: float, name: str,
               e2e_steps: int, dist=None, pin=None) -> dict:
-    """pin = (lanes per atom, "gather" | "staged"): skip the autotuner and use
+    """pin = (lanes per atom, "gather" | "staged" | "compact" | "compact8"): skip the autotuner and use
     that choice (a profiler run reproduces the choice the autotuner makes
     without the profiler, whose serialised timings would mislead it)."""
     import torch
@@ -376,6 +376,8 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
     from cm3d_b200.engine import Engine, tune_cell_scale
     if pin and pin[1] in ("gather", "staged"):
         os.environ["CM3D_NB_PAIR_KERNEL"] = "list" if pin[1] == "gather" else "window"
+    if pin and pin[1] == "compact8":
+        os.environ["CM3D_NB_CW_ROW"] = "8"
     # the cell size by measurement (fresh contexts per candidate, before the
     # measured one; every rank the same way)
     cells = None if pin else tune_cell_scale(systems, device=device)
@@ -383,6 +385,7 @@ def mixed_arm(systems, device: int, steps: int, warmup: int, flush, fp32: float,
                  cell_scale=cells["cell_scale"] if cells else 1.0)
     if pin:
         os.environ.pop("CM3D_NB_PAIR_KERNEL", None)
+        os.environ.pop("CM3D_NB_CW_ROW", None)
     eng.workload_name = name
     eng.step_init()
     tune = {"tpa": pin[0], "kernel": pin[1], "pinned": True} if pin else eng.autotune()
@@ -520,7 +523,7 @@ def main() -> None:
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--tpa", type=int, default=0, choices=[0, 4, 8, 16, 32],
                     help="pin the pair kernel's lanes per atom instead of autotuning (profiling runs)")
-    ap.add_argument("--pair-kernel", default="gather", choices=["gather", "staged", "compact"],
+    ap.add_argument("--pair-kernel", default="gather", choices=["gather", "staged", "compact", "compact8"],
                     help="with --tpa: the pair kernel to pin")
     ap.add_argument("--partition", action="store_true",
                     help="N > 1: split one ensemble over the ranks (LPT on the cost model, strong scaling) "

@@ -94,7 +94,7 @@ static void destroy(Ctx *c) {
                   c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan,
                   c->fxr, c->intra_buf, c->ithm, c->nhc, c->cwl, c->cwn, c->cw_tf, c->cw_tg, c->cw_tl,
                   c->cw_part, c->nvt_kin, c->nvt_chsum, c->th_atoms, c->th_choff, c->th_chunk,
-                  c->cw_sys, c->cw_sitems, c->cw_items, c->cw_gidx};
+                  c->cw_sys, c->cw_sitems, c->cw_items, c->cw_gidx, c->cw_scan};
   cw_destroy(c);
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -1181,7 +1181,8 @@ int cm3d_nb_grid(cm3d_nb_ctx *ctx, int sys, int nc[3], int *nsplit, int *block_t
   if (nc)
     for (int d = 0; d < 3; d++) nc[d] = c->h_sp[sys].nc[d];
   if (nsplit) *nsplit = c->cw_ok ? c->cw_nsplit : 1;
-  if (block_threads) *block_threads = c->cw_ok ? c->cw_nt : 0;
+  if (block_threads)
+    *block_threads = !c->cw_ok ? 0 : (c->cw_batch && c->cw_row == CM3D_CS_LPA ? CM3D_CS_THREADS : c->cw_nt);
   return CM3D_NB_OK;
 }
 
@@ -1201,6 +1202,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   const int cand[4] = {4, 8, 16, 32};
   double best = 1e300;
   int best_tpa = c->tpa, best_win = 0, best_cw = 0, best_split = c->cw_nsplit, best_nt = c->cw_nt;
+  int best_row = c->cw_row;
   cudaEvent_t a, b;
   CK(cudaEventCreate(&a));
   CK(cudaEventCreate(&b));
@@ -1210,20 +1212,32 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
     for (int k = 0; k < 4; k++) ms_per_launch[k] = 1e300;
   // kind 0: the gather kernel; 1: the staged kernel that applies (a single
   // system's 27-cell windows, or a batch's whole systems); 2: the compact
-  // window list (one system, nb_cwin.cu) -- the context runs whichever is
+  // window list (nb_cwin.cu), 32 lanes per atom; 3: a batch's compact list
+  // with 8 lanes per atom (k_pair_cs) -- the context runs whichever is
   // fastest on its live lists
-  for (int kind = 0; kind <= 2; kind++) {
+  for (int kind = 0; kind <= 3; kind++) {
     if (kind == 1 && c->win_env_off) continue;
-    if (kind == 2 && !c->cw_ok) continue;
+    if (kind >= 2 && !c->cw_ok) continue;
+    if (kind == 3 && (!c->cw_batch || c->cw_cap8 == 0)) continue;
     c->win_ok = kind == 1;
-    if (kind == 2 && !c->cw_use) {
-      // the compact lists are kept only while the compact path is in use:
-      // convert every system's master list first
-      c->cw_use = 1;
-      if ((rc = cw_convert(c, false, true))) return rc;
+    if (kind >= 2) {
+      const int row = kind == 3 ? CM3D_CS_LPA : CM3D_CW_ROW;
+      if (!c->cw_use) {
+        // the compact lists are kept only while the compact path is in use:
+        // convert every system's master list first
+        c->cw_use = 1;
+        if (c->cw_batch) {
+          c->cw_row = row;
+          c->cw_cap = row == CM3D_CS_LPA ? c->cw_cap8 : c->cw_cap32;
+        }
+        if ((rc = cw_convert(c, false, true))) return rc;
+      } else if ((rc = cw_set_row(c, row))) {
+        return rc;
+      }
       if (!c->cw_ok) continue;                       // a window did not fit
+      if (c->cw_batch && c->cw_row != row) continue;  // nor the 8-lane kernel's window
     }
-    c->cw_use = kind == 2;
+    c->cw_use = kind >= 2;
     // the compact kernel runs a warp per atom; its tile is the number of
     // parts each cell's atoms are split into (work items per cell, each
     // staging the cell's window): 1, 2, 4, 8.  In a batch the lanes per
@@ -1252,10 +1266,11 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
           best = per;
           best_tpa = cand[k];
           best_win = kind == 1;
-          best_cw = kind == 2;
-          if (kind == 2) {
+          best_cw = kind >= 2;
+          if (kind >= 2) {
             best_split = sp;
             best_nt = nt;
+            best_row = kind == 3 ? CM3D_CS_LPA : CM3D_CW_ROW;
           }
         }
       }
@@ -1269,6 +1284,7 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
   if (c->cw_ok) {
     cw_set_split(c, best_split);
     c->cw_nt = best_nt;
+    if (best_cw && (rc = cw_set_row(c, best_row))) return rc;
   }
   if (tpa_chosen) *tpa_chosen = best_tpa;
   // a captured step holds the old launch configuration; the timing launches

@@ -244,7 +244,9 @@ struct Ctx {
   // compact-window pair path (nb_cwin.cu): one system, >= 3 cells per axis
   int cw_ok = 0;                       // set up and valid for this context
   int cw_use = 0;                      // preferred over the window/gather kernels (autotuner)
-  int cw_cap = 0;                      // window slots
+  int cw_cap = 0;                      // window slots (of the kernel in use)
+  int cw_row = 32;                     // compact-list lanes per atom: 32 (k_pair_cw) or 8 (k_pair_cs)
+  int cw_cap32 = 0, cw_cap8 = 0;       // window slots of each kernel (k_pair_cs: per block group)
   size_t cw_smem = 0;                  // dynamic shared memory of k_pair_cw
   int cw_words = 0;                    // 8-byte words per atom slot of the compact list
   uint2 *cwl = nullptr;                // compact list (16-bit window indices, lane-interleaved blocks)
@@ -263,6 +265,7 @@ struct Ctx {
   int2 *cw_sitems = nullptr;           // per system: its items {first, count} (device)
   int4 *cw_items = nullptr;            // {system, cell of the system, part, parts}, by group (device)
   int *cw_gidx = nullptr;              // sorted atoms of the gather-kernel systems (device)
+  int *cw_scan = nullptr;              // atoms to convert before each system (nsys + 1, device)
   int cw_ng = 0;
   void *cw_grp = nullptr;              // the groups (host, nb_cwin.cu)
   const int *pair_gidx = nullptr;      // a gather launch over these sorted atoms only
@@ -501,6 +504,10 @@ int pair_setup(Ctx *c);                         // nb_pair.cu
 int cw_setup(Ctx *c);                           // nb_cwin.cu: compact-window path (after pair_setup)
 constexpr int CW_MAX_SPLIT = 8;                 // most parts a cell's atoms are split into
 void cw_set_split(Ctx *c, int nsplit);          // nb_cwin.cu
+constexpr int CM3D_CW_ROW = 32;                 // compact-list rows (lanes per atom) of k_pair_cw
+constexpr int CM3D_CS_LPA = 8;                  //   and of k_pair_cs
+constexpr int CM3D_CS_THREADS = 512;            // k_pair_cs block: four groups of four warps
+int cw_set_row(Ctx *c, int row);                // nb_cwin.cu: a batch's list layout, 32 or 8 lanes per atom
 int cw_convert(Ctx *c, bool device_flag, bool all);   // nb_cwin.cu: master list -> compact list
 void cw_destroy(Ctx *c);                        // nb_cwin.cu: host-side group data
 bool cw_applies(Ctx *c, int iflg, bool ns);     // nb_cwin.cu

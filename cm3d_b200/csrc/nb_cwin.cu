@@ -51,7 +51,7 @@ namespace cm3d {
 
 constexpr int CW_THREADS = 512;            // threads of a pair-kernel block (or CW_THREADS_WIDE)
 constexpr int CW_THREADS_WIDE = 640;       // 20 warps at 96 registers: the autotuner picks either
-constexpr int CW_ROW = 32;                  // interleave width (entries per pass of a block)
+constexpr int CW_ROW = CM3D_CW_ROW;         // interleave width (entries per pass of a block)
 constexpr int CW_BLOCK = 4 * CW_ROW;        // entries per block: one 8-byte word per lane
 constexpr uint32_t CW_IDX = 0x3FFFu;        // window index bits of an entry
 constexpr uint32_t CW_EL = 0x4000u;         // LJ-segment entry: the pair is also in CM3D's te list
@@ -78,41 +78,21 @@ struct CwP {
 };
 
 // ------------------------------------------------------------------
-// Master list -> compact list.  Warp per cell-sorted atom t: the 27-cell
+// Master list -> compact list.  Warp per cell-sorted atom t (one system:
+// every atom; a batch: the atoms of the compact systems being rebuilt): the 27-cell
 // window layout of t's cell (stencil cell w = shift code, j-cell = i-cell -
 // k_w, cells in code order) gives delta[w] = window offset - first sorted
 // index (lane w holds it), so entry (u, w) becomes window index u +
 // delta[w].  A window larger than `cap` cannot be indexed: the cell's atoms
 // get empty lists, ST_CWIN counts it (once per cell) and a captured step
 // halts (the host then turns the compact path off).
-__global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words,
-                                                    const int *__restrict__ cell_start,
-                                                    const int *__restrict__ cell_of,
-                                                    const int *__restrict__ sorig,
-                                                    const int *__restrict__ nlen, int stride,
-                                                    const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
-                                                    int2 *__restrict__ cwn, long long *__restrict__ stat,
-                                                    int *__restrict__ halt, const int *__restrict__ gs,
-                                                    const SysP *__restrict__ sp = nullptr,
-                                                    const int *__restrict__ sys_of = nullptr,
-                                                    const int *__restrict__ cwsys = nullptr,
-                                                    const int *__restrict__ sreb = nullptr, int all = 1) {
-  if (gated_off(gs, 1)) return;
-  const int lane = threadIdx.x & 31;
-  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (t >= n) return;                                  // whole warps
-  // a batch (cwsys set): only the atoms of compact systems that were just
-  // rebuilt, each on its own system's grid (a system's sorted indices span
-  // its own atom range, so sys_of[t] is t's system)
-  int c0 = 0;
-  if (cwsys) {
-    const int s = sys_of[t];
-    if (!cwsys[s] || (!all && sreb[s] == 0)) return;
-    ncx = sp[s].nc[0];
-    ncy = sp[s].nc[1];
-    ncz = sp[s].nc[2];
-    c0 = sp[s].c0;
-  }
+__device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int ncx, int ncy, int ncz, int c0,
+                                                int cap, int n, int words, int row,
+                                                const int *__restrict__ cell_start, const int *__restrict__ cell_of,
+                                                const int *__restrict__ sorig, const int *__restrict__ nlen,
+                                                int stride, const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
+                                                int2 *__restrict__ cwn, long long *__restrict__ stat,
+                                                int *__restrict__ halt) {
   const uint32_t dummy = (uint32_t)cap;
   const int c = cell_of[sorig[t]] - c0;
   int delta = 0, tot = 0;
@@ -148,15 +128,18 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
       const int na = fits ? nlen[t] : 0, nb = fits ? nlen[n + t] : 0;
       const uint32_t *src = nbr + (size_t)t * stride;
       uint2 *dst = cwl + (size_t)t * words;
-      const int nba = (na + CW_BLOCK - 1) / CW_BLOCK, nbb = (nb + CW_BLOCK - 1) / CW_BLOCK;
+      // blocks of 4 row entries: row 32 lanes per atom (k_pair_cw) or 8 (k_pair_cs)
+      const int blk = 4 * row;
+      const int nba = (na + blk - 1) / blk, nbb = (nb + blk - 1) / blk;
       // padding first: every slot of the atom's blocks holds the dummy
-      for (int b = 0; b < nba + nbb; b++) dst[b * CW_ROW + lane] = make_uint2(dummy | (dummy << 16), dummy | (dummy << 16));
+      for (int w = lane; w < (nba + nbb) * row; w += 32)
+        dst[w] = make_uint2(dummy | (dummy << 16), dummy | (dummy << 16));
       __syncwarp();
       for (int sg = 0; sg < 2; sg++) {
         const bool front = sg == 0;
         const int m = front ? na : nb;
         const uint32_t *in = front ? src : src + (stride - nb);   // the back segment ends at the slot's end
-        unsigned short *out = reinterpret_cast<unsigned short *>(dst + (front ? 0 : nba * CW_ROW));
+        unsigned short *out = reinterpret_cast<unsigned short *>(dst + (front ? 0 : nba * row));
         // every lane calls it (the delta comes by shuffle); -1 past the end
         auto window_index = [&](int e, uint32_t &o) -> int {
           const bool v = e < m;
@@ -172,9 +155,10 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
         };
         // bank classes: the window slot mod 8 (the 16-byte bank group of
         // the staged position).  Position j of the segment is read by lane
-        // j % 32, so putting a class-(j % 8) entry at j gives the 8 lanes of
-        // each quarter-warp 8 different bank groups; the entries that do
-        // not fit their own class's positions fill the rest in order.
+        // j % row (of the atom's lanes), so putting a class-(j % 8) entry at
+        // j gives the 8 lanes of each quarter-warp 8 different bank groups;
+        // the entries that do not fit their own class's positions fill the
+        // rest in order.
         int cnt[8];
 #pragma unroll
         for (int q = 0; q < 8; q++) cnt[q] = 0;
@@ -218,14 +202,99 @@ __global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, i
               }
               if (pos < 0) pos = 8 * Q + L;
             }
-            // position -> (block, row, lane): 16-bit entry k of word w
-            const int bb = pos / CW_BLOCK, r = pos - bb * CW_BLOCK;
-            out[(bb * CW_ROW + (r & (CW_ROW - 1))) * 4 + (r >> 5)] = (unsigned short)o;
+            // position -> (block, lane, k): 16-bit entry k of the block's
+            // word for lane r % row (row is 8 or 32: a power of two)
+            const int bb = pos / blk, r = pos - bb * blk;
+            out[(bb * row + (r & (row - 1))) * 4 + r / row] = (unsigned short)o;
           }
         }
       }
       if (lane == 0) cwn[t] = make_int2(na, nb);
     }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words, int row,
+                                                    const int *__restrict__ cell_start,
+                                                    const int *__restrict__ cell_of,
+                                                    const int *__restrict__ sorig,
+                                                    const int *__restrict__ nlen, int stride,
+                                                    const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
+                                                    int2 *__restrict__ cwn, long long *__restrict__ stat,
+                                                    int *__restrict__ halt, const int *__restrict__ gs) {
+  if (gated_off(gs, 1)) return;
+  const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (t >= n) return;                                  // whole warps
+  cw_convert_atom(t, threadIdx.x & 31, ncx, ncy, ncz, 0, cap, n, words, row, cell_start, cell_of, sorig, nlen,
+                  stride, nbr, cwl, cwn, stat, halt);
+}
+
+// The atoms to convert in a batch, as one index range: scan[s] is the
+// number of atoms of compact systems being rebuilt (all: every compact
+// system) before system s, scan[nsys] their total.  One block.
+__global__ void __launch_bounds__(1024) k_cw_scan(int nsys, const SysP *__restrict__ sp,
+                                                  const int *__restrict__ cwsys, const int *__restrict__ sreb,
+                                                  int all, int *__restrict__ scan, const int *__restrict__ gs) {
+  if (gated_off(gs, 1)) return;
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int base = 0; base < nsys; base += blockDim.x) {
+    const int sy = base + threadIdx.x;
+    const int v = sy < nsys && cwsys[sy] && (all || sreb[sy] != 0) ? sp[sy].n : 0;
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += u;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+      int x = lane < nw ? warp_tot[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += u;
+      }
+      warp_tot[lane] = x;
+    }
+    __syncthreads();
+    if (sy < nsys) scan[sy] = carry + (w > 0 ? warp_tot[w - 1] : 0) + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_tot[nw - 1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) scan[nsys] = carry;
+}
+
+// A batch: warps walk the scanned range (a fixed grid, so that a captured
+// step converts whatever the device-side rebuild flags select); atom v of the
+// range lies in the last system s with scan[s] <= v, each on its own grid.
+__global__ void __launch_bounds__(256) k_cw_convert_sys(int nsys, const int *__restrict__ scan,
+                                                        const SysP *__restrict__ sp, int cap, int n, int words,
+                                                        int row, const int *__restrict__ cell_start,
+                                                        const int *__restrict__ cell_of,
+                                                        const int *__restrict__ sorig,
+                                                        const int *__restrict__ nlen, int stride,
+                                                        const uint32_t *__restrict__ nbr, uint2 *__restrict__ cwl,
+                                                        int2 *__restrict__ cwn, long long *__restrict__ stat,
+                                                        int *__restrict__ halt, const int *__restrict__ gs) {
+  if (gated_off(gs, 1)) return;
+  const int total = scan[nsys];
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < total; v += nwarps) {
+    int sa = 0, sb = nsys;
+    while (sb - sa > 1) {
+      const int mid = (sa + sb) >> 1;
+      if (scan[mid] <= v) sa = mid;
+      else sb = mid;
+    }
+    const SysP &P = sp[sa];
+    cw_convert_atom(P.a0 + (v - scan[sa]), threadIdx.x & 31, P.nc[0], P.nc[1], P.nc[2], P.c0, cap, n, words, row,
+                    cell_start, cell_of, sorig, nlen, stride, nbr, cwl, cwn, stat, halt);
   }
 }
 
@@ -322,6 +391,7 @@ constexpr int CW_WAIT_LIMIT = 1 << 22;
 // addresses less MAGIC_BITS knots, so that the float bits of the split
 // coordinate address the knot directly (k * stride = bits * stride - MAGIC_BITS
 // * stride, mod 2^32).
+template <int RF = CW_RF, int RG = CW_RG>
 __device__ __forceinline__ void cw_elec(const CwP &P, float qj, float dx, float dy, float dz, float r2,
                                         unsigned tfb, unsigned tgb, CwAcc &A) {
   A.r2min = fminf(A.r2min, r2);
@@ -330,8 +400,8 @@ __device__ __forceinline__ void cw_elec(const CwP &P, float qj, float dx, float 
   const float kf = t - CW_MAGIC;
   const float fr = fmaf(ps, P.pmax, -kf);
   const unsigned kb = __float_as_uint(t);
-  const float4 c = lds_f4(tfb + kb * (unsigned)(CW_RF * sizeof(float4)));
-  const float2 d = lds_f2(tgb + kb * (unsigned)(CW_RG * sizeof(float2)));
+  const float4 c = lds_f4(tfb + kb * (unsigned)(RF * sizeof(float4)));
+  const float2 d = lds_f2(tgb + kb * (unsigned)(RG * sizeof(float2)));
   const float fe = qj * fmaf(fr, fmaf(fr, c.z, c.y), c.x);
   A.eel = fmaf(qj, fmaf(fr, fmaf(fr, d.y, d.x), c.w), A.eel);
   const float ux = fe * dx, uy = fe * dy, uz = fe * dz;
@@ -710,6 +780,341 @@ __global__ void __launch_bounds__(NT, 1) k_pair_cw(
   if (lane == 0 && under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), under);
 }
 
+// ------------------------------------------------------------------
+// Pair kernel for small cells (k_pair_cs): boxes whose cells hold a few
+// tens of atoms, as in a batch of small LJ boxes.  There a block per cell
+// spends most of its time staging the window and waiting for it, and a
+// warp per atom leaves most lanes idle on lists of ~70 entries.  Here
+//   * a block is NG groups of CS_WARPS warps, each group working through
+//     its own items (cells) with its own window, mbarrier and named
+//     barrier, so one group's staging overlaps the others' pairs;
+//   * an atom has CS_LPA = 8 lanes (four atoms per warp) and its compact
+//     list comes in blocks of 32 entries (k_cw_convert with row 8: the
+//     8-byte word of lane l of a block holds entries l, l + 8, l + 16,
+//     l + 24), so a list of n entries pads to a multiple of 32, not 128;
+//   * both segments go through one pair body (the segment is a per-lane
+//     condition here), and every entry of a block is evaluated: padding
+//     names the dummy slot, which contributes exact zeros.
+// The sums are the same as k_pair_cw's: FP32 per lane and pair chunk, FP64
+// across an atom's lanes (forces) and per lane, warp, group and item (the
+// 16 energy/virial quantities), all in a fixed order.
+constexpr int CS_LPA = CM3D_CS_LPA;         // lanes per atom (the list row)
+constexpr int CS_WARPS = 4;                 // warps per group
+constexpr int CS_GT = 32 * CS_WARPS;        // threads per group
+constexpr int CS_BLOCK = 4 * CS_LPA;        // list entries per block
+constexpr int CS_NG = 4;                    // groups per block
+static_assert(CS_NG * CS_GT == CM3D_CS_THREADS, "k_pair_cs block size");
+constexpr int CS_STATIC_SMEM = 12288;       // >= k_pair_cs's static shared arrays
+constexpr int CS_RF = 4;                    // erfc table copies (four groups' windows need the room)
+constexpr int CS_RG = 4;
+
+__device__ __forceinline__ void group_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(CS_GT) : "memory");
+}
+// group barrier that also returns whether `p` holds in every thread of it
+__device__ __forceinline__ bool group_and(int id, bool p) {
+  unsigned r;
+  asm volatile(
+      "{\n .reg .pred a, b;\n setp.ne.u32 a, %1, 0;\n bar.red.and.pred b, %2, %3, a;\n selp.u32 %0, 1, 0, b;\n}"
+      : "=r"(r)
+      : "r"((unsigned)p), "r"(id), "r"(CS_GT)
+      : "memory");
+  return r != 0;
+}
+
+template <bool HAS_EL, int LJM, bool BATCH, int NG = CS_NG>
+__global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
+    CwP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
+    const int *__restrict__ cell_start, const int2 *__restrict__ cwn, const uint2 *__restrict__ cwl,
+    const float4 *__restrict__ gshift, const int *__restrict__ gmap, const float *__restrict__ gfcut,
+    const float4 *__restrict__ gtf, const float2 *__restrict__ gtg, const float4 *__restrict__ gtl,
+    double *__restrict__ fout, double *__restrict__ ipart, long long *__restrict__ stat,
+    const int *__restrict__ gs, const int4 *__restrict__ items = nullptr, const SysP *__restrict__ sp = nullptr,
+    int item0 = 0) {
+  if (gated_off(gs, 0)) return;
+  extern __shared__ float4 sm[];
+  // tables (as k_pair_cw), then NG windows of cap + 1 slots, then (LJM 2)
+  // NG type arrays
+  float4 *tf = sm;
+  float2 *tg = reinterpret_cast<float2 *>(tf + (HAS_EL ? P.ntable * CS_RF : 0));
+  float4 *tl = reinterpret_cast<float4 *>(tg + (HAS_EL ? P.ntable * CS_RG : 0));
+  const int nl = LJM ? 2 * P.ninter * P.ntable : 0;
+  const int g = threadIdx.x / CS_GT, gt = threadIdx.x % CS_GT, gw = gt >> 5;
+  const int lane = threadIdx.x & 31, l8 = lane & (CS_LPA - 1), sub = lane / CS_LPA;
+  const int bar_id = 1 + g;
+  float4 *wx = tl + nl + (size_t)g * (P.cap + 1);
+  unsigned char *wt = reinterpret_cast<unsigned char *>(tl + nl + (size_t)NG * (P.cap + 1)) + (size_t)g * (P.cap + 1);
+  __shared__ int s_cs[NG][27], s_off[NG][28];
+  __shared__ float4 s_shift[BATCH ? NG : 1][54];
+  __shared__ int s_map[256];
+  __shared__ float4 s_cut[64];
+  __shared__ double s_red[NG][CS_WARPS][CQ_COUNT];
+  __shared__ __align__(8) unsigned long long s_mbar[NG];
+  static_assert(CQ_COUNT == 2 * CS_LPA, "the transposing reduction gives lane l quantities 2l and 2l + 1");
+
+  if (!BATCH)
+    for (int k = threadIdx.x; k < 54; k += blockDim.x) s_shift[0][k] = gshift[k];
+  if (HAS_EL) {
+    for (int k = threadIdx.x; k < P.ntable * CS_RF; k += blockDim.x) tf[k] = gtf[k / CS_RF];
+    for (int k = threadIdx.x; k < P.ntable * CS_RG; k += blockDim.x) tg[k] = gtg[k / CS_RG];
+  }
+  for (int k = threadIdx.x; k < nl; k += blockDim.x) tl[k] = gtl[k];
+  if (LJM == 2) {
+    for (int k = threadIdx.x; k < P.ntypes * P.ntypes; k += blockDim.x) {
+      const int in = gmap[P.map0 + k];
+      s_map[k] = in >= 0 ? in - P.inter0 : -1;
+    }
+    for (int k = threadIdx.x; k < P.ninter; k += blockDim.x) {
+      const float *f = gfcut + 8 * (P.inter0 + k);
+      s_cut[k] = make_float4(f[0], f[2], f[1], f[3]);
+    }
+  }
+  const unsigned bar = (unsigned)__cvta_generic_to_shared(&s_mbar[g]);
+  unsigned phase = 0;
+  if (gt == 0) {
+    wx[P.cap] = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);   // the dummy entry's partner: out of range
+    if (LJM == 2) wt[P.cap] = 0;
+    mbar_init(bar);
+  }
+  __syncthreads();
+  const unsigned tfb = (unsigned)__cvta_generic_to_shared(tf + (lane & (CS_RF - 1))) -
+                       CW_MAGIC_BITS * (unsigned)(CS_RF * sizeof(float4));
+  const unsigned tgb = (unsigned)__cvta_generic_to_shared(tg + (lane & (CS_RG - 1))) -
+                       CW_MAGIC_BITS * (unsigned)(CS_RG * sizeof(float2));
+  const unsigned wxb = (unsigned)__cvta_generic_to_shared(wx);
+  const float4 *shift = s_shift[BATCH ? g : 0];
+  unsigned long long under = 0;
+
+  for (int item = blockIdx.x * NG + g; item < P.nitems; item += gridDim.x * NG) {
+    int c, ncx = P.ncx, ncy = P.ncy, ncz = P.ncz, c0 = 0, sys = 0;
+    if (BATCH) {
+      const int4 it = items[item];
+      sys = it.x;
+      c = it.y;
+      ncx = sp[sys].nc[0];
+      ncy = sp[sys].nc[1];
+      ncz = sp[sys].nc[2];
+      c0 = sp[sys].c0;
+    } else {
+      c = item;
+    }
+    const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
+    group_sync(bar_id);                                    // the previous window is no longer read
+    if (BATCH)
+      for (int k = gt; k < 54; k += CS_GT)
+        s_shift[g][k] = k < 27 ? sp[sys].shift[k] : sp[sys].shift_lo[k - 27];
+    if (gw == 0) {
+      int cnt = 0, cs = 0;
+      if (lane < 27) {
+        int jx = cx - (lane / 9 - 1), jy = cy - ((lane / 3) % 3 - 1), jz = cz - (lane % 3 - 1);
+        jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
+        jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
+        jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
+        const int jc = c0 + (jx * ncy + jy) * ncz + jz;
+        cs = cell_start[jc];
+        cnt = cell_start[jc + 1] - cs;
+      }
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      if (lane < 27) {
+        s_cs[g][lane] = cs;
+        s_off[g][lane] = incl - cnt;
+      }
+      if (lane == 26) s_off[g][27] = incl;
+    }
+    group_sync(bar_id);
+    const int tot = s_off[g][27];
+    const bool staged = tot <= P.cap;
+    if (staged) {
+      if (gw == 0) {
+        fence_async_smem();
+        if (lane == 0) mbar_expect(bar, (unsigned)tot * (unsigned)sizeof(float4));
+        __syncwarp();
+        if (lane < 27) {
+          const int cnt = s_off[g][lane + 1] - s_off[g][lane];
+          if (cnt > 0)
+            bulk_g2s(wxb + (unsigned)s_off[g][lane] * (unsigned)sizeof(float4), xq + s_cs[g][lane],
+                     (unsigned)cnt * (unsigned)sizeof(float4), bar);
+        }
+      }
+      const bool arrived = mbar_wait(bar, phase, CW_WAIT_LIMIT);
+      phase ^= 1u;
+      if (!group_and(bar_id, arrived)) {
+        // the copies did not complete (never seen): count it, wait once
+        // more for copies still in flight, and leave the group's remaining
+        // items undone; the host reads the count in the status
+        if (gt == 0) atomicAdd((unsigned long long *)(stat + ST_STAGE_TIMEOUT), 1ull);
+        mbar_wait(bar, phase ^ 1u, CW_WAIT_LIMIT);
+        break;
+      }
+      for (int w = gw; w < 27; w += CS_WARPS) {
+        const float4 sh = shift[w], shl = shift[27 + w];
+        const int g0 = s_off[g][w], g1 = s_off[g][w + 1], u0 = s_cs[g][w] - g0;
+        for (int k = g0 + lane; k < g1; k += 32) {
+          const float4 x = wx[k];
+          wx[k] = make_float4((x.x - sh.x) - shl.x, (x.y - sh.y) - shl.y, (x.z - sh.z) - shl.z, x.w);
+          if (LJM == 2) wt[k] = (unsigned char)styp[u0 + k];
+        }
+      }
+    }
+    group_sync(bar_id);
+    // lane l8 of an atom keeps quantities 2 l8 and 2 l8 + 1 of CQ_* in FP64
+    double Eq0 = 0.0, Eq1 = 0.0, Ehi = 0.0;
+    const int ci0 = s_cs[g][13], cin = staged ? s_off[g][14] - s_off[g][13] : 0, ioff = s_off[g][13];
+    const uint32_t dm = (uint32_t)P.cap | ((uint32_t)P.cap << 16);
+    const uint2 pad = make_uint2(dm, dm);
+    // the group's 16 atom slots (warp gw, quarter sub) over the cell's atoms
+    for (int a0 = 0; a0 < cin; a0 += CS_WARPS * 4) {
+      const int a = a0 + gw * 4 + sub;
+      const bool act = a < cin;
+      const int t = ci0 + (act ? a : 0);
+      const uint2 *words = cwl + (size_t)t * P.words + l8;
+      // the lengths, the first two blocks' words (every slot holds at least
+      // two blocks) and the atom's original index, all in flight together
+      const int2 nn = act ? cwn[t] : make_int2(0, 0);
+      uint2 w0 = __ldg(words);
+      uint2 w1 = __ldg(words + CS_LPA);
+      const int io = sorig[t];
+      const int nba = (nn.x + CS_BLOCK - 1) / CS_BLOCK, nbt = nba + (nn.y + CS_BLOCK - 1) / CS_BLOCK;
+      const int nbw = __reduce_max_sync(0xffffffffu, nbt);
+      if (nbt < 1) w0 = pad;
+      if (nbt < 2) w1 = pad;
+      // an idle quarter sits far from every staged atom: its sums stay zero
+      const float4 xi = act ? wx[ioff + a] : make_float4(-1.0e6f, -1.0e6f, -1.0e6f, 0.f);
+      const int ti = LJM == 2 && act ? wt[ioff + a] : 0;
+      CwAcc A;
+      cw_zero(A);
+      auto geom = [&](uint32_t e, float4 &xj, float &dx, float &dy, float &dz) {
+        xj = lds_f4(wxb + ((e & CW_IDX) << 4));
+        dx = xi.x - xj.x;
+        dy = xi.y - xj.y;
+        dz = xi.z - xj.z;
+        return fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      };
+      auto lj_pair = [&](uint32_t e, float dx, float dy, float dz, float r2, CwAcc &Acc) {
+        if (LJM == 1) {
+          cw_lj(P, dx, dy, dz, r2, P.rc2_l, P.dx2l, P.offl, P.vtl, tl, Acc);
+        } else if (LJM == 2) {
+          const int tj = wt[e & CW_IDX];
+          const int in = s_map[ti * P.ntypes + tj];
+          const float4 cut = s_cut[in < 0 ? 0 : in];
+          cw_lj(P, dx, dy, dz, in < 0 ? 3.0e38f : r2, cut.x, cut.y, cut.z, cut.w,
+                tl + (size_t)2 * (in < 0 ? 0 : in) * P.ntable, Acc);
+        }
+      };
+      // one entry: the front segment (LJ list; electrostatics where the te
+      // flag is set) or the back segment (electrostatics only)
+      auto pair = [&](uint32_t e, bool front, CwAcc &Acc) {
+        float4 xj;
+        float dx, dy, dz;
+        const float r2 = geom(e, xj, dx, dy, dz);
+        if (HAS_EL) {
+          const bool el = !front || (e & CW_EL);
+          cw_elec<CS_RF, CS_RG>(P, el ? xj.w : 0.f, dx, dy, dz, el ? r2 : 3.0e38f, tfb, tgb, Acc);
+        }
+        if (LJM) lj_pair(e, dx, dy, dz, front ? r2 : 3.0e38f, Acc);
+      };
+      for (int b = 0; b < nbw; b++) {
+        const uint2 w2 = b + 2 < nbt ? __ldg(words + (b + 2) * CS_LPA) : pad;
+        const bool front = b < nba;
+        pair(w0.x & 0xFFFFu, front, A);
+        pair(w0.x >> 16, front, A);
+        pair(w0.y & 0xFFFFu, front, A);
+        pair(w0.y >> 16, front, A);
+        w0 = w1;
+        w1 = w2;
+      }
+      // CM3D's table underflow (k < 1), counted per pair: an atom whose
+      // smallest distance or LJ coordinate says it has some is walked again
+      if (__any_sync(0xffffffffu, (HAS_EL && A.r2min < P.r2under) || (LJM && A.pminl < 1.f))) {
+        unsigned cnt = 0;
+        for (int b = 0; b < nbw; b++) {
+          const uint2 w = b < nbt ? __ldg(words + b * CS_LPA) : pad;
+          const uint32_t e[4] = {w.x & 0xFFFFu, w.x >> 16, w.y & 0xFFFFu, w.y >> 16};
+          const bool front = b < nba;
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            float4 xj;
+            float dx, dy, dz;
+            const float r2 = geom(e[k], xj, dx, dy, dz);
+            const bool el = HAS_EL && (!front || (e[k] & CW_EL));
+            cnt += (el && r2 < P.rc2_el && fmaf(r2, P.dx2c, -P.offc) < 1.f) ? 1u : 0u;
+            if (front && LJM) {
+              CwAcc B;
+              cw_zero(B);
+              lj_pair(e[k], dx, dy, dz, r2, B);
+              cnt += B.pminl < 1.f ? 1u : 0u;
+            }
+          }
+        }
+        under += cnt;
+      }
+      // forces: F_i = -(qi sum qj f d + sum f_lj d), each lane's chunk in
+      // FP64, summed over the atom's 8 lanes
+      const double qi = (double)xi.w;
+      double Fx = -(qi * (double)A.fx + (double)A.gx);
+      double Fy = -(qi * (double)A.fy + (double)A.gy);
+      double Fz = -(qi * (double)A.fz + (double)A.gz);
+#pragma unroll
+      for (int o = CS_LPA / 2; o > 0; o >>= 1) {
+        Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+        Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+        Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+      }
+      if (act && l8 < 3) {
+        // the only addition to this element in the launch, so the result
+        // does not depend on timing; a reduction needs no round trip
+        const double Fc = l8 == 0 ? Fx : (l8 == 1 ? Fy : Fz);
+        atomicAdd(fout + (size_t)l8 * P.n + io, Fc);
+      }
+      // the atom's 16 quantities over its 8 lanes: three transposing FP32
+      // levels leave lane l8 with quantities 2 l8 and 2 l8 + 1
+      {
+        const float qf = xi.w;
+        float v[16] = {qf * A.eel, 0.f, qf * A.ve[0], qf * A.ve[1], qf * A.ve[2], qf * A.ve[3], qf * A.ve[4],
+                       qf * A.ve[5], A.elo, A.vsh, A.vl[0], A.vl[1], A.vl[2], A.vl[3], A.vl[4], A.vl[5]};
+#pragma unroll
+        for (int h = 8, o = 4; h >= 2; h >>= 1, o >>= 1) {
+          const bool hi = (lane & o) != 0;
+#pragma unroll
+          for (int i = 0; i < h; i++) {
+            const float snd = hi ? v[i] : v[i + h];
+            const float kp = hi ? v[i + h] : v[i];
+            v[i] = kp + __shfl_xor_sync(0xffffffffu, snd, o);
+          }
+        }
+        Eq0 += (double)v[0];
+        Eq1 += (double)v[1];
+        Ehi += A.elj_hi;
+      }
+    }
+    // the item's sums: the four atom quarters of a warp, the group's warps,
+    // in a fixed order
+    {
+      Eq0 += __shfl_xor_sync(0xffffffffu, Eq0, 8);
+      Eq0 += __shfl_xor_sync(0xffffffffu, Eq0, 16);
+      Eq1 += __shfl_xor_sync(0xffffffffu, Eq1, 8);
+      Eq1 += __shfl_xor_sync(0xffffffffu, Eq1, 16);
+      const double hi = warp_sum(Ehi);
+      if (lane < CS_LPA) {
+        s_red[g][gw][2 * lane] = Eq0 + (2 * lane == CQ_ELJ ? hi : 0.0);
+        s_red[g][gw][2 * lane + 1] = Eq1 + (2 * lane + 1 == CQ_ELJ ? hi : 0.0);
+      }
+    }
+    group_sync(bar_id);
+    if (gt < CQ_COUNT) {
+      double s = 0.0;
+      for (int w = 0; w < CS_WARPS; w++) s += s_red[g][w][gt];
+      ipart[(size_t)(item0 + item) * CQ_COUNT + gt] = s;
+    }
+  }
+  if (lane == 0 && under) atomicAdd((unsigned long long *)(stat + ST_UNDERFLOW), under);
+}
+
 // Sum of the items' partials into CM3D's accumulators: one block, warp q
 // sums quantity q over the items (fixed order), then one thread applies the
 // sums in a fixed order (several quantities feed one accumulator); each pair
@@ -783,9 +1188,9 @@ __global__ void __launch_bounds__(CQ_COUNT * 32) k_cw_ereduce_sys(int mask, cons
 // ------------------------------------------------------------------ host
 static int cw_ljm_of(int ninter) { return ninter == 0 ? 0 : (ninter == 1 ? 1 : 2); }
 
-static size_t cw_table_bytes(bool el, int ljm, int ninter, int ntable) {
+static size_t cw_table_bytes(bool el, int ljm, int ninter, int ntable, int rf = CW_RF, int rg = CW_RG) {
   size_t b = 0;
-  if (el) b += (size_t)ntable * (CW_RF * sizeof(float4) + CW_RG * sizeof(float2));
+  if (el) b += (size_t)ntable * (rf * sizeof(float4) + rg * sizeof(float2));
   if (ljm) b += (size_t)2 * ninter * ntable * sizeof(float4);
   return b;
 }
@@ -850,7 +1255,8 @@ struct CwGroup {
   int ljm = 0;
   CwP P;                   // parameters; nitems = the group's items
   int item0 = 0;           // first item (global item index)
-  size_t smem = 0;
+  size_t smem = 0;         // k_pair_cw's dynamic shared memory
+  size_t smem8 = 0;        // k_pair_cs's (0: its windows do not fit)
   size_t tf0 = 0, tl0 = 0; // offsets of its tables in cw_tf / cw_tg (knots) and cw_tl (float4)
   std::string key;         // tables + parameters, byte for byte
 };
@@ -875,8 +1281,15 @@ static long long cw_env_cap(long long cap) {
 }
 
 // the compact list's 8-byte words per atom slot: each segment rounded up to
-// whole blocks
-static int cw_words_for(long long stride) { return (int)(((stride + CW_BLOCK - 1) / CW_BLOCK + 1) * CW_ROW); }
+// whole blocks of 4 row entries (row lanes per atom: 32 or 8)
+static int cw_words_row(long long stride, int row) {
+  return (int)(((stride + 4 * row - 1) / (4 * row) + 1) * row);
+}
+// room for either layout, so that the autotuner can switch without
+// reallocating
+static int cw_words_for(long long stride) {
+  return std::max(cw_words_row(stride, CW_ROW), cw_words_row(stride, CS_LPA));
+}
 
 static int cw_setup_batch(Ctx *c);
 
@@ -902,7 +1315,8 @@ int cw_setup(Ctx *c) {
   if (tb + (want_cap + 1) * per_slot + 16 > budget) return CM3D_NB_OK;
   long long cap = (long long)((budget - tb - 16) / per_slot) - 1;
   cap = cw_env_cap(std::min<long long>(cap, CW_MAX_CAP));
-  c->cw_cap = (int)cap;
+  c->cw_cap = c->cw_cap32 = (int)cap;
+  c->cw_row = CW_ROW;
   c->cw_smem = tb + ((size_t)cap + 1) * sizeof(float4) + (ljm == 2 ? (size_t)cap + 1 : 0);
   c->cw_smem = (c->cw_smem + 15) / 16 * 16;
   c->cw_words = cw_words_for(c->nbr_stride);
@@ -1066,7 +1480,25 @@ static int cw_setup_batch(Ctx *c) {
     groups->clear();
     return CM3D_NB_OK;
   }
-  c->cw_cap = (int)cap;
+  c->cw_cap32 = (int)cap;
+  // k_pair_cs: CS_NG windows per block next to the tables
+  const size_t budget8 = c->smem_optin > CS_STATIC_SMEM ? c->smem_optin - CS_STATIC_SMEM : 0;
+  long long cap8 = CW_MAX_CAP;
+  for (const CwGroup &G : *groups) {
+    const size_t tb = cw_table_bytes(G.el, G.ljm, G.P.ninter, nt, CS_RF, CS_RG);
+    const size_t per_slot = sizeof(float4) + (G.ljm == 2 ? 1 : 0);
+    const long long room = budget8 > tb + 16 * CS_NG ? (long long)((budget8 - tb - 16 * CS_NG) / (per_slot * CS_NG)) - 1 : 0;
+    cap8 = std::min(cap8, room);
+  }
+  cap8 = cw_env_cap(cap8);
+  c->cw_cap8 = (double)cap8 >= 1.25 * want_window + 64.0 ? (int)cap8 : 0;
+  // the layout: 32 lanes per atom (a system runs as it does alone) until
+  // the autotuner finds the 8-lane kernel faster (cells of a few tens of
+  // atoms); CM3D_NB_CW_ROW=8 starts there
+  c->cw_row = CW_ROW;
+  if (const char *r = getenv("CM3D_NB_CW_ROW"))
+    if (atoi(r) == CS_LPA && c->cw_cap8 > 0) c->cw_row = CS_LPA;
+  c->cw_cap = c->cw_row == CS_LPA ? c->cw_cap8 : c->cw_cap32;
   // items by group, systems in order; tables back to back
   std::vector<int4> items;
   std::vector<int2> sitems(nsys, make_int2(0, 0));
@@ -1083,14 +1515,18 @@ static int cw_setup_batch(Ctx *c) {
     }
     G.P.nitems = (int)items.size() - G.item0;
     G.P.nsplit = 1;
-    G.P.cap = c->cw_cap;
     G.tf0 = atf.size();
     G.tl0 = atl.size();
     atf.insert(atf.end(), gtf[g].begin(), gtf[g].end());
     atg.insert(atg.end(), gtg[g].begin(), gtg[g].end());
     atl.insert(atl.end(), gtl[g].begin(), gtl[g].end());
     const size_t tb = cw_table_bytes(G.el, G.ljm, G.P.ninter, nt);
-    G.smem = (tb + ((size_t)c->cw_cap + 1) * sizeof(float4) + (G.ljm == 2 ? (size_t)c->cw_cap + 1 : 0) + 15) / 16 * 16;
+    G.smem = (tb + ((size_t)c->cw_cap32 + 1) * sizeof(float4) + (G.ljm == 2 ? (size_t)c->cw_cap32 + 1 : 0) + 15) /
+             16 * 16;
+    if (c->cw_cap8 > 0) {
+      const size_t w8 = (size_t)CS_NG * ((size_t)c->cw_cap8 + 1);
+      G.smem8 = (cw_table_bytes(G.el, G.ljm, G.P.ninter, nt, CS_RF, CS_RG) + w8 * sizeof(float4) + (G.ljm == 2 ? w8 : 0) + 15) / 16 * 16;
+    }
   }
   // the gather kernel's atoms: the other systems' (a system's sorted
   // indices span its own atom range)
@@ -1108,6 +1544,7 @@ static int cw_setup_batch(Ctx *c) {
   int rc;
   if ((rc = upload_v(&c->cw_items, items)) || (rc = upload_v(&c->cw_sitems, sitems)) ||
       (rc = upload_v(&c->cw_sys, cwsys)) || (rc = upload_v(&c->cw_gidx, gidx)) || (rc = upload_v(&c->cw_tf, atf)) ||
+      (rc = upload_v(&c->cw_scan, std::vector<int>(nsys + 1, 0))) ||
       (rc = upload_v(&c->cw_tg, atg)) || (rc = upload_v(&c->cw_tl, atl)))
     return rc;
   c->cw_words = cw_words_for(c->nbr_stride);
@@ -1131,6 +1568,30 @@ void cw_set_split(Ctx *c, int nsplit) {
   c->cw_nitems = c->ncells * c->cw_nsplit;
 }
 
+// A batch's compact-list layout and the kernel that reads it: row 32
+// (k_pair_cw) or 8 lanes per atom (k_pair_cs).  The lists in use are
+// converted again; a window beyond the 8-lane kernel's smaller capacity
+// returns the batch to 32 lanes for good.
+int cw_set_row(Ctx *c, int row) {
+  if (!c->cw_ok || !c->cw_batch) return CM3D_NB_OK;
+  if (row == CS_LPA && c->cw_cap8 == 0) row = CW_ROW;
+  if (row == c->cw_row) return CM3D_NB_OK;
+  c->cw_row = row;
+  c->cw_cap = row == CS_LPA ? c->cw_cap8 : c->cw_cap32;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);       // it holds the other kernel
+    c->graph = nullptr;
+  }
+  if (!c->cw_use) return CM3D_NB_OK;      // converted when the compact path is taken up
+  int rc = cw_convert(c, false, true);
+  if (rc || c->cw_ok || row != CS_LPA) return rc;
+  c->cw_ok = c->cw_use = 1;
+  c->cw_cap8 = 0;
+  c->cw_row = CW_ROW;
+  c->cw_cap = c->cw_cap32;
+  return cw_convert(c, false, true);
+}
+
 // after a (gated) rebuild of the master list: the compact list (a batch:
 // of the compact systems being rebuilt, or of all after the slots widened)
 int cw_convert(Ctx *c, bool device_flag, bool all) {
@@ -1138,8 +1599,8 @@ int cw_convert(Ctx *c, bool device_flag, bool all) {
   // the autotuner converts them all before it times the compact path)
   if (!c->cw_ok || !c->cw_use) return CM3D_NB_OK;
   // the master slots widen on overflow (host-driven builds only): so do ours
-  const int words = cw_words_for(c->nbr_stride);
-  if (words > c->cw_words) {
+  if (cw_words_row(c->nbr_stride, c->cw_row) > c->cw_words) {
+    const int words = cw_words_for(c->nbr_stride);
     DevLock lock(device_mutex());
     CK(cudaStreamSynchronize(c->st));
     cudaFree(c->cwl);
@@ -1153,11 +1614,20 @@ int cw_convert(Ctx *c, bool device_flag, bool all) {
     }
   }
   const int *gate = device_flag ? c->istate : nullptr;
-  k_cw_convert<<<grid_for(32LL * c->n, 256), 256, 0, c->st>>>(
-      c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n, c->cw_words, c->cell_start, c->cell_of, c->cell_atoms, c->nlen,
-      c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat, device_flag ? c->istate + IS_HALT : nullptr, gate, c->sp,
-      c->sys_of, c->cw_batch ? c->cw_sys : nullptr, c->sreb, all ? 1 : 0);
-  c->launches++;
+  int *halt = device_flag ? c->istate + IS_HALT : nullptr;
+  if (c->cw_batch) {
+    // only the atoms of the compact systems being rebuilt (all: every one)
+    k_cw_scan<<<1, 1024, 0, c->st>>>(c->nsys, c->sp, c->cw_sys, c->sreb, all ? 1 : 0, c->cw_scan, gate);
+    k_cw_convert_sys<<<8 * c->num_sms, 256, 0, c->st>>>(c->nsys, c->cw_scan, c->sp, c->cw_cap, c->n, c->cw_words,
+                                                         c->cw_row, c->cell_start, c->cell_of, c->cell_atoms, c->nlen,
+                                                         c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat, halt, gate);
+    c->launches += 2;
+  } else {
+    k_cw_convert<<<grid_for(32LL * c->n, 256), 256, 0, c->st>>>(
+        c->nc[0], c->nc[1], c->nc[2], c->cw_cap, c->n, c->cw_words, c->cw_row, c->cell_start, c->cell_of,
+        c->cell_atoms, c->nlen, c->nbr_stride, c->nbr, c->cwl, c->cwn, c->stat, halt, gate);
+    c->launches++;
+  }
   CKL(c);
   if (!device_flag) {
     // a host-driven build: a window that did not fit turns the compact path
@@ -1209,6 +1679,34 @@ static void cw_launch(Ctx *c, bool el, int ljm, const CwP &P, size_t smem, doubl
   }
 }
 
+// k_pair_cs over a batch group's items (CS_NG groups of items per block)
+template <bool EL, int LJM>
+static void cs_launch_t(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
+                        const float4 *tl, const int4 *items, int item0) {
+  auto kern = k_pair_cs<EL, LJM, true>;
+  static unsigned long long attr_devs = 0;
+  if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(c->smem_optin - CS_STATIC_SMEM));
+    attr_devs |= 1ull << c->dev;
+  }
+  const int grid = std::min((P.nitems + CS_NG - 1) / CS_NG, c->num_sms);
+  kern<<<grid, CS_NG * CS_GT, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl,
+                                             c->shift, c->map, c->fcut, tf, tg, tl, fout, c->cw_part, c->stat,
+                                             c->gate, items, c->sp, item0);
+}
+
+static void cs_launch(Ctx *c, bool el, int ljm, const CwP &P, size_t smem, double *fout, const float4 *tf,
+                      const float2 *tg, const float4 *tl, const int4 *items, int item0) {
+  if (el) {
+    if (ljm == 0) cs_launch_t<true, 0>(c, P, smem, fout, tf, tg, tl, items, item0);
+    else if (ljm == 1) cs_launch_t<true, 1>(c, P, smem, fout, tf, tg, tl, items, item0);
+    else cs_launch_t<true, 2>(c, P, smem, fout, tf, tg, tl, items, item0);
+  } else {
+    if (ljm == 1) cs_launch_t<false, 1>(c, P, smem, fout, tf, tg, tl, items, item0);
+    else if (ljm == 2) cs_launch_t<false, 2>(c, P, smem, fout, tf, tg, tl, items, item0);
+  }
+}
+
 bool cw_applies(Ctx *c, int iflg, bool ns) { return c->cw_ok && c->cw_use && iflg == 1 && !ns; }
 
 // full force level through the compact path (the caller checked cw_applies):
@@ -1220,11 +1718,16 @@ int cw_pairs(Ctx *c, int mask, double *fout) {
       CwP P = G.P;
       P.n = c->n;
       P.words = c->cw_words;
+      P.cap = c->cw_cap;
       const bool el = G.el && (mask & 2);
       const int ljm = (mask & 1) ? G.ljm : 0;
       if (!el && !ljm) continue;
-      cw_launch<true>(c, el, ljm, P, G.smem, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,
-                      c->cw_items + G.item0, G.item0);
+      if (c->cw_row == CS_LPA)
+        cs_launch(c, el, ljm, P, G.smem8, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,
+                  c->cw_items + G.item0, G.item0);
+      else
+        cw_launch<true>(c, el, ljm, P, G.smem, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,
+                        c->cw_items + G.item0, G.item0);
       c->launches++;
     }
     CKL(c);

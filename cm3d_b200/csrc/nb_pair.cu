@@ -1080,7 +1080,7 @@ int mixed_pairs(Ctx *c, int iflg, int mask) {
   if (cw_applies(c, iflg, ns)) {
     // one system with >= 3 cells per axis, full force level: the compact
     // window list (nb_cwin.cu) and its own energy sums
-    c->pair_used = CM3D_NB_PAIR_COMPACT;
+    c->pair_used = c->cw_batch && c->cw_row == CM3D_CS_LPA ? CM3D_NB_PAIR_COMPACT8 : CM3D_NB_PAIR_COMPACT;
     c->launches++;                                   // k_xq_update
     int rc = cw_pairs(c, mask, fout);
     if (rc) return rc;

@@ -293,10 +293,11 @@ class Engine:
         return [int(x) for x in nc], int(sp.value), int(nt.value)
 
     def pair_kernel(self) -> tuple[str, int]:
-        """(kernel of the last pair launch: "gather", "window", "system" or "compact", lanes per atom)"""
+        """(kernel of the last pair launch: "gather", "window", "system", "compact" or "compact8" (a
+        batch's compact lists with 8 lanes per atom), lanes per atom of the gather kernel)"""
         k, t = C.c_int(0), C.c_int(0)
         check(load_library().cm3d_nb_pair_kernel(self._h, C.byref(k), C.byref(t)), "pair_kernel")
-        return {0: "gather", 1: "window", 2: "system", 3: "compact"}[k.value], int(t.value)
+        return {0: "gather", 1: "window", 2: "system", 3: "compact", 4: "compact8"}[k.value], int(t.value)
 
     def system_energies(self, sys: int) -> dict:
         """getvireal + geteng of one system of a batch"""

@@ -360,16 +360,22 @@ int cm3d_nb_autotune(cm3d_nb_ctx *ctx, int reps, int *tpa_chosen, double ms_per_
    cells per axis at the full force level (no RESPA switch copy); its list is
    rewritten after each rebuild as 16-bit indices into the i-cell's staged
    27-cell window, and its tables are replicated across the shared-memory
-   banks.  CM3D_NB_PAIR_KERNEL=window keeps a context off the compact kernel.  cm3d_nb_autotune times the
-   gather kernel and the staged one that applies at every lanes-per-atom
-   choice, keeps the fastest, and ms_per_launch[k] is the faster at that
-   choice.  CM3D_NB_PAIR_KERNEL=list in the environment at cm3d_nb_create
+   banks.  In a batch the compact path covers the systems with >= 3 cells
+   per axis, 32 lanes per atom (COMPACT) or, where cells hold a few tens of
+   atoms, 8 lanes per atom with several cells in flight per block
+   (COMPACT8, when the autotuner finds it faster; CM3D_NB_CW_ROW=8 in the
+   environment at create starts there).
+   CM3D_NB_PAIR_KERNEL=window keeps a context off the compact kernel.
+   cm3d_nb_autotune times the gather kernel and the staged and compact ones
+   that apply at every lanes-per-atom choice, keeps the fastest, and
+   ms_per_launch[k] is the faster at that choice.  CM3D_NB_PAIR_KERNEL=list in the environment at cm3d_nb_create
    keeps a context on the gather kernel.  cm3d_nb_pair_kernel reports the
    kernel of the last pair launch and the lanes per atom. */
 #define CM3D_NB_PAIR_GATHER 0
 #define CM3D_NB_PAIR_WINDOW 1
 #define CM3D_NB_PAIR_SYSTEM 2
 #define CM3D_NB_PAIR_COMPACT 3
+#define CM3D_NB_PAIR_COMPACT8 4   /* a batch's compact lists with 8 lanes per atom (small cells) */
 int cm3d_nb_pair_kernel(cm3d_nb_ctx *ctx, int *kernel, int *tpa);
 /* the cell grid of system `sys` (cells per box direction) and, for the
    compact path, the parts each cell's atoms are split into (work items per

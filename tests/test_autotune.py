@@ -26,7 +26,7 @@ def test_autotune_keeps_state(engine_lib, names):
     en0 = e.all_energies()
     res = e.autotune(reps=3)
     assert res["tpa"] in (4, 8, 16, 32)
-    assert res["kernel"] in ("gather", "window", "system", "compact")
+    assert res["kernel"] in ("gather", "window", "system", "compact", "compact8")
     if len(names) > 1:
         assert res["kernel"] in ("gather", "system")   # a batch: gather or whole systems staged
     elif names[0] == "water216":

@@ -80,18 +80,40 @@ def test_ensemble_matches_oracle(engine_lib, boxes):
     assert small > 0, "the slice should contain boxes narrower than three list radii"
 
 
-def test_ensemble_steps_like_oracle(engine_lib, boxes):
-    """20 steps of the whole slice as one batch (graph) against each box's
-    oracle trajectory: energies within the mixed engine's trajectory bound,
-    same list rebuild and RESETPOS counts"""
+@pytest.fixture(scope="module")
+def mid_boxes():
+    """12 boxes of 589-1373 atoms from the ensemble generator: 3 or 4 cells
+    per axis, every one in the compact path of a batch"""
+    from cm3d_b200 import configs, setup
+    return [setup.build_system(w) for w in configs.ensemble(12, seed=11, nmin=500, nmax=1400)]
+
+
+@pytest.mark.parametrize("slice_row", [("small", 0), ("mid", 32), ("mid", 8)])
+def test_ensemble_steps_like_oracle(engine_lib, boxes, mid_boxes, slice_row, monkeypatch):
+    """20 steps of a slice as one batch (graph) against each box's oracle
+    trajectory: energies within the mixed engine's trajectory bound, same
+    list rebuild and RESETPOS counts -- the small boxes with the default
+    kernels, and boxes of 3-4 cells per axis on the 32- and the 8-lane
+    compact kernel (their lists converted again, on the device, at each
+    box's rebuilds)"""
     from oracle import Oracle
     nsteps = 20
+    which, row = slice_row
+    boxes = boxes if which == "small" else mid_boxes
+    if row:
+        monkeypatch.setenv("CM3D_NB_CW_ROW", str(row))
     e = Engine(boxes, mode=_abi.MIXED)
+    monkeypatch.delenv("CM3D_NB_CW_ROW", raising=False)
+    monkeypatch.delenv("CM3D_NB_PAIR_KERNEL", raising=False)
     e.step_init()
+    if row:
+        assert e.pair_kernel()[0] == ("compact" if row == 32 else "compact8")
     e.step(1, nsteps)
     en = e.all_energies()
     rb, rs = e.system_counts()
+    st = e.status()
     e.close()
+    assert st["stage_timeouts"] == 0 and st["overflows"] == 0
     for s, sm in enumerate(boxes):
         o = Oracle(sm, nocell_all=1)
         o.step_init()
@@ -170,14 +192,16 @@ def test_headline_kernel_on_large_boxes(engine_lib, large_boxes, monkeypatch):
             fh.write(line + "\n")
 
 
-def test_compact_batch_on_large_boxes(engine_lib, large_boxes):
-    """the headline's default pair path: the batch's boxes with 3 or more
-    cells per axis in the compact kernel (grouped by their tables), the
+@pytest.mark.parametrize("row", [32, 8])
+def test_compact_batch_on_large_boxes(engine_lib, large_boxes, row, monkeypatch):
+    """the headline's compact pair paths: the batch's boxes with 3 or more
+    cells per axis in the compact kernel (grouped by their tables) with 32
+    lanes per atom (k_pair_cw) or 8 (k_pair_cs, the small-cell kernel), the
     others in the gather kernel in the same force call -- on the headline
     ensemble's largest and smallest boxes against each box's oracle, at
-    positions the oracle reached after 10 steps; the compact boxes' forces
-    are bit-identical to the same box alone (one system, compact kernel),
-    and a repeat of the force call gives the same bits"""
+    positions the oracle reached after 10 steps; with 32 lanes the compact
+    boxes' forces are bit-identical to the same box alone (one system,
+    compact kernel); a repeat of the force call gives the same bits"""
     from oracle import Oracle
     pos = []
     for sm in large_boxes:
@@ -185,11 +209,13 @@ def test_compact_batch_on_large_boxes(engine_lib, large_boxes):
         o.step_init()
         o.step(1, 10)
         pos.append(o.positions())
+    monkeypatch.setenv("CM3D_NB_CW_ROW", str(row))
     e = Engine(large_boxes, mode=_abi.MIXED, tpa=4)
+    monkeypatch.delenv("CM3D_NB_CW_ROW")
     e.set_positions(np.concatenate(pos, axis=1))
     e.get_ngbr()
     e.force(1)
-    assert e.pair_kernel()[0] == "compact"
+    assert e.pair_kernel()[0] == ("compact" if row == 32 else "compact8")
     f = e.forces(_abi.FXL)
     e.force(1)
     np.testing.assert_array_equal(e.forces(_abi.FXL), f)
@@ -204,6 +230,7 @@ def test_compact_batch_on_large_boxes(engine_lib, large_boxes):
         a0, n = e.ranges[s]
         if min(grids[s]) >= 3:
             ncompact += 1
+        if min(grids[s]) >= 3 and row == 32:
             one = Engine(sm, mode=_abi.MIXED)
             one.set_positions(pos[s])
             one.get_ngbr()
@@ -221,7 +248,7 @@ def test_compact_batch_on_large_boxes(engine_lib, large_boxes):
         assert rel_rms(f[:, a0:a0 + n], fo, scale) <= FTOL, s
         d = np.sqrt(((f[:, a0:a0 + n] - fo) ** 2).sum(axis=0))
         stats.append({"natoms": n, "charged": bool(sm.get("ncharge", 0)), "cells": grids[s],
-                      "kernel": "compact" if min(grids[s]) >= 3 else "gather",
+                      "kernel": f"compact{row}" if min(grids[s]) >= 3 else "gather",
                       "rel_rms": rel_rms(f[:, a0:a0 + n], fo),
                       "max_atom_over_rms": float(d.max() / np.sqrt((fo * fo).sum(axis=0).mean()))})
         eo = o.energies()
@@ -231,8 +258,8 @@ def test_compact_batch_on_large_boxes(engine_lib, large_boxes):
     assert 0 < ncompact < len(large_boxes), "the slice should hold compact and gather boxes"
     import json
     import os
-    line = json.dumps({"config": "ensemble_large_boxes_compact", "kernel": "compact batch + gather, 4 lanes",
-                       "boxes": stats})
+    line = json.dumps({"config": f"ensemble_large_boxes_compact{row}",
+                       "kernel": f"compact batch ({row} lanes per atom) + gather, 4 lanes", "boxes": stats})
     print("ERRSTAT", line)
     if os.environ.get("CM3D_NB_ERRLOG"):
         with open(os.environ["CM3D_NB_ERRLOG"], "a") as fh:
