@@ -785,7 +785,7 @@ __global__ void __launch_bounds__(NT, 1) k_pair_cw(
 // tens of atoms, as in a batch of small LJ boxes.  There a block per cell
 // spends most of its time staging the window and waiting for it, and a
 // warp per atom leaves most lanes idle on lists of ~70 entries.  Here
-//   * a block is NG groups of CS_WARPS warps, each group working through
+//   * a block is NG groups of GW warps, each group working through
 //     its own items (cells) with its own window, mbarrier and named
 //     barrier, so one group's staging overlaps the others' pairs;
 //   * an atom has CS_LPA = 8 lanes (four atoms per warp) and its compact
@@ -799,31 +799,34 @@ __global__ void __launch_bounds__(NT, 1) k_pair_cw(
 // across an atom's lanes (forces) and per lane, warp, group and item (the
 // 16 energy/virial quantities), all in a fixed order.
 constexpr int CS_LPA = CM3D_CS_LPA;         // lanes per atom (the list row)
-constexpr int CS_WARPS = 4;                 // warps per group
-constexpr int CS_GT = 32 * CS_WARPS;        // threads per group
 constexpr int CS_BLOCK = 4 * CS_LPA;        // list entries per block
-constexpr int CS_NG = 4;                    // groups per block
-static_assert(CS_NG * CS_GT == CM3D_CS_THREADS, "k_pair_cs block size");
-constexpr int CS_STATIC_SMEM = 12288;       // >= k_pair_cs's static shared arrays
+// a block: NG groups of GW warps, 512 threads -- 4 x 4 where the tables
+// leave room for four windows only, else 8 x 2 (more cells in flight, fewer
+// idle atom slots on cells of ~20 atoms)
+constexpr int CS_NG = 4, CS_GW = 4;
+constexpr int CS_NG_WIDE = 8, CS_GW_WIDE = 2;
+static_assert(CS_NG * CS_GW * 32 == CM3D_CS_THREADS && CS_NG_WIDE * CS_GW_WIDE * 32 == CM3D_CS_THREADS,
+              "k_pair_cs block size");
+constexpr int CS_STATIC_SMEM = 16384;       // >= k_pair_cs's static shared arrays
 constexpr int CS_RF = 4;                    // erfc table copies (four groups' windows need the room)
 constexpr int CS_RG = 4;
 
-__device__ __forceinline__ void group_sync(int id) {
-  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(CS_GT) : "memory");
+__device__ __forceinline__ void group_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 // group barrier that also returns whether `p` holds in every thread of it
-__device__ __forceinline__ bool group_and(int id, bool p) {
+__device__ __forceinline__ bool group_and(int id, int nthreads, bool p) {
   unsigned r;
   asm volatile(
       "{\n .reg .pred a, b;\n setp.ne.u32 a, %1, 0;\n bar.red.and.pred b, %2, %3, a;\n selp.u32 %0, 1, 0, b;\n}"
       : "=r"(r)
-      : "r"((unsigned)p), "r"(id), "r"(CS_GT)
+      : "r"((unsigned)p), "r"(id), "r"(nthreads)
       : "memory");
   return r != 0;
 }
 
-template <bool HAS_EL, int LJM, bool BATCH, int NG = CS_NG>
-__global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
+template <bool HAS_EL, int LJM, bool BATCH, int NG = CS_NG, int GW = CS_GW>
+__global__ void __launch_bounds__(NG *GW * 32, 1) k_pair_cs(
     CwP P, const float4 *__restrict__ xq, const int *__restrict__ styp, const int *__restrict__ sorig,
     const int *__restrict__ cell_start, const int2 *__restrict__ cwn, const uint2 *__restrict__ cwl,
     const float4 *__restrict__ gshift, const int *__restrict__ gmap, const float *__restrict__ gfcut,
@@ -839,7 +842,8 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
   float2 *tg = reinterpret_cast<float2 *>(tf + (HAS_EL ? P.ntable * CS_RF : 0));
   float4 *tl = reinterpret_cast<float4 *>(tg + (HAS_EL ? P.ntable * CS_RG : 0));
   const int nl = LJM ? 2 * P.ninter * P.ntable : 0;
-  const int g = threadIdx.x / CS_GT, gt = threadIdx.x % CS_GT, gw = gt >> 5;
+  constexpr int GT = GW * 32;                     // threads per group
+  const int g = threadIdx.x / GT, gt = threadIdx.x % GT, gw = gt >> 5;
   const int lane = threadIdx.x & 31, l8 = lane & (CS_LPA - 1), sub = lane / CS_LPA;
   const int bar_id = 1 + g;
   float4 *wx = tl + nl + (size_t)g * (P.cap + 1);
@@ -848,7 +852,7 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
   __shared__ float4 s_shift[BATCH ? NG : 1][54];
   __shared__ int s_map[256];
   __shared__ float4 s_cut[64];
-  __shared__ double s_red[NG][CS_WARPS][CQ_COUNT];
+  __shared__ double s_red[NG][GW][CQ_COUNT];
   __shared__ __align__(8) unsigned long long s_mbar[NG];
   static_assert(CQ_COUNT == 2 * CS_LPA, "the transposing reduction gives lane l quantities 2l and 2l + 1");
 
@@ -899,9 +903,9 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
       c = item;
     }
     const int cz = c % ncz, cy = (c / ncz) % ncy, cx = c / (ncz * ncy);
-    group_sync(bar_id);                                    // the previous window is no longer read
+    group_sync(bar_id, GT);                                    // the previous window is no longer read
     if (BATCH)
-      for (int k = gt; k < 54; k += CS_GT)
+      for (int k = gt; k < 54; k += GT)
         s_shift[g][k] = k < 27 ? sp[sys].shift[k] : sp[sys].shift_lo[k - 27];
     if (gw == 0) {
       int cnt = 0, cs = 0;
@@ -926,7 +930,7 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
       }
       if (lane == 26) s_off[g][27] = incl;
     }
-    group_sync(bar_id);
+    group_sync(bar_id, GT);
     const int tot = s_off[g][27];
     const bool staged = tot <= P.cap;
     if (staged) {
@@ -943,7 +947,7 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
       }
       const bool arrived = mbar_wait(bar, phase, CW_WAIT_LIMIT);
       phase ^= 1u;
-      if (!group_and(bar_id, arrived)) {
+      if (!group_and(bar_id, GT, arrived)) {
         // the copies did not complete (never seen): count it, wait once
         // more for copies still in flight, and leave the group's remaining
         // items undone; the host reads the count in the status
@@ -951,7 +955,7 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
         mbar_wait(bar, phase ^ 1u, CW_WAIT_LIMIT);
         break;
       }
-      for (int w = gw; w < 27; w += CS_WARPS) {
+      for (int w = gw; w < 27; w += GW) {
         const float4 sh = shift[w], shl = shift[27 + w];
         const int g0 = s_off[g][w], g1 = s_off[g][w + 1], u0 = s_cs[g][w] - g0;
         for (int k = g0 + lane; k < g1; k += 32) {
@@ -961,14 +965,14 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
         }
       }
     }
-    group_sync(bar_id);
+    group_sync(bar_id, GT);
     // lane l8 of an atom keeps quantities 2 l8 and 2 l8 + 1 of CQ_* in FP64
     double Eq0 = 0.0, Eq1 = 0.0, Ehi = 0.0;
     const int ci0 = s_cs[g][13], cin = staged ? s_off[g][14] - s_off[g][13] : 0, ioff = s_off[g][13];
     const uint32_t dm = (uint32_t)P.cap | ((uint32_t)P.cap << 16);
     const uint2 pad = make_uint2(dm, dm);
-    // the group's 16 atom slots (warp gw, quarter sub) over the cell's atoms
-    for (int a0 = 0; a0 < cin; a0 += CS_WARPS * 4) {
+    // the group's 4 GW atom slots (warp gw, quarter sub) over the cell's atoms
+    for (int a0 = 0; a0 < cin; a0 += GW * 4) {
       const int a = a0 + gw * 4 + sub;
       const bool act = a < cin;
       const int t = ci0 + (act ? a : 0);
@@ -1105,10 +1109,10 @@ __global__ void __launch_bounds__(NG *CS_GT, 1) k_pair_cs(
         s_red[g][gw][2 * lane + 1] = Eq1 + (2 * lane + 1 == CQ_ELJ ? hi : 0.0);
       }
     }
-    group_sync(bar_id);
+    group_sync(bar_id, GT);
     if (gt < CQ_COUNT) {
       double s = 0.0;
-      for (int w = 0; w < CS_WARPS; w++) s += s_red[g][w][gt];
+      for (int w = 0; w < GW; w++) s += s_red[g][w][gt];
       ipart[(size_t)(item0 + item) * CQ_COUNT + gt] = s;
     }
   }
@@ -1257,6 +1261,7 @@ struct CwGroup {
   int item0 = 0;           // first item (global item index)
   size_t smem = 0;         // k_pair_cw's dynamic shared memory
   size_t smem8 = 0;        // k_pair_cs's (0: its windows do not fit)
+  int ng8 = 0;             // k_pair_cs's groups per block (CS_NG or CS_NG_WIDE)
   size_t tf0 = 0, tl0 = 0; // offsets of its tables in cw_tf / cw_tg (knots) and cw_tl (float4)
   std::string key;         // tables + parameters, byte for byte
 };
@@ -1524,8 +1529,15 @@ static int cw_setup_batch(Ctx *c) {
     G.smem = (tb + ((size_t)c->cw_cap32 + 1) * sizeof(float4) + (G.ljm == 2 ? (size_t)c->cw_cap32 + 1 : 0) + 15) /
              16 * 16;
     if (c->cw_cap8 > 0) {
-      const size_t w8 = (size_t)CS_NG * ((size_t)c->cw_cap8 + 1);
-      G.smem8 = (cw_table_bytes(G.el, G.ljm, G.P.ninter, nt, CS_RF, CS_RG) + w8 * sizeof(float4) + (G.ljm == 2 ? w8 : 0) + 15) / 16 * 16;
+      // eight groups of two warps where their windows fit next to the
+      // group's tables, else four of four
+      const size_t tb8 = cw_table_bytes(G.el, G.ljm, G.P.ninter, nt, CS_RF, CS_RG);
+      auto bytes = [&](int ng) {
+        const size_t w8 = (size_t)ng * ((size_t)c->cw_cap8 + 1);
+        return (tb8 + w8 * sizeof(float4) + (G.ljm == 2 ? w8 : 0) + 15) / 16 * 16;
+      };
+      G.ng8 = bytes(CS_NG_WIDE) <= budget8 ? CS_NG_WIDE : CS_NG;
+      G.smem8 = bytes(G.ng8);
     }
   }
   // the gather kernel's atoms: the other systems' (a system's sorted
@@ -1679,31 +1691,38 @@ static void cw_launch(Ctx *c, bool el, int ljm, const CwP &P, size_t smem, doubl
   }
 }
 
-// k_pair_cs over a batch group's items (CS_NG groups of items per block)
-template <bool EL, int LJM>
-static void cs_launch_t(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
+// k_pair_cs over a batch group's items (NG groups of items per block)
+template <bool EL, int LJM, int NG, int GW>
+static void cs_launch_g(Ctx *c, const CwP &P, size_t smem, double *fout, const float4 *tf, const float2 *tg,
                         const float4 *tl, const int4 *items, int item0) {
-  auto kern = k_pair_cs<EL, LJM, true>;
+  auto kern = k_pair_cs<EL, LJM, true, NG, GW>;
   static unsigned long long attr_devs = 0;
   if (c->dev < 64 && !(attr_devs & (1ull << c->dev))) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(c->smem_optin - CS_STATIC_SMEM));
     attr_devs |= 1ull << c->dev;
   }
-  const int grid = std::min((P.nitems + CS_NG - 1) / CS_NG, c->num_sms);
-  kern<<<grid, CS_NG * CS_GT, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl,
+  const int grid = std::min((P.nitems + NG - 1) / NG, c->num_sms);
+  kern<<<grid, NG * GW * 32, smem, c->st>>>(P, c->xq, c->styp, c->cell_atoms, c->cell_start, c->cwn, c->cwl,
                                              c->shift, c->map, c->fcut, tf, tg, tl, fout, c->cw_part, c->stat,
                                              c->gate, items, c->sp, item0);
 }
 
-static void cs_launch(Ctx *c, bool el, int ljm, const CwP &P, size_t smem, double *fout, const float4 *tf,
+template <bool EL, int LJM>
+static void cs_launch_t(Ctx *c, int ng, const CwP &P, size_t smem, double *fout, const float4 *tf,
+                        const float2 *tg, const float4 *tl, const int4 *items, int item0) {
+  if (ng == CS_NG_WIDE) cs_launch_g<EL, LJM, CS_NG_WIDE, CS_GW_WIDE>(c, P, smem, fout, tf, tg, tl, items, item0);
+  else cs_launch_g<EL, LJM, CS_NG, CS_GW>(c, P, smem, fout, tf, tg, tl, items, item0);
+}
+
+static void cs_launch(Ctx *c, int ng, bool el, int ljm, const CwP &P, size_t smem, double *fout, const float4 *tf,
                       const float2 *tg, const float4 *tl, const int4 *items, int item0) {
   if (el) {
-    if (ljm == 0) cs_launch_t<true, 0>(c, P, smem, fout, tf, tg, tl, items, item0);
-    else if (ljm == 1) cs_launch_t<true, 1>(c, P, smem, fout, tf, tg, tl, items, item0);
-    else cs_launch_t<true, 2>(c, P, smem, fout, tf, tg, tl, items, item0);
+    if (ljm == 0) cs_launch_t<true, 0>(c, ng, P, smem, fout, tf, tg, tl, items, item0);
+    else if (ljm == 1) cs_launch_t<true, 1>(c, ng, P, smem, fout, tf, tg, tl, items, item0);
+    else cs_launch_t<true, 2>(c, ng, P, smem, fout, tf, tg, tl, items, item0);
   } else {
-    if (ljm == 1) cs_launch_t<false, 1>(c, P, smem, fout, tf, tg, tl, items, item0);
-    else if (ljm == 2) cs_launch_t<false, 2>(c, P, smem, fout, tf, tg, tl, items, item0);
+    if (ljm == 1) cs_launch_t<false, 1>(c, ng, P, smem, fout, tf, tg, tl, items, item0);
+    else if (ljm == 2) cs_launch_t<false, 2>(c, ng, P, smem, fout, tf, tg, tl, items, item0);
   }
 }
 
@@ -1723,7 +1742,7 @@ int cw_pairs(Ctx *c, int mask, double *fout) {
       const int ljm = (mask & 1) ? G.ljm : 0;
       if (!el && !ljm) continue;
       if (c->cw_row == CS_LPA)
-        cs_launch(c, el, ljm, P, G.smem8, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,
+        cs_launch(c, G.ng8, el, ljm, P, G.smem8, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,
                   c->cw_items + G.item0, G.item0);
       else
         cw_launch<true>(c, el, ljm, P, G.smem, fout, c->cw_tf + G.tf0, c->cw_tg + G.tf0, c->cw_tl + G.tl0,

@@ -280,13 +280,23 @@ __device__ __forceinline__ int exact_flags(const SysP &P, int n, int i, int j, i
 // candidate order, and whenever 32 are waiting the whole warp runs the exact
 // FP64 test on them at once (`decide(first, m)`: lane l < m takes queue entry
 // first + l), so the expensive test runs on full warps.
+//
+// With qr (the full lists of a grid of 3 or more cells per axis) the queue
+// also keeps each survivor's FP32 squared distance and its stencil cell's
+// shift code (bits ENT_CODE_SHIFT and up of the queue entry), for the
+// FP32-first flags (fast_flags); with `prune` (an orthorhombic such grid of
+// cells cw wide) stencil cells wholly beyond lim2 from the atom, by the gaps
+// to their faces less 1e-3 A, are skipped -- none of their atoms would pass
+// the prefilter, so the lists are the same.
 constexpr int LQ = 64;                     // queue entries per warp (> 2 * 32 - 1)
 
 template <class Decide>
 __device__ __forceinline__ void walk_candidates(const SysP &P, int i, int4 ci, float4 xi4, bool half_only,
                                                 const int *__restrict__ cell_atoms,
                                                 const int *__restrict__ cell_start,
-                                                const float4 *__restrict__ xq, int *qbuf, Decide &decide) {
+                                                const float4 *__restrict__ xq, int *qbuf, Decide &decide,
+                                                float *qr = nullptr, bool prune = false,
+                                                float3 cw = make_float3(0.f, 0.f, 0.f)) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int cx = ci.x & 1023, cy = (ci.x >> 10) & 1023, cz = (ci.x >> 20) & 1023;
@@ -297,30 +307,42 @@ __device__ __forceinline__ void walk_candidates(const SysP &P, int i, int4 ci, f
     const int ox = P.sx[a];
     int jx = cx + ox;
     jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
+    const float gx = prune ? fmaxf((ox > 0 ? cw.x - xi4.x : ox < 0 ? xi4.x : 0.f) - 1e-3f, 0.f) : 0.f;
     for (int b = 0; b < P.nsy; b++) {
       const int oy = P.sy[b];
       int jy = cy + oy;
       jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
+      const float gy = prune ? fmaxf((oy > 0 ? cw.y - xi4.y : oy < 0 ? xi4.y : 0.f) - 1e-3f, 0.f) : 0.f;
       for (int cc = 0; cc < P.nsz; cc++) {
         const int oz = P.sz[cc];
+        if (prune) {
+          const float gz = fmaxf((oz > 0 ? cw.z - xi4.z : oz < 0 ? xi4.z : 0.f) - 1e-3f, 0.f);
+          if (gx * gx + gy * gy + gz * gz >= lim2) continue;
+        }
         int jz = cz + oz;
         jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
         const int cell = P.c0 + (jx * ncy + jy) * ncz + jz;
         // cell-corner shift of this stencil offset (k = -offset)
-        const float4 S = P.shift[(1 - ox) * 9 + (1 - oy) * 3 + (1 - oz)];
+        const int scode = (1 - ox) * 9 + (1 - oy) * 3 + (1 - oz);
+        const float4 S = P.shift[scode];
         const int lo = cell_start[cell], hi = cell_start[cell + 1];
         for (int u0 = lo; u0 < hi; u0 += 32) {
           const int u = u0 + lane;
           bool keep = false;
+          float r2f = 0.f;
           if (u < hi) {
             const int j = cell_atoms[u];
             const float4 xj = xq[u];
             const float dx = (xi4.x - xj.x) + S.x, dy = (xi4.y - xj.y) + S.y, dz = (xi4.z - xj.z) + S.z;
-            const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
             keep = j != i && r2f < lim2 && (!half_only || j > i);
           }
           const unsigned bk = __ballot_sync(0xffffffffu, keep);
-          if (keep) qbuf[(tail + __popc(bk & lt_mask)) & (LQ - 1)] = u;
+          if (keep) {
+            const int slot = (tail + __popc(bk & lt_mask)) & (LQ - 1);
+            qbuf[slot] = qr ? (u | (scode << ENT_CODE_SHIFT)) : u;
+            if (qr) qr[slot] = r2f;
+          }
           tail += __popc(bk);
           __syncwarp();
           if (tail - head >= 32) {
@@ -581,9 +603,18 @@ __device__ __forceinline__ void full_list_atom(
           fl = exact_flags(P, n, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
                            cexcl_off, cexcl_idx, cimg, code);
       } else {
-        u = qbuf[slot];
-        fl = exact_flags(P, n, i, cell_atoms[u], ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off,
-                         excl_idx, cexcl_off, cexcl_idx, cimg, code);
+        const int uc = qbuf[slot];
+        u = fast ? (uc & (int)ENT_JMASK) : uc;
+        const int j = cell_atoms[u];
+        bool exact = !fast;
+        if (fast) {
+          fl = fast_flags(P, i, j, ti, itype[j], qi, q[j] != 0.0, qr[slot], map, icut, excl_off, excl_idx,
+                          cexcl_off, cexcl_idx, &exact);
+          code = (int)((unsigned)uc >> ENT_CODE_SHIFT);
+        }
+        if (exact)
+          fl = exact_flags(P, n, i, j, ci, pos, xi, yi, zi, ti, qi, itype, map, icut, q, excl_off, excl_idx,
+                           cexcl_off, cexcl_idx, cimg, code);
       }
     }
     bad |= (fl >> 4) & 1;
@@ -612,7 +643,8 @@ __device__ __forceinline__ void full_list_atom(
     nb += __popc(bb);
   };
   if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide, s_off, s_code, nw, prune, cw);
-  else walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide);
+  else walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide, fast ? qr : nullptr,
+                       prune, cw);
   const int count = na + nb;
   if (lane == 0) {
     if (count <= stride) {
@@ -635,7 +667,7 @@ __device__ __forceinline__ void full_list_atom(
 
 // Mixed mode, warp per atom over every atom (the candidates walked in global
 // memory): the fallback of k_list_win.
-__global__ void __launch_bounds__(256) k_list_full(
+__global__ void __launch_bounds__(256, 3) k_list_full(
     int n, const SysP *__restrict__ sp, const int *__restrict__ sys_of, const int *__restrict__ sreb, int all,
     int stride, const int *__restrict__ cell_atoms, const int *__restrict__ cell_start,
     const float4 *__restrict__ xq, const double *__restrict__ pos, const int *__restrict__ itype,
@@ -645,13 +677,21 @@ __global__ void __launch_bounds__(256) k_list_full(
     int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt, const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   __shared__ int qs[256 / 32][LQ];
+  __shared__ float qrs[256 / 32][LQ];
   const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (t >= n) return;                                     // whole warps
   const int s = sys_of[t];
   if (sys_skip(s, sreb, all)) return;                     // whole warps
-  full_list_atom<false>(sp[s], n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
+  // FP32-first flags and stencil pruning where the grid allows them (as in
+  // k_list_win: 3 or more cells per axis, no near-image pairs)
+  const SysP &P = sp[s];
+  const bool fast = P.nc[0] >= 3 && P.nc[1] >= 3 && P.nc[2] >= 3 && !P.smallbox;
+  const bool ortho = P.h[1] == 0. && P.h[2] == 0. && P.h[3] == 0. && P.h[5] == 0. && P.h[6] == 0. && P.h[7] == 0.;
+  const float3 cw = make_float3(P.hF[0] / (float)P.nc[0], P.hF[4] / (float)P.nc[1], P.hF[8] / (float)P.nc[2]);
+  full_list_atom<false>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                         excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[threadIdx.x >> 5],
-                        nullptr, nullptr, nullptr, nullptr, 0, false);
+                        qrs[threadIdx.x >> 5], nullptr, nullptr, nullptr, 0, fast, nullptr, nullptr, 0,
+                        fast && ortho, cw);
 }
 
 // The cells of the systems being rebuilt, as one index range: rb_scan[s] is
