@@ -296,62 +296,94 @@ __device__ __forceinline__ void walk_candidates(const SysP &P, int i, int4 ci, f
                                                 const int *__restrict__ cell_start,
                                                 const float4 *__restrict__ xq, int *qbuf, Decide &decide,
                                                 float *qr = nullptr, bool prune = false,
-                                                float3 cw = make_float3(0.f, 0.f, 0.f)) {
+                                                float3 cw = make_float3(0.f, 0.f, 0.f), int t = -1) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int cx = ci.x & 1023, cy = (ci.x >> 10) & 1023, cz = (ci.x >> 20) & 1023;
-  const int ncx = P.nc[0], ncy = P.nc[1], ncz = P.nc[2];
   const float lim2 = P.lim2;
+  // the stencil cells in walk order (x offsets outermost), one per lane:
+  // their sorted-atom ranges (empty where pruned) and shift codes, loaded
+  // together up front
+  const int nw = P.nsx * P.nsy * P.nsz;
+  int my_lo = 0, my_hi = 0, my_code = 13;
+  if (lane < nw) {
+    const int ox = P.sx[lane / (P.nsy * P.nsz)], oy = P.sy[(lane / P.nsz) % P.nsy], oz = P.sz[lane % P.nsz];
+    bool vis = true;
+    if (prune) {
+      const float gx = fmaxf((ox > 0 ? cw.x - xi4.x : ox < 0 ? xi4.x : 0.f) - 1e-3f, 0.f);
+      const float gy = fmaxf((oy > 0 ? cw.y - xi4.y : oy < 0 ? xi4.y : 0.f) - 1e-3f, 0.f);
+      const float gz = fmaxf((oz > 0 ? cw.z - xi4.z : oz < 0 ? xi4.z : 0.f) - 1e-3f, 0.f);
+      vis = gx * gx + gy * gy + gz * gz < lim2;
+    }
+    int jx = cx + ox, jy = cy + oy, jz = cz + oz;
+    jx = jx < 0 ? jx + P.nc[0] : (jx >= P.nc[0] ? jx - P.nc[0] : jx);
+    jy = jy < 0 ? jy + P.nc[1] : (jy >= P.nc[1] ? jy - P.nc[1] : jy);
+    jz = jz < 0 ? jz + P.nc[2] : (jz >= P.nc[2] ? jz - P.nc[2] : jz);
+    const int cell = P.c0 + (jx * P.nc[1] + jy) * P.nc[2] + jz;
+    // cell-corner shift of this stencil offset (k = -offset)
+    my_code = (1 - ox) * 9 + (1 - oy) * 3 + (1 - oz);
+    if (vis) {
+      my_lo = cell_start[cell];
+      my_hi = cell_start[cell + 1];
+    }
+  }
+  unsigned left = __ballot_sync(0xffffffffu, my_hi > my_lo);
+  // the chunks of 32 candidates in walk order; the next chunk's positions
+  // are loaded while the current one is tested
+  int w = left ? __ffs(left) - 1 : -1;
+  int u0 = 0, hi = 0, code = 13;
+  float4 S = make_float4(0.f, 0.f, 0.f, 0.f), xn = S;
+  if (w >= 0) {
+    u0 = __shfl_sync(0xffffffffu, my_lo, w);
+    hi = __shfl_sync(0xffffffffu, my_hi, w);
+    code = __shfl_sync(0xffffffffu, my_code, w);
+    S = P.shift[code];
+    if (u0 + lane < hi) xn = xq[u0 + lane];
+  }
   int head = 0, tail = 0;
-  for (int a = 0; a < P.nsx; a++) {
-    const int ox = P.sx[a];
-    int jx = cx + ox;
-    jx = jx < 0 ? jx + ncx : (jx >= ncx ? jx - ncx : jx);
-    const float gx = prune ? fmaxf((ox > 0 ? cw.x - xi4.x : ox < 0 ? xi4.x : 0.f) - 1e-3f, 0.f) : 0.f;
-    for (int b = 0; b < P.nsy; b++) {
-      const int oy = P.sy[b];
-      int jy = cy + oy;
-      jy = jy < 0 ? jy + ncy : (jy >= ncy ? jy - ncy : jy);
-      const float gy = prune ? fmaxf((oy > 0 ? cw.y - xi4.y : oy < 0 ? xi4.y : 0.f) - 1e-3f, 0.f) : 0.f;
-      for (int cc = 0; cc < P.nsz; cc++) {
-        const int oz = P.sz[cc];
-        if (prune) {
-          const float gz = fmaxf((oz > 0 ? cw.z - xi4.z : oz < 0 ? xi4.z : 0.f) - 1e-3f, 0.f);
-          if (gx * gx + gy * gy + gz * gz >= lim2) continue;
-        }
-        int jz = cz + oz;
-        jz = jz < 0 ? jz + ncz : (jz >= ncz ? jz - ncz : jz);
-        const int cell = P.c0 + (jx * ncy + jy) * ncz + jz;
-        // cell-corner shift of this stencil offset (k = -offset)
-        const int scode = (1 - ox) * 9 + (1 - oy) * 3 + (1 - oz);
-        const float4 S = P.shift[scode];
-        const int lo = cell_start[cell], hi = cell_start[cell + 1];
-        for (int u0 = lo; u0 < hi; u0 += 32) {
-          const int u = u0 + lane;
-          bool keep = false;
-          float r2f = 0.f;
-          if (u < hi) {
-            const int j = cell_atoms[u];
-            const float4 xj = xq[u];
-            const float dx = (xi4.x - xj.x) + S.x, dy = (xi4.y - xj.y) + S.y, dz = (xi4.z - xj.z) + S.z;
-            r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            keep = j != i && r2f < lim2 && (!half_only || j > i);
-          }
-          const unsigned bk = __ballot_sync(0xffffffffu, keep);
-          if (keep) {
-            const int slot = (tail + __popc(bk & lt_mask)) & (LQ - 1);
-            qbuf[slot] = qr ? (u | (scode << ENT_CODE_SHIFT)) : u;
-            if (qr) qr[slot] = r2f;
-          }
-          tail += __popc(bk);
-          __syncwarp();
-          if (tail - head >= 32) {
-            decide(head, 32);
-            head += 32;
-            __syncwarp();
-          }
+  while (w >= 0) {
+    const int u = u0 + lane, hcur = hi, ccur = code;
+    const float4 Sc = S, xj = xn;
+    u0 += 32;
+    if (u0 >= hi) {
+      left &= ~(1u << w);
+      w = left ? __ffs(left) - 1 : -1;
+      if (w >= 0) {
+        u0 = __shfl_sync(0xffffffffu, my_lo, w);
+        hi = __shfl_sync(0xffffffffu, my_hi, w);
+        code = __shfl_sync(0xffffffffu, my_code, w);
+        S = P.shift[code];
+      }
+    }
+    if (w >= 0 && u0 + lane < hi) xn = xq[u0 + lane];
+    bool keep = false;
+    float r2f = 0.f;
+    if (u < hcur) {
+      const float dx = (xi4.x - xj.x) + Sc.x, dy = (xi4.y - xj.y) + Sc.y, dz = (xi4.z - xj.z) + Sc.z;
+      r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      keep = r2f < lim2;
+      if (keep) {
+        // the atom itself (sorted index t when given); half lists: j > i
+        if (half_only || t < 0) {
+          const int j = cell_atoms[u];
+          keep = j != i && (!half_only || j > i);
+        } else {
+          keep = u != t;
         }
       }
+    }
+    const unsigned bk = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int slot = (tail + __popc(bk & lt_mask)) & (LQ - 1);
+      qbuf[slot] = qr ? (u | (ccur << ENT_CODE_SHIFT)) : u;
+      if (qr) qr[slot] = r2f;
+    }
+    tail += __popc(bk);
+    __syncwarp();
+    if (tail - head >= 32) {
+      decide(head, 32);
+      head += 32;
+      __syncwarp();
     }
   }
   while (tail > head) {
@@ -644,7 +676,7 @@ __device__ __forceinline__ void full_list_atom(
   };
   if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide, s_off, s_code, nw, prune, cw);
   else walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide, fast ? qr : nullptr,
-                       prune, cw);
+                       prune, cw, t);
   const int count = na + nb;
   if (lane == 0) {
     if (count <= stride) {
