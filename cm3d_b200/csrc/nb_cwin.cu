@@ -123,7 +123,6 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
     if (halt) *halt = 1;
   }
   {
-    const unsigned lt = (1u << lane) - 1u;
     {
       const int na = fits ? nlen[t] : 0, nb = fits ? nlen[n + t] : 0;
       const uint32_t *src = nbr + (size_t)t * stride;
@@ -158,39 +157,61 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
         // j % row (of the atom's lanes), so putting a class-(j % 8) entry at
         // j gives the 8 lanes of each quarter-warp 8 different bank groups;
         // the entries that do not fit their own class's positions fill the
-        // rest in order.
-        int cnt[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) cnt[q] = 0;
+        // rest.  Ranks within a class go lane by lane (lane l's entries l,
+        // l + 32, ... after those of the lanes before it): each lane counts
+        // its classes in 16-bit fields (classes 0-3 in c03, 4-7 in c47), one
+        // warp scan gives the bases -- no warp vote per entry.
+        unsigned long long c03 = 0ull, c47 = 0ull;
         for (int e0 = 0; e0 < m; e0 += 32) {
           uint32_t o;
           const int cl = window_index(e0 + lane, o);
+          if (cl >= 0) {
+            if (cl < 4) c03 += 1ull << (16 * cl);
+            else c47 += 1ull << (16 * (cl - 4));
+          }
+        }
+        unsigned long long i03 = c03, i47 = c47;
 #pragma unroll
-          for (int q = 0; q < 8; q++) cnt[q] += __popc(__ballot_sync(0xffffffffu, cl == q));
+        for (int o = 1; o < 32; o <<= 1) {
+          const unsigned long long a = __shfl_up_sync(0xffffffffu, i03, o);
+          const unsigned long long b = __shfl_up_sync(0xffffffffu, i47, o);
+          if (lane >= o) {
+            i03 += a;
+            i47 += b;
+          }
+        }
+        const unsigned long long t03 = __shfl_sync(0xffffffffu, i03, 31), t47 = __shfl_sync(0xffffffffu, i47, 31);
+        int cnt[8];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          cnt[q] = (int)((t03 >> (16 * q)) & 0xFFFFull);
+          cnt[q + 4] = (int)((t47 >> (16 * q)) & 0xFFFFull);
         }
         const int Q = m >> 3;
-        int run[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++) run[q] = 0;
+        // running ranks: this lane's bases, advanced per entry
+        unsigned long long r03 = i03 - c03, r47 = i47 - c47;
         for (int e0 = 0; e0 < m; e0 += 32) {
           uint32_t o = dummy;
           const int cl = window_index(e0 + lane, o);
-          int rank = 0, lbase = 0;
-#pragma unroll
-          for (int q = 0; q < 8; q++) {
-            const unsigned bq = __ballot_sync(0xffffffffu, cl == q);
-            if (cl == q) rank = run[q] + __popc(bq & lt);
-            if (q < cl) lbase += max(0, cnt[q] - Q);
-            run[q] += __popc(bq);
-          }
           if (cl >= 0) {
+            int rank;
+            if (cl < 4) {
+              rank = (int)((r03 >> (16 * cl)) & 0xFFFFull);
+              r03 += 1ull << (16 * cl);
+            } else {
+              rank = (int)((r47 >> (16 * (cl - 4))) & 0xFFFFull);
+              r47 += 1ull << (16 * (cl - 4));
+            }
             int pos;
             if (rank < Q) {
               pos = cl + 8 * rank;
             } else {
               // the L-th free position: the unused class positions of the
               // classes short of Q entries, in class order, then the tail
-              int L = lbase + rank - Q;
+              int L = rank - Q;
+#pragma unroll
+              for (int q = 0; q < 8; q++)
+                if (q < cl) L += max(0, cnt[q] - Q);
               pos = -1;
 #pragma unroll
               for (int q = 0; q < 8; q++) {
@@ -214,7 +235,7 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
   }
 }
 
-__global__ void __launch_bounds__(256) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words, int row,
+__global__ void __launch_bounds__(256, 3) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words, int row,
                                                     const int *__restrict__ cell_start,
                                                     const int *__restrict__ cell_of,
                                                     const int *__restrict__ sorig,
@@ -273,7 +294,7 @@ __global__ void __launch_bounds__(1024) k_cw_scan(int nsys, const SysP *__restri
 // A batch: warps walk the scanned range (a fixed grid, so that a captured
 // step converts whatever the device-side rebuild flags select); atom v of the
 // range lies in the last system s with scan[s] <= v, each on its own grid.
-__global__ void __launch_bounds__(256) k_cw_convert_sys(int nsys, const int *__restrict__ scan,
+__global__ void __launch_bounds__(256, 3) k_cw_convert_sys(int nsys, const int *__restrict__ scan,
                                                         const SysP *__restrict__ sp, int cap, int n, int words,
                                                         int row, const int *__restrict__ cell_start,
                                                         const int *__restrict__ cell_of,
