@@ -88,7 +88,7 @@ __device__ __forceinline__ float phase_rad(unsigned phi) {
 }
 
 template <bool BATCH, int A = KS_A>
-__global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *__restrict__ kfrac, int nrows,
+__global__ void __launch_bounds__(KS_THREADS, 2) k_sfac_mixed(int nq, const uint4 *__restrict__ kfrac, int nrows,
                                                            const int4 *__restrict__ rows,
                                                            const int *__restrict__ row_k0, int rows_per_block,
                                                            int ktot, double2 *__restrict__ spart,
@@ -156,19 +156,49 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
         s2[j] = make_float2(s[2 * j], s[2 * j + 1]);
       }
     }
+    if constexpr (A % 2 == 0) {
+      // k in groups of KG: each thread's KG (sr, si) pairs, then one
+      // transposing warp reduction -- lane l ends with value l (k = l / 2,
+      // component l % 2) after the same additions, in the same tree, as a
+      // butterfly sum of each value (warp_sum): the same bits, a sixteenth
+      // of the shuffles
+      constexpr int KG = 16;
+      float *redf = reinterpret_cast<float *>(red[w]);
+      for (int kb = 0; kb < len; kb += KG) {
+        float v[2 * KG];
+#pragma unroll
+        for (int q = 0; q < KG; q++) {
+          float sr = 0.f, si = 0.f;
+          if (kb + q < len) {
+            // the sums in atom order; the recursion two atoms at a time
+#pragma unroll
+            for (int j = 0; j < A / 2; j++) {
+              sr = fmaf(tq[2 * j], c2[j].x, sr);
+              si = fmaf(tq[2 * j], s2[j].x, si);
+              sr = fmaf(tq[2 * j + 1], c2[j].y, sr);
+              si = fmaf(tq[2 * j + 1], s2[j].y, si);
+              rot2(c2[j], s2[j], cs2[j], sn2[j], nsn2[j]);
+            }
+          }
+          v[2 * q] = sr;
+          v[2 * q + 1] = si;
+        }
+#pragma unroll
+        for (int h = KG, o = 16; h >= 1; h >>= 1, o >>= 1) {
+          const bool hi = (lane & o) != 0;
+#pragma unroll
+          for (int i = 0; i < h; i++) {
+            const float snd = hi ? v[i] : v[i + h];
+            const float kp = hi ? v[i + h] : v[i];
+            v[i] = kp + __shfl_xor_sync(0xffffffffu, snd, o);
+          }
+        }
+        if (kb + (lane >> 1) < len) redf[2 * kb + lane] = v[0];
+      }
+    } else {
     for (int kk = 0; kk < len; kk++) {
       float sr = 0.f, si = 0.f;
-      if constexpr (A % 2 == 0) {
-        // the sums in atom order as below; the recursion two atoms at a time
-#pragma unroll
-        for (int j = 0; j < A / 2; j++) {
-          sr = fmaf(tq[2 * j], c2[j].x, sr);
-          si = fmaf(tq[2 * j], s2[j].x, si);
-          sr = fmaf(tq[2 * j + 1], c2[j].y, sr);
-          si = fmaf(tq[2 * j + 1], s2[j].y, si);
-          rot2(c2[j], s2[j], cs2[j], sn2[j], nsn2[j]);
-        }
-      } else {
+      {
 #pragma unroll
         for (int m = 0; m < A; m++) {
           sr = fmaf(tq[m], c[m], sr);
@@ -185,6 +215,7 @@ __global__ void __launch_bounds__(KS_THREADS) k_sfac_mixed(int nq, const uint4 *
       sr = warp_sum(sr);
       si = warp_sum(si);
       if (lane == 0) red[w][kk] = make_float2(sr, si);
+    }
     }
     __syncthreads();
     const int k0 = row_k0[r];
