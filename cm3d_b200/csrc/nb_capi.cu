@@ -94,7 +94,7 @@ static void destroy(Ctx *c) {
                   c->ktile_sys, c->ftile_sys, c->k_sys, c->kf_part, c->ered, c->ered_done, c->sys_items, c->ftab_lj2, c->rb_scan,
                   c->fxr, c->intra_buf, c->ithm, c->nhc, c->cwl, c->cwn, c->cw_tf, c->cw_tg, c->cw_tl,
                   c->cw_part, c->nvt_kin, c->nvt_chsum, c->th_atoms, c->th_choff, c->th_chunk,
-                  c->cw_sys, c->cw_sitems, c->cw_items, c->cw_gidx, c->cw_scan};
+                  c->cw_sys, c->cw_sitems, c->cw_items, c->cw_gidx, c->cw_scan, c->grp_work};
   cw_destroy(c);
   for (void *p : ptrs)
     if (p) cudaFree(p);

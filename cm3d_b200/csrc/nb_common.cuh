@@ -233,6 +233,8 @@ struct Ctx {
   double *ered = nullptr;              // k_ereduce: per-block partial sums of one large system
   unsigned *ered_done = nullptr;       // k_ereduce: blocks finished per quantity
   int lw_cap = 0;                      // staged list build: neighbourhood atoms per block (0: off)
+  int *grp_work = nullptr;             // groups with ecorr pairs, bonds or bends (device)
+  int ngwork = 0;
   int *rb_scan = nullptr;              // staged list build: cells rebuilt before each system (nsys + 1)
   size_t lw_smem_max = 0;              // its shared-memory limit (bytes)
   int win_ok = 1;                      // single systems may use the windowed pair kernel

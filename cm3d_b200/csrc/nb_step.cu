@@ -597,7 +597,12 @@ __global__ void k_resetpos(int n, const SysP *__restrict__ sp, const int *__rest
 // collect the group's bonded energies and virials (getvbond / getvbend; the
 // bend virial is the one md_fbend.c always compiles, its tensor formed from
 // absolute positions as there)
-__global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaoff, const int *__restrict__ gatoms,
+// The molecules (groups) with intramolecular Coulomb corrections, bonds or
+// bends, listed in gwork: their energies, virials and ecorr forces.  The
+// force arrays are zeroed beforehand (group_init), so groups without such
+// terms -- every atom of a monatomic fluid -- need no thread.
+__global__ void k_group_init(StepP P, const int *__restrict__ gwork, int ngw, const int *__restrict__ gaoff,
+                             const int *__restrict__ gatoms,
                              const double *__restrict__ pos, const double *__restrict__ q,
                              double *__restrict__ fxl, double *__restrict__ fxs, const int *__restrict__ gcoff,
                              const int2 *__restrict__ cij, const int *__restrict__ gboff,
@@ -607,21 +612,17 @@ __global__ void k_group_init(StepP P, int zero_fxs, const int *__restrict__ gaof
                              const SysP *__restrict__ sp, const int *__restrict__ sys_of,
                              const int *__restrict__ gs) {
   if (gated_off(gs, 0)) return;
-  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int gi = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = P.n;
   // ecorr: pot, prs, t0 t1 t2 t4 t5 t8 | bond: v, w, t0..t8 | bend: v, w, t0..t8
   double v[30];
 #pragma unroll
   for (int k = 0; k < 30; k++) v[k] = 0.;
   int sy = -1;
-  if (g < P.ngroups) {
+  if (gi < ngw) {
+    const int g = gwork[gi];
     sy = sys_of[gatoms[gaoff[g]]];
     const double kappa = sp[sy].kappa, kappa2 = sp[sy].kappa2;
-    for (int a = gaoff[g]; a < gaoff[g + 1]; a++) {
-      int i = gatoms[a];
-      fxl[i] = fxl[n + i] = fxl[2 * n + i] = 0.;
-      if (zero_fxs) fxs[i] = fxs[n + i] = fxs[2 * n + i] = 0.;
-    }
     const double sqrt_pi = 1. / sqrt(M_PI);
     for (int c = gcoff[g]; c < gcoff[g + 1]; c++) {
       int ii = cij[c].x, jj = cij[c].y;
@@ -1262,6 +1263,15 @@ int step_setup(Ctx *c, const cm3d_nb_system *systems, int nsys) {
   CK(cudaMemcpy(c->bend_p, ep.data(), sizeof(double2) * ep.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ecorr_ij, cij.data(), sizeof(int2) * cij.size(), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(c->ecorr_pairs, cpair.data(), sizeof(int2) * cpair.size(), cudaMemcpyHostToDevice));
+  // the groups k_group_init has work for
+  {
+    std::vector<int> work;
+    for (int g = 0; g < ng; g++)
+      if (coff[g + 1] > coff[g] || boff[g + 1] > boff[g] || eoff[g + 1] > eoff[g]) work.push_back(g);
+    c->ngwork = (int)work.size();
+    CK(cudaMalloc(&c->grp_work, sizeof(int) * (work.empty() ? 1 : work.size())));
+    if (!work.empty()) CK(cudaMemcpy(c->grp_work, work.data(), sizeof(int) * work.size(), cudaMemcpyHostToDevice));
+  }
   if ((rc = upload_intra(c, ih, gid, ng))) return rc;
   return nvt_setup(c, systems, nsys);
 }
@@ -1299,12 +1309,18 @@ int group_init(Ctx *c, bool zero_fxs) {
   const int B = 128;
   cudaEvent_t e0;
   tbegin(c, 3, &e0);
-  k_group_init<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, zero_fxs ? 1 : 0, c->grp_atom_off, c->grp_atoms,
-                                                         c->pos, c->q, c->fxl, c->fxs, c->grp_ecorr_off,
-                                                         c->ecorr_ij, c->grp_bond_off, c->bond_ij, c->bond_p,
-                                                         c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc, c->sp,
-                                                         c->sys_of, c->gate);
-  c->launches++;
+  // the force arrays start from zero (a halted graph step zeroes them too:
+  // the host-driven path that finishes it computes them again from here)
+  CK(cudaMemsetAsync(c->fxl, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+  if (zero_fxs) CK(cudaMemsetAsync(c->fxs, 0, sizeof(double) * 3 * (size_t)c->n, c->st));
+  if (c->ngwork > 0) {
+    k_group_init<<<grid_for(c->ngwork, B), B, 0, c->st>>>(P, c->grp_work, c->ngwork, c->grp_atom_off, c->grp_atoms,
+                                                          c->pos, c->q, c->fxl, c->fxs, c->grp_ecorr_off,
+                                                          c->ecorr_ij, c->grp_bond_off, c->bond_ij, c->bond_p,
+                                                          c->grp_bend_off, c->bend_ijk, c->bend_p, c->acc, c->sp,
+                                                          c->sys_of, c->gate);
+    c->launches++;
+  }
   if (c->has_intra_x) {
     k_intra_energy<<<grid_for(c->ngroups, B), B, 0, c->st>>>(P, c->grp_atom_off, c->grp_atoms, c->pos, c->q,
                                                              c->intra, c->acc, c->sys_of, c->gate);
