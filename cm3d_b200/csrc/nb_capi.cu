@@ -317,6 +317,7 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
       return CM3D_NB_ERR_ARG;
     }
     // exclusion lists (CSR over global atom indices)
+    P.excl = P.cexcl = 0;
     for (int i = 0; i < ns; i++) {
       const int e0 = s->excl_off ? s->excl_off[i] : 0, e1 = s->excl_off ? s->excl_off[i + 1] : 0;
       for (int k = e0; k < e1; k++) eidx.push_back(a0 + s->excl_idx[k]);
@@ -324,6 +325,8 @@ static int create(const cm3d_nb_system *systems, int nsys, const cm3d_nb_options
       const int c0 = s->cexcl_off ? s->cexcl_off[i] : 0, c1 = s->cexcl_off ? s->cexcl_off[i + 1] : 0;
       for (int k = c0; k < c1; k++) cidx.push_back(a0 + s->cexcl_idx[k]);
       coff[a0 + i + 1] = (int)cidx.size();
+      if (e1 > e0) P.excl = 1;
+      if (c1 > c0) P.cexcl = 1;
     }
     // interactions: global indices inter0 + local, type map per system
     P.ntypes = s->ntypes;

@@ -70,6 +70,7 @@ struct SysP {
   int inter0, ninter;        // its interactions: global indices [inter0, inter0 + ninter)
   int coul;                  // Coulomb table index (tables at coul * ntable), -1: no charges
   int smallbox;              // box narrower than two list radii: minimum image per pair
+  int excl, cexcl;           // the system has LJ / Coulomb exclusions (0: the list tests skip them)
   int q0, nq;
   int krow0, nrows, kk0, ktot;   // k rows and k-vectors (global indices)
   int ktile0, ktiles;        // structure-factor tiles (global tile ids)

@@ -242,11 +242,11 @@ __device__ __forceinline__ int exact_flags(const SysP &P, int n, int i, int j, i
   const double ez = __dadd_rn(__dadd_rn(__dmul_rn(sx, P.h[6]), __dmul_rn(sy, P.h[7])), __dmul_rn(sz, P.h[8]));
   const double r2 = r2_ref(ex, ey, ez);
   int flags = 0;
-  if (lj_ok && r2 < icut[8 * intr + 5] && !excluded(i, j, excl_off, excl_idx)) {
+  if (lj_ok && r2 < icut[8 * intr + 5] && !(P.excl && excluded(i, j, excl_off, excl_idx))) {
     flags |= 1;
     if (r2 < icut[8 * intr + 4]) flags |= 2;
   }
-  if (el_ok && r2 < P.rmaxl_skin2_e && !excluded(i, j, cexcl_off, cexcl_idx)) {
+  if (el_ok && r2 < P.rmaxl_skin2_e && !(P.cexcl && excluded(i, j, cexcl_off, cexcl_idx))) {
     flags |= 4;
     if (r2 < P.rmaxs_skin2_e) flags |= 8;
   }
@@ -571,11 +571,11 @@ __device__ __forceinline__ int fast_flags(const SysP &P, int i, int j, int ti, i
     return r2f < R2;
   };
   int flags = 0;
-  if (lj_ok && below(icut[8 * intr + 5]) && !excluded(i, j, excl_off, excl_idx)) {
+  if (lj_ok && below(icut[8 * intr + 5]) && !(P.excl && excluded(i, j, excl_off, excl_idx))) {
     flags |= 1;
     if (below(icut[8 * intr + 4])) flags |= 2;
   }
-  if (el_ok && below(P.rmaxl_skin2_e) && !excluded(i, j, cexcl_off, cexcl_idx)) {
+  if (el_ok && below(P.rmaxl_skin2_e) && !(P.cexcl && excluded(i, j, cexcl_off, cexcl_idx))) {
     flags |= 4;
     if (below(P.rmaxs_skin2_e)) flags |= 8;
   }

@@ -852,7 +852,7 @@ __device__ __forceinline__ void ep_to_acc(int q, double s, double *acc, float ta
 // A batch's energy sums: one block per system adds up all its quantities in
 // one pass over its atoms (every quantity in a fixed order, as k_ereduce),
 // instead of a block per (quantity, system).
-constexpr int ERS_THREADS = 128;
+constexpr int ERS_THREADS = 256;
 
 __global__ void __launch_bounds__(ERS_THREADS) k_ereduce_sys(int n, int mask, const SysP *__restrict__ sp,
                                                               const float *__restrict__ epart,
@@ -869,6 +869,9 @@ __global__ void __launch_bounds__(ERS_THREADS) k_ereduce_sys(int n, int mask, co
   double s[EP_COUNT];
 #pragma unroll
   for (int q = 0; q < EP_COUNT; q++) s[q] = 0.0;
+  // (two atoms' loads in flight per thread: a large system's block is the
+  // longest)
+#pragma unroll 2
   for (int t = a0 + threadIdx.x; t < a1; t += blockDim.x) {
     const double h = (mask & 1) ? epart64[t] : 0.0;
 #pragma unroll
