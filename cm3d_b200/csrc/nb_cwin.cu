@@ -140,9 +140,7 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
         const uint32_t *in = front ? src : src + (stride - nb);   // the back segment ends at the slot's end
         unsigned short *out = reinterpret_cast<unsigned short *>(dst + (front ? 0 : nba * row));
         // every lane calls it (the delta comes by shuffle); -1 past the end
-        auto window_index = [&](int e, uint32_t &o) -> int {
-          const bool v = e < m;
-          const uint32_t en = v ? in[e] : 0u;
+        auto window_index_of = [&](bool v, uint32_t en, uint32_t &o) -> int {
           const int code = (en >> ENT_CODE_SHIFT) & 31;
           const int wi = (int)(en & ENT_JMASK) + __shfl_sync(0xffffffffu, delta, code);
           // inside the window by construction (a pair's shift code names
@@ -151,6 +149,10 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
           o = wi >= 0 && wi < tot ? (uint32_t)wi : dummy;
           if (front && (en & ENT_EL) && o != dummy) o |= CW_EL;
           return v ? (int)(o & 7u) : -1;
+        };
+        auto window_index = [&](int e, uint32_t &o) -> int {
+          const bool v = e < m;
+          return window_index_of(v, v ? in[e] : 0u, o);
         };
         // bank classes: the window slot mod 8 (the 16-byte bank group of
         // the staged position).  Position j of the segment is read by lane
@@ -161,13 +163,41 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
         // l + 32, ... after those of the lanes before it): each lane counts
         // its classes in 16-bit fields (classes 0-3 in c03, 4-7 in c47), one
         // warp scan gives the bases -- no warp vote per entry.
+        // a segment of up to CW_KEEP x 32 entries keeps its window indices
+        // in registers between the passes (16 bits each, two per register;
+        // 0xFFFF past the segment's end), with every entry's load issued
+        // up front; longer segments read the master list twice
+        constexpr int CW_KEEP = 24;
+        const bool kept = m <= 32 * CW_KEEP;
+        unsigned pk[CW_KEEP / 2];
         unsigned long long c03 = 0ull, c47 = 0ull;
-        for (int e0 = 0; e0 < m; e0 += 32) {
-          uint32_t o;
-          const int cl = window_index(e0 + lane, o);
-          if (cl >= 0) {
-            if (cl < 4) c03 += 1ull << (16 * cl);
-            else c47 += 1ull << (16 * (cl - 4));
+        auto count = [&](int cl) {
+          if (cl < 4) c03 += 1ull << (16 * cl);
+          else c47 += 1ull << (16 * (cl - 4));
+        };
+        if (kept) {
+          uint32_t en[CW_KEEP];
+#pragma unroll
+          for (int k = 0; k < CW_KEEP; k++) en[k] = k * 32 + lane < m ? in[k * 32 + lane] : 0u;
+#pragma unroll
+          for (int k = 0; k < CW_KEEP; k++) {
+            unsigned ok = 0xFFFFu;
+            if (k * 32 < m) {
+              uint32_t o;
+              const int cl = window_index_of(k * 32 + lane < m, en[k], o);
+              if (cl >= 0) {
+                ok = o;
+                count(cl);
+              }
+            }
+            if (k & 1) pk[k >> 1] |= ok << 16;
+            else pk[k >> 1] = ok;
+          }
+        } else {
+          for (int e0 = 0; e0 < m; e0 += 32) {
+            uint32_t o;
+            const int cl = window_index(e0 + lane, o);
+            if (cl >= 0) count(cl);
           }
         }
         unsigned long long i03 = c03, i47 = c47;
@@ -190,43 +220,54 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
         const int Q = m >> 3;
         // running ranks: this lane's bases, advanced per entry
         unsigned long long r03 = i03 - c03, r47 = i47 - c47;
-        for (int e0 = 0; e0 < m; e0 += 32) {
-          uint32_t o = dummy;
-          const int cl = window_index(e0 + lane, o);
-          if (cl >= 0) {
-            int rank;
-            if (cl < 4) {
-              rank = (int)((r03 >> (16 * cl)) & 0xFFFFull);
-              r03 += 1ull << (16 * cl);
-            } else {
-              rank = (int)((r47 >> (16 * (cl - 4))) & 0xFFFFull);
-              r47 += 1ull << (16 * (cl - 4));
-            }
-            int pos;
-            if (rank < Q) {
-              pos = cl + 8 * rank;
-            } else {
-              // the L-th free position: the unused class positions of the
-              // classes short of Q entries, in class order, then the tail
-              int L = rank - Q;
+        auto place = [&](int cl, uint32_t o) {
+          int rank;
+          if (cl < 4) {
+            rank = (int)((r03 >> (16 * cl)) & 0xFFFFull);
+            r03 += 1ull << (16 * cl);
+          } else {
+            rank = (int)((r47 >> (16 * (cl - 4))) & 0xFFFFull);
+            r47 += 1ull << (16 * (cl - 4));
+          }
+          int pos;
+          if (rank < Q) {
+            pos = cl + 8 * rank;
+          } else {
+            // the L-th free position: the unused class positions of the
+            // classes short of Q entries, in class order, then the tail
+            int L = rank - Q;
 #pragma unroll
-              for (int q = 0; q < 8; q++)
-                if (q < cl) L += max(0, cnt[q] - Q);
-              pos = -1;
+            for (int q = 0; q < 8; q++)
+              if (q < cl) L += max(0, cnt[q] - Q);
+            pos = -1;
 #pragma unroll
-              for (int q = 0; q < 8; q++) {
-                const int d = max(0, Q - cnt[q]);
-                if (pos < 0) {
-                  if (L < d) pos = q + 8 * (cnt[q] + L);
-                  else L -= d;
-                }
+            for (int q = 0; q < 8; q++) {
+              const int d = max(0, Q - cnt[q]);
+              if (pos < 0) {
+                if (L < d) pos = q + 8 * (cnt[q] + L);
+                else L -= d;
               }
-              if (pos < 0) pos = 8 * Q + L;
             }
-            // position -> (block, lane, k): 16-bit entry k of the block's
-            // word for lane r % row (row is 8 or 32: a power of two)
-            const int bb = pos / blk, r = pos - bb * blk;
-            out[(bb * row + (r & (row - 1))) * 4 + r / row] = (unsigned short)o;
+            if (pos < 0) pos = 8 * Q + L;
+          }
+          // position -> (block, lane, k): 16-bit entry k of the block's
+          // word for lane r % row (row is 8 or 32: a power of two)
+          const int bb = pos / blk, r = pos - bb * blk;
+          out[(bb * row + (r & (row - 1))) * 4 + r / row] = (unsigned short)o;
+        };
+        if (kept) {
+#pragma unroll
+          for (int k = 0; k < CW_KEEP; k++) {
+            if (k * 32 < m) {
+              const unsigned o = (k & 1) ? pk[k >> 1] >> 16 : pk[k >> 1] & 0xFFFFu;
+              if (o != 0xFFFFu) place((int)(o & 7u), o);
+            }
+          }
+        } else {
+          for (int e0 = 0; e0 < m; e0 += 32) {
+            uint32_t o = dummy;
+            const int cl = window_index(e0 + lane, o);
+            if (cl >= 0) place(cl, o);
           }
         }
       }
@@ -235,7 +276,7 @@ __device__ __forceinline__ void cw_convert_atom(const int t, const int lane, int
   }
 }
 
-__global__ void __launch_bounds__(256, 3) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words, int row,
+__global__ void __launch_bounds__(256, 2) k_cw_convert(int ncx, int ncy, int ncz, int cap, int n, int words, int row,
                                                     const int *__restrict__ cell_start,
                                                     const int *__restrict__ cell_of,
                                                     const int *__restrict__ sorig,
@@ -294,7 +335,7 @@ __global__ void __launch_bounds__(1024) k_cw_scan(int nsys, const SysP *__restri
 // A batch: warps walk the scanned range (a fixed grid, so that a captured
 // step converts whatever the device-side rebuild flags select); atom v of the
 // range lies in the last system s with scan[s] <= v, each on its own grid.
-__global__ void __launch_bounds__(256, 3) k_cw_convert_sys(int nsys, const int *__restrict__ scan,
+__global__ void __launch_bounds__(256, 2) k_cw_convert_sys(int nsys, const int *__restrict__ scan,
                                                         const SysP *__restrict__ sp, int cap, int n, int words,
                                                         int row, const int *__restrict__ cell_start,
                                                         const int *__restrict__ cell_of,

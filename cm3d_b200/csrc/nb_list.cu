@@ -171,10 +171,10 @@ __device__ __forceinline__ long long sort_key(const int *__restrict__ itype, int
   return ((long long)itype[i] << 32) | (unsigned)i;
 }
 
-constexpr int SORT_CELLS = 8;      // cells per block of k_cell_sort
+constexpr int SORT_CELLS = 8;      // most cells per block of k_cell_sort
 constexpr int SORT_THREADS = 128;
 
-__global__ void __launch_bounds__(SORT_THREADS) k_cell_sort(int ncells, const int *__restrict__ cell_sys,
+__global__ void __launch_bounds__(SORT_THREADS) k_cell_sort(int ncells, int per_block, const int *__restrict__ cell_sys,
                                                              const int *__restrict__ sreb, int all,
                                                              const int *__restrict__ cell_start,
                                                              const int *__restrict__ itype,
@@ -182,10 +182,11 @@ __global__ void __launch_bounds__(SORT_THREADS) k_cell_sort(int ncells, const in
                                                              const int *__restrict__ gate) {
   if (gated_off(gate, 1)) return;
   __shared__ long long s[1024];
-  // SORT_CELLS consecutive cells per block: a batch has tens of thousands of
-  // cells of a few atoms each
-  const int c_end = min(ncells, (blockIdx.x + 1) * SORT_CELLS);
-  for (int c = blockIdx.x * SORT_CELLS; c < c_end; c++) {
+  // per_block consecutive cells per block: up to SORT_CELLS where a batch has
+  // tens of thousands of cells of a few atoms each, one where a grid of few,
+  // crowded cells would otherwise leave most SMs idle
+  const int c_end = min(ncells, (blockIdx.x + 1) * per_block);
+  for (int c = blockIdx.x * per_block; c < c_end; c++) {
     if (sys_skip(cell_sys[c], sreb, all)) continue;     // whole blocks
     const int lo = cell_start[c], hi = cell_start[c + 1], m = hi - lo;
     if (m <= 1) continue;
@@ -1168,8 +1169,12 @@ int build_lists(Ctx *c, bool device_flag, bool all) {
   k_cell_scan<<<c->nsys, 256, 0, c->st>>>(c->sp, c->sreb, al, c->cell_cursor, c->cell_start, gate);
   k_cell_fill<<<grid_for(n, B), B, 0, c->st>>>(n, c->sys_of, c->sreb, al, c->cell_of, c->cell_start,
                                                 c->cell_cursor, c->cell_atoms, gate);
-  k_cell_sort<<<(c->ncells + SORT_CELLS - 1) / SORT_CELLS, SORT_THREADS, 0, c->st>>>(
-      c->ncells, c->cell_sys, c->sreb, al, c->cell_start, c->itype, c->cell_atoms, gate);
+  {
+    // enough blocks for four per SM where the grid allows it
+    const int per_block = std::max(1, std::min(SORT_CELLS, c->ncells / std::max(1, 4 * c->num_sms)));
+    k_cell_sort<<<(c->ncells + per_block - 1) / per_block, SORT_THREADS, 0, c->st>>>(
+        c->ncells, per_block, c->cell_sys, c->sreb, al, c->cell_start, c->itype, c->cell_atoms, gate);
+  }
   k_sorted_init<<<grid_for(n, B), B, 0, c->st>>>(n, c->sp, c->sys_of, c->sreb, al, c->cell_atoms, cimg, c->itype,
                                                   c->pos, c->q, c->rank, c->styp, c->corner, c->xq, gate);
   c->launches += 6;
