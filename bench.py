@@ -267,6 +267,21 @@ def roofline(eng, steps: int, istep0: int, fp32_tflops: float, hbm_gbs: float) -
     return out
 
 
+def compact_roofline(systems, device: int, name: str, fp32: float, hbm: float) -> dict:
+    """The compact pair kernel's roofline on a one-system workload (cell
+    scale 1.0, the kernel the context takes by default), from eager launches
+    timed with CUDA events as in roofline()."""
+    from cm3d_b200 import _abi
+    from cm3d_b200.engine import Engine
+    eng = Engine(systems, mode=_abi.MIXED, device=device, tpa=32)
+    eng.workload_name = name
+    eng.step_init()
+    eng.step(1, 5)
+    out = roofline(eng, 20, 6, fp32, hbm)
+    eng.close()
+    return out
+
+
 # ------------------------------------------------------------ CPU baseline
 def ref_bench_bin() -> str | None:
     p = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
@@ -661,6 +676,11 @@ def main() -> None:
                 "plain_fp64": wplain, "speedup_mixed_vs_plain": (wval / wplain["value"]) if wplain else None,
                 "roofline": wm["roofline"], "autotune": wm["autotune"],
                 "status": {k: wm["status"][k] for k in ("rebuilds", "resets", "table_underflow")}}
+            if wname == "water331776" and wm["autotune"].get("kernel") != "compact":
+                # the step's fastest choice is another kernel (the step is
+                # bound by the reciprocal space on its side stream): the
+                # compact pair kernel's own roofline, measured the same way
+                other[wname]["roofline_compact"] = compact_roofline(wsys, local, wname, fp32, hbm)
         other["abutane1024"] = intra_arm(local, 1024, 200, 10, flush)
 
     nve = None
