@@ -186,21 +186,22 @@ def e2e_run(eng, steps: int, istep0: int, n: int) -> tuple[float, int, int]:
     """The public API with host buffers: every step uploads positions and
     velocities from pinned host memory, runs one step, and reads positions,
     velocities and every system's energies back (CM3D's host loop owning the
-    state)."""
+    state).  The host arrays are registered as the step's outputs
+    (cm3d_nb_set_host_outputs), so the positions come back while the step's
+    forces are computed; cm3d_nb_step_host uploads the inputs and runs the
+    step."""
     px, vx = [pinned(3 * n).reshape(3, n) for _ in range(2)]
     px[:] = eng.positions()
     vx[:] = eng.velocities()
     etab = eng.energies_table()
+    eng.set_host_outputs(px, vx)
     eng.synchronize()
     t0 = time.perf_counter()
     for s in range(steps):
-        eng.set_positions(px)
-        eng.set_velocities(vx)
-        eng.step(istep0 + s, 1)
-        eng.positions(out=px)
-        eng.velocities(out=vx)
+        eng.step_host(istep0 + s, px, vx)
         eng.energies_table(out=etab)
     dt = time.perf_counter() - t0
+    eng.set_host_outputs(None, None)
     h2d = 2 * 3 * n * 8
     d2h = 2 * 3 * n * 8 + 144 * 8 * eng.nsys     # + every system's accumulator block (ACC_STRIDE doubles)
     return dt, h2d, d2h

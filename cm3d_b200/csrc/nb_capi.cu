@@ -115,6 +115,9 @@ static void destroy(Ctx *c) {
   if (c->st2) cudaStreamDestroy(c->st2);
   if (c->ev_fork) cudaEventDestroy(c->ev_fork);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st3) cudaStreamDestroy(c->st3);
+  if (c->ev_f3) cudaEventDestroy(c->ev_f3);
+  if (c->ev_j3) cudaEventDestroy(c->ev_j3);
   delete c;
 }
 
@@ -912,6 +915,48 @@ int cm3d_nb_step_init(cm3d_nb_ctx *ctx) {
 int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps) {
   CTX;
   return run_step(c, istep0, nsteps);
+}
+
+int cm3d_nb_set_host_outputs(cm3d_nb_ctx *ctx, double *pos_out, double *vel_out) {
+  CTX;
+  DevLock lock(device_mutex());
+  if (c->pending) {
+    set_error("set_host_outputs: asynchronous steps are in flight (cm3d_nb_step_wait first)");
+    return CM3D_NB_ERR_STATE;
+  }
+  for (double *p : {pos_out, vel_out}) {
+    if (!p) continue;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      set_error("set_host_outputs: %p is not page-locked host memory (cudaMallocHost / cudaHostRegister)", (void *)p);
+      return CM3D_NB_ERR_ARG;
+    }
+  }
+  if ((pos_out || vel_out) && !c->st3) {
+    CK(cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->ev_f3, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->ev_j3, cudaEventDisableTiming));
+  }
+  c->ho_pos = pos_out;
+  c->ho_vel = vel_out;
+  if (c->graph) {                           // captured with the old outputs
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return CM3D_NB_OK;
+}
+
+int cm3d_nb_step_host(cm3d_nb_ctx *ctx, int istep0, const double *pos_in, const double *vel_in) {
+  CTX;
+  if (c->pending) {
+    set_error("step_host: asynchronous steps are in flight (cm3d_nb_step_wait first)");
+    return CM3D_NB_ERR_STATE;
+  }
+  const size_t b = sizeof(double) * 3 * (size_t)c->n;
+  if (pos_in) CK(cudaMemcpyAsync(c->pos, pos_in, b, cudaMemcpyHostToDevice, c->st));
+  if (vel_in) CK(cudaMemcpyAsync(c->vel, vel_in, b, cudaMemcpyHostToDevice, c->st));
+  return run_step(c, istep0, 1);
 }
 
 int cm3d_nb_step_async(cm3d_nb_ctx *ctx, int istep0, int nsteps) {

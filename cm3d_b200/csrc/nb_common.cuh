@@ -277,6 +277,13 @@ struct Ctx {
   cudaStream_t st = nullptr;
   cudaStream_t st2 = nullptr;                // side stream: force(1)'s k-space beside the list build
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // registered page-locked host outputs (cm3d_nb_set_host_outputs): every
+  // step copies its final positions (on st3, beside the rest of the step)
+  // and velocities there
+  double *ho_pos = nullptr, *ho_vel = nullptr;
+  cudaStream_t st3 = nullptr;
+  cudaEvent_t ev_f3 = nullptr, ev_j3 = nullptr;
+  bool ho_forked = false;
   int mode = CM3D_NB_MIXED;
   int need_short = 0;
   int tpa = 0;
@@ -510,7 +517,8 @@ void cw_set_split(Ctx *c, int nsplit);          // nb_cwin.cu
 constexpr int CM3D_CW_ROW = 32;                 // compact-list rows (lanes per atom) of k_pair_cw
 constexpr int CM3D_CS_LPA = 8;                  //   and of k_pair_cs
 constexpr int CM3D_CS_THREADS = 512;            // k_pair_cs block: four groups of four warps
-int cw_set_row(Ctx *c, int row);                // nb_cwin.cu: a batch's list layout, 32 or 8 lanes per atom
+int cw_set_row(Ctx *c, int row);
+int host_outputs_tail(Ctx *c);                  // nb_step.cu: end of a step with registered host outputs                // nb_cwin.cu: a batch's list layout, 32 or 8 lanes per atom
 int cw_convert(Ctx *c, bool device_flag, bool all);   // nb_cwin.cu: master list -> compact list
 void cw_destroy(Ctx *c);                        // nb_cwin.cu: host-side group data
 bool cw_applies(Ctx *c, int iflg, bool ns);     // nb_cwin.cu

@@ -1469,6 +1469,16 @@ static int one_level(Ctx *c, int intr, bool gated) {
   tend(c, 3, e0);
   CKL(c);
   if ((rc = reset_positions(c))) return rc;
+  if (intr == c->nres_lrf - 1 && c->ho_pos) {
+    // the step's positions are final: their copy to the registered host
+    // buffer runs on a third stream beside the rest of the step (joined at
+    // the step's end)
+    CK(cudaEventRecord(c->ev_f3, c->st));
+    CK(cudaStreamWaitEvent(c->st3, c->ev_f3, 0));
+    CK(cudaMemcpyAsync(c->ho_pos, c->pos, sizeof(double) * 3 * (size_t)c->n, cudaMemcpyDeviceToHost, c->st3));
+    CK(cudaEventRecord(c->ev_j3, c->st3));
+    c->ho_forked = true;
+  }
   // the positions are final for this level: force(1)'s k-space can start on
   // the side stream while the lists are rebuilt and the pair forces run
   const bool fork = intr == c->nres_lrf - 1 && kspace_async_ok(c);
@@ -1493,12 +1503,24 @@ static int one_step(Ctx *c, bool gated) {
     int rc = one_level(c, intr, gated);
     if (rc) return rc;
   }
-  return CM3D_NB_OK;
+  return host_outputs_tail(c);
 }
 
 static int set_istep(Ctx *c, int istep) {
   c->h_istate[IS_ISTEP] = istep;
   CK(cudaMemcpyAsync(c->istate + IS_ISTEP, c->h_istate + IS_ISTEP, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  return CM3D_NB_OK;
+}
+
+// the end of a step with registered host outputs: join the positions' copy
+// and copy the velocities
+int host_outputs_tail(Ctx *c) {
+  if (c->ho_forked) {
+    CK(cudaStreamWaitEvent(c->st, c->ev_j3, 0));
+    c->ho_forked = false;
+  }
+  if (c->ho_vel)
+    CK(cudaMemcpyAsync(c->ho_vel, c->vel, sizeof(double) * 3 * (size_t)c->n, cudaMemcpyDeviceToHost, c->st));
   return CM3D_NB_OK;
 }
 
@@ -1565,7 +1587,12 @@ int launch_steps(Ctx *c, int istep0, int nsteps) {
 // buffers, finish the step on the host-driven path and run the rest.
 int finish_steps(Ctx *c) {
   int rc;
-  if (!c->pending) return CM3D_NB_OK;
+  if (!c->pending) {
+    // eager steps ran here already; their copies to registered host
+    // outputs may still be in flight
+    if (c->ho_pos || c->ho_vel) CK(cudaStreamSynchronize(c->st));
+    return CM3D_NB_OK;
+  }
   CK(cudaEventSynchronize(c->step_ev));
   c->pending = false;
   if (!c->h_istate[IS_HALT]) return CM3D_NB_OK;
@@ -1577,6 +1604,10 @@ int finish_steps(Ctx *c) {
   if ((rc = close_level(c, intr))) return rc;
   for (int lv = intr + 1; lv < c->nres_lrf; lv++)
     if ((rc = one_level(c, lv, false))) return rc;
+  // the halted step copied its positions (final before its list build) and
+  // stale velocities: the step's outputs again, complete before returning
+  if ((rc = host_outputs_tail(c))) return rc;
+  if (c->ho_pos || c->ho_vel) CK(cudaStreamSynchronize(c->st));
   if (c->graph) cudaGraphExecDestroy(c->graph);   // it holds the old buffer addresses
   c->graph = nullptr;
   int done = failed + 1 - istep0;

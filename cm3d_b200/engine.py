@@ -89,6 +89,8 @@ def load_library() -> C.CDLL:
         "cm3d_nb_step_init": (C.c_int, [vp]),
         "cm3d_nb_step": (C.c_int, [vp, C.c_int, C.c_int]),
         "cm3d_nb_step_async": (C.c_int, [vp, C.c_int, C.c_int]),
+        "cm3d_nb_set_host_outputs": (C.c_int, [vp, dp, dp]),
+        "cm3d_nb_step_host": (C.c_int, [vp, C.c_int, dp, dp]),
         "cm3d_nb_step_query": (C.c_int, [vp, ip]),
         "cm3d_nb_step_wait": (C.c_int, [vp]),
         "cm3d_nb_get_energies": (C.c_int, [vp, C.POINTER(_abi.Energies)]),
@@ -359,6 +361,32 @@ class Engine:
     def step_async(self, istep0: int, nsteps: int = 1) -> None:
         """launch the steps and return (cm3d_nb_step_async)"""
         check(load_library().cm3d_nb_step_async(self._h, istep0, nsteps), "step_async")
+
+    def set_host_outputs(self, pos_out=None, vel_out=None) -> None:
+        """register page-locked (3, n) float64 arrays that every later step
+        fills with its final positions and velocities (cm3d_nb_set_host_outputs;
+        None for both stops it); the arrays must stay alive while registered"""
+        self._host_out = (pos_out, vel_out)
+
+        def ptr(a):
+            if a is None:
+                return None
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != 3 * self.n:
+                raise EngineError("host outputs: C-contiguous float64 arrays of 3 x natoms")
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+        check(load_library().cm3d_nb_set_host_outputs(self._h, ptr(pos_out), ptr(vel_out)), "set_host_outputs")
+
+    def step_host(self, istep0: int, pos_in=None, vel_in=None) -> None:
+        """copy the (3, n) float64 host arrays in (page-locked for an
+        asynchronous copy; None keeps the device's) and run one step
+        (cm3d_nb_step_host); registered outputs are complete on return"""
+        def ptr(a):
+            if a is None:
+                return None
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.size != 3 * self.n:
+                raise EngineError("step_host: C-contiguous float64 arrays of 3 x natoms")
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+        check(load_library().cm3d_nb_step_host(self._h, istep0, ptr(pos_in), ptr(vel_in)), "step_host")
 
     def step_done(self) -> bool:
         """non-blocking: have the launched steps completed?"""

@@ -305,8 +305,10 @@ int cm3d_nb_getvewald(cm3d_nb_ctx *ctx, double *pot_ewald, double *prs_ewald,
                      energies. */
 int cm3d_nb_step_init(cm3d_nb_ctx *ctx);
 /* step()            integrate/md_step.c:62, nsteps times starting at
-                     SIMPARMS.istep = istep0 (NVE; torsions, thermostats and
-                     barostats are not part of the engine). */
+                     SIMPARMS.istep = istep0 (NVE, or NVT with the Nose-Hoover
+                     chains of cm3d_nb_system; a barostat stays with CM3D's
+                     host integrator, the engine following its box through
+                     cm3d_nb_set_box). */
 int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps);
 /* The same steps without waiting (no CM3D counterpart): cm3d_nb_step_async
    launches them on the context's stream and returns, so that several
@@ -317,6 +319,20 @@ int cm3d_nb_step(cm3d_nb_ctx *ctx, int istep0, int nsteps);
 int cm3d_nb_step_async(cm3d_nb_ctx *ctx, int istep0, int nsteps);
 int cm3d_nb_step_query(cm3d_nb_ctx *ctx, int *done);
 int cm3d_nb_step_wait(cm3d_nb_ctx *ctx);
+/* A host loop that owns the positions and velocities (CM3D's, which reads
+   them after every step) without a round trip per array (no CM3D
+   counterpart).  cm3d_nb_set_host_outputs registers page-locked host
+   buffers (cudaMallocHost / cudaHostRegister; 3 natoms doubles each, x | y |
+   z blocks, either may be NULL; NULL for both stops it): every later step
+   copies its final positions there as soon as they are final -- on a
+   separate stream, beside the step's list build and forces -- and its
+   velocities at its end, complete when the step call returns.
+   cm3d_nb_step_host copies pos_in and vel_in (x | y | z blocks, page-locked
+   for an asynchronous copy; either may be NULL to keep the device's) to the
+   device and runs one step (SIMPARMS.istep = istep0).  The input and output
+   buffers may be the same. */
+int cm3d_nb_set_host_outputs(cm3d_nb_ctx *ctx, double *pos_out, double *vel_out);
+int cm3d_nb_step_host(cm3d_nb_ctx *ctx, int istep0, const double *pos_in, const double *vel_in);
 /* getvireal(...,1)+geteng() md_fcntr.c:136,259 from the device accumulators */
 int cm3d_nb_get_energies(cm3d_nb_ctx *ctx, cm3d_nb_energies *e);
 
