@@ -677,7 +677,8 @@ __global__ void __launch_bounds__(256, NEED_S ? 2 : 3) k_pair_mixed(
         for (int u = 0; u < PU; u++) {
           const int j = en[u] & ENT_JMASK;
           xj[u] = xq[j];
-          tj[u] = (en[u] & fl_lj) ? styp[j] : 0;
+          // (a one-type system's j is type 0: no load)
+          tj[u] = (ntyp > 1 && (en[u] & fl_lj)) ? styp[j] : 0;
         }
 #pragma unroll
         for (int u = 0; u < PU; u++)
