@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(256) k_list_half(
 template <class Decide>
 __device__ __forceinline__ void walk_staged(int t, float4 xi4, float lim2, const float4 *s_x, const int *s_u,
                                             int cnt, int *qbuf, float *qr, Decide &decide, const int *s_off,
-                                            const int *s_code, int nw, bool prune, float3 cw, int kt = -1) {
+                                            const int *s_code, int nw, bool prune, float3 cw) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   unsigned vis = nw >= 32 ? 0xffffffffu : (1u << nw) - 1u;
@@ -521,11 +521,10 @@ __device__ __forceinline__ void walk_staged(int t, float4 xi4, float lim2, const
     float r2f = 0.f;
     if (k < b) {
       const float4 xs = s_x[k];
+      const int u = s_u[k] & (int)ENT_JMASK;
       const float dx = xi4.x - xs.x, dy = xi4.y - xs.y, dz = xi4.z - xs.z;
       r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      // the atom itself: its staged index kt where it is staged once (3 or
-      // more cells per axis), else every staged copy of its sorted index
-      keep = r2f < lim2 && (kt >= 0 ? k != kt : (s_u[k] & (int)ENT_JMASK) != t);
+      keep = u != t && r2f < lim2;
     }
     const unsigned bk = __ballot_sync(0xffffffffu, keep);
     if (keep) {
@@ -606,7 +605,7 @@ __device__ __forceinline__ void full_list_atom(
     uint32_t *__restrict__ nbr, int *__restrict__ nlen, long long *__restrict__ stat, int *__restrict__ halt,
     int *qbuf, float *qr, const float4 *s_x, const int *s_u, const int *s_j, int scnt,
     bool fast, const int *s_off = nullptr, const int *s_code = nullptr, int nw = 0, bool prune = false,
-    float3 cw = make_float3(0.f, 0.f, 0.f), int kt = -1) {
+    float3 cw = make_float3(0.f, 0.f, 0.f)) {
   const int lane = threadIdx.x & 31;
   const unsigned lt_mask = (1u << lane) - 1u;
   const int i = cell_atoms[t];
@@ -676,7 +675,7 @@ __device__ __forceinline__ void full_list_atom(
     na += __popc(ba);
     nb += __popc(bb);
   };
-  if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide, s_off, s_code, nw, prune, cw, kt);
+  if (STAGED) walk_staged(t, xq[t], P.lim2, s_x, s_u, scnt, qbuf, qr, decide, s_off, s_code, nw, prune, cw);
   else walk_candidates(P, i, ci, xq[t], false, cell_atoms, cell_start, xq, qbuf, decide, fast ? qr : nullptr,
                        prune, cw, t);
   const int count = na + nb;
@@ -799,7 +798,7 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
   int *s_j = s_u + cap;                                  // cap: atom index
   __shared__ int qs[LW_THREADS / 32][LQ];
   __shared__ float qrs[LW_THREADS / 32][LQ];
-  __shared__ int s_cs[27], s_off[27], s_code[27], s_tot, s_nw, s_home;
+  __shared__ int s_cs[27], s_off[27], s_code[27], s_tot, s_nw;
   __shared__ float4 s_sh[27];
   const int warp = threadIdx.x >> 5;
   const int total = rb_scan[nsys];
@@ -845,8 +844,6 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
         if (w >= o) incl += v;
       }
       if (w < nw) s_off[w] = incl - cn;
-      // the home cell (zero shift): its first staged index
-      if (w < nw && s_code[w] == 13) s_home = incl - cn;
       if (w == 31) {
         s_nw = nw;
         s_tot = incl;
@@ -884,8 +881,7 @@ __global__ void __launch_bounds__(LW_THREADS) k_list_win(
       if (staged)
         full_list_atom<true>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                              excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], qrs[warp], s_x,
-                             s_u, s_j, tot, fast, s_off, s_code, nw, fast && ortho && nw == 27, cw,
-                             fast ? s_home + (t - lo) : -1);
+                             s_u, s_j, tot, fast, s_off, s_code, nw, fast && ortho && nw == 27, cw);
       else
         full_list_atom<false>(P, n, t, stride, cell_atoms, cell_start, xq, pos, itype, map, icut, q, excl_off,
                               excl_idx, cexcl_off, cexcl_idx, cimg, nbr, nlen, stat, halt, qs[warp], nullptr,
