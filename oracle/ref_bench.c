@@ -1,6 +1,6 @@
 /*
- * ref_bench.c -- times CM3D's own MD step on the host.  TEST / BASELINE
- * INFRASTRUCTURE ONLY: bench.py's CPU-baseline leg runs it; it is compiled
+ * ref_bench.c -- times CM3D's own MD step on the host.  Test and
+ * CPU-timing infrastructure only: bench.py's CPU-baseline leg runs it; it is compiled
  * against the reference's headers and linked against the reference's
  * archives (oracle/Makefile), never part of the product.
  *
