@@ -468,10 +468,16 @@ def tune_cell_scale(systems, device: int = 0, scales=(1.0, 1.25), steps: int = 2
                       "cells": tune["cells"], "compact_split": tune["compact_split"],
                       "compact_block_threads": tune["compact_block_threads"],
                       "pair_ms": float(min(tune["ms_per_launch"].values()))}
-    fastest = min(v["ms_per_step"] for v in out.values())
-    ties = [k for k in out if out[k]["ms_per_step"] <= 1.02 * fastest]
-    best = min(ties, key=lambda k: (out[k]["pair_ms"], out[k]["ms_per_step"]))
-    return {"cell_scale": best, "candidates": out}
+    return {"cell_scale": pick_cell_scale(out), "candidates": out}
+
+
+def pick_cell_scale(candidates: dict, tie: float = 0.02):
+    """The cell scale of the fastest step among `candidates` ({scale:
+    {"ms_per_step", "pair_ms"}}); steps within `tie` of the fastest count as
+    equal and go to the faster pair kernel (then the faster step)."""
+    fastest = min(v["ms_per_step"] for v in candidates.values())
+    ties = [k for k in candidates if candidates[k]["ms_per_step"] <= (1.0 + tie) * fastest]
+    return min(ties, key=lambda k: (candidates[k]["pair_ms"], candidates[k]["ms_per_step"]))
 
 
 def lj_table(eps, sig, rmin, rmax, rres, rheal, skin, ntable, shift):
